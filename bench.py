@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 supernodal Cholesky: seconds to relative residual <= 1e-10 for the FP64
+direct solve of K u = f on a 48^3 hex8 block (345 744 free DOFs, per-element lognormal E, 64
+Gaussian top-face load cases), the workload BASELINE.json quotes its FP64-on-GPU metric on.
+
+One step = the numeric factorisation of K (values already in HBM), the solve of the 64
+right-hand sides, and the residual check ||f - K u|| / ||f|| of every one of them on the device.
+`value` is the mean seconds per step (lower is better). `e2e` is the same step through the public
+C ABI with host buffers (values and right-hand sides copied in, solutions copied out).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+With N > 1 (torchrun), every rank solves its own replica (the path does not shard: replicas only)
+and the slowest rank's time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "s to rel-res 1e-10: FP32+IR & NN-FCG vs FP64 GPU Cholesky; TFLOP/s, GB/s"
+UNIT = "s"
+N_EL, NRHS, SEED = 48, 64, 2024
+SAMPLE_EL = 24  # the CPU baseline's bounded sample: the same generator at 24^3 elements
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n-el", type=int, default=N_EL)
+    ap.add_argument("--nrhs", type=int, default=NRHS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="a short run for ncu (no baselines, no e2e)")
+    return ap.parse_args()
+
+
+def factor_flops(problem):
+    """Sum of squared column counts of L (the Davis convention the metric's TFLOP/s uses)."""
+    from fieldcraft_b200 import Symbolic
+    a = Symbolic(problem.upper(), 2**62).arrays()
+    w = np.diff(a["first"])
+    m = np.diff(a["rptr"])
+    tot = 0.0
+    for mm, ww in zip(m, w):
+        c = mm - np.arange(ww, dtype=np.float64)
+        tot += float(np.dot(c, c))
+    return tot, int(a["entries"])
+
+
+def oracle_time(problem, threads: int):
+    """The oracle (the reference's CPU algorithm restated) on the host cores: analysis excluded,
+    numeric factorisation + solve of the right-hand sides, seconds."""
+    from oracle import oracle
+    oracle.set_threads(threads)
+    up = problem.upper()
+    s = oracle.Sym(up.n, up.ptr, up.idx)
+    t0 = time.perf_counter()
+    f = oracle.Fac(s, up.val)
+    x = f.solve(problem.rhs.copy())
+    t1 = time.perf_counter()
+    r = np.stack([oracle.spmv(problem.n, problem.csr.ptr, problem.csr.idx, problem.csr.val, x[:, j])
+                  for j in range(x.shape[1])], axis=1) - problem.rhs
+    relres = float(np.max(np.linalg.norm(r, axis=0) / np.linalg.norm(problem.rhs, axis=0)))
+    return t1 - t0, relres
+
+
+def cpu_baseline_sample(full_flops, threads):
+    """Seconds the oracle would take on the full workload, from a bounded sample: the same
+    generator at SAMPLE_EL^3 elements (factor + 64 solves), scaled by the ratio of factor flops."""
+    from fieldcraft_b200 import problems
+    sample = problems.lognormal_block(SAMPLE_EL, nrhs=NRHS, seed=SEED)
+    sflops, _ = factor_flops(sample)
+    t, relres = oracle_time(sample, threads)
+    return {
+        "value": t * full_flops / sflops,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "port",
+        "sample": f"oracle factor + {NRHS} solves of the {SAMPLE_EL}^3 block (n={sample.n}, "
+                  f"{sflops:.3e} flops) took {t:.3f} s on {threads} threads; scaled by factor flops "
+                  f"{full_flops:.3e}/{sflops:.3e}; sample rel-res {relres:.1e}",
+        "sample_seconds": t,
+    }
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dgemm_peak(torch):
+    """Measured FP64 peak: cuBLAS DGEMM 8192^3 (torch.matmul), best of 5, TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU algorithm (the oracle restatement; the Rust reference
+    cannot be built here) on the host cores, per step a bounded sample of the workload scaled to it."""
+    if rank != 0:
+        return
+    from fieldcraft_b200 import problems
+    threads = os.cpu_count() or 1
+    full = problems.lognormal_block(args.n_el, nrhs=args.nrhs, seed=SEED)
+    full_flops, _ = factor_flops(full)
+    del full
+    times = []
+    for it in range(args.warmup + args.steps):
+        cb = cpu_baseline_sample(full_flops, threads)
+        if it >= args.warmup:
+            times.append(cb["value"])
+    value = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"FP64 direct solve, hex8 block {args.n_el}^3 lognormal E, {args.nrhs} RHS",
+                   "n": None, "nrhs": args.nrhs},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    line["cpu_baseline"]["value"] = value
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    from fieldcraft_b200 import Factor, Symbolic, _lib, problems
+    from fieldcraft_b200.cholesky import Status, raise_for
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    lib = _lib.load()
+    p = problems.lognormal_block(args.n_el, nrhs=args.nrhs, seed=SEED + rank)
+    up = p.upper()
+    full_flops, entries = factor_flops(p)
+    sym = Symbolic(up, 2**62)
+    f = Factor(sym, device=local)
+    stream = torch.cuda.Stream()
+    f.set_stream(stream.cuda_stream)
+    n, R = p.n, args.nrhs
+    d_val = torch.from_numpy(up.val).cuda()
+    d_ptr = torch.from_numpy(p.csr.ptr).cuda()
+    d_idx = torch.from_numpy(p.csr.idx).cuda()
+    d_kv = torch.from_numpy(p.csr.val).cuda()
+    d_f = torch.from_numpy(np.ascontiguousarray(p.rhs.T)).cuda()  # [R, n]: column j of the n x R block
+    d_x = torch.empty_like(d_f)
+    d_r = torch.empty_like(d_f)
+    fnorm = torch.linalg.vector_norm(d_f, dim=1)
+    st = Status()
+
+    def step():
+        with torch.cuda.stream(stream):
+            rc = lib.fc_chol_factor_device_async(f.handle, C.c_void_p(d_val.data_ptr()), up.val.size)
+            assert rc == 0
+            d_x.copy_(d_f)
+            rc = lib.fc_chol_solve_device_async(f.handle, C.c_void_p(d_x.data_ptr()), R, n)
+            assert rc == 0
+            lib.fc_csr_spmv_device(n, C.c_void_p(d_ptr.data_ptr()), C.c_void_p(d_idx.data_ptr()),
+                                   C.c_void_p(d_kv.data_ptr()), C.c_void_p(d_x.data_ptr()),
+                                   C.c_void_p(d_r.data_ptr()), R, n, C.c_void_p(stream.cuda_stream))
+            d_r.sub_(d_f)
+            return torch.linalg.vector_norm(d_r, dim=1) / fnorm
+
+    for _ in range(args.warmup):
+        relres = step()
+    stream.synchronize()
+    lib.fc_chol_check(f.handle, C.byref(st))
+    raise_for(st)
+    launches_per_step = f.stat(7) + f.stat(8) + 1
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            relres = step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    lib.fc_chol_check(f.handle, C.byref(st))
+    raise_for(st)
+    worst = float(relres.max().item())
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+    if rank != 0 or args.profile_only:
+        if rank == 0:
+            print(json.dumps({"profile_only": True, "ms_per_step": ms, "relres_max": worst}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # per-kernel times on the same stream (events around every launch), one profiled step
+    kinds = 24
+    ms_k = np.zeros(kinds)
+    cnt_k = np.zeros(kinds, np.int64)
+    lib.fc_chol_profile(f.handle, 1)
+    step()
+    lib.fc_chol_profile_read(f.handle, ms_k.ctypes.data, cnt_k.ctypes.data, kinds)
+    lib.fc_chol_profile(f.handle, 0)
+    gemm_ms = ms_k[3]
+    gemm_flops = float(f.stat(9))
+    peak = dgemm_peak(torch)
+    achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
+    factor_ms = float(ms_k[0:4].sum())
+    solve_ms = float(ms_k[16:24].sum())
+    traffic = None
+    tf = ROOT / "profiles" / "gemm_kernel_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+
+    # end to end through the public API with pinned host buffers
+    hv = torch.from_numpy(up.val).pin_memory()
+    hb = torch.from_numpy(np.asfortranarray(p.rhs).T.copy()).pin_memory()  # [R, n] contiguous = column-major n x R
+    hx = torch.empty_like(hb).pin_memory()
+    e2e = []
+    for it in range(2 + args.steps):
+        hx.copy_(hb)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = lib.fc_chol_factor(f.handle, C.c_void_p(hv.data_ptr()), up.val.size, None, C.byref(st))
+        raise_for(st)
+        rc = lib.fc_chol_solve(f.handle, C.c_void_p(hx.data_ptr()), R, n, C.byref(st))
+        raise_for(st)
+        t1 = time.perf_counter()
+        if it >= 2:
+            e2e.append(t1 - t0)
+    e2e_s = float(np.mean(e2e))
+    xr = hx.numpy()
+    rr = np.stack([np.linalg.norm(p.rhs[:, j]) for j in range(R)])
+    # residual of the e2e result on the device (the same SpMV)
+    d_x.copy_(hx.cuda())
+    lib.fc_csr_spmv_device(n, C.c_void_p(d_ptr.data_ptr()), C.c_void_p(d_idx.data_ptr()), C.c_void_p(d_kv.data_ptr()),
+                           C.c_void_p(d_x.data_ptr()), C.c_void_p(d_r.data_ptr()), R, n, None)
+    torch.cuda.synchronize()
+    e2e_res = float(((d_r - d_f).norm(dim=1) / fnorm).max().item())
+
+    cb = None
+    if not args.no_cpu_baseline:
+        cb = cpu_baseline_sample(full_flops, os.cpu_count() or 1)
+        cb.pop("sample_seconds", None)
+    line = {
+        "metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal E, Gaussian loads)",
+        "config": {"workload": f"FP64 direct solve, hex8 block {args.n_el}^3 lognormal E (sigma 0.5), z=0 clamped, "
+                               f"{R} Gaussian top-face RHS", "n": n, "nnz": int(p.csr.idx.size), "nrhs": R,
+                   "factor_entries": entries, "factor_flops": full_flops, "supernodes": f.stat(4),
+                   "levels": f.stat(0), "l2": "inputs larger than L2 (L alone is %.1f GB)" % (f.stat(2) / 1e9),
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "relres_max": worst, "relres_target": 1e-10, "solved": worst <= 1e-10,
+        "factor_tflops": full_flops / (factor_ms * 1e-3) / 1e12 if factor_ms > 0 else None,
+        "phase_ms": {"factor": factor_ms, "solve": solve_ms,
+                     "by_kernel": {name: round(float(ms_k[k]), 3) for k, name in
+                                   [(0, "assemble"), (1, "potrf"), (2, "trsm"), (3, "gemm"), (19, "solve_gemm"),
+                                    (20, "solve_assemble"), (21, "solve_gather"), (22, "trsv"), (23, "trsv_t")]}},
+        "roofline": {"kernel": "gemm_kernel (FP64 DMMA, factor updates)", "bound": "tensor",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
+                                                        "has no FP64 figure)",
+                     "algorithmic": "useful flops of the factor's GEMM tasks (2 K per lower-triangle output)",
+                     "flops_per_step": gemm_flops, "ms_per_step": float(gemm_ms), "launches": int(cnt_k[3])},
+        "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(up.val.nbytes + hb.numel() * 8),
+                "d2h_bytes_per_step": int(hx.numel() * 8 + 32), "relres_max": e2e_res},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "clocks": clocks,
+    }
+    if cb is not None:
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+    f.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

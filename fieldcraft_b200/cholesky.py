@@ -1,0 +1,278 @@
+"""The reference's Cholesky API for this path, on a B200.
+
+Mirrors ``crates/solver/src/cholesky.rs`` of FieldCraft 0.8.1: ``UpperColumns`` (:102-145),
+``Factor::new`` (:1545), ``Factor::entries`` (:1557), ``Factor::solve`` (:1562),
+``Factor::solve_many`` (:1568) and ``FactorError`` (:346-361), with the same argument meanings and
+the same errors. The symbolic analysis runs on the host (bit for bit the reference's); the numeric
+phase and the solves run on the GPU through ``libfieldcraft_b200.so``; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import Status
+
+FC_OK, FC_NOT_POSITIVE_DEFINITE, FC_SINGULAR, FC_TOO_LARGE, FC_OUT_OF_MEMORY = 0, 1, 2, 3, 4
+FC_INTERNAL, FC_CANCELLED, FC_TIMEOUT, FC_INVALID_ARGUMENT, FC_CUDA_ERROR = 5, 6, 7, 8, 9
+FP64, FP32_IR = 0, 1
+
+
+class FactorError(Exception):
+    """Why a factorization stopped (cholesky.rs:346-361)."""
+
+
+class NotPositiveDefinite(FactorError):
+    def __init__(self, column: int):
+        super().__init__(f"NotPositiveDefinite {{ column: {column} }}")
+        self.column = column
+
+    def __eq__(self, other):
+        return isinstance(other, NotPositiveDefinite) and other.column == self.column
+
+
+class Singular(FactorError):
+    def __init__(self, column: int):
+        super().__init__(f"Singular {{ column: {column} }}")
+        self.column = column
+
+
+class TooLarge(FactorError):
+    def __init__(self, entries: int, limit: int):
+        super().__init__(f"TooLarge {{ entries: {entries}, limit: {limit} }}")
+        self.entries, self.limit = entries, limit
+
+
+class OutOfMemory(FactorError):
+    def __init__(self, entries: int):
+        super().__init__(f"OutOfMemory {{ entries: {entries} }}")
+        self.entries = entries
+
+
+class Internal(FactorError):
+    def __init__(self, what: str):
+        super().__init__(f"Internal({what!r})")
+        self.what = what
+
+
+class Cancelled(FactorError):
+    def __init__(self):
+        super().__init__("Cancelled")
+
+
+class DeviceError(RuntimeError):
+    """The CUDA runtime refused a call (no device, a failed launch)."""
+
+
+class Timeout(RuntimeError):
+    """A bounded device wait gave up."""
+
+
+def raise_for(st: Status):
+    code = st.code
+    msg = st.message.decode(errors="replace")
+    if code == FC_OK:
+        return
+    if code == FC_NOT_POSITIVE_DEFINITE:
+        raise NotPositiveDefinite(int(st.column))
+    if code == FC_SINGULAR:
+        raise Singular(int(st.column))
+    if code == FC_TOO_LARGE:
+        raise TooLarge(int(st.entries), int(st.limit))
+    if code == FC_OUT_OF_MEMORY:
+        raise OutOfMemory(int(st.entries))
+    if code == FC_INTERNAL:
+        raise Internal(msg)
+    if code == FC_CANCELLED:
+        raise Cancelled()
+    if code == FC_TIMEOUT:
+        raise Timeout(msg)
+    if code == FC_INVALID_ARGUMENT:
+        raise ValueError(msg or "invalid argument")
+    raise DeviceError(msg or f"code {code}")
+
+
+@dataclass
+class Csr:
+    """A square sparse matrix by rows, both triangles, sorted columns (sparse.rs:26-31)."""
+    n: int
+    ptr: np.ndarray  # int64 [n+1]
+    idx: np.ndarray  # int32 [nnz]
+    val: np.ndarray  # float64 [nnz]
+
+    @staticmethod
+    def from_dense(a) -> "Csr":
+        a = np.asarray(a, dtype=np.float64)
+        n = a.shape[0]
+        ptr, idx, val = [0], [], []
+        for row in a:
+            nz = np.nonzero(row)[0]
+            idx.extend(nz.tolist())
+            val.extend(row[nz].tolist())
+            ptr.append(len(idx))
+        return Csr(n, np.array(ptr, np.int64), np.array(idx, np.int32), np.array(val, np.float64))
+
+
+@dataclass
+class UpperColumns:
+    """The upper triangle by columns: column k holds A(i, k) for i <= k, rows sorted (cholesky.rs:102-107)."""
+    n: int
+    ptr: np.ndarray  # int64 [n+1]
+    idx: np.ndarray  # int32
+    val: np.ndarray  # float64
+
+    @staticmethod
+    def from_symmetric(a: Csr) -> "UpperColumns":
+        """Row k's entries with column <= k are column k of the upper triangle (cholesky.rs:112-145)."""
+        n = a.n
+        rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(a.ptr))
+        keep = a.idx.astype(np.int64) <= rows
+        counts = np.bincount(rows[keep], minlength=n) if n else np.zeros(0, np.int64)
+        ptr = np.zeros(n + 1, np.int64)
+        np.cumsum(counts, out=ptr[1:])
+        return UpperColumns(n, ptr, np.ascontiguousarray(a.idx[keep], np.int32),
+                            np.ascontiguousarray(a.val[keep], np.float64))
+
+
+class Symbolic:
+    """The structure of the factor (Symbolic::new, cholesky.rs:1212-1378), on the host."""
+
+    def __init__(self, a: UpperColumns, max_entries: int):
+        lib = _lib.load()
+        self._ptr = np.ascontiguousarray(a.ptr, np.int64)
+        self._idx = np.ascontiguousarray(a.idx, np.int32)
+        st = Status()
+        h = C.c_void_p()
+        lib.fc_symbolic_analyse(int(a.n), _lib.ptr(self._ptr), _lib.ptr(self._idx),
+                                min(int(max_entries), 2**64 - 1), C.byref(h), C.byref(st))
+        raise_for(st)
+        self.handle = h
+        self.n = a.n
+
+    def arrays(self) -> dict:
+        """Copies of the analysis' arrays (fc_symbolic_arrays)."""
+        lib = _lib.load()
+        out = _lib.SymbolicArrays()
+        lib.fc_symbolic_get(self.handle, C.byref(out))
+
+        def take(p, count, dtype):
+            if count == 0:
+                return np.zeros(0, dtype)
+            return np.ctypeslib.as_array(p, shape=(count,)).astype(dtype, copy=True)
+
+        ns, n, nnz = out.ns, out.n, out.nnz
+        return {
+            "n": n, "ns": ns, "entries": out.entries,
+            "perm": take(out.perm, n, np.int64), "first": take(out.first, ns + 1, np.int64),
+            "rptr": take(out.rptr, ns + 1, np.int64), "rows": take(out.rows, out.rows_len, np.int64),
+            "lptr": take(out.lptr, n + 1, np.int64), "lidx": take(out.lidx, out.lower_len, np.int64),
+            "slot": take(out.slot, nnz, np.int64), "crow": take(out.crow, nnz, np.int64),
+            "ccol": take(out.ccol, nnz, np.int64), "uptr": take(out.uptr, ns + 1, np.int64),
+            "uk": take(out.uk, out.updates_len, np.int64), "up1": take(out.up1, out.updates_len, np.int64),
+            "up2": take(out.up2, out.updates_len, np.int64),
+            "task_lo": take(out.task_lo, out.tasks_len, np.int64),
+            "task_hi": take(out.task_hi, out.tasks_len, np.int64), "top": take(out.top, out.top_len, np.int64),
+        }
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            _lib.load().fc_symbolic_free(h)
+            self.handle = None
+
+
+class Factor:
+    """A Cholesky factor on the GPU: L by supernodes for the matrix in postorder (cholesky.rs:1534)."""
+
+    def __init__(self, symbolic: Symbolic, precision: int = FP64, device: int = 0):
+        lib = _lib.load()
+        st = Status()
+        h = C.c_void_p()
+        lib.fc_chol_create(symbolic.handle, int(precision), int(device), C.byref(h), C.byref(st))
+        raise_for(st)
+        self.handle = h
+        self.n = symbolic.n
+        self.symbolic = symbolic
+
+    @staticmethod
+    def new(a: UpperColumns, max_entries: int, precision: int = FP64, device: int = 0,
+            cancel: C.c_int32 | None = None) -> "Factor":
+        """Factor::new (cholesky.rs:1545): the analysis (refused with TooLarge above max_entries),
+        then the numeric phase on the GPU. `cancel`, a ctypes int32 set non-zero from another
+        thread, stops the factorization between levels of the supernodal tree (Cancelled)."""
+        sym = Symbolic(a, max_entries)
+        f = Factor(sym, precision, device)
+        f.factor(a.val, cancel)
+        return f
+
+    def factor(self, val: np.ndarray, cancel: C.c_int32 | None = None):
+        """Symbolic::numeric + factor with new values on the analysed pattern."""
+        v = np.ascontiguousarray(val, np.float64)
+        st = Status()
+        _lib.load().fc_chol_factor(self.handle, _lib.ptr(v), int(v.size),
+                                   C.byref(cancel) if cancel is not None else None, C.byref(st))
+        raise_for(st)
+
+    def entries(self) -> int:
+        return int(_lib.load().fc_chol_entries(self.handle))
+
+    def solve(self, b: np.ndarray):
+        """Solve A x = b in place (cholesky.rs:1562); b of the factor's length."""
+        if b.ndim != 1 or b.shape[0] != self.n or b.dtype != np.float64 or not b.flags.c_contiguous:
+            raise ValueError("right-hand side length")
+        self._solve(b, 1, self.n)
+
+    def solve_many(self, bs):
+        """Solve for each of `bs` in place (cholesky.rs:1568): a list of 1-D arrays, or a 2-D
+        Fortran-ordered array whose columns are the right-hand sides."""
+        if isinstance(bs, np.ndarray) and bs.ndim == 2:
+            if bs.shape[0] != self.n or not bs.flags.f_contiguous or bs.dtype != np.float64:
+                raise ValueError("right-hand side length")
+            self._solve(bs, bs.shape[1], self.n)
+            return
+        if any(b.shape != (self.n,) for b in bs):
+            raise ValueError("right-hand side length")
+        if not bs:
+            return
+        block = np.asfortranarray(np.stack(bs, axis=1))
+        self._solve(block, block.shape[1], self.n)
+        for j, b in enumerate(bs):
+            b[:] = block[:, j]
+
+    def _solve(self, b, nrhs, ld):
+        st = Status()
+        _lib.load().fc_chol_solve(self.handle, _lib.ptr(b), int(nrhs), int(ld), C.byref(st))
+        raise_for(st)
+
+    def solve_device(self, b_tensor, nrhs: int, ld: int):
+        """Solve in place on device memory (a CUDA tensor, column-major n x nrhs, leading dimension ld)."""
+        st = Status()
+        _lib.load().fc_chol_solve_device(self.handle, C.c_void_p(b_tensor.data_ptr()), int(nrhs), int(ld),
+                                         C.byref(st))
+        raise_for(st)
+
+    def values(self) -> np.ndarray:
+        """The factor in the reference's layout: per supernode its lower trapezoid by columns."""
+        out = np.empty(self.entries(), np.float64)
+        st = Status()
+        _lib.load().fc_chol_values(self.handle, _lib.ptr(out), C.byref(st))
+        raise_for(st)
+        return out
+
+    def stat(self, what: int) -> int:
+        return int(_lib.load().fc_chol_stat(self.handle, what))
+
+    def set_stream(self, stream_ptr: int | None):
+        _lib.load().fc_chol_set_stream(self.handle, C.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def close(self):
+        h = getattr(self, "handle", None)
+        if h:
+            _lib.load().fc_chol_destroy(h)
+            self.handle = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,1101 @@
+// The C ABI of include/fieldcraft_chol.h: handles, the plan of the numeric phase on the device,
+// and the launches. The numeric phase is multifrontal over the reference's supernodes: every
+// supernode's front (its L panel and its update matrix) is assembled from A and its children's
+// update matrices in child order, factored by panels of NB columns (diagonal block, rows below,
+// right-looking update of the later columns), and its update matrix U = F22 - L21 L21^T is left
+// for its parent. Supernodes are taken level by level of the supernodal tree (a level's
+// supernodes are independent); within a level, panel by panel. The factor holds the same L as
+// the reference's left-looking order (the same numbers up to rounding).
+#include <algorithm>
+#include <climits>
+#include <map>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fieldcraft_chol.h"
+#include "cuda/kernels.cuh"
+#include "host/symbolic.hpp"
+
+struct fc_symbolic {
+  fc::Symbolic s;
+};
+
+namespace {
+
+using fc::Failure;
+
+void set_status(fc_status *st, int code, int64_t column = -1, int64_t entries = 0, int64_t limit = 0,
+                const std::string &msg = std::string()) {
+  if (!st) return;
+  st->code = code;
+  st->reserved = 0;
+  st->column = column;
+  st->entries = entries;
+  st->limit = limit;
+  std::snprintf(st->message, sizeof(st->message), "%s", msg.c_str());
+}
+
+int fail_status(fc_status *st, const Failure &f) {
+  set_status(st, f.code, f.column, f.entries, f.limit, f.message);
+  return f.code;
+}
+
+// A device allocation owned by a handle.
+struct DeviceBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DeviceBuf() = default;
+  DeviceBuf(const DeviceBuf &) = delete;
+  DeviceBuf &operator=(const DeviceBuf &) = delete;
+  ~DeviceBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t alloc(size_t b) {
+    release();
+    if (b == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      return e;
+    }
+    bytes = b;
+    return cudaSuccess;
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+template <class T>
+cudaError_t upload(DeviceBuf &buf, const std::vector<T> &host, cudaStream_t st) {
+  cudaError_t e = buf.alloc(sizeof(T) * host.size());
+  if (e != cudaSuccess || host.empty()) return e;
+  return cudaMemcpyAsync(buf.p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, st);
+}
+
+enum Kind { K_ASSEMBLE, K_POTRF, K_TRSM, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_TRSV, K_TRSV_T };
+
+struct Launch {
+  int kind;
+  int64_t off;
+  int count;
+  int level;  // the level of the supernodal tree the launch belongs to (cancellation points)
+};
+
+}  // namespace
+
+struct fc_chol {
+  int device = 0, precision = FC_PRECISION_FP64;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int64_t n = 0, ns = 0, entries = 0, nnz = 0, levels = 0;
+  double flops = 0;
+  std::vector<int64_t> first, perm, loff, uoff, rows_off, toff;
+  std::vector<int32_t> width, height, rows;
+  std::vector<int64_t> kid_ptr;
+  std::vector<int32_t> kids;
+  std::vector<int32_t> level;
+  int64_t l_len = 0, u_len = 0;
+  // device
+  DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
+  DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_perm, d_val, d_status, d_toff;
+  DeviceBuf d_asm, d_potrf, d_trsm, d_gemm;
+  fc::Tree tree{};
+  std::vector<Launch> program;
+  int64_t gemm_tasks = 0;
+  // solve plan for `solve_R` right-hand sides
+  int solve_R = 0;
+  DeviceBuf d_x, d_v, d_voff, d_b, d_srow, d_strsv, d_sgemm;
+  std::vector<Launch> fwd, bwd;
+  int64_t last_factor_launches = 0, last_solve_launches = 0;
+  double gemm_flops_factor = 0, gemm_flops_solve = 0;
+  // per-launch event timing (fc_chol_profile)
+  bool profiling = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  std::vector<cudaEvent_t> event_pool;
+  size_t events_used = 0;
+  std::mutex lock;
+  ~fc_chol() {
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+  }
+};
+
+namespace {
+
+int cuda_fail(fc_status *st, cudaError_t e, const char *where) {
+  std::string msg = std::string(where) + ": " + cudaGetErrorString(e);
+  set_status(st, FC_CUDA_ERROR, -1, 0, 0, msg);
+  return FC_CUDA_ERROR;
+}
+
+int64_t order_key_work(const fc_chol *h, int64_t s) {
+  int64_t m = h->height[s], w = h->width[s], u = m - w;
+  return m * w * w + u * u * w;
+}
+
+// Supernodes grouped by level (height in the supernodal tree), each level heaviest first.
+std::vector<std::vector<int64_t>> levels_of(fc_chol *h) {
+  h->level.assign(h->ns, 0);
+  int32_t top = 0;
+  for (int64_t s = 0; s < h->ns; ++s) {
+    int32_t lv = 0;
+    for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) lv = std::max(lv, h->level[h->kids[q]] + 1);
+    h->level[s] = lv;
+    top = std::max(top, lv);
+  }
+  std::vector<std::vector<int64_t>> out(h->ns ? top + 1 : 0);
+  for (int64_t s = 0; s < h->ns; ++s) out[h->level[s]].push_back(s);
+  for (auto &l : out)
+    std::stable_sort(l.begin(), l.end(), [&](int64_t a, int64_t b) { return order_key_work(h, a) > order_key_work(h, b); });
+  h->levels = (int64_t)out.size();
+  return out;
+}
+
+void push(std::vector<Launch> &prog, int kind, int64_t off, int64_t count, int level) {
+  if (count > 0) prog.push_back({kind, off, (int)count, level});
+}
+
+// Useful flops of a GEMM task (a diagonal tile computes its lower triangle only).
+double task_flops(const fc::GemmTask &g) {
+  double outputs = (double)g.M * g.N;
+  if (g.flags & 1) {
+    outputs = 0;
+    for (int j = 0; j < g.N; ++j) outputs += std::max(0, g.M - j);
+  }
+  return 2.0 * g.K * outputs;
+}
+
+
+// Offsets in one arena for per-supernode blocks that live from the start of their supernode's
+// level to the end of their parent's assembly (the only reader): level by level, the level's
+// blocks are taken first-fit from the free space, then its children's blocks are given back.
+// Returns the arena's size (entries); offsets are 32-entry aligned.
+int64_t arena_offsets(const fc_chol *h, const std::vector<std::vector<int64_t>> &lv, const std::vector<int64_t> &size,
+                      std::vector<int64_t> &off) {
+  const int64_t ALIGN = 32;
+  auto up = [&](int64_t x) { return (x + ALIGN - 1) / ALIGN * ALIGN; };
+  std::map<int64_t, int64_t> free_blocks;  // offset -> length
+  int64_t top = 0;
+  off.assign(h->ns, 0);
+  auto take = [&](int64_t len) {
+    for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it)
+      if (it->second >= len) {
+        const int64_t at = it->first, rest = it->second - len;
+        free_blocks.erase(it);
+        if (rest > 0) free_blocks[at + len] = rest;
+        return at;
+      }
+    const int64_t at = top;
+    top += len;
+    return at;
+  };
+  auto give = [&](int64_t at, int64_t len) {
+    auto next = free_blocks.lower_bound(at);
+    if (next != free_blocks.end() && at + len == next->first) {
+      len += next->second;
+      free_blocks.erase(next);
+    }
+    auto prev = free_blocks.lower_bound(at);
+    if (prev != free_blocks.begin()) {
+      --prev;
+      if (prev->first + prev->second == at) {
+        prev->second += len;
+        return;
+      }
+    }
+    free_blocks[at] = len;
+  };
+  for (const auto &S : lv) {
+    for (int64_t s : S)
+      if (size[s] > 0) off[s] = take(up(size[s]));
+    for (int64_t s : S)
+      for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) {
+        const int64_t c = h->kids[q];
+        if (size[c] > 0) give(off[c], up(size[c]));
+      }
+  }
+  return top;
+}
+
+// The factor's program: per level, assemble; per panel, POTRF, TRSM, update of later columns;
+// then the update matrices.
+void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
+                 std::vector<fc::PanelTask> &potrf_t, std::vector<fc::PanelTask> &trsm_t,
+                 std::vector<fc::GemmTask> &gemm_t) {
+  double *L = h->d_L.as<double>();
+  double *U = h->d_U.as<double>();
+  const int NB = fc::NB;
+  for (size_t l = 0; l < lv.size(); ++l) {
+    const auto &S = lv[l];
+    int64_t off = (int64_t)asm_t.size();
+    for (int64_t s : S) {
+      const int m = h->height[s];
+      for (int j0 = 0; j0 < m; j0 += fc::ASSEMBLE_COLS)
+        asm_t.push_back({(int32_t)s, j0, std::min(m, j0 + fc::ASSEMBLE_COLS), 0});
+    }
+    push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
+    int P = 0;
+    for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
+    for (int p = 0; p < P; ++p) {
+      int64_t po = (int64_t)potrf_t.size(), to = (int64_t)trsm_t.size(), go = (int64_t)gemm_t.size();
+      for (int64_t s : S) {
+        const int m = h->height[s], w = h->width[s];
+        const int c0 = p * NB;
+        if (c0 >= w) continue;
+        const int c1 = std::min(w, c0 + NB);
+        potrf_t.push_back({(int32_t)s, c0, c1, 0, 0, 0});
+        for (int r0 = c1; r0 < m; r0 += fc::TRSM_ROWS)
+          trsm_t.push_back({(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::TRSM_ROWS), 0});
+        double *Ls = L + h->loff[s];
+        for (int jc = c1; jc < w; jc += fc::GEMM_TN)
+          for (int ic = jc; ic < m; ic += fc::GEMM_TM) {
+            fc::GemmTask g{};
+            g.C = Ls + ic + (int64_t)jc * m;
+            g.A = Ls + ic + (int64_t)c0 * m;
+            g.B = Ls + jc + (int64_t)c0 * m;
+            g.c_si = 1, g.c_sj = m, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
+            g.M = std::min(fc::GEMM_TM, m - ic);
+            g.N = std::min(fc::GEMM_TN, w - jc);
+            g.K = c1 - c0;
+            g.flags = ic == jc ? 1 : 0;
+            gemm_t.push_back(g);
+          }
+      }
+      push(h->program, K_POTRF, po, (int64_t)potrf_t.size() - po, (int)l);
+      push(h->program, K_TRSM, to, (int64_t)trsm_t.size() - to, (int)l);
+      push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+    }
+    int64_t go = (int64_t)gemm_t.size();
+    for (int64_t s : S) {
+      const int m = h->height[s], w = h->width[s], u = m - w;
+      if (u <= 0) continue;
+      const double *Ls = L + h->loff[s];
+      double *Us = U + h->uoff[s];
+      for (int bj = 0; bj < u; bj += fc::GEMM_TN)
+        for (int bi = bj; bi < u; bi += fc::GEMM_TM) {
+          fc::GemmTask g{};
+          g.C = Us + bi + (int64_t)bj * u;
+          g.A = Ls + w + bi;
+          g.B = Ls + w + bj;
+          g.c_si = 1, g.c_sj = u, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
+          g.M = std::min(fc::GEMM_TM, u - bi);
+          g.N = std::min(fc::GEMM_TN, u - bj);
+          g.K = w;
+          g.flags = bi == bj ? 1 : 0;
+          gemm_t.push_back(g);
+        }
+    }
+    push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+  }
+}
+
+int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
+  const int64_t ns = sym.ns, n = sym.n;
+  h->n = n;
+  h->ns = ns;
+  h->entries = sym.entries;
+  h->nnz = (int64_t)sym.upper_idx.size();
+  h->first = sym.first;
+  h->perm = sym.perm;
+  h->rows.assign(sym.rows.begin(), sym.rows.end());
+  h->rows_off.assign(sym.rptr.begin(), sym.rptr.end() - (ns ? 1 : 0));
+  if (ns == 0) h->rows_off.clear();
+  h->width.resize(ns);
+  h->height.resize(ns);
+  h->loff.resize(ns);
+  h->uoff.resize(ns);
+  h->toff.resize(ns);
+  int64_t lsum = 0, usum = 0, tsum = 0;
+  double flops = 0;
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t m = sym.height(s), w = sym.width(s), u = m - w;
+    h->width[s] = (int32_t)w;
+    h->height[s] = (int32_t)m;
+    h->loff[s] = lsum;
+    h->toff[s] = tsum;
+    lsum += m * w;
+    usum += u * u;
+    tsum += fc::trapezoid(m, w);
+    for (int64_t c = 0; c < w; ++c) flops += (double)(m - c) * (double)(m - c);
+  }
+  h->l_len = lsum;
+  h->u_len = usum;
+  h->flops = flops;
+  // children and relative maps
+  h->kid_ptr.assign(ns + 1, 0);
+  for (int64_t s = 0; s < ns; ++s)
+    if (sym.sparent[s] != fc::NONE) ++h->kid_ptr[sym.sparent[s] + 1];
+  for (int64_t s = 0; s < ns; ++s) h->kid_ptr[s + 1] += h->kid_ptr[s];
+  h->kids.resize(h->kid_ptr[ns]);
+  {
+    std::vector<int64_t> at(h->kid_ptr.begin(), h->kid_ptr.end() - 1);
+    for (int64_t s = 0; s < ns; ++s)
+      if (sym.sparent[s] != fc::NONE) h->kids[at[sym.sparent[s]]++] = (int32_t)s;
+  }
+  std::vector<int64_t> rel_off(ns, 0);
+  std::vector<int32_t> rel;
+  for (int64_t c = 0; c < ns; ++c) {
+    rel_off[c] = (int64_t)rel.size();
+    const int64_t p = sym.sparent[c];
+    if (p == fc::NONE) continue;
+    const int32_t *cr = sym.rows.data() + sym.rptr[c];
+    const int32_t *pr = sym.rows.data() + sym.rptr[p];
+    const int64_t pm = sym.height(p);
+    int64_t at = 0;
+    for (int64_t i = sym.width(c); i < sym.height(c); ++i) {
+      while (at < pm && pr[at] < cr[i]) ++at;
+      if (at >= pm || pr[at] != cr[i]) {
+        Failure f;
+        f.code = fc::INTERNAL;
+        f.message = "supernodal structure: a child's row outside its parent";
+        return fail_status(st, f);
+      }
+      rel.push_back((int32_t)at);
+    }
+  }
+  // input entries by postordered column, with their place in L
+  std::vector<int64_t> snode(n);
+  for (int64_t s = 0; s < ns; ++s)
+    for (int64_t j = sym.first[s]; j < sym.first[s + 1]; ++j) snode[j] = s;
+  std::vector<int64_t> a_ptr(n + 1, 0), a_src(h->nnz), a_dst(h->nnz), diag_src(n, -1);
+  for (int64_t e = 0; e < h->nnz; ++e) ++a_ptr[sym.ccol[e] + 1];
+  for (int64_t j = 0; j < n; ++j) a_ptr[j + 1] += a_ptr[j];
+  {
+    std::vector<int64_t> at(a_ptr.begin(), a_ptr.end() - 1);
+    for (int64_t e = 0; e < h->nnz; ++e) {
+      const int64_t r = sym.crow[e], c = sym.ccol[e];
+      const int64_t s = snode[c];
+      const int32_t *sr = sym.rows.data() + sym.rptr[s];
+      const int64_t m = sym.height(s);
+      const int32_t *hit = std::lower_bound(sr, sr + m, (int32_t)r);
+      if (hit == sr + m || *hit != r || (hit - sr) < c - sym.first[s]) {
+        Failure f;
+        f.code = fc::INTERNAL;
+        f.message = "supernodal factorization: an entry of A outside the structure";
+        return fail_status(st, f);
+      }
+      const int64_t pos = at[c]++;
+      a_src[pos] = e;
+      a_dst[pos] = h->loff[s] + (hit - sr) + (c - sym.first[s]) * m;
+      if (r == c) diag_src[c] = e;
+    }
+  }
+  auto lv = levels_of(h);
+  {
+    std::vector<int64_t> usize(ns);
+    for (int64_t s = 0; s < ns; ++s) usize[s] = (int64_t)(h->height[s] - h->width[s]) * (h->height[s] - h->width[s]);
+    usum = arena_offsets(h, lv, usize, h->uoff);
+    h->u_len = usum;
+  }
+  cudaStream_t stream = h->stream;
+  cudaError_t e = cudaSuccess;
+#define UP(buf, vec)                                    \
+  if ((e = upload(buf, vec, stream)) != cudaSuccess) { \
+    return cuda_fail(st, e, "upload " #vec);            \
+  }
+  UP(h->d_first, h->first);
+  UP(h->d_width, h->width);
+  UP(h->d_height, h->height);
+  UP(h->d_rows_off, h->rows_off);
+  UP(h->d_rows, h->rows);
+  UP(h->d_loff, h->loff);
+  UP(h->d_uoff, h->uoff);
+  UP(h->d_kid_ptr, h->kid_ptr);
+  UP(h->d_kids, h->kids);
+  UP(h->d_rel_off, rel_off);
+  UP(h->d_rel, rel);
+  UP(h->d_a_ptr, a_ptr);
+  UP(h->d_a_src, a_src);
+  UP(h->d_a_dst, a_dst);
+  UP(h->d_diag_src, diag_src);
+  UP(h->d_perm, h->perm);
+  UP(h->d_toff, h->toff);
+#undef UP
+  if (h->d_L.alloc(sizeof(double) * (size_t)std::max<int64_t>(lsum, 1)) != cudaSuccess ||
+      h->d_U.alloc(sizeof(double) * (size_t)std::max<int64_t>(usum, 1)) != cudaSuccess ||
+      h->d_val.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->nnz, 1)) != cudaSuccess ||
+      h->d_status.alloc(sizeof(fc::DeviceStatus)) != cudaSuccess) {
+    Failure f;
+    f.code = fc::OUT_OF_MEMORY;
+    f.entries = h->entries;
+    f.message = "device memory for the factor";
+    return fail_status(st, f);
+  }
+  fc::Tree &t = h->tree;
+  t.first = h->d_first.as<int64_t>();
+  t.width = h->d_width.as<int32_t>();
+  t.height = h->d_height.as<int32_t>();
+  t.rows_off = h->d_rows_off.as<int64_t>();
+  t.rows = h->d_rows.as<int32_t>();
+  t.loff = h->d_loff.as<int64_t>();
+  t.uoff = h->d_uoff.as<int64_t>();
+  t.kid_ptr = h->d_kid_ptr.as<int64_t>();
+  t.kids = h->d_kids.as<int32_t>();
+  t.rel_off = h->d_rel_off.as<int64_t>();
+  t.rel = h->d_rel.as<int32_t>();
+  t.a_ptr = h->d_a_ptr.as<int64_t>();
+  t.a_src = h->d_a_src.as<int64_t>();
+  t.a_dst = h->d_a_dst.as<int64_t>();
+  t.diag_src = h->d_diag_src.as<int64_t>();
+  t.L = h->d_L.as<double>();
+  t.U = h->d_U.as<double>();
+  std::vector<fc::AssembleTask> asm_t;
+  std::vector<fc::PanelTask> potrf_t, trsm_t;
+  std::vector<fc::GemmTask> gemm_t;
+  plan_factor(h, lv, asm_t, potrf_t, trsm_t, gemm_t);
+  h->gemm_tasks = (int64_t)gemm_t.size();
+  h->gemm_flops_factor = 0;
+  for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
+  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_potrf, potrf_t, stream)) != cudaSuccess ||
+      (e = upload(h->d_trsm, trsm_t, stream)) != cudaSuccess || (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
+    return cuda_fail(st, e, "upload of the plan");
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
+  return FC_OK;
+}
+
+cudaEvent_t next_event(fc_chol *h) {
+  if (h->events_used == h->event_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    h->event_pool.push_back(e);
+  }
+  return h->event_pool[h->events_used++];
+}
+
+// Brackets one launch with events when profiling.
+struct Mark {
+  fc_chol *h;
+  int kind;
+  cudaEvent_t a = nullptr;
+  Mark(fc_chol *h_, int kind_) : h(h_), kind(kind_) {
+    if (h->profiling) {
+      a = next_event(h);
+      cudaEventRecord(a, h->stream);
+    }
+  }
+  ~Mark() {
+    if (h->profiling) {
+      cudaEvent_t b = next_event(h);
+      cudaEventRecord(b, h->stream);
+      h->marks.push_back({kind, {a, b}});
+    }
+  }
+};
+
+// Enqueues the factor's program. Returns FC_CANCELLED when the flag was set between levels.
+int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
+  cudaStream_t st = h->stream;
+  cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), st);
+  const fc::Tree &t = h->tree;
+  int last_level = -1;
+  int64_t launches = 0;
+  for (const Launch &l : h->program) {
+    if (cancel && l.level != last_level) {
+      if (*cancel != 0) {
+        h->last_factor_launches = launches;
+        return FC_CANCELLED;
+      }
+      last_level = l.level;
+    }
+    Mark mark(h, l.kind);
+    switch (l.kind) {
+      case K_ASSEMBLE: fc::launch_assemble(t, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, l.count, st); break;
+      case K_POTRF:
+        fc::launch_potrf(t, d_val, h->d_potrf.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(), st);
+        break;
+      case K_TRSM: fc::launch_trsm(t, h->d_trsm.as<fc::PanelTask>() + l.off, l.count, st); break;
+      case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, st); break;
+    }
+    ++launches;
+  }
+  h->last_factor_launches = launches;
+  return FC_OK;
+}
+
+int read_status(fc_chol *h, fc_status *st) {
+  fc::DeviceStatus ds{};
+  cudaError_t e = cudaMemcpyAsync(&ds, h->d_status.p, sizeof(ds), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_fail(st, e, "factorisation");
+  if (ds.failed_column != ULLONG_MAX) {
+    const int64_t col = (int64_t)ds.failed_column;
+    const int64_t orig = col < h->n ? h->perm[col] : col;
+    set_status(st, FC_NOT_POSITIVE_DEFINITE, orig, 0, 0, "the pivot is not positive (relative to the diagonal)");
+    return FC_NOT_POSITIVE_DEFINITE;
+  }
+  set_status(st, FC_OK);
+  return FC_OK;
+}
+
+// The solve's program for R right-hand sides (built once per R).
+int plan_solve(fc_chol *h, int R, fc_status *st) {
+  if (h->solve_R == R) return FC_OK;
+  const int NB = fc::NB;
+  std::vector<std::vector<int64_t>> lv(h->levels);
+  for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
+  std::vector<int64_t> voff, vsize(h->ns);
+  for (int64_t s = 0; s < h->ns; ++s) vsize[s] = (int64_t)(h->height[s] - h->width[s]) * R;
+  const int64_t vsum = arena_offsets(h, lv, vsize, voff);
+  cudaError_t e;
+  if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
+      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(vsum, 1)) != cudaSuccess) {
+    h->solve_R = 0;
+    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
+    return FC_OUT_OF_MEMORY;
+  }
+  if ((e = upload(h->d_voff, voff, h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
+  std::vector<fc::RowTask> rows;
+  std::vector<fc::SolveTask> trsv;
+  std::vector<fc::GemmTask> gemm;
+  double *L = h->d_L.as<double>(), *x = h->d_x.as<double>(), *v = h->d_v.as<double>();
+  h->fwd.clear();
+  h->bwd.clear();
+  auto gemm_rows = [&](int64_t s, int r0, int r1, int c0, int c1) {
+    // front rows [r0, r1) -= L[rows, c0:c1] x[own c0:c1], split at w (own rows in x, the rest in v)
+    const int m = h->height[s], w = h->width[s];
+    const double *Ls = L + h->loff[s];
+    for (int i0 = r0; i0 < r1;) {
+      const int lim = i0 < w ? std::min(r1, w) : r1;
+      const int i1 = std::min(lim, i0 + fc::GEMM_TM);
+      for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
+        fc::GemmTask g{};
+        g.C = i0 < w ? x + (h->first[s] + i0) * (int64_t)R + j0 : v + voff[s] + (int64_t)(i0 - w) * R + j0;
+        g.c_si = R, g.c_sj = 1;
+        g.A = Ls + i0 + (int64_t)c0 * m;
+        g.a_si = 1, g.a_sk = m;
+        g.B = x + (h->first[s] + c0) * (int64_t)R + j0;
+        g.b_sj = 1, g.b_sk = R;
+        g.M = i1 - i0;
+        g.N = std::min(fc::GEMM_TN, R - j0);
+        g.K = c1 - c0;
+        g.flags = 0;
+        gemm.push_back(g);
+      }
+      i0 = i1;
+    }
+  };
+  auto pushs = [&](std::vector<Launch> &prog, int kind, int64_t off, int64_t count, int l) { push(prog, kind, off, count, l); };
+  // forward
+  for (size_t l = 0; l < lv.size(); ++l) {
+    const auto &S = lv[l];
+    int64_t ro = (int64_t)rows.size();
+    for (int64_t s : S) {
+      const int m = h->height[s], w = h->width[s];
+      const bool kids = h->kid_ptr[s + 1] > h->kid_ptr[s];
+      if (!kids && m == w) continue;
+      for (int i0 = kids ? 0 : w; i0 < m; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(m, i0 + 64), 0});
+    }
+    pushs(h->fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
+    int P = 0;
+    for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
+    for (int p = 0; p < P; ++p) {
+      int64_t to = (int64_t)trsv.size(), go = (int64_t)gemm.size();
+      for (int64_t s : S) {
+        const int m = h->height[s], w = h->width[s], c0 = p * NB;
+        if (c0 >= w) continue;
+        const int c1 = std::min(w, c0 + NB);
+        for (int j0 = 0; j0 < R; j0 += 64) trsv.push_back({(int32_t)s, c0, c1, j0, std::min(R, j0 + 64), 0});
+        if (c1 < m) gemm_rows(s, c1, m, c0, c1);
+      }
+      pushs(h->fwd, K_TRSV, to, (int64_t)trsv.size() - to, (int)l);
+      pushs(h->fwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+    }
+  }
+  // backward
+  for (int64_t l = (int64_t)lv.size() - 1; l >= 0; --l) {
+    const auto &S = lv[l];
+    int64_t ro = (int64_t)rows.size();
+    for (int64_t s : S) {
+      const int u = h->height[s] - h->width[s];
+      for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
+    }
+    pushs(h->bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
+    int64_t go = (int64_t)gemm.size();
+    for (int64_t s : S) {
+      const int m = h->height[s], w = h->width[s], u = m - w;
+      if (u <= 0) continue;
+      const double *Ls = L + h->loff[s];
+      for (int i0 = 0; i0 < w; i0 += fc::GEMM_TM)
+        for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
+          fc::GemmTask g{};
+          g.C = x + (h->first[s] + i0) * (int64_t)R + j0;
+          g.c_si = R, g.c_sj = 1;
+          g.A = Ls + w + (int64_t)i0 * m;
+          g.a_si = m, g.a_sk = 1;
+          g.B = v + voff[s] + j0;
+          g.b_sj = 1, g.b_sk = R;
+          g.M = std::min(fc::GEMM_TM, w - i0);
+          g.N = std::min(fc::GEMM_TN, R - j0);
+          g.K = u;
+          gemm.push_back(g);
+        }
+    }
+    pushs(h->bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+    int P = 0;
+    for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
+    for (int p = P - 1; p >= 0; --p) {
+      int64_t to = (int64_t)trsv.size(), go2 = (int64_t)gemm.size();
+      for (int64_t s : S) {
+        const int m = h->height[s], w = h->width[s], c0 = p * NB;
+        if (c0 >= w) continue;
+        const int c1 = std::min(w, c0 + NB);
+        for (int j0 = 0; j0 < R; j0 += 64) trsv.push_back({(int32_t)s, c0, c1, j0, std::min(R, j0 + 64), 0});
+        const double *Ls = L + h->loff[s];
+        for (int i0 = 0; i0 < c0; i0 += fc::GEMM_TM)
+          for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
+            fc::GemmTask g{};
+            g.C = x + (h->first[s] + i0) * (int64_t)R + j0;
+            g.c_si = R, g.c_sj = 1;
+            g.A = Ls + c0 + (int64_t)i0 * m;
+            g.a_si = m, g.a_sk = 1;
+            g.B = x + (h->first[s] + c0) * (int64_t)R + j0;
+            g.b_sj = 1, g.b_sk = R;
+            g.M = std::min(fc::GEMM_TM, c0 - i0);
+            g.N = std::min(fc::GEMM_TN, R - j0);
+            g.K = c1 - c0;
+            gemm.push_back(g);
+          }
+      }
+      pushs(h->bwd, K_TRSV_T, to, (int64_t)trsv.size() - to, (int)l);
+      pushs(h->bwd, K_GEMM, go2, (int64_t)gemm.size() - go2, (int)l);
+    }
+  }
+  h->gemm_flops_solve = 0;
+  for (const auto &g : gemm) h->gemm_flops_solve += task_flops(g);
+  if ((e = upload(h->d_srow, rows, h->stream)) != cudaSuccess || (e = upload(h->d_strsv, trsv, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_sgemm, gemm, h->stream)) != cudaSuccess)
+    return cuda_fail(st, e, "solve plan");
+  if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
+  h->solve_R = R;
+  return FC_OK;
+}
+
+void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, int64_t &launches) {
+  cudaStream_t st = h->stream;
+  const fc::Tree &t = h->tree;
+  const int R = h->solve_R;
+  double *x = h->d_x.as<double>(), *v = h->d_v.as<double>();
+  const int64_t *voff = h->d_voff.as<int64_t>();
+  for (const Launch &l : prog) {
+    Mark mark(h, l.kind + 16);
+    switch (l.kind) {
+      case K_SOLVE_ASSEMBLE:
+        fc::launch_solve_assemble(t, x, v, voff, R, h->d_srow.as<fc::RowTask>() + l.off, l.count, st);
+        break;
+      case K_SOLVE_GATHER:
+        fc::launch_solve_gather(t, x, v, voff, R, h->d_srow.as<fc::RowTask>() + l.off, l.count, st);
+        break;
+      case K_TRSV: fc::launch_trsv(t, x, R, false, h->d_strsv.as<fc::SolveTask>() + l.off, l.count, st); break;
+      case K_TRSV_T: fc::launch_trsv(t, x, R, true, h->d_strsv.as<fc::SolveTask>() + l.off, l.count, st); break;
+      case K_GEMM: fc::launch_gemm(h->d_sgemm.as<fc::GemmTask>() + l.off, l.count, st); break;
+    }
+    ++launches;
+  }
+}
+
+// Solves for the R right-hand sides in device memory at d_b (column-major, leading dimension ld).
+int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
+  int rc = plan_solve(h, R, st);
+  if (rc != FC_OK) return rc;
+  int64_t launches = 0;
+  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->stream);
+  run_solve_program(h, h->fwd, launches);
+  run_solve_program(h, h->bwd, launches);
+  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->stream);
+  h->last_solve_launches = launches + 2;
+  return FC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fc_version(void) { return "fieldcraft-b200 0.1.0 (sm_100a)"; }
+
+int fc_symbolic_analyse(int64_t n, const int64_t *ptr, const int32_t *idx, uint64_t max_entries, fc_symbolic **out,
+                        fc_status *status) {
+  if (!out || n < 0 || (n > 0 && (!ptr || !idx))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null or negative argument");
+    return FC_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  std::vector<int64_t> zero_ptr(1, 0);
+  fc::UpperPattern a{n, n > 0 ? ptr : zero_ptr.data(), idx};
+  try {
+    auto s = new fc_symbolic();
+    Failure f;
+    if (!fc::analyse(a, max_entries, s->s, f)) {
+      delete s;
+      return fail_status(status, f);
+    }
+    *out = s;
+  } catch (const std::bad_alloc &) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, 0, 0, "host memory for the analysis");
+    return FC_OUT_OF_MEMORY;
+  }
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+void fc_symbolic_free(fc_symbolic *sym) { delete sym; }
+
+int fc_symbolic_get(const fc_symbolic *sym, fc_symbolic_arrays *o) {
+  if (!sym || !o) return FC_INVALID_ARGUMENT;
+  const fc::Symbolic &s = sym->s;
+  o->n = s.n;
+  o->ns = s.ns;
+  o->entries = s.entries;
+  o->nnz = (int64_t)s.upper_idx.size();
+  o->rows_len = (int64_t)s.rows.size();
+  o->lower_len = (int64_t)s.lidx.size();
+  o->updates_len = (int64_t)s.uk.size();
+  o->tasks_len = (int64_t)s.task_lo.size();
+  o->top_len = (int64_t)s.top.size();
+  o->perm = s.perm.data();
+  o->first = s.first.data();
+  o->rptr = s.rptr.data();
+  o->rows = s.rows.data();
+  o->upper_ptr = s.upper_ptr.data();
+  o->upper_idx = s.upper_idx.data();
+  o->lptr = s.lptr.data();
+  o->lidx = s.lidx.data();
+  o->slot = s.slot.data();
+  o->crow = s.crow.data();
+  o->ccol = s.ccol.data();
+  o->uptr = s.uptr.data();
+  o->uk = s.uk.data();
+  o->up1 = s.up1.data();
+  o->up2 = s.up2.data();
+  o->task_lo = s.task_lo.data();
+  o->task_hi = s.task_hi.data();
+  o->top = s.top.data();
+  return FC_OK;
+}
+
+int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_status *status) {
+  if (!in || !out || in->n < 0 || in->ns < 0) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null or negative argument");
+    return FC_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  try {
+    auto h = new fc_symbolic();
+    fc::Symbolic &s = h->s;
+    auto cp64 = [](std::vector<int64_t> &v, const int64_t *p, int64_t len) { v.assign(p, p + len); };
+    auto cp32 = [](std::vector<int32_t> &v, const int32_t *p, int64_t len) { v.assign(p, p + len); };
+    s.n = in->n;
+    s.ns = in->ns;
+    s.entries = in->entries;
+    cp64(s.perm, in->perm, in->n);
+    cp64(s.first, in->first, in->ns + 1);
+    cp64(s.rptr, in->rptr, in->ns + 1);
+    cp32(s.rows, in->rows, in->rows_len);
+    cp64(s.upper_ptr, in->upper_ptr, in->n + 1);
+    cp32(s.upper_idx, in->upper_idx, in->nnz);
+    cp64(s.lptr, in->lptr, in->n + 1);
+    cp32(s.lidx, in->lidx, in->lower_len);
+    cp64(s.slot, in->slot, in->nnz);
+    cp32(s.crow, in->crow, in->nnz);
+    cp32(s.ccol, in->ccol, in->nnz);
+    cp64(s.uptr, in->uptr, in->ns + 1);
+    cp64(s.uk, in->uk, in->updates_len);
+    cp64(s.up1, in->up1, in->updates_len);
+    cp64(s.up2, in->up2, in->updates_len);
+    cp64(s.task_lo, in->task_lo, in->tasks_len);
+    cp64(s.task_hi, in->task_hi, in->tasks_len);
+    cp64(s.top, in->top, in->top_len);
+    // The supernodal tree from the structures: a supernode's parent holds its first row past
+    // its own columns.
+    bool ok = s.first.front() == 0 && s.first.back() == s.n && s.rptr.front() == 0 &&
+              s.rptr.back() == (int64_t)s.rows.size();
+    std::vector<int64_t> snode(s.n, 0);
+    for (int64_t t = 0; ok && t < s.ns; ++t) {
+      if (s.first[t + 1] <= s.first[t] || s.rptr[t + 1] - s.rptr[t] < s.first[t + 1] - s.first[t]) ok = false;
+      for (int64_t j = s.first[t]; ok && j < s.first[t + 1]; ++j) snode[j] = t;
+    }
+    s.sparent.assign(s.ns, fc::NONE);
+    for (int64_t t = 0; ok && t < s.ns; ++t) {
+      const int64_t w = s.width(t), m = s.height(t);
+      if (m > w) {
+        const int64_t r = s.rows[s.rptr[t] + w];
+        if (r < 0 || r >= s.n) ok = false;
+        else s.sparent[t] = snode[r];
+      }
+    }
+    if (!ok) {
+      delete h;
+      set_status(status, FC_INTERNAL, -1, 0, 0, "supernodal structure: inconsistent arrays");
+      return FC_INTERNAL;
+    }
+    *out = h;
+  } catch (const std::bad_alloc &) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, 0, 0, "host memory");
+    return FC_OUT_OF_MEMORY;
+  }
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **out, fc_status *status) {
+  if (!sym || !out || (precision != FC_PRECISION_FP64 && precision != FC_PRECISION_FP32_IR)) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null argument or unknown precision");
+    return FC_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(status, e, "cudaSetDevice");
+  fc_chol *h = nullptr;
+  try {
+    h = new fc_chol();
+  } catch (const std::bad_alloc &) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, 0, 0, "host memory");
+    return FC_OUT_OF_MEMORY;
+  }
+  h->device = device;
+  h->precision = precision;
+  if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete h;
+    return cuda_fail(status, e, "cudaStreamCreate");
+  }
+  h->own_stream = true;
+  int rc;
+  try {
+    rc = build(h, sym->s, status);
+  } catch (const std::bad_alloc &) {
+    rc = FC_OUT_OF_MEMORY;
+    set_status(status, rc, -1, sym->s.entries, 0, "host memory for the plan");
+  }
+  if (rc != FC_OK) {
+    fc_chol_destroy(h);
+    return rc;
+  }
+  *out = h;
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+void fc_chol_destroy(fc_chol *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  cudaStream_t own = h->own_stream ? h->stream : nullptr;
+  h->stream = nullptr;
+  delete h;  // frees the device buffers
+  if (own) cudaStreamDestroy(own);
+}
+
+int fc_chol_set_stream(fc_chol *h, void *stream) {
+  if (!h) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  if (stream) {
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+  } else if (!h->own_stream) {
+    cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    h->own_stream = true;
+  }
+  return FC_OK;
+}
+
+int fc_chol_factor(fc_chol *h, const double *upper_val, int64_t nnz, const volatile int32_t *cancel, fc_status *status) {
+  if (!h || (nnz > 0 && !upper_val) || nnz != h->nnz) {
+    set_status(status, FC_INTERNAL, -1, 0, 0, "supernodal factorization: the matrix's pattern differs from the analysed one");
+    return h ? FC_INTERNAL : FC_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  cudaError_t e = cudaSuccess;
+  if (nnz > 0) e = cudaMemcpyAsync(h->d_val.p, upper_val, sizeof(double) * nnz, cudaMemcpyHostToDevice, h->stream);
+  if (e != cudaSuccess) return cuda_fail(status, e, "values upload");
+  int rc = enqueue_factor(h, h->d_val.as<double>(), cancel);
+  if (rc == FC_CANCELLED) {
+    cudaStreamSynchronize(h->stream);
+    set_status(status, FC_CANCELLED, -1, 0, 0, "cancelled");
+    return FC_CANCELLED;
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(status, e, "factor launch");
+  return read_status(h, status);
+}
+
+int fc_chol_factor_device_async(fc_chol *h, const double *d_upper_val, int64_t nnz) {
+  if (!h || nnz != h->nnz || (nnz > 0 && !d_upper_val)) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  enqueue_factor(h, d_upper_val, nullptr);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
+}
+
+int fc_chol_check(fc_chol *h, fc_status *status) {
+  if (!h) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  return read_status(h, status);
+}
+
+int fc_chol_factor_device(fc_chol *h, const double *d_upper_val, int64_t nnz, fc_status *status) {
+  int rc = fc_chol_factor_device_async(h, d_upper_val, nnz);
+  if (rc != FC_OK) {
+    set_status(status, rc, -1, 0, 0, rc == FC_CUDA_ERROR ? cudaGetErrorString(cudaGetLastError()) : "bad argument");
+    return rc;
+  }
+  return fc_chol_check(h, status);
+}
+
+int64_t fc_chol_entries(const fc_chol *h) { return h ? h->entries : -1; }
+
+int fc_chol_solve_device_async(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld) {
+  if (!h || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) return FC_INVALID_ARGUMENT;
+  if (nrhs == 0 || h->n == 0) return FC_OK;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  int rc = enqueue_solve(h, d_b, nrhs, ld, nullptr);
+  if (rc != FC_OK) return rc;
+  return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
+}
+
+int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_status *status) {
+  if (!h || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
+    return FC_INVALID_ARGUMENT;
+  }
+  if (nrhs == 0 || h->n == 0) {
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  int rc = enqueue_solve(h, d_b, nrhs, ld, status);
+  if (rc != FC_OK) return rc;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(status, e, "solve");
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *status) {
+  if (!h || nrhs < 0 || (nrhs > 0 && (!b || ld < h->n))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
+    return FC_INVALID_ARGUMENT;
+  }
+  if (nrhs == 0 || h->n == 0) {
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  const size_t bytes = sizeof(double) * (size_t)h->n * nrhs;
+  if (h->d_b.bytes < bytes && h->d_b.alloc(bytes) != cudaSuccess) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the right-hand sides");
+    return FC_OUT_OF_MEMORY;
+  }
+  cudaError_t e = cudaMemcpy2DAsync(h->d_b.p, sizeof(double) * h->n, b, sizeof(double) * ld, sizeof(double) * h->n, nrhs,
+                                    cudaMemcpyHostToDevice, h->stream);
+  if (e != cudaSuccess) return cuda_fail(status, e, "right-hand side upload");
+  int rc = enqueue_solve(h, h->d_b.as<double>(), nrhs, h->n, status);
+  if (rc != FC_OK) return rc;
+  e = cudaMemcpy2DAsync(b, sizeof(double) * ld, h->d_b.p, sizeof(double) * h->n, sizeof(double) * h->n, nrhs,
+                        cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(status, e, "solve");
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_values(fc_chol *h, double *dst, fc_status *status) {
+  if (!h || (h->entries > 0 && !dst)) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null argument");
+    return FC_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  if (h->entries == 0) {
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  DeviceBuf tmp;
+  if (tmp.alloc(sizeof(double) * (size_t)h->entries) != cudaSuccess) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the copy");
+    return FC_OUT_OF_MEMORY;
+  }
+  fc::launch_pack_trapezoids(h->tree, h->ns, h->d_toff.as<int64_t>(), tmp.as<double>(), h->stream);
+  cudaError_t e = cudaMemcpyAsync(dst, tmp.p, sizeof(double) * h->entries, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_fail(status, e, "values");
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int64_t fc_chol_stat(const fc_chol *h, int what) {
+  if (!h) return -1;
+  switch (what) {
+    case 0: return h->levels;
+    case 1: return (int64_t)h->program.size();
+    case 2: return h->l_len * 8;
+    case 3: return h->u_len * 8;
+    case 4: return h->ns;
+    case 5: return (int64_t)h->flops;
+    case 6: return h->gemm_tasks;
+    case 7: return h->last_factor_launches;
+    case 8: return h->last_solve_launches;
+    case 9: return (int64_t)h->gemm_flops_factor;
+    case 10: return (int64_t)h->gemm_flops_solve;
+  }
+  return -1;
+}
+
+int fc_chol_profile(fc_chol *h, int enable) {
+  if (!h) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  h->profiling = enable != 0;
+  h->marks.clear();
+  h->events_used = 0;
+  return FC_OK;
+}
+
+int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kinds) {
+  if (!h || !ms || !launches || kinds <= 0) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return FC_CUDA_ERROR;
+  for (int k = 0; k < kinds; ++k) {
+    ms[k] = 0;
+    launches[k] = 0;
+  }
+  for (auto &m : h->marks) {
+    if (m.first < 0 || m.first >= kinds) continue;
+    float t = 0;
+    if (cudaEventElapsedTime(&t, m.second.first, m.second.second) == cudaSuccess) ms[m.first] += t;
+    launches[m.first] += 1;
+  }
+  h->marks.clear();
+  h->events_used = 0;
+  return FC_OK;
+}
+
+int fc_csr_spmv_device(int64_t n, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val, const double *d_x,
+                       double *d_y, int32_t nrhs, int64_t ld, void *stream) {
+  if (n < 0 || nrhs < 0 || (n > 0 && (!d_ptr || !d_idx || !d_val || !d_x || !d_y || ld < n))) return FC_INVALID_ARGUMENT;
+  fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, d_y, nrhs, ld, (cudaStream_t)stream);
+  return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
+}
+
+}  // extern "C"

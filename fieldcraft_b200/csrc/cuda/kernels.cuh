@@ -1,0 +1,94 @@
+// Device kernels of the supernodal Cholesky and their task records. The host plans the whole
+// numeric phase as a fixed list of launches over task arrays (level by level of the supernodal
+// tree, panel by panel inside a level); each CTA of a launch takes one task.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fc {
+
+// Panel width of the dense partial factorisation of a front, and the tile of the dense kernels.
+constexpr int NB = 64;
+constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_KC = 16;
+constexpr int GEMM_THREADS = 128;
+constexpr int TRSM_ROWS = 128;  // rows of a panel solved by one CTA
+constexpr int ASSEMBLE_COLS = 32;  // front columns assembled by one CTA
+
+// Where each supernode lives on the device. A front of supernode s has m = rows(s) rows and
+// w = width(s) columns of L; its update matrix U_s is the (m-w) x (m-w) Schur complement.
+struct Tree {
+  const int64_t *first;     // [ns+1] first column (postorder)
+  const int32_t *width;     // [ns]
+  const int32_t *height;    // [ns]  m
+  const int64_t *rows_off;  // [ns]
+  const int32_t *rows;      // row structures (postorder indices)
+  const int64_t *loff;      // [ns] L panel: m x w, column-major, ld m
+  const int64_t *uoff;      // [ns] U: (m-w) x (m-w), column-major, ld m-w (lower half used)
+  const int64_t *kid_ptr;   // [ns+1]
+  const int32_t *kids;      // children in increasing order
+  const int64_t *rel_off;   // [ns] where a child's relative map starts (its rows past its columns)
+  const int32_t *rel;       // positions of a child's rows in its parent's structure
+  const int64_t *a_ptr;     // [n+1] input entries by postordered column
+  const int64_t *a_src;     // upper-entry index of each
+  const int64_t *a_dst;     // its place in the L arena
+  const int64_t *diag_src;  // [n] upper-entry index of A(j, j), -1 if absent
+  double *L;
+  double *U;
+};
+
+struct AssembleTask {
+  int32_t s, j0, j1, pad;
+};
+// Diagonal block [c0, c1) of supernode s (POTRF), or rows [r0, r1) below it (TRSM).
+struct PanelTask {
+  int32_t s, c0, c1, r0, r1, pad;
+};
+// C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands; flag 1: store i >= j only.
+struct GemmTask {
+  double *C;
+  const double *A;
+  const double *B;
+  int64_t c_si, c_sj, a_si, a_sk, b_sj, b_sk;
+  int32_t M, N, K, flags;
+};
+// Solve: rows [c0, c1) of supernode s's own block, right-hand sides [j0, j1).
+struct SolveTask {
+  int32_t s, c0, c1, j0, j1, pad;
+};
+// Solve front rows [i0, i1) of supernode s.
+struct RowTask {
+  int32_t s, i0, i1, pad;
+};
+
+// Device status word of a factorisation: the smallest failing pivot column (postorder).
+struct DeviceStatus {
+  unsigned long long failed_column;  // ULLONG_MAX when none
+};
+
+void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, int count,
+                     cudaStream_t st);
+void launch_potrf(const Tree &t, const double *upper_val, const PanelTask *tasks, int count,
+                  DeviceStatus *status, cudaStream_t st);
+void launch_trsm(const Tree &t, const PanelTask *tasks, int count, cudaStream_t st);
+void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st);
+
+// Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
+void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R,
+                           const RowTask *tasks, int count, cudaStream_t st);
+void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R,
+                         const RowTask *tasks, int count, cudaStream_t st);
+void launch_trsv(const Tree &t, double *x, int R, bool transpose, const SolveTask *tasks, int count,
+                 cudaStream_t st);
+// x_post[i*R + j] = b[perm[i] + j*ld] and back.
+void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
+                       cudaStream_t st);
+void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, double *b, int64_t ld,
+                        cudaStream_t st);
+// y = A x for column-major x, y (leading dimension ld).
+void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x,
+                 double *y, int R, int64_t ld, cudaStream_t st);
+// Copies the L panels out into the reference's packed trapezoids (dst offsets per supernode).
+void launch_pack_trapezoids(const Tree &t, int64_t ns, const int64_t *toff, double *dst, cudaStream_t st);
+
+}  // namespace fc

@@ -1,0 +1,148 @@
+/* fieldcraft_chol.h — C ABI of the B200 numeric phase of FieldCraft's supernodal Cholesky.
+ *
+ * The reference's API for this path is Rust (crates/solver/src/cholesky.rs):
+ *   UpperColumns (:102-107), Factor::new(a, max_entries) (:1545), Factor::entries (:1557),
+ *   Factor::solve (:1562), Factor::solve_many (:1568), FactorError (:346-361),
+ *   and the crate-private Symbolic (:1195-1207) whose arrays a Rust caller hands over.
+ * Every entry point below names the reference item it replaces. Plain pointers and sizes only;
+ * no C++ exceptions cross this boundary; every call returns an FC_* code and fills *status
+ * (when status is not NULL) with the code and, for a numeric failure, the column.
+ *
+ * Index types: row pointers int64, row/column indices int32, values double (FP64).
+ * Host buffers are caller-owned; device memory is owned by the handle; one CUDA stream per
+ * handle (settable). Distinct handles may be used from distinct threads.
+ */
+#ifndef FIELDCRAFT_CHOL_H
+#define FIELDCRAFT_CHOL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Codes: FactorError one to one (cholesky.rs:346-361), then the boundary's own. */
+#define FC_OK 0
+#define FC_NOT_POSITIVE_DEFINITE 1 /* FactorError::NotPositiveDefinite { column } */
+#define FC_SINGULAR 2              /* FactorError::Singular { column } (LDLT; unused by Cholesky) */
+#define FC_TOO_LARGE 3             /* FactorError::TooLarge { entries, limit } */
+#define FC_OUT_OF_MEMORY 4         /* FactorError::OutOfMemory { entries } */
+#define FC_INTERNAL 5              /* FactorError::Internal(String) */
+#define FC_CANCELLED 6             /* FactorError::Cancelled */
+#define FC_TIMEOUT 7               /* a bounded device wait gave up */
+#define FC_INVALID_ARGUMENT 8      /* solver::Error::Internal("right-hand side length") and bad pointers */
+#define FC_CUDA_ERROR 9            /* the CUDA runtime refused a call (no device, launch failure) */
+
+/* Precision of the numeric phase. */
+#define FC_PRECISION_FP64 0
+#define FC_PRECISION_FP32_IR 1 /* FP32 factor (FP64 fallback for weak pivots), FP64 refinement */
+
+typedef struct fc_status {
+  int32_t code;
+  int32_t reserved;
+  int64_t column;  /* original column of a NotPositiveDefinite / Singular pivot, else -1 */
+  int64_t entries; /* TooLarge / OutOfMemory: entries of the factor */
+  int64_t limit;   /* TooLarge: the cap */
+  char message[224];
+} fc_status;
+
+typedef struct fc_symbolic fc_symbolic;
+typedef struct fc_chol fc_chol;
+
+/* ---- symbolic analysis (replaces Symbolic::new, cholesky.rs:1212-1378) --------------------------
+ * The upper triangle of a symmetric matrix by columns (UpperColumns, cholesky.rs:102-107): column
+ * k holds rows i <= k, sorted; ptr[n+1], idx[ptr[n]]. Refused with FC_TOO_LARGE before any
+ * numeric memory when the factor would hold more than max_entries entries (cholesky.rs:1217). */
+int fc_symbolic_analyse(int64_t n, const int64_t *ptr, const int32_t *idx, uint64_t max_entries,
+                        fc_symbolic **out, fc_status *status);
+void fc_symbolic_free(fc_symbolic *sym);
+
+/* The arrays of the reference's Symbolic, for a caller that ran its own analysis (the Rust
+ * side) or wants to check this one. Field meanings follow cholesky.rs:385-415, 728-737,
+ * 1195-1207; the update lists are by target supernode in CSR form. */
+typedef struct fc_symbolic_arrays {
+  int64_t n, ns, entries, nnz, rows_len, lower_len, updates_len, tasks_len, top_len;
+  const int64_t *perm;     /* [n]      perm[k]: original column of factor column k */
+  const int64_t *first;    /* [ns+1]   Structure.first */
+  const int64_t *rptr;     /* [ns+1]   Structure.rptr */
+  const int32_t *rows;     /* [rows_len] Structure.rows */
+  const int64_t *upper_ptr;/* [n+1]    Pattern.upper_ptr */
+  const int32_t *upper_idx;/* [nnz]    Pattern.upper_idx */
+  const int64_t *lptr;     /* [n+1]    Pattern.ptr */
+  const int32_t *lidx;     /* [lower_len] Pattern.idx */
+  const int64_t *slot;     /* [nnz]    Pattern.slot */
+  const int32_t *crow;     /* [nnz]    Pattern.coords .0 */
+  const int32_t *ccol;     /* [nnz]    Pattern.coords .1 */
+  const int64_t *uptr;     /* [ns+1]   updates by target */
+  const int64_t *uk, *up1, *up2; /* [updates_len] Update { k, p1, p2 } */
+  const int64_t *task_lo, *task_hi; /* [tasks_len] Symbolic.tasks */
+  const int64_t *top;      /* [top_len] Symbolic.top */
+} fc_symbolic_arrays;
+
+/* Views of the analysis' arrays (valid while sym lives). */
+int fc_symbolic_get(const fc_symbolic *sym, fc_symbolic_arrays *out);
+/* An analysis from a caller's arrays (copied); checked for consistency, FC_INTERNAL if not. */
+int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_status *status);
+
+/* ---- numeric factorisation on a B200 (replaces Factor::from_symbolic, cholesky.rs:1549-1554) ----
+ * fc_chol_create uploads the structure and plans the level schedule on `device`; no values yet.
+ * It copies what it needs: sym may be freed afterwards. */
+int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **out, fc_status *status);
+void fc_chol_destroy(fc_chol *h);
+/* Runs on this CUDA stream (cudaStream_t); NULL for the handle's own stream. */
+int fc_chol_set_stream(fc_chol *h, void *stream);
+
+/* Symbolic::numeric + Symbolic::factor (cholesky.rs:1392-1416, 1443-1529) from host values:
+ * upper_val[nnz] in the order of the analysed UpperColumns. cancel, when not NULL, is read
+ * between levels of the supernodal tree (the reference reads its progress between
+ * supernodes, :1476-1484): non-zero stops with FC_CANCELLED. Errors: FC_NOT_POSITIVE_DEFINITE
+ * with the original column of the first failing pivot in postorder (:1506-1528). */
+int fc_chol_factor(fc_chol *h, const double *upper_val, int64_t nnz, const volatile int32_t *cancel,
+                   fc_status *status);
+/* The same from values already in device memory; synchronises the stream before returning. */
+int fc_chol_factor_device(fc_chol *h, const double *d_upper_val, int64_t nnz, fc_status *status);
+/* Enqueues the factorisation without waiting; fc_chol_check reads its status afterwards. */
+int fc_chol_factor_device_async(fc_chol *h, const double *d_upper_val, int64_t nnz);
+int fc_chol_check(fc_chol *h, fc_status *status);
+
+/* Factor::entries (cholesky.rs:1557): entries of L (the reference's count, trapezoids). */
+int64_t fc_chol_entries(const fc_chol *h);
+/* Factor::solve / solve_many (cholesky.rs:1562-1570): solves A x = b in place for nrhs
+ * right-hand sides stored column-major in b (column j at b + j*ld, ld >= n). */
+int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *status);
+/* The same on device memory; synchronises before returning. */
+int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_status *status);
+int fc_chol_solve_device_async(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld);
+/* The factor's values in the reference's layout: supernode by supernode, each its lower
+ * trapezoid by columns (column c holds rows c..m, cholesky.rs:418-425, 1534-1542). dst has
+ * fc_chol_entries(h) doubles. */
+int fc_chol_values(fc_chol *h, double *dst, fc_status *status);
+
+/* Plan statistics: 0 levels, 1 launches of the factor, 2 bytes of L on device, 3 bytes of the
+ * update matrices, 4 supernodes, 5 factor flops (sum of column counts squared), 6 GEMM tasks,
+ * 7 kernels launched by the last factorisation, 8 kernels launched by the last solve, 9 flops of
+ * the factor's GEMM tasks, 10 flops of the last solve plan's GEMM tasks. */
+int64_t fc_chol_stat(const fc_chol *h, int what);
+
+/* Per-launch timing with CUDA events on the handle's stream (no reference counterpart: the
+ * measurement hook of the benchmark). enable != 0 starts recording; fc_chol_profile_read waits for
+ * the stream and returns, per launch kind, the summed milliseconds and the launch count (arrays of
+ * `kinds` entries, 24 covers all), then clears them. Kinds: 0 front assembly, 1 POTRF, 2 TRSM,
+ * 3 GEMM of the factor; 19 GEMM, 20 front assembly, 21 gather, 22 TRSV, 23 transposed TRSV of
+ * the solve. */
+int fc_chol_profile(fc_chol *h, int enable);
+int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kinds);
+
+/* ---- compressed-row products (Csr::mul, crates/solver/src/sparse.rs:42-50) ---------------------
+ * y = A x on the device for nrhs vectors, x and y column-major with leading dimension ld. */
+int fc_csr_spmv_device(int64_t n, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val,
+                       const double *d_x, double *d_y, int32_t nrhs, int64_t ld, void *stream);
+
+/* Version string of the library. */
+const char *fc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,161 @@
+"""Parity of the B200 numeric phase with the oracle, through the C ABI (via the Python mirror of
+the reference's API). Every case runs the CUDA kernels; FP64 throughout.
+
+Tolerances: the GPU computes each entry of L with a different operation order than the reference
+(blocked right-looking fronts, fused multiply-adds on the FP64 tensor pipe), so parity is to
+rounding: factor entries within 1e-11 of the largest entry, solutions within 1e-10 relative to the
+oracle's, and the reference's own residual bounds where it states them."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import helpers as H
+from fieldcraft_b200 import Cancelled, Factor, NotPositiveDefinite, Symbolic, TooLarge, UpperColumns, problems
+from fieldcraft_b200.cholesky import Csr
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+FACTOR_TOL = 1e-11
+SOLVE_TOL = 1e-10
+
+
+def oracle_factor(csr: Csr):
+    up = UpperColumns.from_symmetric(csr)
+    s = oracle.Sym(up.n, up.ptr, up.idx)
+    return s, oracle.Fac(s, up.val)
+
+
+def cases():
+    yield "grid7x5", lambda: Csr.from_dense(H.grid_7x5())
+    yield "panels", H.panels_matrix
+    yield "blocks40", lambda: Csr.from_dense(H.blocks40())
+    yield "solid5", lambda: H.solid_stiffness(5)
+    yield "solid5-roller", lambda: H.solid_stiffness(5, roller=True)
+    yield "band", lambda: H.band_matrix()[1]
+    yield "cantilever", lambda: problems.cantilever().csr
+    yield "lognormal-12", lambda: problems.lognormal_block(12, nrhs=1).csr
+
+
+@pytest.mark.parametrize("name,make", list(cases()), ids=[c[0] for c in cases()])
+def test_factor_and_solve_match_the_oracle(cuda, name, make):
+    csr = make()
+    up = UpperColumns.from_symmetric(csr)
+    f = Factor.new(up, 2**62)
+    _, ref = oracle_factor(csr)
+    lv, rv = f.values(), ref.values()
+    assert f.entries() == rv.size
+    assert np.max(np.abs(lv - rv)) <= FACTOR_TOL * np.max(np.abs(rv)), name
+    x = H.sin_solution(csr.n)
+    b = oracle.spmv(csr.n, csr.ptr, csr.idx, csr.val, x)
+    got = b.copy()
+    f.solve(got)
+    exp = ref.solve(b.copy())
+    assert np.linalg.norm(got - exp) <= SOLVE_TOL * np.linalg.norm(exp), name
+    r = oracle.spmv(csr.n, csr.ptr, csr.idx, csr.val, got) - b
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b), name
+
+
+def test_reference_residual_bounds(cuda):
+    # cholesky.rs:1707 (1e-13) and :1761 (1e-12) on the GPU factor
+    for csr, tol in ((Csr.from_dense(H.grid_7x5()), 1e-13), (H.panels_matrix(), 1e-12)):
+        f = Factor.new(UpperColumns.from_symmetric(csr), 2**62)
+        x = H.sin_solution(csr.n)
+        b = oracle.spmv(csr.n, csr.ptr, csr.idx, csr.val, x)
+        f.solve(b)
+        assert np.max(np.abs(b - x)) < tol
+
+
+def test_errors_match_the_reference(cuda):
+    csr = Csr.from_dense(H.grid_7x5())
+    up = UpperColumns.from_symmetric(csr)
+    with pytest.raises(TooLarge):
+        Factor.new(up, 10)
+    sing = UpperColumns.from_symmetric(Csr.from_dense(H.grid_7x5(shift=False)))
+    with pytest.raises(NotPositiveDefinite) as e:
+        Factor.new(sing, 2**62)
+    assert e.value.column == 34
+    flag = C.c_int32(1)
+    with pytest.raises(Cancelled):
+        Factor.new(up, 2**62, cancel=flag)
+    empty = UpperColumns(0, np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0))
+    f = Factor.new(empty, 10)
+    assert f.entries() == 0
+    f.solve(np.zeros(0))
+    one = UpperColumns.from_symmetric(Csr.from_dense([[4.0]]))
+    f = Factor.new(one, 10)
+    b = np.array([2.0])
+    f.solve(b)
+    assert b.tolist() == [0.5]
+    with pytest.raises(ValueError):
+        f.solve(np.zeros(2))
+
+
+def test_solve_many_is_each_solve_bit_for_bit(cuda):
+    csr = H.panels_matrix()
+    f = Factor.new(UpperColumns.from_symmetric(csr), 2**62)
+    rhs = [np.sin((np.arange(csr.n) * 7 + s * 13) * 0.11) for s in range(5)]
+    alone = []
+    for b in rhs:
+        x = b.copy()
+        f.solve(x)
+        alone.append(x)
+    together = [b.copy() for b in rhs]
+    f.solve_many(together)
+    for a, t in zip(alone, together):
+        assert np.array_equal(a.view(np.uint64), t.view(np.uint64))
+
+
+def test_factorisation_is_deterministic(cuda):
+    csr = problems.lognormal_block(10, nrhs=1).csr
+    up = UpperColumns.from_symmetric(csr)
+    a = Factor.new(up, 2**62).values()
+    b = Factor.new(up, 2**62).values()
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_device_entry_points(cuda):
+    torch = cuda
+    p = problems.lognormal_block(8, nrhs=4)
+    up = p.upper()
+    sym = Symbolic(up, 2**62)
+    f = Factor(sym)
+    st = __import__("fieldcraft_b200._lib", fromlist=["Status"]).Status()
+    from fieldcraft_b200 import _lib
+    lib = _lib.load()
+    dval = torch.from_numpy(up.val).cuda()
+    assert lib.fc_chol_factor_device(f.handle, C.c_void_p(dval.data_ptr()), up.val.size, C.byref(st)) == 0
+    b = torch.from_numpy(np.ascontiguousarray(p.rhs.T)).cuda()  # rows are right-hand sides: column-major n x 4
+    x = b.clone()
+    f.solve_device(x, 4, p.n)
+    _, ref = oracle_factor(p.csr)
+    exp = ref.solve(p.rhs.copy())
+    got = x.cpu().numpy().T
+    assert np.linalg.norm(got - exp) <= SOLVE_TOL * np.linalg.norm(exp)
+    # y = K x on the device (Csr::mul)
+    dptr = torch.from_numpy(p.csr.ptr).cuda()
+    didx = torch.from_numpy(p.csr.idx).cuda()
+    dv = torch.from_numpy(p.csr.val).cuda()
+    y = torch.empty_like(x)
+    assert lib.fc_csr_spmv_device(p.n, C.c_void_p(dptr.data_ptr()), C.c_void_p(didx.data_ptr()),
+                                  C.c_void_p(dv.data_ptr()), C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), 4,
+                                  p.n, None) == 0
+    torch.cuda.synchronize()
+    yref = np.stack([oracle.spmv(p.n, p.csr.ptr, p.csr.idx, p.csr.val, got[:, j]) for j in range(4)], axis=1)
+    assert np.max(np.abs(y.cpu().numpy().T - yref)) <= 1e-12 * np.max(np.abs(yref))
+
+
+@pytest.mark.parametrize("n_el", [20])
+def test_lognormal_block_residual(cuda, n_el):
+    # the benchmark's workload at a size the oracle finishes in seconds: 20^3 elements, 8 RHS
+    p = problems.lognormal_block(n_el, nrhs=8)
+    f = Factor.new(p.upper(), 2**62)
+    x = np.asfortranarray(p.rhs.copy())
+    f.solve_many(x)
+    _, ref = oracle_factor(p.csr)
+    exp = ref.solve(p.rhs.copy())
+    for j in range(x.shape[1]):
+        assert np.linalg.norm(x[:, j] - exp[:, j]) <= SOLVE_TOL * np.linalg.norm(exp[:, j])
+        r = oracle.spmv(p.n, p.csr.ptr, p.csr.idx, p.csr.val, x[:, j]) - p.rhs[:, j]
+        assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(p.rhs[:, j])
