@@ -244,6 +244,30 @@ def main():
             d_r.sub_(d_f)
             return torch.linalg.vector_norm(d_r, dim=1) / fnorm
 
+    if args.profile_only:
+        # the launch counts per step (for choosing which launches a profiler captures), then the
+        # warm-up steps and nothing else
+        kinds = 24
+        ms_k = np.zeros(kinds)
+        cnt_k = np.zeros(kinds, np.int64)
+        lib.fc_chol_profile(f.handle, 1)
+        step()
+        lib.fc_chol_profile_read(f.handle, ms_k.ctypes.data, cnt_k.ctypes.data, kinds)
+        lib.fc_chol_profile(f.handle, 0)
+        for _ in range(args.warmup):
+            relres = step()
+        stream.synchronize()
+        lib.fc_chol_check(f.handle, C.byref(st))
+        raise_for(st)
+        if rank == 0:
+            print(json.dumps({"profile_only": True, "n": n, "gemm_factor_launches": int(cnt_k[3]),
+                              "gemm_big_ordinal": f.stat(11), "gemm_trail_ordinal": f.stat(12),
+                              "gemm_solve_launches": int(cnt_k[19]), "panel_launches": int(cnt_k[1]),
+                              "relres_max": float(relres.max().item())}), flush=True)
+        f.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     for _ in range(args.warmup):
         relres = step()
     stream.synchronize()
@@ -271,9 +295,7 @@ def main():
         ms = float(t.item())
         dist.barrier()
     clocks = clk.summary()
-    if rank != 0 or args.profile_only:
-        if rank == 0:
-            print(json.dumps({"profile_only": True, "ms_per_step": ms, "relres_max": worst}), flush=True)
+    if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
@@ -340,8 +362,13 @@ def main():
         "factor_tflops": full_flops / (factor_ms * 1e-3) / 1e12 if factor_ms > 0 else None,
         "phase_ms": {"factor": factor_ms, "solve": solve_ms,
                      "by_kernel": {name: round(float(ms_k[k]), 3) for k, name in
-                                   [(0, "assemble"), (1, "potrf"), (2, "trsm"), (3, "gemm"), (19, "solve_gemm"),
-                                    (20, "solve_assemble"), (21, "solve_gather"), (22, "trsv"), (23, "trsv_t")]}},
+                                   [(0, "assemble"), (1, "panel"), (3, "gemm"), (19, "solve_gemm"),
+                                    (20, "solve_assemble"), (21, "solve_gather"), (22, "solve_fwd_panel"),
+                                    (23, "solve_bwd_panel")]},
+                     "launches": {name: int(cnt_k[k]) for k, name in
+                                  [(0, "assemble"), (1, "panel"), (3, "gemm"), (19, "solve_gemm"),
+                                   (20, "solve_assemble"), (21, "solve_gather"), (22, "solve_fwd_panel"),
+                                   (23, "solve_bwd_panel")]}},
         "roofline": {"kernel": "gemm_kernel (FP64 DMMA, factor updates)", "bound": "tensor",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "

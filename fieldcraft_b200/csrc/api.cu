@@ -8,6 +8,7 @@
 // the reference's left-looking order (the same numbers up to rounding).
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <map>
 #include <cstdio>
 #include <cstring>
@@ -83,7 +84,7 @@ cudaError_t upload(DeviceBuf &buf, const std::vector<T> &host, cudaStream_t st) 
   return cudaMemcpyAsync(buf.p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, st);
 }
 
-enum Kind { K_ASSEMBLE, K_POTRF, K_TRSM, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_TRSV, K_TRSV_T };
+enum Kind { K_ASSEMBLE, K_PANEL, K_UNUSED, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD };
 
 struct Launch {
   int kind;
@@ -100,7 +101,7 @@ struct fc_chol {
   bool own_stream = false;
   int64_t n = 0, ns = 0, entries = 0, nnz = 0, levels = 0;
   double flops = 0;
-  std::vector<int64_t> first, perm, loff, uoff, rows_off, toff;
+  std::vector<int64_t> first, perm, loff, uoff, rows_off, toff, doff;
   std::vector<int32_t> width, height, rows;
   std::vector<int64_t> kid_ptr;
   std::vector<int32_t> kids;
@@ -108,24 +109,35 @@ struct fc_chol {
   int64_t l_len = 0, u_len = 0;
   // device
   DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
-  DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_perm, d_val, d_status, d_toff;
-  DeviceBuf d_asm, d_potrf, d_trsm, d_gemm;
+  DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_D, d_perm, d_val, d_status, d_toff, d_doff;
+  DeviceBuf d_asm, d_panel, d_gemm;
   fc::Tree tree{};
   std::vector<Launch> program;
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
-  DeviceBuf d_x, d_v, d_voff, d_b, d_srow, d_strsv, d_sgemm;
+  DeviceBuf d_x, d_x2, d_v, d_voff, d_b, d_srow, d_spanel, d_sgemm;
   std::vector<Launch> fwd, bwd;
   int64_t last_factor_launches = 0, last_solve_launches = 0;
   double gemm_flops_factor = 0, gemm_flops_solve = 0;
+  int64_t gemm_big_ordinal = -1, gemm_trail_ordinal = -1;  // the factor's heaviest GEMM launches
   // per-launch event timing (fc_chol_profile)
   bool profiling = false;
+  // captured programs, replayed while their inputs stay the same (FC_NO_GRAPHS=1 disables)
+  bool graphs = true;
+  cudaGraphExec_t factor_graph = nullptr, solve_graph = nullptr;
+  const double *factor_graph_val = nullptr;
+  cudaStream_t factor_graph_stream = nullptr, solve_graph_stream = nullptr;
+  double *solve_graph_b = nullptr;
+  int solve_graph_R = 0;
+  int64_t solve_graph_ld = 0;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
   std::vector<cudaEvent_t> event_pool;
   size_t events_used = 0;
   std::mutex lock;
   ~fc_chol() {
+    if (factor_graph) cudaGraphExecDestroy(factor_graph);
+    if (solve_graph) cudaGraphExecDestroy(solve_graph);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
   }
 };
@@ -227,11 +239,10 @@ int64_t arena_offsets(const fc_chol *h, const std::vector<std::vector<int64_t>> 
   return top;
 }
 
-// The factor's program: per level, assemble; per panel, POTRF, TRSM, update of later columns;
-// then the update matrices.
+// The factor's program: per level, assemble; per panel, the fused factor/invert/solve of the
+// panel, then the update of the later columns; then the update matrices.
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
-                 std::vector<fc::PanelTask> &potrf_t, std::vector<fc::PanelTask> &trsm_t,
-                 std::vector<fc::GemmTask> &gemm_t) {
+                 std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
   double *L = h->d_L.as<double>();
   double *U = h->d_U.as<double>();
   const int NB = fc::NB;
@@ -247,15 +258,16 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = 0; p < P; ++p) {
-      int64_t po = (int64_t)potrf_t.size(), to = (int64_t)trsm_t.size(), go = (int64_t)gemm_t.size();
+      int64_t po = (int64_t)panel_t.size(), go = (int64_t)gemm_t.size();
       for (int64_t s : S) {
         const int m = h->height[s], w = h->width[s];
         const int c0 = p * NB;
         if (c0 >= w) continue;
         const int c1 = std::min(w, c0 + NB);
-        potrf_t.push_back({(int32_t)s, c0, c1, 0, 0, 0});
-        for (int r0 = c1; r0 < m; r0 += fc::TRSM_ROWS)
-          trsm_t.push_back({(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::TRSM_ROWS), 0});
+        const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
+        if (c1 >= m) panel_t.push_back({(int32_t)s, c0, c1, m, m, 1, doff});
+        for (int r0 = c1; r0 < m; r0 += fc::PANEL_ROWS)
+          panel_t.push_back({(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff});
         double *Ls = L + h->loff[s];
         for (int jc = c1; jc < w; jc += fc::GEMM_TN)
           for (int ic = jc; ic < m; ic += fc::GEMM_TM) {
@@ -271,8 +283,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             gemm_t.push_back(g);
           }
       }
-      push(h->program, K_POTRF, po, (int64_t)potrf_t.size() - po, (int)l);
-      push(h->program, K_TRSM, to, (int64_t)trsm_t.size() - to, (int)l);
+      push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l);
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
     }
     int64_t go = (int64_t)gemm_t.size();
@@ -315,7 +326,8 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   h->loff.resize(ns);
   h->uoff.resize(ns);
   h->toff.resize(ns);
-  int64_t lsum = 0, usum = 0, tsum = 0;
+  h->doff.resize(ns);
+  int64_t lsum = 0, usum = 0, tsum = 0, dsum = 0;
   double flops = 0;
   for (int64_t s = 0; s < ns; ++s) {
     const int64_t m = sym.height(s), w = sym.width(s), u = m - w;
@@ -326,6 +338,11 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
     lsum += m * w;
     usum += u * u;
     tsum += fc::trapezoid(m, w);
+    h->doff[s] = dsum;
+    {
+      const int64_t full = w / fc::NB, last = w % fc::NB;
+      dsum += 2 * (int64_t)fc::NB * fc::NB * full + 2 * last * last;
+    }
     for (int64_t c = 0; c < w; ++c) flops += (double)(m - c) * (double)(m - c);
   }
   h->l_len = lsum;
@@ -420,9 +437,11 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   UP(h->d_diag_src, diag_src);
   UP(h->d_perm, h->perm);
   UP(h->d_toff, h->toff);
+  UP(h->d_doff, h->doff);
 #undef UP
   if (h->d_L.alloc(sizeof(double) * (size_t)std::max<int64_t>(lsum, 1)) != cudaSuccess ||
       h->d_U.alloc(sizeof(double) * (size_t)std::max<int64_t>(usum, 1)) != cudaSuccess ||
+      h->d_D.alloc(sizeof(double) * (size_t)std::max<int64_t>(dsum, 1)) != cudaSuccess ||
       h->d_val.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->nnz, 1)) != cudaSuccess ||
       h->d_status.alloc(sizeof(fc::DeviceStatus)) != cudaSuccess) {
     Failure f;
@@ -447,17 +466,37 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   t.a_src = h->d_a_src.as<int64_t>();
   t.a_dst = h->d_a_dst.as<int64_t>();
   t.diag_src = h->d_diag_src.as<int64_t>();
+  t.doff = h->d_doff.as<int64_t>();
   t.L = h->d_L.as<double>();
   t.U = h->d_U.as<double>();
+  t.D = h->d_D.as<double>();
   std::vector<fc::AssembleTask> asm_t;
-  std::vector<fc::PanelTask> potrf_t, trsm_t;
+  std::vector<fc::PanelTask> panel_t;
   std::vector<fc::GemmTask> gemm_t;
-  plan_factor(h, lv, asm_t, potrf_t, trsm_t, gemm_t);
+  plan_factor(h, lv, asm_t, panel_t, gemm_t);
   h->gemm_tasks = (int64_t)gemm_t.size();
   h->gemm_flops_factor = 0;
   for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
-  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_potrf, potrf_t, stream)) != cudaSuccess ||
-      (e = upload(h->d_trsm, trsm_t, stream)) != cudaSuccess || (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
+  {
+    // ordinals (among the factor's GEMM launches) of the heaviest launch and of the heaviest one
+    // whose tasks all have K <= NB (a panel's update of the later columns)
+    int64_t ordinal = 0;
+    double big = -1, trail = -1;
+    for (const Launch &l : h->program) {
+      if (l.kind != K_GEMM) continue;
+      double fl = 0;
+      int kmax = 0;
+      for (int64_t q = l.off; q < l.off + l.count; ++q) {
+        fl += task_flops(gemm_t[q]);
+        kmax = std::max(kmax, gemm_t[q].K);
+      }
+      if (fl > big) big = fl, h->gemm_big_ordinal = ordinal;
+      if (kmax <= fc::NB && fl > trail) trail = fl, h->gemm_trail_ordinal = ordinal;
+      ++ordinal;
+    }
+  }
+  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_panel, panel_t, stream)) != cudaSuccess ||
+      (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
     return cuda_fail(st, e, "upload of the plan");
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
   return FC_OK;
@@ -492,8 +531,55 @@ struct Mark {
   }
 };
 
-// Enqueues the factor's program. Returns FC_CANCELLED when the flag was set between levels.
+// Runs `enqueue` under stream capture and keeps the instantiated graph in *exec; false if the
+// capture or the instantiation failed (the work is then enqueued directly by the caller).
+template <class F>
+bool capture(fc_chol *h, cudaGraphExec_t *exec, F enqueue) {
+  if (*exec) {
+    cudaGraphExecDestroy(*exec);
+    *exec = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  enqueue();
+  cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+  if (e != cudaSuccess || !graph) {
+    cudaGetLastError();
+    return false;
+  }
+  e = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *exec = nullptr;
+    return false;
+  }
+  return true;
+}
+
+int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_t *cancel);
+
+// Enqueues the factor's program (as a replayed graph when it can). Returns FC_CANCELLED when the
+// flag was set between levels.
 int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
+  if (cancel || h->profiling || !h->graphs) return enqueue_factor_direct(h, d_val, cancel);
+  if (!h->factor_graph || h->factor_graph_val != d_val || h->factor_graph_stream != h->stream) {
+    if (!capture(h, &h->factor_graph, [&] { enqueue_factor_direct(h, d_val, nullptr); })) {
+      h->graphs = false;
+      return enqueue_factor_direct(h, d_val, nullptr);
+    }
+    h->factor_graph_val = d_val;
+    h->factor_graph_stream = h->stream;
+  }
+  cudaGraphLaunch(h->factor_graph, h->stream);
+  h->last_factor_launches = (int64_t)h->program.size();
+  return FC_OK;
+}
+
+int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
   cudaStream_t st = h->stream;
   cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), st);
   const fc::Tree &t = h->tree;
@@ -510,10 +596,9 @@ int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *canc
     Mark mark(h, l.kind);
     switch (l.kind) {
       case K_ASSEMBLE: fc::launch_assemble(t, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, l.count, st); break;
-      case K_POTRF:
-        fc::launch_potrf(t, d_val, h->d_potrf.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(), st);
+      case K_PANEL:
+        fc::launch_panel(t, d_val, h->d_panel.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(), st);
         break;
-      case K_TRSM: fc::launch_trsm(t, h->d_trsm.as<fc::PanelTask>() + l.off, l.count, st); break;
       case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, st); break;
     }
     ++launches;
@@ -537,9 +622,17 @@ int read_status(fc_chol *h, fc_status *st) {
   return FC_OK;
 }
 
-// The solve's program for R right-hand sides (built once per R).
+// The solve's program for R right-hand sides (built once per R). Forward, level by level: each
+// supernode's front collects its children's update vectors, then panel by panel y = Linv x and the
+// rows below -= L y (x accumulates, y lands in x2). Backward, top level first: gather the final
+// values of the rows past the columns, own rows -= L21^T v, then panel by panel from the last
+// z = Linv^T x2 and the own rows above -= L^T z (x2 accumulates, z lands in x).
 int plan_solve(fc_chol *h, int R, fc_status *st) {
   if (h->solve_R == R) return FC_OK;
+  if (h->solve_graph) {
+    cudaGraphExecDestroy(h->solve_graph);
+    h->solve_graph = nullptr;
+  }
   const int NB = fc::NB;
   std::vector<std::vector<int64_t>> lv(h->levels);
   for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
@@ -548,6 +641,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   const int64_t vsum = arena_offsets(h, lv, vsize, voff);
   cudaError_t e;
   if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
+      h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
       h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(vsum, 1)) != cudaSuccess) {
     h->solve_R = 0;
     set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
@@ -555,36 +649,11 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   }
   if ((e = upload(h->d_voff, voff, h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
   std::vector<fc::RowTask> rows;
-  std::vector<fc::SolveTask> trsv;
+  std::vector<fc::SolveTask> panels;
   std::vector<fc::GemmTask> gemm;
-  double *L = h->d_L.as<double>(), *x = h->d_x.as<double>(), *v = h->d_v.as<double>();
+  double *L = h->d_L.as<double>(), *x = h->d_x.as<double>(), *x2 = h->d_x2.as<double>(), *v = h->d_v.as<double>();
   h->fwd.clear();
   h->bwd.clear();
-  auto gemm_rows = [&](int64_t s, int r0, int r1, int c0, int c1) {
-    // front rows [r0, r1) -= L[rows, c0:c1] x[own c0:c1], split at w (own rows in x, the rest in v)
-    const int m = h->height[s], w = h->width[s];
-    const double *Ls = L + h->loff[s];
-    for (int i0 = r0; i0 < r1;) {
-      const int lim = i0 < w ? std::min(r1, w) : r1;
-      const int i1 = std::min(lim, i0 + fc::GEMM_TM);
-      for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
-        fc::GemmTask g{};
-        g.C = i0 < w ? x + (h->first[s] + i0) * (int64_t)R + j0 : v + voff[s] + (int64_t)(i0 - w) * R + j0;
-        g.c_si = R, g.c_sj = 1;
-        g.A = Ls + i0 + (int64_t)c0 * m;
-        g.a_si = 1, g.a_sk = m;
-        g.B = x + (h->first[s] + c0) * (int64_t)R + j0;
-        g.b_sj = 1, g.b_sk = R;
-        g.M = i1 - i0;
-        g.N = std::min(fc::GEMM_TN, R - j0);
-        g.K = c1 - c0;
-        g.flags = 0;
-        gemm.push_back(g);
-      }
-      i0 = i1;
-    }
-  };
-  auto pushs = [&](std::vector<Launch> &prog, int kind, int64_t off, int64_t count, int l) { push(prog, kind, off, count, l); };
   // forward
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
@@ -595,20 +664,30 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
       if (!kids && m == w) continue;
       for (int i0 = kids ? 0 : w; i0 < m; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(m, i0 + 64), 0});
     }
-    pushs(h->fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
+    push(h->fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = 0; p < P; ++p) {
-      int64_t to = (int64_t)trsv.size(), go = (int64_t)gemm.size();
+      int64_t po = (int64_t)panels.size();
       for (int64_t s : S) {
         const int m = h->height[s], w = h->width[s], c0 = p * NB;
         if (c0 >= w) continue;
         const int c1 = std::min(w, c0 + NB);
-        for (int j0 = 0; j0 < R; j0 += 64) trsv.push_back({(int32_t)s, c0, c1, j0, std::min(R, j0 + 64), 0});
-        if (c1 < m) gemm_rows(s, c1, m, c0, c1);
+        const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
+        for (int j0 = 0; j0 < R; j0 += 64) {
+          const int j1 = std::min(R, j0 + 64);
+          if (c1 >= m) panels.push_back({(int32_t)s, c0, c1, m, m, j0, j1, 1, doff});
+          bool first = true;
+          for (int i0 = c1; i0 < m;) {
+            const int lim = i0 < w ? std::min(m, w) : m;
+            const int i1 = std::min(lim, i0 + 64);
+            panels.push_back({(int32_t)s, c0, c1, i0, i1, j0, j1, first ? 1 : 0, doff});
+            first = false;
+            i0 = i1;
+          }
+        }
       }
-      pushs(h->fwd, K_TRSV, to, (int64_t)trsv.size() - to, (int)l);
-      pushs(h->fwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+      push(h->fwd, K_SOLVE_FWD, po, (int64_t)panels.size() - po, (int)l);
     }
   }
   // backward
@@ -619,7 +698,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
       const int u = h->height[s] - h->width[s];
       for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
     }
-    pushs(h->bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
+    push(h->bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
     int64_t go = (int64_t)gemm.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
@@ -628,7 +707,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
       for (int i0 = 0; i0 < w; i0 += fc::GEMM_TM)
         for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
           fc::GemmTask g{};
-          g.C = x + (h->first[s] + i0) * (int64_t)R + j0;
+          g.C = x2 + (h->first[s] + i0) * (int64_t)R + j0;
           g.c_si = R, g.c_sj = 1;
           g.A = Ls + w + (int64_t)i0 * m;
           g.a_si = m, g.a_sk = 1;
@@ -640,39 +719,29 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
           gemm.push_back(g);
         }
     }
-    pushs(h->bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+    push(h->bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = P - 1; p >= 0; --p) {
-      int64_t to = (int64_t)trsv.size(), go2 = (int64_t)gemm.size();
+      int64_t po = (int64_t)panels.size();
       for (int64_t s : S) {
-        const int m = h->height[s], w = h->width[s], c0 = p * NB;
+        const int w = h->width[s], c0 = p * NB;
         if (c0 >= w) continue;
         const int c1 = std::min(w, c0 + NB);
-        for (int j0 = 0; j0 < R; j0 += 64) trsv.push_back({(int32_t)s, c0, c1, j0, std::min(R, j0 + 64), 0});
-        const double *Ls = L + h->loff[s];
-        for (int i0 = 0; i0 < c0; i0 += fc::GEMM_TM)
-          for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
-            fc::GemmTask g{};
-            g.C = x + (h->first[s] + i0) * (int64_t)R + j0;
-            g.c_si = R, g.c_sj = 1;
-            g.A = Ls + c0 + (int64_t)i0 * m;
-            g.a_si = m, g.a_sk = 1;
-            g.B = x + (h->first[s] + c0) * (int64_t)R + j0;
-            g.b_sj = 1, g.b_sk = R;
-            g.M = std::min(fc::GEMM_TM, c0 - i0);
-            g.N = std::min(fc::GEMM_TN, R - j0);
-            g.K = c1 - c0;
-            gemm.push_back(g);
-          }
+        const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
+        for (int j0 = 0; j0 < R; j0 += 64) {
+          const int j1 = std::min(R, j0 + 64);
+          if (c0 == 0) panels.push_back({(int32_t)s, c0, c1, 0, 0, j0, j1, 1, doff});
+          for (int i0 = 0; i0 < c0; i0 += 64)
+            panels.push_back({(int32_t)s, c0, c1, i0, std::min(c0, i0 + 64), j0, j1, i0 == 0 ? 1 : 0, doff});
+        }
       }
-      pushs(h->bwd, K_TRSV_T, to, (int64_t)trsv.size() - to, (int)l);
-      pushs(h->bwd, K_GEMM, go2, (int64_t)gemm.size() - go2, (int)l);
+      push(h->bwd, K_SOLVE_BWD, po, (int64_t)panels.size() - po, (int)l);
     }
   }
   h->gemm_flops_solve = 0;
   for (const auto &g : gemm) h->gemm_flops_solve += task_flops(g);
-  if ((e = upload(h->d_srow, rows, h->stream)) != cudaSuccess || (e = upload(h->d_strsv, trsv, h->stream)) != cudaSuccess ||
+  if ((e = upload(h->d_srow, rows, h->stream)) != cudaSuccess || (e = upload(h->d_spanel, panels, h->stream)) != cudaSuccess ||
       (e = upload(h->d_sgemm, gemm, h->stream)) != cudaSuccess)
     return cuda_fail(st, e, "solve plan");
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
@@ -684,7 +753,7 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, int64_t &lau
   cudaStream_t st = h->stream;
   const fc::Tree &t = h->tree;
   const int R = h->solve_R;
-  double *x = h->d_x.as<double>(), *v = h->d_v.as<double>();
+  double *x = h->d_x.as<double>(), *x2 = h->d_x2.as<double>(), *v = h->d_v.as<double>();
   const int64_t *voff = h->d_voff.as<int64_t>();
   for (const Launch &l : prog) {
     Mark mark(h, l.kind + 16);
@@ -695,25 +764,54 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, int64_t &lau
       case K_SOLVE_GATHER:
         fc::launch_solve_gather(t, x, v, voff, R, h->d_srow.as<fc::RowTask>() + l.off, l.count, st);
         break;
-      case K_TRSV: fc::launch_trsv(t, x, R, false, h->d_strsv.as<fc::SolveTask>() + l.off, l.count, st); break;
-      case K_TRSV_T: fc::launch_trsv(t, x, R, true, h->d_strsv.as<fc::SolveTask>() + l.off, l.count, st); break;
+      case K_SOLVE_FWD:
+        fc::launch_solve_panel(t, false, x, x2, v, voff, R, h->d_spanel.as<fc::SolveTask>() + l.off, l.count, st);
+        break;
+      case K_SOLVE_BWD:
+        fc::launch_solve_panel(t, true, x, x2, v, voff, R, h->d_spanel.as<fc::SolveTask>() + l.off, l.count, st);
+        break;
       case K_GEMM: fc::launch_gemm(h->d_sgemm.as<fc::GemmTask>() + l.off, l.count, st); break;
     }
     ++launches;
   }
 }
 
-// Solves for the R right-hand sides in device memory at d_b (column-major, leading dimension ld).
+void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld);
+
+// Solves for the R right-hand sides in device memory at d_b (column-major, leading dimension ld),
+// as a replayed graph when it can.
 int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
+  const int before = h->solve_R;
   int rc = plan_solve(h, R, st);
   if (rc != FC_OK) return rc;
+  if (h->profiling || !h->graphs) {
+    enqueue_solve_direct(h, d_b, R, ld);
+    return FC_OK;
+  }
+  if (!h->solve_graph || before != R || h->solve_graph_b != d_b || h->solve_graph_R != R || h->solve_graph_ld != ld ||
+      h->solve_graph_stream != h->stream) {
+    if (!capture(h, &h->solve_graph, [&] { enqueue_solve_direct(h, d_b, R, ld); })) {
+      h->graphs = false;
+      enqueue_solve_direct(h, d_b, R, ld);
+      return FC_OK;
+    }
+    h->solve_graph_b = d_b;
+    h->solve_graph_R = R;
+    h->solve_graph_ld = ld;
+    h->solve_graph_stream = h->stream;
+  }
+  cudaGraphLaunch(h->solve_graph, h->stream);
+  h->last_solve_launches = (int64_t)(h->fwd.size() + h->bwd.size() + 2);
+  return FC_OK;
+}
+
+void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   int64_t launches = 0;
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->stream);
   run_solve_program(h, h->fwd, launches);
   run_solve_program(h, h->bwd, launches);
   fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->stream);
   h->last_solve_launches = launches + 2;
-  return FC_OK;
 }
 
 }  // namespace
@@ -863,6 +961,11 @@ int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **
   }
   h->device = device;
   h->precision = precision;
+  {
+    const char *env = std::getenv("FC_NO_GRAPHS");
+    h->graphs = !(env && env[0] == '1');
+  }
+  fc::configure_kernels();
   if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
     delete h;
     return cuda_fail(status, e, "cudaStreamCreate");
@@ -1055,6 +1158,8 @@ int64_t fc_chol_stat(const fc_chol *h, int what) {
     case 8: return h->last_solve_launches;
     case 9: return (int64_t)h->gemm_flops_factor;
     case 10: return (int64_t)h->gemm_flops_solve;
+    case 11: return h->gemm_big_ordinal;
+    case 12: return h->gemm_trail_ordinal;
   }
   return -1;
 }

@@ -90,81 +90,181 @@ __global__ void __launch_bounds__(256) assemble_kernel(Tree t, const double *__r
   }
 }
 
-// ---- diagonal block: unblocked right-looking Cholesky of a <= 64 x 64 block in shared memory ----
-// Pivot test of cholesky.rs:1162-1165: not (d > PIVOT_TOLERANCE |A_jj|) or not finite fails; the
-// smallest failing column (postorder) is kept in the status word. A failed pivot makes NaNs and
-// nothing else: no index depends on a value.
-__global__ void __launch_bounds__(256) potrf_kernel(Tree t, const double *__restrict__ val,
-                                                    const PanelTask *__restrict__ tasks, DeviceStatus *status) {
-  __shared__ double a[NB * (NB + 1)];
-  __shared__ double dpiv;
+// ---- shared-memory tiles and the DMMA product of two of them --------------------------------------
+// A tile holds 64 x 64 doubles as [k][i] with row stride TS (padded so a warp's fragment reads
+// of 4 k-rows x 8 consecutive doubles fall in distinct banks).
+constexpr int TS = 68;
+
+// dst[k * TS + i] = src[i * si + k * sk] for i < rows, k < kk, zero for the other i < 64 and
+// kk <= k < kpad (rows k >= kpad of the tile are not touched). One warp per k (rows contiguous in
+// memory) or one warp per i (k contiguous), so every warp reads a contiguous run.
+__device__ __forceinline__ void load_tile(double *dst, const double *__restrict__ src, int64_t si, int64_t sk, int rows,
+                                          int kk, int kpad) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (si == 1) {
+    for (int k = warp; k < kpad; k += nw)
+      for (int i = lane; i < 64; i += 32)
+        dst[k * TS + i] = (i < rows && k < kk) ? src[i + (int64_t)k * sk] : 0.0;
+  } else {
+    for (int i = warp; i < 64; i += nw)
+      for (int k = lane; k < kpad; k += 32)
+        dst[k * TS + i] = (i < rows && k < kk) ? src[(int64_t)i * si + k * sk] : 0.0;
+  }
+}
+
+// acc(i, j) += sum_{k < K} As[k][i] Bs[k][j] over a 64 x 64 output, 4 warps of 32 x 32.
+__device__ __forceinline__ void mma_tiles(const double *As, const double *Bs, int K, double (&acc)[4][4][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  for (int kk = 0; kk < K; kk += 4) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) av[r] = As[(kk + tg) * TS + wm + r * 8 + g];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bv[c] = Bs[(kk + tg) * TS + wn + c * 8 + g];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dmma(acc[r][c], av[r], bv[c]);
+  }
+}
+
+__device__ __forceinline__ void zero_acc(double (&acc)[4][4][2]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
+}
+
+// Calls f(i, j, value) for every output of a 64 x 64 accumulator held by this thread.
+template <class F>
+__device__ __forceinline__ void each_acc(const double (&acc)[4][4][2], F f) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) f(wm + r * 8 + g, wn + c * 8 + 2 * tg + e, acc[r][c][e]);
+}
+
+// ---- panel: factor the diagonal block, invert it, solve the rows below --------------------------
+// The block (pw <= 64 columns) is factored right-looking in shared memory; the pivot test is the
+// reference's (cholesky.rs:1162-1165): not (d > PIVOT_TOLERANCE |A_jj|) or not finite fails, and
+// the smallest failing column (postorder) is kept in the status word. A failed pivot makes NaNs
+// and nothing else: no index depends on a value. The inverse comes from 8 x 8 diagonal blocks and
+// block forward substitution; the rows below are X = B L^-T on the FP64 tensor pipe.
+constexpr int PANEL_THREADS = 128;
+constexpr size_t PANEL_SMEM = sizeof(double) * (64 * 65 + 2 * 64 * TS + 512 + 128);
+
+__global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const double *__restrict__ val,
+                                                              const PanelTask *__restrict__ tasks,
+                                                              DeviceStatus *status) {
+  extern __shared__ double sm[];
+  double *a = sm;                 // factor, column-major, ld 65
+  double *inv = a + 64 * 65;      // inv[k * TS + i] = Linv(i, k)
+  double *bt = inv + 64 * TS;     // rows below: bt[k * TS + r] = L(r0 + r, c0 + k)
+  double *tt = bt + 64 * TS;      // 8 x (8 x 8) scratch of the inversion
+  double *dg = tt + 512;          // the matrix's own diagonal entries of the panel's columns
+  double *dv = dg + 64;           // the pivots
+  __shared__ int fail;
   const PanelTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], f = t.first[s];
   double *Ls = t.L + t.loff[s];
-  const int c0 = task.c0, pw = task.c1 - task.c0;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < pw * pw; e += blockDim.x) {
-    const int r = e % pw, c = e / pw;
-    if (r >= c) a[c * (NB + 1) + r] = Ls[(c0 + r) + (int64_t)(c0 + c) * m];
+  const int c0 = task.c0, pw = task.c1 - task.c0, rows = task.r1 - task.r0;
+  const int nb8 = (pw + 7) >> 3, P8 = 8 * nb8, K4 = (pw + 3) & ~3;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) fail = pw;
+  // the block's lower triangle, identity past pw (so the padded block inverts to the same
+  // leading pw x pw inverse)
+  for (int c = warp; c < P8; c += PANEL_THREADS / 32)
+    for (int r = lane; r < P8; r += 32)
+      a[c * 65 + r] = (r < pw && c < pw) ? (r >= c ? Ls[(c0 + r) + (int64_t)(c0 + c) * m] : 0.0) : (r == c ? 1.0 : 0.0);
+  for (int c = tid; c < pw; c += PANEL_THREADS) {
+    const int64_t ds = t.diag_src[f + c0 + c];
+    dg[c] = ds >= 0 ? val[ds] : 0.0;
   }
+  for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
+  if (rows > 0) load_tile(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);
   __syncthreads();
+  // right-looking: column c scaled by its pivot, then the trailing triangle; two threads a row
+  const int ri = tid & 63, rh = tid >> 6;
   for (int c = 0; c < pw; ++c) {
+    const double acc = a[c * 65 + c];
+    const double d = sqrt(acc);
+    if (ri > c && ri < pw && rh == 0) a[c * 65 + ri] /= d;
     if (tid == 0) {
-      double d = a[c * (NB + 1) + c];
-      const int64_t col = f + c0 + c;
-      const int64_t ds = t.diag_src[col];
-      const double diag = ds >= 0 ? val[ds] : 0.0;
-      if (!(d > PIVOT_TOLERANCE * fabs(diag)) || !isfinite(d))
-        atomicMin(&status->failed_column, (unsigned long long)col);
-      d = sqrt(d);
-      a[c * (NB + 1) + c] = d;
-      dpiv = d;
+      dv[c] = d;
+      if ((!(acc > PIVOT_TOLERANCE * fabs(dg[c])) || !isfinite(acc)) && fail == pw) fail = c;
     }
     __syncthreads();
-    const double d = dpiv;
-    for (int r = c + 1 + tid; r < pw; r += blockDim.x) a[c * (NB + 1) + r] /= d;
-    __syncthreads();
-    const int rem = pw - c - 1;
-    for (int e = tid; e < rem * rem; e += blockDim.x) {
-      const int i = c + 1 + e % rem, j = c + 1 + e / rem;
-      if (i >= j) a[j * (NB + 1) + i] -= a[c * (NB + 1) + i] * a[c * (NB + 1) + j];
+    if (ri > c && ri < pw) {
+      const double lic = a[c * 65 + ri];
+      for (int j = c + 1 + rh; j <= ri; j += 2) a[j * 65 + ri] -= lic * a[c * 65 + j];
     }
     __syncthreads();
   }
-  for (int e = tid; e < pw * pw; e += blockDim.x) {
-    const int r = e % pw, c = e / pw;
-    if (r >= c) Ls[(c0 + r) + (int64_t)(c0 + c) * m] = a[c * (NB + 1) + r];
-  }
-}
-
-// ---- rows below a factored diagonal block: X = B L^-T, one row per thread -------------------------
-__global__ void __launch_bounds__(TRSM_ROWS) trsm_kernel(Tree t, const PanelTask *__restrict__ tasks) {
-  extern __shared__ double smem[];
-  double *a = smem;                     // NB x (NB+1)
-  double *x = smem + NB * (NB + 1);     // NB x TRSM_ROWS, x[k * TRSM_ROWS + r]
-  const PanelTask task = tasks[blockIdx.x];
-  const int s = task.s;
-  const int64_t m = t.height[s];
-  double *Ls = t.L + t.loff[s];
-  const int c0 = task.c0, pw = task.c1 - task.c0;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < pw * pw; e += blockDim.x) {
-    const int r = e % pw, c = e / pw;
-    if (r >= c) a[c * (NB + 1) + r] = Ls[(c0 + r) + (int64_t)(c0 + c) * m];
-  }
-  const int64_t row = task.r0 + tid;
-  const bool active = row < task.r1;
-  if (active)
-    for (int k = 0; k < pw; ++k) x[k * TRSM_ROWS + tid] = Ls[row + (int64_t)(c0 + k) * m];
+  for (int c = tid; c < pw; c += PANEL_THREADS) a[c * 65 + c] = dv[c];
   __syncthreads();
-  if (active) {
-    for (int c = 0; c < pw; ++c) {
-      double acc = x[c * TRSM_ROWS + tid];
-      for (int k = 0; k < c; ++k) acc -= x[k * TRSM_ROWS + tid] * a[k * (NB + 1) + c];
-      x[c * TRSM_ROWS + tid] = acc / a[c * (NB + 1) + c];
+  // inverse: the diagonal 8 x 8 blocks (a column each) ...
+  if (tid < P8) {
+    const int B = tid >> 3, j = tid & 7, o = 8 * B;
+    double y[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      if (i >= j) {
+        double sum = i == j ? 1.0 : 0.0;
+        for (int k = j; k < i; ++k) sum -= a[(o + k) * 65 + o + i] * y[k];
+        y[i] = sum / a[(o + i) * 65 + o + i];
+      } else {
+        y[i] = 0.0;
+      }
+      inv[(o + j) * TS + o + i] = y[i];
     }
-    for (int k = 0; k < pw; ++k) Ls[row + (int64_t)(c0 + k) * m] = x[k * TRSM_ROWS + tid];
+  }
+  __syncthreads();
+  // ... then block forward substitution: Linv_IJ = -Linv_II sum_{K=J}^{I-1} L_IK Linv_KJ
+  for (int d = 1; d < nb8; ++d) {
+    const int outputs = (nb8 - d) * 64;
+    for (int e = tid; e < outputs; e += PANEL_THREADS) {
+      const int J = e >> 6, I = J + d, i = (e >> 3) & 7, j = e & 7;
+      double sum = 0.0;
+      for (int K = J; K < I; ++K)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) sum += a[(8 * K + k) * 65 + 8 * I + i] * inv[(8 * J + j) * TS + 8 * K + k];
+      tt[J * 64 + i * 8 + j] = sum;
+    }
+    __syncthreads();
+    for (int e = tid; e < outputs; e += PANEL_THREADS) {
+      const int J = e >> 6, I = J + d, i = (e >> 3) & 7, j = e & 7;
+      double sum = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sum -= inv[(8 * I + k) * TS + 8 * I + i] * tt[J * 64 + k * 8 + j];
+      inv[(8 * J + j) * TS + 8 * I + i] = sum;
+    }
+    __syncthreads();
+  }
+  if (task.keep) {
+    double *Dp = t.D + task.doff;
+    for (int c = warp; c < pw; c += PANEL_THREADS / 32)
+      for (int r = lane; r < pw; r += 32) {
+        Dp[c * pw + r] = r >= c ? a[c * 65 + r] : 0.0;
+        Dp[pw * pw + c * pw + r] = inv[c * TS + r];
+      }
+    if (tid == 0 && fail < pw) atomicMin(&status->failed_column, (unsigned long long)(f + c0 + fail));
+  }
+  if (rows > 0) {
+    double acc[4][4][2];
+    zero_acc(acc);
+    mma_tiles(bt, inv, K4, acc);
+    double *dst = Ls + task.r0 + (int64_t)c0 * m;
+    each_acc(acc, [&](int i, int c, double v) {
+      if (i < rows && c < pw) dst[i + (int64_t)c * m] = v;
+    });
   }
 }
 
@@ -304,48 +404,59 @@ __global__ void __launch_bounds__(256) solve_gather_kernel(Tree t, const double 
   }
 }
 
-// Own rows [c0, c1) of supernode s, right-hand sides [j0, j1): forward (L) or backward (L^T)
-// substitution with the diagonal block; one right-hand side per thread.
-__global__ void __launch_bounds__(64) trsv_kernel(Tree t, double *__restrict__ x, int R, int transpose,
-                                                  const SolveTask *__restrict__ tasks) {
-  extern __shared__ double smem[];
-  double *a = smem;                 // NB x (NB+1)
-  double *xs = smem + NB * (NB + 1);  // NB x 64, xs[r * 64 + j]
+// Panel [c0, c1) of supernode s for right-hand sides [j0, j1), with the inverse of its diagonal
+// block from the diagonal arena. Forward: y = Linv x_p (x -> x2), then the front rows [r0, r1)
+// below the panel -= L(rows, panel) y (own rows in x, rows past the columns in v). Backward:
+// z = Linv^T x2_p (x2 -> x), then the own rows [r0, r1) above -= L(panel, rows)^T z in x2.
+constexpr size_t SOLVE_SMEM = sizeof(double) * 3 * 64 * TS;
+
+template <bool BACKWARD>
+__global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__restrict__ x, double *__restrict__ x2,
+                                                         double *__restrict__ v, const int64_t *__restrict__ voff, int R,
+                                                         const SolveTask *__restrict__ tasks) {
+  extern __shared__ double sm[];
+  double *inv = sm, *xs = sm + 64 * TS, *bt = sm + 2 * 64 * TS;
   const SolveTask task = tasks[blockIdx.x];
   const int s = task.s;
-  const int64_t m = t.height[s], f = t.first[s];
+  const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
   const double *Ls = t.L + t.loff[s];
-  const int c0 = task.c0, pw = task.c1 - task.c0, j0 = task.j0, nj = task.j1 - task.j0;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < pw * pw; e += blockDim.x) {
-    const int r = e % pw, c = e / pw;
-    if (r >= c) a[c * (NB + 1) + r] = Ls[(c0 + r) + (int64_t)(c0 + c) * m];
-  }
-  for (int e = tid; e < pw * nj; e += blockDim.x) {
-    const int r = e / nj, j = e % nj;
-    xs[r * 64 + j] = x[(f + c0 + r) * R + j0 + j];
-  }
-  __syncthreads();
-  if (tid < nj) {
-    if (!transpose) {
-      for (int r = 0; r < pw; ++r) {
-        double acc = xs[r * 64 + tid];
-        for (int k = 0; k < r; ++k) acc -= a[k * (NB + 1) + r] * xs[k * 64 + tid];
-        xs[r * 64 + tid] = acc / a[r * (NB + 1) + r];
-      }
-    } else {
-      for (int r = pw - 1; r >= 0; --r) {
-        double acc = xs[r * 64 + tid];
-        for (int k = r + 1; k < pw; ++k) acc -= a[r * (NB + 1) + k] * xs[k * 64 + tid];
-        xs[r * 64 + tid] = acc / a[r * (NB + 1) + r];
-      }
-    }
+  const double *Li = t.D + task.doff + (int64_t)(task.c1 - task.c0) * (task.c1 - task.c0);
+  const int c0 = task.c0, pw = task.c1 - task.c0, rows = task.r1 - task.r0, j0 = task.j0, nj = task.j1 - task.j0;
+  double *src = BACKWARD ? x2 : x;
+  double *out = BACKWARD ? x : x2;
+  const int K4 = (pw + 3) & ~3;
+  if (BACKWARD)
+    load_tile(inv, Li, pw, 1, pw, pw, K4);  // inv[k][i] = Linv(k, i)
+  else
+    load_tile(inv, Li, 1, pw, pw, pw, K4);  // inv[k][i] = Linv(i, k)
+  load_tile(xs, src + (f + c0) * R + j0, 1, R, nj, pw, K4);
+  if (rows > 0) {
+    if (BACKWARD)
+      load_tile(bt, Ls + c0 + task.r0 * m, m, 1, rows, pw, K4);  // bt[k][r] = L(c0 + k, r0 + r)
+    else
+      load_tile(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);  // bt[k][r] = L(r0 + r, c0 + k)
   }
   __syncthreads();
-  for (int e = tid; e < pw * nj; e += blockDim.x) {
-    const int r = e / nj, j = e % nj;
-    x[(f + c0 + r) * R + j0 + j] = xs[r * 64 + j];
-  }
+  double acc[4][4][2];
+  zero_acc(acc);
+  mma_tiles(inv, xs, K4, acc);
+  __syncthreads();
+  each_acc(acc, [&](int i, int j, double val) {
+    if (i < K4) xs[i * TS + j] = val;
+    if (task.keep && i < pw && j < nj) out[(f + c0 + i) * R + j0 + j] = val;
+  });
+  if (rows <= 0) return;
+  __syncthreads();
+  zero_acc(acc);
+  mma_tiles(bt, xs, K4, acc);
+  double *dst;
+  if (BACKWARD)
+    dst = x2 + (f + task.r0) * R + j0;
+  else
+    dst = task.r0 < w ? x + (f + task.r0) * R + j0 : v + voff[s] + (task.r0 - w) * R + j0;
+  each_acc(acc, [&](int i, int j, double val) {
+    if (i < rows && j < nj) dst[(int64_t)i * R + j] -= val;
+  });
 }
 
 __global__ void permute_in_kernel(const int64_t *__restrict__ perm, int64_t n, const double *__restrict__ b,
@@ -388,30 +499,33 @@ __global__ void pack_kernel(Tree t, const int64_t *__restrict__ toff, double *__
   double *d = dst + toff[s];
   for (int64_t c = 0; c < w; ++c) {
     const int64_t start = c * m - c * (c > 0 ? c - 1 : 0) / 2;
-    for (int64_t r = c + threadIdx.x; r < m; r += blockDim.x) d[start + r - c] = Ls[r + c * m];
+    const int64_t p = c / NB, c0 = p * NB, c1 = c0 + NB < w ? c0 + NB : w, pw = c1 - c0;
+    const double *Dp = t.D + t.doff[s] + 2 * (int64_t)NB * NB * p;
+    for (int64_t r = c + threadIdx.x; r < m; r += blockDim.x)
+      d[start + r - c] = r < c1 ? Dp[(c - c0) * pw + (r - c0)] : Ls[r + c * m];
   }
 }
 
 }  // namespace
 
+void configure_kernels() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM);
+  cudaFuncSetAttribute(solve_panel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SOLVE_SMEM);
+  cudaFuncSetAttribute(solve_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SOLVE_SMEM);
+  done = true;
+}
+
 void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, int count, cudaStream_t st) {
   if (count > 0) assemble_kernel<<<count, 256, 0, st>>>(t, upper_val, tasks);
 }
 
-void launch_potrf(const Tree &t, const double *upper_val, const PanelTask *tasks, int count, DeviceStatus *status,
+void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count, DeviceStatus *status,
                   cudaStream_t st) {
-  if (count > 0) potrf_kernel<<<count, 256, 0, st>>>(t, upper_val, tasks, status);
-}
-
-void launch_trsm(const Tree &t, const PanelTask *tasks, int count, cudaStream_t st) {
   if (count <= 0) return;
-  const size_t smem = sizeof(double) * (NB * (NB + 1) + NB * TRSM_ROWS);
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
-  trsm_kernel<<<count, TRSM_ROWS, smem, st>>>(t, tasks);
+  configure_kernels();
+  panel_kernel<<<count, PANEL_THREADS, PANEL_SMEM, st>>>(t, upper_val, tasks, status);
 }
 
 void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st) {
@@ -428,15 +542,14 @@ void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_
   if (count > 0) solve_gather_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks);
 }
 
-void launch_trsv(const Tree &t, double *x, int R, bool transpose, const SolveTask *tasks, int count, cudaStream_t st) {
+void launch_solve_panel(const Tree &t, bool backward, double *x, double *x2, double *v, const int64_t *voff, int R,
+                        const SolveTask *tasks, int count, cudaStream_t st) {
   if (count <= 0) return;
-  const size_t smem = sizeof(double) * (NB * (NB + 1) + NB * 64);
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(trsv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
-  trsv_kernel<<<count, 64, smem, st>>>(t, x, R, transpose ? 1 : 0, tasks);
+  configure_kernels();
+  if (backward)
+    solve_panel_kernel<true><<<count, 128, SOLVE_SMEM, st>>>(t, x, x2, v, voff, R, tasks);
+  else
+    solve_panel_kernel<false><<<count, 128, SOLVE_SMEM, st>>>(t, x, x2, v, voff, R, tasks);
 }
 
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R, cudaStream_t st) {

@@ -12,7 +12,7 @@ namespace fc {
 constexpr int NB = 64;
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_KC = 16;
 constexpr int GEMM_THREADS = 128;
-constexpr int TRSM_ROWS = 128;  // rows of a panel solved by one CTA
+constexpr int PANEL_ROWS = 64;  // rows of a panel solved by one CTA
 constexpr int ASSEMBLE_COLS = 32;  // front columns assembled by one CTA
 
 // Where each supernode lives on the device. A front of supernode s has m = rows(s) rows and
@@ -33,16 +33,23 @@ struct Tree {
   const int64_t *a_src;     // upper-entry index of each
   const int64_t *a_dst;     // its place in the L arena
   const int64_t *diag_src;  // [n] upper-entry index of A(j, j), -1 if absent
+  const int64_t *doff;      // [ns] diagonal arena: panel p of s keeps its factored block and its
+                            // inverse (pw x pw each, column-major) at doff[s] + 2 NB NB p
   double *L;
   double *U;
+  double *D;
 };
 
 struct AssembleTask {
   int32_t s, j0, j1, pad;
 };
-// Diagonal block [c0, c1) of supernode s (POTRF), or rows [r0, r1) below it (TRSM).
+// Panel [c0, c1) of supernode s: factor its diagonal block, invert it, and solve the rows
+// [r0, r1) below it (r0 >= c1; an empty range for a task that only keeps the block). The task
+// with `keep` set writes the factored block and its inverse to the diagonal arena at `doff` and
+// reports the pivots; every task of the panel factors the block itself (no CTA waits on another).
 struct PanelTask {
-  int32_t s, c0, c1, r0, r1, pad;
+  int32_t s, c0, c1, r0, r1, keep;
+  int64_t doff;
 };
 // C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands; flag 1: store i >= j only.
 struct GemmTask {
@@ -52,9 +59,12 @@ struct GemmTask {
   int64_t c_si, c_sj, a_si, a_sk, b_sj, b_sk;
   int32_t M, N, K, flags;
 };
-// Solve: rows [c0, c1) of supernode s's own block, right-hand sides [j0, j1).
+// Solve, panel [c0, c1) of supernode s, right-hand sides [j0, j1): apply the inverse of the
+// diagonal block (forward: L^-1, backward: L^-T), then update the front rows [r0, r1) (forward:
+// below the panel; backward: the own rows above it). `keep`: this task stores the panel's result.
 struct SolveTask {
-  int32_t s, c0, c1, j0, j1, pad;
+  int32_t s, c0, c1, r0, r1, j0, j1, keep;
+  int64_t doff;
 };
 // Solve front rows [i0, i1) of supernode s.
 struct RowTask {
@@ -66,11 +76,13 @@ struct DeviceStatus {
   unsigned long long failed_column;  // ULLONG_MAX when none
 };
 
+// Sets the kernels' shared-memory limits (once per process; before any stream capture).
+void configure_kernels();
+
 void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, int count,
                      cudaStream_t st);
-void launch_potrf(const Tree &t, const double *upper_val, const PanelTask *tasks, int count,
+void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count,
                   DeviceStatus *status, cudaStream_t st);
-void launch_trsm(const Tree &t, const PanelTask *tasks, int count, cudaStream_t st);
 void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st);
 
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
@@ -78,8 +90,10 @@ void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *v
                            const RowTask *tasks, int count, cudaStream_t st);
 void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R,
                          const RowTask *tasks, int count, cudaStream_t st);
-void launch_trsv(const Tree &t, double *x, int R, bool transpose, const SolveTask *tasks, int count,
-                 cudaStream_t st);
+// Forward: y = L_pp^-1 x_p into x2, then x (own rows) / v (rows past the columns) -= L y.
+// Backward: z = L_pp^-T x2_p into x, then x2 (own rows above) -= L^T z.
+void launch_solve_panel(const Tree &t, bool backward, double *x, double *x2, double *v, const int64_t *voff,
+                        int R, const SolveTask *tasks, int count, cudaStream_t st);
 // x_post[i*R + j] = b[perm[i] + j*ld] and back.
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
                        cudaStream_t st);

@@ -122,15 +122,17 @@ int fc_chol_values(fc_chol *h, double *dst, fc_status *status);
 /* Plan statistics: 0 levels, 1 launches of the factor, 2 bytes of L on device, 3 bytes of the
  * update matrices, 4 supernodes, 5 factor flops (sum of column counts squared), 6 GEMM tasks,
  * 7 kernels launched by the last factorisation, 8 kernels launched by the last solve, 9 flops of
- * the factor's GEMM tasks, 10 flops of the last solve plan's GEMM tasks. */
+ * the factor's GEMM tasks, 10 flops of the last solve plan's GEMM tasks, 11 the ordinal among the
+ * factor's GEMM launches of the one with the most flops, 12 the same among the launches whose
+ * tasks all have K <= 64 (the panels' updates of later columns). */
 int64_t fc_chol_stat(const fc_chol *h, int what);
 
 /* Per-launch timing with CUDA events on the handle's stream (no reference counterpart: the
  * measurement hook of the benchmark). enable != 0 starts recording; fc_chol_profile_read waits for
  * the stream and returns, per launch kind, the summed milliseconds and the launch count (arrays of
- * `kinds` entries, 24 covers all), then clears them. Kinds: 0 front assembly, 1 POTRF, 2 TRSM,
- * 3 GEMM of the factor; 19 GEMM, 20 front assembly, 21 gather, 22 TRSV, 23 transposed TRSV of
- * the solve. */
+ * `kinds` entries, 24 covers all), then clears them. Kinds: 0 front assembly, 1 panel (factor,
+ * invert and solve below a diagonal block), 3 GEMM of the factor; 19 GEMM, 20 front assembly,
+ * 21 gather, 22 forward panel, 23 backward panel of the solve. */
 int fc_chol_profile(fc_chol *h, int enable);
 int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kinds);
 
