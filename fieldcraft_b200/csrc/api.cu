@@ -627,33 +627,35 @@ int read_status(fc_chol *h, fc_status *st) {
 // rows below -= L y (x accumulates, y lands in x2). Backward, top level first: gather the final
 // values of the rows past the columns, own rows -= L21^T v, then panel by panel from the last
 // z = Linv^T x2 and the own rows above -= L^T z (x2 accumulates, z lands in x).
-int plan_solve(fc_chol *h, int R, fc_status *st) {
-  if (h->solve_R == R) return FC_OK;
-  if (h->solve_graph) {
-    cudaGraphExecDestroy(h->solve_graph);
-    h->solve_graph = nullptr;
-  }
-  const int NB = fc::NB;
-  std::vector<std::vector<int64_t>> lv(h->levels);
-  for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
-  std::vector<int64_t> voff, vsize(h->ns);
-  for (int64_t s = 0; s < h->ns; ++s) vsize[s] = (int64_t)(h->height[s] - h->width[s]) * R;
-  const int64_t vsum = arena_offsets(h, lv, vsize, voff);
-  cudaError_t e;
-  if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
-      h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
-      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(vsum, 1)) != cudaSuccess) {
-    h->solve_R = 0;
-    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
-    return FC_OUT_OF_MEMORY;
-  }
-  if ((e = upload(h->d_voff, voff, h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
+// The solve's task lists for R right-hand sides: the update vectors' offsets (liveness-reused,
+// like the update matrices), then the tasks over given device vectors x, x2 (n x R each) and v.
+struct SolvePlan {
+  std::vector<int64_t> voff;
+  int64_t vsum = 0;
   std::vector<fc::RowTask> rows;
   std::vector<fc::SolveTask> panels;
   std::vector<fc::GemmTask> gemm;
-  double *L = h->d_L.as<double>(), *x = h->d_x.as<double>(), *x2 = h->d_x2.as<double>(), *v = h->d_v.as<double>();
-  h->fwd.clear();
-  h->bwd.clear();
+  std::vector<Launch> fwd, bwd;
+};
+
+void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
+  std::vector<std::vector<int64_t>> lv(h->levels);
+  for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
+  std::vector<int64_t> vsize(h->ns);
+  for (int64_t s = 0; s < h->ns; ++s) vsize[s] = (int64_t)(h->height[s] - h->width[s]) * R;
+  p.vsum = arena_offsets(h, lv, vsize, p.voff);
+}
+
+void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, SolvePlan &p) {
+  const int NB = fc::NB;
+  std::vector<std::vector<int64_t>> lv(h->levels);
+  for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
+  const std::vector<int64_t> &voff = p.voff;
+  std::vector<fc::RowTask> &rows = p.rows;
+  std::vector<fc::SolveTask> &panels = p.panels;
+  std::vector<fc::GemmTask> &gemm = p.gemm;
+  std::vector<Launch> &fwd = p.fwd, &bwd = p.bwd;
+  double *L = h->d_L.as<double>();
   // forward
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
@@ -664,7 +666,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
       if (!kids && m == w) continue;
       for (int i0 = kids ? 0 : w; i0 < m; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(m, i0 + 64), 0});
     }
-    push(h->fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
+    push(fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = 0; p < P; ++p) {
@@ -687,7 +689,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
           }
         }
       }
-      push(h->fwd, K_SOLVE_FWD, po, (int64_t)panels.size() - po, (int)l);
+      push(fwd, K_SOLVE_FWD, po, (int64_t)panels.size() - po, (int)l);
     }
   }
   // backward
@@ -698,7 +700,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
       const int u = h->height[s] - h->width[s];
       for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
     }
-    push(h->bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
+    push(bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
     int64_t go = (int64_t)gemm.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
@@ -719,7 +721,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
           gemm.push_back(g);
         }
     }
-    push(h->bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+    push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = P - 1; p >= 0; --p) {
@@ -736,41 +738,71 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
             panels.push_back({(int32_t)s, c0, c1, i0, std::min(c0, i0 + 64), j0, j1, i0 == 0 ? 1 : 0, doff});
         }
       }
-      push(h->bwd, K_SOLVE_BWD, po, (int64_t)panels.size() - po, (int)l);
+      push(bwd, K_SOLVE_BWD, po, (int64_t)panels.size() - po, (int)l);
     }
   }
+}
+
+// The handle's own solve buffers and task arrays for R right-hand sides (built once per R).
+int plan_solve(fc_chol *h, int R, fc_status *st) {
+  if (h->solve_R == R) return FC_OK;
+  if (h->solve_graph) {
+    cudaGraphExecDestroy(h->solve_graph);
+    h->solve_graph = nullptr;
+  }
+  SolvePlan p;
+  solve_offsets(h, R, p);
+  cudaError_t e;
+  if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
+      h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
+      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess) {
+    h->solve_R = 0;
+    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
+    return FC_OUT_OF_MEMORY;
+  }
+  if ((e = upload(h->d_voff, p.voff, h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
+  solve_tasks(h, R, h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), p);
+  h->fwd = std::move(p.fwd);
+  h->bwd = std::move(p.bwd);
   h->gemm_flops_solve = 0;
-  for (const auto &g : gemm) h->gemm_flops_solve += task_flops(g);
-  if ((e = upload(h->d_srow, rows, h->stream)) != cudaSuccess || (e = upload(h->d_spanel, panels, h->stream)) != cudaSuccess ||
-      (e = upload(h->d_sgemm, gemm, h->stream)) != cudaSuccess)
+  for (const auto &g : p.gemm) h->gemm_flops_solve += task_flops(g);
+  if ((e = upload(h->d_srow, p.rows, h->stream)) != cudaSuccess || (e = upload(h->d_spanel, p.panels, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_sgemm, p.gemm, h->stream)) != cudaSuccess)
     return cuda_fail(st, e, "solve plan");
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
   h->solve_R = R;
   return FC_OK;
 }
 
-void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, int64_t &launches) {
+// The device buffers a solve program runs on.
+struct SolveBuffers {
+  double *x, *x2, *v;
+  const int64_t *voff;
+  const fc::RowTask *rows;
+  const fc::SolveTask *panels;
+  const fc::GemmTask *gemm;
+};
+
+SolveBuffers own_buffers(fc_chol *h) {
+  return {h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), h->d_voff.as<int64_t>(),
+          h->d_srow.as<fc::RowTask>(), h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>()};
+}
+
+void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveBuffers &b, int R, int64_t &launches) {
   cudaStream_t st = h->stream;
   const fc::Tree &t = h->tree;
-  const int R = h->solve_R;
-  double *x = h->d_x.as<double>(), *x2 = h->d_x2.as<double>(), *v = h->d_v.as<double>();
-  const int64_t *voff = h->d_voff.as<int64_t>();
   for (const Launch &l : prog) {
     Mark mark(h, l.kind + 16);
     switch (l.kind) {
-      case K_SOLVE_ASSEMBLE:
-        fc::launch_solve_assemble(t, x, v, voff, R, h->d_srow.as<fc::RowTask>() + l.off, l.count, st);
-        break;
-      case K_SOLVE_GATHER:
-        fc::launch_solve_gather(t, x, v, voff, R, h->d_srow.as<fc::RowTask>() + l.off, l.count, st);
-        break;
+      case K_SOLVE_ASSEMBLE: fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
+      case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_FWD:
-        fc::launch_solve_panel(t, false, x, x2, v, voff, R, h->d_spanel.as<fc::SolveTask>() + l.off, l.count, st);
+        fc::launch_solve_panel(t, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, st);
         break;
       case K_SOLVE_BWD:
-        fc::launch_solve_panel(t, true, x, x2, v, voff, R, h->d_spanel.as<fc::SolveTask>() + l.off, l.count, st);
+        fc::launch_solve_panel(t, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, st);
         break;
-      case K_GEMM: fc::launch_gemm(h->d_sgemm.as<fc::GemmTask>() + l.off, l.count, st); break;
+      case K_GEMM: fc::launch_gemm(b.gemm + l.off, l.count, st); break;
     }
     ++launches;
   }
@@ -807,12 +839,43 @@ int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
 
 void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   int64_t launches = 0;
+  const SolveBuffers b = own_buffers(h);
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->stream);
-  run_solve_program(h, h->fwd, launches);
-  run_solve_program(h, h->bwd, launches);
+  run_solve_program(h, h->fwd, b, R, launches);
+  run_solve_program(h, h->bwd, b, R, launches);
   fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->stream);
   h->last_solve_launches = launches + 2;
 }
+
+}  // namespace
+
+// Scratch of fc_chol_solve_device_noalloc: the solve's vectors and task lists for callers that
+// cannot allocate device memory. A file-scope device array, so loading the library reserves it
+// on every device the process uses, until exit. Host code may not use its name as an address;
+// the address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char fc_noalloc_scratch[FC_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex noalloc_setup_lock;
+constexpr int NOALLOC_DEVICES = 64;
+unsigned char *noalloc_base[NOALLOC_DEVICES] = {};
+
+// The scratch's device address on the current device (set up on the first call there).
+cudaError_t noalloc_scratch(int device, unsigned char **base) {
+  if (device < 0 || device >= NOALLOC_DEVICES) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(noalloc_setup_lock);
+  if (!noalloc_base[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, fc_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    noalloc_base[device] = static_cast<unsigned char *>(p);
+  }
+  *base = noalloc_base[device];
+  return cudaSuccess;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 
@@ -1084,6 +1147,69 @@ int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_s
   int rc = enqueue_solve(h, d_b, nrhs, ld, status);
   if (rc != FC_OK) return rc;
   cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(status, e, "solve");
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_status *status) {
+  if (!h || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
+    return FC_INVALID_ARGUMENT;
+  }
+  if (nrhs == 0 || h->n == 0) {
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  unsigned char *base = nullptr;
+  cudaError_t e = noalloc_scratch(h->device, &base);
+  if (e != cudaSuccess) return cuda_fail(status, e, "cudaGetSymbolAddress of the solve scratch");
+  const int R = nrhs;
+  // Layout in the scratch: x | x2 | v | voff | row tasks | panel tasks | GEMM tasks.
+  SolvePlan p;
+  solve_offsets(h, R, p);
+  const size_t vec = align256(sizeof(double) * (size_t)h->n * R);
+  const size_t at_x = 0, at_x2 = vec, at_v = 2 * vec;
+  const size_t at_voff = at_v + align256(sizeof(double) * (size_t)p.vsum);
+  auto too_large = [&](size_t need) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "the solve needs %zu bytes of scratch; the no-allocation limit is %zu",
+                  need, (size_t)FC_NOALLOC_SCRATCH_BYTES);
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, msg);
+    return FC_INVALID_ARGUMENT;
+  };
+  if (at_voff > FC_NOALLOC_SCRATCH_BYTES) return too_large(at_voff);
+  solve_tasks(h, R, reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
+              reinterpret_cast<double *>(base + at_v), p);
+  const size_t at_rows = at_voff + align256(sizeof(int64_t) * p.voff.size());
+  const size_t at_panels = at_rows + align256(sizeof(fc::RowTask) * p.rows.size());
+  const size_t at_gemm = at_panels + align256(sizeof(fc::SolveTask) * p.panels.size());
+  const size_t need = at_gemm + sizeof(fc::GemmTask) * p.gemm.size();
+  if (need > FC_NOALLOC_SCRATCH_BYTES) return too_large(need);
+  // Every region is written before it is read in this call: the task lists and offsets here, x by
+  // the permutation, x2 by the forward panels, each update vector's rows zeroed by its assembly.
+  auto put = [&](size_t at, const void *src, size_t bytes) {
+    if (bytes && e == cudaSuccess) e = cudaMemcpyAsync(base + at, src, bytes, cudaMemcpyHostToDevice, h->stream);
+  };
+  put(at_voff, p.voff.data(), sizeof(int64_t) * p.voff.size());
+  put(at_rows, p.rows.data(), sizeof(fc::RowTask) * p.rows.size());
+  put(at_panels, p.panels.data(), sizeof(fc::SolveTask) * p.panels.size());
+  put(at_gemm, p.gemm.data(), sizeof(fc::GemmTask) * p.gemm.size());
+  if (e != cudaSuccess) return cuda_fail(status, e, "copy of the solve plan into the scratch");
+  const SolveBuffers b{reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
+                       reinterpret_cast<double *>(base + at_v), reinterpret_cast<const int64_t *>(base + at_voff),
+                       reinterpret_cast<const fc::RowTask *>(base + at_rows),
+                       reinterpret_cast<const fc::SolveTask *>(base + at_panels),
+                       reinterpret_cast<const fc::GemmTask *>(base + at_gemm)};
+  int64_t launches = 0;
+  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, b.x, R, h->stream);
+  run_solve_program(h, p.fwd, b, R, launches);
+  run_solve_program(h, p.bwd, b, R, launches);
+  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, b.x, R, d_b, ld, h->stream);
+  e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(status, e, "solve");
   set_status(status, FC_OK);

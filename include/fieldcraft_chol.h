@@ -114,6 +114,20 @@ int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *st
 /* The same on device memory; synchronises before returning. */
 int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_status *status);
 int fc_chol_solve_device_async(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld);
+/* A solve that allocates no device memory. It has no counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc, such as a host application whose own allocator owns all of
+ * the device's memory under a fixed budget, where an extra allocation could fail or fragment
+ * that pool. It solves like fc_chol_solve_device (d_b column-major, leading dimension ld, in
+ * place), but takes its working memory (the solve vectors and task lists) from one file-scope
+ * device array of FC_NOALLOC_SCRATCH_BYTES that the library reserves on every device it is
+ * loaded on, until the process exits. Calls that need more than that are refused with
+ * FC_INVALID_ARGUMENT and a message giving the size needed. The first call on each device looks
+ * the array's address up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array and each leaves its contents behind: calls whose work overlaps on
+ * the GPU (several handles or threads on one device at once) race on it. Synchronises before
+ * returning. */
+#define FC_NOALLOC_SCRATCH_BYTES (32u << 20)
+int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_status *status);
 /* The factor's values in the reference's layout: supernode by supernode, each its lower
  * trapezoid by columns (column c holds rows c..m, cholesky.rs:418-425, 1534-1542). dst has
  * fc_chol_entries(h) doubles. */
