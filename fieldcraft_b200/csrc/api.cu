@@ -91,6 +91,7 @@ struct Launch {
   int64_t off;
   int count;
   int level;  // the level of the supernodal tree the launch belongs to (cancellation points)
+  int width;  // panel launches: the widest panel, padded (sizes the kernel's shared memory)
 };
 
 }  // namespace
@@ -173,8 +174,8 @@ std::vector<std::vector<int64_t>> levels_of(fc_chol *h) {
   return out;
 }
 
-void push(std::vector<Launch> &prog, int kind, int64_t off, int64_t count, int level) {
-  if (count > 0) prog.push_back({kind, off, (int)count, level});
+void push(std::vector<Launch> &prog, int kind, int64_t off, int64_t count, int level, int width = 0) {
+  if (count > 0) prog.push_back({kind, off, (int)count, level, width});
 }
 
 // Useful flops of a GEMM task (a diagonal tile computes its lower triangle only).
@@ -259,11 +260,13 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = 0; p < P; ++p) {
       int64_t po = (int64_t)panel_t.size(), go = (int64_t)gemm_t.size();
+      int p8max = 8;
       for (int64_t s : S) {
         const int m = h->height[s], w = h->width[s];
         const int c0 = p * NB;
         if (c0 >= w) continue;
         const int c1 = std::min(w, c0 + NB);
+        p8max = std::max(p8max, (c1 - c0 + 7) / 8 * 8);
         const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
         if (c1 >= m) panel_t.push_back({(int32_t)s, c0, c1, m, m, 1, doff});
         for (int r0 = c1; r0 < m; r0 += fc::PANEL_ROWS)
@@ -283,7 +286,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             gemm_t.push_back(g);
           }
       }
-      push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l);
+      push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l, p8max);
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
     }
     int64_t go = (int64_t)gemm_t.size();
@@ -597,7 +600,8 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
     switch (l.kind) {
       case K_ASSEMBLE: fc::launch_assemble(t, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, l.count, st); break;
       case K_PANEL:
-        fc::launch_panel(t, d_val, h->d_panel.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(), st);
+        fc::launch_panel(t, d_val, h->d_panel.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(),
+                         l.width, st);
         break;
       case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, st); break;
     }
@@ -671,10 +675,12 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = 0; p < P; ++p) {
       int64_t po = (int64_t)panels.size();
+      int k4max = 4;
       for (int64_t s : S) {
         const int m = h->height[s], w = h->width[s], c0 = p * NB;
         if (c0 >= w) continue;
         const int c1 = std::min(w, c0 + NB);
+        k4max = std::max(k4max, (c1 - c0 + 3) / 4 * 4);
         const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
         for (int j0 = 0; j0 < R; j0 += 64) {
           const int j1 = std::min(R, j0 + 64);
@@ -689,7 +695,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
           }
         }
       }
-      push(fwd, K_SOLVE_FWD, po, (int64_t)panels.size() - po, (int)l);
+      push(fwd, K_SOLVE_FWD, po, (int64_t)panels.size() - po, (int)l, k4max);
     }
   }
   // backward
@@ -726,10 +732,12 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = P - 1; p >= 0; --p) {
       int64_t po = (int64_t)panels.size();
+      int k4max = 4;
       for (int64_t s : S) {
         const int w = h->width[s], c0 = p * NB;
         if (c0 >= w) continue;
         const int c1 = std::min(w, c0 + NB);
+        k4max = std::max(k4max, (c1 - c0 + 3) / 4 * 4);
         const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
         for (int j0 = 0; j0 < R; j0 += 64) {
           const int j1 = std::min(R, j0 + 64);
@@ -738,7 +746,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
             panels.push_back({(int32_t)s, c0, c1, i0, std::min(c0, i0 + 64), j0, j1, i0 == 0 ? 1 : 0, doff});
         }
       }
-      push(bwd, K_SOLVE_BWD, po, (int64_t)panels.size() - po, (int)l);
+      push(bwd, K_SOLVE_BWD, po, (int64_t)panels.size() - po, (int)l, k4max);
     }
   }
 }
@@ -797,10 +805,10 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
       case K_SOLVE_ASSEMBLE: fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_FWD:
-        fc::launch_solve_panel(t, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, st);
+        fc::launch_solve_panel(t, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
         break;
       case K_SOLVE_BWD:
-        fc::launch_solve_panel(t, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, st);
+        fc::launch_solve_panel(t, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
         break;
       case K_GEMM: fc::launch_gemm(b.gemm + l.off, l.count, st); break;
     }

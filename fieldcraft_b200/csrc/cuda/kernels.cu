@@ -158,16 +158,17 @@ __device__ __forceinline__ void each_acc(const double (&acc)[4][4][2], F f) {
 // and nothing else: no index depends on a value. The inverse comes from 8 x 8 diagonal blocks and
 // block forward substitution; the rows below are X = B L^-T on the FP64 tensor pipe.
 constexpr int PANEL_THREADS = 128;
-constexpr size_t PANEL_SMEM = sizeof(double) * (64 * 65 + 2 * 64 * TS + 512 + 128);
+// Shared memory of a panel launch whose widest panel is padded to p8 columns (a multiple of 8).
+__host__ __device__ constexpr size_t panel_smem(int p8) { return sizeof(double) * (p8 * (65 + 2 * TS) + 512 + 128); }
 
 __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const double *__restrict__ val,
                                                               const PanelTask *__restrict__ tasks,
-                                                              DeviceStatus *status) {
+                                                              DeviceStatus *status, int p8max) {
   extern __shared__ double sm[];
-  double *a = sm;                 // factor, column-major, ld 65
-  double *inv = a + 64 * 65;      // inv[k * TS + i] = Linv(i, k)
-  double *bt = inv + 64 * TS;     // rows below: bt[k * TS + r] = L(r0 + r, c0 + k)
-  double *tt = bt + 64 * TS;      // 8 x (8 x 8) scratch of the inversion
+  double *a = sm;                   // factor, column-major, ld 65 (p8max columns)
+  double *inv = a + p8max * 65;     // inv[k * TS + i] = Linv(i, k) (p8max rows)
+  double *bt = inv + p8max * TS;    // rows below: bt[k * TS + r] = L(r0 + r, c0 + k)
+  double *tt = bt + p8max * TS;     // 8 x (8 x 8) scratch of the inversion
   double *dg = tt + 512;          // the matrix's own diagonal entries of the panel's columns
   double *dv = dg + 64;           // the pivots
   __shared__ int fail;
@@ -269,65 +270,81 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
 }
 
 // ---- tiled C -= A B^T on the FP64 tensor pipe ---------------------------------------------------
-// 64 x 64 tile per CTA, 4 warps of 32 x 32 (4 x 4 DMMA tiles), K in chunks of 16 double-buffered
-// through shared memory. Shared rows are padded to 68 doubles so the fragment reads of a warp
-// (4 k-rows x 8 consecutive doubles) fall in distinct banks.
+// 64 x 64 tile per CTA, 4 warps of 32 x 32 (4 x 4 DMMA tiles), K in chunks of 16 through a
+// three-stage cp.async pipeline in shared memory (rows padded to 68 doubles so a warp's fragment
+// reads of 4 k-rows x 8 consecutive doubles fall in distinct banks). Four CTAs fit an SM.
 constexpr int SROW = 68;
+constexpr int GEMM_STAGES = 3;
+constexpr size_t GEMM_SMEM = sizeof(double) * GEMM_STAGES * 2 * GEMM_KC * SROW;
 
-__global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(const GemmTask *__restrict__ tasks) {
-  const GemmTask tk = tasks[blockIdx.x];
-  __shared__ __align__(16) double As[2][GEMM_KC][SROW];
-  __shared__ __align__(16) double Bs[2][GEMM_KC][SROW];
+// This thread's 8 elements of a 64 x 16 operand tile: a fixed row and k = k0 + 2q when the rows
+// are contiguous in memory (si == 1), else a fixed k and row i0 + 8q (k contiguous).
+struct TileLoader {
+  const double *p;
+  int64_t dq, dstage;
+  int i0, k0, di, dk, lim;
+  __device__ __forceinline__ void init(const double *base, int64_t si, int64_t sk, int rows, int tid) {
+    if (si == 1) {
+      i0 = tid & 63, k0 = tid >> 6, di = 0, dk = 2;
+      p = base + i0 + (int64_t)k0 * sk;
+      dq = 2 * sk;
+      dstage = GEMM_KC * sk;
+    } else {
+      i0 = tid >> 4, k0 = tid & 15, di = 8, dk = 0;
+      p = base + (int64_t)i0 * si + k0;
+      dq = 8 * si;
+      dstage = GEMM_KC;
+    }
+    lim = rows;
+  }
+  __device__ __forceinline__ void load(double (*S)[SROW], int kbase, int K, const double *safe) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int i = i0 + q * di, k = k0 + q * dk;
+      const bool ok = i < lim && kbase + k < K;
+      cp_async8(&S[k][i], ok ? p + q * dq : safe, ok ? 8 : 0);
+    }
+    p += dstage;
+  }
+};
+
+__global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *__restrict__ tasks) {
+  extern __shared__ __align__(16) double gsm[];
+  double(*As)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm);
+  double(*Bs)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm + GEMM_STAGES * GEMM_KC * SROW);
+  const GemmTask *tp = tasks + blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tg = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int M = tk.M, N = tk.N, K = tk.K;
+  const int K = tp->K;
+  const double *abase = tp->A, *bbase = tp->B;
+  TileLoader la, lb;
+  la.init(abase, tp->a_si, tp->a_sk, tp->M, tid);
+  lb.init(bbase, tp->b_sj, tp->b_sk, tp->N, tid);
   double acc[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  const bool a_rows = tk.a_si == 1, b_rows = tk.b_sj == 1;
-  auto load = [&](int stage, int k0) {
+  const int nk = (K + GEMM_KC - 1) / GEMM_KC;
 #pragma unroll
-    for (int q = 0; q < (GEMM_TM * GEMM_KC) / GEMM_THREADS; ++q) {
-      const int e = tid + GEMM_THREADS * q;
-      int i, k;
-      if (a_rows) {
-        i = e & (GEMM_TM - 1);
-        k = e / GEMM_TM;
-      } else {
-        i = e / GEMM_KC;
-        k = e & (GEMM_KC - 1);
-      }
-      const bool ok = i < M && k0 + k < K;
-      const double *src = ok ? tk.A + (int64_t)i * tk.a_si + (int64_t)(k0 + k) * tk.a_sk : tk.A;
-      cp_async8(&As[stage][k][i], src, ok ? 8 : 0);
-      int j;
-      if (b_rows) {
-        j = e & (GEMM_TN - 1);
-        k = e / GEMM_TN;
-      } else {
-        j = e / GEMM_KC;
-        k = e & (GEMM_KC - 1);
-      }
-      const bool okb = j < N && k0 + k < K;
-      const double *srcb = okb ? tk.B + (int64_t)j * tk.b_sj + (int64_t)(k0 + k) * tk.b_sk : tk.B;
-      cp_async8(&Bs[stage][k][j], srcb, okb ? 8 : 0);
+  for (int st = 0; st < GEMM_STAGES - 1; ++st) {
+    if (st < nk) {
+      la.load(As[st], st * GEMM_KC, K, abase);
+      lb.load(Bs[st], st * GEMM_KC, K, bbase);
     }
     cp_async_commit();
-  };
-  const int nk = (K + GEMM_KC - 1) / GEMM_KC;
-  if (nk > 0) load(0, 0);
+  }
   for (int kt = 0; kt < nk; ++kt) {
-    if (kt + 1 < nk) {
-      load((kt + 1) & 1, (kt + 1) * GEMM_KC);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    cp_async_wait<GEMM_STAGES - 2>();
     __syncthreads();
-    const int st = kt & 1;
+    const int pf = kt + GEMM_STAGES - 1;
+    if (pf < nk) {
+      la.load(As[pf % GEMM_STAGES], pf * GEMM_KC, K, abase);
+      lb.load(Bs[pf % GEMM_STAGES], pf * GEMM_KC, K, bbase);
+    }
+    cp_async_commit();
+    const int st = kt % GEMM_STAGES;
 #pragma unroll
     for (int kk = 0; kk < GEMM_KC; kk += 4) {
       double av[4], bv[4];
@@ -340,9 +357,12 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(const GemmTask *__re
 #pragma unroll
         for (int c = 0; c < 4; ++c) dmma(acc[r][c], av[r], bv[c]);
     }
-    __syncthreads();
   }
-  const bool lower = tk.flags & 1;
+  cp_async_wait<0>();
+  const int M = tp->M, N = tp->N;
+  const bool lower = tp->flags & 1;
+  double *C = tp->C;
+  const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -350,10 +370,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(const GemmTask *__re
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int i = wm + r * 8 + g, j = wn + c * 8 + 2 * tg + e;
-        if (i < M && j < N && (!lower || i >= j)) {
-          double *dst = tk.C + (int64_t)i * tk.c_si + (int64_t)j * tk.c_sj;
-          *dst -= acc[r][c][e];
-        }
+        if (i < M && j < N && (!lower || i >= j)) C[(int64_t)i * c_si + (int64_t)j * c_sj] -= acc[r][c][e];
       }
 }
 
@@ -408,14 +425,14 @@ __global__ void __launch_bounds__(256) solve_gather_kernel(Tree t, const double 
 // block from the diagonal arena. Forward: y = Linv x_p (x -> x2), then the front rows [r0, r1)
 // below the panel -= L(rows, panel) y (own rows in x, rows past the columns in v). Backward:
 // z = Linv^T x2_p (x2 -> x), then the own rows [r0, r1) above -= L(panel, rows)^T z in x2.
-constexpr size_t SOLVE_SMEM = sizeof(double) * 3 * 64 * TS;
+__host__ __device__ constexpr size_t solve_smem(int k4) { return sizeof(double) * 3 * k4 * TS; }
 
 template <bool BACKWARD>
 __global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__restrict__ x, double *__restrict__ x2,
                                                          double *__restrict__ v, const int64_t *__restrict__ voff, int R,
-                                                         const SolveTask *__restrict__ tasks) {
+                                                         const SolveTask *__restrict__ tasks, int k4max) {
   extern __shared__ double sm[];
-  double *inv = sm, *xs = sm + 64 * TS, *bt = sm + 2 * 64 * TS;
+  double *inv = sm, *xs = sm + k4max * TS, *bt = sm + 2 * k4max * TS;
   const SolveTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
@@ -511,9 +528,10 @@ __global__ void pack_kernel(Tree t, const int64_t *__restrict__ toff, double *__
 void configure_kernels() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM);
-  cudaFuncSetAttribute(solve_panel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SOLVE_SMEM);
-  cudaFuncSetAttribute(solve_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SOLVE_SMEM);
+  cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem(64));
+  cudaFuncSetAttribute(solve_panel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(64));
+  cudaFuncSetAttribute(solve_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(64));
+  cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
   done = true;
 }
 
@@ -522,14 +540,16 @@ void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask 
 }
 
 void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count, DeviceStatus *status,
-                  cudaStream_t st) {
+                  int p8max, cudaStream_t st) {
   if (count <= 0) return;
   configure_kernels();
-  panel_kernel<<<count, PANEL_THREADS, PANEL_SMEM, st>>>(t, upper_val, tasks, status);
+  panel_kernel<<<count, PANEL_THREADS, panel_smem(p8max), st>>>(t, upper_val, tasks, status, p8max);
 }
 
 void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st) {
-  if (count > 0) gemm_kernel<<<count, GEMM_THREADS, 0, st>>>(tasks);
+  if (count <= 0) return;
+  configure_kernels();
+  gemm_kernel<<<count, GEMM_THREADS, GEMM_SMEM, st>>>(tasks);
 }
 
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,
@@ -543,13 +563,13 @@ void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_
 }
 
 void launch_solve_panel(const Tree &t, bool backward, double *x, double *x2, double *v, const int64_t *voff, int R,
-                        const SolveTask *tasks, int count, cudaStream_t st) {
+                        const SolveTask *tasks, int count, int k4max, cudaStream_t st) {
   if (count <= 0) return;
   configure_kernels();
   if (backward)
-    solve_panel_kernel<true><<<count, 128, SOLVE_SMEM, st>>>(t, x, x2, v, voff, R, tasks);
+    solve_panel_kernel<true><<<count, 128, solve_smem(k4max), st>>>(t, x, x2, v, voff, R, tasks, k4max);
   else
-    solve_panel_kernel<false><<<count, 128, SOLVE_SMEM, st>>>(t, x, x2, v, voff, R, tasks);
+    solve_panel_kernel<false><<<count, 128, solve_smem(k4max), st>>>(t, x, x2, v, voff, R, tasks, k4max);
 }
 
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R, cudaStream_t st) {

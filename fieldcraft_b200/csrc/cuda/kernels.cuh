@@ -81,8 +81,9 @@ void configure_kernels();
 
 void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, int count,
                      cudaStream_t st);
+// p8max: the widest panel of the launch, rounded up to a multiple of 8 (sizes shared memory).
 void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count,
-                  DeviceStatus *status, cudaStream_t st);
+                  DeviceStatus *status, int p8max, cudaStream_t st);
 void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st);
 
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
@@ -92,8 +93,9 @@ void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_
                          const RowTask *tasks, int count, cudaStream_t st);
 // Forward: y = L_pp^-1 x_p into x2, then x (own rows) / v (rows past the columns) -= L y.
 // Backward: z = L_pp^-T x2_p into x, then x2 (own rows above) -= L^T z.
+// k4max: the widest panel of the launch, rounded up to a multiple of 4.
 void launch_solve_panel(const Tree &t, bool backward, double *x, double *x2, double *v, const int64_t *voff,
-                        int R, const SolveTask *tasks, int count, cudaStream_t st);
+                        int R, const SolveTask *tasks, int count, int k4max, cudaStream_t st);
 // x_post[i*R + j] = b[perm[i] + j*ld] and back.
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
                        cudaStream_t st);
