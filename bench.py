@@ -362,13 +362,13 @@ def main():
         "factor_tflops": full_flops / (factor_ms * 1e-3) / 1e12 if factor_ms > 0 else None,
         "phase_ms": {"factor": factor_ms, "solve": solve_ms,
                      "by_kernel": {name: round(float(ms_k[k]), 3) for k, name in
-                                   [(0, "assemble"), (1, "panel"), (3, "gemm"), (19, "solve_gemm"),
+                                   [(0, "assemble"), (1, "panel"), (3, "gemm"), (18, "solve_reduce"), (19, "solve_gemm"),
                                     (20, "solve_assemble"), (21, "solve_gather"), (22, "solve_fwd_panel"),
                                     (23, "solve_bwd_panel")]},
                      "launches": {name: int(cnt_k[k]) for k, name in
-                                  [(0, "assemble"), (1, "panel"), (3, "gemm"), (19, "solve_gemm"),
-                                   (20, "solve_assemble"), (21, "solve_gather"), (22, "solve_fwd_panel"),
-                                   (23, "solve_bwd_panel")]}},
+                                  [(0, "assemble"), (1, "panel"), (3, "gemm"), (18, "solve_reduce"),
+                                   (19, "solve_gemm"), (20, "solve_assemble"), (21, "solve_gather"),
+                                   (22, "solve_fwd_panel"), (23, "solve_bwd_panel")]}},
         "roofline": {"kernel": "gemm_kernel (FP64 DMMA, factor updates)", "bound": "tensor",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "

@@ -84,7 +84,7 @@ cudaError_t upload(DeviceBuf &buf, const std::vector<T> &host, cudaStream_t st) 
   return cudaMemcpyAsync(buf.p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, st);
 }
 
-enum Kind { K_ASSEMBLE, K_PANEL, K_UNUSED, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD };
+enum Kind { K_ASSEMBLE, K_PANEL, K_REDUCE, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD };
 
 struct Launch {
   int kind;
@@ -106,18 +106,20 @@ struct fc_chol {
   std::vector<int32_t> width, height, rows;
   std::vector<int64_t> kid_ptr;
   std::vector<int32_t> kids;
+  std::vector<int64_t> rel_off;  // host copies of the relative maps (for planning)
+  std::vector<int32_t> rel;
   std::vector<int32_t> level;
   int64_t l_len = 0, u_len = 0;
   // device
   DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
   DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_D, d_perm, d_val, d_status, d_toff, d_doff;
-  DeviceBuf d_asm, d_panel, d_gemm;
+  DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
   fc::Tree tree{};
   std::vector<Launch> program;
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
-  DeviceBuf d_x, d_x2, d_v, d_voff, d_b, d_srow, d_spanel, d_sgemm;
+  DeviceBuf d_x, d_x2, d_v, d_part, d_voff, d_b, d_srow, d_sranges, d_spanel, d_sgemm, d_sreduce;
   std::vector<Launch> fwd, bwd;
   int64_t last_factor_launches = 0, last_solve_launches = 0;
   double gemm_flops_factor = 0, gemm_flops_solve = 0;
@@ -176,6 +178,21 @@ std::vector<std::vector<int64_t>> levels_of(fc_chol *h) {
 
 void push(std::vector<Launch> &prog, int kind, int64_t off, int64_t count, int level, int width = 0) {
   if (count > 0) prog.push_back({kind, off, (int)count, level, width});
+}
+
+// For front positions [lo, hi) of supernode s: each child's positions (in its update matrix) whose
+// place in s's front falls in [lo, hi), appended to `ranges`; returns where they start.
+int32_t child_ranges(const fc_chol *h, int64_t s, int lo, int hi, std::vector<int2> &ranges) {
+  const int32_t at = (int32_t)ranges.size();
+  for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) {
+    const int64_t c = h->kids[q];
+    const int uc = h->height[c] - h->width[c];
+    const int32_t *rel = h->rel.data() + h->rel_off[c];
+    const int a = (int)(std::lower_bound(rel, rel + uc, lo) - rel);
+    const int b = (int)(std::lower_bound(rel, rel + uc, hi) - rel);
+    ranges.push_back(make_int2(a, b));
+  }
+  return at;
 }
 
 // Useful flops of a GEMM task (a diagonal tile computes its lower triangle only).
@@ -243,7 +260,7 @@ int64_t arena_offsets(const fc_chol *h, const std::vector<std::vector<int64_t>> 
 // The factor's program: per level, assemble; per panel, the fused factor/invert/solve of the
 // panel, then the update of the later columns; then the update matrices.
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
-                 std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
+                 std::vector<int2> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
   double *L = h->d_L.as<double>();
   double *U = h->d_U.as<double>();
   const int NB = fc::NB;
@@ -251,9 +268,11 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     const auto &S = lv[l];
     int64_t off = (int64_t)asm_t.size();
     for (int64_t s : S) {
-      const int m = h->height[s];
-      for (int j0 = 0; j0 < m; j0 += fc::ASSEMBLE_COLS)
-        asm_t.push_back({(int32_t)s, j0, std::min(m, j0 + fc::ASSEMBLE_COLS), 0});
+      const int w = h->width[s];
+      for (int j0 = 0; j0 < w; j0 += fc::ASSEMBLE_COLS) {
+        const int j1 = std::min(w, j0 + fc::ASSEMBLE_COLS);
+        asm_t.push_back({(int32_t)s, j0, j1, child_ranges(h, s, j0, j1, ranges)});
+      }
     }
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
     int P = 0;
@@ -305,11 +324,22 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
           g.M = std::min(fc::GEMM_TM, u - bi);
           g.N = std::min(fc::GEMM_TN, u - bj);
           g.K = w;
-          g.flags = bi == bj ? 1 : 0;
+          g.flags = (bi == bj ? 1 : 0) | 2;
           gemm_t.push_back(g);
         }
     }
     push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+    // the children's contributions to the update matrices, on top of -L21 L21^T
+    off = (int64_t)asm_t.size();
+    for (int64_t s : S) {
+      const int m = h->height[s], w = h->width[s];
+      if (h->kid_ptr[s + 1] == h->kid_ptr[s]) continue;
+      for (int j0 = w; j0 < m; j0 += fc::ASSEMBLE_COLS) {
+        const int j1 = std::min(m, j0 + fc::ASSEMBLE_COLS);
+        asm_t.push_back({(int32_t)s, j0, j1, child_ranges(h, s, j0, j1, ranges)});
+      }
+    }
+    push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
   }
 }
 
@@ -410,6 +440,8 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       if (r == c) diag_src[c] = e;
     }
   }
+  h->rel_off = rel_off;
+  h->rel = rel;
   auto lv = levels_of(h);
   {
     std::vector<int64_t> usize(ns);
@@ -474,9 +506,10 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   t.U = h->d_U.as<double>();
   t.D = h->d_D.as<double>();
   std::vector<fc::AssembleTask> asm_t;
+  std::vector<int2> ranges;
   std::vector<fc::PanelTask> panel_t;
   std::vector<fc::GemmTask> gemm_t;
-  plan_factor(h, lv, asm_t, panel_t, gemm_t);
+  plan_factor(h, lv, asm_t, ranges, panel_t, gemm_t);
   h->gemm_tasks = (int64_t)gemm_t.size();
   h->gemm_flops_factor = 0;
   for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
@@ -498,7 +531,8 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       ++ordinal;
     }
   }
-  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_panel, panel_t, stream)) != cudaSuccess ||
+  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_ranges, ranges, stream)) != cudaSuccess ||
+      (e = upload(h->d_panel, panel_t, stream)) != cudaSuccess ||
       (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
     return cuda_fail(st, e, "upload of the plan");
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
@@ -598,7 +632,9 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
     }
     Mark mark(h, l.kind);
     switch (l.kind) {
-      case K_ASSEMBLE: fc::launch_assemble(t, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, l.count, st); break;
+      case K_ASSEMBLE:
+        fc::launch_assemble(t, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, h->d_ranges.as<int2>(), l.count, st);
+        break;
       case K_PANEL:
         fc::launch_panel(t, d_val, h->d_panel.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(),
                          l.width, st);
@@ -636,7 +672,10 @@ int read_status(fc_chol *h, fc_status *st) {
 struct SolvePlan {
   std::vector<int64_t> voff;
   int64_t vsum = 0;
+  int64_t psum = 0;  // doubles of the split GEMMs' partial tiles
+  std::vector<fc::ReduceTask> reduce;
   std::vector<fc::RowTask> rows;
+  std::vector<int2> ranges;
   std::vector<fc::SolveTask> panels;
   std::vector<fc::GemmTask> gemm;
   std::vector<Launch> fwd, bwd;
@@ -648,9 +687,22 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
   std::vector<int64_t> vsize(h->ns);
   for (int64_t s = 0; s < h->ns; ++s) vsize[s] = (int64_t)(h->height[s] - h->width[s]) * R;
   p.vsum = arena_offsets(h, lv, vsize, p.voff);
+  // the backward update of a supernode's own rows by its rows below (K = u) is split in chunks of
+  // SPLIT_K when u is long; its partial tiles are reused level after level
+  int64_t most = 0;
+  for (const auto &S : lv) {
+    int64_t level = 0;
+    for (int64_t s : S) {
+      const int64_t u = h->height[s] - h->width[s], w = h->width[s];
+      if (u > 2 * fc::SPLIT_K)
+        level += (u + fc::SPLIT_K - 1) / fc::SPLIT_K * ((w + 63) / 64) * ((R + 63) / 64) * 4096;
+    }
+    most = std::max(most, level);
+  }
+  p.psum = most;
 }
 
-void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, SolvePlan &p) {
+void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, double *part, SolvePlan &p) {
   const int NB = fc::NB;
   std::vector<std::vector<int64_t>> lv(h->levels);
   for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
@@ -668,7 +720,10 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
       const int m = h->height[s], w = h->width[s];
       const bool kids = h->kid_ptr[s + 1] > h->kid_ptr[s];
       if (!kids && m == w) continue;
-      for (int i0 = kids ? 0 : w; i0 < m; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(m, i0 + 64), 0});
+      for (int i0 = kids ? 0 : w; i0 < m; i0 += 64) {
+        const int i1 = std::min(m, i0 + 64);
+        rows.push_back({(int32_t)s, i0, i1, child_ranges(h, s, i0, i1, p.ranges)});
+      }
     }
     push(fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
     int P = 0;
@@ -707,27 +762,43 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
       for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
     }
     push(bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
-    int64_t go = (int64_t)gemm.size();
+    int64_t go = (int64_t)gemm.size(), ro2 = (int64_t)p.reduce.size(), pat = 0;
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
       if (u <= 0) continue;
       const double *Ls = L + h->loff[s];
+      const bool split = u > 2 * fc::SPLIT_K;
+      const int chunks = split ? (u + fc::SPLIT_K - 1) / fc::SPLIT_K : 1;
       for (int i0 = 0; i0 < w; i0 += fc::GEMM_TM)
         for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
-          fc::GemmTask g{};
-          g.C = x2 + (h->first[s] + i0) * (int64_t)R + j0;
-          g.c_si = R, g.c_sj = 1;
-          g.A = Ls + w + (int64_t)i0 * m;
-          g.a_si = m, g.a_sk = 1;
-          g.B = v + voff[s] + j0;
-          g.b_sj = 1, g.b_sk = R;
-          g.M = std::min(fc::GEMM_TM, w - i0);
-          g.N = std::min(fc::GEMM_TN, R - j0);
-          g.K = u;
-          gemm.push_back(g);
+          const int M = std::min(fc::GEMM_TM, w - i0), N = std::min(fc::GEMM_TN, R - j0);
+          double *tile = x2 + (h->first[s] + i0) * (int64_t)R + j0;
+          for (int q = 0; q < chunks; ++q) {
+            const int k0 = split ? q * fc::SPLIT_K : 0, k1 = split ? std::min(u, k0 + fc::SPLIT_K) : u;
+            fc::GemmTask g{};
+            if (split) {
+              g.C = part + pat + (int64_t)q * 4096;
+              g.c_si = 64, g.c_sj = 1;
+              g.flags = 4;
+            } else {
+              g.C = tile;
+              g.c_si = R, g.c_sj = 1;
+            }
+            g.A = Ls + w + k0 + (int64_t)i0 * m;
+            g.a_si = m, g.a_sk = 1;
+            g.B = v + voff[s] + (int64_t)k0 * R + j0;
+            g.b_sj = 1, g.b_sk = R;
+            g.M = M, g.N = N, g.K = k1 - k0;
+            gemm.push_back(g);
+          }
+          if (split) {
+            p.reduce.push_back({tile, part + pat, (int64_t)R, M, N, chunks, 0});
+            pat += (int64_t)chunks * 4096;
+          }
         }
     }
     push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+    push(bwd, K_REDUCE, ro2, (int64_t)p.reduce.size() - ro2, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     for (int p = P - 1; p >= 0; --p) {
@@ -763,18 +834,20 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   cudaError_t e;
   if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
       h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
-      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess) {
+      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess ||
+      h->d_part.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.psum, 1)) != cudaSuccess) {
     h->solve_R = 0;
     set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
     return FC_OUT_OF_MEMORY;
   }
   if ((e = upload(h->d_voff, p.voff, h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
-  solve_tasks(h, R, h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), p);
+  solve_tasks(h, R, h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), h->d_part.as<double>(), p);
   h->fwd = std::move(p.fwd);
   h->bwd = std::move(p.bwd);
   h->gemm_flops_solve = 0;
   for (const auto &g : p.gemm) h->gemm_flops_solve += task_flops(g);
-  if ((e = upload(h->d_srow, p.rows, h->stream)) != cudaSuccess || (e = upload(h->d_spanel, p.panels, h->stream)) != cudaSuccess ||
+  if ((e = upload(h->d_srow, p.rows, h->stream)) != cudaSuccess || (e = upload(h->d_sranges, p.ranges, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_spanel, p.panels, h->stream)) != cudaSuccess || (e = upload(h->d_sreduce, p.reduce, h->stream)) != cudaSuccess ||
       (e = upload(h->d_sgemm, p.gemm, h->stream)) != cudaSuccess)
     return cuda_fail(st, e, "solve plan");
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
@@ -787,13 +860,16 @@ struct SolveBuffers {
   double *x, *x2, *v;
   const int64_t *voff;
   const fc::RowTask *rows;
+  const int2 *ranges;
   const fc::SolveTask *panels;
   const fc::GemmTask *gemm;
+  const fc::ReduceTask *reduce;
 };
 
 SolveBuffers own_buffers(fc_chol *h) {
-  return {h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), h->d_voff.as<int64_t>(),
-          h->d_srow.as<fc::RowTask>(), h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>()};
+  return {h->d_x.as<double>(),       h->d_x2.as<double>(),        h->d_v.as<double>(),
+          h->d_voff.as<int64_t>(),     h->d_srow.as<fc::RowTask>(), h->d_sranges.as<int2>(),
+          h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>(), h->d_sreduce.as<fc::ReduceTask>()};
 }
 
 void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveBuffers &b, int R, int64_t &launches) {
@@ -802,7 +878,9 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
   for (const Launch &l : prog) {
     Mark mark(h, l.kind + 16);
     switch (l.kind) {
-      case K_SOLVE_ASSEMBLE: fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
+      case K_SOLVE_ASSEMBLE:
+        fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st);
+        break;
       case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_FWD:
         fc::launch_solve_panel(t, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
@@ -811,6 +889,7 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         fc::launch_solve_panel(t, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
         break;
       case K_GEMM: fc::launch_gemm(b.gemm + l.off, l.count, st); break;
+      case K_REDUCE: fc::launch_reduce(b.reduce + l.off, l.count, st); break;
     }
     ++launches;
   }
@@ -1176,12 +1255,14 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   cudaError_t e = noalloc_scratch(h->device, &base);
   if (e != cudaSuccess) return cuda_fail(status, e, "cudaGetSymbolAddress of the solve scratch");
   const int R = nrhs;
-  // Layout in the scratch: x | x2 | v | voff | row tasks | panel tasks | GEMM tasks.
+  // Layout in the scratch: x | x2 | v | partial tiles | voff | row tasks | child ranges | panel
+  // tasks | GEMM tasks | reduction tasks.
   SolvePlan p;
   solve_offsets(h, R, p);
   const size_t vec = align256(sizeof(double) * (size_t)h->n * R);
   const size_t at_x = 0, at_x2 = vec, at_v = 2 * vec;
-  const size_t at_voff = at_v + align256(sizeof(double) * (size_t)p.vsum);
+  const size_t at_part = at_v + align256(sizeof(double) * (size_t)p.vsum);
+  const size_t at_voff = at_part + align256(sizeof(double) * (size_t)p.psum);
   auto too_large = [&](size_t need) {
     char msg[160];
     std::snprintf(msg, sizeof(msg), "the solve needs %zu bytes of scratch; the no-allocation limit is %zu",
@@ -1191,27 +1272,34 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   };
   if (at_voff > FC_NOALLOC_SCRATCH_BYTES) return too_large(at_voff);
   solve_tasks(h, R, reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
-              reinterpret_cast<double *>(base + at_v), p);
+              reinterpret_cast<double *>(base + at_v), reinterpret_cast<double *>(base + at_part), p);
   const size_t at_rows = at_voff + align256(sizeof(int64_t) * p.voff.size());
-  const size_t at_panels = at_rows + align256(sizeof(fc::RowTask) * p.rows.size());
+  const size_t at_ranges = at_rows + align256(sizeof(fc::RowTask) * p.rows.size());
+  const size_t at_panels = at_ranges + align256(sizeof(int2) * p.ranges.size());
   const size_t at_gemm = at_panels + align256(sizeof(fc::SolveTask) * p.panels.size());
-  const size_t need = at_gemm + sizeof(fc::GemmTask) * p.gemm.size();
+  const size_t at_reduce = at_gemm + align256(sizeof(fc::GemmTask) * p.gemm.size());
+  const size_t need = at_reduce + sizeof(fc::ReduceTask) * p.reduce.size();
   if (need > FC_NOALLOC_SCRATCH_BYTES) return too_large(need);
   // Every region is written before it is read in this call: the task lists and offsets here, x by
-  // the permutation, x2 by the forward panels, each update vector's rows zeroed by its assembly.
+  // the permutation, x2 by the forward panels, each update vector's rows zeroed by its assembly,
+  // each partial tile stored by its GEMM task before its reduction reads it.
   auto put = [&](size_t at, const void *src, size_t bytes) {
     if (bytes && e == cudaSuccess) e = cudaMemcpyAsync(base + at, src, bytes, cudaMemcpyHostToDevice, h->stream);
   };
   put(at_voff, p.voff.data(), sizeof(int64_t) * p.voff.size());
   put(at_rows, p.rows.data(), sizeof(fc::RowTask) * p.rows.size());
+  put(at_ranges, p.ranges.data(), sizeof(int2) * p.ranges.size());
   put(at_panels, p.panels.data(), sizeof(fc::SolveTask) * p.panels.size());
   put(at_gemm, p.gemm.data(), sizeof(fc::GemmTask) * p.gemm.size());
+  put(at_reduce, p.reduce.data(), sizeof(fc::ReduceTask) * p.reduce.size());
   if (e != cudaSuccess) return cuda_fail(status, e, "copy of the solve plan into the scratch");
   const SolveBuffers b{reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
                        reinterpret_cast<double *>(base + at_v), reinterpret_cast<const int64_t *>(base + at_voff),
                        reinterpret_cast<const fc::RowTask *>(base + at_rows),
+                       reinterpret_cast<const int2 *>(base + at_ranges),
                        reinterpret_cast<const fc::SolveTask *>(base + at_panels),
-                       reinterpret_cast<const fc::GemmTask *>(base + at_gemm)};
+                       reinterpret_cast<const fc::GemmTask *>(base + at_gemm),
+                       reinterpret_cast<const fc::ReduceTask *>(base + at_reduce)};
   int64_t launches = 0;
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, b.x, R, h->stream);
   run_solve_program(h, p.fwd, b, R, launches);

@@ -45,11 +45,14 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
 }
 
 // ---- front assembly ----------------------------------------------------------------------------
-// Columns [j0, j1) of supernode s's front: zero them, place A's entries, then add each child's
-// update matrix in child order (the front is the multifrontal form of the reference's
-// own(rel(i), rel(c)) -= S(i, c), cholesky.rs:636-686, summed child by child).
-__global__ void __launch_bounds__(256) assemble_kernel(Tree t, const double *__restrict__ val,
-                                                       const AssembleTask *__restrict__ tasks) {
+// Columns [j0, j1) of supernode s's front, then each child's update matrix added in child order
+// (the multifrontal form of the reference's own(rel(i), rel(c)) -= S(i, c), cholesky.rs:636-686,
+// summed child by child). Columns of the L panel (j < w) are zeroed and take A's entries first,
+// before the panel is factored; columns of the update matrix (j >= w) are assembled after its
+// GEMM stored -L21 L21^T there.
+__global__ void __launch_bounds__(ASSEMBLE_THREADS) assemble_kernel(Tree t, const double *__restrict__ val,
+                                                       const AssembleTask *__restrict__ tasks,
+                                                       const int2 *__restrict__ ranges) {
   const AssembleTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], w = t.width[s], u = m - w, f = t.first[s];
@@ -57,14 +60,10 @@ __global__ void __launch_bounds__(256) assemble_kernel(Tree t, const double *__r
   double *Us = t.U + t.uoff[s];
   const int j0 = task.j0, j1 = task.j1;
   const int tid = threadIdx.x;
-  for (int j = j0; j < j1; ++j) {
-    if (j < w) {
-      double *col = Ls + (int64_t)j * m;
-      for (int64_t i = tid; i < m; i += blockDim.x) col[i] = 0.0;
-    } else {
-      double *col = Us + (int64_t)(j - w) * u;
-      for (int64_t i = (j - w) + tid; i < u; i += blockDim.x) col[i] = 0.0;
-    }
+  // the L panel's columns start from zero; the update matrix's were stored by its GEMM already
+  for (int j = j0; j < j1 && j < w; ++j) {
+    double *col = Ls + (int64_t)j * m;
+    for (int64_t i = tid; i < m; i += blockDim.x) col[i] = 0.0;
   }
   __syncthreads();
   const int jend = j1 < w ? j1 : (int)w;
@@ -74,17 +73,34 @@ __global__ void __launch_bounds__(256) assemble_kernel(Tree t, const double *__r
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-  for (int64_t kp = t.kid_ptr[s]; kp < t.kid_ptr[s + 1]; ++kp) {
+  const int64_t k0 = t.kid_ptr[s], k1 = t.kid_ptr[s + 1];
+  for (int64_t kp = k0; kp < k1; ++kp) {
     const int c = t.kids[kp];
     const int uc = t.height[c] - t.width[c];
     const int32_t *rel = t.rel + t.rel_off[c];
     const double *Uc = t.U + t.uoff[c];
-    const int lo = lower_bound_i32(rel, uc, j0), hi = lower_bound_i32(rel, uc, j1);
+    const int2 range = ranges[task.ranges + (kp - k0)];
+    const int lo = range.x, hi = range.y;
     for (int jc = lo + warp; jc < hi; jc += nwarps) {
       const int64_t J = rel[jc];
       const double *src = Uc + (int64_t)jc * uc;
       double *dst = J < w ? Ls + J * m : Us + (J - w) * u - w;
-      for (int ic = jc + lane; ic < uc; ic += 32) dst[rel[ic]] += src[ic];
+      // four rows a lane in flight: the loads of a batch are issued before its stores
+      int ic = jc + lane;
+      for (; ic + 96 < uc; ic += 128) {
+        int r[4];
+        double v[4], d[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          r[q] = rel[ic + 32 * q];
+          v[q] = src[ic + 32 * q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = dst[r[q]];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dst[r[q]] = d[q] + v[q];
+      }
+      for (; ic < uc; ic += 32) dst[rel[ic]] += src[ic];
     }
     __syncthreads();
   }
@@ -96,19 +112,24 @@ __global__ void __launch_bounds__(256) assemble_kernel(Tree t, const double *__r
 constexpr int TS = 68;
 
 // dst[k * TS + i] = src[i * si + k * sk] for i < rows, k < kk, zero for the other i < 64 and
-// kk <= k < kpad (rows k >= kpad of the tile are not touched). One warp per k (rows contiguous in
-// memory) or one warp per i (k contiguous), so every warp reads a contiguous run.
+// kk <= k < kpad (rows k >= kpad of the tile are not touched). Issued as cp.async copies, so a
+// tile's loads are all in flight at once; the caller commits, waits and synchronises. One warp per
+// k (rows contiguous in memory) or one warp per i (k contiguous): every warp reads a contiguous run.
 __device__ __forceinline__ void load_tile(double *dst, const double *__restrict__ src, int64_t si, int64_t sk, int rows,
                                           int kk, int kpad) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (si == 1) {
     for (int k = warp; k < kpad; k += nw)
-      for (int i = lane; i < 64; i += 32)
-        dst[k * TS + i] = (i < rows && k < kk) ? src[i + (int64_t)k * sk] : 0.0;
+      for (int i = lane; i < 64; i += 32) {
+        const bool ok = i < rows && k < kk;
+        cp_async8(&dst[k * TS + i], ok ? src + i + (int64_t)k * sk : src, ok ? 8 : 0);
+      }
   } else {
     for (int i = warp; i < 64; i += nw)
-      for (int k = lane; k < kpad; k += 32)
-        dst[k * TS + i] = (i < rows && k < kk) ? src[(int64_t)i * si + k * sk] : 0.0;
+      for (int k = lane; k < kpad; k += 32) {
+        const bool ok = i < rows && k < kk;
+        cp_async8(&dst[k * TS + i], ok ? src + (int64_t)i * si + k * sk : src, ok ? 8 : 0);
+      }
   }
 }
 
@@ -183,34 +204,76 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
   // the block's lower triangle, identity past pw (so the padded block inverts to the same
   // leading pw x pw inverse)
   for (int c = warp; c < P8; c += PANEL_THREADS / 32)
-    for (int r = lane; r < P8; r += 32)
-      a[c * 65 + r] = (r < pw && c < pw) ? (r >= c ? Ls[(c0 + r) + (int64_t)(c0 + c) * m] : 0.0) : (r == c ? 1.0 : 0.0);
+    for (int r = lane; r < P8; r += 32) {
+      if (r < pw && c < pw && r >= c)
+        cp_async8(&a[c * 65 + r], Ls + (c0 + r) + (int64_t)(c0 + c) * m, 8);
+      else
+        a[c * 65 + r] = (r >= pw || c >= pw) && r == c ? 1.0 : 0.0;
+    }
   for (int c = tid; c < pw; c += PANEL_THREADS) {
     const int64_t ds = t.diag_src[f + c0 + c];
     dg[c] = ds >= 0 ? val[ds] : 0.0;
   }
   for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
   if (rows > 0) load_tile(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
-  // right-looking: column c scaled by its pivot, then the trailing triangle; two threads a row
-  const int ri = tid & 63, rh = tid >> 6;
-  for (int c = 0; c < pw; ++c) {
-    const double acc = a[c * 65 + c];
-    const double d = sqrt(acc);
-    if (ri > c && ri < pw && rh == 0) a[c * 65 + ri] /= d;
-    if (tid == 0) {
-      dv[c] = d;
-      if ((!(acc > PIVOT_TOLERANCE * fabs(dg[c])) || !isfinite(acc)) && fail == pw) fail = c;
+  // right-looking by strips of 8 columns: one warp factors a strip (two rows a lane, pivots and
+  // multipliers broadcast by shuffles), then the four warps update the trailing lower triangle
+  // with DMMA (a rank-8 update per 8 x 8 block); padding past pw factors as the identity
+  for (int B = 0; B < nb8; ++B) {
+    const int o = 8 * B;
+    if (warp == 0) {
+      const int r0 = o + lane, r1 = o + 32 + lane;
+      double s0[8], s1[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        s0[k] = r0 < P8 ? a[(o + k) * 65 + r0] : 0.0;
+        s1[k] = r1 < P8 ? a[(o + k) * 65 + r1] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double acc = __shfl_sync(0xffffffffu, s0[j], j);
+        const double d = sqrt(acc);
+        const double rd = 1.0 / d;
+        if (lane == j) {
+          s0[j] = d;
+          dv[o + j] = rd;
+          if (o + j < pw && (!(acc > PIVOT_TOLERANCE * fabs(dg[o + j])) || !isfinite(acc)) && fail == pw) fail = o + j;
+        } else if (lane > j) {
+          s0[j] *= rd;
+        }
+        s1[j] *= rd;
+#pragma unroll
+        for (int k = j + 1; k < 8; ++k) {
+          const double lk = __shfl_sync(0xffffffffu, s0[j], k);
+          if (lane > j) s0[k] -= s0[j] * lk;
+          s1[k] -= s1[j] * lk;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (r0 < P8) a[(o + k) * 65 + r0] = s0[k];
+        if (r1 < P8) a[(o + k) * 65 + r1] = s1[k];
+      }
     }
     __syncthreads();
-    if (ri > c && ri < pw) {
-      const double lic = a[c * 65 + ri];
-      for (int j = c + 1 + rh; j <= ri; j += 2) a[j * 65 + ri] -= lic * a[c * 65 + j];
-    }
+    const int nrem = nb8 - B - 1;
+    int q = 0;
+    for (int qi = 0; qi < nrem; ++qi)
+      for (int qj = 0; qj <= qi; ++qj, ++q) {
+        if ((q & 3) != warp) continue;
+        const int I = 8 * (B + 1 + qi), J = 8 * (B + 1 + qj);
+        const int g = lane >> 2, tg = lane & 3;
+        double c[2] = {0.0, 0.0};
+        dmma(c, a[(o + tg) * 65 + I + g], a[(o + tg) * 65 + J + g]);
+        dmma(c, a[(o + 4 + tg) * 65 + I + g], a[(o + 4 + tg) * 65 + J + g]);
+        a[(J + 2 * tg) * 65 + I + g] -= c[0];
+        a[(J + 2 * tg + 1) * 65 + I + g] -= c[1];
+      }
     __syncthreads();
   }
-  for (int c = tid; c < pw; c += PANEL_THREADS) a[c * 65 + c] = dv[c];
-  __syncthreads();
   // inverse: the diagonal 8 x 8 blocks (a column each) ...
   if (tid < P8) {
     const int B = tid >> 3, j = tid & 7, o = 8 * B;
@@ -219,8 +282,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
     for (int i = 0; i < 8; ++i) {
       if (i >= j) {
         double sum = i == j ? 1.0 : 0.0;
-        for (int k = j; k < i; ++k) sum -= a[(o + k) * 65 + o + i] * y[k];
-        y[i] = sum / a[(o + i) * 65 + o + i];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (k >= j && k < i) sum -= a[(o + k) * 65 + o + i] * y[k];
+        y[i] = sum * dv[o + i];
       } else {
         y[i] = 0.0;
       }
@@ -360,7 +425,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
   }
   cp_async_wait<0>();
   const int M = tp->M, N = tp->N;
-  const bool lower = tp->flags & 1;
+  const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
   double *C = tp->C;
   const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
 #pragma unroll
@@ -370,8 +435,28 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int i = wm + r * 8 + g, j = wn + c * 8 + 2 * tg + e;
-        if (i < M && j < N && (!lower || i >= j)) C[(int64_t)i * c_si + (int64_t)j * c_sj] -= acc[r][c][e];
+        if (i < M && j < N && (!lower || i >= j)) {
+          double *dst = C + (int64_t)i * c_si + (int64_t)j * c_sj;
+          if (partial)
+            *dst = acc[r][c][e];
+          else if (store)
+            *dst = -acc[r][c][e];
+          else
+            *dst -= acc[r][c][e];
+        }
       }
+}
+
+// ---- the reduction of a split GEMM's partials, in a fixed order ----------------------------------
+__global__ void __launch_bounds__(256) reduce_kernel(const ReduceTask *__restrict__ tasks) {
+  const ReduceTask tk = tasks[blockIdx.x];
+  for (int e = threadIdx.x; e < tk.M * 64; e += blockDim.x) {
+    const int i = e >> 6, j = e & 63;
+    if (j >= tk.N) continue;
+    double sum = 0.0;
+    for (int q = 0; q < tk.count; ++q) sum += tk.P[(int64_t)q * 4096 + i * 64 + j];
+    tk.C[(int64_t)i * tk.c_si + j] -= sum;
+  }
 }
 
 // ---- solve -------------------------------------------------------------------------------------
@@ -379,7 +464,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
 // update vectors in child order.
 __global__ void __launch_bounds__(256) solve_assemble_kernel(Tree t, double *__restrict__ x, double *__restrict__ v,
                                                              const int64_t *__restrict__ voff, int R,
-                                                             const RowTask *__restrict__ tasks) {
+                                                             const RowTask *__restrict__ tasks,
+                                                             const int2 *__restrict__ ranges) {
   const RowTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
@@ -388,12 +474,13 @@ __global__ void __launch_bounds__(256) solve_assemble_kernel(Tree t, double *__r
   const int64_t z0 = task.i0 > w ? task.i0 : w;
   for (int64_t e = tid; e < (task.i1 - z0) * R; e += blockDim.x) vs[(z0 - w) * R + e] = 0.0;
   __syncthreads();
-  for (int64_t kp = t.kid_ptr[s]; kp < t.kid_ptr[s + 1]; ++kp) {
+  const int64_t k0 = t.kid_ptr[s], k1 = t.kid_ptr[s + 1];
+  for (int64_t kp = k0; kp < k1; ++kp) {
     const int c = t.kids[kp];
-    const int uc = t.height[c] - t.width[c];
     const int32_t *rel = t.rel + t.rel_off[c];
     const double *vc = v + voff[c];
-    const int lo = lower_bound_i32(rel, uc, task.i0), hi = lower_bound_i32(rel, uc, task.i1);
+    const int2 range = ranges[task.ranges + (kp - k0)];
+    const int lo = range.x, hi = range.y;
     for (int64_t e = tid; e < (int64_t)(hi - lo) * R; e += blockDim.x) {
       const int ic = lo + (int)(e / R), j = (int)(e % R);
       const int64_t I = rel[ic];
@@ -453,6 +540,8 @@ __global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__rest
     else
       load_tile(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);  // bt[k][r] = L(r0 + r, c0 + k)
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   double acc[4][4][2];
   zero_acc(acc);
@@ -535,8 +624,9 @@ void configure_kernels() {
   done = true;
 }
 
-void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, int count, cudaStream_t st) {
-  if (count > 0) assemble_kernel<<<count, 256, 0, st>>>(t, upper_val, tasks);
+void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, const int2 *ranges, int count,
+                     cudaStream_t st) {
+  if (count > 0) assemble_kernel<<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
 }
 
 void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count, DeviceStatus *status,
@@ -552,9 +642,13 @@ void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st) {
   gemm_kernel<<<count, GEMM_THREADS, GEMM_SMEM, st>>>(tasks);
 }
 
+void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st) {
+  if (count > 0) reduce_kernel<<<count, 256, 0, st>>>(tasks);
+}
+
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,
-                           int count, cudaStream_t st) {
-  if (count > 0) solve_assemble_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks);
+                           const int2 *ranges, int count, cudaStream_t st) {
+  if (count > 0) solve_assemble_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks, ranges);
 }
 
 void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,

@@ -13,7 +13,9 @@ constexpr int NB = 64;
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_KC = 16;
 constexpr int GEMM_THREADS = 128;
 constexpr int PANEL_ROWS = 64;  // rows of a panel solved by one CTA
-constexpr int ASSEMBLE_COLS = 32;  // front columns assembled by one CTA
+constexpr int ASSEMBLE_COLS = 8;  // front columns assembled by one CTA
+constexpr int ASSEMBLE_THREADS = 128;
+constexpr int SPLIT_K = 512;  // K chunk of a split GEMM (a long sum over few outputs)
 
 // Where each supernode lives on the device. A front of supernode s has m = rows(s) rows and
 // w = width(s) columns of L; its update matrix U_s is the (m-w) x (m-w) Schur complement.
@@ -40,8 +42,10 @@ struct Tree {
   double *D;
 };
 
+// Front columns [j0, j1) of supernode s; ranges[q] (from `ranges`) is child q's columns (in its
+// update matrix) that land in them.
 struct AssembleTask {
-  int32_t s, j0, j1, pad;
+  int32_t s, j0, j1, ranges;
 };
 // Panel [c0, c1) of supernode s: factor its diagonal block, invert it, and solve the rows
 // [r0, r1) below it (r0 >= c1; an empty range for a task that only keeps the block). The task
@@ -51,13 +55,23 @@ struct PanelTask {
   int32_t s, c0, c1, r0, r1, keep;
   int64_t doff;
 };
-// C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands; flag 1: store i >= j only.
+// C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands. Flags: 1 touches
+// i >= j only (a diagonal tile of a symmetric matrix); 2 stores C = -sum instead of subtracting;
+// 4 stores C = +sum (one partial of a split sum, reduced later by a ReduceTask).
 struct GemmTask {
   double *C;
   const double *A;
   const double *B;
   int64_t c_si, c_sj, a_si, a_sk, b_sj, b_sk;
   int32_t M, N, K, flags;
+};
+// C(i, j) -= sum_q P[q][i][j] for i < M, j < N: the partials of a split GEMM (64 x 64 tiles,
+// row-major, one after another), summed in order.
+struct ReduceTask {
+  double *C;
+  const double *P;
+  int64_t c_si;
+  int32_t M, N, count, pad;
 };
 // Solve, panel [c0, c1) of supernode s, right-hand sides [j0, j1): apply the inverse of the
 // diagonal block (forward: L^-1, backward: L^-T), then update the front rows [r0, r1) (forward:
@@ -66,9 +80,9 @@ struct SolveTask {
   int32_t s, c0, c1, r0, r1, j0, j1, keep;
   int64_t doff;
 };
-// Solve front rows [i0, i1) of supernode s.
+// Solve front rows [i0, i1) of supernode s; `ranges` as in AssembleTask, for the children's rows.
 struct RowTask {
-  int32_t s, i0, i1, pad;
+  int32_t s, i0, i1, ranges;
 };
 
 // Device status word of a factorisation: the smallest failing pivot column (postorder).
@@ -79,16 +93,17 @@ struct DeviceStatus {
 // Sets the kernels' shared-memory limits (once per process; before any stream capture).
 void configure_kernels();
 
-void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, int count,
-                     cudaStream_t st);
+void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, const int2 *ranges,
+                     int count, cudaStream_t st);
 // p8max: the widest panel of the launch, rounded up to a multiple of 8 (sizes shared memory).
 void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count,
                   DeviceStatus *status, int p8max, cudaStream_t st);
 void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st);
+void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st);
 
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R,
-                           const RowTask *tasks, int count, cudaStream_t st);
+                           const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st);
 void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R,
                          const RowTask *tasks, int count, cudaStream_t st);
 // Forward: y = L_pp^-1 x_p into x2, then x (own rows) / v (rows past the columns) -= L y.

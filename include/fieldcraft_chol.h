@@ -145,8 +145,8 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  * measurement hook of the benchmark). enable != 0 starts recording; fc_chol_profile_read waits for
  * the stream and returns, per launch kind, the summed milliseconds and the launch count (arrays of
  * `kinds` entries, 24 covers all), then clears them. Kinds: 0 front assembly, 1 panel (factor,
- * invert and solve below a diagonal block), 3 GEMM of the factor; 19 GEMM, 20 front assembly,
- * 21 gather, 22 forward panel, 23 backward panel of the solve. */
+ * invert and solve below a diagonal block), 3 GEMM of the factor; 18 reduction of split sums, 19 GEMM,
+ * 20 front assembly, 21 gather, 22 forward panel, 23 backward panel of the solve. */
 int fc_chol_profile(fc_chol *h, int enable);
 int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kinds);
 

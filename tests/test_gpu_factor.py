@@ -159,3 +159,33 @@ def test_lognormal_block_residual(cuda, n_el):
         assert np.linalg.norm(x[:, j] - exp[:, j]) <= SOLVE_TOL * np.linalg.norm(exp[:, j])
         r = oracle.spmv(p.n, p.csr.ptr, p.csr.idx, p.csr.val, x[:, j]) - p.rhs[:, j]
         assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(p.rhs[:, j])
+
+
+def test_batch_of_uneven_systems(cuda):
+    # independent boxes of uneven sizes factored and solved together in one handle; each
+    # system's solution matches the oracle's, and a singular system is reported as its own
+    from fieldcraft_b200.batch import BatchFactor
+    boxes = list(problems.uneven_boxes(count=6, lo=2, hi=7, nrhs=3, seed=5))
+    parts = [b.upper() for b in boxes]
+    bf = BatchFactor(parts, 2**62)
+    bf.factor([p.val for p in parts])
+    xs = bf.solve([b.rhs for b in boxes])
+    for b, x in zip(boxes, xs):
+        _, ref = oracle_factor(b.csr)
+        exp = ref.solve(b.rhs.copy())
+        assert np.linalg.norm(x - exp) <= SOLVE_TOL * np.linalg.norm(exp)
+    # a box held nowhere is singular: the batch names the system and its own column, the column
+    # a factorisation of that box alone names
+    i, j, k = problems.node_grid(3, 2, 2)
+    free = problems.box(3, 2, 2, 3.0, 2.0, 2.0, 1000.0, 0.3, np.zeros(i.size, bool))
+    alone = None
+    try:
+        Factor.new(free.upper(), 2**62)
+    except NotPositiveDefinite as e:
+        alone = e.column
+    assert alone is not None
+    parts2 = [parts[0], free.upper(), parts[1]]
+    bf2 = BatchFactor(parts2, 2**62)
+    with pytest.raises(NotPositiveDefinite) as e:
+        bf2.factor([p.val for p in parts2])
+    assert e.value.system == 1 and e.value.column == alone
