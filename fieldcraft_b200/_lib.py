@@ -48,6 +48,7 @@ SIGNATURES = {
     "fc_chol_solve_device_noalloc": (i32, [P, P, i32, i64, C.POINTER(Status)]),
     "fc_chol_values": (i32, [P, P, C.POINTER(Status)]),
     "fc_chol_stat": (i64, [P, i32]),
+    "fc_chol_refine_solve_device": (i32, [P, P, P, P, P, P, i32, i64, f64, i32, P, P, C.POINTER(Status)]),
     "fc_chol_profile": (i32, [P, i32]),
     "fc_chol_profile_read": (i32, [P, P, P, i32]),
     "fc_csr_spmv_device": (i32, [i64, P, P, P, P, P, i32, i64, P]),

@@ -254,6 +254,25 @@ class Factor:
                                          C.byref(st))
         raise_for(st)
 
+    def refine_solve_device(self, csr_device, b, x, nrhs: int, ld: int, tol: float = 1e-10, max_iter: int = 20):
+        """Iterative refinement in FP64 around this factor (the mixed-precision mode's FP32 factor or
+        the FP64 one): solves A x = b to ||b - A x|| <= tol ||b|| per right-hand side. csr_device =
+        (ptr, idx, val) CUDA tensors of A by rows; b, x CUDA tensors, column-major n x nrhs with
+        leading dimension ld. Returns (relative residuals, iterations); raises Timeout if max_iter
+        solves were not enough."""
+        ptr, idx, val = csr_device
+        rel = np.zeros(nrhs)
+        it = C.c_int32(0)
+        st = Status()
+        _lib.load().fc_chol_refine_solve_device(self.handle, C.c_void_p(ptr.data_ptr()), C.c_void_p(idx.data_ptr()),
+                                                C.c_void_p(val.data_ptr()), C.c_void_p(b.data_ptr()),
+                                                C.c_void_p(x.data_ptr()), int(nrhs), int(ld), float(tol),
+                                                int(max_iter), _lib.ptr(rel), C.byref(it), C.byref(st))
+        if st.code == FC_TIMEOUT:
+            raise Timeout(f"{st.message.decode()} after {it.value} solves, residuals {rel}")
+        raise_for(st)
+        return rel, it.value
+
     def values(self) -> np.ndarray:
         """The factor in the reference's layout: per supernode its lower trapezoid by columns."""
         out = np.empty(self.entries(), np.float64)

@@ -8,6 +8,7 @@
 // the reference's left-looking order (the same numbers up to rounding).
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdlib>
 #include <map>
 #include <cstdio>
@@ -98,6 +99,8 @@ struct Launch {
 
 struct fc_chol {
   int device = 0, precision = FC_PRECISION_FP64;
+  bool fp32 = false;   // L and the update matrices in FP32 (the mixed-precision factorisation)
+  size_t esize = 8;    // bytes of an entry of L / U
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int64_t n = 0, ns = 0, entries = 0, nnz = 0, levels = 0;
@@ -113,6 +116,8 @@ struct fc_chol {
   // device
   DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
   DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_D, d_perm, d_val, d_status, d_toff, d_doff;
+  DeviceBuf d_a_row, d_a_col, d_scale;   // mixed precision only
+  DeviceBuf d_ir_r, d_ir_d, d_ir_sum;    // iterative refinement workspace
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
   fc::Tree tree{};
   std::vector<Launch> program;
@@ -195,6 +200,11 @@ int32_t child_ranges(const fc_chol *h, int64_t s, int lo, int hi, std::vector<in
   return at;
 }
 
+// The address of entry `off` of the L or U arena (entries of h->esize bytes).
+void *arena_at(const DeviceBuf &buf, const fc_chol *h, int64_t off) {
+  return static_cast<char *>(buf.p) + (size_t)off * h->esize;
+}
+
 // Useful flops of a GEMM task (a diagonal tile computes its lower triangle only).
 double task_flops(const fc::GemmTask &g) {
   double outputs = (double)g.M * g.N;
@@ -261,8 +271,8 @@ int64_t arena_offsets(const fc_chol *h, const std::vector<std::vector<int64_t>> 
 // panel, then the update of the later columns; then the update matrices.
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
                  std::vector<int2> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
-  double *L = h->d_L.as<double>();
-  double *U = h->d_U.as<double>();
+  auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
+  auto Up = [&](int64_t off) { return arena_at(h->d_U, h, off); };
   const int NB = fc::NB;
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
@@ -290,13 +300,13 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         if (c1 >= m) panel_t.push_back({(int32_t)s, c0, c1, m, m, 1, doff});
         for (int r0 = c1; r0 < m; r0 += fc::PANEL_ROWS)
           panel_t.push_back({(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff});
-        double *Ls = L + h->loff[s];
+        const int64_t lo = h->loff[s];
         for (int jc = c1; jc < w; jc += fc::GEMM_TN)
           for (int ic = jc; ic < m; ic += fc::GEMM_TM) {
             fc::GemmTask g{};
-            g.C = Ls + ic + (int64_t)jc * m;
-            g.A = Ls + ic + (int64_t)c0 * m;
-            g.B = Ls + jc + (int64_t)c0 * m;
+            g.C = Lp(lo + ic + (int64_t)jc * m);
+            g.A = Lp(lo + ic + (int64_t)c0 * m);
+            g.B = Lp(lo + jc + (int64_t)c0 * m);
             g.c_si = 1, g.c_sj = m, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
             g.M = std::min(fc::GEMM_TM, m - ic);
             g.N = std::min(fc::GEMM_TN, w - jc);
@@ -312,14 +322,13 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
       if (u <= 0) continue;
-      const double *Ls = L + h->loff[s];
-      double *Us = U + h->uoff[s];
+      const int64_t lo = h->loff[s], uo = h->uoff[s];
       for (int bj = 0; bj < u; bj += fc::GEMM_TN)
         for (int bi = bj; bi < u; bi += fc::GEMM_TM) {
           fc::GemmTask g{};
-          g.C = Us + bi + (int64_t)bj * u;
-          g.A = Ls + w + bi;
-          g.B = Ls + w + bj;
+          g.C = Up(uo + bi + (int64_t)bj * u);
+          g.A = Lp(lo + w + bi);
+          g.B = Lp(lo + w + bj);
           g.c_si = 1, g.c_sj = u, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
           g.M = std::min(fc::GEMM_TM, u - bi);
           g.N = std::min(fc::GEMM_TN, u - bj);
@@ -348,6 +357,8 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   h->n = n;
   h->ns = ns;
   h->entries = sym.entries;
+  h->fp32 = h->precision == FC_PRECISION_FP32_IR;
+  h->esize = h->fp32 ? sizeof(float) : sizeof(double);
   h->nnz = (int64_t)sym.upper_idx.size();
   h->first = sym.first;
   h->perm = sym.perm;
@@ -473,9 +484,19 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   UP(h->d_perm, h->perm);
   UP(h->d_toff, h->toff);
   UP(h->d_doff, h->doff);
+  if (h->fp32) {
+    std::vector<int32_t> a_row(h->nnz), a_col(h->nnz);
+    for (int64_t q = 0; q < h->nnz; ++q) {
+      a_row[q] = sym.crow[a_src[q]];
+      a_col[q] = sym.ccol[a_src[q]];
+    }
+    UP(h->d_a_row, a_row);
+    UP(h->d_a_col, a_col);
+  }
 #undef UP
-  if (h->d_L.alloc(sizeof(double) * (size_t)std::max<int64_t>(lsum, 1)) != cudaSuccess ||
-      h->d_U.alloc(sizeof(double) * (size_t)std::max<int64_t>(usum, 1)) != cudaSuccess ||
+  if (h->d_L.alloc(h->esize * (size_t)std::max<int64_t>(lsum, 1)) != cudaSuccess ||
+      h->d_U.alloc(h->esize * (size_t)std::max<int64_t>(usum, 1)) != cudaSuccess ||
+      (h->fp32 && h->d_scale.alloc(sizeof(double) * (size_t)std::max<int64_t>(n, 1)) != cudaSuccess) ||
       h->d_D.alloc(sizeof(double) * (size_t)std::max<int64_t>(dsum, 1)) != cudaSuccess ||
       h->d_val.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->nnz, 1)) != cudaSuccess ||
       h->d_status.alloc(sizeof(fc::DeviceStatus)) != cudaSuccess) {
@@ -502,8 +523,11 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   t.a_dst = h->d_a_dst.as<int64_t>();
   t.diag_src = h->d_diag_src.as<int64_t>();
   t.doff = h->d_doff.as<int64_t>();
-  t.L = h->d_L.as<double>();
-  t.U = h->d_U.as<double>();
+  t.a_row = h->d_a_row.as<int32_t>();
+  t.a_col = h->d_a_col.as<int32_t>();
+  t.scale = h->fp32 ? h->d_scale.as<double>() : nullptr;
+  t.L = h->d_L.p;
+  t.U = h->d_U.p;
   t.D = h->d_D.as<double>();
   std::vector<fc::AssembleTask> asm_t;
   std::vector<int2> ranges;
@@ -619,6 +643,8 @@ int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *canc
 int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
   cudaStream_t st = h->stream;
   cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), st);
+  if (h->fp32) fc::launch_scale(h->n, h->d_diag_src.as<int64_t>(), d_val, h->d_scale.as<double>(), st);
+  const fc::GemmKind gk = h->fp32 ? fc::GemmKind::F32_TF32X3 : fc::GemmKind::F64;
   const fc::Tree &t = h->tree;
   int last_level = -1;
   int64_t launches = 0;
@@ -633,13 +659,14 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
     Mark mark(h, l.kind);
     switch (l.kind) {
       case K_ASSEMBLE:
-        fc::launch_assemble(t, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, h->d_ranges.as<int2>(), l.count, st);
+        fc::launch_assemble(t, h->fp32, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, h->d_ranges.as<int2>(), l.count,
+                            st);
         break;
       case K_PANEL:
-        fc::launch_panel(t, d_val, h->d_panel.as<fc::PanelTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(),
-                         l.width, st);
+        fc::launch_panel(t, h->fp32, d_val, h->d_panel.as<fc::PanelTask>() + l.off, l.count,
+                         h->d_status.as<fc::DeviceStatus>(), l.width, st);
         break;
-      case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, st); break;
+      case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, gk, st); break;
     }
     ++launches;
   }
@@ -711,7 +738,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
   std::vector<fc::SolveTask> &panels = p.panels;
   std::vector<fc::GemmTask> &gemm = p.gemm;
   std::vector<Launch> &fwd = p.fwd, &bwd = p.bwd;
-  double *L = h->d_L.as<double>();
+  auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
   // forward
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
@@ -766,7 +793,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
       if (u <= 0) continue;
-      const double *Ls = L + h->loff[s];
+      const int64_t lo = h->loff[s];
       const bool split = u > 2 * fc::SPLIT_K;
       const int chunks = split ? (u + fc::SPLIT_K - 1) / fc::SPLIT_K : 1;
       for (int i0 = 0; i0 < w; i0 += fc::GEMM_TM)
@@ -784,7 +811,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
               g.C = tile;
               g.c_si = R, g.c_sj = 1;
             }
-            g.A = Ls + w + k0 + (int64_t)i0 * m;
+            g.A = Lp(lo + w + k0 + (int64_t)i0 * m);
             g.a_si = m, g.a_sk = 1;
             g.B = v + voff[s] + (int64_t)k0 * R + j0;
             g.b_sj = 1, g.b_sk = R;
@@ -883,12 +910,14 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         break;
       case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_FWD:
-        fc::launch_solve_panel(t, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
+        fc::launch_solve_panel(t, h->fp32, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
         break;
       case K_SOLVE_BWD:
-        fc::launch_solve_panel(t, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
+        fc::launch_solve_panel(t, h->fp32, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
         break;
-      case K_GEMM: fc::launch_gemm(b.gemm + l.off, l.count, st); break;
+      case K_GEMM:
+        fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
+        break;
       case K_REDUCE: fc::launch_reduce(b.reduce + l.off, l.count, st); break;
     }
     ++launches;
@@ -927,10 +956,10 @@ int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
 void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   int64_t launches = 0;
   const SolveBuffers b = own_buffers(h);
-  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->stream);
+  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
   run_solve_program(h, h->fwd, b, R, launches);
   run_solve_program(h, h->bwd, b, R, launches);
-  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->stream);
+  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->tree.scale, h->stream);
   h->last_solve_launches = launches + 2;
 }
 
@@ -1301,13 +1330,88 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
                        reinterpret_cast<const fc::GemmTask *>(base + at_gemm),
                        reinterpret_cast<const fc::ReduceTask *>(base + at_reduce)};
   int64_t launches = 0;
-  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, b.x, R, h->stream);
+  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, b.x, R, h->tree.scale, h->stream);
   run_solve_program(h, p.fwd, b, R, launches);
   run_solve_program(h, p.bwd, b, R, launches);
-  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, b.x, R, d_b, ld, h->stream);
+  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, b.x, R, d_b, ld, h->tree.scale, h->stream);
   e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(status, e, "solve");
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val,
+                                const double *d_b, double *d_x, int32_t nrhs, int64_t ld, double tol, int32_t max_iter,
+                                double *relres, int32_t *iterations, fc_status *status) {
+  if (iterations) *iterations = 0;
+  if (!h || nrhs < 0 || max_iter < 1 || (nrhs > 0 && (!d_b || !d_x || ld < h->n || !d_ptr || !d_idx || !d_val))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
+    return FC_INVALID_ARGUMENT;
+  }
+  if (nrhs == 0 || h->n == 0) {
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  const int R = nrhs;
+  const int64_t n = h->n;
+  const size_t block = sizeof(double) * (size_t)n * R;
+  if ((h->d_ir_r.bytes < block && h->d_ir_r.alloc(block) != cudaSuccess) ||
+      (h->d_ir_d.bytes < block && h->d_ir_d.alloc(block) != cudaSuccess) ||
+      (h->d_ir_sum.bytes < 2 * sizeof(double) * R && h->d_ir_sum.alloc(2 * sizeof(double) * R) != cudaSuccess)) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the refinement");
+    return FC_OUT_OF_MEMORY;
+  }
+  cudaStream_t st = h->stream;
+  double *r = h->d_ir_r.as<double>(), *d = h->d_ir_d.as<double>(), *sums = h->d_ir_sum.as<double>();
+  std::vector<double> host(2 * R), rel(R, 0.0);
+  cudaError_t e = cudaSuccess;
+  // x = 0, r = b
+  for (int j = 0; j < R && e == cudaSuccess; ++j) {
+    e = cudaMemsetAsync(d_x + (int64_t)j * ld, 0, sizeof(double) * n, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(r + (int64_t)j * n, d_b + (int64_t)j * ld, sizeof(double) * n, cudaMemcpyDeviceToDevice, st);
+  }
+  if (e != cudaSuccess) return cuda_fail(status, e, "refinement set-up");
+  fc::launch_sumsq(n, R, n, r, sums + R, st);
+  int it = 0;
+  bool done = false;
+  while (it < max_iter) {
+    e = cudaMemcpyAsync(d, r, block, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
+    int rc = enqueue_solve(h, d, R, n, status);
+    if (rc != FC_OK) return rc;
+    ++it;
+    for (int j = 0; j < R; ++j) fc::launch_update(n, 1, ld, d + (int64_t)j * n, d_x + (int64_t)j * ld, st);
+    for (int j = 0; j < R; ++j) {
+      fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x + (int64_t)j * ld, r + (int64_t)j * n, 1, n, st);
+      fc::launch_residual(n, 1, n, d_b + (int64_t)j * ld, r + (int64_t)j * n, st);
+    }
+    fc::launch_sumsq(n, R, n, r, sums, st);
+    e = cudaMemcpyAsync(host.data(), sums, 2 * sizeof(double) * R, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
+    double worst = 0.0;
+    for (int j = 0; j < R; ++j) {
+      const double bb = host[R + j];
+      rel[j] = bb > 0.0 ? std::sqrt(host[j] / bb) : std::sqrt(host[j]);
+      worst = std::max(worst, rel[j]);
+    }
+    if (!(worst > tol)) {
+      done = worst == worst;  // NaN never converges
+      if (done) break;
+    }
+  }
+  if (relres)
+    for (int j = 0; j < R; ++j) relres[j] = rel[j];
+  if (iterations) *iterations = it;
+  if (!done) {
+    set_status(status, FC_TIMEOUT, -1, 0, 0, "the refinement did not reach the tolerance");
+    return FC_TIMEOUT;
+  }
   set_status(status, FC_OK);
   return FC_OK;
 }
@@ -1358,7 +1462,7 @@ int fc_chol_values(fc_chol *h, double *dst, fc_status *status) {
     set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the copy");
     return FC_OUT_OF_MEMORY;
   }
-  fc::launch_pack_trapezoids(h->tree, h->ns, h->d_toff.as<int64_t>(), tmp.as<double>(), h->stream);
+  fc::launch_pack_trapezoids(h->tree, h->fp32, h->ns, h->d_toff.as<int64_t>(), tmp.as<double>(), h->stream);
   cudaError_t e = cudaMemcpyAsync(dst, tmp.p, sizeof(double) * h->entries, cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return cuda_fail(status, e, "values");

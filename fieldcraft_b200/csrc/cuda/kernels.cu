@@ -1,6 +1,10 @@
-// Kernels of the supernodal Cholesky on B200 (sm_100a). FP64 throughout: the dense updates run
-// on the FP64 tensor pipe (DMMA, mma.sync m8n8k4 .f64 — Blackwell's tcgen05 has no FP64 kind),
-// operands staged through shared memory by cp.async; the rest is SIMT.
+// Kernels of the supernodal Cholesky on B200 (sm_100a).
+//
+// Storage of L and of the update matrices is FP64, or FP32 for the mixed-precision factorisation;
+// the diagonal blocks, their inverses, the solve's vectors and every triangular solve stay FP64.
+// FP64 updates run on the FP64 tensor pipe (DMMA, mma.sync .f64 — tcgen05 has no FP64 kind); FP32
+// updates run as 3xTF32 split products on the tensor pipe with FP32 accumulation. Operands are
+// staged through shared memory by cp.async; the rest is SIMT.
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -14,22 +18,12 @@ namespace {
 
 constexpr double PIVOT_TOLERANCE = 1e-10;  // crates/solver/src/cholesky.rs:48
 
-__device__ __forceinline__ int lower_bound_i32(const int32_t *a, int n, int key) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (a[mid] < key)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(src_bytes));
 }
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) { cp_async<8>(smem, gmem, src_bytes); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -44,32 +38,63 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// D = A B + C on one 16x8x8 FP64 tile (sm_90 and later): a = A[g][tg], A[g+8][tg], A[g][tg+4],
+// A[g+8][tg+4]; b = B[tg][g], B[tg+4][g]; c/d = C[g][2tg], C[g][2tg+1], C[g+8][2tg], C[g+8][2tg+1].
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// The same 16x8x8 shape on TF32 operands with FP32 accumulation (the fragments' positions are
+// those of dmma16).
+__device__ __forceinline__ void tmma16(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// x = hi + lo with hi = x rounded to TF32 and lo = (x - hi) rounded to TF32: three products of
+// such halves (hi hi + hi lo + lo hi) keep FP32 accuracy (the 3xTF32 split).
+__device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(hi) : "f"(x));
+  const float rest = x - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(lo) : "f"(rest));
+}
+
 // ---- front assembly ----------------------------------------------------------------------------
 // Columns [j0, j1) of supernode s's front, then each child's update matrix added in child order
 // (the multifrontal form of the reference's own(rel(i), rel(c)) -= S(i, c), cholesky.rs:636-686,
 // summed child by child). Columns of the L panel (j < w) are zeroed and take A's entries first,
 // before the panel is factored; columns of the update matrix (j >= w) are assembled after its
-// GEMM stored -L21 L21^T there.
+// GEMM stored -L21 L21^T there. With a scale (the mixed-precision factorisation) the entries
+// placed are those of S A S, S = diag(A)^-1/2.
+template <class T>
 __global__ void __launch_bounds__(ASSEMBLE_THREADS) assemble_kernel(Tree t, const double *__restrict__ val,
-                                                       const AssembleTask *__restrict__ tasks,
-                                                       const int2 *__restrict__ ranges) {
+                                                                    const AssembleTask *__restrict__ tasks,
+                                                                    const int2 *__restrict__ ranges) {
   const AssembleTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], w = t.width[s], u = m - w, f = t.first[s];
-  double *Ls = t.L + t.loff[s];
-  double *Us = t.U + t.uoff[s];
+  T *L = static_cast<T *>(t.L), *U = static_cast<T *>(t.U);
+  T *Ls = L + t.loff[s];
+  T *Us = U + t.uoff[s];
   const int j0 = task.j0, j1 = task.j1;
   const int tid = threadIdx.x;
-  // the L panel's columns start from zero; the update matrix's were stored by its GEMM already
   for (int j = j0; j < j1 && j < w; ++j) {
-    double *col = Ls + (int64_t)j * m;
-    for (int64_t i = tid; i < m; i += blockDim.x) col[i] = 0.0;
+    T *col = Ls + (int64_t)j * m;
+    for (int64_t i = tid; i < m; i += blockDim.x) col[i] = T(0);
   }
   __syncthreads();
   const int jend = j1 < w ? j1 : (int)w;
   if (j0 < jend) {
     const int64_t e0 = t.a_ptr[f + j0], e1 = t.a_ptr[f + jend];
-    for (int64_t e = e0 + tid; e < e1; e += blockDim.x) t.L[t.a_dst[e]] = val[t.a_src[e]];
+    if (t.scale) {
+      for (int64_t e = e0 + tid; e < e1; e += blockDim.x)
+        L[t.a_dst[e]] = T(val[t.a_src[e]] * t.scale[t.a_row[e]] * t.scale[t.a_col[e]]);
+    } else {
+      for (int64_t e = e0 + tid; e < e1; e += blockDim.x) L[t.a_dst[e]] = T(val[t.a_src[e]]);
+    }
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
@@ -78,18 +103,18 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS) assemble_kernel(Tree t, cons
     const int c = t.kids[kp];
     const int uc = t.height[c] - t.width[c];
     const int32_t *rel = t.rel + t.rel_off[c];
-    const double *Uc = t.U + t.uoff[c];
+    const T *Uc = U + t.uoff[c];
     const int2 range = ranges[task.ranges + (kp - k0)];
     const int lo = range.x, hi = range.y;
     for (int jc = lo + warp; jc < hi; jc += nwarps) {
       const int64_t J = rel[jc];
-      const double *src = Uc + (int64_t)jc * uc;
-      double *dst = J < w ? Ls + J * m : Us + (J - w) * u - w;
+      const T *src = Uc + (int64_t)jc * uc;
+      T *dst = J < w ? Ls + J * m : Us + (J - w) * u - w;
       // four rows a lane in flight: the loads of a batch are issued before its stores
       int ic = jc + lane;
       for (; ic + 96 < uc; ic += 128) {
         int r[4];
-        double v[4], d[4];
+        T v[4], d[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           r[q] = rel[ic + 32 * q];
@@ -106,42 +131,61 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS) assemble_kernel(Tree t, cons
   }
 }
 
+// S = diag(A)^-1/2 over the postordered columns (the mixed-precision factorisation's scaling).
+__global__ void scale_kernel(int64_t n, const int64_t *__restrict__ diag_src, const double *__restrict__ val,
+                             double *__restrict__ scale) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t ds = diag_src[j];
+  const double d = ds >= 0 ? fabs(val[ds]) : 0.0;
+  scale[j] = d > 0.0 ? 1.0 / sqrt(d) : 1.0;
+}
+
 // ---- shared-memory tiles and the DMMA product of two of them --------------------------------------
-// A tile holds 64 x 64 doubles as [k][i] with row stride TS (padded so a warp's fragment reads
-// of 4 k-rows x 8 consecutive doubles fall in distinct banks).
+// A tile holds 64 x 64 elements as [k][i] with a padded row stride: 68 doubles or 72 floats, so a
+// warp's fragment reads of 4 k-rows x 8 consecutive elements fall in distinct banks.
+template <class T>
+__host__ __device__ constexpr int tile_stride() {
+  return sizeof(T) == 8 ? 68 : 72;
+}
 constexpr int TS = 68;
 
-// dst[k * TS + i] = src[i * si + k * sk] for i < rows, k < kk, zero for the other i < 64 and
+// dst[k * S + i] = src[i * si + k * sk] for i < rows, k < kk, zero for the other i < 64 and
 // kk <= k < kpad (rows k >= kpad of the tile are not touched). Issued as cp.async copies, so a
 // tile's loads are all in flight at once; the caller commits, waits and synchronises. One warp per
 // k (rows contiguous in memory) or one warp per i (k contiguous): every warp reads a contiguous run.
-__device__ __forceinline__ void load_tile(double *dst, const double *__restrict__ src, int64_t si, int64_t sk, int rows,
-                                          int kk, int kpad) {
+template <class T>
+__device__ __forceinline__ void load_tile(T *dst, const T *__restrict__ src, int64_t si, int64_t sk, int rows, int kk,
+                                          int kpad) {
+  constexpr int S = tile_stride<T>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (si == 1) {
     for (int k = warp; k < kpad; k += nw)
       for (int i = lane; i < 64; i += 32) {
         const bool ok = i < rows && k < kk;
-        cp_async8(&dst[k * TS + i], ok ? src + i + (int64_t)k * sk : src, ok ? 8 : 0);
+        cp_async<sizeof(T)>(&dst[k * S + i], ok ? src + i + (int64_t)k * sk : src, ok ? (int)sizeof(T) : 0);
       }
   } else {
     for (int i = warp; i < 64; i += nw)
       for (int k = lane; k < kpad; k += 32) {
         const bool ok = i < rows && k < kk;
-        cp_async8(&dst[k * TS + i], ok ? src + (int64_t)i * si + k * sk : src, ok ? 8 : 0);
+        cp_async<sizeof(T)>(&dst[k * S + i], ok ? src + (int64_t)i * si + k * sk : src, ok ? (int)sizeof(T) : 0);
       }
   }
 }
 
-// acc(i, j) += sum_{k < K} As[k][i] Bs[k][j] over a 64 x 64 output, 4 warps of 32 x 32.
-__device__ __forceinline__ void mma_tiles(const double *As, const double *Bs, int K, double (&acc)[4][4][2]) {
+// acc(i, j) += sum_{k < K} As[k][i] Bs[k][j] over a 64 x 64 output, 4 warps of 32 x 32, in FP64
+// (an FP32 A tile is widened as it is read).
+template <class TA>
+__device__ __forceinline__ void mma_tiles(const TA *As, const double *Bs, int K, double (&acc)[4][4][2]) {
+  constexpr int SA = tile_stride<TA>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, tg = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   for (int kk = 0; kk < K; kk += 4) {
     double av[4], bv[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) av[r] = As[(kk + tg) * TS + wm + r * 8 + g];
+    for (int r = 0; r < 4; ++r) av[r] = (double)As[(kk + tg) * SA + wm + r * 8 + g];
 #pragma unroll
     for (int c = 0; c < 4; ++c) bv[c] = Bs[(kk + tg) * TS + wn + c * 8 + g];
 #pragma unroll
@@ -173,30 +217,36 @@ __device__ __forceinline__ void each_acc(const double (&acc)[4][4][2], F f) {
 }
 
 // ---- panel: factor the diagonal block, invert it, solve the rows below --------------------------
-// The block (pw <= 64 columns) is factored right-looking in shared memory; the pivot test is the
-// reference's (cholesky.rs:1162-1165): not (d > PIVOT_TOLERANCE |A_jj|) or not finite fails, and
-// the smallest failing column (postorder) is kept in the status word. A failed pivot makes NaNs
-// and nothing else: no index depends on a value. The inverse comes from 8 x 8 diagonal blocks and
-// block forward substitution; the rows below are X = B L^-T on the FP64 tensor pipe.
+// The block (pw <= 64 columns) is factored in FP64 in shared memory by strips of 8 columns; the
+// pivot test is the reference's (cholesky.rs:1162-1165): not (d > PIVOT_TOLERANCE |A_jj|) or not
+// finite fails, and the smallest failing column (postorder) is kept in the status word. A failed
+// pivot makes NaNs and nothing else: no index depends on a value. The inverse comes from 8 x 8
+// diagonal blocks and block forward substitution; the rows below are X = B L^-T on the FP64
+// tensor pipe. L may be stored in FP32 (widened on load, rounded on store); the diagonal arena
+// stays FP64.
 constexpr int PANEL_THREADS = 128;
 // Shared memory of a panel launch whose widest panel is padded to p8 columns (a multiple of 8).
-__host__ __device__ constexpr size_t panel_smem(int p8) { return sizeof(double) * (p8 * (65 + 2 * TS) + 512 + 128); }
+template <class T>
+__host__ __device__ constexpr size_t panel_smem(int p8) {
+  return sizeof(double) * (p8 * (65 + TS) + 512 + 128) + sizeof(T) * p8 * tile_stride<T>();
+}
 
+template <class T>
 __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const double *__restrict__ val,
                                                               const PanelTask *__restrict__ tasks,
                                                               DeviceStatus *status, int p8max) {
   extern __shared__ double sm[];
   double *a = sm;                   // factor, column-major, ld 65 (p8max columns)
   double *inv = a + p8max * 65;     // inv[k * TS + i] = Linv(i, k) (p8max rows)
-  double *bt = inv + p8max * TS;    // rows below: bt[k * TS + r] = L(r0 + r, c0 + k)
-  double *tt = bt + p8max * TS;     // 8 x (8 x 8) scratch of the inversion
-  double *dg = tt + 512;          // the matrix's own diagonal entries of the panel's columns
-  double *dv = dg + 64;           // the pivots
+  double *tt = inv + p8max * TS;    // 8 x (8 x 8) scratch of the inversion
+  double *dg = tt + 512;            // the matrix's own diagonal entries of the panel's columns
+  double *dv = dg + 64;             // the pivots' reciprocals
+  T *bt = reinterpret_cast<T *>(dv + 64);  // rows below: bt[k * S + r] = L(r0 + r, c0 + k)
   __shared__ int fail;
   const PanelTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], f = t.first[s];
-  double *Ls = t.L + t.loff[s];
+  T *Ls = static_cast<T *>(t.L) + t.loff[s];
   const int c0 = task.c0, pw = task.c1 - task.c0, rows = task.r1 - task.r0;
   const int nb8 = (pw + 7) >> 3, P8 = 8 * nb8, K4 = (pw + 3) & ~3;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -205,17 +255,22 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
   // leading pw x pw inverse)
   for (int c = warp; c < P8; c += PANEL_THREADS / 32)
     for (int r = lane; r < P8; r += 32) {
-      if (r < pw && c < pw && r >= c)
-        cp_async8(&a[c * 65 + r], Ls + (c0 + r) + (int64_t)(c0 + c) * m, 8);
-      else
+      if (r < pw && c < pw && r >= c) {
+        if (sizeof(T) == 8)
+          cp_async8(&a[c * 65 + r], Ls + (c0 + r) + (int64_t)(c0 + c) * m, 8);
+        else
+          a[c * 65 + r] = (double)Ls[(c0 + r) + (int64_t)(c0 + c) * m];
+      } else {
         a[c * 65 + r] = (r >= pw || c >= pw) && r == c ? 1.0 : 0.0;
+      }
     }
   for (int c = tid; c < pw; c += PANEL_THREADS) {
-    const int64_t ds = t.diag_src[f + c0 + c];
-    dg[c] = ds >= 0 ? val[ds] : 0.0;
+    const int64_t j = f + c0 + c, ds = t.diag_src[j];
+    const double d = ds >= 0 ? val[ds] : 0.0;
+    dg[c] = t.scale ? d * t.scale[j] * t.scale[j] : d;
   }
   for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
-  if (rows > 0) load_tile(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);
+  if (rows > 0) load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
@@ -326,71 +381,93 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
   if (rows > 0) {
     double acc[4][4][2];
     zero_acc(acc);
-    mma_tiles(bt, inv, K4, acc);
-    double *dst = Ls + task.r0 + (int64_t)c0 * m;
+    mma_tiles<T>(bt, inv, K4, acc);
+    T *dst = Ls + task.r0 + (int64_t)c0 * m;
     each_acc(acc, [&](int i, int c, double v) {
-      if (i < rows && c < pw) dst[i + (int64_t)c * m] = v;
+      if (i < rows && c < pw) dst[i + (int64_t)c * m] = T(v);
     });
   }
 }
 
 // ---- tiled C -= A B^T on the FP64 tensor pipe ---------------------------------------------------
-// 64 x 64 tile per CTA, 4 warps of 32 x 32 (4 x 4 DMMA tiles), K in chunks of 16 through a
+// 64 x 64 tile per CTA, 4 warps of 32 x 32 (2 x 4 DMMA 16x8x8 tiles), K in chunks of 16 through a
 // three-stage cp.async pipeline in shared memory (rows padded to 68 doubles so a warp's fragment
-// reads of 4 k-rows x 8 consecutive doubles fall in distinct banks). Four CTAs fit an SM.
+// reads of 4 k-rows x 8 consecutive doubles fall in distinct banks). Four CTAs fit an SM. An FP32
+// A operand (the solve's L21^T v on an FP32 factor) is staged as FP32 and widened when read.
 constexpr int SROW = 68;
 constexpr int GEMM_STAGES = 3;
-constexpr size_t GEMM_SMEM = sizeof(double) * GEMM_STAGES * 2 * GEMM_KC * SROW;
+template <class TA>
+__host__ __device__ constexpr size_t gemm_smem() {
+  return GEMM_STAGES * GEMM_KC * (sizeof(TA) * tile_stride<TA>() + sizeof(double) * SROW);
+}
 
-// This thread's 8 elements of a 64 x 16 operand tile: a fixed row and k = k0 + 2q when the rows
-// are contiguous in memory (si == 1), else a fixed k and row i0 + 8q (k contiguous).
+// This thread's elements of a 64 x KC operand tile: a fixed row and k = k0 + 2q when the rows
+// are contiguous in memory (si == 1), else a fixed k and row i0 + (128 / KC) q (k contiguous).
+template <class T, int KC>
 struct TileLoader {
-  const double *p;
+  static constexpr int PER = 64 * KC / GEMM_THREADS;  // elements per thread per stage
+  const T *p;
   int64_t dq, dstage;
   int i0, k0, di, dk, lim;
-  __device__ __forceinline__ void init(const double *base, int64_t si, int64_t sk, int rows, int tid) {
+  __device__ __forceinline__ void init(const T *base, int64_t si, int64_t sk, int rows, int tid) {
     if (si == 1) {
       i0 = tid & 63, k0 = tid >> 6, di = 0, dk = 2;
       p = base + i0 + (int64_t)k0 * sk;
       dq = 2 * sk;
-      dstage = GEMM_KC * sk;
+      dstage = KC * sk;
     } else {
-      i0 = tid >> 4, k0 = tid & 15, di = 8, dk = 0;
+      i0 = tid / KC, k0 = tid % KC, di = GEMM_THREADS / KC, dk = 0;
       p = base + (int64_t)i0 * si + k0;
-      dq = 8 * si;
-      dstage = GEMM_KC;
+      dq = (int64_t)(GEMM_THREADS / KC) * si;
+      dstage = KC;
     }
     lim = rows;
   }
-  __device__ __forceinline__ void load(double (*S)[SROW], int kbase, int K, const double *safe) {
+  template <int S>
+  __device__ __forceinline__ void load(T (*Sm)[S], int kbase, int K, const T *safe) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < PER; ++q) {
       const int i = i0 + q * di, k = k0 + q * dk;
       const bool ok = i < lim && kbase + k < K;
-      cp_async8(&S[k][i], ok ? p + q * dq : safe, ok ? 8 : 0);
+      cp_async<sizeof(T)>(&Sm[k][i], ok ? p + q * dq : safe, ok ? (int)sizeof(T) : 0);
     }
     p += dstage;
   }
 };
 
+// Stores one output of a GEMM task by its flags: a partial (flag 4), -sum (flag 2), or C - sum.
+template <class T, class V>
+__device__ __forceinline__ void gemm_out(T *dst, bool partial, bool store, V v) {
+  if (partial)
+    *dst = T(v);
+  else if (store)
+    *dst = T(-v);
+  else
+    *dst = T(*dst - v);
+}
+
+template <class TA>
 __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *__restrict__ tasks) {
+  constexpr int SA = tile_stride<TA>();
   extern __shared__ __align__(16) double gsm[];
-  double(*As)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm);
-  double(*Bs)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm + GEMM_STAGES * GEMM_KC * SROW);
+  double(*Bs)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm);
+  TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + GEMM_STAGES * GEMM_KC * SROW);
   const GemmTask *tp = tasks + blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tg = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   const int K = tp->K;
-  const double *abase = tp->A, *bbase = tp->B;
-  TileLoader la, lb;
+  const TA *abase = static_cast<const TA *>(tp->A);
+  const double *bbase = static_cast<const double *>(tp->B);
+  TileLoader<TA, GEMM_KC> la;
+  TileLoader<double, GEMM_KC> lb;
   la.init(abase, tp->a_si, tp->a_sk, tp->M, tid);
   lb.init(bbase, tp->b_sj, tp->b_sk, tp->N, tid);
-  double acc[4][4][2];
+  double acc[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.0;
   const int nk = (K + GEMM_KC - 1) / GEMM_KC;
 #pragma unroll
   for (int st = 0; st < GEMM_STAGES - 1; ++st) {
@@ -411,39 +488,128 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
     cp_async_commit();
     const int st = kt % GEMM_STAGES;
 #pragma unroll
-    for (int kk = 0; kk < GEMM_KC; kk += 4) {
-      double av[4], bv[4];
+    for (int kk = 0; kk < GEMM_KC; kk += 8) {
+      double av[2][4], bv[4][2];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) av[r] = As[st][kk + tg][wm + r * 8 + g];
+      for (int r = 0; r < 2; ++r) {
+        const int i = wm + r * 16 + g;
+        av[r][0] = (double)As[st][kk + tg][i];
+        av[r][1] = (double)As[st][kk + tg][i + 8];
+        av[r][2] = (double)As[st][kk + tg + 4][i];
+        av[r][3] = (double)As[st][kk + tg + 4][i + 8];
+      }
 #pragma unroll
-      for (int c = 0; c < 4; ++c) bv[c] = Bs[st][kk + tg][wn + c * 8 + g];
+      for (int c = 0; c < 4; ++c) {
+        bv[c][0] = Bs[st][kk + tg][wn + c * 8 + g];
+        bv[c][1] = Bs[st][kk + tg + 4][wn + c * 8 + g];
+      }
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) dmma(acc[r][c], av[r], bv[c]);
+        for (int c = 0; c < 4; ++c) dmma16(acc[r][c], av[r], bv[c]);
     }
   }
   cp_async_wait<0>();
   const int M = tp->M, N = tp->N;
   const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
-  double *C = tp->C;
+  double *C = static_cast<double *>(tp->C);
   const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+  for (int r = 0; r < 2; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int i = wm + r * 8 + g, j = wn + c * 8 + 2 * tg + e;
-        if (i < M && j < N && (!lower || i >= j)) {
-          double *dst = C + (int64_t)i * c_si + (int64_t)j * c_sj;
-          if (partial)
-            *dst = acc[r][c][e];
-          else if (store)
-            *dst = -acc[r][c][e];
-          else
-            *dst -= acc[r][c][e];
+      for (int e = 0; e < 4; ++e) {
+        const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
+        if (i < M && j < N && (!lower || i >= j))
+          gemm_out(C + (int64_t)i * c_si + (int64_t)j * c_sj, partial, store, acc[r][c][e]);
+      }
+}
+
+// ---- tiled C -= A B^T in FP32 by 3xTF32 on the tensor pipe ---------------------------------------
+// The FP32 factorisation's updates: the same 64 x 64 tiles and 32 x 32 warp tiles as gemm_kernel,
+// K in chunks of 32 floats; every operand x = hi + lo (TF32 halves) and each product is
+// hi*hi + hi*lo + lo*hi, accumulated in FP32.
+constexpr int FKC = 32, FS = 72;
+constexpr size_t GEMM_F32_SMEM = sizeof(float) * GEMM_STAGES * 2 * FKC * FS;
+
+__global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_tf32x3_kernel(const GemmTask *__restrict__ tasks) {
+  extern __shared__ __align__(16) float fsm[];
+  float(*As)[FKC][FS] = reinterpret_cast<float(*)[FKC][FS]>(fsm);
+  float(*Bs)[FKC][FS] = reinterpret_cast<float(*)[FKC][FS]>(fsm + GEMM_STAGES * FKC * FS);
+  const GemmTask *tp = tasks + blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int K = tp->K;
+  const float *abase = static_cast<const float *>(tp->A), *bbase = static_cast<const float *>(tp->B);
+  TileLoader<float, FKC> la, lb;
+  la.init(abase, tp->a_si, tp->a_sk, tp->M, tid);
+  lb.init(bbase, tp->b_sj, tp->b_sk, tp->N, tid);
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.f;
+  const int nk = (K + FKC - 1) / FKC;
+#pragma unroll
+  for (int st = 0; st < GEMM_STAGES - 1; ++st) {
+    if (st < nk) {
+      la.load(As[st], st * FKC, K, abase);
+      lb.load(Bs[st], st * FKC, K, bbase);
+    }
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<GEMM_STAGES - 2>();
+    __syncthreads();
+    const int pf = kt + GEMM_STAGES - 1;
+    if (pf < nk) {
+      la.load(As[pf % GEMM_STAGES], pf * FKC, K, abase);
+      lb.load(Bs[pf % GEMM_STAGES], pf * FKC, K, bbase);
+    }
+    cp_async_commit();
+    const int st = kt % GEMM_STAGES;
+#pragma unroll
+    for (int kk = 0; kk < FKC; kk += 8) {
+      uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int i = wm + r * 16 + g;
+        tf32_split(As[st][kk + tg][i], ah[r][0], al[r][0]);
+        tf32_split(As[st][kk + tg][i + 8], ah[r][1], al[r][1]);
+        tf32_split(As[st][kk + tg + 4][i], ah[r][2], al[r][2]);
+        tf32_split(As[st][kk + tg + 4][i + 8], ah[r][3], al[r][3]);
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        tf32_split(Bs[st][kk + tg][wn + c * 8 + g], bh[c][0], bl[c][0]);
+        tf32_split(Bs[st][kk + tg + 4][wn + c * 8 + g], bh[c][1], bl[c][1]);
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          tmma16(acc[r][c], al[r], bh[c]);
+          tmma16(acc[r][c], ah[r], bl[c]);
+          tmma16(acc[r][c], ah[r], bh[c]);
         }
+    }
+  }
+  cp_async_wait<0>();
+  const int M = tp->M, N = tp->N;
+  const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
+  float *C = static_cast<float *>(tp->C);
+  const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
+        if (i < M && j < N && (!lower || i >= j))
+          gemm_out(C + (int64_t)i * c_si + (int64_t)j * c_sj, partial, store, acc[r][c][e]);
       }
 }
 
@@ -468,7 +634,7 @@ __global__ void __launch_bounds__(256) solve_assemble_kernel(Tree t, double *__r
                                                              const int2 *__restrict__ ranges) {
   const RowTask task = tasks[blockIdx.x];
   const int s = task.s;
-  const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
+  const int64_t w = t.width[s], f = t.first[s];
   double *vs = v + voff[s];
   const int tid = threadIdx.x;
   const int64_t z0 = task.i0 > w ? task.i0 : w;
@@ -489,7 +655,6 @@ __global__ void __launch_bounds__(256) solve_assemble_kernel(Tree t, double *__r
     }
     __syncthreads();
   }
-  (void)m;
 }
 
 // v_s rows [i0, i1) <- x at the supernode's rows below its columns (final by the backward pass).
@@ -512,40 +677,44 @@ __global__ void __launch_bounds__(256) solve_gather_kernel(Tree t, const double 
 // block from the diagonal arena. Forward: y = Linv x_p (x -> x2), then the front rows [r0, r1)
 // below the panel -= L(rows, panel) y (own rows in x, rows past the columns in v). Backward:
 // z = Linv^T x2_p (x2 -> x), then the own rows [r0, r1) above -= L(panel, rows)^T z in x2.
-__host__ __device__ constexpr size_t solve_smem(int k4) { return sizeof(double) * 3 * k4 * TS; }
+template <class T>
+__host__ __device__ constexpr size_t solve_smem(int k4) {
+  return sizeof(double) * 2 * k4 * TS + sizeof(T) * k4 * tile_stride<T>();
+}
 
-template <bool BACKWARD>
+template <bool BACKWARD, class T>
 __global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__restrict__ x, double *__restrict__ x2,
                                                          double *__restrict__ v, const int64_t *__restrict__ voff, int R,
                                                          const SolveTask *__restrict__ tasks, int k4max) {
   extern __shared__ double sm[];
-  double *inv = sm, *xs = sm + k4max * TS, *bt = sm + 2 * k4max * TS;
+  double *inv = sm, *xs = sm + k4max * TS;
+  T *bt = reinterpret_cast<T *>(sm + 2 * k4max * TS);
   const SolveTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
-  const double *Ls = t.L + t.loff[s];
+  const T *Ls = static_cast<const T *>(t.L) + t.loff[s];
   const double *Li = t.D + task.doff + (int64_t)(task.c1 - task.c0) * (task.c1 - task.c0);
   const int c0 = task.c0, pw = task.c1 - task.c0, rows = task.r1 - task.r0, j0 = task.j0, nj = task.j1 - task.j0;
   double *src = BACKWARD ? x2 : x;
   double *out = BACKWARD ? x : x2;
   const int K4 = (pw + 3) & ~3;
   if (BACKWARD)
-    load_tile(inv, Li, pw, 1, pw, pw, K4);  // inv[k][i] = Linv(k, i)
+    load_tile<double>(inv, Li, pw, 1, pw, pw, K4);  // inv[k][i] = Linv(k, i)
   else
-    load_tile(inv, Li, 1, pw, pw, pw, K4);  // inv[k][i] = Linv(i, k)
-  load_tile(xs, src + (f + c0) * R + j0, 1, R, nj, pw, K4);
+    load_tile<double>(inv, Li, 1, pw, pw, pw, K4);  // inv[k][i] = Linv(i, k)
+  load_tile<double>(xs, src + (f + c0) * R + j0, 1, R, nj, pw, K4);
   if (rows > 0) {
     if (BACKWARD)
-      load_tile(bt, Ls + c0 + task.r0 * m, m, 1, rows, pw, K4);  // bt[k][r] = L(c0 + k, r0 + r)
+      load_tile<T>(bt, Ls + c0 + task.r0 * m, m, 1, rows, pw, K4);  // bt[k][r] = L(c0 + k, r0 + r)
     else
-      load_tile(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);  // bt[k][r] = L(r0 + r, c0 + k)
+      load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);  // bt[k][r] = L(r0 + r, c0 + k)
   }
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
   double acc[4][4][2];
   zero_acc(acc);
-  mma_tiles(inv, xs, K4, acc);
+  mma_tiles<double>(inv, xs, K4, acc);
   __syncthreads();
   each_acc(acc, [&](int i, int j, double val) {
     if (i < K4) xs[i * TS + j] = val;
@@ -554,7 +723,7 @@ __global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__rest
   if (rows <= 0) return;
   __syncthreads();
   zero_acc(acc);
-  mma_tiles(bt, xs, K4, acc);
+  mma_tiles<T>(bt, xs, K4, acc);
   double *dst;
   if (BACKWARD)
     dst = x2 + (f + task.r0) * R + j0;
@@ -565,23 +734,25 @@ __global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__rest
   });
 }
 
+// x[i*R + j] = b[perm[i] + j*ld] (times scale[i] when scaled), and back.
 __global__ void permute_in_kernel(const int64_t *__restrict__ perm, int64_t n, const double *__restrict__ b,
-                                  int64_t ld, double *__restrict__ x, int R) {
+                                  int64_t ld, double *__restrict__ x, int R, const double *__restrict__ scale) {
   const int64_t total = n * R;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = e / R;
     const int j = (int)(e % R);
-    x[e] = b[perm[i] + j * ld];
+    const double v = b[perm[i] + j * ld];
+    x[e] = scale ? v * scale[i] : v;
   }
 }
 
 __global__ void permute_out_kernel(const int64_t *__restrict__ perm, int64_t n, const double *__restrict__ x, int R,
-                                   double *__restrict__ b, int64_t ld) {
+                                   double *__restrict__ b, int64_t ld, const double *__restrict__ scale) {
   const int64_t total = n * R;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = e / R;
     const int j = (int)(e % R);
-    b[perm[i] + j * ld] = x[e];
+    b[perm[i] + j * ld] = scale ? x[e] * scale[i] : x[e];
   }
 }
 
@@ -598,18 +769,63 @@ __global__ void spmv_kernel(int64_t n, const int64_t *__restrict__ ptr, const in
   y[r + j * ld] = acc;
 }
 
+// The refinement's vector steps on column-major n x R blocks with leading dimension ld:
+// r = b - Ax (residual) and x += d (update).
+__global__ void residual_kernel(int64_t n, int R, int64_t ld, const double *__restrict__ b, double *__restrict__ ax) {
+  const int64_t total = n * R;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % n, j = e / n;
+    ax[i + j * ld] = b[i + j * ld] - ax[i + j * ld];
+  }
+}
+
+__global__ void update_kernel(int64_t n, int R, int64_t ld, const double *__restrict__ d, double *__restrict__ x) {
+  const int64_t total = n * R;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % n, j = e / n;
+    x[i + j * ld] += d[i + j * ld];
+  }
+}
+
+// out[j] = sum_i v(i, j)^2 for each column j (one CTA a column, a fixed tree order).
+__global__ void __launch_bounds__(256) sumsq_kernel(int64_t n, int64_t ld, const double *__restrict__ v,
+                                                    double *__restrict__ out) {
+  __shared__ double part[256];
+  const double *col = v + blockIdx.x * ld;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += col[i] * col[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) part[threadIdx.x] += part[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = part[0];
+}
+
+// The factor in the reference's packed trapezoids; an FP32 factor of S A S is brought back to A's
+// (L(A) = S^-1 L(S A S), row by row).
+template <class T>
 __global__ void pack_kernel(Tree t, const int64_t *__restrict__ toff, double *__restrict__ dst) {
   const int s = blockIdx.x;
   const int64_t m = t.height[s], w = t.width[s];
-  const double *Ls = t.L + t.loff[s];
+  const T *Ls = static_cast<const T *>(t.L) + t.loff[s];
+  const int32_t *rows = t.rows + t.rows_off[s];
   double *d = dst + toff[s];
   for (int64_t c = 0; c < w; ++c) {
     const int64_t start = c * m - c * (c > 0 ? c - 1 : 0) / 2;
     const int64_t p = c / NB, c0 = p * NB, c1 = c0 + NB < w ? c0 + NB : w, pw = c1 - c0;
     const double *Dp = t.D + t.doff[s] + 2 * (int64_t)NB * NB * p;
-    for (int64_t r = c + threadIdx.x; r < m; r += blockDim.x)
-      d[start + r - c] = r < c1 ? Dp[(c - c0) * pw + (r - c0)] : Ls[r + c * m];
+    for (int64_t r = c + threadIdx.x; r < m; r += blockDim.x) {
+      const double v = r < c1 ? Dp[(c - c0) * pw + (r - c0)] : (double)Ls[r + c * m];
+      d[start + r - c] = t.scale ? v / t.scale[rows[r]] : v;
+    }
   }
+}
+
+template <class K>
+void set_smem(K kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 }  // namespace
@@ -617,29 +833,49 @@ __global__ void pack_kernel(Tree t, const int64_t *__restrict__ toff, double *__
 void configure_kernels() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_smem(64));
-  cudaFuncSetAttribute(solve_panel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(64));
-  cudaFuncSetAttribute(solve_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(64));
-  cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+  set_smem(panel_kernel<double>, panel_smem<double>(64));
+  set_smem(panel_kernel<float>, panel_smem<float>(64));
+  set_smem(solve_panel_kernel<false, double>, solve_smem<double>(64));
+  set_smem(solve_panel_kernel<true, double>, solve_smem<double>(64));
+  set_smem(solve_panel_kernel<false, float>, solve_smem<float>(64));
+  set_smem(solve_panel_kernel<true, float>, solve_smem<float>(64));
+  set_smem(gemm_kernel<double>, gemm_smem<double>());
+  set_smem(gemm_kernel<float>, gemm_smem<float>());
+  set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
   done = true;
 }
 
-void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, const int2 *ranges, int count,
-                     cudaStream_t st) {
-  if (count > 0) assemble_kernel<<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
+void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double *scale, cudaStream_t st) {
+  if (n > 0) scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, diag_src, val, scale);
 }
 
-void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count, DeviceStatus *status,
-                  int p8max, cudaStream_t st) {
+void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const AssembleTask *tasks, const int2 *ranges,
+                     int count, cudaStream_t st) {
   if (count <= 0) return;
-  configure_kernels();
-  panel_kernel<<<count, PANEL_THREADS, panel_smem(p8max), st>>>(t, upper_val, tasks, status, p8max);
+  if (fp32)
+    assemble_kernel<float><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
+  else
+    assemble_kernel<double><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
 }
 
-void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st) {
+void launch_panel(const Tree &t, bool fp32, const double *upper_val, const PanelTask *tasks, int count,
+                  DeviceStatus *status, int p8max, cudaStream_t st) {
   if (count <= 0) return;
   configure_kernels();
-  gemm_kernel<<<count, GEMM_THREADS, GEMM_SMEM, st>>>(tasks);
+  if (fp32)
+    panel_kernel<float><<<count, PANEL_THREADS, panel_smem<float>(p8max), st>>>(t, upper_val, tasks, status, p8max);
+  else
+    panel_kernel<double><<<count, PANEL_THREADS, panel_smem<double>(p8max), st>>>(t, upper_val, tasks, status, p8max);
+}
+
+void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st) {
+  if (count <= 0) return;
+  configure_kernels();
+  switch (kind) {
+    case GemmKind::F64: gemm_kernel<double><<<count, GEMM_THREADS, gemm_smem<double>(), st>>>(tasks); break;
+    case GemmKind::F32A_F64: gemm_kernel<float><<<count, GEMM_THREADS, gemm_smem<float>(), st>>>(tasks); break;
+    case GemmKind::F32_TF32X3: gemm_tf32x3_kernel<<<count, GEMM_THREADS, GEMM_F32_SMEM, st>>>(tasks); break;
+  }
 }
 
 void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st) {
@@ -656,29 +892,39 @@ void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_
   if (count > 0) solve_gather_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks);
 }
 
-void launch_solve_panel(const Tree &t, bool backward, double *x, double *x2, double *v, const int64_t *voff, int R,
-                        const SolveTask *tasks, int count, int k4max, cudaStream_t st) {
+void launch_solve_panel(const Tree &t, bool fp32, bool backward, double *x, double *x2, double *v, const int64_t *voff,
+                        int R, const SolveTask *tasks, int count, int k4max, cudaStream_t st) {
   if (count <= 0) return;
   configure_kernels();
-  if (backward)
-    solve_panel_kernel<true><<<count, 128, solve_smem(k4max), st>>>(t, x, x2, v, voff, R, tasks, k4max);
-  else
-    solve_panel_kernel<false><<<count, 128, solve_smem(k4max), st>>>(t, x, x2, v, voff, R, tasks, k4max);
+  if (fp32) {
+    const size_t smem = solve_smem<float>(k4max);
+    if (backward)
+      solve_panel_kernel<true, float><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
+    else
+      solve_panel_kernel<false, float><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
+  } else {
+    const size_t smem = solve_smem<double>(k4max);
+    if (backward)
+      solve_panel_kernel<true, double><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
+    else
+      solve_panel_kernel<false, double><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
+  }
 }
 
-void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R, cudaStream_t st) {
+void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
+                       const double *scale, cudaStream_t st) {
   const int64_t total = n * R;
   if (total <= 0) return;
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
-  permute_in_kernel<<<blocks, 256, 0, st>>>(perm, n, b, ld, x, R);
+  permute_in_kernel<<<blocks, 256, 0, st>>>(perm, n, b, ld, x, R, scale);
 }
 
 void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, double *b, int64_t ld,
-                        cudaStream_t st) {
+                        const double *scale, cudaStream_t st) {
   const int64_t total = n * R;
   if (total <= 0) return;
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
-  permute_out_kernel<<<blocks, 256, 0, st>>>(perm, n, x, R, b, ld);
+  permute_out_kernel<<<blocks, 256, 0, st>>>(perm, n, x, R, b, ld, scale);
 }
 
 void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, double *y,
@@ -688,8 +934,28 @@ void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double
   spmv_kernel<<<grid, 128, 0, st>>>(n, ptr, idx, val, x, y, R, ld);
 }
 
-void launch_pack_trapezoids(const Tree &t, int64_t ns, const int64_t *toff, double *dst, cudaStream_t st) {
-  if (ns > 0) pack_kernel<<<(unsigned)ns, 128, 0, st>>>(t, toff, dst);
+void launch_residual(int64_t n, int R, int64_t ld, const double *b, double *ax, cudaStream_t st) {
+  const int64_t total = n * R;
+  if (total <= 0) return;
+  residual_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, ld, b, ax);
+}
+
+void launch_update(int64_t n, int R, int64_t ld, const double *d, double *x, cudaStream_t st) {
+  const int64_t total = n * R;
+  if (total <= 0) return;
+  update_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, ld, d, x);
+}
+
+void launch_sumsq(int64_t n, int R, int64_t ld, const double *v, double *out, cudaStream_t st) {
+  if (R > 0) sumsq_kernel<<<R, 256, 0, st>>>(n, ld, v, out);
+}
+
+void launch_pack_trapezoids(const Tree &t, bool fp32, int64_t ns, const int64_t *toff, double *dst, cudaStream_t st) {
+  if (ns <= 0) return;
+  if (fp32)
+    pack_kernel<float><<<(unsigned)ns, 128, 0, st>>>(t, toff, dst);
+  else
+    pack_kernel<double><<<(unsigned)ns, 128, 0, st>>>(t, toff, dst);
 }
 
 }  // namespace fc

@@ -37,8 +37,11 @@ struct Tree {
   const int64_t *diag_src;  // [n] upper-entry index of A(j, j), -1 if absent
   const int64_t *doff;      // [ns] diagonal arena: panel p of s keeps its factored block and its
                             // inverse (pw x pw each, column-major) at doff[s] + 2 NB NB p
-  double *L;
-  double *U;
+  const int32_t *a_row;     // mixed precision: each input entry's postordered row and column
+  const int32_t *a_col;
+  const double *scale;      // mixed precision: S = diag(A)^-1/2 (postorder); null in FP64
+  void *L;                  // L panels and update matrices: double, or float in mixed precision
+  void *U;
   double *D;
 };
 
@@ -59,9 +62,9 @@ struct PanelTask {
 // i >= j only (a diagonal tile of a symmetric matrix); 2 stores C = -sum instead of subtracting;
 // 4 stores C = +sum (one partial of a split sum, reduced later by a ReduceTask).
 struct GemmTask {
-  double *C;
-  const double *A;
-  const double *B;
+  void *C;
+  const void *A;
+  const void *B;
   int64_t c_si, c_sj, a_si, a_sk, b_sj, b_sk;
   int32_t M, N, K, flags;
 };
@@ -93,12 +96,18 @@ struct DeviceStatus {
 // Sets the kernels' shared-memory limits (once per process; before any stream capture).
 void configure_kernels();
 
-void launch_assemble(const Tree &t, const double *upper_val, const AssembleTask *tasks, const int2 *ranges,
-                     int count, cudaStream_t st);
+// The operand types of a GEMM launch: FP64 throughout (DMMA); an FP32 A with FP64 B and C (DMMA,
+// the solve on an FP32 factor); FP32 throughout by 3xTF32 (the FP32 factorisation).
+enum class GemmKind { F64, F32A_F64, F32_TF32X3 };
+
+// S = diag(A)^-1/2 for the mixed-precision factorisation.
+void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double *scale, cudaStream_t st);
+void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const AssembleTask *tasks,
+                     const int2 *ranges, int count, cudaStream_t st);
 // p8max: the widest panel of the launch, rounded up to a multiple of 8 (sizes shared memory).
-void launch_panel(const Tree &t, const double *upper_val, const PanelTask *tasks, int count,
+void launch_panel(const Tree &t, bool fp32, const double *upper_val, const PanelTask *tasks, int count,
                   DeviceStatus *status, int p8max, cudaStream_t st);
-void launch_gemm(const GemmTask *tasks, int count, cudaStream_t st);
+void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st);
 void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st);
 
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
@@ -109,17 +118,23 @@ void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_
 // Forward: y = L_pp^-1 x_p into x2, then x (own rows) / v (rows past the columns) -= L y.
 // Backward: z = L_pp^-T x2_p into x, then x2 (own rows above) -= L^T z.
 // k4max: the widest panel of the launch, rounded up to a multiple of 4.
-void launch_solve_panel(const Tree &t, bool backward, double *x, double *x2, double *v, const int64_t *voff,
-                        int R, const SolveTask *tasks, int count, int k4max, cudaStream_t st);
-// x_post[i*R + j] = b[perm[i] + j*ld] and back.
+void launch_solve_panel(const Tree &t, bool fp32, bool backward, double *x, double *x2, double *v,
+                        const int64_t *voff, int R, const SolveTask *tasks, int count, int k4max, cudaStream_t st);
+// x_post[i*R + j] = b[perm[i] + j*ld] (times scale[i] if given) and back.
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
-                       cudaStream_t st);
+                       const double *scale, cudaStream_t st);
 void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, double *b, int64_t ld,
-                        cudaStream_t st);
+                        const double *scale, cudaStream_t st);
+// Iterative refinement on column-major n x R blocks (leading dimension ld): ax <- b - ax,
+// x <- x + d, out[j] <- sum of squares of column j.
+void launch_residual(int64_t n, int R, int64_t ld, const double *b, double *ax, cudaStream_t st);
+void launch_update(int64_t n, int R, int64_t ld, const double *d, double *x, cudaStream_t st);
+void launch_sumsq(int64_t n, int R, int64_t ld, const double *v, double *out, cudaStream_t st);
 // y = A x for column-major x, y (leading dimension ld).
 void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x,
                  double *y, int R, int64_t ld, cudaStream_t st);
 // Copies the L panels out into the reference's packed trapezoids (dst offsets per supernode).
-void launch_pack_trapezoids(const Tree &t, int64_t ns, const int64_t *toff, double *dst, cudaStream_t st);
+void launch_pack_trapezoids(const Tree &t, bool fp32, int64_t ns, const int64_t *toff, double *dst,
+                            cudaStream_t st);
 
 }  // namespace fc

@@ -133,6 +133,19 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
  * fc_chol_entries(h) doubles. */
 int fc_chol_values(fc_chol *h, double *dst, fc_status *status);
 
+/* Solve A x = b to a relative residual by iterative refinement in FP64 around the handle's
+ * factor (the mixed-precision mode's FP32 factor of S A S, or the FP64 factor): x = 0, then
+ * d = solve(r), x += d, r = b - A x (FP64 SpMV on A by rows: d_ptr[n+1], d_idx, d_val, both
+ * triangles, the matrix the factor was made from) until ||r_j|| <= tol ||b_j|| for every
+ * right-hand side j or max_iter solves. No counterpart in the reference (its only refinement,
+ * Symmetric::solve_refined, crates/solver/src/ldlt.rs:529-566, is in working precision).
+ * b and x are column-major n x nrhs with leading dimension ld, in device memory. relres (host,
+ * nrhs entries, may be NULL) receives the final relative residuals, *iterations the solves done.
+ * FC_TIMEOUT when max_iter solves did not reach tol (x holds the last iterate). */
+int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val,
+                                const double *d_b, double *d_x, int32_t nrhs, int64_t ld, double tol,
+                                int32_t max_iter, double *relres, int32_t *iterations, fc_status *status);
+
 /* Plan statistics: 0 levels, 1 launches of the factor, 2 bytes of L on device, 3 bytes of the
  * update matrices, 4 supernodes, 5 factor flops (sum of column counts squared), 6 GEMM tasks,
  * 7 kernels launched by the last factorisation, 8 kernels launched by the last solve, 9 flops of

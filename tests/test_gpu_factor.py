@@ -189,3 +189,43 @@ def test_batch_of_uneven_systems(cuda):
     with pytest.raises(NotPositiveDefinite) as e:
         bf2.factor([p.val for p in parts2])
     assert e.value.system == 1 and e.value.column == alone
+
+
+def device_csr(torch, csr):
+    return (torch.from_numpy(csr.ptr).cuda(), torch.from_numpy(csr.idx).cuda(), torch.from_numpy(csr.val).cuda())
+
+
+@pytest.mark.parametrize("name,make,values_tol", [("lognormal-12", lambda: problems.lognormal_block(12, nrhs=4), 1e-4),
+                                                  ("cantilever", problems.cantilever, None)],
+                         ids=["lognormal-12", "cantilever"])
+def test_mixed_precision_refines_to_the_fp64_answer(cuda, name, make, values_tol):
+    # FP32 factor (3xTF32 updates, FP64 diagonal blocks) of S A S + FP64 refinement: every
+    # right-hand side reaches ||b - A x|| <= 1e-10 ||b||, and x agrees with the FP64 direct solve
+    # to what the system's conditioning allows (1e-6 relative). On the well-conditioned block the
+    # FP32 factor itself is the FP64 one to FP32 precision; on the slender cantilever (condition
+    # ~1e9) its trailing pivots are not, which is what the refinement is for.
+    from fieldcraft_b200 import FP32_IR
+    torch = cuda
+    p = make()
+    up = p.upper()
+    sym = Symbolic(up, 2**62)
+    f32 = Factor(sym, precision=FP32_IR)
+    f32.factor(up.val)
+    k = p.rhs.shape[1]
+    b = torch.from_numpy(np.ascontiguousarray(p.rhs.T)).cuda()
+    x = torch.zeros_like(b)
+    rel, its = f32.refine_solve_device(device_csr(torch, p.csr), b, x, k, p.n, tol=1e-10, max_iter=30)
+    assert np.all(rel <= 1e-10) and its <= 30, (rel, its)
+    _, ref = oracle_factor(p.csr)
+    exp = ref.solve(p.rhs.copy())
+    got = x.cpu().numpy().T
+    assert np.linalg.norm(got - exp) <= 1e-6 * np.linalg.norm(exp)
+    if values_tol is not None:
+        lv, rv = f32.values(), ref.values()
+        assert np.max(np.abs(lv - rv)) <= values_tol * np.max(np.abs(rv))
+    # the FP64 factor refines in one or two solves
+    f64 = Factor(sym)
+    f64.factor(up.val)
+    x64 = torch.zeros_like(b)
+    rel64, its64 = f64.refine_solve_device(device_csr(torch, p.csr), b, x64, k, p.n, tol=1e-10, max_iter=5)
+    assert np.all(rel64 <= 1e-10) and its64 <= 2
