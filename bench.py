@@ -248,7 +248,7 @@ def main():
     if args.profile_only:
         # the launch counts per step (for choosing which launches a profiler captures), then the
         # warm-up steps and nothing else
-        kinds = 24
+        kinds = 26
         ms_k = np.zeros(kinds)
         cnt_k = np.zeros(kinds, np.int64)
         lib.fc_chol_profile(f.handle, 1)
@@ -302,7 +302,7 @@ def main():
         return
 
     # per-kernel times on the same stream (events around every launch), one profiled step
-    kinds = 24
+    kinds = 26
     ms_k = np.zeros(kinds)
     cnt_k = np.zeros(kinds, np.int64)
     lib.fc_chol_profile(f.handle, 1)

@@ -49,8 +49,11 @@ SIGNATURES = {
     "fc_chol_values": (i32, [P, P, C.POINTER(Status)]),
     "fc_chol_stat": (i64, [P, i32]),
     "fc_chol_refine_solve_device": (i32, [P, P, P, P, P, P, i32, i64, f64, i32, P, P, C.POINTER(Status)]),
+    "fc_chol_option": (i32, [P, i32, i64]),
+    "fc_chol_trace_read": (i64, [P, P, i64]),
     "fc_chol_profile": (i32, [P, i32]),
     "fc_chol_profile_read": (i32, [P, P, P, i32]),
+    "fc_chol_profile_launches": (i64, [P, P, P, P, P, i64]),
     "fc_csr_spmv_device": (i32, [i64, P, P, P, P, P, i32, i64, P]),
     "fc_version": (C.c_char_p, []),
     # fieldcraft_fem.h

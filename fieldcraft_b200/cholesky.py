@@ -180,7 +180,10 @@ class Symbolic:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            _lib.load().fc_symbolic_free(h)
+            try:
+                _lib.load().fc_symbolic_free(h)
+            except TypeError:  # interpreter shutdown: the module's globals are gone
+                pass
             self.handle = None
 
 
@@ -284,6 +287,14 @@ class Factor:
     def stat(self, what: int) -> int:
         return int(_lib.load().fc_chol_stat(self.handle, what))
 
+    # fc_chol_option: the solve's schedule (0 level by level, 1 persistent), the persistent solve's
+    # wait limit in nanoseconds, and (tests) a planted dependency that no task meets
+    SOLVE_SCHEDULE, WAIT_LIMIT_NS, PLANT_UNMET_WAIT, TRACE = 1, 2, 3, 4
+
+    def option(self, option: int, value: int):
+        if _lib.load().fc_chol_option(self.handle, int(option), int(value)) != 0:
+            raise ValueError(f"option {option} = {value}")
+
     def set_stream(self, stream_ptr: int | None):
         _lib.load().fc_chol_set_stream(self.handle, C.c_void_p(stream_ptr) if stream_ptr else None)
 
@@ -294,4 +305,7 @@ class Factor:
             self.handle = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except TypeError:  # interpreter shutdown: the module's globals are gone
+            pass

@@ -85,7 +85,10 @@ cudaError_t upload(DeviceBuf &buf, const std::vector<T> &host, cudaStream_t st) 
   return cudaMemcpyAsync(buf.p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, st);
 }
 
-enum Kind { K_ASSEMBLE, K_PANEL, K_REDUCE, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD };
+enum Kind {
+  K_ASSEMBLE, K_PANEL, K_REDUCE, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD,
+  K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD
+};
 
 struct Launch {
   int kind;
@@ -126,6 +129,16 @@ struct fc_chol {
   int solve_R = 0;
   DeviceBuf d_x, d_x2, d_v, d_part, d_voff, d_b, d_srow, d_sranges, d_spanel, d_sgemm, d_sreduce;
   std::vector<Launch> fwd, bwd;
+  // the solve as two dependency-driven persistent launches instead of level by level
+  // (FC_OPTION_SOLVE_SCHEDULE, or FC_SOLVE_PERSISTENT=1 in the environment)
+  bool dag = false;
+  DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
+  int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
+  int dag_grid = 0;
+  long long dag_limit_ns = 4000000000LL;  // a wait longer than this fails the solve (FC_TIMEOUT)
+  bool dag_trace = false;                 // per-task times of the persistent solve
+  DeviceBuf d_dtrace;
+  bool dag_plant = false;                 // test hook: the next plan holds a dependency nothing meets
   int64_t last_factor_launches = 0, last_solve_launches = 0;
   double gemm_flops_factor = 0, gemm_flops_solve = 0;
   int64_t gemm_big_ordinal = -1, gemm_trail_ordinal = -1;  // the factor's heaviest GEMM launches
@@ -139,7 +152,11 @@ struct fc_chol {
   double *solve_graph_b = nullptr;
   int solve_graph_R = 0;
   int64_t solve_graph_ld = 0;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  struct MarkRec {
+    int kind, level, count;
+    cudaEvent_t a, b;
+  };
+  std::vector<MarkRec> marks;
   std::vector<cudaEvent_t> event_pool;
   size_t events_used = 0;
   std::mutex lock;
@@ -151,6 +168,12 @@ struct fc_chol {
 };
 
 namespace {
+
+int prop_sms(int device) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+  return v > 0 ? v : 1;
+}
 
 int cuda_fail(fc_status *st, cudaError_t e, const char *where) {
   std::string msg = std::string(where) + ": " + cudaGetErrorString(e);
@@ -575,9 +598,9 @@ cudaEvent_t next_event(fc_chol *h) {
 // Brackets one launch with events when profiling.
 struct Mark {
   fc_chol *h;
-  int kind;
+  int kind, level, count;
   cudaEvent_t a = nullptr;
-  Mark(fc_chol *h_, int kind_) : h(h_), kind(kind_) {
+  Mark(fc_chol *h_, int kind_, int level_ = -1, int count_ = 0) : h(h_), kind(kind_), level(level_), count(count_) {
     if (h->profiling) {
       a = next_event(h);
       cudaEventRecord(a, h->stream);
@@ -587,7 +610,7 @@ struct Mark {
     if (h->profiling) {
       cudaEvent_t b = next_event(h);
       cudaEventRecord(b, h->stream);
-      h->marks.push_back({kind, {a, b}});
+      h->marks.push_back({kind, level, count, a, b});
     }
   }
 };
@@ -656,7 +679,7 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
       }
       last_level = l.level;
     }
-    Mark mark(h, l.kind);
+    Mark mark(h, l.kind, l.level, l.count);
     switch (l.kind) {
       case K_ASSEMBLE:
         fc::launch_assemble(t, h->fp32, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, h->d_ranges.as<int2>(), l.count,
@@ -849,6 +872,400 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
   }
 }
 
+
+// The solve as two task lists, forward and backward, for the persistent kernel. Supernodes with
+// at most NODE_ROWS front rows are one task per direction (and block of 64 right-hand sides);
+// larger ones are split in chunks of 64 front rows. Per chunk and block of right-hand sides a
+// counter counts the updates the chunk has taken, in the order the level-by-level launches apply
+// them: forward, its assembly (if any) then one per earlier panel; backward, its product with the
+// rows past the columns (if any) then one per later panel. A task waits for the counts its inputs
+// must have reached, so every entry sees the same operations in the same order on every run.
+// FIN(s) counts the final update vectors of s (the parent assembles them), DONE(s) the solved
+// panels of s (the children's backward products read them). Update vectors and split-product
+// partials get space of their own: levels overlap here.
+constexpr int NODE_ROWS = 512;
+constexpr int ASSEMBLE_GROUP = 4;  // chunks per assembly task of a large supernode
+constexpr int PANEL_GROUP = 4;     // chunks per panel task past the first chunk
+
+struct DagPlan {
+  std::vector<fc::DagTask> fwd, bwd;
+  std::vector<fc::DagDep> deps;
+  std::vector<fc::DagChild> children;
+  std::vector<int64_t> voff;
+  int64_t vsum = 0, psum = 0, counters = 0;
+};
+
+void dag_plan(const fc_chol *h, int R, bool plant, DagPlan &p) {
+  const int NB = fc::NB;
+  const int J = (R + 63) / 64;
+  const int64_t ns = h->ns;
+  std::vector<std::vector<int64_t>> lv(h->levels);
+  for (int64_t s = 0; s < ns; ++s) lv[h->level[s]].push_back(s);
+  std::vector<int64_t> parent(ns, -1), cbase(ns + 1, 0);
+  for (int64_t s = 0; s < ns; ++s)
+    for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) parent[h->kids[q]] = s;
+  auto panels = [&](int64_t s) { return (h->width[s] + NB - 1) / NB; };
+  auto below = [&](int64_t s) { return (h->height[s] - h->width[s] + 63) / 64; };
+  auto whole = [&](int64_t s) { return h->height[s] <= NODE_ROWS; };
+  p.voff.assign(ns, 0);
+  for (int64_t s = 0; s < ns; ++s) {
+    p.voff[s] = p.vsum;
+    p.vsum += (int64_t)(h->height[s] - h->width[s]) * R;
+    cbase[s + 1] = cbase[s] + panels(s) + below(s);
+  }
+  const int64_t NC = cbase[ns] * J;
+  auto F = [&](int64_t s, int c, int jc) { return (int32_t)((cbase[s] + c) * J + jc); };
+  auto G = [&](int64_t s, int c, int jc) { return (int32_t)(NC + (cbase[s] + c) * J + jc); };
+  auto PC = [&](int64_t s, int c, int jc) { return (int32_t)(2 * NC + (cbase[s] + c) * J + jc); };
+  auto Y = [&](int64_t s, int c, int jc) { return (int32_t)(3 * NC + (cbase[s] + c) * J + jc); };
+  auto Z = [&](int64_t s, int c, int jc) { return (int32_t)(4 * NC + (cbase[s] + c) * J + jc); };
+  auto FIN = [&](int64_t s, int jc) { return (int32_t)(5 * NC + s * J + jc); };
+  auto DONE = [&](int64_t s, int jc) { return (int32_t)(5 * NC + (ns + s) * J + jc); };
+  p.counters = 5 * NC + 2 * ns * J;
+  auto kids = [&](int64_t s) { return h->kid_ptr[s + 1] > h->kid_ptr[s]; };
+  auto assembled = [&](int64_t s, int c) { return kids(s) || c >= panels(s); };
+  auto chunk = [&](int64_t s, int c, int &i0, int &i1) {
+    const int P = panels(s), w = h->width[s], m = h->height[s];
+    if (c < P) {
+      i0 = c * 64, i1 = std::min(w, i0 + 64);
+    } else {
+      i0 = w + (c - P) * 64, i1 = std::min(m, i0 + 64);
+    }
+  };
+  auto dep = [&](int32_t counter, int32_t value) {
+    if (value > 0) p.deps.push_back({counter, value});
+  };
+  auto task = [&](int32_t kind, int64_t s, int i0, int i1, int r0, int r1, int jc) {
+    fc::DagTask t{};
+    t.kind = kind, t.s = (int32_t)s, t.i0 = i0, t.i1 = i1, t.r0 = r0, t.r1 = r1;
+    t.j0 = jc * 64, t.j1 = std::min(R, jc * 64 + 64);
+    t.dep0 = t.dep1 = (int32_t)p.deps.size();
+    t.sig0 = t.sig1 = t.sigmid = -1;
+    t.aux = -1;
+    return t;
+  };
+  // the children's rows landing in front rows [i0, i1) of s
+  auto children = [&](int64_t s, int i0, int i1) {
+    std::vector<int2> r;
+    child_ranges(h, s, i0, i1, r);
+    const int32_t at = (int32_t)p.children.size();
+    for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) {
+      const int64_t c = h->kids[q];
+      const int2 rg = r[q - h->kid_ptr[s]];
+      p.children.push_back({h->rel_off[c], p.voff[c], rg.x, rg.y});
+    }
+    return at;
+  };
+  auto wait_children = [&](int64_t s, int jc) {
+    for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) dep(FIN(h->kids[q], jc), below(h->kids[q]));
+  };
+  auto doff = [&](int64_t s, int pp) { return h->doff[s] + 2 * (int64_t)NB * NB * pp; };
+  // forward
+  for (size_t l = 0; l < lv.size(); ++l) {
+    const auto &S = lv[l];
+    for (int64_t s : S) {
+      if (!whole(s)) continue;
+      const int32_t rec = children(s, 0, h->height[s]);
+      for (int jc = 0; jc < J; ++jc) {
+        fc::DagTask t = task(fc::DAG_NODE, s, 0, h->height[s], 0, 0, jc);
+        t.child = rec;
+        wait_children(s, jc);
+        t.dep1 = (int32_t)p.deps.size();
+        if (below(s) > 0) t.sig1 = FIN(s, jc), t.inc1 = below(s);
+        p.fwd.push_back(t);
+      }
+    }
+    for (int64_t s : S) {
+      if (whole(s)) continue;
+      const int P = panels(s), C = P + below(s);
+      for (int c = kids(s) ? 0 : P; c < C; c += ASSEMBLE_GROUP) {
+        const int ce = std::min(C, c + ASSEMBLE_GROUP);
+        int i0, i1, e0, e1;
+        chunk(s, c, i0, e0);
+        chunk(s, ce - 1, e1, i1);
+        const int32_t rec = children(s, i0, i1);
+        for (int jc = 0; jc < J; ++jc) {
+          fc::DagTask t = task(fc::DAG_ASSEMBLE, s, i0, i1, c, ce, jc);
+          t.child = rec;
+          wait_children(s, jc);
+          t.dep1 = (int32_t)p.deps.size();
+          t.sig0 = F(s, c, jc), t.sigstep = J, t.nsig = ce - c;
+          p.fwd.push_back(t);
+        }
+      }
+    }
+    int Pmax = 0;
+    for (int64_t s : S)
+      if (!whole(s)) Pmax = std::max(Pmax, panels(s));
+    for (int pp = 0; pp < Pmax; ++pp) {
+      for (int64_t s : S) {
+        const int P = panels(s), C = P + below(s), m = h->height[s], w = h->width[s];
+        if (whole(s) || pp >= P) continue;
+        const int c0 = pp * NB, c1 = std::min(w, c0 + NB);
+        const int need_p = (assembled(s, pp) ? 1 : 0) + pp;
+        for (int jc = 0; jc < J; ++jc) {
+          if (c1 >= m) {  // no rows below: the panel's solution only
+            fc::DagTask t = task(fc::DAG_PANEL, s, c0, c1, C, C, jc);
+            dep(F(s, pp, jc), need_p);
+            t.dep1 = (int32_t)p.deps.size();
+            t.keep = 1, t.aux = doff(s, pp);
+            p.fwd.push_back(t);
+            continue;
+          }
+          // the first chunk below applies the inverse and stores y; the others read y
+          for (int c = pp + 1; c < C;) {
+            const bool first = c == pp + 1;
+            const int ce = first ? c + 1 : std::min(C, c + PANEL_GROUP);
+            fc::DagTask t = task(fc::DAG_PANEL, s, c0, c1, c, ce, jc);
+            if (first)
+              dep(F(s, pp, jc), need_p);
+            else
+              dep(Y(s, pp, jc), 1);
+            for (int q = c; q < ce; ++q) dep(F(s, q, jc), (assembled(s, q) ? 1 : 0) + pp);
+            t.dep1 = (int32_t)p.deps.size();
+            t.keep = first ? 1 : -1, t.aux = doff(s, pp);
+            t.sigmid = first ? Y(s, pp, jc) : -1;
+            t.sig0 = F(s, c, jc), t.sigstep = J;
+            if (pp == P - 1) t.sig1 = FIN(s, jc), t.inc1 = ce - c;  // final update vectors
+            p.fwd.push_back(t);
+            c = ce;
+          }
+        }
+      }
+    }
+  }
+  // backward
+  for (int64_t l = (int64_t)lv.size() - 1; l >= 0; --l) {
+    const auto &S = lv[l];
+    auto wait_parent = [&](int64_t s, int jc) {
+      if (parent[s] >= 0) dep(DONE(parent[s], jc), panels(parent[s]));
+    };
+    for (int64_t s : S) {
+      if (!whole(s)) continue;
+      for (int jc = 0; jc < J; ++jc) {
+        fc::DagTask t = task(fc::DAG_NODE, s, 0, h->height[s], 0, 0, jc);
+        wait_parent(s, jc);
+        t.dep1 = (int32_t)p.deps.size();
+        t.sig1 = DONE(s, jc), t.inc1 = panels(s);
+        p.bwd.push_back(t);
+      }
+    }
+    std::vector<fc::DagTask> reduce;
+    for (int64_t s : S) {
+      const int u = h->height[s] - h->width[s], w = h->width[s], P = panels(s);
+      if (whole(s) || u <= 0) continue;
+      const bool split = u > 2 * fc::SPLIT_K;
+      const int chunks = split ? (u + fc::SPLIT_K - 1) / fc::SPLIT_K : 1;
+      for (int i = 0; i < P; ++i)
+        for (int jc = 0; jc < J; ++jc) {
+          const int i0 = 64 * i, i1 = std::min(w, i0 + 64);
+          for (int q = 0; q < chunks; ++q) {
+            const int k0 = split ? q * fc::SPLIT_K : 0, k1 = split ? std::min(u, k0 + fc::SPLIT_K) : u;
+            fc::DagTask t = task(fc::DAG_GEMM, s, i0, i1, k0, k1, jc);
+            wait_parent(s, jc);
+            t.dep1 = (int32_t)p.deps.size();
+            if (split)
+              t.aux = p.psum + (int64_t)q * 4096, t.sig1 = PC(s, i, jc);
+            else
+              t.sig1 = G(s, i, jc);
+            t.inc1 = 1;
+            p.bwd.push_back(t);
+          }
+          if (split) {
+            fc::DagTask t = task(fc::DAG_REDUCE, s, i0, i1, 0, 0, jc);
+            t.count = chunks, t.aux = p.psum;
+            t.sig1 = G(s, i, jc), t.inc1 = 1;
+            reduce.push_back(t);
+            p.psum += (int64_t)chunks * 4096;
+          }
+        }
+    }
+    for (fc::DagTask t : reduce) {  // after the level's products
+      t.dep0 = (int32_t)p.deps.size();
+      dep(PC(t.s, t.i0 / 64, t.j0 / 64), t.count);
+      t.dep1 = (int32_t)p.deps.size();
+      p.bwd.push_back(t);
+    }
+    int Pmax = 0;
+    for (int64_t s : S)
+      if (!whole(s)) Pmax = std::max(Pmax, panels(s));
+    for (int pp = Pmax - 1; pp >= 0; --pp) {
+      for (int64_t s : S) {
+        const int P = panels(s), u = h->height[s] - h->width[s], w = h->width[s];
+        if (whole(s) || pp >= P) continue;
+        const int c0 = pp * NB, c1 = std::min(w, c0 + NB);
+        const int need = (u > 0 ? 1 : 0) + (P - 1 - pp);
+        for (int jc = 0; jc < J; ++jc) {
+          if (c0 == 0) {
+            fc::DagTask t = task(fc::DAG_PANEL, s, c0, c1, 0, 0, jc);
+            dep(G(s, pp, jc), need);
+            t.dep1 = (int32_t)p.deps.size();
+            t.keep = 1, t.aux = doff(s, pp);
+            t.sig1 = DONE(s, jc), t.inc1 = 1;
+            p.bwd.push_back(t);
+            continue;
+          }
+          // the chunk just above (the next panel to solve) applies the inverse and stores z; the
+          // chunks further up read z
+          {
+            fc::DagTask t = task(fc::DAG_PANEL, s, c0, c1, pp - 1, pp, jc);
+            dep(G(s, pp, jc), need);
+            dep(G(s, pp - 1, jc), need);
+            t.dep1 = (int32_t)p.deps.size();
+            t.keep = 1, t.aux = doff(s, pp);
+            t.sigmid = Z(s, pp, jc);
+            t.sig0 = G(s, pp - 1, jc), t.sigstep = J;
+            t.sig1 = DONE(s, jc), t.inc1 = 1;
+            p.bwd.push_back(t);
+          }
+          for (int r = 0; r < pp - 1; r += PANEL_GROUP) {
+            const int re = std::min(pp - 1, r + PANEL_GROUP);
+            fc::DagTask t = task(fc::DAG_PANEL, s, c0, c1, r, re, jc);
+            dep(Z(s, pp, jc), 1);
+            for (int q = r; q < re; ++q) dep(G(s, q, jc), need);
+            t.dep1 = (int32_t)p.deps.size();
+            t.keep = -1, t.aux = doff(s, pp);
+            t.sig0 = G(s, r, jc), t.sigstep = J;
+            p.bwd.push_back(t);
+          }
+        }
+      }
+    }
+  }
+  if (plant && !p.fwd.empty()) {  // the last forward task also waits for a count nothing reaches
+    fc::DagTask &t = p.fwd.back();
+    std::vector<fc::DagDep> extra(p.deps.begin() + t.dep0, p.deps.begin() + t.dep1);
+    extra.push_back({0, INT32_MAX});
+    t.dep0 = (int32_t)p.deps.size();
+    p.deps.insert(p.deps.end(), extra.begin(), extra.end());
+    t.dep1 = (int32_t)p.deps.size();
+  }
+}
+
+// Runs the lists in order on the host's counters (one CTA taking every task in turn): every wait
+// must be met by earlier tasks, and every counter index must be in range. Each counter is raised
+// either by a chain of tasks that each wait for the count before their own, or by tasks whose
+// waiter needs all of them, so a count is never reached early with more CTAs.
+bool check_dag(const DagPlan &p, std::string &why) {
+  std::vector<int32_t> cnt((size_t)p.counters, 0);
+  int64_t id = 0;
+  for (const auto *list : {&p.fwd, &p.bwd}) {
+    for (const fc::DagTask &t : *list) {
+      if (t.dep0 < 0 || t.dep1 < t.dep0 || t.dep1 > (int64_t)p.deps.size()) {
+        why = "task " + std::to_string(id) + ": dependency range";
+        return false;
+      }
+      for (int32_t e = t.dep0; e < t.dep1; ++e) {
+        const fc::DagDep d = p.deps[e];
+        if (d.counter < 0 || d.counter >= p.counters || cnt[d.counter] < d.value) {
+          why = "task " + std::to_string(id) + " waits for a count no earlier task reaches";
+          return false;
+        }
+      }
+      std::vector<std::pair<int64_t, int32_t>> raised;
+      const int nsig = t.kind == fc::DAG_PANEL ? t.r1 - t.r0 : t.nsig;
+      if (t.sig0 >= 0)
+        for (int k = 0; k < nsig; ++k) raised.push_back({(int64_t)t.sig0 + (int64_t)k * t.sigstep, 1});
+      if (t.sig1 >= 0) raised.push_back({t.sig1, t.inc1});
+      if (t.sigmid >= 0) raised.push_back({t.sigmid, 1});
+      for (const auto &r : raised) {
+        if (r.first < 0 || r.first >= p.counters) {
+          why = "task " + std::to_string(id) + ": counter out of range";
+          return false;
+        }
+        cnt[r.first] += r.second;
+      }
+      ++id;
+    }
+  }
+  return true;
+}
+
+int plan_solve_dag(fc_chol *h, int R, fc_status *st) {
+  DagPlan p;
+  dag_plan(h, R, h->dag_plant, p);
+  std::string why;
+  if (!h->dag_plant && !check_dag(p, why)) {
+    set_status(st, FC_INTERNAL, -1, 0, 0, "solve plan: " + why);
+    return FC_INTERNAL;
+  }
+  h->dag_plant = false;
+  if (p.counters >= INT32_MAX || p.deps.size() >= (size_t)INT32_MAX || p.fwd.size() >= (size_t)INT32_MAX ||
+      p.bwd.size() >= (size_t)INT32_MAX) {
+    set_status(st, FC_INTERNAL, -1, 0, 0, "solve plan too large");
+    return FC_INTERNAL;
+  }
+  if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
+      h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
+      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess ||
+      h->d_part.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.psum, 1)) != cudaSuccess ||
+      h->d_dcount.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(p.counters, 1)) != cudaSuccess ||
+      h->d_dctl.alloc(sizeof(fc::DagControl)) != cudaSuccess) {
+    h->solve_R = 0;
+    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
+    return FC_OUT_OF_MEMORY;
+  }
+  std::vector<fc::DagTask> all(p.fwd);
+  all.insert(all.end(), p.bwd.begin(), p.bwd.end());
+  cudaError_t e;
+  if ((e = upload(h->d_voff, p.voff, h->stream)) != cudaSuccess || (e = upload(h->d_dtasks, all, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_ddeps, p.deps, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_dranges, p.children, h->stream)) != cudaSuccess)
+    return cuda_fail(st, e, "solve plan");
+  if ((e = cudaMemsetAsync(h->d_dctl.p, 0, sizeof(fc::DagControl), h->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
+    return cuda_fail(st, e, "solve plan");
+  if (h->dag_trace && h->d_dtrace.alloc(sizeof(long long) * 4 * std::max<size_t>(all.size(), 1)) != cudaSuccess) {
+    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve trace");
+    return FC_OUT_OF_MEMORY;
+  }
+  h->dag_fwd = (int64_t)p.fwd.size();
+  h->dag_bwd = (int64_t)p.bwd.size();
+  h->dag_counters = p.counters;
+  h->dag_grid = prop_sms(h->device) * fc::solve_dag_blocks_per_sm(h->fp32);
+  h->gemm_flops_solve = 0;
+  h->solve_R = R;
+  return FC_OK;
+}
+
+// The launch record of one direction of the persistent solve.
+fc::SolveDag solve_dag(fc_chol *h, bool backward, int R) {
+  fc::SolveDag d{};
+  d.tasks = h->d_dtasks.as<fc::DagTask>() + (backward ? h->dag_fwd : 0);
+  d.count = (int32_t)(backward ? h->dag_bwd : h->dag_fwd);
+  d.deps = h->d_ddeps.as<fc::DagDep>();
+  d.counters = h->d_dcount.as<int32_t>();
+  d.ctl = h->d_dctl.as<fc::DagControl>();
+  d.x = h->d_x.as<double>();
+  d.x2 = h->d_x2.as<double>();
+  d.v = h->d_v.as<double>();
+  d.part = h->d_part.as<double>();
+  d.voff = h->d_voff.as<int64_t>();
+  d.children = h->d_dranges.as<fc::DagChild>();
+  d.R = R;
+  d.limit_ns = h->dag_limit_ns;
+  d.trace = h->dag_trace ? h->d_dtrace.as<long long>() + (backward ? 4 * h->dag_fwd : 0) : nullptr;
+  return d;
+}
+
+// FC_TIMEOUT when the last persistent solve gave up on a wait (after the stream is idle).
+int solve_wait_status(fc_chol *h, fc_status *st) {
+  if (!h->dag || !h->d_dctl.p) return FC_OK;
+  fc::DagControl c{};
+  cudaError_t e = cudaMemcpy(&c, h->d_dctl.p, sizeof(c), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(st, e, "solve status");
+  if (c.error) {
+    h->solve_R = 0;  // the next solve plans (and captures) afresh
+    if (h->solve_graph) {
+      cudaGraphExecDestroy(h->solve_graph);
+      h->solve_graph = nullptr;
+    }
+    set_status(st, FC_TIMEOUT, -1, 0, 0, "a wait of the solve ran past its limit (task " + std::to_string(c.task) + ")");
+    return FC_TIMEOUT;
+  }
+  return FC_OK;
+}
+
 // The handle's own solve buffers and task arrays for R right-hand sides (built once per R).
 int plan_solve(fc_chol *h, int R, fc_status *st) {
   if (h->solve_R == R) return FC_OK;
@@ -856,6 +1273,7 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
     cudaGraphExecDestroy(h->solve_graph);
     h->solve_graph = nullptr;
   }
+  if (h->dag) return plan_solve_dag(h, R, st);
   SolvePlan p;
   solve_offsets(h, R, p);
   cudaError_t e;
@@ -903,7 +1321,7 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
   cudaStream_t st = h->stream;
   const fc::Tree &t = h->tree;
   for (const Launch &l : prog) {
-    Mark mark(h, l.kind + 16);
+    Mark mark(h, l.kind + 16, l.level, l.count);
     switch (l.kind) {
       case K_SOLVE_ASSEMBLE:
         fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st);
@@ -949,12 +1367,28 @@ int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
     h->solve_graph_stream = h->stream;
   }
   cudaGraphLaunch(h->solve_graph, h->stream);
-  h->last_solve_launches = (int64_t)(h->fwd.size() + h->bwd.size() + 2);
+  h->last_solve_launches = h->dag ? 4 : (int64_t)(h->fwd.size() + h->bwd.size() + 2);
   return FC_OK;
 }
 
 void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   int64_t launches = 0;
+  if (h->dag) {
+    cudaMemsetAsync(h->d_dcount.p, 0, sizeof(int32_t) * (size_t)h->dag_counters, h->stream);
+    cudaMemsetAsync(h->d_dctl.p, 0, sizeof(fc::DagControl), h->stream);
+    fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
+    {
+      Mark mark(h, K_SOLVE_DAG_FWD + 16, -1, (int)h->dag_fwd);
+      fc::launch_solve_dag(h->tree, h->fp32, false, solve_dag(h, false, R), h->dag_grid, h->stream);
+    }
+    {
+      Mark mark(h, K_SOLVE_DAG_BWD + 16, -1, (int)h->dag_bwd);
+      fc::launch_solve_dag(h->tree, h->fp32, true, solve_dag(h, true, R), h->dag_grid, h->stream);
+    }
+    fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->tree.scale, h->stream);
+    h->last_solve_launches = 4;
+    return;
+  }
   const SolveBuffers b = own_buffers(h);
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
   run_solve_program(h, h->fwd, b, R, launches);
@@ -1143,6 +1577,8 @@ int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **
   {
     const char *env = std::getenv("FC_NO_GRAPHS");
     h->graphs = !(env && env[0] == '1');
+    const char *persistent = std::getenv("FC_SOLVE_PERSISTENT");
+    h->dag = persistent && persistent[0] == '1';
   }
   fc::configure_kernels();
   if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -1225,7 +1661,57 @@ int fc_chol_check(fc_chol *h, fc_status *status) {
   if (!h) return FC_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(h->lock);
   cudaSetDevice(h->device);
-  return read_status(h, status);
+  const int rc = read_status(h, status);
+  if (rc != FC_OK) return rc;
+  return solve_wait_status(h, status);
+}
+
+int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
+  if (!h) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  auto replan = [&] {
+    h->solve_R = 0;
+    if (h->solve_graph) {
+      cudaGraphExecDestroy(h->solve_graph);
+      h->solve_graph = nullptr;
+    }
+  };
+  switch (option) {
+    case FC_OPTION_SOLVE_SCHEDULE:
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      h->dag = value == 1;
+      replan();
+      return FC_OK;
+    case FC_OPTION_WAIT_LIMIT_NS:
+      if (value <= 0) return FC_INVALID_ARGUMENT;
+      h->dag_limit_ns = value;
+      replan();
+      return FC_OK;
+    case FC_OPTION_PLANT_UNMET_WAIT:
+      h->dag_plant = value != 0;
+      replan();
+      return FC_OK;
+    case FC_OPTION_TRACE:
+      h->dag_trace = value != 0;
+      replan();
+      return FC_OK;
+  }
+  return FC_INVALID_ARGUMENT;
+}
+
+int64_t fc_chol_trace_read(fc_chol *h, int64_t *out, int64_t cap) {
+  if (!h || cap < 0 || (cap > 0 && !out)) return -FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  if (!h->dag_trace || !h->dag || h->solve_R == 0) return 0;
+  const int64_t tasks = h->dag_fwd + h->dag_bwd;
+  const int64_t words = std::min(cap, 4 * tasks);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+      (words > 0 && cudaMemcpy(out, h->d_dtrace.p, sizeof(int64_t) * words, cudaMemcpyDeviceToHost) != cudaSuccess))
+    return -FC_CUDA_ERROR;
+  return tasks;
 }
 
 int fc_chol_factor_device(fc_chol *h, const double *d_upper_val, int64_t nnz, fc_status *status) {
@@ -1265,6 +1751,7 @@ int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_s
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(status, e, "solve");
+  if ((rc = solve_wait_status(h, status)) != FC_OK) return rc;
   set_status(status, FC_OK);
   return FC_OK;
 }
@@ -1394,6 +1881,7 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
+    if ((rc = solve_wait_status(h, status)) != FC_OK) return rc;
     double worst = 0.0;
     for (int j = 0; j < R; ++j) {
       const double bb = host[R + j];
@@ -1442,6 +1930,7 @@ int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *st
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(status, e, "solve");
+  if ((rc = solve_wait_status(h, status)) != FC_OK) return rc;
   set_status(status, FC_OK);
   return FC_OK;
 }
@@ -1486,6 +1975,8 @@ int64_t fc_chol_stat(const fc_chol *h, int what) {
     case 10: return (int64_t)h->gemm_flops_solve;
     case 11: return h->gemm_big_ordinal;
     case 12: return h->gemm_trail_ordinal;
+    case 13: return h->dag ? h->dag_fwd : 0;
+    case 14: return h->dag ? h->dag_bwd : 0;
   }
   return -1;
 }
@@ -1512,14 +2003,31 @@ int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kind
     launches[k] = 0;
   }
   for (auto &m : h->marks) {
-    if (m.first < 0 || m.first >= kinds) continue;
+    if (m.kind < 0 || m.kind >= kinds) continue;
     float t = 0;
-    if (cudaEventElapsedTime(&t, m.second.first, m.second.second) == cudaSuccess) ms[m.first] += t;
-    launches[m.first] += 1;
+    if (cudaEventElapsedTime(&t, m.a, m.b) == cudaSuccess) ms[m.kind] += t;
+    launches[m.kind] += 1;
   }
   h->marks.clear();
   h->events_used = 0;
   return FC_OK;
+}
+
+int64_t fc_chol_profile_launches(fc_chol *h, int32_t *kind, int32_t *level, int32_t *tasks, float *ms, int64_t cap) {
+  if (!h || cap < 0 || (cap > 0 && (!kind || !level || !tasks || !ms))) return -FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return -FC_CUDA_ERROR;
+  const int64_t count = (int64_t)h->marks.size();
+  for (int64_t i = 0; i < std::min(count, cap); ++i) {
+    const auto &m = h->marks[i];
+    kind[i] = m.kind;
+    level[i] = m.level;
+    tasks[i] = m.count;
+    ms[i] = 0;
+    cudaEventElapsedTime(&ms[i], m.a, m.b);
+  }
+  return count;
 }
 
 int fc_csr_spmv_device(int64_t n, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val, const double *d_x,

@@ -11,32 +11,15 @@
 #include <cstdio>
 
 #include "kernels.cuh"
+#include "tiles.cuh"
 
 namespace fc {
 
 namespace {
 
+using namespace tiles;
+
 constexpr double PIVOT_TOLERANCE = 1e-10;  // crates/solver/src/cholesky.rs:48
-
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem, const void *gmem, int src_bytes) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) { cp_async<8>(smem, gmem, src_bytes); }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-// D = A B + C on one 8x8x4 FP64 tile: a = A[g][tg], b = B[tg][g], c/d = C[g][2 tg + {0, 1}]
-// with g = lane / 4, tg = lane % 4.
-__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c[0]), "+d"(c[1])
-               : "d"(a), "d"(b));
-}
 
 // D = A B + C on one 16x8x8 FP64 tile (sm_90 and later): a = A[g][tg], A[g+8][tg], A[g][tg+4],
 // A[g+8][tg+4]; b = B[tg][g], B[tg+4][g]; c/d = C[g][2tg], C[g][2tg+1], C[g+8][2tg], C[g+8][2tg+1].
@@ -139,81 +122,6 @@ __global__ void scale_kernel(int64_t n, const int64_t *__restrict__ diag_src, co
   const int64_t ds = diag_src[j];
   const double d = ds >= 0 ? fabs(val[ds]) : 0.0;
   scale[j] = d > 0.0 ? 1.0 / sqrt(d) : 1.0;
-}
-
-// ---- shared-memory tiles and the DMMA product of two of them --------------------------------------
-// A tile holds 64 x 64 elements as [k][i] with a padded row stride: 68 doubles or 72 floats, so a
-// warp's fragment reads of 4 k-rows x 8 consecutive elements fall in distinct banks.
-template <class T>
-__host__ __device__ constexpr int tile_stride() {
-  return sizeof(T) == 8 ? 68 : 72;
-}
-constexpr int TS = 68;
-
-// dst[k * S + i] = src[i * si + k * sk] for i < rows, k < kk, zero for the other i < 64 and
-// kk <= k < kpad (rows k >= kpad of the tile are not touched). Issued as cp.async copies, so a
-// tile's loads are all in flight at once; the caller commits, waits and synchronises. One warp per
-// k (rows contiguous in memory) or one warp per i (k contiguous): every warp reads a contiguous run.
-template <class T>
-__device__ __forceinline__ void load_tile(T *dst, const T *__restrict__ src, int64_t si, int64_t sk, int rows, int kk,
-                                          int kpad) {
-  constexpr int S = tile_stride<T>();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (si == 1) {
-    for (int k = warp; k < kpad; k += nw)
-      for (int i = lane; i < 64; i += 32) {
-        const bool ok = i < rows && k < kk;
-        cp_async<sizeof(T)>(&dst[k * S + i], ok ? src + i + (int64_t)k * sk : src, ok ? (int)sizeof(T) : 0);
-      }
-  } else {
-    for (int i = warp; i < 64; i += nw)
-      for (int k = lane; k < kpad; k += 32) {
-        const bool ok = i < rows && k < kk;
-        cp_async<sizeof(T)>(&dst[k * S + i], ok ? src + (int64_t)i * si + k * sk : src, ok ? (int)sizeof(T) : 0);
-      }
-  }
-}
-
-// acc(i, j) += sum_{k < K} As[k][i] Bs[k][j] over a 64 x 64 output, 4 warps of 32 x 32, in FP64
-// (an FP32 A tile is widened as it is read).
-template <class TA>
-__device__ __forceinline__ void mma_tiles(const TA *As, const double *Bs, int K, double (&acc)[4][4][2]) {
-  constexpr int SA = tile_stride<TA>();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, tg = lane & 3;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  for (int kk = 0; kk < K; kk += 4) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) av[r] = (double)As[(kk + tg) * SA + wm + r * 8 + g];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) bv[c] = Bs[(kk + tg) * TS + wn + c * 8 + g];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) dmma(acc[r][c], av[r], bv[c]);
-  }
-}
-
-__device__ __forceinline__ void zero_acc(double (&acc)[4][4][2]) {
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
-}
-
-// Calls f(i, j, value) for every output of a 64 x 64 accumulator held by this thread.
-template <class F>
-__device__ __forceinline__ void each_acc(const double (&acc)[4][4][2], F f) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, tg = lane & 3;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) f(wm + r * 8 + g, wn + c * 8 + 2 * tg + e, acc[r][c][e]);
 }
 
 // ---- panel: factor the diagonal block, invert it, solve the rows below --------------------------
@@ -435,15 +343,52 @@ struct TileLoader {
   }
 };
 
-// Stores one output of a GEMM task by its flags: a partial (flag 4), -sum (flag 2), or C - sum.
+// Writes a GEMM task's 64 x 64 tile (acc[r][c][e] of the m16n8k8 fragments of a 32 x 32 warp
+// tile) by its flags: a partial (flag 4), -sum (flag 2), or C - sum. For C - sum every old value
+// is loaded before any store, so the loads are in flight together.
 template <class T, class V>
-__device__ __forceinline__ void gemm_out(T *dst, bool partial, bool store, V v) {
-  if (partial)
-    *dst = T(v);
-  else if (store)
-    *dst = T(-v);
-  else
-    *dst = T(*dst - v);
+__device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)[2][4][4], int wm, int wn, int g,
+                                              int tg) {
+  const int M = tp->M, N = tp->N;
+  const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
+  T *C = static_cast<T *>(tp->C);
+  const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
+  auto at = [&](int r, int c, int e, T *&dst) {
+    const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
+    dst = C + (int64_t)i * c_si + (int64_t)j * c_sj;
+    return i < M && j < N && (!lower || i >= j);
+  };
+  if (partial || store) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          T *dst;
+          if (at(r, c, e, dst)) *dst = T(partial ? acc[r][c][e] : -acc[r][c][e]);
+        }
+    return;
+  }
+  T old[2][4][4];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        T *dst;
+        old[r][c][e] = at(r, c, e, dst) ? *dst : T(0);
+      }
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        T *dst;
+        if (at(r, c, e, dst)) *dst = T(old[r][c][e] - acc[r][c][e]);
+      }
 }
 
 template <class TA>
@@ -510,20 +455,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
     }
   }
   cp_async_wait<0>();
-  const int M = tp->M, N = tp->N;
-  const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
-  double *C = static_cast<double *>(tp->C);
-  const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
-        if (i < M && j < N && (!lower || i >= j))
-          gemm_out(C + (int64_t)i * c_si + (int64_t)j * c_sj, partial, store, acc[r][c][e]);
-      }
+  gemm_epilogue<double>(tp, acc, wm, wn, g, tg);
 }
 
 // ---- tiled C -= A B^T in FP32 by 3xTF32 on the tensor pipe ---------------------------------------
@@ -597,20 +529,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_tf32x3_kernel(const Gemm
     }
   }
   cp_async_wait<0>();
-  const int M = tp->M, N = tp->N;
-  const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
-  float *C = static_cast<float *>(tp->C);
-  const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
-        if (i < M && j < N && (!lower || i >= j))
-          gemm_out(C + (int64_t)i * c_si + (int64_t)j * c_sj, partial, store, acc[r][c][e]);
-      }
+  gemm_epilogue<float>(tp, acc, wm, wn, g, tg);
 }
 
 // ---- the reduction of a split GEMM's partials, in a fixed order ----------------------------------
@@ -683,13 +602,11 @@ __host__ __device__ constexpr size_t solve_smem(int k4) {
 }
 
 template <bool BACKWARD, class T>
-__global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__restrict__ x, double *__restrict__ x2,
-                                                         double *__restrict__ v, const int64_t *__restrict__ voff, int R,
-                                                         const SolveTask *__restrict__ tasks, int k4max) {
-  extern __shared__ double sm[];
+__device__ __forceinline__ void solve_panel_body(const Tree &t, double *__restrict__ x, double *__restrict__ x2,
+                                                 double *__restrict__ v, const int64_t *__restrict__ voff, int R,
+                                                 const SolveTask &task, int k4max, double *sm) {
   double *inv = sm, *xs = sm + k4max * TS;
   T *bt = reinterpret_cast<T *>(sm + 2 * k4max * TS);
-  const SolveTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
   const T *Ls = static_cast<const T *>(t.L) + t.loff[s];
@@ -729,9 +646,16 @@ __global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__rest
     dst = x2 + (f + task.r0) * R + j0;
   else
     dst = task.r0 < w ? x + (f + task.r0) * R + j0 : v + voff[s] + (task.r0 - w) * R + j0;
-  each_acc(acc, [&](int i, int j, double val) {
-    if (i < rows && j < nj) dst[(int64_t)i * R + j] -= val;
-  });
+  sub_acc(acc, rows, nj, [&](int i, int j) { return dst + (int64_t)i * R + j; });
+}
+
+template <bool BACKWARD, class T>
+__global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__restrict__ x, double *__restrict__ x2,
+                                                         double *__restrict__ v, const int64_t *__restrict__ voff, int R,
+                                                         const SolveTask *__restrict__ tasks, int k4max) {
+  extern __shared__ double sm[];
+  const SolveTask task = tasks[blockIdx.x];
+  solve_panel_body<BACKWARD, T>(t, x, x2, v, voff, R, task, k4max, sm);
 }
 
 // x[i*R + j] = b[perm[i] + j*ld] (times scale[i] when scaled), and back.
@@ -842,6 +766,7 @@ void configure_kernels() {
   set_smem(gemm_kernel<double>, gemm_smem<double>());
   set_smem(gemm_kernel<float>, gemm_smem<float>());
   set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
+  configure_solve_dag();
   done = true;
 }
 

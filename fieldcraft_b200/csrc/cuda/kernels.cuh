@@ -88,6 +88,70 @@ struct RowTask {
   int32_t s, i0, i1, ranges;
 };
 
+// ---- the solve as one dependency-driven launch per direction ----------------------------------
+// Every CTA of a persistent grid takes the next task of a topologically ordered list (an atomic
+// ticket), waits until the task's dependencies are met (counters raised by the tasks it depends
+// on), does it, and raises the task's own counters. A task only waits on tasks taken before it, so
+// the list completes with any number of resident CTAs. Waits are bounded: past `limit_ns` the
+// waiting CTA records FC_TIMEOUT in the control block and every CTA drains the list without work.
+//
+// A supernode's front rows fall in chunks of at most 64 rows: chunk c < P is own columns
+// [64c, 64c + 64) (P panels of 64), chunk P + b is rows past the columns [w + 64b, w + 64b + 64).
+constexpr int32_t DAG_TIMEOUT = 7;  // the FC_TIMEOUT status code
+enum DagKind : int32_t {
+  DAG_ASSEMBLE = 0,  // forward: rows [i0, i1) (chunks [r0, r1)): zero the update rows, add the children
+  DAG_PANEL = 1,     // panel columns [i0, i1), front chunks [r0, r1) updated, one after another
+  DAG_NODE = 2,      // a whole small supernode: forward, assembly and every panel; backward, the
+                     // product with the rows past the columns and every panel
+  DAG_GEMM = 3,      // backward: own rows [i0, i1) -= L(w + k, rows)^T x(row k) for k in [r0, r1)
+  DAG_REDUCE = 4,    // backward: own rows [i0, i1) -= the `count` partial tiles from aux on, in order
+};
+// Panel tasks: keep = 1 applies the inverse of the diagonal block and stores the panel's result
+// (y in x2 forward, z in x backward), raising `sigmid` once it is stored; keep = -1 reads it from
+// there. A panel task raises counter sig0 + k sigstep after its k-th chunk; other tasks raise
+// sig0 + k sigstep for k < nsig at the end. Every task adds inc1 to sig1 at the end.
+struct DagTask {
+  int32_t kind, s, i0, i1, r0, r1, j0, j1;
+  int32_t keep, child, count;  // child: first record of the children's ranges (assembly)
+  int32_t dep0, dep1;          // [dep0, dep1) in the dependency list
+  int32_t sig0, sigstep, nsig, sig1, inc1, sigmid;
+  int32_t pad;
+  int64_t aux;  // panel: the diagonal block's offset in the diagonal arena; gemm, reduce: partial
+                // tile offset (-1: subtract in place)
+};
+struct DagDep {
+  int32_t counter, value;  // wait until counters[counter] >= value
+};
+// One child's rows [lo, hi) (of its rows past its columns) that land in an assembly task's rows.
+struct DagChild {
+  int64_t rel;  // offset of the child's relative map
+  int64_t v;    // offset of the child's update vectors
+  int32_t lo, hi;
+};
+struct DagControl {
+  int32_t next[2];  // tickets of the forward and the backward lists
+  int32_t error;    // 0, or the FC_* code of the first failed wait
+  int32_t task;     // the task whose wait failed
+};
+struct SolveDag {
+  const DagTask *tasks;
+  int32_t count;
+  const DagDep *deps;
+  const DagChild *children;
+  int32_t *counters;
+  DagControl *ctl;
+  double *x, *x2, *v, *part;
+  const int64_t *voff;
+  int32_t R;
+  long long limit_ns;
+  long long *trace;  // null, or per task: taken, ready and done times (ns), kind << 32 | SM
+};
+// Sets the persistent kernels' shared-memory limits (called by configure_kernels).
+void configure_solve_dag();
+// CTAs per SM of the solve's persistent kernel (for sizing its grid).
+int solve_dag_blocks_per_sm(bool fp32);
+void launch_solve_dag(const Tree &t, bool fp32, bool backward, const SolveDag &d, int grid, cudaStream_t st);
+
 // Device status word of a factorisation: the smallest failing pivot column (postorder).
 struct DeviceStatus {
   unsigned long long failed_column;  // ULLONG_MAX when none

@@ -151,17 +151,43 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
  * 7 kernels launched by the last factorisation, 8 kernels launched by the last solve, 9 flops of
  * the factor's GEMM tasks, 10 flops of the last solve plan's GEMM tasks, 11 the ordinal among the
  * factor's GEMM launches of the one with the most flops, 12 the same among the launches whose
- * tasks all have K <= 64 (the panels' updates of later columns). */
+ * tasks all have K <= 64 (the panels' updates of later columns), 13 and 14 the tasks of the
+ * persistent solve's forward and backward lists. */
 int64_t fc_chol_stat(const fc_chol *h, int what);
+
+/* Execution options of a handle (no reference counterpart). Each takes effect from the next solve.
+ *   FC_OPTION_SOLVE_SCHEDULE   0: the solve runs level by level, one launch per panel step
+ *                              (default); 1: as two persistent dependency-driven launches.
+ *   FC_OPTION_WAIT_LIMIT_NS    a wait of the persistent solve longer than this many nanoseconds
+ *                              fails the solve with FC_TIMEOUT (default 4e9).
+ *   FC_OPTION_PLANT_UNMET_WAIT (tests) value != 0: the next solve plan holds one dependency that no
+ *                              task meets, so that solve ends with FC_TIMEOUT after the limit.
+ *   FC_OPTION_TRACE            value != 0: the persistent solve records per task when it was taken,
+ *                              when its inputs were ready and when it was done (fc_chol_trace_read). */
+#define FC_OPTION_SOLVE_SCHEDULE 1
+#define FC_OPTION_WAIT_LIMIT_NS 2
+#define FC_OPTION_PLANT_UNMET_WAIT 3
+#define FC_OPTION_TRACE 4
+int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
+/* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
+ * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |
+ * SM index (kinds 0 assembly, 1 panel, 2 gather, 3 product, 4 reduction). Copies at most cap words;
+ * returns the number of tasks (0 when not tracing; negative: -FC_INVALID_ARGUMENT, -FC_CUDA_ERROR). */
+int64_t fc_chol_trace_read(fc_chol *h, int64_t *out, int64_t cap);
 
 /* Per-launch timing with CUDA events on the handle's stream (no reference counterpart: the
  * measurement hook of the benchmark). enable != 0 starts recording; fc_chol_profile_read waits for
  * the stream and returns, per launch kind, the summed milliseconds and the launch count (arrays of
- * `kinds` entries, 24 covers all), then clears them. Kinds: 0 front assembly, 1 panel (factor,
+ * `kinds` entries), then clears them. Kinds: 0 front assembly, 1 panel (factor,
  * invert and solve below a diagonal block), 3 GEMM of the factor; 18 reduction of split sums, 19 GEMM,
- * 20 front assembly, 21 gather, 22 forward panel, 23 backward panel of the solve. */
+ * 20 front assembly, 21 gather, 22 forward panel, 23 backward panel of the solve (level by level);
+ * 24 forward, 25 backward persistent launch of the solve (26 covers all). */
 int fc_chol_profile(fc_chol *h, int enable);
 int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kinds);
+/* The recorded launches one by one, oldest first, without clearing them: kind (as above), level
+ * of the supernodal tree, number of tasks (CTAs) and milliseconds. Fills at most cap entries and
+ * returns how many are recorded (negative: -FC_INVALID_ARGUMENT or -FC_CUDA_ERROR). */
+int64_t fc_chol_profile_launches(fc_chol *h, int32_t *kind, int32_t *level, int32_t *tasks, float *ms, int64_t cap);
 
 /* ---- compressed-row products (Csr::mul, crates/solver/src/sparse.rs:42-50) ---------------------
  * y = A x on the device for nrhs vectors, x and y column-major with leading dimension ld. */

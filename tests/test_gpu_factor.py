@@ -229,3 +229,43 @@ def test_mixed_precision_refines_to_the_fp64_answer(cuda, name, make, values_tol
     x64 = torch.zeros_like(b)
     rel64, its64 = f64.refine_solve_device(device_csr(torch, p.csr), b, x64, k, p.n, tol=1e-10, max_iter=5)
     assert np.all(rel64 <= 1e-10) and its64 <= 2
+
+
+@pytest.mark.parametrize("name,make", [("lognormal-12", lambda: problems.lognormal_block(12, nrhs=70)),
+                                       ("cantilever", problems.cantilever)], ids=["lognormal-12", "cantilever"])
+def test_solve_schedules_agree(cuda, name, make):
+    # the persistent dependency-driven solve and the level-by-level launches both match the
+    # oracle; the persistent one is bit-for-bit the same on every run (70 right-hand sides: two
+    # blocks of columns)
+    p = make()
+    up = p.upper()
+    f = Factor.new(up, 2**62)
+    _, ref = oracle_factor(p.csr)
+    exp = ref.solve(p.rhs.copy())
+    runs = []
+    for schedule in (1, 1, 0):
+        f.option(Factor.SOLVE_SCHEDULE, schedule)
+        x = np.asfortranarray(p.rhs.copy())
+        f.solve_many(x)
+        runs.append(x)
+        for j in range(x.shape[1]):
+            assert np.linalg.norm(x[:, j] - exp[:, j]) <= SOLVE_TOL * np.linalg.norm(exp[:, j]), (name, schedule, j)
+    assert np.array_equal(runs[0].view(np.uint64), runs[1].view(np.uint64))
+
+
+def test_solve_wait_limit_reports_timeout(cuda):
+    # a dependency that nothing meets ends the persistent solve with Timeout after the wait limit
+    # (the CTAs return; no fault), and the handle keeps working afterwards
+    from fieldcraft_b200 import Timeout
+    csr = H.panels_matrix()
+    f = Factor.new(UpperColumns.from_symmetric(csr), 2**62)
+    x = H.sin_solution(csr.n)
+    b = oracle.spmv(csr.n, csr.ptr, csr.idx, csr.val, x)
+    f.option(Factor.SOLVE_SCHEDULE, 1)
+    f.option(Factor.WAIT_LIMIT_NS, 50_000_000)
+    f.option(Factor.PLANT_UNMET_WAIT, 1)
+    with pytest.raises(Timeout):
+        f.solve(b.copy())
+    got = b.copy()
+    f.solve(got)
+    assert np.max(np.abs(got - x)) < 1e-12
