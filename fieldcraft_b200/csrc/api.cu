@@ -87,7 +87,9 @@ cudaError_t upload(DeviceBuf &buf, const std::vector<T> &host, cudaStream_t st) 
 
 enum Kind {
   K_ASSEMBLE, K_PANEL, K_REDUCE, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD,
-  K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD
+  K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD,
+  K_GEMM_MIXED,  // A in the factor's storage type, B and C FP64
+  K_GEMM_F64     // FP64 throughout (the diagonal blocks' inverses)
 };
 
 struct Launch {
@@ -109,6 +111,8 @@ struct fc_chol {
   int64_t n = 0, ns = 0, entries = 0, nnz = 0, levels = 0;
   double flops = 0;
   std::vector<int64_t> first, perm, loff, uoff, rows_off, toff, doff;
+  std::vector<int64_t> ioff;  // where each supernode's diagonal-block inverses start in Dinv
+  int64_t i_len = 0, t_len = 0;
   std::vector<int32_t> width, height, rows;
   std::vector<int64_t> kid_ptr;
   std::vector<int32_t> kids;
@@ -120,6 +124,7 @@ struct fc_chol {
   DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
   DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_D, d_perm, d_val, d_status, d_toff, d_doff;
   DeviceBuf d_a_row, d_a_col, d_scale;   // mixed precision only
+  DeviceBuf d_Dinv, d_T;                 // diagonal-block inverses; the doubling's products
   DeviceBuf d_ir_r, d_ir_d, d_ir_sum;    // iterative refinement workspace
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
   fc::Tree tree{};
@@ -228,6 +233,14 @@ void *arena_at(const DeviceBuf &buf, const fc_chol *h, int64_t off) {
   return static_cast<char *>(buf.p) + (size_t)off * h->esize;
 }
 
+// Block b (columns [b SB, b SB + bw)) of supernode s's diagonal-block inverses: its offset in
+// Dinv and its width (the leading dimension of its column-major bw x bw storage).
+int64_t inv_block(const fc_chol *h, int64_t s, int b, int &bw) {
+  const int w = h->width[s];
+  bw = std::min(fc::SB, w - b * fc::SB);
+  return h->ioff[s] + (int64_t)b * fc::SB * fc::SB;  // every earlier block is full
+}
+
 // Useful flops of a GEMM task (a diagonal tile computes its lower triangle only).
 double task_flops(const fc::GemmTask &g) {
   double outputs = (double)g.M * g.N;
@@ -292,6 +305,63 @@ int64_t arena_offsets(const fc_chol *h, const std::vector<std::vector<int64_t>> 
 
 // The factor's program: per level, assemble; per panel, the fused factor/invert/solve of the
 // panel, then the update of the later columns; then the update matrices.
+// The inverses of the diagonal blocks of the supernodes of one level, by doubling: from the
+// panels' 64 x 64 inverses, each step h (64, 128, ... < SB) joins neighbouring inverses A^-1 and
+// C^-1 of h columns into the inverse of [[A, 0], [B, C]], whose lower-left block is
+// -C^-1 (B A^-1). Step h is two GEMM launches: T = B A^-1 into the scratch T (first), then
+// -C^-1 T into Dinv (second); A^-1 and C^-1 are lower triangular, so the K ranges stop at the
+// triangle. Returns the scratch doubles the level needs (T may be null to size only).
+int64_t inverse_doubling(fc_chol *h, const std::vector<int64_t> &S, double *T, int step_h,
+                         std::vector<fc::GemmTask> *first, std::vector<fc::GemmTask> *second) {
+  auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
+  double *Dinv = h->d_Dinv.as<double>();
+  int64_t toff = 0;
+  const int hh = step_h;
+  for (int64_t s : S) {
+    const int w = h->width[s], m = h->height[s];
+    if (w <= hh) continue;
+    for (int b = 0; b * fc::SB < w; ++b) {
+      int bw;
+      const int64_t base = inv_block(h, s, b, bw);
+      const int scol = b * fc::SB;
+      for (int a0 = 0; a0 + hh < bw; a0 += 2 * hh) {
+        const int c0 = a0 + hh, hc = std::min(hh, bw - c0), ha = hh;
+        if (first && T) {
+          double *Tp = T + toff;
+          for (int i = 0; i < hc; i += 64)
+            for (int j = 0; j < ha; j += 64) {
+              fc::GemmTask g{};  // T(i, j) = sum_k L(c0 + i, a0 + k) Ainv(k, j), k >= j
+              g.C = Tp + i + (int64_t)j * hc;
+              g.c_si = 1, g.c_sj = hc;
+              g.A = Lp(h->loff[s] + (scol + c0 + i) + (int64_t)(scol + a0 + j) * m);
+              g.a_si = 1, g.a_sk = m;
+              g.B = Dinv + base + (a0 + j) + (int64_t)(a0 + j) * bw;
+              g.b_sj = bw, g.b_sk = 1;
+              g.M = std::min(64, hc - i), g.N = std::min(64, ha - j), g.K = ha - j;
+              g.flags = 4;
+              first->push_back(g);
+            }
+          for (int i = 0; i < hc; i += 64)
+            for (int j = 0; j < ha; j += 64) {
+              fc::GemmTask g{};  // X(i, j) = -sum_k Cinv(i, k) T(k, j), k <= i
+              g.C = Dinv + base + (c0 + i) + (int64_t)(a0 + j) * bw;
+              g.c_si = 1, g.c_sj = bw;
+              g.A = Dinv + base + (c0 + i) + (int64_t)c0 * bw;
+              g.a_si = 1, g.a_sk = bw;
+              g.B = Tp + (int64_t)j * hc;
+              g.b_sj = hc, g.b_sk = 1;
+              g.M = std::min(64, hc - i), g.N = std::min(64, ha - j), g.K = std::min(hc, i + 64);
+              g.flags = 2;
+              second->push_back(g);
+            }
+        }
+        toff += (int64_t)hc * ha;
+      }
+    }
+  }
+  return toff;
+}
+
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
                  std::vector<int2> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
@@ -320,9 +390,13 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         const int c1 = std::min(w, c0 + NB);
         p8max = std::max(p8max, (c1 - c0 + 7) / 8 * 8);
         const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
-        if (c1 >= m) panel_t.push_back({(int32_t)s, c0, c1, m, m, 1, doff});
+        int bw;
+        const int64_t ib = inv_block(h, s, c0 / fc::SB, bw), in = c0 % fc::SB;
+        const int64_t ioff = ib + in + in * bw;
+        if (c1 >= m) panel_t.push_back({(int32_t)s, c0, c1, m, m, 1, doff, ioff, bw, 0});
         for (int r0 = c1; r0 < m; r0 += fc::PANEL_ROWS)
-          panel_t.push_back({(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff});
+          panel_t.push_back(
+              {(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff, ioff, bw, 0});
         const int64_t lo = h->loff[s];
         for (int jc = c1; jc < w; jc += fc::GEMM_TN)
           for (int ic = jc; ic < m; ic += fc::GEMM_TM) {
@@ -340,6 +414,17 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       }
       push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l, p8max);
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+    }
+    for (int hh = NB; hh < fc::SB; hh *= 2) {
+      std::vector<fc::GemmTask> first, second;
+      inverse_doubling(h, S, h->d_T.as<double>(), hh, &first, &second);
+      if (first.empty()) break;
+      int64_t go = (int64_t)gemm_t.size();
+      gemm_t.insert(gemm_t.end(), first.begin(), first.end());
+      push(h->program, K_GEMM_MIXED, go, (int64_t)first.size(), (int)l);
+      go = (int64_t)gemm_t.size();
+      gemm_t.insert(gemm_t.end(), second.begin(), second.end());
+      push(h->program, K_GEMM_F64, go, (int64_t)second.size(), (int)l);
     }
     int64_t go = (int64_t)gemm_t.size();
     for (int64_t s : S) {
@@ -394,7 +479,8 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   h->uoff.resize(ns);
   h->toff.resize(ns);
   h->doff.resize(ns);
-  int64_t lsum = 0, usum = 0, tsum = 0, dsum = 0;
+  h->ioff.resize(ns);
+  int64_t lsum = 0, usum = 0, tsum = 0, dsum = 0, isum = 0;
   double flops = 0;
   for (int64_t s = 0; s < ns; ++s) {
     const int64_t m = sym.height(s), w = sym.width(s), u = m - w;
@@ -406,6 +492,11 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
     usum += u * u;
     tsum += fc::trapezoid(m, w);
     h->doff[s] = dsum;
+    h->ioff[s] = isum;
+    for (int64_t b = 0; b * fc::SB < w; ++b) {
+      const int64_t bw = std::min<int64_t>(fc::SB, w - b * fc::SB);
+      isum += bw * bw;
+    }
     {
       const int64_t full = w / fc::NB, last = w % fc::NB;
       dsum += 2 * (int64_t)fc::NB * fc::NB * full + 2 * last * last;
@@ -521,6 +612,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       h->d_U.alloc(h->esize * (size_t)std::max<int64_t>(usum, 1)) != cudaSuccess ||
       (h->fp32 && h->d_scale.alloc(sizeof(double) * (size_t)std::max<int64_t>(n, 1)) != cudaSuccess) ||
       h->d_D.alloc(sizeof(double) * (size_t)std::max<int64_t>(dsum, 1)) != cudaSuccess ||
+      h->d_Dinv.alloc(sizeof(double) * (size_t)std::max<int64_t>(isum, 1)) != cudaSuccess ||
       h->d_val.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->nnz, 1)) != cudaSuccess ||
       h->d_status.alloc(sizeof(fc::DeviceStatus)) != cudaSuccess) {
     Failure f;
@@ -552,6 +644,23 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   t.L = h->d_L.p;
   t.U = h->d_U.p;
   t.D = h->d_D.as<double>();
+  t.Dinv = h->d_Dinv.as<double>();
+  h->i_len = isum;
+  {
+    // the inverses' upper triangles stay zero; the doubling's scratch fits its largest level step
+    cudaError_t e = cudaMemsetAsync(h->d_Dinv.p, 0, sizeof(double) * (size_t)std::max<int64_t>(isum, 1), h->stream);
+    int64_t most = 0;
+    for (const auto &S : lv)
+      for (int hh = fc::NB; hh < fc::SB; hh *= 2) most = std::max(most, inverse_doubling(h, S, nullptr, hh, nullptr, nullptr));
+    h->t_len = most;
+    if (e != cudaSuccess || h->d_T.alloc(sizeof(double) * (size_t)std::max<int64_t>(most, 1)) != cudaSuccess) {
+      Failure f;
+      f.code = fc::OUT_OF_MEMORY;
+      f.entries = h->entries;
+      f.message = "device memory for the diagonal-block inverses";
+      return fail_status(st, f);
+    }
+  }
   std::vector<fc::AssembleTask> asm_t;
   std::vector<int2> ranges;
   std::vector<fc::PanelTask> panel_t;
@@ -690,6 +799,11 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
                          h->d_status.as<fc::DeviceStatus>(), l.width, st);
         break;
       case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, gk, st); break;
+      case K_GEMM_MIXED:
+        fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count,
+                        h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
+        break;
+      case K_GEMM_F64: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, fc::GemmKind::F64, st); break;
     }
     ++launches;
   }
@@ -753,12 +867,10 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
 }
 
 void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, double *part, SolvePlan &p) {
-  const int NB = fc::NB;
   std::vector<std::vector<int64_t>> lv(h->levels);
   for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
   const std::vector<int64_t> &voff = p.voff;
   std::vector<fc::RowTask> &rows = p.rows;
-  std::vector<fc::SolveTask> &panels = p.panels;
   std::vector<fc::GemmTask> &gemm = p.gemm;
   std::vector<Launch> &fwd = p.fwd, &bwd = p.bwd;
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
@@ -776,31 +888,59 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
       }
     }
     push(fwd, K_SOLVE_ASSEMBLE, ro, (int64_t)rows.size() - ro, (int)l);
-    int P = 0;
-    for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
-    for (int p = 0; p < P; ++p) {
-      int64_t po = (int64_t)panels.size();
-      int k4max = 4;
+    // blocks of SB columns: y = Dinv x (a GEMM with the block's inverse), then the front rows
+    // below the block -= L(rows, block) y
+    int K = 0;
+    for (int64_t s : S) K = std::max(K, (h->width[s] + fc::SB - 1) / fc::SB);
+    for (int k = 0; k < K; ++k) {
+      int64_t go = (int64_t)gemm.size();
       for (int64_t s : S) {
-        const int m = h->height[s], w = h->width[s], c0 = p * NB;
-        if (c0 >= w) continue;
-        const int c1 = std::min(w, c0 + NB);
-        k4max = std::max(k4max, (c1 - c0 + 3) / 4 * 4);
-        const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
-        for (int j0 = 0; j0 < R; j0 += 64) {
-          const int j1 = std::min(R, j0 + 64);
-          if (c1 >= m) panels.push_back({(int32_t)s, c0, c1, m, m, j0, j1, 1, doff});
-          bool first = true;
-          for (int i0 = c1; i0 < m;) {
-            const int lim = i0 < w ? std::min(m, w) : m;
-            const int i1 = std::min(lim, i0 + 64);
-            panels.push_back({(int32_t)s, c0, c1, i0, i1, j0, j1, first ? 1 : 0, doff});
-            first = false;
-            i0 = i1;
+        const int w = h->width[s];
+        const int64_t f = h->first[s];
+        if (k * fc::SB >= w) continue;
+        int bw;
+        const int64_t base = inv_block(h, s, k, bw);
+        const int c0 = k * fc::SB;
+        for (int i0 = 0; i0 < bw; i0 += 64)
+          for (int j0 = 0; j0 < R; j0 += 64) {
+            fc::GemmTask g{};
+            g.C = x2 + (f + c0 + i0) * R + j0;
+            g.c_si = R, g.c_sj = 1;
+            g.A = h->d_Dinv.as<double>() + base + i0;
+            g.a_si = 1, g.a_sk = bw;
+            g.B = x + (f + c0) * R + j0;
+            g.b_sj = 1, g.b_sk = R;
+            g.M = std::min(64, bw - i0), g.N = std::min(64, R - j0), g.K = std::min(bw, i0 + 64);
+            g.flags = 4;
+            gemm.push_back(g);
           }
+      }
+      push(fwd, K_SOLVE_FWD, go, (int64_t)gemm.size() - go, (int)l);
+      go = (int64_t)gemm.size();
+      for (int64_t s : S) {
+        const int w = h->width[s], m = h->height[s];
+        const int64_t f = h->first[s];
+        if (k * fc::SB >= w) continue;
+        int bw;
+        inv_block(h, s, k, bw);
+        const int c0 = k * fc::SB, c1 = c0 + bw;
+        for (int r0 = c1; r0 < m;) {
+          const int r1 = std::min(r0 < w ? w : m, r0 + 64);
+          for (int j0 = 0; j0 < R; j0 += 64) {
+            fc::GemmTask g{};
+            g.C = r0 < w ? x + (f + r0) * R + j0 : v + voff[s] + (int64_t)(r0 - w) * R + j0;
+            g.c_si = R, g.c_sj = 1;
+            g.A = Lp(h->loff[s] + r0 + (int64_t)c0 * m);
+            g.a_si = 1, g.a_sk = m;
+            g.B = x2 + (f + c0) * R + j0;
+            g.b_sj = 1, g.b_sk = R;
+            g.M = r1 - r0, g.N = std::min(64, R - j0), g.K = bw;
+            gemm.push_back(g);
+          }
+          r0 = r1;
         }
       }
-      push(fwd, K_SOLVE_FWD, po, (int64_t)panels.size() - po, (int)l, k4max);
+      push(fwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     }
   }
   // backward
@@ -849,25 +989,56 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
     }
     push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     push(bwd, K_REDUCE, ro2, (int64_t)p.reduce.size() - ro2, (int)l);
-    int P = 0;
-    for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
-    for (int p = P - 1; p >= 0; --p) {
-      int64_t po = (int64_t)panels.size();
-      int k4max = 4;
+    // blocks of SB columns from the last: z = Dinv^T x2 (into x), then the own rows above the
+    // block -= L(block, rows)^T z
+    int K = 0;
+    for (int64_t s : S) K = std::max(K, (h->width[s] + fc::SB - 1) / fc::SB);
+    for (int k = K - 1; k >= 0; --k) {
+      int64_t go = (int64_t)gemm.size();
       for (int64_t s : S) {
-        const int w = h->width[s], c0 = p * NB;
-        if (c0 >= w) continue;
-        const int c1 = std::min(w, c0 + NB);
-        k4max = std::max(k4max, (c1 - c0 + 3) / 4 * 4);
-        const int64_t doff = h->doff[s] + 2 * (int64_t)NB * NB * p;
-        for (int j0 = 0; j0 < R; j0 += 64) {
-          const int j1 = std::min(R, j0 + 64);
-          if (c0 == 0) panels.push_back({(int32_t)s, c0, c1, 0, 0, j0, j1, 1, doff});
-          for (int i0 = 0; i0 < c0; i0 += 64)
-            panels.push_back({(int32_t)s, c0, c1, i0, std::min(c0, i0 + 64), j0, j1, i0 == 0 ? 1 : 0, doff});
-        }
+        const int w = h->width[s];
+        const int64_t f = h->first[s];
+        if (k * fc::SB >= w) continue;
+        int bw;
+        const int64_t base = inv_block(h, s, k, bw);
+        const int c0 = k * fc::SB;
+        for (int i0 = 0; i0 < bw; i0 += 64)
+          for (int j0 = 0; j0 < R; j0 += 64) {
+            fc::GemmTask g{};
+            g.C = x + (f + c0 + i0) * R + j0;
+            g.c_si = R, g.c_sj = 1;
+            g.A = h->d_Dinv.as<double>() + base + i0 + (int64_t)i0 * bw;
+            g.a_si = bw, g.a_sk = 1;
+            g.B = x2 + (f + c0 + i0) * R + j0;
+            g.b_sj = 1, g.b_sk = R;
+            g.M = std::min(64, bw - i0), g.N = std::min(64, R - j0), g.K = bw - i0;
+            g.flags = 4;
+            gemm.push_back(g);
+          }
       }
-      push(bwd, K_SOLVE_BWD, po, (int64_t)panels.size() - po, (int)l, k4max);
+      push(bwd, K_SOLVE_BWD, go, (int64_t)gemm.size() - go, (int)l);
+      go = (int64_t)gemm.size();
+      for (int64_t s : S) {
+        const int w = h->width[s], m = h->height[s];
+        const int64_t f = h->first[s];
+        if (k * fc::SB >= w || k == 0) continue;
+        int bw;
+        inv_block(h, s, k, bw);
+        const int c0 = k * fc::SB;
+        for (int r0 = 0; r0 < c0; r0 += 64)
+          for (int j0 = 0; j0 < R; j0 += 64) {
+            fc::GemmTask g{};
+            g.C = x2 + (f + r0) * R + j0;
+            g.c_si = R, g.c_sj = 1;
+            g.A = Lp(h->loff[s] + c0 + (int64_t)r0 * m);
+            g.a_si = m, g.a_sk = 1;
+            g.B = x + (f + c0) * R + j0;
+            g.b_sj = 1, g.b_sk = R;
+            g.M = std::min(64, c0 - r0), g.N = std::min(64, R - j0), g.K = bw;
+            gemm.push_back(g);
+          }
+      }
+      if ((int64_t)gemm.size() > go) push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     }
   }
 }
@@ -1327,12 +1498,8 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st);
         break;
       case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
-      case K_SOLVE_FWD:
-        fc::launch_solve_panel(t, h->fp32, false, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
-        break;
-      case K_SOLVE_BWD:
-        fc::launch_solve_panel(t, h->fp32, true, b.x, b.x2, b.v, b.voff, R, b.panels + l.off, l.count, l.width, st);
-        break;
+      case K_SOLVE_FWD:  // the diagonal blocks' inverses applied (FP64 throughout)
+      case K_SOLVE_BWD: fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st); break;
       case K_GEMM:
         fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
         break;
@@ -1871,11 +2038,9 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
     int rc = enqueue_solve(h, d, R, n, status);
     if (rc != FC_OK) return rc;
     ++it;
-    for (int j = 0; j < R; ++j) fc::launch_update(n, 1, ld, d + (int64_t)j * n, d_x + (int64_t)j * ld, st);
-    for (int j = 0; j < R; ++j) {
-      fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x + (int64_t)j * ld, r + (int64_t)j * n, 1, n, st);
-      fc::launch_residual(n, 1, n, d_b + (int64_t)j * ld, r + (int64_t)j * n, st);
-    }
+    fc::launch_update(n, R, d, n, d_x, ld, st);
+    fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, r, n, R, st);
+    fc::launch_residual(n, R, d_b, ld, r, n, st);
     fc::launch_sumsq(n, R, n, r, sums, st);
     e = cudaMemcpyAsync(host.data(), sums, 2 * sizeof(double) * R, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -2033,7 +2198,7 @@ int64_t fc_chol_profile_launches(fc_chol *h, int32_t *kind, int32_t *level, int3
 int fc_csr_spmv_device(int64_t n, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val, const double *d_x,
                        double *d_y, int32_t nrhs, int64_t ld, void *stream) {
   if (n < 0 || nrhs < 0 || (n > 0 && (!d_ptr || !d_idx || !d_val || !d_x || !d_y || ld < n))) return FC_INVALID_ARGUMENT;
-  fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, d_y, nrhs, ld, (cudaStream_t)stream);
+  fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, d_y, ld, nrhs, (cudaStream_t)stream);
   return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
 }
 

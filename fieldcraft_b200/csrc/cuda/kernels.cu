@@ -278,11 +278,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
     __syncthreads();
   }
   if (task.keep) {
-    double *Dp = t.D + task.doff;
+    double *Dp = t.D + task.doff, *Ip = t.Dinv + task.ioff;
     for (int c = warp; c < pw; c += PANEL_THREADS / 32)
       for (int r = lane; r < pw; r += 32) {
         Dp[c * pw + r] = r >= c ? a[c * 65 + r] : 0.0;
         Dp[pw * pw + c * pw + r] = inv[c * TS + r];
+        Ip[(int64_t)c * task.ild + r] = r >= c ? inv[c * TS + r] : 0.0;
       }
     if (tid == 0 && fail < pw) atomicMin(&status->failed_column, (unsigned long long)(f + c0 + fail));
   }
@@ -592,72 +593,6 @@ __global__ void __launch_bounds__(256) solve_gather_kernel(Tree t, const double 
   }
 }
 
-// Panel [c0, c1) of supernode s for right-hand sides [j0, j1), with the inverse of its diagonal
-// block from the diagonal arena. Forward: y = Linv x_p (x -> x2), then the front rows [r0, r1)
-// below the panel -= L(rows, panel) y (own rows in x, rows past the columns in v). Backward:
-// z = Linv^T x2_p (x2 -> x), then the own rows [r0, r1) above -= L(panel, rows)^T z in x2.
-template <class T>
-__host__ __device__ constexpr size_t solve_smem(int k4) {
-  return sizeof(double) * 2 * k4 * TS + sizeof(T) * k4 * tile_stride<T>();
-}
-
-template <bool BACKWARD, class T>
-__device__ __forceinline__ void solve_panel_body(const Tree &t, double *__restrict__ x, double *__restrict__ x2,
-                                                 double *__restrict__ v, const int64_t *__restrict__ voff, int R,
-                                                 const SolveTask &task, int k4max, double *sm) {
-  double *inv = sm, *xs = sm + k4max * TS;
-  T *bt = reinterpret_cast<T *>(sm + 2 * k4max * TS);
-  const int s = task.s;
-  const int64_t m = t.height[s], w = t.width[s], f = t.first[s];
-  const T *Ls = static_cast<const T *>(t.L) + t.loff[s];
-  const double *Li = t.D + task.doff + (int64_t)(task.c1 - task.c0) * (task.c1 - task.c0);
-  const int c0 = task.c0, pw = task.c1 - task.c0, rows = task.r1 - task.r0, j0 = task.j0, nj = task.j1 - task.j0;
-  double *src = BACKWARD ? x2 : x;
-  double *out = BACKWARD ? x : x2;
-  const int K4 = (pw + 3) & ~3;
-  if (BACKWARD)
-    load_tile<double>(inv, Li, pw, 1, pw, pw, K4);  // inv[k][i] = Linv(k, i)
-  else
-    load_tile<double>(inv, Li, 1, pw, pw, pw, K4);  // inv[k][i] = Linv(i, k)
-  load_tile<double>(xs, src + (f + c0) * R + j0, 1, R, nj, pw, K4);
-  if (rows > 0) {
-    if (BACKWARD)
-      load_tile<T>(bt, Ls + c0 + task.r0 * m, m, 1, rows, pw, K4);  // bt[k][r] = L(c0 + k, r0 + r)
-    else
-      load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);  // bt[k][r] = L(r0 + r, c0 + k)
-  }
-  cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  double acc[4][4][2];
-  zero_acc(acc);
-  mma_tiles<double>(inv, xs, K4, acc);
-  __syncthreads();
-  each_acc(acc, [&](int i, int j, double val) {
-    if (i < K4) xs[i * TS + j] = val;
-    if (task.keep && i < pw && j < nj) out[(f + c0 + i) * R + j0 + j] = val;
-  });
-  if (rows <= 0) return;
-  __syncthreads();
-  zero_acc(acc);
-  mma_tiles<T>(bt, xs, K4, acc);
-  double *dst;
-  if (BACKWARD)
-    dst = x2 + (f + task.r0) * R + j0;
-  else
-    dst = task.r0 < w ? x + (f + task.r0) * R + j0 : v + voff[s] + (task.r0 - w) * R + j0;
-  sub_acc(acc, rows, nj, [&](int i, int j) { return dst + (int64_t)i * R + j; });
-}
-
-template <bool BACKWARD, class T>
-__global__ void __launch_bounds__(128) solve_panel_kernel(Tree t, double *__restrict__ x, double *__restrict__ x2,
-                                                         double *__restrict__ v, const int64_t *__restrict__ voff, int R,
-                                                         const SolveTask *__restrict__ tasks, int k4max) {
-  extern __shared__ double sm[];
-  const SolveTask task = tasks[blockIdx.x];
-  solve_panel_body<BACKWARD, T>(t, x, x2, v, voff, R, task, k4max, sm);
-}
-
 // x[i*R + j] = b[perm[i] + j*ld] (times scale[i] when scaled), and back.
 __global__ void permute_in_kernel(const int64_t *__restrict__ perm, int64_t n, const double *__restrict__ b,
                                   int64_t ld, double *__restrict__ x, int R, const double *__restrict__ scale) {
@@ -680,34 +615,55 @@ __global__ void permute_out_kernel(const int64_t *__restrict__ perm, int64_t n, 
   }
 }
 
-// y = A x: one row per thread, each row summed in column order (crates/solver/src/sparse.rs:42-50).
-__global__ void spmv_kernel(int64_t n, const int64_t *__restrict__ ptr, const int32_t *__restrict__ idx,
-                            const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y, int R,
-                            int64_t ld) {
-  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  if (r >= n || j >= R) return;
-  const double *xj = x + j * ld;
-  double acc = -0.0;
-  for (int64_t p = ptr[r]; p < ptr[r + 1]; ++p) acc += val[p] * xj[idx[p]];
-  y[r + j * ld] = acc;
-}
-
-// The refinement's vector steps on column-major n x R blocks with leading dimension ld:
-// r = b - Ax (residual) and x += d (update).
-__global__ void residual_kernel(int64_t n, int R, int64_t ld, const double *__restrict__ b, double *__restrict__ ax) {
-  const int64_t total = n * R;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e % n, j = e / n;
-    ax[i + j * ld] = b[i + j * ld] - ax[i + j * ld];
+// y = A x for RB right-hand sides at once: one warp per row, its lanes over the row's entries
+// (so a warp reads the row's indices and values once, contiguously, for all RB vectors), then a
+// butterfly sum of the lanes. x and y are column-major with leading dimensions ldx and ldy.
+template <int RB>
+__global__ void __launch_bounds__(256) spmv_kernel(int64_t n, const int64_t *__restrict__ ptr,
+                                                   const int32_t *__restrict__ idx, const double *__restrict__ val,
+                                                   const double *__restrict__ x, int64_t ldx, double *__restrict__ y,
+                                                   int64_t ldy, int R) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int j0 = blockIdx.y * RB;
+  if (row >= n) return;
+  const int nb = min(RB, R - j0);
+  const double *xj = x + j0 * ldx;
+  double acc[RB];
+#pragma unroll
+  for (int j = 0; j < RB; ++j) acc[j] = 0.0;
+  for (int64_t p = ptr[row] + lane; p < ptr[row + 1]; p += 32) {
+    const double v = val[p];
+    const int64_t c = idx[p];
+#pragma unroll
+    for (int j = 0; j < RB; ++j)
+      if (j < nb) acc[j] += v * xj[c + j * ldx];
+  }
+#pragma unroll
+  for (int j = 0; j < RB; ++j) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    if (lane == j && j < nb) y[row + (j0 + j) * ldy] = acc[j];
   }
 }
 
-__global__ void update_kernel(int64_t n, int R, int64_t ld, const double *__restrict__ d, double *__restrict__ x) {
+// The refinement's vector steps on column-major n x R blocks: r = b - Ax (residual, in place of
+// Ax) and x += d (update), each block with its own leading dimension.
+__global__ void residual_kernel(int64_t n, int R, const double *__restrict__ b, int64_t ldb, double *__restrict__ ax,
+                                int64_t ldax) {
   const int64_t total = n * R;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = e % n, j = e / n;
-    x[i + j * ld] += d[i + j * ld];
+    ax[i + j * ldax] = b[i + j * ldb] - ax[i + j * ldax];
+  }
+}
+
+__global__ void update_kernel(int64_t n, int R, const double *__restrict__ d, int64_t ldd, double *__restrict__ x,
+                              int64_t ldx) {
+  const int64_t total = n * R;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % n, j = e / n;
+    x[i + j * ldx] += d[i + j * ldd];
   }
 }
 
@@ -759,10 +715,6 @@ void configure_kernels() {
   if (done) return;
   set_smem(panel_kernel<double>, panel_smem<double>(64));
   set_smem(panel_kernel<float>, panel_smem<float>(64));
-  set_smem(solve_panel_kernel<false, double>, solve_smem<double>(64));
-  set_smem(solve_panel_kernel<true, double>, solve_smem<double>(64));
-  set_smem(solve_panel_kernel<false, float>, solve_smem<float>(64));
-  set_smem(solve_panel_kernel<true, float>, solve_smem<float>(64));
   set_smem(gemm_kernel<double>, gemm_smem<double>());
   set_smem(gemm_kernel<float>, gemm_smem<float>());
   set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
@@ -817,25 +769,6 @@ void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_
   if (count > 0) solve_gather_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks);
 }
 
-void launch_solve_panel(const Tree &t, bool fp32, bool backward, double *x, double *x2, double *v, const int64_t *voff,
-                        int R, const SolveTask *tasks, int count, int k4max, cudaStream_t st) {
-  if (count <= 0) return;
-  configure_kernels();
-  if (fp32) {
-    const size_t smem = solve_smem<float>(k4max);
-    if (backward)
-      solve_panel_kernel<true, float><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
-    else
-      solve_panel_kernel<false, float><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
-  } else {
-    const size_t smem = solve_smem<double>(k4max);
-    if (backward)
-      solve_panel_kernel<true, double><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
-    else
-      solve_panel_kernel<false, double><<<count, 128, smem, st>>>(t, x, x2, v, voff, R, tasks, k4max);
-  }
-}
-
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
                        const double *scale, cudaStream_t st) {
   const int64_t total = n * R;
@@ -852,23 +785,24 @@ void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, 
   permute_out_kernel<<<blocks, 256, 0, st>>>(perm, n, x, R, b, ld, scale);
 }
 
-void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, double *y,
-                 int R, int64_t ld, cudaStream_t st) {
+void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, int64_t ldx,
+                 double *y, int64_t ldy, int R, cudaStream_t st) {
   if (n <= 0 || R <= 0) return;
-  dim3 grid((unsigned)((n + 127) / 128), (unsigned)R);
-  spmv_kernel<<<grid, 128, 0, st>>>(n, ptr, idx, val, x, y, R, ld);
+  constexpr int RB = 8;
+  dim3 grid((unsigned)((n + 7) / 8), (unsigned)((R + RB - 1) / RB));
+  spmv_kernel<RB><<<grid, 256, 0, st>>>(n, ptr, idx, val, x, ldx, y, ldy, R);
 }
 
-void launch_residual(int64_t n, int R, int64_t ld, const double *b, double *ax, cudaStream_t st) {
+void launch_residual(int64_t n, int R, const double *b, int64_t ldb, double *ax, int64_t ldax, cudaStream_t st) {
   const int64_t total = n * R;
   if (total <= 0) return;
-  residual_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, ld, b, ax);
+  residual_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, b, ldb, ax, ldax);
 }
 
-void launch_update(int64_t n, int R, int64_t ld, const double *d, double *x, cudaStream_t st) {
+void launch_update(int64_t n, int R, const double *d, int64_t ldd, double *x, int64_t ldx, cudaStream_t st) {
   const int64_t total = n * R;
   if (total <= 0) return;
-  update_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, ld, d, x);
+  update_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, d, ldd, x, ldx);
 }
 
 void launch_sumsq(int64_t n, int R, int64_t ld, const double *v, double *out, cudaStream_t st) {

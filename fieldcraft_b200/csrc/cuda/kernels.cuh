@@ -16,6 +16,11 @@ constexpr int PANEL_ROWS = 64;  // rows of a panel solved by one CTA
 constexpr int ASSEMBLE_COLS = 8;  // front columns assembled by one CTA
 constexpr int ASSEMBLE_THREADS = 128;
 constexpr int SPLIT_K = 512;  // K chunk of a split GEMM (a long sum over few outputs)
+// The solve applies the inverse of a supernode's diagonal block SB columns at a time: the inverses
+// of its diagonal blocks of up to SB columns are formed during the factorisation (from the 64 x 64
+// inverses of the panels, by doubling), so a solve step is a GEMM over SB columns, not a chain of
+// SB / 64 dependent panel steps.
+constexpr int SB = 1024;
 
 // Where each supernode lives on the device. A front of supernode s has m = rows(s) rows and
 // w = width(s) columns of L; its update matrix U_s is the (m-w) x (m-w) Schur complement.
@@ -43,6 +48,8 @@ struct Tree {
   void *L;                  // L panels and update matrices: double, or float in mixed precision
   void *U;
   double *D;
+  double *Dinv;             // inverses of the diagonal blocks of up to SB columns (column-major,
+                            // lower triangular, zero above)
 };
 
 // Front columns [j0, j1) of supernode s; ranges[q] (from `ranges`) is child q's columns (in its
@@ -57,6 +64,8 @@ struct AssembleTask {
 struct PanelTask {
   int32_t s, c0, c1, r0, r1, keep;
   int64_t doff;
+  int64_t ioff;  // keep task: where the block's inverse goes in Dinv (leading dimension ild)
+  int32_t ild, pad;
 };
 // C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands. Flags: 1 touches
 // i >= j only (a diagonal tile of a symmetric matrix); 2 stores C = -sum instead of subtracting;
@@ -179,24 +188,19 @@ void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *v
                            const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st);
 void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R,
                          const RowTask *tasks, int count, cudaStream_t st);
-// Forward: y = L_pp^-1 x_p into x2, then x (own rows) / v (rows past the columns) -= L y.
-// Backward: z = L_pp^-T x2_p into x, then x2 (own rows above) -= L^T z.
-// k4max: the widest panel of the launch, rounded up to a multiple of 4.
-void launch_solve_panel(const Tree &t, bool fp32, bool backward, double *x, double *x2, double *v,
-                        const int64_t *voff, int R, const SolveTask *tasks, int count, int k4max, cudaStream_t st);
 // x_post[i*R + j] = b[perm[i] + j*ld] (times scale[i] if given) and back.
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
                        const double *scale, cudaStream_t st);
 void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, double *b, int64_t ld,
                         const double *scale, cudaStream_t st);
-// Iterative refinement on column-major n x R blocks (leading dimension ld): ax <- b - ax,
-// x <- x + d, out[j] <- sum of squares of column j.
-void launch_residual(int64_t n, int R, int64_t ld, const double *b, double *ax, cudaStream_t st);
-void launch_update(int64_t n, int R, int64_t ld, const double *d, double *x, cudaStream_t st);
+// Iterative refinement on column-major n x R blocks, each with its own leading dimension:
+// ax <- b - ax, x <- x + d, out[j] <- sum of squares of column j.
+void launch_residual(int64_t n, int R, const double *b, int64_t ldb, double *ax, int64_t ldax, cudaStream_t st);
+void launch_update(int64_t n, int R, const double *d, int64_t ldd, double *x, int64_t ldx, cudaStream_t st);
 void launch_sumsq(int64_t n, int R, int64_t ld, const double *v, double *out, cudaStream_t st);
-// y = A x for column-major x, y (leading dimension ld).
-void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x,
-                 double *y, int R, int64_t ld, cudaStream_t st);
+// y = A x for column-major x, y (leading dimensions ldx, ldy).
+void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, int64_t ldx,
+                 double *y, int64_t ldy, int R, cudaStream_t st);
 // Copies the L panels out into the reference's packed trapezoids (dst offsets per supernode).
 void launch_pack_trapezoids(const Tree &t, bool fp32, int64_t ns, const int64_t *toff, double *dst,
                             cudaStream_t st);
