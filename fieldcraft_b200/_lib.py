@@ -70,6 +70,20 @@ SIGNATURES = {
     "fc_fill_reducing_order": (i32, [i64, P, P, P, P]),
     "fc_fill": (i64, [i64, P, P, P]),
     "fc_hex8_stiffness": (i32, [P, f64, f64, P]),
+    # fieldcraft_unet.h
+    "fc_unet_create": (i32, [i32, i32, i32, i64, P, P, f64, u64, i32, C.POINTER(P), C.POINTER(Status)]),
+    "fc_unet_destroy": (None, [P]),
+    "fc_unet_set_stream": (i32, [P, P]),
+    "fc_unet_param_count": (i64, [P]),
+    "fc_unet_get_params": (i32, [P, P]),
+    "fc_unet_set_params": (i32, [P, P]),
+    "fc_unet_get_grads": (i32, [P, P]),
+    "fc_unet_forward_grid": (i32, [P, P, P]),
+    "fc_unet_backward_grid": (i32, [P, P]),
+    "fc_unet_apply": (i32, [P, P, P]),
+    "fc_unet_train_step": (i32, [P, P, P, P, P, P, C.c_float, i32, P]),
+    "fc_fcg_solve": (i32, [P, P, i64, P, P, P, P, P, f64, i32, i32, C.POINTER(i32), C.POINTER(f64), C.POINTER(i32),
+                           C.POINTER(Status)]),
 }
 
 _lib = None

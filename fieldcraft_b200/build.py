@@ -35,7 +35,7 @@ def _nvcc() -> str:
 
 def _sources():
     host = sorted((CSRC / "host").glob("*.cpp"))
-    cuda = sorted((CSRC / "cuda").glob("*.cu")) + [CSRC / "api.cu"]
+    cuda = sorted((CSRC / "cuda").glob("*.cu")) + sorted(CSRC.glob("*.cu"))
     headers = sorted(CSRC.rglob("*.cuh")) + sorted(CSRC.rglob("*.hpp")) + sorted((ROOT / "include").glob("*.h"))
     return host, cuda, headers
 

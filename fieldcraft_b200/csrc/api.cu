@@ -21,6 +21,7 @@
 
 #include "../../include/fieldcraft_chol.h"
 #include "cuda/kernels.cuh"
+#include "device_buf.hpp"
 #include "host/symbolic.hpp"
 
 struct fc_symbolic {
@@ -30,59 +31,13 @@ struct fc_symbolic {
 namespace {
 
 using fc::Failure;
-
-void set_status(fc_status *st, int code, int64_t column = -1, int64_t entries = 0, int64_t limit = 0,
-                const std::string &msg = std::string()) {
-  if (!st) return;
-  st->code = code;
-  st->reserved = 0;
-  st->column = column;
-  st->entries = entries;
-  st->limit = limit;
-  std::snprintf(st->message, sizeof(st->message), "%s", msg.c_str());
-}
+using fc::host::DeviceBuf;
+using fc::host::set_status;
+using fc::host::upload;
 
 int fail_status(fc_status *st, const Failure &f) {
   set_status(st, f.code, f.column, f.entries, f.limit, f.message);
   return f.code;
-}
-
-// A device allocation owned by a handle.
-struct DeviceBuf {
-  void *p = nullptr;
-  size_t bytes = 0;
-  DeviceBuf() = default;
-  DeviceBuf(const DeviceBuf &) = delete;
-  DeviceBuf &operator=(const DeviceBuf &) = delete;
-  ~DeviceBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  cudaError_t alloc(size_t b) {
-    release();
-    if (b == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      cudaGetLastError();
-      return e;
-    }
-    bytes = b;
-    return cudaSuccess;
-  }
-  template <class T>
-  T *as() const {
-    return static_cast<T *>(p);
-  }
-};
-
-template <class T>
-cudaError_t upload(DeviceBuf &buf, const std::vector<T> &host, cudaStream_t st) {
-  cudaError_t e = buf.alloc(sizeof(T) * host.size());
-  if (e != cudaSuccess || host.empty()) return e;
-  return cudaMemcpyAsync(buf.p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, st);
 }
 
 enum Kind {

@@ -25,6 +25,7 @@ class Problem:
     eq: np.ndarray          # equation of each mesh DOF (3 per node), -1 when held
     nodes_xyz: np.ndarray   # [nodes, 3]
     rhs: np.ndarray = field(default=None)  # [n, nrhs], Fortran order
+    young: np.ndarray = field(default=None)  # element moduli (when the workload keeps them)
 
     @property
     def n(self) -> int:
@@ -160,3 +161,53 @@ def uneven_boxes(count: int = 256, lo: int = 4, hi: int = 24, nrhs: int = 8, see
             rhs[:, r] = nodal_load(p, top, rng.standard_normal((top.size, 3)))
         p.rhs = rhs
         yield p
+
+
+def plate(nx: int = 128, ny: int = 128, nz: int = 8, corr: float = 8.0, contrast: float = 100.0, seed: int = 5,
+          nrhs: int = 1) -> Problem:
+    """The learned-preconditioner workload: an nx x ny x nz plate of unit hex8 elements, E from a
+    seeded lognormal Gaussian random field (correlation `corr` elements, E at +-3 sigma spanning
+    `contrast`), nu = 0.3, the four side faces clamped, `nrhs` random top-face pressures (a
+    smooth random field of vertical nodal forces). p.young holds the element moduli."""
+    g = gaussian_field((nz, ny, nx), corr, seed)
+    young = 210000.0 * np.exp(np.log(contrast) / 6.0 * g).reshape(-1)
+    i, j, k = node_grid(nx, ny, nz)
+    clamped = (i == 0) | (i == nx) | (j == 0) | (j == ny)
+    p = box(nx, ny, nz, float(nx), float(ny), float(nz), young, 0.3, clamped, name=f"plate-{nx}x{ny}x{nz}")
+    p.young = young
+    p.rhs = top_pressures(p, nrhs, seed + 1)
+    return p
+
+
+def top_pressures(p: Problem, count: int, seed: int) -> np.ndarray:
+    """`count` random top-face pressure loads: vertical nodal forces from a smooth random field
+    (correlation 8 nodes) over the top nodes, each column scaled to unit norm."""
+    nx, ny, nz = p.dims
+    i, j, k = node_grid(nx, ny, nz)
+    top = np.nonzero(k == nz)[0]
+    rng = np.random.default_rng(seed)
+    out = np.empty((p.n, count), order="F")
+    for c in range(count):
+        field = gaussian_field((ny + 1, nx + 1), 8.0, int(rng.integers(1 << 31))).reshape(-1)
+        vec = np.zeros((top.size, 3))
+        vec[:, 2] = -(1.0 + 0.5 * field)
+        f = nodal_load(p, top, vec)
+        out[:, c] = f / np.linalg.norm(f)
+    return out
+
+
+def node_feature(p: Problem) -> np.ndarray:
+    """Per node: the mean log Young's modulus of the elements around it, standardised (the
+    learned preconditioner's fixed input channel)."""
+    nx, ny, nz = p.dims
+    le = np.log(np.broadcast_to(np.asarray(p.young, np.float64), (nx * ny * nz,))).reshape(nz, ny, nx)
+    acc = np.zeros((nz + 1, ny + 1, nx + 1))
+    cnt = np.zeros_like(acc)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                acc[dz:dz + nz, dy:dy + ny, dx:dx + nx] += le
+                cnt[dz:dz + nz, dy:dy + ny, dx:dx + nx] += 1
+    f = acc / cnt
+    sd = f.std()
+    return ((f - f.mean()) / (sd if sd > 0 else 1.0)).reshape(-1).astype(np.float32)

@@ -1,0 +1,163 @@
+"""The learned preconditioner and flexible CG (include/fieldcraft_unet.h), for the same K u = f the
+Cholesky factor solves. No reference counterpart: the reference is a direct solver only
+(docs/linear-solvers.md:375-376). The Cholesky factor produces the training pairs (r, K^-1 r), is
+the fallback when FCG does not converge, and judges FCG's error.
+
+Device arrays are CUDA tensors (torch is only the allocator here); the network's forward and
+backward passes, Adam and FCG run on this library's kernels."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .cholesky import Factor, Status, raise_for
+from .problems import Problem, node_feature
+
+
+def _p(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+class UNet:
+    """The 3-level, 32-channel 3D-convolution U-Net on the node grid of a box problem."""
+
+    def __init__(self, problem: Problem, seed: int = 0, device: int = 0, kref: float | None = None):
+        lib = _lib.load()
+        nx, ny, nz = problem.dims
+        if kref is None:
+            csr = problem.csr
+            rows = np.repeat(np.arange(csr.n), np.diff(csr.ptr))
+            kref = float(np.mean(csr.val[csr.idx == rows]))
+        self.kref = float(kref)
+        eq = np.ascontiguousarray(problem.eq, np.int64)
+        feat = node_feature(problem)
+        st = Status()
+        h = C.c_void_p()
+        lib.fc_unet_create(nx, ny, nz, problem.n, _lib.ptr(eq), _lib.ptr(feat), self.kref, seed, device, C.byref(h),
+                           C.byref(st))
+        raise_for(st)
+        self.handle = h
+        self.n = problem.n
+        self.voxels = (nx + 1) * (ny + 1) * (nz + 1)
+
+    def set_stream(self, stream_ptr: int | None):
+        _lib.load().fc_unet_set_stream(self.handle, C.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def param_count(self) -> int:
+        return int(_lib.load().fc_unet_param_count(self.handle))
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), np.float32)
+        if _lib.load().fc_unet_get_params(self.handle, _lib.ptr(out)) != 0:
+            raise RuntimeError("fc_unet_get_params")
+        return out
+
+    def set_params(self, flat: np.ndarray):
+        v = np.ascontiguousarray(flat, np.float32)
+        if v.size != self.param_count() or _lib.load().fc_unet_set_params(self.handle, _lib.ptr(v)) != 0:
+            raise ValueError("parameter vector")
+
+    def grads(self) -> np.ndarray:
+        out = np.empty(self.param_count(), np.float32)
+        if _lib.load().fc_unet_get_grads(self.handle, _lib.ptr(out)) != 0:
+            raise RuntimeError("fc_unet_get_grads")
+        return out
+
+    def forward_grid(self, x, y):
+        """y = net(x) on device FP32 grids [voxels, 16]."""
+        if _lib.load().fc_unet_forward_grid(self.handle, _p(x), _p(y)) != 0:
+            raise RuntimeError("fc_unet_forward_grid")
+
+    def backward_grid(self, dy):
+        if _lib.load().fc_unet_backward_grid(self.handle, _p(dy)) != 0:
+            raise RuntimeError("fc_unet_backward_grid")
+
+    def apply(self, r, z):
+        """z = M(r) for device FP64 equation vectors."""
+        if _lib.load().fc_unet_apply(self.handle, _p(r), _p(z)) != 0:
+            raise RuntimeError("fc_unet_apply")
+
+    def train_step(self, r, e, lr: float, step: int, loss=None, csr_device=None):
+        """One Adam step on the pair (r, e = K^-1 r); with csr_device = (ptr, idx, val) of K the loss
+        is the energy norm of the error, else its Euclidean norm (both relative)."""
+        k = [_p(a) for a in csr_device] if csr_device is not None else [None, None, None]
+        if _lib.load().fc_unet_train_step(self.handle, _p(r), _p(e), *k, C.c_float(lr), int(step),
+                                          _p(loss) if loss is not None else None) != 0:
+            raise RuntimeError("fc_unet_train_step")
+
+    def close(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                _lib.load().fc_unet_destroy(h)
+            except TypeError:
+                pass
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
+def fcg(csr_device, b, x, net: UNet | None = None, fallback: Factor | None = None, tol: float = 1e-10,
+        max_iter: int = 1000, keep: int = 4):
+    """Flexible CG on K x = b (device FP64 vectors; csr_device = (ptr, idx, val) CUDA tensors),
+    preconditioned by `net` (None: plain CG), with the Cholesky `fallback`. Returns (iterations,
+    relative residual, used_fallback); raises Timeout when neither reached tol."""
+    ptr, idx, val = csr_device
+    it, rel, fb = C.c_int32(0), C.c_double(0.0), C.c_int32(0)
+    st = Status()
+    _lib.load().fc_fcg_solve(net.handle if net else None, fallback.handle if fallback else None, int(b.numel()),
+                             _p(ptr), _p(idx), _p(val), _p(b), _p(x), float(tol), int(max_iter), int(keep),
+                             C.byref(it), C.byref(rel), C.byref(fb), C.byref(st))
+    raise_for(st)
+    return it.value, rel.value, bool(fb.value)
+
+
+def training_pairs(factor: Factor, problem: Problem, count: int, seed: int, torch, block: int = 64):
+    """`count` pairs (r, K^-1 r) from the Cholesky solve: half white-noise residuals, half random
+    top-face pressures, each r of unit norm. Returns two CUDA tensors [count, n] (FP64)."""
+    from .problems import top_pressures
+    n = problem.n
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    R = torch.empty((count, n), dtype=torch.float64, device="cuda")
+    half = count // 2
+    R[:half] = torch.randn((half, n), dtype=torch.float64, device="cuda", generator=g)
+    R[half:] = torch.from_numpy(np.ascontiguousarray(top_pressures(problem, count - half, seed + 7).T)).cuda()
+    R /= torch.linalg.vector_norm(R, dim=1, keepdim=True)
+    E = R.clone()
+    for s in range(0, count, block):
+        e = min(count, s + block)
+        factor.solve_device(E[s:e], e - s, n)  # rows of E are column-major right-hand sides
+    torch.cuda.synchronize()
+    return R, E
+
+
+def output_scale(R, E) -> float:
+    """The network's output scale for pairs (r, K^-1 r): the median of ||r|| / ||e||, so that the
+    network's outputs are of order one."""
+    import torch
+    return float(torch.median(torch.linalg.vector_norm(R, dim=1) / torch.linalg.vector_norm(E, dim=1)).item())
+
+
+def train(net: UNet, R, E, epochs: int, lr: float, torch, seed: int = 0, lr_decay: float = 0.3, csr_device=None,
+          warmup: int = 200):
+    """Adam over the pairs for `epochs` passes in a seeded order (one pair per step); the learning
+    rate ramps up over the first `warmup` steps and steps down by lr_decay for the last epoch.
+    Returns the mean loss of each epoch."""
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    losses = []
+    rng = np.random.default_rng(seed)
+    step = 0
+    count = R.shape[0]
+    for ep in range(epochs):
+        acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+        rate = lr * (lr_decay if epochs > 1 and ep == epochs - 1 else 1.0)
+        for i in rng.permutation(count):
+            step += 1
+            net.train_step(R[i], E[i], rate * min(1.0, step / warmup), step, loss, csr_device)
+            acc += loss
+        losses.append(float(acc.item()) / count)
+    return losses

@@ -1,0 +1,103 @@
+"""The learned preconditioner on the GPU: the network's forward and backward kernels against the
+CPU oracle (oracle/unet_oracle.py, with the same BF16 rounding points), its training on pairs from
+the Cholesky solve, and what it gains flexible CG over plain CG, with the Cholesky fallback.
+
+Tolerances: BF16 keeps 8 bits; the GPU sums in FP32 in another order than the oracle, which moves
+some BF16 roundings by one unit: outputs agree to 2e-2 of their largest entry, each layer's
+gradients to 2e-2 in norm (and every entry to 0.1 of the layer's largest); the first two layers'
+gradients, which carry the rounding of every layer above them, to 5e-2 in norm."""
+import numpy as np
+import pytest
+
+from fieldcraft_b200 import Factor, Symbolic, problems
+from oracle import unet_oracle as U
+
+pytestmark = pytest.mark.gpu
+TOL = 2e-2
+
+
+def small_plate(nx=10, ny=9, nz=3, seed=5):
+    return problems.plate(nx, ny, nz, corr=3.0, contrast=100.0, seed=seed, nrhs=4)
+
+
+def test_forward_and_backward_match_the_oracle(cuda):
+    torch = cuda
+    from fieldcraft_b200.unet import UNet
+    p = small_plate()
+    net = UNet(p, seed=1)
+    flat = U.init_params(2)
+    net.set_params(flat)
+    nx, ny, nz = p.dims
+    shape = (nz + 1, ny + 1, nx + 1)
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal(shape + (U.CIO,)).astype(np.float32)
+    dy = rng.standard_normal(shape + (U.CIO,)).astype(np.float32)
+    dx, dyd = torch.from_numpy(x.reshape(-1)).cuda(), torch.from_numpy(dy.reshape(-1)).cuda()
+    y = torch.empty_like(dx)
+    net.forward_grid(dx, y)
+    net.backward_grid(dyd)
+    ref = U.Net(flat.astype(np.float64), use_bf16=True)
+    yr = ref.forward(x.astype(np.float64))
+    gw, gb = ref.backward(dy.astype(np.float64))
+    got_y = y.cpu().numpy().reshape(yr.shape)
+    assert np.max(np.abs(got_y - yr)) <= TOL * np.max(np.abs(yr))
+    got = net.grads()
+    exp = U.join_params(gw, gb)
+    off, errs = 0, []
+    for l, (cin, cout, _) in enumerate(U.LAYERS):
+        nw = 27 * cin * cout
+        for name, a, b in (("w", got[off:off + nw], exp[off:off + nw]),
+                           ("b", got[off + nw:off + nw + cout], exp[off + nw:off + nw + cout])):
+            errs.append((l, name, np.linalg.norm(a - b) / np.linalg.norm(b),
+                         np.max(np.abs(a - b)) / np.max(np.abs(b))))
+        off += nw + cout
+    for l, name, rel, top in errs:
+        tol = TOL if l >= 2 else 2.5 * TOL  # the first layers' gradients pass through every layer
+        assert rel <= tol and top <= 0.1, errs
+
+
+def test_training_and_fcg_gain_over_plain_cg(cuda):
+    # trained on pairs (r, K^-1 r) from the Cholesky solve, the network cuts the iterations flexible
+    # CG needs to reach 1e-10 well below plain CG's on held-out top-face pressures; every answer
+    # agrees with the Cholesky solution
+    torch = cuda
+    from fieldcraft_b200.unet import UNet, fcg, output_scale, train, training_pairs
+    p = problems.plate(24, 24, 4, corr=4.0, contrast=100.0, seed=9, nrhs=3)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62))
+    f.factor(up.val)
+    csr = tuple(torch.from_numpy(a).cuda() for a in (p.csr.ptr, p.csr.idx, p.csr.val))
+    R, E = training_pairs(f, p, 512, seed=3, torch=torch)
+    net = UNet(p, seed=0, kref=output_scale(R, E))
+    losses = train(net, R, E, epochs=6, lr=5e-4, torch=torch, csr_device=csr)
+    assert losses[-1] < 0.3 * losses[0], losses
+    its_nn, its_cg = [], []
+    for j in range(p.rhs.shape[1]):
+        b = torch.from_numpy(np.ascontiguousarray(p.rhs[:, j])).cuda()
+        exact = b.clone()
+        f.solve_device(exact, 1, p.n)
+        for use, its in ((net, its_nn), (None, its_cg)):
+            x = torch.zeros_like(b)
+            it, rel, fb = fcg(csr, b, x, net=use, tol=1e-10, max_iter=3000, keep=4)
+            assert rel <= 1e-10 and not fb
+            its.append(it)
+            err = torch.linalg.vector_norm(x - exact) / torch.linalg.vector_norm(exact)
+            assert err.item() < 1e-6
+    assert max(its_nn) < 0.5 * min(its_cg), (its_nn, its_cg)
+
+
+def test_fcg_falls_back_to_cholesky(cuda):
+    torch = cuda
+    from fieldcraft_b200.unet import fcg
+    p = small_plate()
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62))
+    f.factor(up.val)
+    csr = tuple(torch.from_numpy(a).cuda() for a in (p.csr.ptr, p.csr.idx, p.csr.val))
+    b = torch.from_numpy(np.ascontiguousarray(p.rhs[:, 0])).cuda()
+    x = torch.zeros_like(b)
+    it, rel, fb = fcg(csr, b, x, net=None, fallback=f, tol=1e-10, max_iter=3)
+    assert it == 3 and fb and rel <= 1e-10
+    from fieldcraft_b200 import Timeout
+    with pytest.raises(Timeout):
+        fcg(csr, b, torch.zeros_like(b), net=None, fallback=None, tol=1e-10, max_iter=3)
