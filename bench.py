@@ -35,6 +35,10 @@ METRIC = "s to rel-res 1e-10: FP32+IR & NN-FCG vs FP64 GPU Cholesky; TFLOP/s, GB
 UNIT = "s"
 N_EL, NRHS, SEED = 48, 64, 2024
 SAMPLE_EL = 24  # the CPU baseline's bounded sample: the same generator at 24^3 elements
+# profile kinds (fc_chol_profile_read) and their names
+KERNEL_KINDS = [(0, "assemble"), (1, "panel"), (3, "gemm"), (10, "inverse_products"), (11, "inverse_blocks"),
+                (18, "solve_reduce"), (19, "solve_gemm"), (20, "solve_assemble"), (21, "solve_gather"),
+                (22, "solve_fwd_inverse"), (23, "solve_bwd_inverse")]
 
 
 def parse():
@@ -48,6 +52,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--profile-only", action="store_true", help="a short run for ncu (no baselines, no e2e)")
+    ap.add_argument("--no-nn", action="store_true", help="skip the learned-preconditioner measurement")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=2,
+                    help="workload: 2 (default) the 48^3 block the metric is quoted on; 1 cantilever, 3 256 "
+                         "uneven boxes batched, 4 64^3 random-field block to 1e-12, 5 128x128x8 plate (NN-FCG)")
     return ap.parse_args()
 
 
@@ -197,6 +205,187 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def cpu_rate(threads: int) -> dict:
+    """The oracle's throughput on the host cores (factor flops per second, factor + solves of the
+    24^3 block), for estimating the CPU reference's time on other workloads by their flops."""
+    from fieldcraft_b200 import problems
+    sample = problems.lognormal_block(SAMPLE_EL, nrhs=NRHS, seed=SEED)
+    sflops, _ = factor_flops(sample)
+    t, _ = oracle_time(sample, threads)
+    return {"flops_per_s": sflops / t, "sample": f"oracle factor + {NRHS} solves of the {SAMPLE_EL}^3 block took "
+                                                 f"{t:.3f} s on {threads} threads ({sflops:.3e} factor flops)"}
+
+
+def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap: int, chol_ms: float) -> dict:
+    """The learned preconditioner on the same K: pairs (r, K^-1 r) from the Cholesky solve, Adam
+    training on the GPU, then flexible CG to rel-res 1e-10 from zero on held-out right-hand sides,
+    with and without the network (both capped at `cap` iterations, the Cholesky solve as fallback).
+    chol_ms: the FP64 Cholesky's time for one right-hand side (factor + solve) on the same K."""
+    from fieldcraft_b200.unet import UNet, fcg, output_scale, train, training_pairs
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    R, E = training_pairs(factor64, p, pairs, seed=SEED + 5, torch=torch)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    net = UNet(p, seed=0, kref=output_scale(R, E))
+    losses = train(net, R, E, epochs=epochs, lr=3e-4, torch=torch, csr_device=csr_dev)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    del R, E
+    runs = []
+    for j in cols:
+        b = torch.from_numpy(np.ascontiguousarray(p.rhs[:, j])).cuda()
+        exact = b.clone()
+        factor64.solve_device(exact, 1, p.n)
+        row = {}
+        for name, use in (("nn_fcg", net), ("cg", None)):
+            x = torch.zeros_like(b)
+            torch.cuda.synchronize()
+            ta = time.perf_counter()
+            it, rel, fb = fcg(csr_dev, b, x, net=use, fallback=factor64, tol=1e-10, max_iter=cap, keep=4)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - ta
+            err = float((torch.linalg.vector_norm(x - exact) / torch.linalg.vector_norm(exact)).item())
+            row[name] = {"iterations": it, "s": dt, "relres": rel, "fallback": fb, "err_vs_cholesky": err}
+        runs.append(row)
+    nn_s = [r["nn_fcg"]["s"] for r in runs]
+    net.close()
+    return {"value": float(np.mean(nn_s)), "unit": UNIT,
+            "speedup_vs_fp64": (chol_ms / 1e3) / float(np.mean(nn_s)),
+            "fp64_cholesky_1rhs_s": chol_ms / 1e3, "pairs": pairs, "epochs": epochs, "pairs_s": t1 - t0,
+            "train_s": t2 - t1, "loss_by_epoch": losses, "cap": cap, "rhs": runs,
+            "what": "3-level 32-channel BF16 3D-conv U-Net trained (energy-norm loss, Adam) on pairs from the "
+                    "Cholesky solve; flexible CG (4 kept directions) from zero to rel-res 1e-10 on held-out "
+                    "right-hand sides; 'cg' is the same solver without the network; a run that did not converge "
+                    "within the cap falls back to the Cholesky solve (fallback true, time included)"}
+
+
+def block_csr(parts):
+    """The rows of diag(A_0, A_1, ...) from each system's rows."""
+    from fieldcraft_b200.cholesky import Csr
+    ptr, idx, val = [np.zeros(1, np.int64)], [], []
+    col0 = nnz0 = 0
+    for c in parts:
+        ptr.append(c.ptr[1:].astype(np.int64) + nnz0)
+        idx.append(c.idx.astype(np.int64) + col0)
+        val.append(c.val)
+        col0 += c.n
+        nnz0 += int(c.ptr[-1])
+    return Csr(col0, np.concatenate(ptr), np.concatenate(idx).astype(np.int32), np.concatenate(val))
+
+
+def run_config(args, cfg: int, torch, lib, local: int):
+    """Configs other than the headline: FP64 direct solve vs FP32+IR to the config's tolerance on
+    the same K (and, for the plate, the learned preconditioner), each timed on the device from
+    values and right-hand sides in HBM to the verified residual. One JSON line."""
+    from fieldcraft_b200 import FP32_IR, FP64, Factor, Symbolic, problems
+    from fieldcraft_b200.batch import block_diagonal
+    t_host = time.perf_counter()
+    sizes = None
+    if cfg == 1:
+        p = problems.cantilever()
+        csr, up, rhs, tol = p.csr, p.upper(), p.rhs, 1e-10
+        workload = "cantilever 40x4x4 hex8 (100x10x10 mm, E 210 GPa, nu 0.3), x=0 clamped, 1 kN tip load, 1 RHS"
+    elif cfg == 4:
+        p = problems.field_block(64, nrhs=16)
+        csr, up, rhs, tol = p.csr, p.upper(), p.rhs, 1e-12
+        workload = "hex8 block 64^3, lognormal random-field E (corr 6, contrast 1e3), z=0 clamped, 16 RHS, to 1e-12"
+    elif cfg == 5:
+        p = problems.plate(128, 128, 8, nrhs=4)
+        csr, up, rhs, tol = p.csr, p.upper(), p.rhs, 1e-10
+        workload = "hex8 plate 128x128x8, lognormal random-field E (corr 8, contrast 100), sides clamped, top pressures"
+    else:
+        boxes = list(problems.uneven_boxes(count=256, lo=4, hi=24, nrhs=8, seed=11))
+        up = block_diagonal([b.upper() for b in boxes])
+        csr = block_csr([b.csr for b in boxes])
+        rhs = np.concatenate([b.rhs for b in boxes], axis=0)
+        sizes = np.array([b.n for b in boxes])
+        p = None
+        tol = 1e-10
+        workload = "256 independent hex8 boxes, nx,ny,nz ~ U{4..24}, E ~ U[70,210] GPa, nu ~ U[0.25,0.35], " \
+                   "z=0 clamped, 8 RHS each, one block-diagonal factorisation and solve"
+    sym = Symbolic(up, 2**62)
+    host_s = time.perf_counter() - t_host
+    n, R = csr.n, rhs.shape[1]
+    stream = torch.cuda.Stream()
+    csr_dev = tuple(torch.from_numpy(a).cuda() for a in (csr.ptr, csr.idx, csr.val))
+    d_val = torch.from_numpy(up.val).cuda()
+    d_b = torch.from_numpy(np.ascontiguousarray(rhs.T)).cuda()
+    res, keep64 = {}, None
+    for prec in (FP64, FP32_IR):
+        f = Factor(sym, precision=prec, device=local)
+        f.set_stream(stream.cuda_stream)
+        times, its, rels = [], 0, None
+        x = torch.zeros_like(d_b)
+        for it in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                assert lib.fc_chol_factor_device_async(f.handle, C.c_void_p(d_val.data_ptr()), up.val.size) == 0
+            rel, its = f.refine_solve_device(csr_dev, d_b, x, R, n, tol=tol, max_iter=40)
+            e1.record(stream)
+            e1.synchronize()
+            if it >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        res[prec] = {"ms": float(np.mean(times)), "solves": int(its), "relres_max": float(np.max(rel)), "x": x}
+        if prec == FP64:
+            keep64 = f
+            flops = float(f.stat(5))
+            entries = int(f.entries())
+        else:
+            f.close()
+    x64, x32 = res[FP64]["x"], res[FP32_IR]["x"]
+    err = (torch.linalg.vector_norm(x32 - x64, dim=1) / torch.linalg.vector_norm(x64, dim=1)).cpu().numpy()
+    line = {
+        "metric": METRIC, "value": res[FP64]["ms"] / 1e3, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res[FP64]["ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": workload, "config": cfg, "n": n, "nnz": int(csr.idx.size), "nrhs": R,
+                   "factor_entries": entries, "factor_flops": flops, "host_prep_s": host_s, "parallelism": "1 GPU"},
+        "relres_max": res[FP64]["relres_max"], "relres_target": tol, "solved": res[FP64]["relres_max"] <= tol,
+        "factor_tflops_incl_solve": flops / (res[FP64]["ms"] * 1e-3) / 1e12,
+        "fp32_ir": {"value": res[FP32_IR]["ms"] / 1e3, "unit": UNIT, "refinement_solves": res[FP32_IR]["solves"],
+                    "relres_max": res[FP32_IR]["relres_max"], "speedup_vs_fp64": res[FP64]["ms"] / res[FP32_IR]["ms"],
+                    "err_vs_fp64_per_rhs": [float(e) for e in err]},
+    }
+    if sizes is not None:
+        # every system's own residual of the FP64 batch solution
+        r = torch.empty_like(x64)
+        lib.fc_csr_spmv_device(n, *(C.c_void_p(a.data_ptr()) for a in csr_dev), C.c_void_p(x64.data_ptr()),
+                               C.c_void_p(r.data_ptr()), R, n, None)
+        r = (d_b - r) ** 2
+        bb = d_b ** 2
+        off = np.concatenate([[0], np.cumsum(sizes)])
+        seg = torch.tensor(np.repeat(np.arange(sizes.size), sizes), device="cuda")
+        rs = torch.zeros((R, sizes.size), dtype=torch.float64, device="cuda").index_add_(1, seg, r)
+        bs = torch.zeros_like(rs).index_add_(1, seg, bb)
+        line["per_system_relres_max"] = float(torch.sqrt(rs / bs).max().item())
+        line["systems"] = int(sizes.size)
+    if cfg == 5 and not args.no_nn:
+        # FP64 Cholesky for one right-hand side on the same K (factor + solve), the NN-FCG's comparator
+        b1 = d_b[0:1].clone()
+        tt = []
+        for it in range(3):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                lib.fc_chol_factor_device_async(keep64.handle, C.c_void_p(d_val.data_ptr()), up.val.size)
+                lib.fc_chol_solve_device_async(keep64.handle, C.c_void_p(b1.data_ptr()), 1, n)
+            e1.record(stream)
+            e1.synchronize()
+            tt.append(e0.elapsed_time(e1))
+        line["nn_fcg"] = nn_fcg_block(p, keep64, csr_dev, torch, pairs=2000, epochs=2, cols=range(min(R, 2)),
+                                      cap=3000, chol_ms=float(np.min(tt[1:])))
+    if not args.no_cpu_baseline:
+        rate = cpu_rate(os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": flops / rate["flops_per_s"], "unit": UNIT, "cores": os.cpu_count() or 1,
+                                "kind": "port", "sample": rate["sample"] + "; scaled by this workload's factor flops"}
+    keep64.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -214,6 +403,12 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     lib = _lib.load()
+    if args.config != 2:
+        if rank == 0:
+            run_config(args, args.config, torch, lib, local)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     p = problems.lognormal_block(args.n_el, nrhs=args.nrhs, seed=SEED + rank)
     up = p.upper()
     full_flops, entries = factor_flops(p)
@@ -313,8 +508,8 @@ def main():
     gemm_flops = float(f.stat(9))
     peak = dgemm_peak(torch)
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
-    factor_ms = float(ms_k[0:4].sum())
-    solve_ms = float(ms_k[16:24].sum())
+    factor_ms = float(ms_k[0:4].sum() + ms_k[10] + ms_k[11])
+    solve_ms = float(ms_k[16:26].sum())
     traffic = None
     tf = ROOT / "profiles" / "gemm_kernel_traffic.json"
     if tf.exists():
@@ -347,6 +542,25 @@ def main():
     e2e_res = float(((d_r - d_f).norm(dim=1) / fnorm).max().item())
 
     stats = {"supernodes": f.stat(4), "levels": f.stat(0), "l_bytes": f.stat(2)}
+    # the learned preconditioner on the same K (a short training; see nn_fcg_block)
+    nn = None
+    if not args.no_nn:
+        b1 = d_f[0:1].clone()
+        tt = []
+        for it in range(3):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                lib.fc_chol_factor_device_async(f.handle, C.c_void_p(d_val.data_ptr()), up.val.size)
+                lib.fc_chol_solve_device_async(f.handle, C.c_void_p(b1.data_ptr()), 1, n)
+            e1.record(stream)
+            e1.synchronize()
+            tt.append(e0.elapsed_time(e1))
+        f.set_stream(None)
+        nn = nn_fcg_block(p, f, (d_ptr, d_idx, d_kv), torch, pairs=256, epochs=2, cols=[0], cap=1500,
+                          chol_ms=float(np.min(tt[1:])))
+        f.set_stream(stream.cuda_stream)
     # FP32 (3xTF32) factorisation of S A S + FP64 refinement to the same rel-res, same system
     fp32 = None
     if not args.no_fp32:
@@ -394,14 +608,8 @@ def main():
         "relres_max": worst, "relres_target": 1e-10, "solved": worst <= 1e-10,
         "factor_tflops": full_flops / (factor_ms * 1e-3) / 1e12 if factor_ms > 0 else None,
         "phase_ms": {"factor": factor_ms, "solve": solve_ms,
-                     "by_kernel": {name: round(float(ms_k[k]), 3) for k, name in
-                                   [(0, "assemble"), (1, "panel"), (3, "gemm"), (18, "solve_reduce"), (19, "solve_gemm"),
-                                    (20, "solve_assemble"), (21, "solve_gather"), (22, "solve_fwd_panel"),
-                                    (23, "solve_bwd_panel")]},
-                     "launches": {name: int(cnt_k[k]) for k, name in
-                                  [(0, "assemble"), (1, "panel"), (3, "gemm"), (18, "solve_reduce"),
-                                   (19, "solve_gemm"), (20, "solve_assemble"), (21, "solve_gather"),
-                                   (22, "solve_fwd_panel"), (23, "solve_bwd_panel")]}},
+                     "by_kernel": {name: round(float(ms_k[k]), 3) for k, name in KERNEL_KINDS},
+                     "launches": {name: int(cnt_k[k]) for k, name in KERNEL_KINDS}},
         "roofline": {"kernel": "gemm_kernel (FP64 DMMA, factor updates)", "bound": "tensor",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
@@ -417,6 +625,8 @@ def main():
         line["cpu_baseline"] = cb
     if fp32 is not None:
         line["fp32_ir"] = fp32
+    if nn is not None:
+        line["nn_fcg"] = nn
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -103,6 +103,7 @@ def lognormal_block(n_el: int = 48, nrhs: int = 64, seed: int = 2024, sigma: flo
     i, j, k = node_grid(n_el, n_el, n_el)
     p = box(n_el, n_el, n_el, float(n_el), float(n_el), float(n_el), young, 0.3, k == 0,
             name=f"lognormal-block-{n_el}^3")
+    p.young = young
     top = np.nonzero(k == n_el)[0]
     rhs = np.empty((p.n, nrhs), order="F")
     for r in range(nrhs):
@@ -135,6 +136,7 @@ def field_block(n_el: int = 64, nrhs: int = 16, corr: float = 6.0, contrast: flo
     i, j, k = node_grid(n_el, n_el, n_el)
     p = box(n_el, n_el, n_el, float(n_el), float(n_el), float(n_el), young, 0.3, k == 0,
             name=f"field-block-{n_el}^3")
+    p.young = young
     rng = np.random.default_rng(seed + 1)
     top = np.nonzero(k == n_el)[0]
     rhs = np.empty((p.n, nrhs), order="F")
