@@ -81,6 +81,8 @@ struct fc_chol {
   DeviceBuf d_a_row, d_a_col, d_scale;   // mixed precision only
   DeviceBuf d_Dinv, d_T;                 // diagonal-block inverses; the doubling's products
   DeviceBuf d_ir_r, d_ir_d, d_ir_sum;    // iterative refinement workspace
+  DeviceBuf d_ir_p, d_ir_q, d_ir_t, d_ir_done;
+  bool refine_pcg = true;                // refinement by preconditioned CG (else plain refinement)
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
   fc::Tree tree{};
   std::vector<Launch> program;
@@ -1819,6 +1821,10 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
       h->dag_trace = value != 0;
       replan();
       return FC_OK;
+    case FC_OPTION_REFINEMENT:
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      h->refine_pcg = value == 0;
+      return FC_OK;
   }
   return FC_INVALID_ARGUMENT;
 }
@@ -1967,15 +1973,19 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
   const int R = nrhs;
   const int64_t n = h->n;
   const size_t block = sizeof(double) * (size_t)n * R;
-  if ((h->d_ir_r.bytes < block && h->d_ir_r.alloc(block) != cudaSuccess) ||
-      (h->d_ir_d.bytes < block && h->d_ir_d.alloc(block) != cudaSuccess) ||
-      (h->d_ir_sum.bytes < 2 * sizeof(double) * R && h->d_ir_sum.alloc(2 * sizeof(double) * R) != cudaSuccess)) {
+  const bool pcg = h->refine_pcg;
+  auto need = [&](DeviceBuf &b, size_t bytes) { return b.bytes >= bytes || b.alloc(bytes) == cudaSuccess; };
+  if (!need(h->d_ir_r, block) || !need(h->d_ir_d, block) || !need(h->d_ir_sum, 6 * sizeof(double) * R) ||
+      (pcg && (!need(h->d_ir_p, block) || !need(h->d_ir_q, block) || !need(h->d_ir_t, block) ||
+               !need(h->d_ir_done, sizeof(int) * R)))) {
     set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the refinement");
     return FC_OUT_OF_MEMORY;
   }
   cudaStream_t st = h->stream;
-  double *r = h->d_ir_r.as<double>(), *d = h->d_ir_d.as<double>(), *sums = h->d_ir_sum.as<double>();
+  double *r = h->d_ir_r.as<double>(), *z = h->d_ir_d.as<double>(), *sums = h->d_ir_sum.as<double>();
+  // sums: [0, R) residual norms^2, [R, 2R) ||b||^2, [2R, 3R) r.z, [3R, 4R) r.z new, [4R, 5R) p.q
   std::vector<double> host(2 * R), rel(R, 0.0);
+  std::vector<int> done(R, 0);
   cudaError_t e = cudaSuccess;
   // x = 0, r = b
   for (int j = 0; j < R && e == cudaSuccess; ++j) {
@@ -1985,38 +1995,81 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
   }
   if (e != cudaSuccess) return cuda_fail(status, e, "refinement set-up");
   fc::launch_sumsq(n, R, n, r, sums + R, st);
-  int it = 0;
-  bool done = false;
-  while (it < max_iter) {
-    e = cudaMemcpyAsync(d, r, block, cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
-    int rc = enqueue_solve(h, d, R, n, status);
-    if (rc != FC_OK) return rc;
-    ++it;
-    fc::launch_update(n, R, d, n, d_x, ld, st);
-    fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, r, n, R, st);
-    fc::launch_residual(n, R, d_b, ld, r, n, st);
-    fc::launch_sumsq(n, R, n, r, sums, st);
-    e = cudaMemcpyAsync(host.data(), sums, 2 * sizeof(double) * R, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
-    if ((rc = solve_wait_status(h, status)) != FC_OK) return rc;
-    double worst = 0.0;
+  // the true residual's relative norms of the current x (into rel); true when every column is done
+  auto check = [&](double *t) -> int {
+    fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, t, n, R, st);
+    fc::launch_residual(n, R, d_b, ld, t, n, st);
+    fc::launch_sumsq(n, R, n, t, sums, st);
+    cudaError_t e2 = cudaMemcpyAsync(host.data(), sums, 2 * sizeof(double) * R, cudaMemcpyDeviceToHost, st);
+    if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
+    if (e2 == cudaSuccess) e2 = cudaGetLastError();
+    if (e2 != cudaSuccess) return cuda_fail(status, e2, "refinement");
+    int rc2 = solve_wait_status(h, status);
+    if (rc2 != FC_OK) return rc2;
+    bool all = true;
     for (int j = 0; j < R; ++j) {
       const double bb = host[R + j];
       rel[j] = bb > 0.0 ? std::sqrt(host[j] / bb) : std::sqrt(host[j]);
-      worst = std::max(worst, rel[j]);
+      done[j] = rel[j] <= tol;  // NaN never converges
+      all = all && done[j];
     }
-    if (!(worst > tol)) {
-      done = worst == worst;  // NaN never converges
-      if (done) break;
+    return all ? -1 : FC_OK;
+  };
+  int it = 0, rc = FC_OK;
+  bool converged = false;
+  if (!pcg) {
+    // plain refinement: x += M (b - A x)
+    while (it < max_iter) {
+      e = cudaMemcpyAsync(z, r, block, cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
+      if ((rc = enqueue_solve(h, z, R, n, status)) != FC_OK) return rc;
+      ++it;
+      fc::launch_update(n, R, z, n, d_x, ld, st);
+      rc = check(r);
+      if (rc == -1) {
+        converged = true;
+        break;
+      }
+      if (rc != FC_OK) return rc;
+    }
+  } else {
+    // conjugate gradients preconditioned by this factor (an FP32 factor makes M ~ A^-1 to a few
+    // digits), one recurrence per right-hand side; convergence is judged on b - A x itself
+    double *p = h->d_ir_p.as<double>(), *q = h->d_ir_q.as<double>(), *t = h->d_ir_t.as<double>();
+    double *rz = sums + 2 * R, *rz_new = sums + 3 * R, *pq = sums + 4 * R;
+    int *d_done = h->d_ir_done.as<int>();
+    e = cudaMemcpyAsync(z, r, block, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
+    if ((rc = enqueue_solve(h, z, R, n, status)) != FC_OK) return rc;
+    ++it;
+    cudaMemcpyAsync(p, z, block, cudaMemcpyDeviceToDevice, st);
+    fc::launch_coldot(n, R, r, n, z, n, rz, st);
+    cudaMemsetAsync(d_done, 0, sizeof(int) * R, st);
+    for (;;) {
+      fc::launch_spmv(n, d_ptr, d_idx, d_val, p, n, q, n, R, st);
+      fc::launch_coldot(n, R, p, n, q, n, pq, st);
+      fc::launch_pcg_step(n, R, rz, pq, d_done, p, q, d_x, ld, r, st);
+      rc = check(t);
+      if (rc == -1) {
+        converged = true;
+        break;
+      }
+      if (rc != FC_OK) return rc;
+      if (it >= max_iter) break;
+      e = cudaMemcpyAsync(d_done, done.data(), sizeof(int) * R, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(z, r, block, cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return cuda_fail(status, e, "refinement");
+      if ((rc = enqueue_solve(h, z, R, n, status)) != FC_OK) return rc;
+      ++it;
+      fc::launch_coldot(n, R, r, n, z, n, rz_new, st);
+      fc::launch_pcg_direction(n, R, rz_new, rz, z, p, st);
+      std::swap(rz, rz_new);
     }
   }
   if (relres)
     for (int j = 0; j < R; ++j) relres[j] = rel[j];
   if (iterations) *iterations = it;
-  if (!done) {
+  if (!converged) {
     set_status(status, FC_TIMEOUT, -1, 0, 0, "the refinement did not reach the tolerance");
     return FC_TIMEOUT;
   }

@@ -667,6 +667,50 @@ __global__ void update_kernel(int64_t n, int R, const double *__restrict__ d, in
   }
 }
 
+// Preconditioned CG on column-major n x R blocks, one independent recurrence per column, every
+// scalar on the device: out[j] = sum_i a(i, j) b(i, j) (one CTA a column, a fixed tree order).
+__global__ void __launch_bounds__(256) coldot_kernel(int64_t n, const double *__restrict__ a, int64_t lda,
+                                                     const double *__restrict__ b, int64_t ldb,
+                                                     double *__restrict__ out) {
+  __shared__ double part[256];
+  const double *ca = a + blockIdx.x * lda, *cb = b + blockIdx.x * ldb;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += ca[i] * cb[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) part[threadIdx.x] += part[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = part[0];
+}
+
+// alpha_j = rz[j] / pq[j]; x_j += alpha_j p_j; r_j -= alpha_j q_j (columns with done[j] set keep x, r).
+__global__ void pcg_step_kernel(int64_t n, int R, const double *__restrict__ rz, const double *__restrict__ pq,
+                                const int *__restrict__ done, const double *__restrict__ p, const double *__restrict__ q,
+                                double *__restrict__ x, int64_t ldx, double *__restrict__ r) {
+  const int64_t total = n * R;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % n, j = e / n;
+    if (done[j]) continue;
+    const double alpha = pq[j] != 0.0 ? rz[j] / pq[j] : 0.0;
+    x[i + j * ldx] += alpha * p[e];
+    r[e] -= alpha * q[e];
+  }
+}
+
+// p_j = z_j + (rz_new[j] / rz_old[j]) p_j
+__global__ void pcg_direction_kernel(int64_t n, int R, const double *__restrict__ rz_new,
+                                     const double *__restrict__ rz_old, const double *__restrict__ z,
+                                     double *__restrict__ p) {
+  const int64_t total = n * R;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / n;
+    const double beta = rz_old[j] != 0.0 ? rz_new[j] / rz_old[j] : 0.0;
+    p[e] = z[e] + beta * p[e];
+  }
+}
+
 // out[j] = sum_i v(i, j)^2 for each column j (one CTA a column, a fixed tree order).
 __global__ void __launch_bounds__(256) sumsq_kernel(int64_t n, int64_t ld, const double *__restrict__ v,
                                                     double *__restrict__ out) {
@@ -803,6 +847,28 @@ void launch_update(int64_t n, int R, const double *d, int64_t ldd, double *x, in
   const int64_t total = n * R;
   if (total <= 0) return;
   update_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, d, ldd, x, ldx);
+}
+
+void launch_coldot(int64_t n, int R, const double *a, int64_t lda, const double *b, int64_t ldb, double *out,
+                   cudaStream_t st) {
+  if (n <= 0 || R <= 0) return;
+  coldot_kernel<<<R, 256, 0, st>>>(n, a, lda, b, ldb, out);
+}
+
+void launch_pcg_step(int64_t n, int R, const double *rz, const double *pq, const int *done, const double *p,
+                     const double *q, double *x, int64_t ldx, double *r, cudaStream_t st) {
+  const int64_t total = n * R;
+  if (total <= 0) return;
+  pcg_step_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, rz, pq, done, p, q, x,
+                                                                                         ldx, r);
+}
+
+void launch_pcg_direction(int64_t n, int R, const double *rz_new, const double *rz_old, const double *z, double *p,
+                          cudaStream_t st) {
+  const int64_t total = n * R;
+  if (total <= 0) return;
+  pcg_direction_kernel<<<(int)std::min<int64_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(n, R, rz_new, rz_old, z,
+                                                                                              p);
 }
 
 void launch_sumsq(int64_t n, int R, int64_t ld, const double *v, double *out, cudaStream_t st) {

@@ -198,6 +198,15 @@ void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, 
 void launch_residual(int64_t n, int R, const double *b, int64_t ldb, double *ax, int64_t ldax, cudaStream_t st);
 void launch_update(int64_t n, int R, const double *d, int64_t ldd, double *x, int64_t ldx, cudaStream_t st);
 void launch_sumsq(int64_t n, int R, int64_t ld, const double *v, double *out, cudaStream_t st);
+// Preconditioned CG per column (scalars on the device): out[j] = a_j . b_j;
+// x_j += (rz_j / pq_j) p_j and r_j -= (rz_j / pq_j) q_j unless done[j]; p_j = z_j + (rzn_j / rzo_j) p_j.
+// p, q, r, z are n x R with leading dimension n.
+void launch_coldot(int64_t n, int R, const double *a, int64_t lda, const double *b, int64_t ldb, double *out,
+                   cudaStream_t st);
+void launch_pcg_step(int64_t n, int R, const double *rz, const double *pq, const int *done, const double *p,
+                     const double *q, double *x, int64_t ldx, double *r, cudaStream_t st);
+void launch_pcg_direction(int64_t n, int R, const double *rz_new, const double *rz_old, const double *z, double *p,
+                          cudaStream_t st);
 // y = A x for column-major x, y (leading dimensions ldx, ldy).
 void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, int64_t ldx,
                  double *y, int64_t ldy, int R, cudaStream_t st);

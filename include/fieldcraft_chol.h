@@ -133,9 +133,11 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
  * fc_chol_entries(h) doubles. */
 int fc_chol_values(fc_chol *h, double *dst, fc_status *status);
 
-/* Solve A x = b to a relative residual by iterative refinement in FP64 around the handle's
- * factor (the mixed-precision mode's FP32 factor of S A S, or the FP64 factor): x = 0, then
- * d = solve(r), x += d, r = b - A x (FP64 SpMV on A by rows: d_ptr[n+1], d_idx, d_val, both
+/* Solve A x = b to a relative residual in FP64 around the handle's factor (the mixed-precision
+ * mode's FP32 factor of S A S, or the FP64 factor) as the preconditioner M: by default conjugate
+ * gradients preconditioned by M, one recurrence per right-hand side, from x = 0 (the first step is
+ * x = M b); FC_OPTION_REFINEMENT = 1 selects plain refinement x += M (b - A x). Convergence is
+ * judged on the true residual b - A x (FP64 SpMV on A by rows: d_ptr[n+1], d_idx, d_val, both
  * triangles, the matrix the factor was made from) until ||r_j|| <= tol ||b_j|| for every
  * right-hand side j or max_iter solves. No counterpart in the reference (its only refinement,
  * Symmetric::solve_refined, crates/solver/src/ldlt.rs:529-566, is in working precision).
@@ -163,11 +165,15 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *   FC_OPTION_PLANT_UNMET_WAIT (tests) value != 0: the next solve plan holds one dependency that no
  *                              task meets, so that solve ends with FC_TIMEOUT after the limit.
  *   FC_OPTION_TRACE            value != 0: the persistent solve records per task when it was taken,
- *                              when its inputs were ready and when it was done (fc_chol_trace_read). */
+ *                              when its inputs were ready and when it was done (fc_chol_trace_read).
+ *   FC_OPTION_REFINEMENT       fc_chol_refine_solve_device's iteration: 0 conjugate gradients
+ *                              preconditioned by the factor (default), 1 plain refinement
+ *                              x += M (b - A x). */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3
 #define FC_OPTION_TRACE 4
+#define FC_OPTION_REFINEMENT 5
 int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
 /* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
  * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |

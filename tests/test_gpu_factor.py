@@ -216,6 +216,13 @@ def test_mixed_precision_refines_to_the_fp64_answer(cuda, name, make, values_tol
     x = torch.zeros_like(b)
     rel, its = f32.refine_solve_device(device_csr(torch, p.csr), b, x, k, p.n, tol=1e-10, max_iter=30)
     assert np.all(rel <= 1e-10) and its <= 30, (rel, its)
+    # plain refinement reaches the same answer, in at least as many solves as the CG form
+    f32.option(Factor.REFINEMENT, 1)
+    xp = torch.zeros_like(b)
+    relp, itsp = f32.refine_solve_device(device_csr(torch, p.csr), b, xp, k, p.n, tol=1e-10, max_iter=60)
+    f32.option(Factor.REFINEMENT, 0)
+    assert np.all(relp <= 1e-10) and itsp >= its, (itsp, its)
+    assert torch.linalg.vector_norm(xp - x).item() <= 1e-8 * torch.linalg.vector_norm(x).item()
     _, ref = oracle_factor(p.csr)
     exp = ref.solve(p.rhs.copy())
     got = x.cpu().numpy().T
