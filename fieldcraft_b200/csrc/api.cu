@@ -44,7 +44,8 @@ enum Kind {
   K_ASSEMBLE, K_PANEL, K_REDUCE, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD,
   K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD,
   K_GEMM_MIXED,  // A in the factor's storage type, B and C FP64
-  K_GEMM_F64     // FP64 throughout (the diagonal blocks' inverses)
+  K_GEMM_F64,    // FP64 throughout (the diagonal blocks' inverses)
+  K_GEMM_TC      // FP32 3xTF32 on tcgen05 (the update matrices of the mixed-precision factor)
 };
 
 struct Launch {
@@ -83,6 +84,7 @@ struct fc_chol {
   DeviceBuf d_ir_r, d_ir_d, d_ir_sum;    // iterative refinement workspace
   DeviceBuf d_ir_p, d_ir_q, d_ir_t, d_ir_done;
   bool refine_pcg = true;                // refinement by preconditioned CG (else plain refinement)
+  bool tc = true;                        // FP32 updates on tcgen05 (FC_TF32_MMA_SYNC=1: on mma.sync)
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
   fc::Tree tree{};
   std::vector<Launch> program;
@@ -324,6 +326,12 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
   auto Up = [&](int64_t off) { return arena_at(h->d_U, h, off); };
   const int NB = fc::NB;
+  // a factor GEMM tile: 64 x 64, and 128 x 128 for the update matrices' long products on the
+  // tcgen05 path (the first tile of a column block starts on the diagonal, so 'lower' still means
+  // local i >= j); the panels' short updates of later columns (K <= 64) stay on 64 x 64 tiles
+  const int TM = fc::GEMM_TM;
+  const int TMU = h->fp32 && h->tc ? fc::GEMM_TC_M : fc::GEMM_TM;
+  const int TNU = h->fp32 && h->tc ? fc::GEMM_TC_N : fc::GEMM_TN;
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
     int64_t off = (int64_t)asm_t.size();
@@ -356,13 +364,13 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
               {(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff, ioff, bw, 0});
         const int64_t lo = h->loff[s];
         for (int jc = c1; jc < w; jc += fc::GEMM_TN)
-          for (int ic = jc; ic < m; ic += fc::GEMM_TM) {
+          for (int ic = jc; ic < m; ic += TM) {
             fc::GemmTask g{};
             g.C = Lp(lo + ic + (int64_t)jc * m);
             g.A = Lp(lo + ic + (int64_t)c0 * m);
             g.B = Lp(lo + jc + (int64_t)c0 * m);
             g.c_si = 1, g.c_sj = m, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
-            g.M = std::min(fc::GEMM_TM, m - ic);
+            g.M = std::min(TM, m - ic);
             g.N = std::min(fc::GEMM_TN, w - jc);
             g.K = c1 - c0;
             g.flags = ic == jc ? 1 : 0;
@@ -388,21 +396,21 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       const int m = h->height[s], w = h->width[s], u = m - w;
       if (u <= 0) continue;
       const int64_t lo = h->loff[s], uo = h->uoff[s];
-      for (int bj = 0; bj < u; bj += fc::GEMM_TN)
-        for (int bi = bj; bi < u; bi += fc::GEMM_TM) {
+      for (int bj = 0; bj < u; bj += TNU)
+        for (int bi = bj; bi < u; bi += TMU) {
           fc::GemmTask g{};
           g.C = Up(uo + bi + (int64_t)bj * u);
           g.A = Lp(lo + w + bi);
           g.B = Lp(lo + w + bj);
           g.c_si = 1, g.c_sj = u, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
-          g.M = std::min(fc::GEMM_TM, u - bi);
-          g.N = std::min(fc::GEMM_TN, u - bj);
+          g.M = std::min(TMU, u - bi);
+          g.N = std::min(TNU, u - bj);
           g.K = w;
           g.flags = (bi == bj ? 1 : 0) | 2;
           gemm_t.push_back(g);
         }
     }
-    push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+    push(h->program, h->fp32 && h->tc ? K_GEMM_TC : K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
     // the children's contributions to the update matrices, on top of -L21 L21^T
     off = (int64_t)asm_t.size();
     for (int64_t s : S) {
@@ -632,7 +640,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
     int64_t ordinal = 0;
     double big = -1, trail = -1;
     for (const Launch &l : h->program) {
-      if (l.kind != K_GEMM) continue;
+      if (l.kind != K_GEMM && l.kind != K_GEMM_TC) continue;
       double fl = 0;
       int kmax = 0;
       for (int64_t q = l.off; q < l.off + l.count; ++q) {
@@ -756,6 +764,9 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
                          h->d_status.as<fc::DeviceStatus>(), l.width, st);
         break;
       case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, gk, st); break;
+      case K_GEMM_TC:
+        fc::launch_gemm_tc(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(), st);
+        break;
       case K_GEMM_MIXED:
         fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count,
                         h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
@@ -773,6 +784,10 @@ int read_status(fc_chol *h, fc_status *st) {
   cudaError_t e = cudaMemcpyAsync(&ds, h->d_status.p, sizeof(ds), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return cuda_fail(st, e, "factorisation");
+  if (ds.timeout != 0xFFFFFFFFu) {
+    set_status(st, FC_TIMEOUT, -1, 0, 0, "a bounded wait of the tensor-core GEMM gave up");
+    return FC_TIMEOUT;
+  }
   if (ds.failed_column != ULLONG_MAX) {
     const int64_t col = (int64_t)ds.failed_column;
     const int64_t orig = col < h->n ? h->perm[col] : col;
@@ -1701,6 +1716,8 @@ int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **
   {
     const char *env = std::getenv("FC_NO_GRAPHS");
     h->graphs = !(env && env[0] == '1');
+    const char *mma_sync = std::getenv("FC_TF32_MMA_SYNC");
+    h->tc = !(mma_sync && mma_sync[0] == '1');
     const char *persistent = std::getenv("FC_SOLVE_PERSISTENT");
     h->dag = persistent && persistent[0] == '1';
   }

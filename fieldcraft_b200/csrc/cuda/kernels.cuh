@@ -164,6 +164,8 @@ void launch_solve_dag(const Tree &t, bool fp32, bool backward, const SolveDag &d
 // Device status word of a factorisation: the smallest failing pivot column (postorder).
 struct DeviceStatus {
   unsigned long long failed_column;  // ULLONG_MAX when none
+  unsigned int timeout;              // 0xFFFFFFFF when none; set when a bounded device wait gave up
+  unsigned int pad;
 };
 
 // Sets the kernels' shared-memory limits (once per process; before any stream capture).
@@ -172,6 +174,10 @@ void configure_kernels();
 // The operand types of a GEMM launch: FP64 throughout (DMMA); an FP32 A with FP64 B and C (DMMA,
 // the solve on an FP32 factor); FP32 throughout by 3xTF32 (the FP32 factorisation).
 enum class GemmKind { F64, F32A_F64, F32_TF32X3 };
+// FP32 3xTF32 GEMM tasks on the tcgen05 tensor cores (tiles of up to GEMM_TC_M x GEMM_TC_N, A and
+// B with unit row stride); a wait that gives up sets status->timeout.
+constexpr int GEMM_TC_M = 128, GEMM_TC_N = 128;
+void launch_gemm_tc(const GemmTask *tasks, int count, DeviceStatus *status, cudaStream_t st);
 
 // S = diag(A)^-1/2 for the mixed-precision factorisation.
 void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double *scale, cudaStream_t st);
