@@ -29,6 +29,28 @@ def block_diagonal(parts: list[UpperColumns]) -> UpperColumns:
                         np.concatenate(val).astype(np.float64))
 
 
+def shard(costs, world: int) -> list[list[int]]:
+    """Independent systems over `world` ranks with no collective on the data path: longest first,
+    each to the least-loaded rank (ties to the lowest rank), so every rank gets a deterministic
+    share of about the same estimated work. Returns each rank's system indices in increasing order."""
+    load = [0.0] * world
+    share: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        share[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(x) for x in share]
+
+
+def factor_cost(part: UpperColumns) -> float:
+    """Estimated factor work of one system: the sum of squared column counts of its analysis."""
+    a = Symbolic(part, 2**62).arrays()
+    w = np.diff(a["first"])
+    m = np.diff(a["rptr"])
+    return float(sum(float(np.dot(mm - np.arange(ww, dtype=np.float64), mm - np.arange(ww, dtype=np.float64)))
+                     for mm, ww in zip(m, w)))
+
+
 class BatchFactor:
     """Factors of several SPD systems at once. `offsets[b]` is system b's first unknown in the
     stacked vectors; a failing pivot is reported as (system, column)."""
