@@ -425,6 +425,51 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
   }
 }
 
+// The factorisation's launch program and task arrays (again after an option changes the kernels'
+// tiles), uploaded; the captured factor graph is dropped.
+int plan_factor_upload(fc_chol *h, fc_status *st) {
+  cudaStream_t stream = h->stream;
+  cudaError_t e;
+  if (h->factor_graph) {
+    cudaGraphExecDestroy(h->factor_graph);
+    h->factor_graph = nullptr;
+  }
+  h->program.clear();
+  const std::vector<std::vector<int64_t>> lv = levels_of(h);
+  std::vector<fc::AssembleTask> asm_t;
+  std::vector<int2> ranges;
+  std::vector<fc::PanelTask> panel_t;
+  std::vector<fc::GemmTask> gemm_t;
+  plan_factor(h, lv, asm_t, ranges, panel_t, gemm_t);
+  h->gemm_tasks = (int64_t)gemm_t.size();
+  h->gemm_flops_factor = 0;
+  for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
+  {
+    // ordinals (among the factor's GEMM launches) of the heaviest launch and of the heaviest one
+    // whose tasks all have K <= NB (a panel's update of the later columns)
+    int64_t ordinal = 0;
+    double big = -1, trail = -1;
+    for (const Launch &l : h->program) {
+      if (l.kind != K_GEMM && l.kind != K_GEMM_TC) continue;
+      double fl = 0;
+      int kmax = 0;
+      for (int64_t q = l.off; q < l.off + l.count; ++q) {
+        fl += task_flops(gemm_t[q]);
+        kmax = std::max(kmax, gemm_t[q].K);
+      }
+      if (fl > big) big = fl, h->gemm_big_ordinal = ordinal;
+      if (kmax <= fc::NB && fl > trail) trail = fl, h->gemm_trail_ordinal = ordinal;
+      ++ordinal;
+    }
+  }
+  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_ranges, ranges, stream)) != cudaSuccess ||
+      (e = upload(h->d_panel, panel_t, stream)) != cudaSuccess ||
+      (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
+    return cuda_fail(st, e, "upload of the plan");
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
+  return FC_OK;
+}
+
 int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   const int64_t ns = sym.ns, n = sym.n;
   h->n = n;
@@ -626,38 +671,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       return fail_status(st, f);
     }
   }
-  std::vector<fc::AssembleTask> asm_t;
-  std::vector<int2> ranges;
-  std::vector<fc::PanelTask> panel_t;
-  std::vector<fc::GemmTask> gemm_t;
-  plan_factor(h, lv, asm_t, ranges, panel_t, gemm_t);
-  h->gemm_tasks = (int64_t)gemm_t.size();
-  h->gemm_flops_factor = 0;
-  for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
-  {
-    // ordinals (among the factor's GEMM launches) of the heaviest launch and of the heaviest one
-    // whose tasks all have K <= NB (a panel's update of the later columns)
-    int64_t ordinal = 0;
-    double big = -1, trail = -1;
-    for (const Launch &l : h->program) {
-      if (l.kind != K_GEMM && l.kind != K_GEMM_TC) continue;
-      double fl = 0;
-      int kmax = 0;
-      for (int64_t q = l.off; q < l.off + l.count; ++q) {
-        fl += task_flops(gemm_t[q]);
-        kmax = std::max(kmax, gemm_t[q].K);
-      }
-      if (fl > big) big = fl, h->gemm_big_ordinal = ordinal;
-      if (kmax <= fc::NB && fl > trail) trail = fl, h->gemm_trail_ordinal = ordinal;
-      ++ordinal;
-    }
-  }
-  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_ranges, ranges, stream)) != cudaSuccess ||
-      (e = upload(h->d_panel, panel_t, stream)) != cudaSuccess ||
-      (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
-    return cuda_fail(st, e, "upload of the plan");
-  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
-  return FC_OK;
+  return plan_factor_upload(h, st);
 }
 
 cudaEvent_t next_event(fc_chol *h) {
@@ -1842,6 +1856,13 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       h->refine_pcg = value == 0;
       return FC_OK;
+    case FC_OPTION_FP32_UPDATES: {
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      if (h->tc == (value == 0)) return FC_OK;
+      h->tc = value == 0;
+      fc_status ignore{};
+      return h->fp32 ? plan_factor_upload(h, &ignore) : FC_OK;
+    }
   }
   return FC_INVALID_ARGUMENT;
 }

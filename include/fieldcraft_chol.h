@@ -168,12 +168,16 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *                              when its inputs were ready and when it was done (fc_chol_trace_read).
  *   FC_OPTION_REFINEMENT       fc_chol_refine_solve_device's iteration: 0 conjugate gradients
  *                              preconditioned by the factor (default), 1 plain refinement
- *                              x += M (b - A x). */
+ *                              x += M (b - A x).
+ *   FC_OPTION_FP32_UPDATES     the mixed-precision factor's update-matrix products: 0 on tcgen05
+ *                              in 128 x 128 tiles (default), 1 on mma.sync in 64 x 64 tiles
+ *                              (re-plans the factorisation; takes effect from the next one). */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3
 #define FC_OPTION_TRACE 4
 #define FC_OPTION_REFINEMENT 5
+#define FC_OPTION_FP32_UPDATES 6
 int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
 /* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
  * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |

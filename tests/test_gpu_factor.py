@@ -276,3 +276,36 @@ def test_solve_wait_limit_reports_timeout(cuda):
     got = b.copy()
     f.solve(got)
     assert np.max(np.abs(got - x)) < 1e-12
+
+
+def test_autotuner_picks_a_working_variant(cuda, tmp_path):
+    # every candidate (update kernel x solve schedule x refinement) solves the batch to the
+    # tolerance; the autotuner keeps the fastest and a second call reads it from the cache
+    from fieldcraft_b200 import FP32_IR
+    from fieldcraft_b200.autotune import autotune, candidates
+    from fieldcraft_b200.batch import block_diagonal
+    torch = cuda
+    boxes = list(problems.uneven_boxes(count=5, lo=3, hi=8, nrhs=2, seed=7))
+    up = block_diagonal([b.upper() for b in boxes])
+    rows = [b.csr for b in boxes]
+    ptr = [np.zeros(1, np.int64)]
+    idx, val, c0, z0 = [], [], 0, 0
+    for c in rows:
+        ptr.append(c.ptr[1:] + z0)
+        idx.append(c.idx.astype(np.int64) + c0)
+        val.append(c.val)
+        c0 += c.n
+        z0 += int(c.ptr[-1])
+    csr = Csr(c0, np.concatenate(ptr), np.concatenate(idx).astype(np.int32), np.concatenate(val))
+    rhs = np.concatenate([b.rhs for b in boxes], axis=0)
+    f = Factor(Symbolic(up, 2**62), precision=FP32_IR)
+    d_val = torch.from_numpy(up.val).cuda()
+    d_b = torch.from_numpy(np.ascontiguousarray(rhs.T)).cuda()
+    cache = tmp_path / "tune.json"
+    res = autotune(f, FP32_IR, d_val, up.val.size, device_csr(torch, csr), d_b, 2, 1e-10, torch, repeats=1, cache=cache)
+    assert len(res["ms"]) == len(candidates(FP32_IR)) and cache.exists()
+    again = autotune(f, FP32_IR, d_val, up.val.size, device_csr(torch, csr), d_b, 2, 1e-10, torch, cache=cache)
+    assert again["options"] == res["options"]
+    x = torch.zeros_like(d_b)
+    rel, _ = f.refine_solve_device(device_csr(torch, csr), d_b, x, 2, c0, tol=1e-10, max_iter=30)
+    assert np.all(rel <= 1e-10)
