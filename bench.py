@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--profile-only", action="store_true", help="a short run for ncu (no baselines, no e2e)")
     ap.add_argument("--no-nn", action="store_true", help="skip the learned-preconditioner measurement")
+    ap.add_argument("--profile-kernels", choices=["fp32-factor", "unet"], default=None,
+                    help="a short run for a profiler: two FP32 factorisations of the --n-el block, or the "
+                         "U-Net's forward and backward passes on a 64x64x8 plate, twice")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=2,
                     help="workload: 2 (default) the 48^3 block the metric is quoted on; 1 cantilever, 3 256 "
                          "uneven boxes batched, 4 64^3 random-field block to 1e-12, 5 128x128x8 plate (NN-FCG)")
@@ -397,6 +400,34 @@ def run_config(args, cfg: int, torch, lib, local: int):
     print(json.dumps(line), flush=True)
 
 
+def profile_kernels(args, torch, lib):
+    """Runs for a profiler (no timing): the FP32 factorisation of the --n-el block twice (the
+    tcgen05 update GEMMs), or the U-Net's forward and backward passes twice."""
+    from fieldcraft_b200 import FP32_IR, Factor, Symbolic, problems
+    if args.profile_kernels == "fp32-factor":
+        p = problems.lognormal_block(args.n_el, nrhs=1, seed=SEED)
+        up = p.upper()
+        f = Factor(Symbolic(up, 2**62), precision=FP32_IR)
+        d_val = torch.from_numpy(up.val).cuda()
+        for _ in range(2):
+            assert lib.fc_chol_factor_device_async(f.handle, C.c_void_p(d_val.data_ptr()), up.val.size) == 0
+        torch.cuda.synchronize()
+        f.close()
+        print(json.dumps({"profile_kernels": "fp32-factor", "n": p.n}), flush=True)
+    else:
+        from fieldcraft_b200.unet import UNet
+        p = problems.plate(64, 64, 8, nrhs=1)
+        net = UNet(p, seed=0, kref=100.0)
+        x = torch.randn(net.voxels * 16, device="cuda", dtype=torch.float32)
+        y = torch.empty_like(x)
+        for _ in range(2):
+            net.forward_grid(x, y)
+            net.backward_grid(x)
+        torch.cuda.synchronize()
+        net.close()
+        print(json.dumps({"profile_kernels": "unet", "voxels": net.voxels}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -414,6 +445,9 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     lib = _lib.load()
+    if args.profile_kernels:
+        profile_kernels(args, torch, lib)
+        return
     if args.config != 2:
         if rank == 0:
             run_config(args, args.config, torch, lib, local)
