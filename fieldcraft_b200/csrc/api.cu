@@ -54,6 +54,12 @@ struct Launch {
   int count;
   int level;  // the level of the supernodal tree the launch belongs to (cancellation points)
   int width;  // panel launches: the widest panel, padded (sizes the kernel's shared memory)
+  // the factorisation runs on two streams (lanes): a panel step's update of the columns after the
+  // next panel goes on lane 1, so it overlaps the next panel; `dep` is a launch on the other lane
+  // this one waits for (-1: none), `record` marks a launch another waits for
+  int lane = 0;
+  int dep = -1;
+  bool record = false;
 };
 
 }  // namespace
@@ -88,6 +94,9 @@ struct fc_chol {
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
   fc::Tree tree{};
   std::vector<Launch> program;
+  cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch)
+  std::vector<cudaEvent_t> lane_events;   // per launch of the program that another waits for
+  cudaEvent_t fork_event = nullptr, join_event = nullptr;
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
@@ -128,6 +137,11 @@ struct fc_chol {
     if (factor_graph) cudaGraphExecDestroy(factor_graph);
     if (solve_graph) cudaGraphExecDestroy(solve_graph);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : lane_events)
+      if (e) cudaEventDestroy(e);
+    if (fork_event) cudaEventDestroy(fork_event);
+    if (join_event) cudaEventDestroy(join_event);
+    if (side) cudaStreamDestroy(side);
   }
 };
 
@@ -332,7 +346,20 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
   const int TM = fc::GEMM_TM;
   const int TMU = h->fp32 && h->tc ? fc::GEMM_TC_M : fc::GEMM_TM;
   const int TNU = h->fp32 && h->tc ? fc::GEMM_TC_N : fc::GEMM_TN;
+  int pending_join = -1;  // a lane-1 launch the next lane-0 launch after the panel steps waits for
+  auto join = [&]() {
+    if (pending_join >= 0 && (int)h->program.size() > pending_join + 1) {
+      for (size_t q = pending_join + 1; q < h->program.size(); ++q)
+        if (h->program[q].lane == 0) {
+          h->program[q].dep = pending_join;
+          h->program[pending_join].record = true;
+          pending_join = -1;
+          break;
+        }
+    }
+  };
   for (size_t l = 0; l < lv.size(); ++l) {
+    join();
     const auto &S = lv[l];
     int64_t off = (int64_t)asm_t.size();
     for (int64_t s : S) {
@@ -345,8 +372,10 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
+    int last_rest = -1;  // the level's latest lane-1 launch
     for (int p = 0; p < P; ++p) {
       int64_t po = (int64_t)panel_t.size(), go = (int64_t)gemm_t.size();
+      std::vector<fc::GemmTask> rest;  // updates of the columns past the next panel (lane 1)
       int p8max = 8;
       for (int64_t s : S) {
         const int m = h->height[s], w = h->width[s];
@@ -374,12 +403,29 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             g.N = std::min(fc::GEMM_TN, w - jc);
             g.K = c1 - c0;
             g.flags = ic == jc ? 1 : 0;
-            gemm_t.push_back(g);
+            (jc == c1 ? gemm_t : rest).push_back(g);
           }
       }
       push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l, p8max);
+      const int panel_at = (int)h->program.size() - 1;
+      const size_t before = h->program.size();
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+      if (h->program.size() > before && last_rest >= 0) {  // the next panel's columns after rest(p-1)
+        h->program.back().dep = last_rest;
+        h->program[last_rest].record = true;
+      }
+      if (!rest.empty()) {
+        const int64_t ro = (int64_t)gemm_t.size();
+        gemm_t.insert(gemm_t.end(), rest.begin(), rest.end());
+        push(h->program, K_GEMM, ro, (int64_t)rest.size(), (int)l);
+        Launch &r = h->program.back();
+        r.lane = 1;
+        r.dep = panel_at;
+        h->program[panel_at].record = true;
+        last_rest = (int)h->program.size() - 1;
+      }
     }
+    pending_join = last_rest;
     for (int hh = NB; hh < fc::SB; hh *= 2) {
       std::vector<fc::GemmTask> first, second;
       inverse_doubling(h, S, h->d_T.as<double>(), hh, &first, &second);
@@ -423,6 +469,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     }
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
   }
+  join();
 }
 
 // The factorisation's launch program and task arrays (again after an option changes the kernels'
@@ -467,6 +514,16 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
       (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
     return cuda_fail(st, e, "upload of the plan");
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
+  for (cudaEvent_t ev : h->lane_events)
+    if (ev) cudaEventDestroy(ev);
+  h->lane_events.assign(h->program.size(), nullptr);
+  for (size_t q = 0; q < h->program.size(); ++q)
+    if (h->program[q].record && (e = cudaEventCreateWithFlags(&h->lane_events[q], cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_fail(st, e, "lane events");
+  if (!h->side && ((e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess ||
+                   (e = cudaEventCreateWithFlags(&h->fork_event, cudaEventDisableTiming)) != cudaSuccess ||
+                   (e = cudaEventCreateWithFlags(&h->join_event, cudaEventDisableTiming)) != cudaSuccess))
+    return cuda_fail(st, e, "lane stream");
   return FC_OK;
 }
 
@@ -752,21 +809,37 @@ int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *canc
 }
 
 int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
-  cudaStream_t st = h->stream;
-  cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), st);
-  if (h->fp32) fc::launch_scale(h->n, h->d_diag_src.as<int64_t>(), d_val, h->d_scale.as<double>(), st);
+  cudaStream_t main = h->stream;
+  cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), main);
+  if (h->fp32) fc::launch_scale(h->n, h->d_diag_src.as<int64_t>(), d_val, h->d_scale.as<double>(), main);
   const fc::GemmKind gk = h->fp32 ? fc::GemmKind::F32_TF32X3 : fc::GemmKind::F64;
   const fc::Tree &t = h->tree;
+  // lane 1 forks from the main stream here and joins it at the end; profiling keeps one lane
+  const bool lanes = h->side && !h->profiling;
+  if (lanes) {
+    cudaEventRecord(h->fork_event, main);
+    cudaStreamWaitEvent(h->side, h->fork_event, 0);
+  }
+  auto join = [&]() {
+    if (lanes) {
+      cudaEventRecord(h->join_event, h->side);
+      cudaStreamWaitEvent(main, h->join_event, 0);
+    }
+  };
   int last_level = -1;
   int64_t launches = 0;
-  for (const Launch &l : h->program) {
+  for (size_t li = 0; li < h->program.size(); ++li) {
+    const Launch &l = h->program[li];
     if (cancel && l.level != last_level) {
       if (*cancel != 0) {
+        join();
         h->last_factor_launches = launches;
         return FC_CANCELLED;
       }
       last_level = l.level;
     }
+    const cudaStream_t st = lanes && l.lane ? h->side : main;
+    if (lanes && l.dep >= 0) cudaStreamWaitEvent(st, h->lane_events[l.dep], 0);
     Mark mark(h, l.kind, l.level, l.count);
     switch (l.kind) {
       case K_ASSEMBLE:
@@ -787,8 +860,10 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
         break;
       case K_GEMM_F64: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, fc::GemmKind::F64, st); break;
     }
+    if (lanes && l.record) cudaEventRecord(h->lane_events[li], st);
     ++launches;
   }
+  join();
   h->last_factor_launches = launches;
   return FC_OK;
 }

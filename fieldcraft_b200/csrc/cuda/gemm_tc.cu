@@ -4,10 +4,9 @@
 // One CTA of 256 threads per task tile of up to 128 x 128 outputs (M = 128 rows of A, N = 128
 // rows of B). K advances in chunks of 32 through a three-stage ring. cp.async copies each chunk's FP32
 // operands (A and B with unit row stride: the factor's column-major panels) straight into the
-// canonical K-major, no-swizzle layout (8-row x 16-byte core matrices), two chunks ahead. These
-// raw values are the "hi" operands: the tensor core reads an FP32 operand as TF32 by dropping its
-// low 13 bits, so hi = x truncated. The threads add the "lo" tiles, lo = x - hi (exact in FP32),
-// and thread 0 issues the chunk's 4 x 3 MMAs (hi hi + hi lo + lo hi; M 128, N 128, K 8 each),
+// canonical K-major, no-swizzle layout (8-row x 16-byte core matrices), two chunks ahead. The
+// threads round each value in place to TF32 (hi, which the tensor core then reads exactly) and
+// write the "lo" tiles, lo = x - hi (exact in FP32), and thread 0 issues the chunk's 4 x 3 MMAs (hi hi + hi lo + lo hi; M 128, N 128, K 8 each),
 // committed to the stage's mbarrier; a stage is refilled once its MMAs are done. The epilogue
 // reads the accumulator with tcgen05.ld (warps w and w + 4 own TMEM lanes 32w..32w+31, the rows,
 // one half of the 128 columns each) and writes C. Every mbarrier wait is bounded
@@ -138,9 +137,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(const GemmTask *
     }
     asm volatile("cp.async.commit_group;\n" ::);  // an empty group past the end keeps the count uniform
   };
-  auto lo4 = [](float4 x) {
-    auto lo = [](float v) { return v - __uint_as_float(__float_as_uint(v) & 0xFFFFE000u); };
-    return make_float4(lo(x.x), lo(x.y), lo(x.z), lo(x.w));
+  // x -> (hi, lo): hi = x rounded to TF32 (so the tensor core's reading of it drops nothing),
+  // lo = x - hi (exact in FP32)
+  auto split = [](float v, float &hi, float &lo) {
+    uint32_t h;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(v));
+    hi = __uint_as_float(h);
+    lo = v - hi;
   };
   issue(0);
   issue(1);
@@ -150,11 +153,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(const GemmTask *
     asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // chunk q has landed (this thread's copies)
     __syncthreads();
     if (s_fail) break;  // every thread reads the same value after the barrier
-    // lo tiles: 16-byte groups (4 consecutive k of one row); A: 1024 groups, B: 1024
+    // hi in place and the lo tiles: 16-byte groups (4 consecutive k of one row); A: 1024, B: 1024
     for (int g = tid; g < (A_BYTES + B_BYTES) / 16; g += TC_THREADS) {
       const int off = g < A_BYTES / 16 ? g * 16 : A_BYTES + g * 16;  // A hi | A lo | B hi | B lo
       const float4 x = *reinterpret_cast<const float4 *>(st + off);
-      *reinterpret_cast<float4 *>(st + off + (g < A_BYTES / 16 ? A_BYTES : B_BYTES)) = lo4(x);
+      float4 hi, lo;
+      split(x.x, hi.x, lo.x);
+      split(x.y, hi.y, lo.y);
+      split(x.z, hi.z, lo.z);
+      split(x.w, hi.w, lo.w);
+      *reinterpret_cast<float4 *>(st + off) = hi;
+      *reinterpret_cast<float4 *>(st + off + (g < A_BYTES / 16 ? A_BYTES : B_BYTES)) = lo;
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
