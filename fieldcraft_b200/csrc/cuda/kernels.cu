@@ -136,7 +136,7 @@ constexpr int PANEL_THREADS = 128;
 // Shared memory of a panel launch whose widest panel is padded to p8 columns (a multiple of 8).
 template <class T>
 __host__ __device__ constexpr size_t panel_smem(int p8) {
-  return sizeof(double) * (p8 * (65 + TS) + 512 + 128) + sizeof(T) * p8 * tile_stride<T>();
+  return sizeof(double) * (p8 * (65 + TS) + 1024 + 128) + sizeof(T) * p8 * tile_stride<T>();
 }
 
 template <class T>
@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
   extern __shared__ double sm[];
   double *a = sm;                   // factor, column-major, ld 65 (p8max columns)
   double *inv = a + p8max * 65;     // inv[k * TS + i] = Linv(i, k) (p8max rows)
-  double *tt = inv + p8max * TS;    // 8 x (8 x 8) scratch of the inversion
-  double *dg = tt + 512;            // the matrix's own diagonal entries of the panel's columns
+  double *tt = inv + p8max * TS;    // scratch of the inversion's products (<= 1024 doubles)
+  double *dg = tt + 1024;           // the matrix's own diagonal entries of the panel's columns
   double *dv = dg + 64;             // the pivots' reciprocals
   T *bt = reinterpret_cast<T *>(dv + 64);  // rows below: bt[k * S + r] = L(r0 + r, c0 + k)
   __shared__ int fail;
@@ -256,24 +256,40 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
     }
   }
   __syncthreads();
-  // ... then block forward substitution: Linv_IJ = -Linv_II sum_{K=J}^{I-1} L_IK Linv_KJ
-  for (int d = 1; d < nb8; ++d) {
-    const int outputs = (nb8 - d) * 64;
-    for (int e = tid; e < outputs; e += PANEL_THREADS) {
-      const int J = e >> 6, I = J + d, i = (e >> 3) & 7, j = e & 7;
-      double sum = 0.0;
-      for (int K = J; K < I; ++K)
-#pragma unroll
-        for (int k = 0; k < 8; ++k) sum += a[(8 * K + k) * 65 + 8 * I + i] * inv[(8 * J + j) * TS + 8 * K + k];
-      tt[J * 64 + i * 8 + j] = sum;
+  // ... then by doubling (h = 8, 16, 32): neighbouring inverses A^-1, C^-1 of h columns give the
+  // inverse of [[A, 0], [B, C]], whose lower-left block is -C^-1 (B A^-1); both products on DMMA,
+  // 8 x 8 output tiles round-robin over the warps, T = B A^-1 in the scratch
+  for (int h = 8; h < P8; h *= 2) {
+    int tile = 0;
+    for (int a0 = 0; a0 + h < P8; a0 += 2 * h) {
+      const int c0b = a0 + h, hc = min(h, P8 - c0b);
+      for (int ti = 0; ti < hc; ti += 8)
+        for (int tj = 0; tj < h; tj += 8, ++tile) {
+          if ((tile & 3) != warp) continue;
+          const int g = lane >> 2, tg = lane & 3;
+          double c[2] = {0.0, 0.0};
+          for (int k = tj; k < h; k += 4)  // A^-1 (k, j) = 0 for k < j
+            dmma(c, a[(a0 + k + tg) * 65 + c0b + ti + g], inv[(a0 + tj + g) * TS + a0 + k + tg]);
+          const int base = (a0 / (2 * h)) * h * h;  // the pair's hc x h product, column-major, ld h
+          tt[base + (tj + 2 * tg) * h + ti + g] = c[0];
+          tt[base + (tj + 2 * tg + 1) * h + ti + g] = c[1];
+        }
     }
     __syncthreads();
-    for (int e = tid; e < outputs; e += PANEL_THREADS) {
-      const int J = e >> 6, I = J + d, i = (e >> 3) & 7, j = e & 7;
-      double sum = 0.0;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) sum -= inv[(8 * I + k) * TS + 8 * I + i] * tt[J * 64 + k * 8 + j];
-      inv[(8 * J + j) * TS + 8 * I + i] = sum;
+    tile = 0;
+    for (int a0 = 0; a0 + h < P8; a0 += 2 * h) {
+      const int c0b = a0 + h, hc = min(h, P8 - c0b);
+      const int base = (a0 / (2 * h)) * h * h;
+      for (int ti = 0; ti < hc; ti += 8)
+        for (int tj = 0; tj < h; tj += 8, ++tile) {
+          if ((tile & 3) != warp) continue;
+          const int g = lane >> 2, tg = lane & 3;
+          double c[2] = {0.0, 0.0};
+          for (int k = 0; k <= ti + 4 && k < hc; k += 4)  // C^-1 (i, k) = 0 for k > i
+            dmma(c, inv[(c0b + k + tg) * TS + c0b + ti + g], tt[base + (tj + g) * h + k + tg]);
+          inv[(a0 + tj + 2 * tg) * TS + c0b + ti + g] = -c[0];
+          inv[(a0 + tj + 2 * tg + 1) * TS + c0b + ti + g] = -c[1];
+        }
     }
     __syncthreads();
   }
