@@ -159,83 +159,109 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
   const int nb8 = (pw + 7) >> 3, P8 = 8 * nb8, K4 = (pw + 3) & ~3;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) fail = pw;
-  // the block's lower triangle, identity past pw (so the padded block inverts to the same
-  // leading pw x pw inverse)
-  for (int c = warp; c < P8; c += PANEL_THREADS / 32)
-    for (int r = lane; r < P8; r += 32) {
-      if (r < pw && c < pw && r >= c) {
-        if (sizeof(T) == 8)
-          cp_async8(&a[c * 65 + r], Ls + (c0 + r) + (int64_t)(c0 + c) * m, 8);
-        else
-          a[c * 65 + r] = (double)Ls[(c0 + r) + (int64_t)(c0 + c) * m];
-      } else {
-        a[c * 65 + r] = (r >= pw || c >= pw) && r == c ? 1.0 : 0.0;
-      }
-    }
+  // the matrix's own diagonal entries first (two dependent loads each), then the block's lower
+  // triangle, identity past pw (so the padded block inverts to the same leading pw x pw inverse)
   for (int c = tid; c < pw; c += PANEL_THREADS) {
     const int64_t j = f + c0 + c, ds = t.diag_src[j];
     const double d = ds >= 0 ? val[ds] : 0.0;
     dg[c] = t.scale ? d * t.scale[j] * t.scale[j] : d;
+  }
+  if (sizeof(T) == 8) {
+    for (int c = warp; c < P8; c += PANEL_THREADS / 32)
+      for (int r = lane; r < P8; r += 32) {
+        if (r < pw && c < pw && r >= c)
+          cp_async8(&a[c * 65 + r], Ls + (c0 + r) + (int64_t)(c0 + c) * m, 8);
+        else
+          a[c * 65 + r] = (double)(r == c);
+      }
+  } else {
+    // FP32 panels: every load of the thread in flight before the widening stores
+    float v[16][2];
+#pragma unroll
+    for (int ci = 0; ci < 16; ++ci)
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const int c = warp + 4 * ci, r = lane + 32 * ri;
+        v[ci][ri] = r < pw && c < pw && r >= c ? (float)Ls[(c0 + r) + (int64_t)(c0 + c) * m] : (float)(r == c);
+      }
+#pragma unroll
+    for (int ci = 0; ci < 16; ++ci)
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const int c = warp + 4 * ci, r = lane + 32 * ri;
+        if (c < P8 && r < P8) a[c * 65 + r] = (double)v[ci][ri];
+      }
   }
   for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
   if (rows > 0) load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  // right-looking by strips of 8 columns: one warp factors a strip (two rows a lane, pivots and
-  // multipliers broadcast by shuffles), then the four warps update the trailing lower triangle
-  // with DMMA (a rank-8 update per 8 x 8 block); padding past pw factors as the identity
-  for (int B = 0; B < nb8; ++B) {
+  // right-looking by strips of 8 columns with look-ahead: warp 0 factors a strip (two rows a
+  // lane, pivots and multipliers broadcast by shuffles); then all warps update the next strip's
+  // columns, and warp 0 factors that strip while warps 1-3 update the rest of the trailing lower
+  // triangle (DMMA, a rank-8 update per 8 x 8 block); padding past pw factors as the identity
+  auto factor_strip = [&](int B) {
     const int o = 8 * B;
-    if (warp == 0) {
-      const int r0 = o + lane, r1 = o + 32 + lane;
-      double s0[8], s1[8];
+    const int r0 = o + lane, r1 = o + 32 + lane;
+    double s0[8], s1[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        s0[k] = r0 < P8 ? a[(o + k) * 65 + r0] : 0.0;
-        s1[k] = r1 < P8 ? a[(o + k) * 65 + r1] : 0.0;
+    for (int k = 0; k < 8; ++k) {
+      s0[k] = r0 < P8 ? a[(o + k) * 65 + r0] : 0.0;
+      s1[k] = r1 < P8 ? a[(o + k) * 65 + r1] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double acc = __shfl_sync(0xffffffffu, s0[j], j);
+      const double rd = rsqrt(acc);
+      const double d = acc * rd;
+      if (lane == j) {
+        s0[j] = d;
+        dv[o + j] = rd;
+        if (o + j < pw && (!(acc > PIVOT_TOLERANCE * fabs(dg[o + j])) || !isfinite(acc)) && fail == pw) fail = o + j;
+      } else if (lane > j) {
+        s0[j] *= rd;
       }
+      s1[j] *= rd;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const double acc = __shfl_sync(0xffffffffu, s0[j], j);
-        const double d = sqrt(acc);
-        const double rd = 1.0 / d;
-        if (lane == j) {
-          s0[j] = d;
-          dv[o + j] = rd;
-          if (o + j < pw && (!(acc > PIVOT_TOLERANCE * fabs(dg[o + j])) || !isfinite(acc)) && fail == pw) fail = o + j;
-        } else if (lane > j) {
-          s0[j] *= rd;
-        }
-        s1[j] *= rd;
-#pragma unroll
-        for (int k = j + 1; k < 8; ++k) {
-          const double lk = __shfl_sync(0xffffffffu, s0[j], k);
-          if (lane > j) s0[k] -= s0[j] * lk;
-          s1[k] -= s1[j] * lk;
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if (r0 < P8) a[(o + k) * 65 + r0] = s0[k];
-        if (r1 < P8) a[(o + k) * 65 + r1] = s1[k];
+      for (int k = j + 1; k < 8; ++k) {
+        const double lk = __shfl_sync(0xffffffffu, s0[j], k);
+        if (lane > j) s0[k] -= s0[j] * lk;
+        s1[k] -= s1[j] * lk;
       }
     }
-    __syncthreads();
-    const int nrem = nb8 - B - 1;
-    int q = 0;
-    for (int qi = 0; qi < nrem; ++qi)
-      for (int qj = 0; qj <= qi; ++qj, ++q) {
-        if ((q & 3) != warp) continue;
-        const int I = 8 * (B + 1 + qi), J = 8 * (B + 1 + qj);
-        const int g = lane >> 2, tg = lane & 3;
-        double c[2] = {0.0, 0.0};
-        dmma(c, a[(o + tg) * 65 + I + g], a[(o + tg) * 65 + J + g]);
-        dmma(c, a[(o + 4 + tg) * 65 + I + g], a[(o + 4 + tg) * 65 + J + g]);
-        a[(J + 2 * tg) * 65 + I + g] -= c[0];
-        a[(J + 2 * tg + 1) * 65 + I + g] -= c[1];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (r0 < P8) a[(o + k) * 65 + r0] = s0[k];
+      if (r1 < P8) a[(o + k) * 65 + r1] = s1[k];
+    }
+  };
+  // the rank-8 update by strip B of the 8 x 8 block (I, J) (I >= J > B)
+  auto update_tile = [&](int B, int I, int J) {
+    const int o = 8 * B, g = lane >> 2, tg = lane & 3;
+    double c[2] = {0.0, 0.0};
+    dmma(c, a[(o + tg) * 65 + I + g], a[(o + tg) * 65 + J + g]);
+    dmma(c, a[(o + 4 + tg) * 65 + I + g], a[(o + 4 + tg) * 65 + J + g]);
+    a[(J + 2 * tg) * 65 + I + g] -= c[0];
+    a[(J + 2 * tg + 1) * 65 + I + g] -= c[1];
+  };
+  if (warp == 0) factor_strip(0);
+  __syncthreads();
+  for (int B = 0; B < nb8; ++B) {
+    if (B + 1 < nb8) {
+      // the next strip's block column, all warps
+      for (int qi = B + 1 + warp; qi < nb8; qi += PANEL_THREADS / 32) update_tile(B, 8 * qi, 8 * (B + 1));
+      __syncthreads();
+      if (warp == 0) {
+        factor_strip(B + 1);
+      } else {
+        int q = 0;
+        for (int qj = B + 2; qj < nb8; ++qj)
+          for (int qi = qj; qi < nb8; ++qi, ++q)
+            if (q % 3 == warp - 1) update_tile(B, 8 * qi, 8 * qj);
       }
-    __syncthreads();
+      __syncthreads();
+    }
   }
   // inverse: the diagonal 8 x 8 blocks (a column each) ...
   if (tid < P8) {
