@@ -81,6 +81,8 @@ struct fc_chol {
   std::vector<int64_t> rel_off;  // host copies of the relative maps (for planning)
   std::vector<int32_t> rel;
   std::vector<int32_t> level;
+  std::vector<int64_t> a_ptr;    // host copies of the input entries' column starts and their rows
+  std::vector<int32_t> a_lrow;   // in the front (sorted within each assembly column block)
   int64_t l_len = 0, u_len = 0;
   // device
   DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
@@ -199,6 +201,57 @@ int32_t child_ranges(const fc_chol *h, int64_t s, int lo, int hi, std::vector<in
     ranges.push_back(make_int2(a, b));
   }
   return at;
+}
+
+// Assembly tiles of supernode s (see assemble_kernel): ASM_L over the L panel's columns, or the
+// update matrix's columns as ASM_U (only tiles some child lands in: the rest keep what the GEMM
+// stored) or ASM_U_PRODUCT (all tiles). A block of ASSEMBLE_COLS columns is cut into row tiles
+// of ASSEMBLE_ROWS from its first column down; each tile's child ranges come from `at`, per child
+// the first row of its update matrix whose place in the front is >= r, for every r in [0, m].
+void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::AssembleTask> &out,
+                    std::vector<int4> &ranges) {
+  const int m = h->height[s], w = h->width[s];
+  const int jlo = mode == fc::ASM_L ? 0 : w, jhi = mode == fc::ASM_L ? w : m;
+  const int64_t q0 = h->kid_ptr[s], nk = h->kid_ptr[s + 1] - q0;
+  std::vector<std::vector<int32_t>> at((size_t)nk);
+  for (int64_t q = 0; q < nk; ++q) {
+    const int64_t c = h->kids[q0 + q];
+    const int uc = h->height[c] - h->width[c];
+    const int32_t *rel = h->rel.data() + h->rel_off[c];
+    at[q].resize((size_t)m + 1);
+    int i = 0;
+    for (int r = 0; r <= m; ++r) {
+      while (i < uc && rel[i] < r) ++i;
+      at[q][r] = i;
+    }
+  }
+  const int64_t f = h->first[s];
+  for (int j0 = jlo; j0 < jhi; j0 += fc::ASSEMBLE_COLS) {
+    const int j1 = std::min(jhi, j0 + fc::ASSEMBLE_COLS);
+    for (int i0 = j0; i0 < m; i0 += fc::ASSEMBLE_ROWS) {
+      const int i1 = std::min(m, i0 + fc::ASSEMBLE_ROWS);
+      const int32_t base = (int32_t)ranges.size();
+      bool touched = false;
+      for (int64_t q = 0; q < nk; ++q) {
+        const int4 g = make_int4(at[q][j0], at[q][j1], at[q][i0], at[q][i1]);
+        touched |= g.x < g.y && g.z < g.w && g.w - 1 >= g.x;
+        ranges.push_back(g);
+      }
+      if (mode == fc::ASM_U && !touched) {
+        ranges.resize(base);
+        continue;
+      }
+      fc::AssembleTask k{};
+      k.s = (int32_t)s, k.j0 = j0, k.j1 = j1, k.i0 = i0, k.i1 = i1, k.mode = mode, k.ranges = base;
+      if (mode == fc::ASM_L) {
+        const int64_t b0 = h->a_ptr[f + j0], b1 = h->a_ptr[f + j1];
+        const int32_t *lr = h->a_lrow.data();
+        k.e0 = std::lower_bound(lr + b0, lr + b1, i0) - lr;
+        k.e1 = std::lower_bound(lr + b0, lr + b1, i1) - lr;
+      }
+      out.push_back(k);
+    }
+  }
 }
 
 // The address of entry `off` of the L or U arena (entries of h->esize bytes).
@@ -336,7 +389,7 @@ int64_t inverse_doubling(fc_chol *h, const std::vector<int64_t> &S, double *T, i
 }
 
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
-                 std::vector<int2> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
+                 std::vector<int4> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
   auto Up = [&](int64_t off) { return arena_at(h->d_U, h, off); };
   const int NB = fc::NB;
@@ -362,13 +415,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     join();
     const auto &S = lv[l];
     int64_t off = (int64_t)asm_t.size();
-    for (int64_t s : S) {
-      const int w = h->width[s];
-      for (int j0 = 0; j0 < w; j0 += fc::ASSEMBLE_COLS) {
-        const int j1 = std::min(w, j0 + fc::ASSEMBLE_COLS);
-        asm_t.push_back({(int32_t)s, j0, j1, child_ranges(h, s, j0, j1, ranges)});
-      }
-    }
+    for (int64_t s : S) assemble_tiles(h, s, fc::ASM_L, asm_t, ranges);
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
@@ -440,7 +487,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     int64_t go = (int64_t)gemm_t.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
-      if (u <= 0) continue;
+      if (u <= 0 || w <= fc::ASSEMBLE_THIN) continue;  // a thin one's is formed by its assembly
       const int64_t lo = h->loff[s], uo = h->uoff[s];
       for (int bj = 0; bj < u; bj += TNU)
         for (int bi = bj; bi < u; bi += TMU) {
@@ -458,14 +505,15 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     }
     push(h->program, h->fp32 && h->tc ? K_GEMM_TC : K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
     // the children's contributions to the update matrices, on top of -L21 L21^T
+    // (a thin supernode's update matrix is formed here whole, -L21 L21^T included)
     off = (int64_t)asm_t.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s];
-      if (h->kid_ptr[s + 1] == h->kid_ptr[s]) continue;
-      for (int j0 = w; j0 < m; j0 += fc::ASSEMBLE_COLS) {
-        const int j1 = std::min(m, j0 + fc::ASSEMBLE_COLS);
-        asm_t.push_back({(int32_t)s, j0, j1, child_ranges(h, s, j0, j1, ranges)});
-      }
+      if (m == w) continue;
+      if (w <= fc::ASSEMBLE_THIN)
+        assemble_tiles(h, s, fc::ASM_U_PRODUCT, asm_t, ranges);
+      else if (h->kid_ptr[s + 1] > h->kid_ptr[s])
+        assemble_tiles(h, s, fc::ASM_U, asm_t, ranges);
     }
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
   }
@@ -484,7 +532,7 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   h->program.clear();
   const std::vector<std::vector<int64_t>> lv = levels_of(h);
   std::vector<fc::AssembleTask> asm_t;
-  std::vector<int2> ranges;
+  std::vector<int4> ranges;
   std::vector<fc::PanelTask> panel_t;
   std::vector<fc::GemmTask> gemm_t;
   plan_factor(h, lv, asm_t, ranges, panel_t, gemm_t);
@@ -632,6 +680,33 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       if (r == c) diag_src[c] = e;
     }
   }
+  // within each block of ASSEMBLE_COLS columns of a supernode, the entries by their row in the
+  // front (an assembly tile takes the contiguous run of its rows)
+  std::vector<int32_t> a_lrow(h->nnz);
+  {
+    std::vector<std::pair<int32_t, int64_t>> run;
+    std::vector<int64_t> src2, dst2;
+    for (int64_t s = 0; s < ns; ++s) {
+      const int64_t f = sym.first[s], w = sym.first[s + 1] - f, m = sym.height(s);
+      for (int64_t j0 = 0; j0 < w; j0 += fc::ASSEMBLE_COLS) {
+        const int64_t b0 = a_ptr[f + j0], b1 = a_ptr[f + std::min(w, j0 + fc::ASSEMBLE_COLS)];
+        run.clear();
+        for (int64_t q = b0; q < b1; ++q) run.emplace_back((int32_t)((a_dst[q] - h->loff[s]) % m), q);
+        std::sort(run.begin(), run.end());
+        src2.resize(run.size());
+        dst2.resize(run.size());
+        for (size_t q = 0; q < run.size(); ++q) {
+          src2[q] = a_src[run[q].second];
+          dst2[q] = a_dst[run[q].second];
+          a_lrow[b0 + q] = run[q].first;
+        }
+        std::copy(src2.begin(), src2.end(), a_src.begin() + b0);
+        std::copy(dst2.begin(), dst2.end(), a_dst.begin() + b0);
+      }
+    }
+  }
+  h->a_ptr = a_ptr;
+  h->a_lrow = std::move(a_lrow);
   h->rel_off = rel_off;
   h->rel = rel;
   auto lv = levels_of(h);
@@ -843,7 +918,7 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
     Mark mark(h, l.kind, l.level, l.count);
     switch (l.kind) {
       case K_ASSEMBLE:
-        fc::launch_assemble(t, h->fp32, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, h->d_ranges.as<int2>(), l.count,
+        fc::launch_assemble(t, h->fp32, d_val, h->d_asm.as<fc::AssembleTask>() + l.off, h->d_ranges.as<int4>(), l.count,
                             st);
         break;
       case K_PANEL:

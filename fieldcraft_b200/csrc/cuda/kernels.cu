@@ -46,71 +46,116 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
 }
 
 // ---- front assembly ----------------------------------------------------------------------------
-// Columns [j0, j1) of supernode s's front, then each child's update matrix added in child order
-// (the multifrontal form of the reference's own(rel(i), rel(c)) -= S(i, c), cholesky.rs:636-686,
-// summed child by child). Columns of the L panel (j < w) are zeroed and take A's entries first,
-// before the panel is factored; columns of the update matrix (j >= w) are assembled after its
-// GEMM stored -L21 L21^T there. With a scale (the mixed-precision factorisation) the entries
-// placed are those of S A S, S = diag(A)^-1/2.
+// One tile of supernode s's front: columns [j0, j1) (at most ASSEMBLE_COLS) by rows [i0, i1) (at
+// most ASSEMBLE_ROWS), built in shared memory and written once. The tile starts as
+//   ASM_L          zero, then A's entries (columns of the L panel, assembled before the panel is
+//                  factored; with a scale, the entries of S A S, S = diag(A)^-1/2);
+//   ASM_U          the update matrix's tile as its GEMM stored it (-L21 L21^T);
+//   ASM_U_PRODUCT  -L21 L21^T formed here (a thin supernode, w <= ASSEMBLE_THIN, whose update
+//                  matrix no GEMM writes: each entry is a w-term dot product of two rows of L21);
+// then each child's update matrix entries that land in the tile are added, child by child (the
+// multifrontal form of the reference's own(rel(i), rel(c)) -= S(i, c), cholesky.rs:636-686).
+// ranges[task.ranges + q] = {columns lo, hi, rows lo, hi} of child q's update matrix whose places
+// fall in the tile; only its lower triangle (row >= column) is read. No destination is read and
+// written through global memory: the child's rows and values stream in coalesced, the scatter is
+// to shared memory, and every entry of the tile's lower part is stored once.
 template <class T>
 __global__ void __launch_bounds__(ASSEMBLE_THREADS) assemble_kernel(Tree t, const double *__restrict__ val,
                                                                     const AssembleTask *__restrict__ tasks,
-                                                                    const int2 *__restrict__ ranges) {
+                                                                    const int4 *__restrict__ ranges) {
+  static_assert(ASSEMBLE_ROWS == ASSEMBLE_THREADS && ASSEMBLE_COLS * 32 == ASSEMBLE_THREADS, "tile shape");
+  __shared__ T tile[ASSEMBLE_COLS][ASSEMBLE_ROWS];
+  __shared__ T lj[ASSEMBLE_THIN][ASSEMBLE_COLS];
   const AssembleTask task = tasks[blockIdx.x];
   const int s = task.s;
-  const int64_t m = t.height[s], w = t.width[s], u = m - w, f = t.first[s];
-  T *L = static_cast<T *>(t.L), *U = static_cast<T *>(t.U);
-  T *Ls = L + t.loff[s];
-  T *Us = U + t.uoff[s];
-  const int j0 = task.j0, j1 = task.j1;
-  const int tid = threadIdx.x;
-  for (int j = j0; j < j1 && j < w; ++j) {
-    T *col = Ls + (int64_t)j * m;
-    for (int64_t i = tid; i < m; i += blockDim.x) col[i] = T(0);
-  }
-  __syncthreads();
-  const int jend = j1 < w ? j1 : (int)w;
-  if (j0 < jend) {
-    const int64_t e0 = t.a_ptr[f + j0], e1 = t.a_ptr[f + jend];
-    if (t.scale) {
-      for (int64_t e = e0 + tid; e < e1; e += blockDim.x)
-        L[t.a_dst[e]] = T(val[t.a_src[e]] * t.scale[t.a_row[e]] * t.scale[t.a_col[e]]);
-    } else {
-      for (int64_t e = e0 + tid; e < e1; e += blockDim.x) L[t.a_dst[e]] = T(val[t.a_src[e]]);
-    }
-  }
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-  const int64_t k0 = t.kid_ptr[s], k1 = t.kid_ptr[s + 1];
-  for (int64_t kp = k0; kp < k1; ++kp) {
-    const int c = t.kids[kp];
-    const int uc = t.height[c] - t.width[c];
-    const int32_t *rel = t.rel + t.rel_off[c];
-    const T *Uc = U + t.uoff[c];
-    const int2 range = ranges[task.ranges + (kp - k0)];
-    const int lo = range.x, hi = range.y;
-    for (int jc = lo + warp; jc < hi; jc += nwarps) {
-      const int64_t J = rel[jc];
-      const T *src = Uc + (int64_t)jc * uc;
-      T *dst = J < w ? Ls + J * m : Us + (J - w) * u - w;
-      // four rows a lane in flight: the loads of a batch are issued before its stores
-      int ic = jc + lane;
-      for (; ic + 96 < uc; ic += 128) {
-        int r[4];
-        T v[4], d[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          r[q] = rel[ic + 32 * q];
-          v[q] = src[ic + 32 * q];
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) d[q] = dst[r[q]];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dst[r[q]] = d[q] + v[q];
-      }
-      for (; ic < uc; ic += 32) dst[rel[ic]] += src[ic];
+  const int m = t.height[s], w = t.width[s], u = m - w;
+  T *Ls = static_cast<T *>(t.L) + t.loff[s];
+  T *Us = static_cast<T *>(t.U) + t.uoff[s];
+  const int j0 = task.j0, nc = task.j1 - task.j0, i0 = task.i0, nr = task.i1 - task.i0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // column jj of the tile, indexed by front row
+  auto column = [&](int jj) -> T * {
+    const int J = j0 + jj;
+    return J < w ? Ls + (int64_t)J * m : Us + (int64_t)(J - w) * u - w;
+  };
+  // thread tid owns tile row tid for the initial values and the store
+  const int ii = tid, r = i0 + tid;
+  if (task.mode == ASM_U_PRODUCT) {
+    for (int q = tid; q < w * nc; q += ASSEMBLE_THREADS) {
+      const int k = q / nc, jj = q - k * nc;
+      lj[k][jj] = Ls[(int64_t)k * m + j0 + jj];
     }
     __syncthreads();
+    if (ii < nr) {
+      T acc[ASSEMBLE_COLS];
+#pragma unroll
+      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = T(0);
+      for (int k = 0; k < w; ++k) {
+        const T a = Ls[(int64_t)k * m + r];
+#pragma unroll
+        for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = fma(a, lj[k][jj], acc[jj]);
+      }
+#pragma unroll
+      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) tile[jj][ii] = -acc[jj];
+    }
+  } else if (task.mode == ASM_U) {
+    if (ii < nr) {
+      T v[ASSEMBLE_COLS];
+#pragma unroll
+      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj)
+        if (jj < nc && r >= j0 + jj) v[jj] = column(jj)[r];
+#pragma unroll
+      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj)
+        if (jj < nc && r >= j0 + jj) tile[jj][ii] = v[jj];
+    }
+  } else {
+#pragma unroll
+    for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) tile[jj][ii] = T(0);
+    __syncthreads();
+    // A's entries of the tile: the block's entries are sorted by row, [e0, e1) are this tile's
+    const int64_t lo = t.loff[s];
+    for (int64_t e = task.e0 + tid; e < task.e1; e += ASSEMBLE_THREADS) {
+      const int p = (int)(t.a_dst[e] - lo), J = p / m, row = p - J * m;
+      const double a = t.scale ? val[t.a_src[e]] * t.scale[t.a_row[e]] * t.scale[t.a_col[e]] : val[t.a_src[e]];
+      tile[J - j0][row - i0] = T(a);
+    }
+  }
+  __syncthreads();
+  // the children: warp q takes the child's q-th column in the tile (a child has at most one column
+  // per tile column), its lanes the rows, eight loads a lane in flight before the adds
+  const int k0 = (int)t.kid_ptr[s], k1 = (int)t.kid_ptr[s + 1];
+  for (int kp = k0; kp < k1; ++kp) {
+    const int4 g = ranges[task.ranges + (kp - k0)];
+    const int jc = g.x + warp;
+    if (g.x < g.y && g.z < g.w) {
+      if (jc < g.y) {
+        const int c = t.kids[kp];
+        const int uc = t.height[c] - t.width[c];
+        const int32_t *rel = t.rel + t.rel_off[c];
+        const T *src = static_cast<const T *>(t.U) + t.uoff[c] + (int64_t)jc * uc;
+        const int jj = rel[jc] - j0;
+        const int a = g.z > jc ? g.z : jc;
+        int at[ASSEMBLE_ROWS / 32];
+        T v[ASSEMBLE_ROWS / 32];
+#pragma unroll
+        for (int q = 0; q < ASSEMBLE_ROWS / 32; ++q) {
+          const int ic = a + lane + 32 * q;
+          if (ic < g.w) {
+            at[q] = rel[ic];
+            v[q] = src[ic];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < ASSEMBLE_ROWS / 32; ++q)
+          if (a + lane + 32 * q < g.w) tile[jj][at[q] - i0] += v[q];
+      }
+      __syncthreads();
+    }
+  }
+  if (ii < nr) {
+#pragma unroll
+    for (int jj = 0; jj < ASSEMBLE_COLS; ++jj)
+      if (jj < nc && r >= j0 + jj) column(jj)[r] = tile[jj][ii];
   }
 }
 
@@ -812,7 +857,7 @@ void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double 
   if (n > 0) scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, diag_src, val, scale);
 }
 
-void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const AssembleTask *tasks, const int2 *ranges,
+void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const AssembleTask *tasks, const int4 *ranges,
                      int count, cudaStream_t st) {
   if (count <= 0) return;
   if (fp32)

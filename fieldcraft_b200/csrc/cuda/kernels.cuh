@@ -13,8 +13,10 @@ constexpr int NB = 64;
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_KC = 16;
 constexpr int GEMM_THREADS = 128;
 constexpr int PANEL_ROWS = 64;  // rows of a panel solved by one CTA
-constexpr int ASSEMBLE_COLS = 8;  // front columns assembled by one CTA
-constexpr int ASSEMBLE_THREADS = 128;
+// A front is assembled by tiles of ASSEMBLE_COLS columns by ASSEMBLE_ROWS rows, one CTA each
+// (a thread per row, a warp per child column); a supernode at most ASSEMBLE_THIN columns wide has
+// its update matrix formed by the assembly itself instead of by a GEMM.
+constexpr int ASSEMBLE_COLS = 8, ASSEMBLE_ROWS = 256, ASSEMBLE_THREADS = 256, ASSEMBLE_THIN = 16;
 constexpr int SPLIT_K = 512;  // K chunk of a split GEMM (a long sum over few outputs)
 // The solve applies the inverse of a supernode's diagonal block SB columns at a time: the inverses
 // of its diagonal blocks of up to SB columns are formed during the factorisation (from the 64 x 64
@@ -52,10 +54,13 @@ struct Tree {
                             // lower triangular, zero above)
 };
 
-// Front columns [j0, j1) of supernode s; ranges[q] (from `ranges`) is child q's columns (in its
-// update matrix) that land in them.
+// Front tile columns [j0, j1) x rows [i0, i1) of supernode s; ranges[q] (from `ranges`) is child
+// q's {columns lo, hi, rows lo, hi} of its update matrix that land in the tile; [e0, e1) are the
+// input entries of an ASM_L tile.
+enum AssembleMode : int32_t { ASM_L = 0, ASM_U = 1, ASM_U_PRODUCT = 2 };
 struct AssembleTask {
-  int32_t s, j0, j1, ranges;
+  int32_t s, j0, j1, i0, i1, mode, ranges, pad;
+  int64_t e0, e1;
 };
 // Panel [c0, c1) of supernode s: factor its diagonal block, invert it, and solve the rows
 // [r0, r1) below it (r0 >= c1; an empty range for a task that only keeps the block). The task
@@ -182,7 +187,7 @@ void launch_gemm_tc(const GemmTask *tasks, int count, DeviceStatus *status, cuda
 // S = diag(A)^-1/2 for the mixed-precision factorisation.
 void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double *scale, cudaStream_t st);
 void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const AssembleTask *tasks,
-                     const int2 *ranges, int count, cudaStream_t st);
+                     const int4 *ranges, int count, cudaStream_t st);
 // p8max: the widest panel of the launch, rounded up to a multiple of 8 (sizes shared memory).
 void launch_panel(const Tree &t, bool fp32, const double *upper_val, const PanelTask *tasks, int count,
                   DeviceStatus *status, int p8max, cudaStream_t st);
