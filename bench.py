@@ -39,7 +39,8 @@ SAMPLE_EL = 24  # the CPU baseline's bounded sample: the same generator at 24^3 
 KERNEL_KINDS = [(0, "assemble"), (1, "panel"), (3, "gemm"), (12, "gemm_tcgen05"), (10, "inverse_products"),
                 (11, "inverse_blocks"),
                 (18, "solve_reduce"), (19, "solve_gemm"), (20, "solve_assemble"), (21, "solve_gather"),
-                (22, "solve_fwd_inverse"), (23, "solve_bwd_inverse")]
+                (22, "solve_fwd_inverse"), (23, "solve_bwd_inverse"), (29, "solve_thin_fwd"),
+                (30, "solve_thin_bwd")]
 
 
 def parse():
@@ -488,7 +489,7 @@ def main():
     if args.profile_only:
         # the launch counts per step (for choosing which launches a profiler captures), then the
         # warm-up steps and nothing else
-        kinds = 26
+        kinds = 32
         ms_k = np.zeros(kinds)
         cnt_k = np.zeros(kinds, np.int64)
         lib.fc_chol_profile(f.handle, 1)
@@ -542,7 +543,7 @@ def main():
         return
 
     # per-kernel times on the same stream (events around every launch), one profiled step
-    kinds = 26
+    kinds = 32
     ms_k = np.zeros(kinds)
     cnt_k = np.zeros(kinds, np.int64)
     lib.fc_chol_profile(f.handle, 1)
@@ -554,7 +555,7 @@ def main():
     peak = dgemm_peak(torch)
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
     factor_ms = float(ms_k[0:4].sum() + ms_k[10:13].sum())
-    solve_ms = float(ms_k[16:26].sum())
+    solve_ms = float(ms_k[16:32].sum())
     traffic = None
     tf = ROOT / "profiles" / "gemm_kernel_traffic.json"
     if tf.exists():

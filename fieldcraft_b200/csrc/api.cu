@@ -45,7 +45,8 @@ enum Kind {
   K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD,
   K_GEMM_MIXED,  // A in the factor's storage type, B and C FP64
   K_GEMM_F64,    // FP64 throughout (the diagonal blocks' inverses)
-  K_GEMM_TC      // FP32 3xTF32 on tcgen05 (the update matrices of the mixed-precision factor)
+  K_GEMM_TC,     // FP32 3xTF32 on tcgen05 (the update matrices of the mixed-precision factor)
+  K_SOLVE_THIN_FWD, K_SOLVE_THIN_BWD  // the thin supernodes' steps of a solve level
 };
 
 struct Launch {
@@ -103,6 +104,9 @@ struct fc_chol {
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
   DeviceBuf d_x, d_x2, d_v, d_part, d_voff, d_b, d_srow, d_sranges, d_spanel, d_sgemm, d_sreduce;
+  DeviceBuf d_thin, d_tranges, d_tbwd, d_tpart, d_tcount;  // the thin supernodes' solve tasks
+  int solve_lg = 6;
+  int64_t solve_tcount = 0;
   std::vector<Launch> fwd, bwd;
   // the solve as two dependency-driven persistent launches instead of level by level
   // (FC_OPTION_SOLVE_SCHEDULE, or FC_SOLVE_PERSISTENT=1 in the environment)
@@ -973,6 +977,11 @@ struct SolvePlan {
   std::vector<int64_t> voff;
   int64_t vsum = 0;
   int64_t psum = 0;  // doubles of the split GEMMs' partial tiles
+  int lg = 6;        // the thin tasks' block of right-hand sides: 1 << lg columns
+  int64_t tpart = 0, tcount = 0;  // the thin backward chunks' partial sums and counters (a level's)
+  std::vector<fc::ThinTask> thin;
+  std::vector<int4> tranges;
+  std::vector<fc::ThinBwdTask> tbwd;
   std::vector<fc::ReduceTask> reduce;
   std::vector<fc::RowTask> rows;
   std::vector<int2> ranges;
@@ -1000,6 +1009,20 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
     most = std::max(most, level);
   }
   p.psum = most;
+  p.lg = 0;
+  while ((1 << p.lg) < std::min(R, 64)) ++p.lg;
+  const int64_t jb = (R + 63) / 64;
+  for (const auto &S : lv) {
+    int64_t part = 0, count = 0;
+    for (int64_t s : S) {
+      const int64_t u = h->height[s] - h->width[s];
+      if (h->width[s] > fc::SOLVE_THIN || u <= fc::THIN_CHUNK) continue;
+      part += (u + fc::THIN_CHUNK - 1) / fc::THIN_CHUNK * fc::SOLVE_THIN * 64 * jb;
+      count += jb;
+    }
+    p.tpart = std::max(p.tpart, part);
+    p.tcount = std::max(p.tcount, count);
+  }
 }
 
 void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, double *part, SolvePlan &p) {
@@ -1010,14 +1033,37 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
   std::vector<fc::GemmTask> &gemm = p.gemm;
   std::vector<Launch> &fwd = p.fwd, &bwd = p.bwd;
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
+  auto thin = [&](int64_t s) { return h->width[s] <= fc::SOLVE_THIN; };
+  const int RP = 1 << p.lg, TR = fc::THIN_ROWS;
   // forward
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
+    const int64_t to = (int64_t)p.thin.size();
+    for (int64_t s : S) {
+      if (!thin(s)) continue;
+      const int m = h->height[s], w = h->width[s];
+      const int64_t q0 = h->kid_ptr[s], q1 = h->kid_ptr[s + 1];
+      for (int i0 = w; i0 < m || i0 == w; i0 += TR) {
+        const int i1 = std::min(m, i0 + TR);
+        const int32_t at = (int32_t)p.tranges.size();
+        for (int64_t q = q0; q < q1; ++q) {
+          const int64_t c = h->kids[q];
+          const int uc = h->height[c] - h->width[c];
+          const int32_t *rel = h->rel.data() + h->rel_off[c];
+          auto pos = [&](int r) { return (int)(std::lower_bound(rel, rel + uc, r) - rel); };
+          p.tranges.push_back(make_int4(pos(w), pos(i0), pos(i1), 0));
+        }
+        for (int j0 = 0; j0 < R; j0 += RP)
+          p.thin.push_back({(int32_t)s, i0, i1, j0, at, i0 == w ? 1 : 0, h->ioff[s]});
+        if (i1 >= m) break;
+      }
+    }
+    push(fwd, K_SOLVE_THIN_FWD, to, (int64_t)p.thin.size() - to, (int)l);
     int64_t ro = (int64_t)rows.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s];
       const bool kids = h->kid_ptr[s + 1] > h->kid_ptr[s];
-      if (!kids && m == w) continue;
+      if (thin(s) || (!kids && m == w)) continue;
       for (int i0 = kids ? 0 : w; i0 < m; i0 += 64) {
         const int i1 = std::min(m, i0 + 64);
         rows.push_back({(int32_t)s, i0, i1, child_ranges(h, s, i0, i1, p.ranges)});
@@ -1027,13 +1073,14 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
     // blocks of SB columns: y = Dinv x (a GEMM with the block's inverse), then the front rows
     // below the block -= L(rows, block) y
     int K = 0;
-    for (int64_t s : S) K = std::max(K, (h->width[s] + fc::SB - 1) / fc::SB);
+    for (int64_t s : S)
+      if (!thin(s)) K = std::max(K, (h->width[s] + fc::SB - 1) / fc::SB);
     for (int k = 0; k < K; ++k) {
       int64_t go = (int64_t)gemm.size();
       for (int64_t s : S) {
         const int w = h->width[s];
         const int64_t f = h->first[s];
-        if (k * fc::SB >= w) continue;
+        if (thin(s) || k * fc::SB >= w) continue;
         int bw;
         const int64_t base = inv_block(h, s, k, bw);
         const int c0 = k * fc::SB;
@@ -1056,7 +1103,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
       for (int64_t s : S) {
         const int w = h->width[s], m = h->height[s];
         const int64_t f = h->first[s];
-        if (k * fc::SB >= w) continue;
+        if (thin(s) || k * fc::SB >= w) continue;
         int bw;
         inv_block(h, s, k, bw);
         const int c0 = k * fc::SB, c1 = c0 + bw;
@@ -1082,8 +1129,27 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
   // backward
   for (int64_t l = (int64_t)lv.size() - 1; l >= 0; --l) {
     const auto &S = lv[l];
+    const int64_t tb = (int64_t)p.tbwd.size();
+    int64_t tpat = 0;
+    int32_t tcnt = 0;
+    for (int64_t s : S) {
+      if (!thin(s)) continue;
+      const int u = h->height[s] - h->width[s];
+      const int chunks = u > fc::THIN_CHUNK ? (u + fc::THIN_CHUNK - 1) / fc::THIN_CHUNK : 1;
+      for (int j0 = 0; j0 < R; j0 += RP) {
+        for (int q = 0; q < chunks; ++q)
+          p.tbwd.push_back({(int32_t)s, q * fc::THIN_CHUNK, std::min(u, (q + 1) * fc::THIN_CHUNK), j0, chunks, q,
+                            chunks > 1 ? tcnt : -1, 0, h->ioff[s], chunks > 1 ? tpat : 0});
+        if (chunks > 1) {
+          tpat += (int64_t)chunks * fc::SOLVE_THIN * 64;
+          ++tcnt;
+        }
+      }
+    }
+    push(bwd, K_SOLVE_THIN_BWD, tb, (int64_t)p.tbwd.size() - tb, (int)l);
     int64_t ro = (int64_t)rows.size();
     for (int64_t s : S) {
+      if (thin(s)) continue;
       const int u = h->height[s] - h->width[s];
       for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
     }
@@ -1091,7 +1157,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
     int64_t go = (int64_t)gemm.size(), ro2 = (int64_t)p.reduce.size(), pat = 0;
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
-      if (u <= 0) continue;
+      if (u <= 0 || thin(s)) continue;
       const int64_t lo = h->loff[s];
       const bool split = u > 2 * fc::SPLIT_K;
       const int chunks = split ? (u + fc::SPLIT_K - 1) / fc::SPLIT_K : 1;
@@ -1128,13 +1194,14 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
     // blocks of SB columns from the last: z = Dinv^T x2 (into x), then the own rows above the
     // block -= L(block, rows)^T z
     int K = 0;
-    for (int64_t s : S) K = std::max(K, (h->width[s] + fc::SB - 1) / fc::SB);
+    for (int64_t s : S)
+      if (!thin(s)) K = std::max(K, (h->width[s] + fc::SB - 1) / fc::SB);
     for (int k = K - 1; k >= 0; --k) {
       int64_t go = (int64_t)gemm.size();
       for (int64_t s : S) {
         const int w = h->width[s];
         const int64_t f = h->first[s];
-        if (k * fc::SB >= w) continue;
+        if (thin(s) || k * fc::SB >= w) continue;
         int bw;
         const int64_t base = inv_block(h, s, k, bw);
         const int c0 = k * fc::SB;
@@ -1157,7 +1224,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
       for (int64_t s : S) {
         const int w = h->width[s], m = h->height[s];
         const int64_t f = h->first[s];
-        if (k * fc::SB >= w || k == 0) continue;
+        if (thin(s) || k * fc::SB >= w || k == 0) continue;
         int bw;
         inv_block(h, s, k, bw);
         const int c0 = k * fc::SB;
@@ -1587,7 +1654,9 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
       h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
       h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess ||
-      h->d_part.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.psum, 1)) != cudaSuccess) {
+      h->d_part.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.psum, 1)) != cudaSuccess ||
+      h->d_tpart.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.tpart, 1)) != cudaSuccess ||
+      h->d_tcount.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount, 1)) != cudaSuccess) {
     h->solve_R = 0;
     set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
     return FC_OUT_OF_MEMORY;
@@ -1600,9 +1669,13 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   for (const auto &g : p.gemm) h->gemm_flops_solve += task_flops(g);
   if ((e = upload(h->d_srow, p.rows, h->stream)) != cudaSuccess || (e = upload(h->d_sranges, p.ranges, h->stream)) != cudaSuccess ||
       (e = upload(h->d_spanel, p.panels, h->stream)) != cudaSuccess || (e = upload(h->d_sreduce, p.reduce, h->stream)) != cudaSuccess ||
-      (e = upload(h->d_sgemm, p.gemm, h->stream)) != cudaSuccess)
+      (e = upload(h->d_sgemm, p.gemm, h->stream)) != cudaSuccess || (e = upload(h->d_thin, p.thin, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_tranges, p.tranges, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_tbwd, p.tbwd, h->stream)) != cudaSuccess)
     return cuda_fail(st, e, "solve plan");
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
+  h->solve_lg = p.lg;
+  h->solve_tcount = p.tcount;
   h->solve_R = R;
   return FC_OK;
 }
@@ -1616,12 +1689,20 @@ struct SolveBuffers {
   const fc::SolveTask *panels;
   const fc::GemmTask *gemm;
   const fc::ReduceTask *reduce;
+  const fc::ThinTask *thin;
+  const int4 *tranges;
+  const fc::ThinBwdTask *tbwd;
+  double *tpart;
+  int32_t *tcount;
+  int lg;
 };
 
 SolveBuffers own_buffers(fc_chol *h) {
-  return {h->d_x.as<double>(),       h->d_x2.as<double>(),        h->d_v.as<double>(),
-          h->d_voff.as<int64_t>(),     h->d_srow.as<fc::RowTask>(), h->d_sranges.as<int2>(),
-          h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>(), h->d_sreduce.as<fc::ReduceTask>()};
+  return {h->d_x.as<double>(),         h->d_x2.as<double>(),           h->d_v.as<double>(),
+          h->d_voff.as<int64_t>(),       h->d_srow.as<fc::RowTask>(),    h->d_sranges.as<int2>(),
+          h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>(), h->d_sreduce.as<fc::ReduceTask>(),
+          h->d_thin.as<fc::ThinTask>(),  h->d_tranges.as<int4>(),        h->d_tbwd.as<fc::ThinBwdTask>(),
+          h->d_tpart.as<double>(),       h->d_tcount.as<int32_t>(),      h->solve_lg};
 }
 
 void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveBuffers &b, int R, int64_t &launches) {
@@ -1640,6 +1721,12 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
         break;
       case K_REDUCE: fc::launch_reduce(b.reduce + l.off, l.count, st); break;
+      case K_SOLVE_THIN_FWD:
+        fc::launch_thin_fwd(t, h->fp32, b.x, b.x2, b.v, b.voff, R, b.lg, b.thin + l.off, b.tranges, l.count, st);
+        break;
+      case K_SOLVE_THIN_BWD:
+        fc::launch_thin_bwd(t, h->fp32, b.x, b.x2, R, b.lg, b.tbwd + l.off, b.tpart, b.tcount, l.count, st);
+        break;
     }
     ++launches;
   }
@@ -1693,6 +1780,8 @@ void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
     return;
   }
   const SolveBuffers b = own_buffers(h);
+  // the thin backward chunks' counters start at zero (their last chunk also leaves them so)
+  cudaMemsetAsync(h->d_tcount.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(h->solve_tcount, 1), h->stream);
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
   run_solve_program(h, h->fwd, b, R, launches);
   run_solve_program(h, h->bwd, b, R, launches);
@@ -2088,7 +2177,8 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   if (e != cudaSuccess) return cuda_fail(status, e, "cudaGetSymbolAddress of the solve scratch");
   const int R = nrhs;
   // Layout in the scratch: x | x2 | v | partial tiles | voff | row tasks | child ranges | panel
-  // tasks | GEMM tasks | reduction tasks.
+  // tasks | GEMM tasks | reduction tasks | thin forward tasks | their child ranges | thin backward
+  // tasks | their partial sums | their counters.
   SolvePlan p;
   solve_offsets(h, R, p);
   const size_t vec = align256(sizeof(double) * (size_t)h->n * R);
@@ -2110,11 +2200,17 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   const size_t at_panels = at_ranges + align256(sizeof(int2) * p.ranges.size());
   const size_t at_gemm = at_panels + align256(sizeof(fc::SolveTask) * p.panels.size());
   const size_t at_reduce = at_gemm + align256(sizeof(fc::GemmTask) * p.gemm.size());
-  const size_t need = at_reduce + sizeof(fc::ReduceTask) * p.reduce.size();
+  const size_t at_thin = at_reduce + align256(sizeof(fc::ReduceTask) * p.reduce.size());
+  const size_t at_tranges = at_thin + align256(sizeof(fc::ThinTask) * p.thin.size());
+  const size_t at_tbwd = at_tranges + align256(sizeof(int4) * p.tranges.size());
+  const size_t at_tpart = at_tbwd + align256(sizeof(fc::ThinBwdTask) * p.tbwd.size());
+  const size_t at_tcount = at_tpart + align256(sizeof(double) * (size_t)p.tpart);
+  const size_t need = at_tcount + sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount, 1);
   if (need > FC_NOALLOC_SCRATCH_BYTES) return too_large(need);
   // Every region is written before it is read in this call: the task lists and offsets here, x by
-  // the permutation, x2 by the forward panels, each update vector's rows zeroed by its assembly,
-  // each partial tile stored by its GEMM task before its reduction reads it.
+  // the permutation, x2 by the forward panels, each update vector's rows zeroed by its assembly
+  // (or stored whole by a thin forward tile), each partial tile stored by its GEMM task before its
+  // reduction reads it, the thin counters zeroed here.
   auto put = [&](size_t at, const void *src, size_t bytes) {
     if (bytes && e == cudaSuccess) e = cudaMemcpyAsync(base + at, src, bytes, cudaMemcpyHostToDevice, h->stream);
   };
@@ -2124,6 +2220,11 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   put(at_panels, p.panels.data(), sizeof(fc::SolveTask) * p.panels.size());
   put(at_gemm, p.gemm.data(), sizeof(fc::GemmTask) * p.gemm.size());
   put(at_reduce, p.reduce.data(), sizeof(fc::ReduceTask) * p.reduce.size());
+  put(at_thin, p.thin.data(), sizeof(fc::ThinTask) * p.thin.size());
+  put(at_tranges, p.tranges.data(), sizeof(int4) * p.tranges.size());
+  put(at_tbwd, p.tbwd.data(), sizeof(fc::ThinBwdTask) * p.tbwd.size());
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(base + at_tcount, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount, 1), h->stream);
   if (e != cudaSuccess) return cuda_fail(status, e, "copy of the solve plan into the scratch");
   const SolveBuffers b{reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
                        reinterpret_cast<double *>(base + at_v), reinterpret_cast<const int64_t *>(base + at_voff),
@@ -2131,7 +2232,13 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
                        reinterpret_cast<const int2 *>(base + at_ranges),
                        reinterpret_cast<const fc::SolveTask *>(base + at_panels),
                        reinterpret_cast<const fc::GemmTask *>(base + at_gemm),
-                       reinterpret_cast<const fc::ReduceTask *>(base + at_reduce)};
+                       reinterpret_cast<const fc::ReduceTask *>(base + at_reduce),
+                       reinterpret_cast<const fc::ThinTask *>(base + at_thin),
+                       reinterpret_cast<const int4 *>(base + at_tranges),
+                       reinterpret_cast<const fc::ThinBwdTask *>(base + at_tbwd),
+                       reinterpret_cast<double *>(base + at_tpart),
+                       reinterpret_cast<int32_t *>(base + at_tcount),
+                       p.lg};
   int64_t launches = 0;
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, b.x, R, h->tree.scale, h->stream);
   run_solve_program(h, p.fwd, b, R, launches);

@@ -664,6 +664,216 @@ __global__ void __launch_bounds__(256) solve_assemble_kernel(Tree t, double *__r
   }
 }
 
+// ---- thin supernodes' solve steps ---------------------------------------------------------------
+// Forward, one tile (THIN_ROWS rows) of a thin supernode's update vector: the own rows (x plus the
+// children's rows that land on them, child by child), y = Dinv x, then the tile = -L(rows, :) y
+// plus the children's rows that land in it, stored once. Every tile of the supernode forms y the
+// same way (w <= SOLVE_THIN rows), so no tile waits for another. Each phase issues its global
+// loads together (the tile's rows of L, the inverse and the own rows are staged in shared memory
+// first; a child's rows are read a warp per row, several rows in flight). Values stay FP64; an
+// FP32 L is widened. Per entry the operations and their order do not depend on R.
+constexpr int THIN_THREADS = 256, THIN_WARPS = THIN_THREADS / 32;
+
+template <class T>
+__global__ void __launch_bounds__(THIN_THREADS) thin_fwd_kernel(Tree t, const double *__restrict__ x,
+                                                                double *__restrict__ x2, double *__restrict__ v,
+                                                                const int64_t *__restrict__ voff, int R, int lg,
+                                                                const ThinTask *__restrict__ tasks,
+                                                                const int4 *__restrict__ ranges) {
+  __shared__ double tile[THIN_ROWS * 64];
+  __shared__ double xs[SOLVE_THIN * 64], ys[SOLVE_THIN * 64];
+  __shared__ double lt[SOLVE_THIN * THIN_ROWS];  // lt[k * THIN_ROWS + r] = L(i0 + r, k)
+  __shared__ double di[SOLVE_THIN * SOLVE_THIN];
+  const ThinTask task = tasks[blockIdx.x];
+  const int s = task.s, RP = 1 << lg, j0 = task.j0, nj = min(RP, R - j0);
+  const int m = t.height[s], w = t.width[s];
+  const int64_t f = t.first[s];
+  const T *Ls = static_cast<const T *>(t.L) + t.loff[s];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int k0 = (int)t.kid_ptr[s], k1 = (int)t.kid_ptr[s + 1];
+  const int i0 = task.i0, nr = task.i1 - task.i0;
+#pragma unroll
+  for (int q = 0; q < SOLVE_THIN * 64 / THIN_THREADS; ++q) {
+    const int e = tid + q * THIN_THREADS, k = e >> 6, j = e & 63;
+    if (k < w && j < RP) xs[(k << lg) + j] = j < nj ? x[(f + k) * R + j0 + j] : 0.0;
+    if (k < w) lt[k * THIN_ROWS + j] = j < nr ? (double)Ls[(int64_t)k * m + i0 + j] : 0.0;
+  }
+  if (tid < w * w) di[tid] = t.Dinv[task.dinv + tid];
+  __syncthreads();
+  for (int kp = k0; kp < k1; ++kp) {
+    const int4 g = ranges[task.ranges + (kp - k0)];
+    if (g.x == 0) continue;  // the same for the whole block
+    const int c = t.kids[kp];
+    const int32_t *rel = t.rel + t.rel_off[c];
+    const double *vc = v + voff[c];
+    // at most w rows: a warp each
+    for (int ic = warp; ic < g.x; ic += THIN_WARPS) {
+      const int row = rel[ic];
+      for (int j = lane; j < nj; j += 32) xs[(row << lg) + j] += vc[(int64_t)ic * R + j0 + j];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < w << lg; e += THIN_THREADS) {
+    const int i = e >> lg, j = e & (RP - 1);
+    double acc = 0.0;
+    for (int k = 0; k <= i; ++k) acc = fma(di[i + k * w], xs[(k << lg) + j], acc);
+    ys[e] = acc;
+    if (task.first && j < nj) x2[(f + i) * R + j0 + j] = acc;
+  }
+  __syncthreads();
+  for (int e = tid; e < nr << lg; e += THIN_THREADS) {
+    const int r = e >> lg, j = e & (RP - 1);
+    double acc = 0.0;
+    for (int k = 0; k < w; ++k) acc = fma(lt[k * THIN_ROWS + r], ys[(k << lg) + j], acc);
+    tile[e] = -acc;
+  }
+  __syncthreads();
+  for (int kp = k0; kp < k1; ++kp) {
+    const int4 g = ranges[task.ranges + (kp - k0)];
+    if (g.y >= g.z) continue;  // the same for the whole block
+    const int c = t.kids[kp];
+    const int32_t *rel = t.rel + t.rel_off[c];
+    const double *vc = v + voff[c];
+    // a warp per child row (they land on distinct rows), four rows a warp in flight
+    for (int b = g.y + warp; b < g.z; b += 4 * THIN_WARPS) {
+      int at[4];
+      double va[4], vb[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int ic = b + q * THIN_WARPS;
+        at[q] = -1;
+        if (ic < g.z) {
+          at[q] = (rel[ic] - i0) << lg;
+          const double *src = vc + (int64_t)ic * R + j0;
+          va[q] = lane < nj ? src[lane] : 0.0;
+          vb[q] = lane + 32 < nj ? src[lane + 32] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (at[q] >= 0) {
+          if (lane < nj) tile[at[q] + lane] += va[q];
+          if (lane + 32 < nj) tile[at[q] + lane + 32] += vb[q];
+        }
+    }
+    __syncthreads();
+  }
+  double *vs = v + voff[s];
+  for (int e = tid; e < nr << lg; e += THIN_THREADS) {
+    const int r = e >> lg, j = e & (RP - 1);
+    if (j < nj) vs[(int64_t)(i0 + r - w) * R + j0 + j] = tile[e];
+  }
+}
+
+// Backward, one chunk (THIN_CHUNK rows) of a thin supernode's rows past its columns:
+// z_part = L21(rows, :)^T x(rows), the rows' final values read straight from x. The chunk's row
+// indices and rows of L21 are staged in shared memory; warp q takes rows q, q + 8, ... (a row's
+// right-hand sides across its lanes, four rows in flight), and the warps' sums are added in warp
+// order, whatever R is. A supernode of several chunks keeps the partial sums; the last chunk to
+// finish (an atomic count, reset by it for the next solve; no CTA waits) adds them in chunk order
+// and forms z = x2 - sum and x = Dinv^T z on the supernode's own rows.
+template <class T>
+__global__ void __launch_bounds__(THIN_THREADS) thin_bwd_kernel(Tree t, double *__restrict__ x,
+                                                                const double *__restrict__ x2, int R, int lg,
+                                                                const ThinBwdTask *__restrict__ tasks,
+                                                                double *__restrict__ part,
+                                                                int32_t *__restrict__ counters) {
+  __shared__ int32_t ridx[THIN_CHUNK];
+  __shared__ double lt[THIN_CHUNK * SOLVE_THIN];  // lt[i * SOLVE_THIN + k] = L21(k0 + i, k)
+  __shared__ double red[THIN_WARPS * SOLVE_THIN * 64];
+  __shared__ double zs[SOLVE_THIN * 64];
+  __shared__ int last;
+  const ThinBwdTask task = tasks[blockIdx.x];
+  const int s = task.s, RP = 1 << lg, j0 = task.j0, nj = min(RP, R - j0);
+  const int m = t.height[s], w = t.width[s];
+  const int64_t f = t.first[s];
+  const T *Lb = static_cast<const T *>(t.L) + t.loff[s] + w;  // Lb[k m + i] = L21(i, k)
+  const int32_t *rows = t.rows + t.rows_off[s] + w;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int n = task.k1 - task.k0;
+  if (tid < n) ridx[tid] = rows[task.k0 + tid];
+#pragma unroll
+  for (int q = 0; q < THIN_CHUNK * SOLVE_THIN / THIN_THREADS; ++q) {
+    const int e = tid + q * THIN_THREADS, k = e / THIN_CHUNK, i = e - k * THIN_CHUNK;
+    if (k < w && i < n) lt[i * SOLVE_THIN + k] = (double)Lb[(int64_t)k * m + task.k0 + i];
+  }
+  __syncthreads();
+  double acc[SOLVE_THIN][2];
+#pragma unroll
+  for (int k = 0; k < SOLVE_THIN; ++k) acc[k][0] = acc[k][1] = 0.0;
+  const bool la = lane < nj, lb = lane + 32 < nj;
+  for (int b = warp; b < n; b += 4 * THIN_WARPS) {
+    double xa[4], xb[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = b + q * THIN_WARPS;
+      xa[q] = xb[q] = 0.0;
+      if (i < n) {
+        const double *src = x + (int64_t)ridx[i] * R + j0;
+        if (la) xa[q] = src[lane];
+        if (lb) xb[q] = src[lane + 32];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = b + q * THIN_WARPS;
+      if (i < n) {
+#pragma unroll
+        for (int k = 0; k < SOLVE_THIN; ++k)
+          if (k < w) {
+            const double l = lt[i * SOLVE_THIN + k];
+            acc[k][0] = fma(l, xa[q], acc[k][0]);
+            acc[k][1] = fma(l, xb[q], acc[k][1]);
+          }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < SOLVE_THIN; ++k)
+    if (k < w) {
+      red[(warp * SOLVE_THIN + k) * 64 + lane] = acc[k][0];
+      red[(warp * SOLVE_THIN + k) * 64 + lane + 32] = acc[k][1];
+    }
+  __syncthreads();
+  for (int e = tid; e < w * 64; e += THIN_THREADS) {
+    const int k = e >> 6, j = e & 63;
+    double sum = 0.0;
+    for (int q = 0; q < THIN_WARPS; ++q) sum += red[(q * SOLVE_THIN + k) * 64 + j];
+    zs[e] = sum;
+  }
+  if (task.chunks > 1) {
+    double *mine = part + task.part + (int64_t)task.chunk * SOLVE_THIN * 64;
+    for (int e = tid; e < w * 64; e += THIN_THREADS) mine[e] = zs[e];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(counters + task.counter, 1) == task.chunks - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const double *all = part + task.part;
+    for (int e = tid; e < w * 64; e += THIN_THREADS) {
+      double sum = 0.0;
+      for (int q = 0; q < task.chunks; ++q) sum += __ldcg(all + (int64_t)q * SOLVE_THIN * 64 + e);
+      zs[e] = sum;
+    }
+    if (tid == 0) counters[task.counter] = 0;
+  }
+  __syncthreads();
+  for (int e = tid; e < w * 64; e += THIN_THREADS) {
+    const int k = e >> 6, j = e & 63;
+    zs[e] = j < nj ? x2[(f + k) * R + j0 + j] - zs[e] : 0.0;
+  }
+  __syncthreads();
+  const double *Di = t.Dinv + task.dinv;
+  for (int e = tid; e < w * 64; e += THIN_THREADS) {
+    const int i = e >> 6, j = e & 63;
+    if (j >= nj) continue;
+    double acc2 = 0.0;
+    for (int k = i; k < w; ++k) acc2 = fma(Di[k + i * w], zs[(k << 6) + j], acc2);
+    x[(f + i) * R + j0 + j] = acc2;
+  }
+}
+
 // v_s rows [i0, i1) <- x at the supernode's rows below its columns (final by the backward pass).
 __global__ void __launch_bounds__(256) solve_gather_kernel(Tree t, const double *__restrict__ x, double *__restrict__ v,
                                                            const int64_t *__restrict__ voff, int R,
@@ -893,6 +1103,24 @@ void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st) {
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,
                            const int2 *ranges, int count, cudaStream_t st) {
   if (count > 0) solve_assemble_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks, ranges);
+}
+
+void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, double *v, const int64_t *voff, int R,
+                     int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st) {
+  if (count <= 0) return;
+  if (fp32)
+    thin_fwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, v, voff, R, lg, tasks, ranges);
+  else
+    thin_fwd_kernel<double><<<count, THIN_THREADS, 0, st>>>(t, x, x2, v, voff, R, lg, tasks, ranges);
+}
+
+void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int R, int lg, const ThinBwdTask *tasks,
+                     double *part, int32_t *counters, int count, cudaStream_t st) {
+  if (count <= 0) return;
+  if (fp32)
+    thin_bwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
+  else
+    thin_bwd_kernel<double><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
 }
 
 void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,

@@ -97,9 +97,28 @@ struct SolveTask {
   int32_t s, c0, c1, r0, r1, j0, j1, keep;
   int64_t doff;
 };
-// Solve front rows [i0, i1) of supernode s; `ranges` as in AssembleTask, for the children's rows.
+// Solve front rows [i0, i1) of supernode s; ranges[q] (from `ranges`) is child q's rows of its
+// update vector whose places fall in [i0, i1).
 struct RowTask {
   int32_t s, i0, i1, ranges;
+};
+
+// A supernode at most SOLVE_THIN columns wide takes each direction of the solve in one launch:
+// forward, ThinTask tiles of its update vector (rows [i0, i1) of the front, right-hand sides from
+// j0), each forming y = Dinv x of the supernode's own rows itself (`first` also stores it); per
+// child the int4 at ranges[q] is {own rows' end, tile rows lo, hi, 0} in its update vector.
+// Backward, ThinBwdTask chunks of the rows past the columns: each sums L21^T x over its rows, and
+// the last chunk to finish (a counter) adds the chunks' sums in order and applies Dinv^T.
+constexpr int SOLVE_THIN = 8;
+constexpr int THIN_ROWS = 64;      // update-vector rows of a forward tile (by up to 64 right-hand sides)
+constexpr int THIN_CHUNK = 128;    // rows past the columns per backward task
+struct ThinTask {
+  int32_t s, i0, i1, j0, ranges, first;
+  int64_t dinv;  // the supernode's diagonal-block inverse in Dinv (w x w, column-major)
+};
+struct ThinBwdTask {
+  int32_t s, k0, k1, j0, chunks, chunk, counter, pad;
+  int64_t dinv, part;  // part: the chunks' partial sums (chunks x SOLVE_THIN x 64 doubles)
 };
 
 // ---- the solve as one dependency-driven launch per direction ----------------------------------
@@ -197,6 +216,12 @@ void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st);
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R,
                            const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st);
+// The thin supernodes' steps of a level; lg = log2 of the right-hand-side block (a power of two
+// <= 64 covering R, or 64).
+void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, double *v, const int64_t *voff, int R,
+                     int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st);
+void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int R, int lg, const ThinBwdTask *tasks,
+                     double *part, int32_t *counters, int count, cudaStream_t st);
 void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R,
                          const RowTask *tasks, int count, cudaStream_t st);
 // x_post[i*R + j] = b[perm[i] + j*ld] (times scale[i] if given) and back.

@@ -189,9 +189,11 @@ int64_t fc_chol_trace_read(fc_chol *h, int64_t *out, int64_t cap);
  * measurement hook of the benchmark). enable != 0 starts recording; fc_chol_profile_read waits for
  * the stream and returns, per launch kind, the summed milliseconds and the launch count (arrays of
  * `kinds` entries), then clears them. Kinds: 0 front assembly, 1 panel (factor,
- * invert and solve below a diagonal block), 3 GEMM of the factor; 18 reduction of split sums, 19 GEMM,
- * 20 front assembly, 21 gather, 22 forward panel, 23 backward panel of the solve (level by level);
- * 24 forward, 25 backward persistent launch of the solve (26 covers all). */
+ * invert and solve below a diagonal block), 3 GEMM of the factor, 10 and 11 the two GEMMs of a
+ * doubling step of the diagonal-block inverses, 12 the tcgen05 GEMM of the mixed-precision factor;
+ * 18 reduction of split sums, 19 GEMM, 20 front assembly, 21 gather, 22 forward inverse, 23
+ * backward inverse of the solve (level by level), 24 forward, 25 backward persistent launch of the
+ * solve, 29 forward, 30 backward step of the thin supernodes (32 covers all). */
 int fc_chol_profile(fc_chol *h, int enable);
 int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kinds);
 /* The recorded launches one by one, oldest first, without clearing them: kind (as above), level
