@@ -36,7 +36,8 @@ UNIT = "s"
 N_EL, NRHS, SEED = 48, 64, 2024
 SAMPLE_EL = 24  # the CPU baseline's bounded sample: the same generator at 24^3 elements
 # profile kinds (fc_chol_profile_read) and their names
-KERNEL_KINDS = [(0, "assemble"), (1, "panel"), (3, "gemm"), (12, "gemm_tcgen05"), (10, "inverse_products"),
+KERNEL_KINDS = [(0, "assemble"), (1, "panel"), (3, "gemm"), (12, "gemm_tcgen05"), (15, "pack_tcgen05"),
+                (10, "inverse_products"),
                 (11, "inverse_blocks"),
                 (18, "solve_reduce"), (19, "solve_gemm"), (20, "solve_assemble"), (21, "solve_gather"),
                 (22, "solve_fwd_inverse"), (23, "solve_bwd_inverse"), (29, "solve_thin_fwd"),
@@ -554,7 +555,7 @@ def main():
     gemm_flops = float(f.stat(9))
     peak = dgemm_peak(torch)
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
-    factor_ms = float(ms_k[0:4].sum() + ms_k[10:13].sum())
+    factor_ms = float(ms_k[0:4].sum() + ms_k[10:13].sum() + ms_k[15])
     solve_ms = float(ms_k[16:32].sum())
     traffic = None
     tf = ROOT / "profiles" / "gemm_kernel_traffic.json"

@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "../../include/fieldcraft_chol.h"
+#include <cuda.h>  // CUtensorMap and its encoder's signature (looked up through the runtime)
+
 #include "cuda/kernels.cuh"
 #include "device_buf.hpp"
 #include "host/symbolic.hpp"
@@ -46,7 +48,8 @@ enum Kind {
   K_GEMM_MIXED,  // A in the factor's storage type, B and C FP64
   K_GEMM_F64,    // FP64 throughout (the diagonal blocks' inverses)
   K_GEMM_TC,     // FP32 3xTF32 on tcgen05 (the update matrices of the mixed-precision factor)
-  K_SOLVE_THIN_FWD, K_SOLVE_THIN_BWD  // the thin supernodes' steps of a solve level
+  K_SOLVE_THIN_FWD, K_SOLVE_THIN_BWD,  // the thin supernodes' steps of a solve level
+  K_PACK_TC                            // the tcgen05 products' operands packed (K-major hi | lo)
 };
 
 struct Launch {
@@ -95,6 +98,10 @@ struct fc_chol {
   bool refine_pcg = true;                // refinement by preconditioned CG (else plain refinement)
   bool tc = true;                        // FP32 updates on tcgen05 (FC_TF32_MMA_SYNC=1: on mma.sync)
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
+  // the mixed-precision factor's tcgen05 update products: packed operands (reused level after
+  // level), their pack and tile tasks, and one TMA tensor map per supernode
+  DeviceBuf d_pack, d_pack_t, d_tc_t, d_maps;
+  int64_t pack_len = 0;
   fc::Tree tree{};
   std::vector<Launch> program;
   cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch)
@@ -392,8 +399,15 @@ int64_t inverse_doubling(fc_chol *h, const std::vector<int64_t> &S, double *T, i
   return toff;
 }
 
+// A tensor map of a supernode's packed L21 (u rows of 2 wpad FP32 values at pack offset poff).
+struct MapSpec {
+  int64_t poff, u;
+  int wpad;
+};
+
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
-                 std::vector<int4> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t) {
+                 std::vector<int4> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t,
+                 std::vector<fc::PackTask> &pack_t, std::vector<fc::TcTask> &tc_t, std::vector<MapSpec> &maps) {
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
   auto Up = [&](int64_t off) { return arena_at(h->d_U, h, off); };
   const int NB = fc::NB;
@@ -401,8 +415,8 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
   // tcgen05 path (the first tile of a column block starts on the diagonal, so 'lower' still means
   // local i >= j); the panels' short updates of later columns (K <= 64) stay on 64 x 64 tiles
   const int TM = fc::GEMM_TM;
-  const int TMU = h->fp32 && h->tc ? fc::GEMM_TC_M : fc::GEMM_TM;
-  const int TNU = h->fp32 && h->tc ? fc::GEMM_TC_N : fc::GEMM_TN;
+  const bool tc = h->fp32 && h->tc;
+  h->pack_len = 0;
   int pending_join = -1;  // a lane-1 launch the next lane-0 launch after the panel steps waits for
   auto join = [&]() {
     if (pending_join >= 0 && (int)h->program.size() > pending_join + 1) {
@@ -488,26 +502,55 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       gemm_t.insert(gemm_t.end(), second.begin(), second.end());
       push(h->program, K_GEMM_F64, go, (int64_t)second.size(), (int)l);
     }
-    int64_t go = (int64_t)gemm_t.size();
-    for (int64_t s : S) {
-      const int m = h->height[s], w = h->width[s], u = m - w;
-      if (u <= 0 || w <= fc::ASSEMBLE_THIN) continue;  // a thin one's is formed by its assembly
-      const int64_t lo = h->loff[s], uo = h->uoff[s];
-      for (int bj = 0; bj < u; bj += TNU)
-        for (int bi = bj; bi < u; bi += TMU) {
-          fc::GemmTask g{};
-          g.C = Up(uo + bi + (int64_t)bj * u);
-          g.A = Lp(lo + w + bi);
-          g.B = Lp(lo + w + bj);
-          g.c_si = 1, g.c_sj = u, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
-          g.M = std::min(TMU, u - bi);
-          g.N = std::min(TNU, u - bj);
-          g.K = w;
-          g.flags = (bi == bj ? 1 : 0) | 2;
-          gemm_t.push_back(g);
-        }
+    if (tc) {
+      // pack each supernode's L21 (K-major hi | lo), then its 128 x 128 tiles by TMA + tcgen05
+      const int64_t po = (int64_t)pack_t.size(), to = (int64_t)tc_t.size();
+      int64_t at = 0;
+      for (int64_t s : S) {
+        const int m = h->height[s], w = h->width[s], u = m - w;
+        if (u <= 0 || w <= fc::ASSEMBLE_THIN) continue;  // a thin one's is formed by its assembly
+        const int wpad = (w + fc::TC_KPAD - 1) / fc::TC_KPAD * fc::TC_KPAD;
+        const int32_t map = (int32_t)maps.size();
+        maps.push_back({at, u, wpad});
+        for (int r0 = 0; r0 < u; r0 += fc::TC_PACK_ROWS) pack_t.push_back({(int32_t)s, r0, wpad, 0, at});
+        at += ((int64_t)u * 2 * wpad + 63) / 64 * 64;  // 256-byte aligned regions
+        const int64_t uo = h->uoff[s];
+        for (int bj = 0; bj < u; bj += fc::GEMM_TC_N)
+          for (int bi = bj; bi < u; bi += fc::GEMM_TC_M) {
+            fc::TcTask g{};
+            g.map = map, g.bi = bi, g.bj = bj;
+            g.M = std::min(fc::GEMM_TC_M, u - bi), g.N = std::min(fc::GEMM_TC_N, u - bj), g.K = w, g.wpad = wpad;
+            g.flags = (bi == bj ? 1 : 0) | 2;
+            g.C = static_cast<float *>(Up(uo + bi + (int64_t)bj * u));
+            g.c_sj = u;
+            tc_t.push_back(g);
+          }
+      }
+      h->pack_len = std::max(h->pack_len, at);
+      push(h->program, K_PACK_TC, po, (int64_t)pack_t.size() - po, (int)l);
+      push(h->program, K_GEMM_TC, to, (int64_t)tc_t.size() - to, (int)l);
+    } else {
+      int64_t go = (int64_t)gemm_t.size();
+      for (int64_t s : S) {
+        const int m = h->height[s], w = h->width[s], u = m - w;
+        if (u <= 0 || w <= fc::ASSEMBLE_THIN) continue;  // a thin one's is formed by its assembly
+        const int64_t lo = h->loff[s], uo = h->uoff[s];
+        for (int bj = 0; bj < u; bj += fc::GEMM_TN)
+          for (int bi = bj; bi < u; bi += fc::GEMM_TM) {
+            fc::GemmTask g{};
+            g.C = Up(uo + bi + (int64_t)bj * u);
+            g.A = Lp(lo + w + bi);
+            g.B = Lp(lo + w + bj);
+            g.c_si = 1, g.c_sj = u, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
+            g.M = std::min(fc::GEMM_TM, u - bi);
+            g.N = std::min(fc::GEMM_TN, u - bj);
+            g.K = w;
+            g.flags = (bi == bj ? 1 : 0) | 2;
+            gemm_t.push_back(g);
+          }
+      }
+      push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
     }
-    push(h->program, h->fp32 && h->tc ? K_GEMM_TC : K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
     // the children's contributions to the update matrices, on top of -L21 L21^T
     // (a thin supernode's update matrix is formed here whole, -L21 L21^T included)
     off = (int64_t)asm_t.size();
@@ -539,17 +582,64 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   std::vector<int4> ranges;
   std::vector<fc::PanelTask> panel_t;
   std::vector<fc::GemmTask> gemm_t;
-  plan_factor(h, lv, asm_t, ranges, panel_t, gemm_t);
-  h->gemm_tasks = (int64_t)gemm_t.size();
+  std::vector<fc::PackTask> pack_t;
+  std::vector<fc::TcTask> tc_t;
+  std::vector<MapSpec> specs;
+  plan_factor(h, lv, asm_t, ranges, panel_t, gemm_t, pack_t, tc_t, specs);
+  h->gemm_tasks = (int64_t)(gemm_t.size() + tc_t.size());
   h->gemm_flops_factor = 0;
   for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
+  for (const auto &g : tc_t) {
+    double outputs = (double)g.M * g.N;
+    if (g.flags & 1) {
+      outputs = 0;
+      for (int j = 0; j < g.N; ++j) outputs += std::max(0, g.M - j);
+    }
+    h->gemm_flops_factor += 2.0 * g.K * outputs;
+  }
+  if (!tc_t.empty()) {
+    // the packed operands and their tensor maps (TMA boxes of 128 rows x 32 FP32, 128-byte swizzle)
+    if (h->d_pack.alloc(sizeof(float) * (size_t)std::max<int64_t>(h->pack_len, 1)) != cudaSuccess) {
+      set_status(st, FC_OUT_OF_MEMORY, -1, h->pack_len, 0, "device memory for the packed operands");
+      return FC_OUT_OF_MEMORY;
+    }
+    using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      set_status(st, FC_CUDA_ERROR, -1, 0, 0, "cuTensorMapEncodeTiled is not available");
+      return FC_CUDA_ERROR;
+    }
+    const Encode encode = reinterpret_cast<Encode>(fn);
+    std::vector<CUtensorMap> maps(specs.size());
+    for (size_t i = 0; i < specs.size(); ++i) {
+      const MapSpec &m = specs[i];
+      const cuuint64_t dims[2] = {(cuuint64_t)2 * m.wpad, (cuuint64_t)m.u};
+      const cuuint64_t strides[1] = {(cuuint64_t)2 * m.wpad * sizeof(float)};
+      const cuuint32_t box[2] = {(cuuint32_t)fc::TC_KPAD, (cuuint32_t)fc::GEMM_TC_M};
+      const cuuint32_t estr[2] = {1, 1};
+      const CUresult r = encode(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, h->d_pack.as<float>() + m.poff, dims,
+                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        set_status(st, FC_CUDA_ERROR, -1, (int64_t)r, 0, "cuTensorMapEncodeTiled of a packed operand");
+        return FC_CUDA_ERROR;
+      }
+    }
+    if ((e = upload(h->d_maps, maps, stream)) != cudaSuccess || (e = upload(h->d_pack_t, pack_t, stream)) != cudaSuccess ||
+        (e = upload(h->d_tc_t, tc_t, stream)) != cudaSuccess)
+      return cuda_fail(st, e, "upload of the tcgen05 plan");
+  }
   {
     // ordinals (among the factor's GEMM launches) of the heaviest launch and of the heaviest one
     // whose tasks all have K <= NB (a panel's update of the later columns)
     int64_t ordinal = 0;
     double big = -1, trail = -1;
     for (const Launch &l : h->program) {
-      if (l.kind != K_GEMM && l.kind != K_GEMM_TC) continue;
+      if (l.kind != K_GEMM) continue;
       double fl = 0;
       int kmax = 0;
       for (int64_t q = l.off; q < l.off + l.count; ++q) {
@@ -930,8 +1020,10 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
                          h->d_status.as<fc::DeviceStatus>(), l.width, st);
         break;
       case K_GEMM: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, gk, st); break;
+      case K_PACK_TC: fc::launch_pack_tc(t, h->d_pack_t.as<fc::PackTask>() + l.off, h->d_pack.as<float>(), l.count, st); break;
       case K_GEMM_TC:
-        fc::launch_gemm_tc(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, h->d_status.as<fc::DeviceStatus>(), st);
+        fc::launch_syrk_tc(h->d_tc_t.as<fc::TcTask>() + l.off, h->d_maps.p, l.count, h->d_status.as<fc::DeviceStatus>(),
+                           st);
         break;
       case K_GEMM_MIXED:
         fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count,

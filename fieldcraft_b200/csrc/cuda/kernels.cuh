@@ -198,10 +198,25 @@ void configure_kernels();
 // The operand types of a GEMM launch: FP64 throughout (DMMA); an FP32 A with FP64 B and C (DMMA,
 // the solve on an FP32 factor); FP32 throughout by 3xTF32 (the FP32 factorisation).
 enum class GemmKind { F64, F32A_F64, F32_TF32X3 };
-// FP32 3xTF32 GEMM tasks on the tcgen05 tensor cores (tiles of up to GEMM_TC_M x GEMM_TC_N, A and
-// B with unit row stride); a wait that gives up sets status->timeout.
-constexpr int GEMM_TC_M = 128, GEMM_TC_N = 128;
-void launch_gemm_tc(const GemmTask *tasks, int count, DeviceStatus *status, cudaStream_t st);
+// The mixed-precision factor's update matrices on the tcgen05 tensor cores. Each supernode's L21
+// is first packed as a K-major FP32 array P: row i = [hi(L21(i, 0..wpad)) | lo(...)], wpad = w
+// rounded up to TC_KPAD, at P + poff, by PackTask row blocks of TC_PACK_ROWS. A TcTask is one
+// tile C(bi.., bj..) of up to GEMM_TC_M x GEMM_TC_N of U -= L21 L21^T (flags as GemmTask: 1 lower
+// triangle only, 2 store -product), its operands read by TMA through tensor map `map` of the
+// supernode's P (an array of 128-byte CUtensorMap objects in device memory); a wait that gives up
+// sets status->timeout.
+constexpr int GEMM_TC_M = 128, GEMM_TC_N = 128, TC_KPAD = 32, TC_PACK_ROWS = 64;
+struct PackTask {
+  int32_t s, r0, wpad, pad;
+  int64_t poff;
+};
+struct TcTask {
+  int32_t map, bi, bj, M, N, K, wpad, flags;
+  float *C;
+  int64_t c_sj;  // C(i, j) at C[i + j c_sj]
+};
+void launch_pack_tc(const Tree &t, const PackTask *tasks, float *P, int count, cudaStream_t st);
+void launch_syrk_tc(const TcTask *tasks, const void *maps, int count, DeviceStatus *status, cudaStream_t st);
 
 // S = diag(A)^-1/2 for the mixed-precision factorisation.
 void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double *scale, cudaStream_t st);
