@@ -114,6 +114,7 @@ struct fc_chol {
   DeviceBuf d_thin, d_tranges, d_tbwd, d_tpart, d_tcount;  // the thin supernodes' solve tasks
   int solve_lg = 6;
   int64_t solve_tcount = 0;
+  std::vector<cudaEvent_t> solve_events;  // the solve's level joins of its two streams
   std::vector<Launch> fwd, bwd;
   // the solve as two dependency-driven persistent launches instead of level by level
   // (FC_OPTION_SOLVE_SCHEDULE, or FC_SOLVE_PERSISTENT=1 in the environment)
@@ -152,6 +153,7 @@ struct fc_chol {
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : lane_events)
       if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : solve_events) cudaEventDestroy(e);
     if (fork_event) cudaEventDestroy(fork_event);
     if (join_event) cudaEventDestroy(join_event);
     if (side) cudaStreamDestroy(side);
@@ -1733,6 +1735,16 @@ int solve_wait_status(fc_chol *h, fc_status *st) {
 }
 
 // The handle's own solve buffers and task arrays for R right-hand sides (built once per R).
+std::vector<char> beside(const std::vector<Launch> &prog);
+
+// Events the two-stream solve uses: a fork and a join per level with a thin launch beside wide ones.
+size_t solve_events_needed(const fc_chol *h) {
+  size_t n = 0;
+  for (const auto *prog : {&h->fwd, &h->bwd})
+    for (char c : beside(*prog)) n += c ? 2 : 0;
+  return n;
+}
+
 int plan_solve(fc_chol *h, int R, fc_status *st) {
   if (h->solve_R == R) return FC_OK;
   if (h->solve_graph) {
@@ -1768,6 +1780,11 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
   h->solve_lg = p.lg;
   h->solve_tcount = p.tcount;
+  while (h->solve_events.size() < solve_events_needed(h)) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(st, e, "solve events");
+    h->solve_events.push_back(ev);
+  }
   h->solve_R = R;
   return FC_OK;
 }
@@ -1797,10 +1814,54 @@ SolveBuffers own_buffers(fc_chol *h) {
           h->d_tpart.as<double>(),       h->d_tcount.as<int32_t>(),      h->solve_lg};
 }
 
-void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveBuffers &b, int R, int64_t &launches) {
-  cudaStream_t st = h->stream;
+// Whether each launch of a solve program is the thin launch of a level that also has wide ones
+// (then it can run beside them).
+std::vector<char> beside(const std::vector<Launch> &prog) {
+  std::vector<char> out(prog.size(), 0);
+  for (size_t a = 0; a < prog.size();) {
+    size_t b = a;
+    bool thin = false, wide = false;
+    for (; b < prog.size() && prog[b].level == prog[a].level; ++b) {
+      const bool t = prog[b].kind == K_SOLVE_THIN_FWD || prog[b].kind == K_SOLVE_THIN_BWD;
+      thin |= t;
+      wide |= !t;
+    }
+    if (thin && wide)
+      for (size_t q = a; q < b; ++q)
+        out[q] = prog[q].kind == K_SOLVE_THIN_FWD || prog[q].kind == K_SOLVE_THIN_BWD;
+    a = b;
+  }
+  return out;
+}
+
+// With `events` (two per level that has both a thin and a wide launch, from *ev on), such a
+// level's thin launch runs on the side stream beside its wide launches: the side stream forks
+// from the main one at the level's start and joins it at the level's end (the next level reads
+// what both wrote). Other levels stay on the main stream.
+void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveBuffers &b, int R, int64_t &launches,
+                       const std::vector<cudaEvent_t> *events = nullptr, size_t *ev = nullptr) {
+  const cudaStream_t main = h->stream;
   const fc::Tree &t = h->tree;
-  for (const Launch &l : prog) {
+  const bool lanes = events && ev && h->side;
+  const std::vector<char> side = lanes ? beside(prog) : std::vector<char>(prog.size(), 0);
+  bool forked = false;
+  int level = INT_MIN;
+  for (size_t q = 0; q < prog.size(); ++q) {
+    const Launch &l = prog[q];
+    if (l.level != level) {
+      if (forked) {  // the previous level's join
+        cudaEventRecord((*events)[*ev], h->side);
+        cudaStreamWaitEvent(main, (*events)[(*ev)++], 0);
+        forked = false;
+      }
+      level = l.level;
+    }
+    if (side[q] && !forked) {
+      cudaEventRecord((*events)[*ev], main);
+      cudaStreamWaitEvent(h->side, (*events)[(*ev)++], 0);
+      forked = true;
+    }
+    const cudaStream_t st = side[q] ? h->side : main;
     Mark mark(h, l.kind + 16, l.level, l.count);
     switch (l.kind) {
       case K_SOLVE_ASSEMBLE:
@@ -1821,6 +1882,10 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         break;
     }
     ++launches;
+  }
+  if (forked) {
+    cudaEventRecord((*events)[*ev], h->side);
+    cudaStreamWaitEvent(main, (*events)[(*ev)++], 0);
   }
 }
 
@@ -1875,8 +1940,11 @@ void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   // the thin backward chunks' counters start at zero (their last chunk also leaves them so)
   cudaMemsetAsync(h->d_tcount.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(h->solve_tcount, 1), h->stream);
   fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
-  run_solve_program(h, h->fwd, b, R, launches);
-  run_solve_program(h, h->bwd, b, R, launches);
+  // the thin launches beside the wide ones (not while profiling: then every launch is timed alone)
+  const bool lanes = h->side && !h->profiling && h->solve_events.size() >= solve_events_needed(h);
+  size_t ev = 0;
+  run_solve_program(h, h->fwd, b, R, launches, lanes ? &h->solve_events : nullptr, &ev);
+  run_solve_program(h, h->bwd, b, R, launches, lanes ? &h->solve_events : nullptr, &ev);
   fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->tree.scale, h->stream);
   h->last_solve_launches = launches + 2;
 }
