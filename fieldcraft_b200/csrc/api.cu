@@ -43,7 +43,7 @@ int fail_status(fc_status *st, const Failure &f) {
 }
 
 enum Kind {
-  K_ASSEMBLE, K_PANEL, K_REDUCE, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD,
+  K_ASSEMBLE, K_PANEL, K_UNUSED_2, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD,
   K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD,
   K_GEMM_MIXED,  // A in the factor's storage type, B and C FP64
   K_GEMM_F64,    // FP64 throughout (the diagonal blocks' inverses)
@@ -110,7 +110,7 @@ struct fc_chol {
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
-  DeviceBuf d_x, d_x2, d_v, d_part, d_voff, d_b, d_srow, d_sranges, d_spanel, d_sgemm, d_sreduce;
+  DeviceBuf d_x, d_x2, d_v, d_part, d_voff, d_b, d_srow, d_sranges, d_spanel, d_sgemm;
   DeviceBuf d_thin, d_tranges, d_tbwd, d_tpart, d_tcount;  // the thin supernodes' solve tasks
   int solve_lg = 6;
   int64_t solve_tcount = 0;
@@ -1070,13 +1070,13 @@ int read_status(fc_chol *h, fc_status *st) {
 struct SolvePlan {
   std::vector<int64_t> voff;
   int64_t vsum = 0;
-  int64_t psum = 0;  // doubles of the split GEMMs' partial tiles
+  int64_t psum = 0;    // doubles of the split GEMMs' partial tiles (the largest launch's)
+  int64_t scount = 0;  // their counters (the largest launch's), after the thin ones
   int lg = 6;        // the thin tasks' block of right-hand sides: 1 << lg columns
   int64_t tpart = 0, tcount = 0;  // the thin backward chunks' partial sums and counters (a level's)
   std::vector<fc::ThinTask> thin;
   std::vector<int4> tranges;
   std::vector<fc::ThinBwdTask> tbwd;
-  std::vector<fc::ReduceTask> reduce;
   std::vector<fc::RowTask> rows;
   std::vector<int2> ranges;
   std::vector<fc::SolveTask> panels;
@@ -1090,19 +1090,6 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
   std::vector<int64_t> vsize(h->ns);
   for (int64_t s = 0; s < h->ns; ++s) vsize[s] = (int64_t)(h->height[s] - h->width[s]) * R;
   p.vsum = arena_offsets(h, lv, vsize, p.voff);
-  // the backward update of a supernode's own rows by its rows below (K = u) is split in chunks of
-  // SPLIT_K when u is long; its partial tiles are reused level after level
-  int64_t most = 0;
-  for (const auto &S : lv) {
-    int64_t level = 0;
-    for (int64_t s : S) {
-      const int64_t u = h->height[s] - h->width[s], w = h->width[s];
-      if (u > 2 * fc::SPLIT_K)
-        level += (u + fc::SPLIT_K - 1) / fc::SPLIT_K * ((w + 63) / 64) * ((R + 63) / 64) * 4096;
-    }
-    most = std::max(most, level);
-  }
-  p.psum = most;
   p.lg = 0;
   while ((1 << p.lg) < std::min(R, 64)) ++p.lg;
   const int64_t jb = (R + 63) / 64;
@@ -1119,12 +1106,67 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
   }
 }
 
-void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, double *part, SolvePlan &p) {
+// In a solve launch with too few output tiles to fill the GPU twice, a GEMM whose K is long is
+// split in chunks of SOLVE_KC: the chunks run as separate CTAs and the last one adds their
+// partials in order (GemmTask flag 8). The choice depends on the tiles of one block of 64
+// right-hand sides and on K, not on how many right-hand sides are solved together, so a column's
+// result does not either. Partials and counters are offsets into buffers given at launch, reused
+// launch after launch.
+constexpr int SOLVE_KC = 256;
+
+struct SplitPush {
+  SolvePlan &p;
+  int waves_tiles;  // a launch with fewer output tiles (per block of right-hand sides) is split
+  std::vector<std::pair<fc::GemmTask, std::pair<size_t, size_t>>> pending;
+  int tiles = 0;
+  // g's K range [0, K) may be split; a_es / b_es: bytes of an A / B element; first: g is in the
+  // first block of right-hand sides (counts the launch's tiles)
+  void add(const fc::GemmTask &g, size_t a_es, size_t b_es, bool first) {
+    pending.push_back({g, {a_es, b_es}});
+    tiles += first ? 1 : 0;
+  }
+  // the end of a launch: its tasks go to the plan (split when the launch is short of tiles); its
+  // partials and counters are free again after it
+  void close() {
+    const bool split = tiles < waves_tiles;
+    int64_t at = 0;
+    int32_t cnt = 0;
+    for (auto &pg : pending) {
+      const fc::GemmTask &g = pg.first;
+      if (!split || g.K <= SOLVE_KC + SOLVE_KC / 2) {
+        p.gemm.push_back(g);
+        continue;
+      }
+      const int chunks = (g.K + SOLVE_KC - 1) / SOLVE_KC;
+      for (int q = 0; q < chunks; ++q) {
+        fc::GemmTask c = g;
+        const int64_t k0 = (int64_t)q * SOLVE_KC;
+        c.A = static_cast<const char *>(g.A) + k0 * g.a_sk * (int64_t)pg.second.first;
+        c.B = static_cast<const char *>(g.B) + k0 * g.b_sk * (int64_t)pg.second.second;
+        c.K = (int)std::min<int64_t>(SOLVE_KC, g.K - k0);
+        c.flags = g.flags | 8;
+        c.part_off = at, c.chunks = chunks, c.chunk = q, c.counter = (int32_t)p.tcount + cnt;
+        p.gemm.push_back(c);
+      }
+      at += (int64_t)chunks * 4096;
+      ++cnt;
+    }
+    p.psum = std::max(p.psum, at);
+    p.scount = std::max<int64_t>(p.scount, cnt);
+    pending.clear();
+    tiles = 0;
+  }
+};
+
+void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, SolvePlan &p) {
   std::vector<std::vector<int64_t>> lv(h->levels);
   for (int64_t s = 0; s < h->ns; ++s) lv[h->level[s]].push_back(s);
   const std::vector<int64_t> &voff = p.voff;
   std::vector<fc::RowTask> &rows = p.rows;
   std::vector<fc::GemmTask> &gemm = p.gemm;
+  SplitPush sp{p, 2 * prop_sms(h->device)};
+  const size_t es = h->esize;
+  p.psum = 0, p.scount = 0;
   std::vector<Launch> &fwd = p.fwd, &bwd = p.bwd;
   auto Lp = [&](int64_t off) { return arena_at(h->d_L, h, off); };
   auto thin = [&](int64_t s) { return h->width[s] <= fc::SOLVE_THIN; };
@@ -1189,9 +1231,10 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
             g.b_sj = 1, g.b_sk = R;
             g.M = std::min(64, bw - i0), g.N = std::min(64, R - j0), g.K = std::min(bw, i0 + 64);
             g.flags = 4;
-            gemm.push_back(g);
+            sp.add(g, sizeof(double), sizeof(double), j0 == 0);
           }
       }
+      sp.close();
       push(fwd, K_SOLVE_FWD, go, (int64_t)gemm.size() - go, (int)l);
       go = (int64_t)gemm.size();
       for (int64_t s : S) {
@@ -1212,11 +1255,12 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
             g.B = x2 + (f + c0) * R + j0;
             g.b_sj = 1, g.b_sk = R;
             g.M = r1 - r0, g.N = std::min(64, R - j0), g.K = bw;
-            gemm.push_back(g);
+            sp.add(g, es, sizeof(double), j0 == 0);
           }
           r0 = r1;
         }
       }
+      sp.close();
       push(fwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     }
   }
@@ -1248,43 +1292,26 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
       for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
     }
     push(bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
-    int64_t go = (int64_t)gemm.size(), ro2 = (int64_t)p.reduce.size(), pat = 0;
+    int64_t go = (int64_t)gemm.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
       if (u <= 0 || thin(s)) continue;
       const int64_t lo = h->loff[s];
-      const bool split = u > 2 * fc::SPLIT_K;
-      const int chunks = split ? (u + fc::SPLIT_K - 1) / fc::SPLIT_K : 1;
       for (int i0 = 0; i0 < w; i0 += fc::GEMM_TM)
         for (int j0 = 0; j0 < R; j0 += fc::GEMM_TN) {
-          const int M = std::min(fc::GEMM_TM, w - i0), N = std::min(fc::GEMM_TN, R - j0);
-          double *tile = x2 + (h->first[s] + i0) * (int64_t)R + j0;
-          for (int q = 0; q < chunks; ++q) {
-            const int k0 = split ? q * fc::SPLIT_K : 0, k1 = split ? std::min(u, k0 + fc::SPLIT_K) : u;
-            fc::GemmTask g{};
-            if (split) {
-              g.C = part + pat + (int64_t)q * 4096;
-              g.c_si = 64, g.c_sj = 1;
-              g.flags = 4;
-            } else {
-              g.C = tile;
-              g.c_si = R, g.c_sj = 1;
-            }
-            g.A = Lp(lo + w + k0 + (int64_t)i0 * m);
-            g.a_si = m, g.a_sk = 1;
-            g.B = v + voff[s] + (int64_t)k0 * R + j0;
-            g.b_sj = 1, g.b_sk = R;
-            g.M = M, g.N = N, g.K = k1 - k0;
-            gemm.push_back(g);
-          }
-          if (split) {
-            p.reduce.push_back({tile, part + pat, (int64_t)R, M, N, chunks, 0});
-            pat += (int64_t)chunks * 4096;
-          }
+          fc::GemmTask g{};
+          g.C = x2 + (h->first[s] + i0) * (int64_t)R + j0;
+          g.c_si = R, g.c_sj = 1;
+          g.A = Lp(lo + w + (int64_t)i0 * m);
+          g.a_si = m, g.a_sk = 1;
+          g.B = v + voff[s] + j0;
+          g.b_sj = 1, g.b_sk = R;
+          g.M = std::min(fc::GEMM_TM, w - i0), g.N = std::min(fc::GEMM_TN, R - j0), g.K = u;
+          sp.add(g, es, sizeof(double), j0 == 0);
         }
     }
+    sp.close();
     push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
-    push(bwd, K_REDUCE, ro2, (int64_t)p.reduce.size() - ro2, (int)l);
     // blocks of SB columns from the last: z = Dinv^T x2 (into x), then the own rows above the
     // block -= L(block, rows)^T z
     int K = 0;
@@ -1310,9 +1337,10 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
             g.b_sj = 1, g.b_sk = R;
             g.M = std::min(64, bw - i0), g.N = std::min(64, R - j0), g.K = bw - i0;
             g.flags = 4;
-            gemm.push_back(g);
+            sp.add(g, sizeof(double), sizeof(double), j0 == 0);
           }
       }
+      sp.close();
       push(bwd, K_SOLVE_BWD, go, (int64_t)gemm.size() - go, (int)l);
       go = (int64_t)gemm.size();
       for (int64_t s : S) {
@@ -1332,9 +1360,10 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, doub
             g.B = x + (f + c0) * R + j0;
             g.b_sj = 1, g.b_sk = R;
             g.M = std::min(64, c0 - r0), g.N = std::min(64, R - j0), g.K = bw;
-            gemm.push_back(g);
+            sp.add(g, es, sizeof(double), j0 == 0);
           }
       }
+      sp.close();
       if ((int64_t)gemm.size() > go) push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
     }
   }
@@ -1757,29 +1786,33 @@ int plan_solve(fc_chol *h, int R, fc_status *st) {
   cudaError_t e;
   if (h->d_x.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
       h->d_x2.alloc(sizeof(double) * (size_t)std::max<int64_t>(h->n * R, 1)) != cudaSuccess ||
-      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess ||
-      h->d_part.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.psum, 1)) != cudaSuccess ||
-      h->d_tpart.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.tpart, 1)) != cudaSuccess ||
-      h->d_tcount.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount, 1)) != cudaSuccess) {
+      h->d_v.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.vsum, 1)) != cudaSuccess) {
     h->solve_R = 0;
     set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
     return FC_OUT_OF_MEMORY;
   }
   if ((e = upload(h->d_voff, p.voff, h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
-  solve_tasks(h, R, h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), h->d_part.as<double>(), p);
+  solve_tasks(h, R, h->d_x.as<double>(), h->d_x2.as<double>(), h->d_v.as<double>(), p);
+  if (h->d_part.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.psum, 1)) != cudaSuccess ||
+      h->d_tpart.alloc(sizeof(double) * (size_t)std::max<int64_t>(p.tpart, 1)) != cudaSuccess ||
+      h->d_tcount.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount + p.scount, 1)) != cudaSuccess) {
+    h->solve_R = 0;
+    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the solve");
+    return FC_OUT_OF_MEMORY;
+  }
   h->fwd = std::move(p.fwd);
   h->bwd = std::move(p.bwd);
   h->gemm_flops_solve = 0;
   for (const auto &g : p.gemm) h->gemm_flops_solve += task_flops(g);
   if ((e = upload(h->d_srow, p.rows, h->stream)) != cudaSuccess || (e = upload(h->d_sranges, p.ranges, h->stream)) != cudaSuccess ||
-      (e = upload(h->d_spanel, p.panels, h->stream)) != cudaSuccess || (e = upload(h->d_sreduce, p.reduce, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_spanel, p.panels, h->stream)) != cudaSuccess ||
       (e = upload(h->d_sgemm, p.gemm, h->stream)) != cudaSuccess || (e = upload(h->d_thin, p.thin, h->stream)) != cudaSuccess ||
       (e = upload(h->d_tranges, p.tranges, h->stream)) != cudaSuccess ||
       (e = upload(h->d_tbwd, p.tbwd, h->stream)) != cudaSuccess)
     return cuda_fail(st, e, "solve plan");
   if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_fail(st, e, "solve plan");
   h->solve_lg = p.lg;
-  h->solve_tcount = p.tcount;
+  h->solve_tcount = p.tcount + p.scount;
   while (h->solve_events.size() < solve_events_needed(h)) {
     cudaEvent_t ev;
     if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(st, e, "solve events");
@@ -1797,7 +1830,7 @@ struct SolveBuffers {
   const int2 *ranges;
   const fc::SolveTask *panels;
   const fc::GemmTask *gemm;
-  const fc::ReduceTask *reduce;
+  double *part;
   const fc::ThinTask *thin;
   const int4 *tranges;
   const fc::ThinBwdTask *tbwd;
@@ -1809,7 +1842,7 @@ struct SolveBuffers {
 SolveBuffers own_buffers(fc_chol *h) {
   return {h->d_x.as<double>(),         h->d_x2.as<double>(),           h->d_v.as<double>(),
           h->d_voff.as<int64_t>(),       h->d_srow.as<fc::RowTask>(),    h->d_sranges.as<int2>(),
-          h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>(), h->d_sreduce.as<fc::ReduceTask>(),
+          h->d_spanel.as<fc::SolveTask>(), h->d_sgemm.as<fc::GemmTask>(), h->d_part.as<double>(),
           h->d_thin.as<fc::ThinTask>(),  h->d_tranges.as<int4>(),        h->d_tbwd.as<fc::ThinBwdTask>(),
           h->d_tpart.as<double>(),       h->d_tcount.as<int32_t>(),      h->solve_lg};
 }
@@ -1869,11 +1902,11 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         break;
       case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_FWD:  // the diagonal blocks' inverses applied (FP64 throughout)
-      case K_SOLVE_BWD: fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st); break;
+      case K_SOLVE_BWD: fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st, b.part, b.tcount); break;
       case K_GEMM:
-        fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
+        fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st, b.part,
+                        b.tcount);
         break;
-      case K_REDUCE: fc::launch_reduce(b.reduce + l.off, l.count, st); break;
       case K_SOLVE_THIN_FWD:
         fc::launch_thin_fwd(t, h->fp32, b.x, b.x2, b.v, b.voff, R, b.lg, b.thin + l.off, b.tranges, l.count, st);
         break;
@@ -2336,15 +2369,14 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   cudaError_t e = noalloc_scratch(h->device, &base);
   if (e != cudaSuccess) return cuda_fail(status, e, "cudaGetSymbolAddress of the solve scratch");
   const int R = nrhs;
-  // Layout in the scratch: x | x2 | v | partial tiles | voff | row tasks | child ranges | panel
-  // tasks | GEMM tasks | reduction tasks | thin forward tasks | their child ranges | thin backward
-  // tasks | their partial sums | their counters.
+  // Layout in the scratch: x | x2 | v | voff | row tasks | child ranges | panel tasks | GEMM tasks
+  // | split partial tiles | thin forward tasks | their child ranges | thin backward tasks | their
+  // partial sums | the counters (thin, then split).
   SolvePlan p;
   solve_offsets(h, R, p);
   const size_t vec = align256(sizeof(double) * (size_t)h->n * R);
   const size_t at_x = 0, at_x2 = vec, at_v = 2 * vec;
-  const size_t at_part = at_v + align256(sizeof(double) * (size_t)p.vsum);
-  const size_t at_voff = at_part + align256(sizeof(double) * (size_t)p.psum);
+  const size_t at_voff = at_v + align256(sizeof(double) * (size_t)p.vsum);
   auto too_large = [&](size_t need) {
     char msg[160];
     std::snprintf(msg, sizeof(msg), "the solve needs %zu bytes of scratch; the no-allocation limit is %zu",
@@ -2354,23 +2386,24 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   };
   if (at_voff > FC_NOALLOC_SCRATCH_BYTES) return too_large(at_voff);
   solve_tasks(h, R, reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
-              reinterpret_cast<double *>(base + at_v), reinterpret_cast<double *>(base + at_part), p);
+              reinterpret_cast<double *>(base + at_v), p);
   const size_t at_rows = at_voff + align256(sizeof(int64_t) * p.voff.size());
   const size_t at_ranges = at_rows + align256(sizeof(fc::RowTask) * p.rows.size());
   const size_t at_panels = at_ranges + align256(sizeof(int2) * p.ranges.size());
   const size_t at_gemm = at_panels + align256(sizeof(fc::SolveTask) * p.panels.size());
-  const size_t at_reduce = at_gemm + align256(sizeof(fc::GemmTask) * p.gemm.size());
-  const size_t at_thin = at_reduce + align256(sizeof(fc::ReduceTask) * p.reduce.size());
+  const size_t at_part = at_gemm + align256(sizeof(fc::GemmTask) * p.gemm.size());
+  const size_t at_thin = at_part + align256(sizeof(double) * (size_t)p.psum);
   const size_t at_tranges = at_thin + align256(sizeof(fc::ThinTask) * p.thin.size());
   const size_t at_tbwd = at_tranges + align256(sizeof(int4) * p.tranges.size());
   const size_t at_tpart = at_tbwd + align256(sizeof(fc::ThinBwdTask) * p.tbwd.size());
   const size_t at_tcount = at_tpart + align256(sizeof(double) * (size_t)p.tpart);
-  const size_t need = at_tcount + sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount, 1);
+  const size_t counters = (size_t)std::max<int64_t>(p.tcount + p.scount, 1);
+  const size_t need = at_tcount + sizeof(int32_t) * counters;
   if (need > FC_NOALLOC_SCRATCH_BYTES) return too_large(need);
   // Every region is written before it is read in this call: the task lists and offsets here, x by
   // the permutation, x2 by the forward panels, each update vector's rows zeroed by its assembly
-  // (or stored whole by a thin forward tile), each partial tile stored by its GEMM task before its
-  // reduction reads it, the thin counters zeroed here.
+  // (or stored whole by a thin forward tile), each partial tile stored by its chunk before the
+  // last chunk of its sum reads it, the counters zeroed here.
   auto put = [&](size_t at, const void *src, size_t bytes) {
     if (bytes && e == cudaSuccess) e = cudaMemcpyAsync(base + at, src, bytes, cudaMemcpyHostToDevice, h->stream);
   };
@@ -2379,12 +2412,10 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   put(at_ranges, p.ranges.data(), sizeof(int2) * p.ranges.size());
   put(at_panels, p.panels.data(), sizeof(fc::SolveTask) * p.panels.size());
   put(at_gemm, p.gemm.data(), sizeof(fc::GemmTask) * p.gemm.size());
-  put(at_reduce, p.reduce.data(), sizeof(fc::ReduceTask) * p.reduce.size());
   put(at_thin, p.thin.data(), sizeof(fc::ThinTask) * p.thin.size());
   put(at_tranges, p.tranges.data(), sizeof(int4) * p.tranges.size());
   put(at_tbwd, p.tbwd.data(), sizeof(fc::ThinBwdTask) * p.tbwd.size());
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(base + at_tcount, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(p.tcount, 1), h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + at_tcount, 0, sizeof(int32_t) * counters, h->stream);
   if (e != cudaSuccess) return cuda_fail(status, e, "copy of the solve plan into the scratch");
   const SolveBuffers b{reinterpret_cast<double *>(base + at_x), reinterpret_cast<double *>(base + at_x2),
                        reinterpret_cast<double *>(base + at_v), reinterpret_cast<const int64_t *>(base + at_voff),
@@ -2392,7 +2423,7 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
                        reinterpret_cast<const int2 *>(base + at_ranges),
                        reinterpret_cast<const fc::SolveTask *>(base + at_panels),
                        reinterpret_cast<const fc::GemmTask *>(base + at_gemm),
-                       reinterpret_cast<const fc::ReduceTask *>(base + at_reduce),
+                       reinterpret_cast<double *>(base + at_part),
                        reinterpret_cast<const fc::ThinTask *>(base + at_thin),
                        reinterpret_cast<const int4 *>(base + at_tranges),
                        reinterpret_cast<const fc::ThinBwdTask *>(base + at_tbwd),

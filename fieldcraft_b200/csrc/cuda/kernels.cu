@@ -432,13 +432,13 @@ struct TileLoader {
 };
 
 // Writes a GEMM task's 64 x 64 tile (acc[r][c][e] of the m16n8k8 fragments of a 32 x 32 warp
-// tile) by its flags: a partial (flag 4), -sum (flag 2), or C - sum. For C - sum every old value
-// is loaded before any store, so the loads are in flight together.
+// tile) by `flags`: C = +sum (flag 4), -sum (flag 2), or C - sum. For C - sum the old values of a
+// half tile are all loaded before any of its stores, so those loads are in flight together.
 template <class T, class V>
-__device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)[2][4][4], int wm, int wn, int g,
-                                              int tg) {
+__device__ __forceinline__ void gemm_store(const GemmTask *tp, int flags, const V (&acc)[2][4][4], int wm, int wn,
+                                           int g, int tg) {
   const int M = tp->M, N = tp->N;
-  const bool lower = tp->flags & 1, store = tp->flags & 2, partial = tp->flags & 4;
+  const bool lower = flags & 1, store = flags & 2, partial = flags & 4;
   T *C = static_cast<T *>(tp->C);
   const int64_t c_si = tp->c_si, c_sj = tp->c_sj;
   auto at = [&](int r, int c, int e, T *&dst) {
@@ -458,29 +458,89 @@ __device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)
         }
     return;
   }
-  T old[2][4][4];
+  // by halves of the warp tile's rows: 16 loads in flight, registers for the accumulator besides
 #pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        T *dst;
-        old[r][c][e] = at(r, c, e, dst) ? *dst : T(0);
-      }
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
+  for (int r = 0; r < 2; ++r) {
+    T old[4][4];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         T *dst;
-        if (at(r, c, e, dst)) *dst = T(old[r][c][e] - acc[r][c][e]);
+        old[c][e] = at(r, c, e, dst) ? *dst : T(0);
       }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        T *dst;
+        if (at(r, c, e, dst)) *dst = T(old[c][e] - acc[r][c][e]);
+      }
+  }
+}
+
+// The tile by the task's flags; for one chunk of a split sum (flag 8, FP64 C): its partial is
+// stored, and the last chunk to finish adds all the partials in chunk order (each thread over its
+// own fragment positions, a chunk's loads in flight together) and writes the total.
+template <class T, class V>
+__device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)[2][4][4], int wm, int wn, int g,
+                                              int tg, double *part = nullptr, int32_t *counters = nullptr) {
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (tp->flags & 8) {
+      __shared__ int last;
+      double *P = part + tp->part_off;
+      double *mine = P + (int64_t)tp->chunk * 4096;
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
+            mine[i * 64 + j] = acc[r][c][e];
+          }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) last = atomicAdd(counters + tp->counter, 1) == tp->chunks - 1;
+      __syncthreads();
+      if (!last) return;
+      __threadfence();
+      double tot[2][4][4];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) tot[r][c][e] = 0.0;
+      for (int q = 0; q < tp->chunks; ++q) {
+        const double *Pq = P + (int64_t)q * 4096;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          double v[4][4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
+              v[c][e] = __ldcg(Pq + i * 64 + j);
+            }
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) tot[r][c][e] += v[c][e];
+        }
+      }
+      if (threadIdx.x == 0) counters[tp->counter] = 0;
+      gemm_store<T>(tp, tp->flags & ~8, tot, wm, wn, g, tg);
+      return;
+    }
+  }
+  gemm_store<T>(tp, tp->flags, acc, wm, wn, g, tg);
 }
 
 template <class TA>
-__global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *__restrict__ tasks) {
+__global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *__restrict__ tasks, double *part,
+                                                               int32_t *counters) {
   constexpr int SA = tile_stride<TA>();
   extern __shared__ __align__(16) double gsm[];
   double(*Bs)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm);
@@ -543,7 +603,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
     }
   }
   cp_async_wait<0>();
-  gemm_epilogue<double>(tp, acc, wm, wn, g, tg);
+  gemm_epilogue<double>(tp, acc, wm, wn, g, tg, part, counters);
 }
 
 // ---- tiled C -= A B^T in FP32 by 3xTF32 on the tensor pipe ---------------------------------------
@@ -618,18 +678,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_tf32x3_kernel(const Gemm
   }
   cp_async_wait<0>();
   gemm_epilogue<float>(tp, acc, wm, wn, g, tg);
-}
-
-// ---- the reduction of a split GEMM's partials, in a fixed order ----------------------------------
-__global__ void __launch_bounds__(256) reduce_kernel(const ReduceTask *__restrict__ tasks) {
-  const ReduceTask tk = tasks[blockIdx.x];
-  for (int e = threadIdx.x; e < tk.M * 64; e += blockDim.x) {
-    const int i = e >> 6, j = e & 63;
-    if (j >= tk.N) continue;
-    double sum = 0.0;
-    for (int q = 0; q < tk.count; ++q) sum += tk.P[(int64_t)q * 4096 + i * 64 + j];
-    tk.C[(int64_t)i * tk.c_si + j] -= sum;
-  }
 }
 
 // ---- solve -------------------------------------------------------------------------------------
@@ -1086,18 +1134,18 @@ void launch_panel(const Tree &t, bool fp32, const double *upper_val, const Panel
     panel_kernel<double><<<count, PANEL_THREADS, panel_smem<double>(p8max), st>>>(t, upper_val, tasks, status, p8max);
 }
 
-void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st) {
+void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st, double *part, int32_t *counters) {
   if (count <= 0) return;
   configure_kernels();
   switch (kind) {
-    case GemmKind::F64: gemm_kernel<double><<<count, GEMM_THREADS, gemm_smem<double>(), st>>>(tasks); break;
-    case GemmKind::F32A_F64: gemm_kernel<float><<<count, GEMM_THREADS, gemm_smem<float>(), st>>>(tasks); break;
+    case GemmKind::F64:
+      gemm_kernel<double><<<count, GEMM_THREADS, gemm_smem<double>(), st>>>(tasks, part, counters);
+      break;
+    case GemmKind::F32A_F64:
+      gemm_kernel<float><<<count, GEMM_THREADS, gemm_smem<float>(), st>>>(tasks, part, counters);
+      break;
     case GemmKind::F32_TF32X3: gemm_tf32x3_kernel<<<count, GEMM_THREADS, GEMM_F32_SMEM, st>>>(tasks); break;
   }
-}
-
-void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st) {
-  if (count > 0) reduce_kernel<<<count, 256, 0, st>>>(tasks);
 }
 
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,

@@ -74,21 +74,18 @@ struct PanelTask {
 };
 // C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands. Flags: 1 touches
 // i >= j only (a diagonal tile of a symmetric matrix); 2 stores C = -sum instead of subtracting;
-// 4 stores C = +sum (one partial of a split sum, reduced later by a ReduceTask).
+// 4 stores C = +sum. Flag 8 (FP64 C only): this task is chunk `chunk` of `chunks` of one split
+// sum over K; each chunk stores its 64 x 64 partial at part + part_off + chunk * 4096 (`part`
+// given at launch), and the last chunk to finish (counters[counter], reset by it) adds the
+// partials in chunk order and applies the total to C by the other flags. No chunk waits.
 struct GemmTask {
   void *C;
   const void *A;
   const void *B;
   int64_t c_si, c_sj, a_si, a_sk, b_sj, b_sk;
   int32_t M, N, K, flags;
-};
-// C(i, j) -= sum_q P[q][i][j] for i < M, j < N: the partials of a split GEMM (64 x 64 tiles,
-// row-major, one after another), summed in order.
-struct ReduceTask {
-  double *C;
-  const double *P;
-  int64_t c_si;
-  int32_t M, N, count, pad;
+  int64_t part_off;
+  int32_t chunks, chunk, counter, pad;
 };
 // Solve, panel [c0, c1) of supernode s, right-hand sides [j0, j1): apply the inverse of the
 // diagonal block (forward: L^-1, backward: L^-T), then update the front rows [r0, r1) (forward:
@@ -225,9 +222,9 @@ void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const As
 // p8max: the widest panel of the launch, rounded up to a multiple of 8 (sizes shared memory).
 void launch_panel(const Tree &t, bool fp32, const double *upper_val, const PanelTask *tasks, int count,
                   DeviceStatus *status, int p8max, cudaStream_t st);
-void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st);
-void launch_reduce(const ReduceTask *tasks, int count, cudaStream_t st);
-
+// part and counters: the partial sums and counters of split tasks (flag 8), null when there are none.
+void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st, double *part = nullptr,
+                 int32_t *counters = nullptr);
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R,
                            const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st);
