@@ -600,7 +600,7 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
     h->gemm_flops_factor += 2.0 * g.K * outputs;
   }
   if (!tc_t.empty()) {
-    // the packed operands and their tensor maps (TMA boxes of 128 rows x 32 FP32, 128-byte swizzle)
+    // the packed operands and their tensor maps (TMA boxes of 128 rows x 16 FP32, 64-byte swizzle)
     if (h->d_pack.alloc(sizeof(float) * (size_t)std::max<int64_t>(h->pack_len, 1)) != cudaSuccess) {
       set_status(st, FC_OUT_OF_MEMORY, -1, h->pack_len, 0, "device memory for the packed operands");
       return FC_OUT_OF_MEMORY;
@@ -621,10 +621,10 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
       const MapSpec &m = specs[i];
       const cuuint64_t dims[2] = {(cuuint64_t)2 * m.wpad, (cuuint64_t)m.u};
       const cuuint64_t strides[1] = {(cuuint64_t)2 * m.wpad * sizeof(float)};
-      const cuuint32_t box[2] = {(cuuint32_t)fc::TC_KPAD, (cuuint32_t)fc::GEMM_TC_M};
+      const cuuint32_t box[2] = {(cuuint32_t)fc::TC_KBOX, (cuuint32_t)fc::GEMM_TC_M};
       const cuuint32_t estr[2] = {1, 1};
       const CUresult r = encode(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, h->d_pack.as<float>() + m.poff, dims,
-                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS) {
         set_status(st, FC_CUDA_ERROR, -1, (int64_t)r, 0, "cuTensorMapEncodeTiled of a packed operand");

@@ -9,10 +9,11 @@
 // per-tile conversion work.
 //
 // syrk_tc_kernel: one CTA of 128 threads per tile of up to 128 x 128 outputs. Thread 0 is the
-// producer: per K chunk of 32 it issues four 2D TMA loads (A hi, A lo, B hi, B lo: boxes of
-// 128 rows x 128 bytes, 128-byte swizzle, rows past the end zero-filled) into a three-stage ring,
-// completing on the stage's "full" mbarrier. Thread 32 issues the chunk's 4 x 3 MMAs (M 128,
-// N 128, K 8 each) and commits them to the stage's "empty" mbarrier, which the producer waits on
+// producer: per K chunk of 16 it issues four 2D TMA loads (A hi, A lo, B hi, B lo: boxes of
+// 128 rows x 64 bytes, 64-byte swizzle, rows past the end zero-filled) into a three-stage ring
+// (97 KB: two CTAs share an SM, one's loads and epilogue beside the other's MMAs), completing on
+// the stage's "full" mbarrier. Thread 32 issues the chunk's 2 x 3 MMAs (M 128, N 128, K 8 each)
+// and commits them to the stage's "empty" mbarrier, which the producer waits on
 // before refilling the stage. A diagonal tile (A = B) loads one operand pair. All four warps then
 // read the accumulator (warp q owns TMEM lanes 32q..32q+31, the tile's rows) and write C. Every
 // wait is bounded by time: a wait that gives up records DeviceStatus::timeout, and the CTA drains
@@ -25,14 +26,14 @@ namespace fc {
 
 namespace {
 
-constexpr int TC_M = 128, TC_N = 128, TC_KC = 32, TC_THREADS = 128, TC_COLS = 128;
-constexpr int TILE_BYTES = TC_M * TC_KC * 4;             // one operand tile of a chunk (16 KB)
+constexpr int TC_M = 128, TC_N = 128, TC_KC = TC_KBOX, TC_THREADS = 128, TC_COLS = 128;
+constexpr int TILE_BYTES = TC_M * TC_KC * 4;             // one operand tile of a chunk (8 KB)
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;              // A hi, A lo, B hi, B lo
 constexpr int STAGES = 3;
-constexpr size_t TC_SMEM = STAGES * STAGE_BYTES + 1024;  // + alignment slack (1024-byte atoms)
+constexpr size_t TC_SMEM = STAGES * STAGE_BYTES + 1024;  // + alignment slack: two CTAs fit on an SM
 constexpr unsigned long long WAIT_NS = 2000000000ull;    // a wait longer than 2 s gives up
 constexpr int TMAP_BYTES = 128;                          // sizeof(CUtensorMap)
-static_assert(TC_M == GEMM_TC_M && TC_N == GEMM_TC_N && TC_KC == TC_KPAD, "tile shape");
+static_assert(TC_M == GEMM_TC_M && TC_N == GEMM_TC_N && TC_KPAD % TC_KC == 0 && TC_KC * 4 == 64, "tile shape");
 
 // instruction descriptor: D FP32, A and B TF32, both K-major, N = 128, M = 128
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
@@ -40,12 +41,12 @@ constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Shared-memory operand descriptor of a K-major tile with 128-byte swizzle (what the TMA writes
-// for 128-byte rows): 8-row atoms of 1024 bytes (SBO), LBO unused (1), version 1, layout type 2.
+// Shared-memory operand descriptor of a K-major tile with 64-byte swizzle (what the TMA writes
+// for 64-byte rows): 8-row atoms of 512 bytes (SBO), LBO unused (1), version 1, layout type 4.
 // A step of 8 K values inside the atom adds 32 bytes to the start address.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
-         (2ull << 61);
+  return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
+         (4ull << 61);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar) {
@@ -76,7 +77,7 @@ __device__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
 __device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// 2D tile load (x = the K element, a multiple of 32 here; y = the row) completing on `bar`
+// 2D tile load (x = the K element, a multiple of 16 here; y = the row) completing on `bar`
 __device__ __forceinline__ void tma_load(void *dst, const void *map, int x, int y, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
@@ -107,7 +108,7 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, 
       "l"(a), "l"(b), "r"(IDESC), "r"(accumulate));
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) syrk_tc_kernel(const TcTask *__restrict__ tasks,
+__global__ void __launch_bounds__(TC_THREADS, 2) syrk_tc_kernel(const TcTask *__restrict__ tasks,
                                                                 const unsigned char *__restrict__ maps,
                                                                 DeviceStatus *__restrict__ status) {
   extern __shared__ __align__(16) unsigned char tc_raw[];
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) syrk_tc_kernel(const TcTask *__
       const uint32_t b_hi = diag ? a_hi : a_hi + 2 * TILE_BYTES, b_lo = diag ? a_lo : a_hi + 3 * TILE_BYTES;
 #pragma unroll
       for (int k8 = 0; k8 < TC_KC / 8; ++k8) {
-        const uint32_t step = k8 * 32;  // 8 FP32 values along K inside the 128-byte swizzle atom
+        const uint32_t step = k8 * 32;  // 8 FP32 values along K inside the 64-byte swizzle atom
         const uint64_t ah = smem_desc(a_hi + step), al = smem_desc(a_lo + step);
         const uint64_t bh = smem_desc(b_hi + step), bl = smem_desc(b_lo + step);
         mma_tf32(tmem, ah, bh, (q > 0 || k8 > 0) ? 1u : 0u);
@@ -243,21 +244,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) syrk_tc_kernel(const TcTask *__
 // the writes (along a row) are coalesced.
 __global__ void __launch_bounds__(256) pack_tc_kernel(Tree t, const PackTask *__restrict__ tasks,
                                                        float *__restrict__ P) {
-  __shared__ float tile[TC_KC][TC_PACK_ROWS + 1];
+  __shared__ float tile[TC_KPAD][TC_PACK_ROWS + 1];
   const PackTask task = tasks[blockIdx.x];
   const int s = task.s;
   const int m = t.height[s], w = t.width[s], u = m - w;
   const float *Lb = static_cast<const float *>(t.L) + t.loff[s] + w;  // Lb[k m + i] = L21(i, k)
   const int r0 = task.r0, nr = min(TC_PACK_ROWS, u - r0), wpad = task.wpad;
   float *Pp = P + task.poff;
-  for (int kc = 0; kc < wpad; kc += TC_KC) {
-    for (int e = threadIdx.x; e < TC_KC * TC_PACK_ROWS; e += blockDim.x) {
+  for (int kc = 0; kc < wpad; kc += TC_KPAD) {
+    for (int e = threadIdx.x; e < TC_KPAD * TC_PACK_ROWS; e += blockDim.x) {
       const int k = e / TC_PACK_ROWS, r = e - k * TC_PACK_ROWS;
       tile[k][r] = kc + k < w && r < nr ? Lb[(int64_t)(kc + k) * m + r0 + r] : 0.f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < TC_KC * TC_PACK_ROWS; e += blockDim.x) {
-      const int r = e / TC_KC, k = e - r * TC_KC;
+    for (int e = threadIdx.x; e < TC_KPAD * TC_PACK_ROWS; e += blockDim.x) {
+      const int r = e / TC_KPAD, k = e - r * TC_KPAD;
       if (r < nr) {
         const float x = tile[k][r];
         uint32_t h;

@@ -60,7 +60,7 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
 // written through global memory: the child's rows and values stream in coalesced, the scatter is
 // to shared memory, and every entry of the tile's lower part is stored once.
 template <class T>
-__global__ void __launch_bounds__(ASSEMBLE_THREADS) assemble_kernel(Tree t, const double *__restrict__ val,
+__global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, const double *__restrict__ val,
                                                                     const AssembleTask *__restrict__ tasks,
                                                                     const int4 *__restrict__ ranges) {
   static_assert(ASSEMBLE_ROWS == ASSEMBLE_THREADS && ASSEMBLE_COLS * 32 == ASSEMBLE_THREADS, "tile shape");

@@ -203,6 +203,7 @@ enum class GemmKind { F64, F32A_F64, F32_TF32X3 };
 // supernode's P (an array of 128-byte CUtensorMap objects in device memory); a wait that gives up
 // sets status->timeout.
 constexpr int GEMM_TC_M = 128, GEMM_TC_N = 128, TC_KPAD = 32, TC_PACK_ROWS = 64;
+constexpr int TC_KBOX = 16;  // K values of a TMA box (64 bytes: 64-byte swizzle)
 struct PackTask {
   int32_t s, r0, wpad, pad;
   int64_t poff;
