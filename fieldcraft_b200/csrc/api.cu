@@ -407,6 +407,9 @@ struct MapSpec {
   int wpad;
 };
 
+// Panels per outer block of the factorisation of a front's own columns (see plan_factor).
+constexpr int OUTER_PANELS = 4;
+
 void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::vector<fc::AssembleTask> &asm_t,
                  std::vector<int4> &ranges, std::vector<fc::PanelTask> &panel_t, std::vector<fc::GemmTask> &gemm_t,
                  std::vector<fc::PackTask> &pack_t, std::vector<fc::TcTask> &tc_t, std::vector<MapSpec> &maps) {
@@ -439,10 +442,34 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
+    // Two-level blocking: panels are grouped in outer blocks of OUTER_PANELS. A panel's update of
+    // the later columns of its own block (K = one panel) runs on lane 0 right after it; the update
+    // of the columns past the block by the whole block (K = its width) runs once, after the
+    // block's last panel: the next block's columns on lane 0 (after the previous such update on
+    // lane 1, which also wrote them), the rest on lane 1 beside the next block's panels.
+    const int OP = OUTER_PANELS;
     int last_rest = -1;  // the level's latest lane-1 launch
+    auto tiles = [&](int64_t s, int jlo, int jhi, int k0, int k1, std::vector<fc::GemmTask> &out) {
+      const int m = h->height[s];
+      const int64_t lo = h->loff[s];
+      for (int jc = jlo; jc < jhi; jc += fc::GEMM_TN)
+        for (int ic = jc; ic < m; ic += TM) {
+          fc::GemmTask g{};
+          g.C = Lp(lo + ic + (int64_t)jc * m);
+          g.A = Lp(lo + ic + (int64_t)k0 * m);
+          g.B = Lp(lo + jc + (int64_t)k0 * m);
+          g.c_si = 1, g.c_sj = m, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
+          g.M = std::min(TM, m - ic);
+          g.N = std::min(fc::GEMM_TN, jhi - jc);
+          g.K = k1 - k0;
+          g.flags = ic == jc ? 1 : 0;
+          out.push_back(g);
+        }
+    };
     for (int p = 0; p < P; ++p) {
       int64_t po = (int64_t)panel_t.size(), go = (int64_t)gemm_t.size();
-      std::vector<fc::GemmTask> rest;  // updates of the columns past the next panel (lane 1)
+      std::vector<fc::GemmTask> rest;  // updates of the columns past the next block (lane 1)
+      bool outer = false;              // this step's lane-0 launch updates a next block's columns
       int p8max = 8;
       for (int64_t s : S) {
         const int m = h->height[s], w = h->width[s];
@@ -458,26 +485,20 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         for (int r0 = c1; r0 < m; r0 += fc::PANEL_ROWS)
           panel_t.push_back(
               {(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff, ioff, bw, 0});
-        const int64_t lo = h->loff[s];
-        for (int jc = c1; jc < w; jc += fc::GEMM_TN)
-          for (int ic = jc; ic < m; ic += TM) {
-            fc::GemmTask g{};
-            g.C = Lp(lo + ic + (int64_t)jc * m);
-            g.A = Lp(lo + ic + (int64_t)c0 * m);
-            g.B = Lp(lo + jc + (int64_t)c0 * m);
-            g.c_si = 1, g.c_sj = m, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = m;
-            g.M = std::min(TM, m - ic);
-            g.N = std::min(fc::GEMM_TN, w - jc);
-            g.K = c1 - c0;
-            g.flags = ic == jc ? 1 : 0;
-            (jc == c1 ? gemm_t : rest).push_back(g);
-          }
+        const int bs = p / OP * OP * NB, be = std::min(w, bs + OP * NB);  // this panel's block
+        if (c1 < be) tiles(s, c1, be, c0, c1, gemm_t);                     // within the block
+        if (c1 == be && be < w) {                                         // past the block
+          const int nx = std::min(w, be + OP * NB);
+          tiles(s, be, nx, bs, be, gemm_t);
+          outer = true;
+          if (nx < w) tiles(s, nx, w, bs, be, rest);
+        }
       }
       push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l, p8max);
       const int panel_at = (int)h->program.size() - 1;
       const size_t before = h->program.size();
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
-      if (h->program.size() > before && last_rest >= 0) {  // the next panel's columns after rest(p-1)
+      if (h->program.size() > before && outer && last_rest >= 0) {  // the next block after rest(b - 1)
         h->program.back().dep = last_rest;
         h->program[last_rest].record = true;
       }
