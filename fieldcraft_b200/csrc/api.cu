@@ -2502,6 +2502,9 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
   }
   if (e != cudaSuccess) return cuda_fail(status, e, "refinement set-up");
   fc::launch_sumsq(n, R, n, r, sums + R, st);
+  e = cudaMemcpyAsync(host.data() + R, sums + R, sizeof(double) * R, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(status, e, "refinement set-up");
   // the true residual's relative norms of the current x (into rel); true when every column is done
   auto check = [&](double *t) -> int {
     fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, t, n, R, st);
@@ -2552,11 +2555,29 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
     cudaMemcpyAsync(p, z, block, cudaMemcpyDeviceToDevice, st);
     fc::launch_coldot(n, R, r, n, z, n, rz, st);
     cudaMemsetAsync(d_done, 0, sizeof(int) * R, st);
+    // the recurrence's residual r (one norm per column, read each iteration) says when to look
+    // at the true residual; only the true residual decides convergence and which columns stop
+    auto recurrence_small = [&]() -> int {
+      fc::launch_sumsq(n, R, n, r, sums, st);
+      cudaError_t e2 = cudaMemcpyAsync(host.data(), sums, sizeof(double) * R, cudaMemcpyDeviceToHost, st);
+      if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
+      if (e2 == cudaSuccess) e2 = cudaGetLastError();
+      if (e2 != cudaSuccess) return cuda_fail(status, e2, "refinement");
+      int rc2 = solve_wait_status(h, status);
+      if (rc2 != FC_OK) return rc2;
+      for (int j = 0; j < R; ++j) {
+        const double bb = host[R + j];  // ||b||^2 of column j, read by the last true check
+        const double rr = bb > 0.0 ? std::sqrt(host[j] / bb) : std::sqrt(host[j]);
+        if (!done[j] && !(rr <= tol)) return FC_OK;
+      }
+      return -1;
+    };
     for (;;) {
       fc::launch_spmv(n, d_ptr, d_idx, d_val, p, n, q, n, R, st);
       fc::launch_coldot(n, R, p, n, q, n, pq, st);
       fc::launch_pcg_step(n, R, rz, pq, d_done, p, q, d_x, ld, r, st);
-      rc = check(t);
+      rc = recurrence_small();
+      if (rc == -1) rc = check(t);
       if (rc == -1) {
         converged = true;
         break;
