@@ -95,6 +95,7 @@ struct fc_chol {
   DeviceBuf d_Dinv, d_T;                 // diagonal-block inverses; the doubling's products
   DeviceBuf d_ir_r, d_ir_d, d_ir_sum;    // iterative refinement workspace
   DeviceBuf d_ir_p, d_ir_q, d_ir_t, d_ir_done;
+  DeviceBuf d_ir_sc;                     // the refinement's SpMV: row-major copies of x and y
   bool refine_pcg = true;                // refinement by preconditioned CG (else plain refinement)
   bool tc = true;                        // FP32 updates on tcgen05 (FC_TF32_MMA_SYNC=1: on mma.sync)
   DeviceBuf d_asm, d_ranges, d_panel, d_gemm;
@@ -2483,6 +2484,7 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
   const bool pcg = h->refine_pcg;
   auto need = [&](DeviceBuf &b, size_t bytes) { return b.bytes >= bytes || b.alloc(bytes) == cudaSuccess; };
   if (!need(h->d_ir_r, block) || !need(h->d_ir_d, block) || !need(h->d_ir_sum, 6 * sizeof(double) * R) ||
+      !need(h->d_ir_sc, 2 * block) ||
       (pcg && (!need(h->d_ir_p, block) || !need(h->d_ir_q, block) || !need(h->d_ir_t, block) ||
                !need(h->d_ir_done, sizeof(int) * R)))) {
     set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the refinement");
@@ -2507,7 +2509,7 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
   if (e != cudaSuccess) return cuda_fail(status, e, "refinement set-up");
   // the true residual's relative norms of the current x (into rel); true when every column is done
   auto check = [&](double *t) -> int {
-    fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, t, n, R, st);
+    fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, t, n, R, st, h->d_ir_sc.as<double>());
     fc::launch_residual(n, R, d_b, ld, t, n, st);
     fc::launch_sumsq(n, R, n, t, sums, st);
     cudaError_t e2 = cudaMemcpyAsync(host.data(), sums, 2 * sizeof(double) * R, cudaMemcpyDeviceToHost, st);
@@ -2573,7 +2575,7 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
       return -1;
     };
     for (;;) {
-      fc::launch_spmv(n, d_ptr, d_idx, d_val, p, n, q, n, R, st);
+      fc::launch_spmv(n, d_ptr, d_idx, d_val, p, n, q, n, R, st, h->d_ir_sc.as<double>());
       fc::launch_coldot(n, R, p, n, q, n, pq, st);
       fc::launch_pcg_step(n, R, rz, pq, d_done, p, q, d_x, ld, r, st);
       rc = recurrence_small();
@@ -2734,7 +2736,16 @@ int64_t fc_chol_profile_launches(fc_chol *h, int32_t *kind, int32_t *level, int3
 int fc_csr_spmv_device(int64_t n, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val, const double *d_x,
                        double *d_y, int32_t nrhs, int64_t ld, void *stream) {
   if (n < 0 || nrhs < 0 || (n > 0 && (!d_ptr || !d_idx || !d_val || !d_x || !d_y || ld < n))) return FC_INVALID_ARGUMENT;
-  fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, d_y, ld, nrhs, (cudaStream_t)stream);
+  const cudaStream_t st = (cudaStream_t)stream;
+  // several right-hand sides: through row-major copies in stream-ordered scratch (freed in order)
+  double *scratch = nullptr;
+  if (n > 0 && nrhs >= fc::SPMV_ROWS_MIN_R &&
+      cudaMallocAsync(reinterpret_cast<void **>(&scratch), sizeof(double) * 2 * (size_t)n * nrhs, st) != cudaSuccess) {
+    cudaGetLastError();
+    scratch = nullptr;
+  }
+  fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, ld, d_y, ld, nrhs, st, scratch);
+  if (scratch) cudaFreeAsync(scratch, st);
   return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
 }
 

@@ -960,6 +960,90 @@ __global__ void permute_out_kernel(const int64_t *__restrict__ perm, int64_t n, 
   }
 }
 
+// y = A x with x and y row-major (n x R: a row's right-hand sides contiguous): one warp per row and
+// block of 64 right-hand sides, two a lane, the row's entries in order (index and value the same
+// for the whole warp, the x row of each entry read as 512 contiguous bytes; four entries in
+// flight). Each output is one thread's sum over the row in entry order, whatever R is.
+__global__ void __launch_bounds__(256) spmv_rows_kernel(int64_t n, const int64_t *__restrict__ ptr,
+                                                        const int32_t *__restrict__ idx,
+                                                        const double *__restrict__ val,
+                                                        const double *__restrict__ x, double *__restrict__ y, int R) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const int ja = blockIdx.y * 64 + lane, jb = ja + 32;
+  const bool oka = ja < R, okb = jb < R;
+  double a0 = 0.0, a1 = 0.0;
+  const int64_t e1 = ptr[row + 1];
+  int64_t e = ptr[row];
+  for (; e + 3 < e1; e += 4) {
+    int c[4];
+    double v[4], xa[4], xb[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      c[q] = idx[e + q];
+      v[q] = val[e + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double *xr = x + (int64_t)c[q] * R;
+      xa[q] = oka ? xr[ja] : 0.0;
+      xb[q] = okb ? xr[jb] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      a0 = fma(v[q], xa[q], a0);
+      a1 = fma(v[q], xb[q], a1);
+    }
+  }
+  for (; e < e1; ++e) {
+    const double v = val[e];
+    const double *xr = x + (int64_t)idx[e] * R;
+    if (oka) a0 = fma(v, xr[ja], a0);
+    if (okb) a1 = fma(v, xr[jb], a1);
+  }
+  if (oka) y[row * R + ja] = a0;
+  if (okb) y[row * R + jb] = a1;
+}
+
+// dst (n x R row-major) <- src (column-major, leading dimension ld), and back: 32 x 32 tiles
+// through shared memory, both sides coalesced.
+__global__ void __launch_bounds__(256) to_rows_kernel(int64_t n, int R, const double *__restrict__ src, int64_t ld,
+                                                      double *__restrict__ dst) {
+  __shared__ double tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32;
+  const int j0 = blockIdx.y * 32, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int k = ty; k < 32; k += 8) {
+    const int64_t i = i0 + tx;
+    const int j = j0 + k;
+    if (i < n && j < R) tile[k][tx] = src[i + (int64_t)j * ld];
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {
+    const int64_t i = i0 + k;
+    const int j = j0 + tx;
+    if (i < n && j < R) dst[i * R + j] = tile[tx][k];
+  }
+}
+
+__global__ void __launch_bounds__(256) to_cols_kernel(int64_t n, int R, const double *__restrict__ src,
+                                                      double *__restrict__ dst, int64_t ld) {
+  __shared__ double tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32;
+  const int j0 = blockIdx.y * 32, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int k = ty; k < 32; k += 8) {
+    const int64_t i = i0 + k;
+    const int j = j0 + tx;
+    if (i < n && j < R) tile[tx][k] = src[i * R + j];
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {
+    const int64_t i = i0 + tx;
+    const int j = j0 + k;
+    if (i < n && j < R) dst[i + (int64_t)j * ld] = tile[k][tx];
+  }
+}
+
 // y = A x for RB right-hand sides at once: one warp per row, its lanes over the row's entries
 // (so a warp reads the row's indices and values once, contiguously, for all RB vectors), then a
 // butterfly sum of the lanes. x and y are column-major with leading dimensions ldx and ldy.
@@ -1193,8 +1277,17 @@ void launch_permute_out(const int64_t *perm, int64_t n, const double *x, int R, 
 }
 
 void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, int64_t ldx,
-                 double *y, int64_t ldy, int R, cudaStream_t st) {
+                 double *y, int64_t ldy, int R, cudaStream_t st, double *scratch) {
   if (n <= 0 || R <= 0) return;
+  if (scratch && R >= SPMV_ROWS_MIN_R) {
+    double *xr = scratch, *yr = scratch + n * R;
+    const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((R + 31) / 32));
+    to_rows_kernel<<<tgrid, 256, 0, st>>>(n, R, x, ldx, xr);
+    spmv_rows_kernel<<<dim3((unsigned)((n + 7) / 8), (unsigned)((R + 63) / 64)), 256, 0, st>>>(n, ptr, idx, val, xr,
+                                                                                              yr, R);
+    to_cols_kernel<<<tgrid, 256, 0, st>>>(n, R, yr, y, ldy);
+    return;
+  }
   constexpr int RB = 8;
   dim3 grid((unsigned)((n + 7) / 8), (unsigned)((R + RB - 1) / RB));
   spmv_kernel<RB><<<grid, 256, 0, st>>>(n, ptr, idx, val, x, ldx, y, ldy, R);

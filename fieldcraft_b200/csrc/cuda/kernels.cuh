@@ -256,9 +256,13 @@ void launch_pcg_step(int64_t n, int R, const double *rz, const double *pq, const
                      const double *q, double *x, int64_t ldx, double *r, cudaStream_t st);
 void launch_pcg_direction(int64_t n, int R, const double *rz_new, const double *rz_old, const double *z, double *p,
                           cudaStream_t st);
-// y = A x for column-major x, y (leading dimensions ldx, ldy).
+// y = A x for column-major x, y (leading dimensions ldx, ldy). With `scratch` (2 n R doubles) and
+// R >= SPMV_ROWS_MIN_R, x is transposed to row-major there, multiplied with every row's right-hand
+// sides contiguous, and the result transposed back (the column-major gather reads one sector per
+// entry and right-hand side).
+constexpr int SPMV_ROWS_MIN_R = 4;
 void launch_spmv(int64_t n, const int64_t *ptr, const int32_t *idx, const double *val, const double *x, int64_t ldx,
-                 double *y, int64_t ldy, int R, cudaStream_t st);
+                 double *y, int64_t ldy, int R, cudaStream_t st, double *scratch = nullptr);
 // Copies the L panels out into the reference's packed trapezoids (dst offsets per supernode).
 void launch_pack_trapezoids(const Tree &t, bool fp32, int64_t ns, const int64_t *toff, double *dst,
                             cudaStream_t st);
