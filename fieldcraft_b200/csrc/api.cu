@@ -90,6 +90,7 @@ struct fc_chol {
   int64_t l_len = 0, u_len = 0;
   // device
   DeviceBuf d_first, d_width, d_height, d_rows_off, d_rows, d_loff, d_uoff, d_kid_ptr, d_kids, d_rel_off, d_rel;
+  DeviceBuf d_kid_meta;
   DeviceBuf d_a_ptr, d_a_src, d_a_dst, d_diag_src, d_L, d_U, d_D, d_perm, d_val, d_status, d_toff, d_doff;
   DeviceBuf d_a_row, d_a_col, d_scale;   // mixed precision only
   DeviceBuf d_Dinv, d_T;                 // diagonal-block inverses; the doubling's products
@@ -257,6 +258,7 @@ void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::Assem
       }
       fc::AssembleTask k{};
       k.s = (int32_t)s, k.j0 = j0, k.j1 = j1, k.i0 = i0, k.i1 = i1, k.mode = mode, k.ranges = base;
+      k.nk = (int32_t)nk, k.k0 = (int32_t)q0, k.m = m, k.w = w, k.loff = h->loff[s], k.uoff = h->uoff[s];
       if (mode == fc::ASM_L) {
         const int64_t b0 = h->a_ptr[f + j0], b1 = h->a_ptr[f + j1];
         const int32_t *lr = h->a_lrow.data();
@@ -849,6 +851,14 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   UP(h->d_uoff, h->uoff);
   UP(h->d_kid_ptr, h->kid_ptr);
   UP(h->d_kids, h->kids);
+  {
+    std::vector<fc::KidMeta> meta(h->kids.size());
+    for (size_t q = 0; q < h->kids.size(); ++q) {
+      const int64_t c = h->kids[q];
+      meta[q] = {h->uoff[c], rel_off[c], h->height[c] - h->width[c], 0};
+    }
+    UP(h->d_kid_meta, meta);
+  }
   UP(h->d_rel_off, rel_off);
   UP(h->d_rel, rel);
   UP(h->d_a_ptr, a_ptr);
@@ -891,6 +901,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   t.uoff = h->d_uoff.as<int64_t>();
   t.kid_ptr = h->d_kid_ptr.as<int64_t>();
   t.kids = h->d_kids.as<int32_t>();
+  t.kid_meta = h->d_kid_meta.as<fc::KidMeta>();
   t.rel_off = h->d_rel_off.as<int64_t>();
   t.rel = h->d_rel.as<int32_t>();
   t.a_ptr = h->d_a_ptr.as<int64_t>();

@@ -66,13 +66,20 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
   static_assert(ASSEMBLE_ROWS == ASSEMBLE_THREADS && ASSEMBLE_COLS * 32 == ASSEMBLE_THREADS, "tile shape");
   __shared__ T tile[ASSEMBLE_COLS][ASSEMBLE_ROWS];
   __shared__ T lj[ASSEMBLE_THIN][ASSEMBLE_COLS];
+  __shared__ int4 s_rg[ASSEMBLE_KIDS];
+  __shared__ KidMeta s_km[ASSEMBLE_KIDS];
   const AssembleTask task = tasks[blockIdx.x];
-  const int s = task.s;
-  const int m = t.height[s], w = t.width[s], u = m - w;
-  T *Ls = static_cast<T *>(t.L) + t.loff[s];
-  T *Us = static_cast<T *>(t.U) + t.uoff[s];
+  const int m = task.m, w = task.w, u = m - w, nk = task.nk;
+  T *Ls = static_cast<T *>(t.L) + task.loff;
+  T *Us = static_cast<T *>(t.U) + task.uoff;
   const int j0 = task.j0, nc = task.j1 - task.j0, i0 = task.i0, nr = task.i1 - task.i0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the children's ranges and whereabouts, loaded beside the initial values (the task carries the
+  // supernode's own, so no load waits for another before the children's rows)
+  if (tid < nk && tid < ASSEMBLE_KIDS) {
+    s_rg[tid] = ranges[task.ranges + tid];
+    s_km[tid] = t.kid_meta[task.k0 + tid];
+  }
   // column jj of the tile, indexed by front row
   auto column = [&](int jj) -> T * {
     const int J = j0 + jj;
@@ -113,9 +120,8 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
     for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) tile[jj][ii] = T(0);
     __syncthreads();
     // A's entries of the tile: the block's entries are sorted by row, [e0, e1) are this tile's
-    const int64_t lo = t.loff[s];
     for (int64_t e = task.e0 + tid; e < task.e1; e += ASSEMBLE_THREADS) {
-      const int p = (int)(t.a_dst[e] - lo), J = p / m, row = p - J * m;
+      const int p = (int)(t.a_dst[e] - task.loff), J = p / m, row = p - J * m;
       const double a = t.scale ? val[t.a_src[e]] * t.scale[t.a_row[e]] * t.scale[t.a_col[e]] : val[t.a_src[e]];
       tile[J - j0][row - i0] = T(a);
     }
@@ -123,31 +129,30 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
   __syncthreads();
   // the children: warp q takes the child's q-th column in the tile (a child has at most one column
   // per tile column), its lanes the rows, eight loads a lane in flight before the adds
-  const int k0 = (int)t.kid_ptr[s], k1 = (int)t.kid_ptr[s + 1];
-  for (int kp = k0; kp < k1; ++kp) {
-    const int4 g = ranges[task.ranges + (kp - k0)];
+  for (int q = 0; q < nk; ++q) {
+    const int4 g = q < ASSEMBLE_KIDS ? s_rg[q] : ranges[task.ranges + q];
     const int jc = g.x + warp;
     if (g.x < g.y && g.z < g.w) {
       if (jc < g.y) {
-        const int c = t.kids[kp];
-        const int uc = t.height[c] - t.width[c];
-        const int32_t *rel = t.rel + t.rel_off[c];
-        const T *src = static_cast<const T *>(t.U) + t.uoff[c] + (int64_t)jc * uc;
-        const int jj = rel[jc] - j0;
+        const KidMeta km = q < ASSEMBLE_KIDS ? s_km[q] : t.kid_meta[task.k0 + q];
+        const int32_t *rel = t.rel + km.rel_off;
+        const T *src = static_cast<const T *>(t.U) + km.uoff + (int64_t)jc * km.uc;
         const int a = g.z > jc ? g.z : jc;
         int at[ASSEMBLE_ROWS / 32];
         T v[ASSEMBLE_ROWS / 32];
+        const int relj = rel[jc];
 #pragma unroll
-        for (int q = 0; q < ASSEMBLE_ROWS / 32; ++q) {
-          const int ic = a + lane + 32 * q;
+        for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k) {
+          const int ic = a + lane + 32 * k;
           if (ic < g.w) {
-            at[q] = rel[ic];
-            v[q] = src[ic];
+            at[k] = rel[ic];
+            v[k] = src[ic];
           }
         }
+        const int jj = relj - j0;
 #pragma unroll
-        for (int q = 0; q < ASSEMBLE_ROWS / 32; ++q)
-          if (a + lane + 32 * q < g.w) tile[jj][at[q] - i0] += v[q];
+        for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k)
+          if (a + lane + 32 * k < g.w) tile[jj][at[k] - i0] += v[k];
       }
       __syncthreads();
     }

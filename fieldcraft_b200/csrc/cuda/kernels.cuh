@@ -17,12 +17,19 @@ constexpr int PANEL_ROWS = 64;  // rows of a panel solved by one CTA
 // (a thread per row, a warp per child column); a supernode at most ASSEMBLE_THIN columns wide has
 // its update matrix formed by the assembly itself instead of by a GEMM.
 constexpr int ASSEMBLE_COLS = 8, ASSEMBLE_ROWS = 256, ASSEMBLE_THREADS = 256, ASSEMBLE_THIN = 16;
+constexpr int ASSEMBLE_KIDS = 8;  // children whose ranges a tile keeps in shared memory (the rest: global)
 constexpr int SPLIT_K = 512;  // K chunk of a split GEMM (a long sum over few outputs)
 // The solve applies the inverse of a supernode's diagonal block SB columns at a time: the inverses
 // of its diagonal blocks of up to SB columns are formed during the factorisation (from the 64 x 64
 // inverses of the panels, by doubling), so a solve step is a GEMM over SB columns, not a chain of
 // SB / 64 dependent panel steps.
 constexpr int SB = 1024;
+
+// A child as its parent's assembly reads it: its update matrix (offset, height) and relative map.
+struct KidMeta {
+  int64_t uoff, rel_off;
+  int32_t uc, pad;
+};
 
 // Where each supernode lives on the device. A front of supernode s has m = rows(s) rows and
 // w = width(s) columns of L; its update matrix U_s is the (m-w) x (m-w) Schur complement.
@@ -36,6 +43,7 @@ struct Tree {
   const int64_t *uoff;      // [ns] U: (m-w) x (m-w), column-major, ld m-w (lower half used)
   const int64_t *kid_ptr;   // [ns+1]
   const int32_t *kids;      // children in increasing order
+  const KidMeta *kid_meta;  // per entry of kids
   const int64_t *rel_off;   // [ns] where a child's relative map starts (its rows past its columns)
   const int32_t *rel;       // positions of a child's rows in its parent's structure
   const int64_t *a_ptr;     // [n+1] input entries by postordered column
@@ -59,8 +67,10 @@ struct Tree {
 // input entries of an ASM_L tile.
 enum AssembleMode : int32_t { ASM_L = 0, ASM_U = 1, ASM_U_PRODUCT = 2 };
 struct AssembleTask {
-  int32_t s, j0, j1, i0, i1, mode, ranges, pad;
+  int32_t s, j0, j1, i0, i1, mode, ranges, nk;  // nk: the supernode's children
   int64_t e0, e1;
+  int64_t loff, uoff;    // the supernode's L and update-matrix offsets
+  int32_t m, w, k0, pad;  // its height and width; its first child's place in the kid lists
 };
 // Panel [c0, c1) of supernode s: factor its diagonal block, invert it, and solve the rows
 // [r0, r1) below it (r0 >= c1; an empty range for a task that only keeps the block). The task
