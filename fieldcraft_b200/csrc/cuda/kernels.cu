@@ -94,13 +94,20 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
     }
     __syncthreads();
     if (ii < nr) {
+      // the row's values of L21 four at a time in flight, then their dot products
       T acc[ASSEMBLE_COLS];
 #pragma unroll
       for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = T(0);
-      for (int k = 0; k < w; ++k) {
-        const T a = Ls[(int64_t)k * m + r];
+      for (int k0 = 0; k0 < w; k0 += 4) {
+        T a[4];
 #pragma unroll
-        for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = fma(a, lj[k][jj], acc[jj]);
+        for (int k = 0; k < 4; ++k) a[k] = k0 + k < w ? Ls[(int64_t)(k0 + k) * m + r] : T(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (k0 + k < w) {
+#pragma unroll
+            for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = fma(a[k], lj[k0 + k][jj], acc[jj]);
+          }
       }
 #pragma unroll
       for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) tile[jj][ii] = -acc[jj];
