@@ -106,9 +106,10 @@ struct fc_chol {
   int64_t pack_len = 0;
   fc::Tree tree{};
   std::vector<Launch> program;
-  cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch)
+  cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch), lowest priority
+  cudaStream_t hi = nullptr;              // lane 0 of the factorisation, highest priority
   std::vector<cudaEvent_t> lane_events;   // per launch of the program that another waits for
-  cudaEvent_t fork_event = nullptr, join_event = nullptr;
+  cudaEvent_t fork_event = nullptr, join_event = nullptr, hi_join_event = nullptr;
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
@@ -157,8 +158,10 @@ struct fc_chol {
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : solve_events) cudaEventDestroy(e);
     if (fork_event) cudaEventDestroy(fork_event);
+    if (hi_join_event) cudaEventDestroy(hi_join_event);
     if (join_event) cudaEventDestroy(join_event);
     if (side) cudaStreamDestroy(side);
+    if (hi) cudaStreamDestroy(hi);
   }
 };
 
@@ -688,9 +691,15 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   for (size_t q = 0; q < h->program.size(); ++q)
     if (h->program[q].record && (e = cudaEventCreateWithFlags(&h->lane_events[q], cudaEventDisableTiming)) != cudaSuccess)
       return cuda_fail(st, e, "lane events");
-  if (!h->side && ((e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess ||
+  // lane 0 (the panels' chain, on the critical path) at the highest priority, lane 1 (the long
+  // updates beside it) at the lowest: a free SM takes the next panel's CTAs before more updates
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (!h->side && ((e = cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least)) != cudaSuccess ||
+                   (e = cudaStreamCreateWithPriority(&h->hi, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->fork_event, cudaEventDisableTiming)) != cudaSuccess ||
-                   (e = cudaEventCreateWithFlags(&h->join_event, cudaEventDisableTiming)) != cudaSuccess))
+                   (e = cudaEventCreateWithFlags(&h->join_event, cudaEventDisableTiming)) != cudaSuccess ||
+                   (e = cudaEventCreateWithFlags(&h->hi_join_event, cudaEventDisableTiming)) != cudaSuccess))
     return cuda_fail(st, e, "lane stream");
   return FC_OK;
 }
@@ -983,7 +992,7 @@ bool capture(fc_chol *h, cudaGraphExec_t *exec, F enqueue) {
     cudaGetLastError();
     return false;
   }
-  e = cudaGraphInstantiate(exec, graph, 0);
+  e = cudaGraphInstantiate(exec, graph, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1013,21 +1022,26 @@ int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *canc
 }
 
 int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
-  cudaStream_t main = h->stream;
-  cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), main);
-  if (h->fp32) fc::launch_scale(h->n, h->d_diag_src.as<int64_t>(), d_val, h->d_scale.as<double>(), main);
+  const cudaStream_t user = h->stream;
+  cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), user);
+  if (h->fp32) fc::launch_scale(h->n, h->d_diag_src.as<int64_t>(), d_val, h->d_scale.as<double>(), user);
   const fc::GemmKind gk = h->fp32 ? fc::GemmKind::F32_TF32X3 : fc::GemmKind::F64;
   const fc::Tree &t = h->tree;
-  // lane 1 forks from the main stream here and joins it at the end; profiling keeps one lane
-  const bool lanes = h->side && !h->profiling;
+  // both lanes fork from the caller's stream here and join it at the end (lane 0 on the
+  // high-priority stream, lane 1 on the low-priority one); profiling keeps one lane
+  const bool lanes = h->side && h->hi && !h->profiling;
+  const cudaStream_t main = lanes ? h->hi : user;
   if (lanes) {
-    cudaEventRecord(h->fork_event, main);
+    cudaEventRecord(h->fork_event, user);
     cudaStreamWaitEvent(h->side, h->fork_event, 0);
+    cudaStreamWaitEvent(h->hi, h->fork_event, 0);
   }
   auto join = [&]() {
     if (lanes) {
       cudaEventRecord(h->join_event, h->side);
-      cudaStreamWaitEvent(main, h->join_event, 0);
+      cudaStreamWaitEvent(user, h->join_event, 0);
+      cudaEventRecord(h->hi_join_event, h->hi);
+      cudaStreamWaitEvent(user, h->hi_join_event, 0);
     }
   };
   int last_level = -1;
