@@ -107,6 +107,30 @@ def test_solve_many_is_each_solve_bit_for_bit(cuda):
         assert np.array_equal(a.view(np.uint64), t.view(np.uint64))
 
 
+def test_split_solve_does_not_depend_on_how_many_are_solved(cuda):
+    """The 16^3 block's top separator (867 columns) makes the solve split its long GEMMs in chunks
+    whose last CTA adds the partials: a right-hand side's solution is still bit for bit the same
+    solved alone, among 5, and among 70 (two blocks of 64 right-hand sides)."""
+    csr = problems.lognormal_block(16, nrhs=1).csr
+    f = Factor.new(UpperColumns.from_symmetric(csr), 2**62)
+    rng = np.random.default_rng(5)
+    rhs = rng.standard_normal((70, csr.n))
+    alone = {}
+    for j in (0, 3, 69):
+        x = rhs[j].copy()
+        f.solve(x)
+        alone[j] = x
+    five = [rhs[j].copy() for j in range(5)]
+    f.solve_many(five)
+    many = [rhs[j].copy() for j in range(70)]
+    f.solve_many(many)
+    same = lambda a, b: np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert same(alone[0], five[0]) and same(alone[3], five[3])
+    assert same(alone[0], many[0]) and same(alone[3], many[3]) and same(alone[69], many[69])
+    r = oracle.spmv(csr.n, csr.ptr, csr.idx, csr.val, alone[69]) - rhs[69]
+    assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rhs[69])
+
+
 def test_factorisation_is_deterministic(cuda):
     csr = problems.lognormal_block(10, nrhs=1).csr
     up = UpperColumns.from_symmetric(csr)
