@@ -191,6 +191,7 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     full = problems.lognormal_block(args.n_el, nrhs=args.nrhs, seed=SEED)
     full_flops, _ = factor_flops(full)
+    n, nnz = full.n, int(full.csr.idx.size)
     del full
     times = []
     for it in range(args.warmup + args.steps):
@@ -202,8 +203,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"FP64 direct solve, hex8 block {args.n_el}^3 lognormal E, {args.nrhs} RHS",
-                   "n": None, "nrhs": args.nrhs},
+        "config": {"workload": f"FP64 direct solve, hex8 block {args.n_el}^3 lognormal E (sigma 0.5), z=0 clamped, "
+                               f"{args.nrhs} Gaussian top-face RHS", "n": n, "nnz": nnz, "nrhs": args.nrhs},
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
