@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
       }
   }
   for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
-  if (rows > 0) load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, rows, pw, K4);
+  if (rows > 0) load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, min(rows, 64), pw, K4);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
@@ -386,13 +386,22 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
       }
     if (tid == 0 && fail < pw) atomicMin(&status->failed_column, (unsigned long long)(f + c0 + fail));
   }
-  if (rows > 0) {
+  // the rows below, 64 at a time (the first 64 loaded with the block)
+  for (int rr = 0; rr < rows; rr += 64) {
+    const int nrr = min(64, rows - rr);
+    if (rr > 0) {
+      __syncthreads();  // the previous rows' tile is read
+      load_tile<T>(bt, Ls + task.r0 + rr + (int64_t)c0 * m, 1, m, nrr, pw, K4);
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+    }
     double acc[4][4][2];
     zero_acc(acc);
     mma_tiles<T>(bt, inv, K4, acc);
-    T *dst = Ls + task.r0 + (int64_t)c0 * m;
+    T *dst = Ls + task.r0 + rr + (int64_t)c0 * m;
     each_acc(acc, [&](int i, int c, double v) {
-      if (i < rows && c < pw) dst[i + (int64_t)c * m] = T(v);
+      if (i < nrr && c < pw) dst[i + (int64_t)c * m] = T(v);
     });
   }
 }

@@ -12,7 +12,7 @@ namespace fc {
 constexpr int NB = 64;
 constexpr int GEMM_TM = 64, GEMM_TN = 64, GEMM_KC = 16;
 constexpr int GEMM_THREADS = 128;
-constexpr int PANEL_ROWS = 64;  // rows of a panel solved by one CTA
+constexpr int PANEL_ROWS = 128;  // rows of a panel solved by one CTA (64 at a time)
 // A front is assembled by tiles of ASSEMBLE_COLS columns by ASSEMBLE_ROWS rows, one CTA each
 // (a thread per row, a warp per child column); a supernode at most ASSEMBLE_THIN columns wide has
 // its update matrix formed by the assembly itself instead of by a GEMM.
