@@ -58,8 +58,9 @@ struct Launch {
   int count;
   int level;  // the level of the supernodal tree the launch belongs to (cancellation points)
   int width;  // panel launches: the widest panel, padded (sizes the kernel's shared memory)
-  // the factorisation runs on two streams (lanes): a panel step's update of the columns after the
-  // next panel goes on lane 1, so it overlaps the next panel; `dep` is a launch on the other lane
+  // the factorisation runs on three streams (lanes): lane 0 the chain of panels and what needs
+  // them, lane 1 the updates of columns past the next outer block (beside the next panels), lane 2
+  // the diagonal blocks' inverses (needed by the solve only); `dep` is a launch on another lane
   // this one waits for (-1: none), `record` marks a launch another waits for
   int lane = 0;
   int dep = -1;
@@ -108,8 +109,9 @@ struct fc_chol {
   std::vector<Launch> program;
   cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch), lowest priority
   cudaStream_t hi = nullptr;              // lane 0 of the factorisation, highest priority
+  cudaStream_t side2 = nullptr;           // lane 2: the diagonal blocks' inverses, lowest priority
   std::vector<cudaEvent_t> lane_events;   // per launch of the program that another waits for
-  cudaEvent_t fork_event = nullptr, join_event = nullptr, hi_join_event = nullptr;
+  cudaEvent_t fork_event = nullptr, join_event = nullptr, hi_join_event = nullptr, join2_event = nullptr;
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
@@ -162,6 +164,8 @@ struct fc_chol {
     if (join_event) cudaEventDestroy(join_event);
     if (side) cudaStreamDestroy(side);
     if (hi) cudaStreamDestroy(hi);
+    if (side2) cudaStreamDestroy(side2);
+    if (join2_event) cudaEventDestroy(join2_event);
   }
 };
 
@@ -520,6 +524,11 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       }
     }
     pending_join = last_rest;
+    // the diagonal blocks' inverses serve only the solve: lane 2, after the level's panels, beside
+    // everything after them (the doublings of all levels in order on that one stream)
+    int panels_done = -1;
+    for (int q = (int)h->program.size() - 1; q >= 0 && panels_done < 0; --q)
+      if (h->program[q].lane == 0) panels_done = q;
     for (int hh = NB; hh < fc::SB; hh *= 2) {
       std::vector<fc::GemmTask> first, second;
       inverse_doubling(h, S, h->d_T.as<double>(), hh, &first, &second);
@@ -527,9 +536,15 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       int64_t go = (int64_t)gemm_t.size();
       gemm_t.insert(gemm_t.end(), first.begin(), first.end());
       push(h->program, K_GEMM_MIXED, go, (int64_t)first.size(), (int)l);
+      h->program.back().lane = 2;
+      if (hh == NB && panels_done >= 0) {
+        h->program.back().dep = panels_done;
+        h->program[panels_done].record = true;
+      }
       go = (int64_t)gemm_t.size();
       gemm_t.insert(gemm_t.end(), second.begin(), second.end());
       push(h->program, K_GEMM_F64, go, (int64_t)second.size(), (int)l);
+      h->program.back().lane = 2;
     }
     if (tc) {
       // pack each supernode's L21 (K-major hi | lo), then its 128 x 128 tiles by TMA + tcgen05
@@ -697,6 +712,8 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   cudaDeviceGetStreamPriorityRange(&least, &greatest);
   if (!h->side && ((e = cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least)) != cudaSuccess ||
                    (e = cudaStreamCreateWithPriority(&h->hi, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
+                   (e = cudaStreamCreateWithPriority(&h->side2, cudaStreamNonBlocking, least)) != cudaSuccess ||
+                   (e = cudaEventCreateWithFlags(&h->join2_event, cudaEventDisableTiming)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->fork_event, cudaEventDisableTiming)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->join_event, cudaEventDisableTiming)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->hi_join_event, cudaEventDisableTiming)) != cudaSuccess))
@@ -1029,17 +1046,20 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
   const fc::Tree &t = h->tree;
   // both lanes fork from the caller's stream here and join it at the end (lane 0 on the
   // high-priority stream, lane 1 on the low-priority one); profiling keeps one lane
-  const bool lanes = h->side && h->hi && !h->profiling;
+  const bool lanes = h->side && h->hi && h->side2 && !h->profiling;
   const cudaStream_t main = lanes ? h->hi : user;
   if (lanes) {
     cudaEventRecord(h->fork_event, user);
     cudaStreamWaitEvent(h->side, h->fork_event, 0);
+    cudaStreamWaitEvent(h->side2, h->fork_event, 0);
     cudaStreamWaitEvent(h->hi, h->fork_event, 0);
   }
   auto join = [&]() {
     if (lanes) {
       cudaEventRecord(h->join_event, h->side);
       cudaStreamWaitEvent(user, h->join_event, 0);
+      cudaEventRecord(h->join2_event, h->side2);
+      cudaStreamWaitEvent(user, h->join2_event, 0);
       cudaEventRecord(h->hi_join_event, h->hi);
       cudaStreamWaitEvent(user, h->hi_join_event, 0);
     }
@@ -1056,7 +1076,7 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
       }
       last_level = l.level;
     }
-    const cudaStream_t st = lanes && l.lane ? h->side : main;
+    const cudaStream_t st = !lanes || l.lane == 0 ? main : l.lane == 1 ? h->side : h->side2;
     if (lanes && l.dep >= 0) cudaStreamWaitEvent(st, h->lane_events[l.dep], 0);
     Mark mark(h, l.kind, l.level, l.count);
     switch (l.kind) {
