@@ -1209,7 +1209,10 @@ struct SplitPush {
         fc::GemmTask c = g;
         const int64_t k0 = (int64_t)q * SOLVE_KC;
         c.A = static_cast<const char *>(g.A) + k0 * g.a_sk * (int64_t)pg.second.first;
-        c.B = static_cast<const char *>(g.B) + k0 * g.b_sk * (int64_t)pg.second.second;
+        if (g.flags & 16)
+          c.b_rows = g.b_rows + k0;  // B's rows through the row list
+        else
+          c.B = static_cast<const char *>(g.B) + k0 * g.b_sk * (int64_t)pg.second.second;
         c.K = (int)std::min<int64_t>(SOLVE_KC, g.K - k0);
         c.flags = g.flags | 8;
         c.part_off = at, c.chunks = chunks, c.chunk = q, c.counter = (int32_t)p.tcount + cnt;
@@ -1352,13 +1355,8 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
       }
     }
     push(bwd, K_SOLVE_THIN_BWD, tb, (int64_t)p.tbwd.size() - tb, (int)l);
-    int64_t ro = (int64_t)rows.size();
-    for (int64_t s : S) {
-      if (thin(s)) continue;
-      const int u = h->height[s] - h->width[s];
-      for (int i0 = 0; i0 < u; i0 += 64) rows.push_back({(int32_t)s, i0, std::min(u, i0 + 64), 0});
-    }
-    push(bwd, K_SOLVE_GATHER, ro, (int64_t)rows.size() - ro, (int)l);
+    // own rows -= L21^T x(rows past the columns): the GEMM reads those rows of x through the
+    // supernode's row list (final by now: they belong to supernodes of higher levels)
     int64_t go = (int64_t)gemm.size();
     for (int64_t s : S) {
       const int m = h->height[s], w = h->width[s], u = m - w;
@@ -1371,8 +1369,10 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
           g.c_si = R, g.c_sj = 1;
           g.A = Lp(lo + w + (int64_t)i0 * m);
           g.a_si = m, g.a_sk = 1;
-          g.B = v + voff[s] + j0;
+          g.B = x + j0;
           g.b_sj = 1, g.b_sk = R;
+          g.b_rows = h->d_rows.as<int32_t>() + h->rows_off[s] + w;
+          g.flags = 16;
           g.M = std::min(fc::GEMM_TM, w - i0), g.N = std::min(fc::GEMM_TN, R - j0), g.K = u;
           sp.add(g, es, sizeof(double), j0 == 0);
         }

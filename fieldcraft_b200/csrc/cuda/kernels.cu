@@ -450,6 +450,24 @@ struct TileLoader {
     }
     p += dstage;
   }
+  // the same tile with row k of the operand at base + rows[k] * sk (unit stride along i, the
+  // layout init gives for si == 1): a gather through a row list, the stage's indices loaded first
+  template <int S>
+  __device__ __forceinline__ void load_rows(T (*Sm)[S], int kbase, int K, const T *base, const int32_t *rows,
+                                            int64_t sk, const T *safe) {
+    int r[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int k = k0 + q * dk;
+      r[q] = kbase + k < K ? rows[kbase + k] : 0;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int i = i0 + q * di, k = k0 + q * dk;
+      const bool ok = i < lim && kbase + k < K;
+      cp_async<sizeof(T)>(&Sm[k][i], ok ? base + (int64_t)r[q] * sk + i : safe, ok ? (int)sizeof(T) : 0);
+    }
+  }
 };
 
 // Writes a GEMM task's 64 x 64 tile (acc[r][c][e] of the m16n8k8 fragments of a 32 x 32 warp
@@ -584,10 +602,19 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.0;
   const int nk = (K + GEMM_KC - 1) / GEMM_KC;
 #pragma unroll
+  const bool gather = tp->flags & 16;
+  const int32_t *brows = tp->b_rows;
+  const int64_t bsk = tp->b_sk;
+  auto load_b = [&](int stage, int kbase) {
+    if (gather)
+      lb.load_rows(Bs[stage], kbase, K, bbase, brows, bsk, bbase);
+    else
+      lb.load(Bs[stage], kbase, K, bbase);
+  };
   for (int st = 0; st < GEMM_STAGES - 1; ++st) {
     if (st < nk) {
       la.load(As[st], st * GEMM_KC, K, abase);
-      lb.load(Bs[st], st * GEMM_KC, K, bbase);
+      load_b(st, st * GEMM_KC);
     }
     cp_async_commit();
   }
@@ -597,7 +624,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *_
     const int pf = kt + GEMM_STAGES - 1;
     if (pf < nk) {
       la.load(As[pf % GEMM_STAGES], pf * GEMM_KC, K, abase);
-      lb.load(Bs[pf % GEMM_STAGES], pf * GEMM_KC, K, bbase);
+      load_b(pf % GEMM_STAGES, pf * GEMM_KC);
     }
     cp_async_commit();
     const int st = kt % GEMM_STAGES;

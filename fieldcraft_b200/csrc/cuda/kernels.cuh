@@ -84,7 +84,8 @@ struct PanelTask {
 };
 // C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands. Flags: 1 touches
 // i >= j only (a diagonal tile of a symmetric matrix); 2 stores C = -sum instead of subtracting;
-// 4 stores C = +sum. Flag 8 (FP64 C only): this task is chunk `chunk` of `chunks` of one split
+// 4 stores C = +sum. Flag 16 (FP64 B, unit j stride): B's row k is at B + b_rows[k] * b_sk (a
+// gather through a row list). Flag 8 (FP64 C only): this task is chunk `chunk` of `chunks` of one split
 // sum over K; each chunk stores its 64 x 64 partial at part + part_off + chunk * 4096 (`part`
 // given at launch), and the last chunk to finish (counters[counter], reset by it) adds the
 // partials in chunk order and applies the total to C by the other flags. No chunk waits.
@@ -96,6 +97,7 @@ struct GemmTask {
   int32_t M, N, K, flags;
   int64_t part_off;
   int32_t chunks, chunk, counter, pad;
+  const int32_t *b_rows;
 };
 // Solve, panel [c0, c1) of supernode s, right-hand sides [j0, j1): apply the inverse of the
 // diagonal block (forward: L^-1, backward: L^-T), then update the front rows [r0, r1) (forward:
