@@ -559,9 +559,11 @@ def main():
     factor_ms = float(ms_k[0:4].sum() + ms_k[10:13].sum() + ms_k[15])
     solve_ms = float(ms_k[16:32].sum())
     traffic = None
-    tf = ROOT / "profiles" / "gemm_kernel_traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+    tf = ROOT / "profiles" / "gemm_kernel_traffic_block48.md"  # an ncu capture's summary
+    if tf.exists() and args.n_el == N_EL:
+        for line_ in tf.read_text().splitlines():
+            if line_.startswith("bytes_per_launch:"):
+                traffic = int(line_.split(":")[1])
 
     # end to end through the public API with pinned host buffers
     hv = torch.from_numpy(up.val).pin_memory()
