@@ -203,7 +203,10 @@ int fc_chol_profile_read(fc_chol *h, double *ms, int64_t *launches, int32_t kind
 int64_t fc_chol_profile_launches(fc_chol *h, int32_t *kind, int32_t *level, int32_t *tasks, float *ms, int64_t cap);
 
 /* ---- compressed-row products (Csr::mul, crates/solver/src/sparse.rs:42-50) ---------------------
- * y = A x on the device for nrhs vectors, x and y column-major with leading dimension ld. */
+ * y = A x on the device for nrhs vectors, x and y column-major with leading dimension ld. With 4
+ * or more vectors the product goes through row-major copies in scratch of 16 n nrhs bytes taken
+ * from the stream-ordered allocator on `stream` and released on it (cudaMallocAsync /
+ * cudaFreeAsync); if that allocation fails the column-major kernel runs instead. */
 int fc_csr_spmv_device(int64_t n, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val,
                        const double *d_x, double *d_y, int32_t nrhs, int64_t ld, void *stream);
 
