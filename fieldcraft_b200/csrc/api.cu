@@ -464,6 +464,22 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     // lane 1, which also wrote them), the rest on lane 1 beside the next block's panels.
     const int OP = OUTER_PANELS;
     int last_rest = -1;   // the level's latest lane-1 launch
+    int64_t blk_at = 0;   // the level's packed blocks (the update matrices' packs reuse the space)
+    auto tc_tiles = [&](int64_t s, int jlo, int jhi, int32_t map, int kw, int wpad, int row0,
+                        std::vector<fc::TcTask> &out) {
+      const int m = h->height[s];
+      const int64_t lo = h->loff[s];
+      for (int jc = jlo; jc < jhi; jc += fc::GEMM_TC_N)
+        for (int ic = jc; ic < m; ic += fc::GEMM_TC_M) {
+          fc::TcTask g{};
+          g.map = map, g.bi = ic - row0, g.bj = jc - row0;
+          g.M = std::min(fc::GEMM_TC_M, m - ic), g.N = std::min(fc::GEMM_TC_N, jhi - jc), g.K = kw, g.wpad = wpad;
+          g.flags = ic == jc ? 1 : 0;
+          g.C = static_cast<float *>(Lp(lo + ic + (int64_t)jc * m));
+          g.c_sj = m;
+          out.push_back(g);
+        }
+    };
     int last_inner = -1;  // the previous step's lane-3 launch (the block's columns past the next panel)
     auto tiles = [&](int64_t s, int jlo, int jhi, int k0, int k1, std::vector<fc::GemmTask> &out) {
       const int m = h->height[s];
@@ -486,6 +502,8 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       int64_t po = (int64_t)panel_t.size(), go = (int64_t)gemm_t.size();
       std::vector<fc::GemmTask> rest;   // updates of the columns past the next block (lane 1)
       std::vector<fc::GemmTask> inner;  // of the block's columns past the next panel (lane 3)
+      std::vector<fc::PackTask> blk_pack;       // tcgen05 path: the ending blocks' columns packed
+      std::vector<fc::TcTask> tc_next, tc_rest;  // and their updates past the block (lanes 0, 1)
       bool outer = false;              // this step's lane-0 launch updates a next block's columns
       int p8max = 8;
       for (int64_t s : S) {
@@ -510,18 +528,40 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         }
         if (c1 == be && be < w) {                                         // past the block
           const int nx = std::min(w, be + OP * NB);
-          tiles(s, be, nx, bs, be, gemm_t);
           outer = true;
-          if (nx < w) tiles(s, nx, w, bs, be, rest);
+          if (tc) {  // the block's columns packed once, the updates on tcgen05
+            const int kw = be - bs, wpad = (kw + fc::TC_KPAD - 1) / fc::TC_KPAD * fc::TC_KPAD, ub = m - be;
+            const int32_t map = (int32_t)maps.size();
+            maps.push_back({blk_at, ub, wpad});
+            for (int r0 = 0; r0 < ub; r0 += fc::TC_PACK_ROWS)
+              blk_pack.push_back({(int32_t)s, r0, wpad, kw, blk_at, bs, be});
+            blk_at += ((int64_t)ub * 2 * wpad + 63) / 64 * 64;
+            tc_tiles(s, be, nx, map, kw, wpad, be, tc_next);
+            if (nx < w) tc_tiles(s, nx, w, map, kw, wpad, be, tc_rest);
+          } else {
+            tiles(s, be, nx, bs, be, gemm_t);
+            if (nx < w) tiles(s, nx, w, bs, be, rest);
+          }
         }
       }
       push(h->program, K_PANEL, po, (int64_t)panel_t.size() - po, (int)l, p8max);
-      const int panel_at = (int)h->program.size() - 1;
+      int panel_at = (int)h->program.size() - 1;  // lane 1's updates read what it is after
+      if (!blk_pack.empty()) {
+        const int64_t bo = (int64_t)pack_t.size();
+        pack_t.insert(pack_t.end(), blk_pack.begin(), blk_pack.end());
+        push(h->program, K_PACK_TC, bo, (int64_t)blk_pack.size(), (int)l);
+        panel_at = (int)h->program.size() - 1;
+      }
       const size_t before = h->program.size();
+      if (!tc_next.empty()) {
+        const int64_t to = (int64_t)tc_t.size();
+        tc_t.insert(tc_t.end(), tc_next.begin(), tc_next.end());
+        push(h->program, K_GEMM_TC, to, (int64_t)tc_next.size(), (int)l);
+      }
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
       const int after = outer ? last_rest : last_inner;  // the next panel's columns after the
       if (h->program.size() > before && after >= 0) {   // previous update of the same columns
-        h->program.back().dep = after;
+        h->program[before].dep = after;
         h->program[after].record = true;
       }
       last_inner = -1;
@@ -535,10 +575,16 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         h->program[panel_at].record = true;
         last_inner = (int)h->program.size() - 1;
       }
-      if (!rest.empty()) {
-        const int64_t ro = (int64_t)gemm_t.size();
-        gemm_t.insert(gemm_t.end(), rest.begin(), rest.end());
-        push(h->program, K_GEMM, ro, (int64_t)rest.size(), (int)l);
+      if (!rest.empty() || !tc_rest.empty()) {
+        if (!rest.empty()) {
+          const int64_t ro = (int64_t)gemm_t.size();
+          gemm_t.insert(gemm_t.end(), rest.begin(), rest.end());
+          push(h->program, K_GEMM, ro, (int64_t)rest.size(), (int)l);
+        } else {
+          const int64_t to = (int64_t)tc_t.size();
+          tc_t.insert(tc_t.end(), tc_rest.begin(), tc_rest.end());
+          push(h->program, K_GEMM_TC, to, (int64_t)tc_rest.size(), (int)l);
+        }
         Launch &r = h->program.back();
         r.lane = 1;
         r.dep = panel_at;
@@ -579,7 +625,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         const int wpad = (w + fc::TC_KPAD - 1) / fc::TC_KPAD * fc::TC_KPAD;
         const int32_t map = (int32_t)maps.size();
         maps.push_back({at, u, wpad});
-        for (int r0 = 0; r0 < u; r0 += fc::TC_PACK_ROWS) pack_t.push_back({(int32_t)s, r0, wpad, 0, at});
+        for (int r0 = 0; r0 < u; r0 += fc::TC_PACK_ROWS) pack_t.push_back({(int32_t)s, r0, wpad, w, at, 0, w});
         at += ((int64_t)u * 2 * wpad + 63) / 64 * 64;  // 256-byte aligned regions
         const int64_t uo = h->uoff[s];
         for (int bj = 0; bj < u; bj += fc::GEMM_TC_N)
@@ -593,7 +639,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             tc_t.push_back(g);
           }
       }
-      h->pack_len = std::max(h->pack_len, at);
+      h->pack_len = std::max(h->pack_len, std::max(at, blk_at));
       push(h->program, K_PACK_TC, po, (int64_t)pack_t.size() - po, (int)l);
       push(h->program, K_GEMM_TC, to, (int64_t)tc_t.size() - to, (int)l);
     } else {

@@ -4,7 +4,8 @@
 //
 // Before a level's products, pack_tc_kernel writes each supernode's L21 once as a K-major FP32
 // array P (row i of L21 = row i of P: [hi(0..wpad) | lo(0..wpad)], wpad = w rounded up to 32,
-// hi = x rounded to TF32 and lo = x - hi, exact in FP32; the padding is zero). The tensor core
+// hi = x rounded to TF32 and lo = x - hi, exact in FP32; the padding is zero); likewise, at the
+// end of an outer block of panels, the block's columns below it for the updates past the block. The tensor core
 // then reads hi exactly, and hi hi + hi lo + lo hi keeps FP32 accuracy (the 3xTF32 split) with no
 // per-tile conversion work.
 //
@@ -239,16 +240,17 @@ __global__ void __launch_bounds__(TC_THREADS, 2) syrk_tc_kernel(const TcTask *__
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_COLS));
 }
 
-// P rows [r0, r0 + TC_PACK_ROWS) of supernode s: hi and lo of L21 (FP32 in the L arena,
-// column-major) as K-major rows, through a shared tile so that both the reads (down a column) and
-// the writes (along a row) are coalesced.
+// P rows [r0, r0 + TC_PACK_ROWS) of a block of supernode s's L (FP32 in the L arena, column-major):
+// hi and lo as K-major rows, through a shared tile so that both the reads (down a column) and the
+// writes (along a row) are coalesced.
 __global__ void __launch_bounds__(256) pack_tc_kernel(Tree t, const PackTask *__restrict__ tasks,
                                                        float *__restrict__ P) {
   __shared__ float tile[TC_KPAD][TC_PACK_ROWS + 1];
   const PackTask task = tasks[blockIdx.x];
   const int s = task.s;
-  const int m = t.height[s], w = t.width[s], u = m - w;
-  const float *Lb = static_cast<const float *>(t.L) + t.loff[s] + w;  // Lb[k m + i] = L21(i, k)
+  const int m = t.height[s], u = m - task.row0, w = task.kw;
+  // Lb[k m + i] = L(row0 + i, c0 + k)
+  const float *Lb = static_cast<const float *>(t.L) + t.loff[s] + (int64_t)task.c0 * m + task.row0;
   const int r0 = task.r0, nr = min(TC_PACK_ROWS, u - r0), wpad = task.wpad;
   float *Pp = P + task.poff;
   for (int kc = 0; kc < wpad; kc += TC_KPAD) {

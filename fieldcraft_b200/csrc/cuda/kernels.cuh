@@ -207,18 +207,21 @@ void configure_kernels();
 // The operand types of a GEMM launch: FP64 throughout (DMMA); an FP32 A with FP64 B and C (DMMA,
 // the solve on an FP32 factor); FP32 throughout by 3xTF32 (the FP32 factorisation).
 enum class GemmKind { F64, F32A_F64, F32_TF32X3 };
-// The mixed-precision factor's update matrices on the tcgen05 tensor cores. Each supernode's L21
-// is first packed as a K-major FP32 array P: row i = [hi(L21(i, 0..wpad)) | lo(...)], wpad = w
-// rounded up to TC_KPAD, at P + poff, by PackTask row blocks of TC_PACK_ROWS. A TcTask is one
-// tile C(bi.., bj..) of up to GEMM_TC_M x GEMM_TC_N of U -= L21 L21^T (flags as GemmTask: 1 lower
-// triangle only, 2 store -product), its operands read by TMA through tensor map `map` of the
-// supernode's P (an array of 128-byte CUtensorMap objects in device memory); a wait that gives up
-// sets status->timeout.
+// The mixed-precision factor's long products on the tcgen05 tensor cores: the update matrices
+// (U = -L21 L21^T) and a front's updates past an outer block (C -= L(rows, block) L(cols, block)^T).
+// The operand block of L (columns [c0, c0 + kw), front rows from row0 down) is first packed as a
+// K-major FP32 array P: row i = [hi(L(row0 + i, c0..c0 + wpad)) | lo(...)], wpad = kw rounded up
+// to TC_KPAD, at P + poff, by PackTask row blocks of TC_PACK_ROWS. A TcTask is one tile
+// C(bi.., bj..) of up to GEMM_TC_M x GEMM_TC_N (bi, bj: rows of P; flags as GemmTask: 1 lower
+// triangle only, 2 store -product, else subtract), its operands read by TMA through tensor map
+// `map` of the block's P (an array of 128-byte CUtensorMap objects in device memory); a wait that
+// gives up sets status->timeout.
 constexpr int GEMM_TC_M = 128, GEMM_TC_N = 128, TC_KPAD = 32, TC_PACK_ROWS = 64;
 constexpr int TC_KBOX = 16;  // K values of a TMA box (64 bytes: 64-byte swizzle)
 struct PackTask {
-  int32_t s, r0, wpad, pad;
+  int32_t s, r0, wpad, kw;  // rows [r0, r0 + TC_PACK_ROWS) of the packed block, kw columns
   int64_t poff;
+  int32_t c0, row0;  // the block: columns [c0, c0 + kw) of L from front row row0 down
 };
 struct TcTask {
   int32_t map, bi, bj, M, N, K, wpad, flags;
