@@ -58,10 +58,9 @@ struct Launch {
   int count;
   int level;  // the level of the supernodal tree the launch belongs to (cancellation points)
   int width;  // panel launches: the widest panel, padded (sizes the kernel's shared memory)
-  // the factorisation runs on four streams (lanes): lane 0 the chain of panels and what needs
+  // the factorisation runs on three streams (lanes): lane 0 the chain of panels and what needs
   // them, lane 1 the updates of columns past the next outer block (beside the next panels), lane 2
-  // the diagonal blocks' inverses (needed by the solve only), lane 3 a panel's update of its
-  // block's columns past the next panel (beside the next panel); `dep` is a launch on another lane
+  // the diagonal blocks' inverses (needed by the solve only); `dep` is a launch on another lane
   // this one waits for (-1: none), `record` marks a launch another waits for
   int lane = 0;
   int dep = -1;
@@ -111,10 +110,8 @@ struct fc_chol {
   cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch), lowest priority
   cudaStream_t hi = nullptr;              // lane 0 of the factorisation, highest priority
   cudaStream_t side2 = nullptr;           // lane 2: the diagonal blocks' inverses, lowest priority
-  cudaStream_t side3 = nullptr;           // lane 3: a block's columns past the next panel, highest
   std::vector<cudaEvent_t> lane_events;   // per launch of the program that another waits for
-  cudaEvent_t fork_event = nullptr, join_event = nullptr, hi_join_event = nullptr, join2_event = nullptr,
-              join3_event = nullptr;
+  cudaEvent_t fork_event = nullptr, join_event = nullptr, hi_join_event = nullptr, join2_event = nullptr;
   int64_t gemm_tasks = 0;
   // solve plan for `solve_R` right-hand sides
   int solve_R = 0;
@@ -168,8 +165,6 @@ struct fc_chol {
     if (side) cudaStreamDestroy(side);
     if (hi) cudaStreamDestroy(hi);
     if (side2) cudaStreamDestroy(side2);
-    if (side3) cudaStreamDestroy(side3);
-    if (join3_event) cudaEventDestroy(join3_event);
     if (join2_event) cudaEventDestroy(join2_event);
   }
 };
@@ -480,7 +475,6 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
           out.push_back(g);
         }
     };
-    int last_inner = -1;  // the previous step's lane-3 launch (the block's columns past the next panel)
     auto tiles = [&](int64_t s, int jlo, int jhi, int k0, int k1, std::vector<fc::GemmTask> &out) {
       const int m = h->height[s];
       const int64_t lo = h->loff[s];
@@ -501,7 +495,6 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
     for (int p = 0; p < P; ++p) {
       int64_t po = (int64_t)panel_t.size(), go = (int64_t)gemm_t.size();
       std::vector<fc::GemmTask> rest;   // updates of the columns past the next block (lane 1)
-      std::vector<fc::GemmTask> inner;  // of the block's columns past the next panel (lane 3)
       std::vector<fc::PackTask> blk_pack;       // tcgen05 path: the ending blocks' columns packed
       std::vector<fc::TcTask> tc_next, tc_rest;  // and their updates past the block (lanes 0, 1)
       bool outer = false;              // this step's lane-0 launch updates a next block's columns
@@ -521,11 +514,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
           panel_t.push_back(
               {(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff, ioff, bw, 0});
         const int bs = p / OP * OP * NB, be = std::min(w, bs + OP * NB);  // this panel's block
-        if (c1 < be) {  // within the block: the next panel's columns now, the rest beside it
-          const int nn = std::min(be, c1 + NB);
-          tiles(s, c1, nn, c0, c1, gemm_t);
-          if (nn < be) tiles(s, nn, be, c0, c1, inner);
-        }
+        if (c1 < be) tiles(s, c1, be, c0, c1, gemm_t);                     // within the block
         if (c1 == be && be < w) {                                         // past the block
           const int nx = std::min(w, be + OP * NB);
           outer = true;
@@ -559,21 +548,9 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         push(h->program, K_GEMM_TC, to, (int64_t)tc_next.size(), (int)l);
       }
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
-      const int after = outer ? last_rest : last_inner;  // the next panel's columns after the
-      if (h->program.size() > before && after >= 0) {   // previous update of the same columns
-        h->program[before].dep = after;
-        h->program[after].record = true;
-      }
-      last_inner = -1;
-      if (!inner.empty()) {
-        const int64_t io = (int64_t)gemm_t.size();
-        gemm_t.insert(gemm_t.end(), inner.begin(), inner.end());
-        push(h->program, K_GEMM, io, (int64_t)inner.size(), (int)l);
-        Launch &r = h->program.back();
-        r.lane = 3;
-        r.dep = panel_at;
-        h->program[panel_at].record = true;
-        last_inner = (int)h->program.size() - 1;
+      if (h->program.size() > before && outer && last_rest >= 0) {  // the next block after rest(b - 1)
+        h->program[before].dep = last_rest;
+        h->program[last_rest].record = true;
       }
       if (!rest.empty() || !tc_rest.empty()) {
         if (!rest.empty()) {
@@ -782,8 +759,6 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   if (!h->side && ((e = cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least)) != cudaSuccess ||
                    (e = cudaStreamCreateWithPriority(&h->hi, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
                    (e = cudaStreamCreateWithPriority(&h->side2, cudaStreamNonBlocking, least)) != cudaSuccess ||
-                   (e = cudaStreamCreateWithPriority(&h->side3, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
-                   (e = cudaEventCreateWithFlags(&h->join3_event, cudaEventDisableTiming)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->join2_event, cudaEventDisableTiming)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->fork_event, cudaEventDisableTiming)) != cudaSuccess ||
                    (e = cudaEventCreateWithFlags(&h->join_event, cudaEventDisableTiming)) != cudaSuccess ||
@@ -1117,13 +1092,12 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
   const fc::Tree &t = h->tree;
   // both lanes fork from the caller's stream here and join it at the end (lane 0 on the
   // high-priority stream, lane 1 on the low-priority one); profiling keeps one lane
-  const bool lanes = h->side && h->hi && h->side2 && h->side3 && !h->profiling;
+  const bool lanes = h->side && h->hi && h->side2 && !h->profiling;
   const cudaStream_t main = lanes ? h->hi : user;
   if (lanes) {
     cudaEventRecord(h->fork_event, user);
     cudaStreamWaitEvent(h->side, h->fork_event, 0);
     cudaStreamWaitEvent(h->side2, h->fork_event, 0);
-    cudaStreamWaitEvent(h->side3, h->fork_event, 0);
     cudaStreamWaitEvent(h->hi, h->fork_event, 0);
   }
   auto join = [&]() {
@@ -1132,8 +1106,6 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
       cudaStreamWaitEvent(user, h->join_event, 0);
       cudaEventRecord(h->join2_event, h->side2);
       cudaStreamWaitEvent(user, h->join2_event, 0);
-      cudaEventRecord(h->join3_event, h->side3);
-      cudaStreamWaitEvent(user, h->join3_event, 0);
       cudaEventRecord(h->hi_join_event, h->hi);
       cudaStreamWaitEvent(user, h->hi_join_event, 0);
     }
@@ -1150,7 +1122,7 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
       }
       last_level = l.level;
     }
-    const cudaStream_t st = !lanes || l.lane == 0 ? main : l.lane == 1 ? h->side : l.lane == 2 ? h->side2 : h->side3;
+    const cudaStream_t st = !lanes || l.lane == 0 ? main : l.lane == 1 ? h->side : h->side2;
     if (lanes && l.dep >= 0) cudaStreamWaitEvent(st, h->lane_events[l.dep], 0);
     Mark mark(h, l.kind, l.level, l.count);
     switch (l.kind) {
