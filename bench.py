@@ -39,7 +39,7 @@ SAMPLE_EL = 24  # the CPU baseline's bounded sample: the same generator at 24^3 
 KERNEL_KINDS = [(0, "assemble"), (1, "panel"), (3, "gemm"), (12, "gemm_tcgen05"), (15, "pack_tcgen05"),
                 (10, "inverse_products"),
                 (11, "inverse_blocks"),
-                (18, "solve_reduce"), (19, "solve_gemm"), (20, "solve_assemble"), (21, "solve_gather"),
+                (19, "solve_gemm"), (20, "solve_assemble"),
                 (22, "solve_fwd_inverse"), (23, "solve_bwd_inverse"), (29, "solve_thin_fwd"),
                 (30, "solve_thin_bwd")]
 

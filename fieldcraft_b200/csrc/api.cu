@@ -43,7 +43,7 @@ int fail_status(fc_status *st, const Failure &f) {
 }
 
 enum Kind {
-  K_ASSEMBLE, K_PANEL, K_UNUSED_2, K_GEMM, K_SOLVE_ASSEMBLE, K_SOLVE_GATHER, K_SOLVE_FWD, K_SOLVE_BWD,
+  K_ASSEMBLE, K_PANEL, K_RETIRED_2, K_GEMM, K_SOLVE_ASSEMBLE, K_RETIRED_5, K_SOLVE_FWD, K_SOLVE_BWD,
   K_SOLVE_DAG_FWD, K_SOLVE_DAG_BWD,
   K_GEMM_MIXED,  // A in the factor's storage type, B and C FP64
   K_GEMM_F64,    // FP64 throughout (the diagonal blocks' inverses)
@@ -2013,7 +2013,6 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
       case K_SOLVE_ASSEMBLE:
         fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st);
         break;
-      case K_SOLVE_GATHER: fc::launch_solve_gather(t, b.x, b.v, b.voff, R, b.rows + l.off, l.count, st); break;
       case K_SOLVE_FWD:  // the diagonal blocks' inverses applied (FP64 throughout)
       case K_SOLVE_BWD: fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st, b.part, b.tcount); break;
       case K_GEMM:

@@ -970,22 +970,6 @@ __global__ void __launch_bounds__(THIN_THREADS) thin_bwd_kernel(Tree t, double *
   }
 }
 
-// v_s rows [i0, i1) <- x at the supernode's rows below its columns (final by the backward pass).
-__global__ void __launch_bounds__(256) solve_gather_kernel(Tree t, const double *__restrict__ x, double *__restrict__ v,
-                                                           const int64_t *__restrict__ voff, int R,
-                                                           const RowTask *__restrict__ tasks) {
-  const RowTask task = tasks[blockIdx.x];
-  const int s = task.s;
-  const int64_t w = t.width[s];
-  const int32_t *rows = t.rows + t.rows_off[s] + w;
-  double *vs = v + voff[s];
-  for (int64_t e = threadIdx.x; e < (int64_t)(task.i1 - task.i0) * R; e += blockDim.x) {
-    const int64_t i = task.i0 + e / R;
-    const int j = (int)(e % R);
-    vs[i * R + j] = x[(int64_t)rows[i] * R + j];
-  }
-}
-
 // x[i*R + j] = b[perm[i] + j*ld] (times scale[i] when scaled), and back.
 __global__ void permute_in_kernel(const int64_t *__restrict__ perm, int64_t n, const double *__restrict__ b,
                                   int64_t ld, double *__restrict__ x, int R, const double *__restrict__ scale) {
@@ -1301,11 +1285,6 @@ void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int 
     thin_bwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
   else
     thin_bwd_kernel<double><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
-}
-
-void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,
-                         int count, cudaStream_t st) {
-  if (count > 0) solve_gather_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks);
 }
 
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,

@@ -250,8 +250,6 @@ void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, doub
                      int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st);
 void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int R, int lg, const ThinBwdTask *tasks,
                      double *part, int32_t *counters, int count, cudaStream_t st);
-void launch_solve_gather(const Tree &t, const double *x, double *v, const int64_t *voff, int R,
-                         const RowTask *tasks, int count, cudaStream_t st);
 // x_post[i*R + j] = b[perm[i] + j*ld] (times scale[i] if given) and back.
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
                        const double *scale, cudaStream_t st);

@@ -192,7 +192,7 @@ int64_t fc_chol_trace_read(fc_chol *h, int64_t *out, int64_t cap);
  * invert and solve below a diagonal block), 3 GEMM of the factor, 10 and 11 the two GEMMs of a
  * doubling step of the diagonal-block inverses, 12 the tcgen05 GEMM of the mixed-precision factor
  * and 15 the packing of its operands;
- * 19 GEMM, 20 front assembly, 21 gather, 22 forward inverse, 23
+ * 19 GEMM, 20 front assembly, 22 forward inverse, 23
  * backward inverse of the solve (level by level), 24 forward, 25 backward persistent launch of the
  * solve, 29 forward, 30 backward step of the thin supernodes (32 covers all). */
 int fc_chol_profile(fc_chol *h, int enable);
