@@ -1173,13 +1173,14 @@ int read_status(fc_chol *h, fc_status *st) {
   return FC_OK;
 }
 
-// The solve's program for R right-hand sides (built once per R). Forward, level by level: each
-// supernode's front collects its children's update vectors, then panel by panel y = Linv x and the
-// rows below -= L y (x accumulates, y lands in x2). Backward, top level first: gather the final
-// values of the rows past the columns, own rows -= L21^T v, then panel by panel from the last
-// z = Linv^T x2 and the own rows above -= L^T z (x2 accumulates, z lands in x).
-// The solve's task lists for R right-hand sides: the update vectors' offsets (liveness-reused,
-// like the update matrices), then the tasks over given device vectors x, x2 (n x R each) and v.
+// The solve's program for R right-hand sides (built once per R). Forward, level by level: a thin
+// supernode is one launch of tiles (own rows, y = Dinv x, its update vector); a wide one's front
+// collects its children's update vectors, then per block of up to SB columns y = Dinv x and the
+// rows below -= L y (x accumulates, y lands in x2). Backward, top level first: thin supernodes by
+// chunks summing L21^T x; a wide one's own rows -= L21^T x(rows past its columns, read through
+// its row list), then per block from the last z = Dinv^T x2 and the own rows above -= L^T z (x2
+// accumulates, z lands in x). The task lists hold the update vectors' offsets (liveness-reused,
+// like the update matrices) and the tasks over given device vectors x, x2 (n x R each) and v.
 struct SolvePlan {
   std::vector<int64_t> voff;
   int64_t vsum = 0;

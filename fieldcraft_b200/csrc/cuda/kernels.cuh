@@ -18,7 +18,7 @@ constexpr int PANEL_ROWS = 128;  // rows of a panel solved by one CTA (64 at a t
 // its update matrix formed by the assembly itself instead of by a GEMM.
 constexpr int ASSEMBLE_COLS = 8, ASSEMBLE_ROWS = 256, ASSEMBLE_THREADS = 256, ASSEMBLE_THIN = 16;
 constexpr int ASSEMBLE_KIDS = 8;  // children whose ranges a tile keeps in shared memory (the rest: global)
-constexpr int SPLIT_K = 512;  // K chunk of a split GEMM (a long sum over few outputs)
+constexpr int SPLIT_K = 512;  // K chunk of the persistent solve's split products
 // The solve applies the inverse of a supernode's diagonal block SB columns at a time: the inverses
 // of its diagonal blocks of up to SB columns are formed during the factorisation (from the 64 x 64
 // inverses of the panels, by doubling), so a solve step is a GEMM over SB columns, not a chain of
