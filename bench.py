@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the B200 supernodal Cholesky: seconds to relative residual <= 1e-10 for the FP64
 direct solve of K u = f on a 48^3 hex8 block (345 744 free DOFs, per-element lognormal E, 64
-Gaussian top-face load cases), the workload BASELINE.json quotes its FP64-on-GPU metric on.
+Gaussian top-face load cases), the workload the headline FP64-on-GPU metric is quoted on.
 
 One step = the numeric factorisation of K (values already in HBM), the solve of the 64
 right-hand sides, and the residual check ||f - K u|| / ||f|| of every one of them on the device.

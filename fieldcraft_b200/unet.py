@@ -1,7 +1,7 @@
 """The learned preconditioner and flexible CG (include/fieldcraft_unet.h), for the same K u = f the
 Cholesky factor solves. No reference counterpart: the reference is a direct solver only
 (docs/linear-solvers.md:375-376). The Cholesky factor produces the training pairs (r, K^-1 r), is
-the fallback when FCG does not converge, and judges FCG's error.
+the fallback when FCG does not converge, and the reference against which FCG's error is measured.
 
 Device arrays are CUDA tensors (torch is only the allocator here); the network's forward and
 backward passes, Adam and FCG run on this library's kernels."""
