@@ -578,7 +578,7 @@ __device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)
 }
 
 template <class TA>
-__global__ void __launch_bounds__(GEMM_THREADS, 4) gemm_kernel(const GemmTask *__restrict__ tasks, double *part,
+__global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *__restrict__ tasks, double *part,
                                                                int32_t *counters) {
   constexpr int SA = tile_stride<TA>();
   extern __shared__ __align__(16) double gsm[];
