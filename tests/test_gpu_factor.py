@@ -4,7 +4,7 @@ the reference's API). Every case runs the CUDA kernels; FP64 throughout.
 Tolerances: the GPU computes each entry of L with a different operation order than the reference
 (blocked right-looking fronts, fused multiply-adds on the FP64 tensor pipe), so parity is to
 rounding: factor entries within 1e-11 of the largest entry, solutions within 1e-10 relative to the
-oracle's, and the reference's own residual bounds where it states them."""
+oracle's (the path's stated accuracy bar), and the reference's own residual bounds where it states them."""
 import ctypes as C
 
 import numpy as np
