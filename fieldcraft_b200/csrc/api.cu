@@ -2192,7 +2192,18 @@ int fc_symbolic_get(const fc_symbolic *sym, fc_symbolic_arrays *o) {
 }
 
 int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_status *status) {
-  if (!in || !out || in->n < 0 || in->ns < 0) {
+  bool args = in && out && in->n >= 0 && in->ns >= 0 && in->nnz >= 0 && in->rows_len >= 0 && in->lower_len >= 0 &&
+              in->updates_len >= 0 && in->tasks_len >= 0 && in->top_len >= 0;
+  if (args) {
+    // every array with a positive length has an address
+    auto has = [](const void *p, int64_t len) { return len == 0 || p != nullptr; };
+    args = has(in->perm, in->n) && in->first && in->rptr && has(in->rows, in->rows_len) && in->upper_ptr &&
+           has(in->upper_idx, in->nnz) && in->lptr && has(in->lidx, in->lower_len) && has(in->slot, in->nnz) &&
+           has(in->crow, in->nnz) && has(in->ccol, in->nnz) && in->uptr && has(in->uk, in->updates_len) &&
+           has(in->up1, in->updates_len) && has(in->up2, in->updates_len) && has(in->task_lo, in->tasks_len) &&
+           has(in->task_hi, in->tasks_len) && has(in->top, in->top_len);
+  }
+  if (!args) {
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null or negative argument");
     return FC_INVALID_ARGUMENT;
   }
@@ -2223,27 +2234,52 @@ int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_statu
     cp64(s.task_lo, in->task_lo, in->tasks_len);
     cp64(s.task_hi, in->task_hi, in->tasks_len);
     cp64(s.top, in->top, in->top_len);
-    // The supernodal tree from the structures: a supernode's parent holds its first row past
-    // its own columns.
-    bool ok = s.first.front() == 0 && s.first.back() == s.n && s.rptr.front() == 0 &&
-              s.rptr.back() == (int64_t)s.rows.size();
+    // Everything the device plan indexes with is checked here, so that no inconsistent array
+    // reaches an index on the host or the device. The supernodal tree follows from the
+    // structures: a supernode's parent holds its first row past its own columns.
+    const char *why = nullptr;
+    if (s.first.front() != 0 || s.first.back() != s.n || s.rptr.front() != 0 ||
+        s.rptr.back() != (int64_t)s.rows.size())
+      why = "supernodal structure: first/rptr do not span the columns and rows";
     std::vector<int64_t> snode(s.n, 0);
-    for (int64_t t = 0; ok && t < s.ns; ++t) {
-      if (s.first[t + 1] <= s.first[t] || s.rptr[t + 1] - s.rptr[t] < s.first[t + 1] - s.first[t]) ok = false;
-      for (int64_t j = s.first[t]; ok && j < s.first[t + 1]; ++j) snode[j] = t;
+    for (int64_t t = 0; !why && t < s.ns; ++t) {
+      if (s.first[t + 1] <= s.first[t] || s.rptr[t + 1] - s.rptr[t] < s.first[t + 1] - s.first[t])
+        why = "supernodal structure: a supernode narrower than zero or taller than its rows";
+      for (int64_t j = s.first[t]; !why && j < s.first[t + 1]; ++j) snode[j] = t;
     }
     s.sparent.assign(s.ns, fc::NONE);
-    for (int64_t t = 0; ok && t < s.ns; ++t) {
+    for (int64_t t = 0; !why && t < s.ns; ++t) {
       const int64_t w = s.width(t), m = s.height(t);
-      if (m > w) {
-        const int64_t r = s.rows[s.rptr[t] + w];
-        if (r < 0 || r >= s.n) ok = false;
-        else s.sparent[t] = snode[r];
+      const int32_t *r = s.rows.data() + s.rptr[t];
+      for (int64_t i = 0; !why && i < m; ++i) {
+        if (i < w ? r[i] != s.first[t] + i : (r[i] <= r[i - 1] || r[i] >= s.n))
+          why = "supernodal structure: a supernode's rows are not its columns followed by increasing rows below";
+      }
+      if (!why && m > w) {
+        s.sparent[t] = snode[r[w]];
+        if (s.sparent[t] <= t) why = "supernodal structure: a parent before its child";
       }
     }
-    if (!ok) {
+    if (!why) {
+      std::vector<char> seen(s.n, 0);
+      for (int64_t k = 0; !why && k < s.n; ++k) {
+        const int64_t c = s.perm[k];
+        if (c < 0 || c >= s.n || seen[c]) why = "perm is not a permutation";
+        else seen[c] = 1;
+      }
+    }
+    if (!why && (s.upper_ptr.front() != 0 || s.upper_ptr.back() != in->nnz))
+      why = "upper_ptr does not span the entries";
+    for (int64_t j = 0; !why && j < s.n; ++j)
+      if (s.upper_ptr[j + 1] < s.upper_ptr[j]) why = "upper_ptr decreases";
+    for (int64_t e = 0; !why && e < in->nnz; ++e) {
+      const int64_t r = s.crow[e], c = s.ccol[e], i = s.upper_idx[e];
+      if (r < 0 || r >= s.n || c < 0 || c > r || i < 0 || i >= s.n)
+        why = "an entry's coordinates outside the lower triangle";
+    }
+    if (why) {
       delete h;
-      set_status(status, FC_INTERNAL, -1, 0, 0, "supernodal structure: inconsistent arrays");
+      set_status(status, FC_INTERNAL, -1, 0, 0, why);
       return FC_INTERNAL;
     }
     *out = h;
@@ -2322,16 +2358,22 @@ int fc_chol_set_stream(fc_chol *h, void *stream) {
     h->stream = (cudaStream_t)stream;
     h->own_stream = false;
   } else if (!h->own_stream) {
-    cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    cudaStream_t own = nullptr;
+    if (cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking) != cudaSuccess) return FC_CUDA_ERROR;
+    h->stream = own;
     h->own_stream = true;
   }
   return FC_OK;
 }
 
 int fc_chol_factor(fc_chol *h, const double *upper_val, int64_t nnz, const volatile int32_t *cancel, fc_status *status) {
-  if (!h || (nnz > 0 && !upper_val) || nnz != h->nnz) {
+  if (!h || (nnz > 0 && !upper_val)) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null handle or values");
+    return FC_INVALID_ARGUMENT;
+  }
+  if (nnz != h->nnz) {
     set_status(status, FC_INTERNAL, -1, 0, 0, "supernodal factorization: the matrix's pattern differs from the analysed one");
-    return h ? FC_INTERNAL : FC_INVALID_ARGUMENT;
+    return FC_INTERNAL;
   }
   std::lock_guard<std::mutex> g(h->lock);
   cudaSetDevice(h->device);
@@ -2352,7 +2394,8 @@ int fc_chol_factor_device_async(fc_chol *h, const double *d_upper_val, int64_t n
   if (!h || nnz != h->nnz || (nnz > 0 && !d_upper_val)) return FC_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(h->lock);
   cudaSetDevice(h->device);
-  enqueue_factor(h, d_upper_val, nullptr);
+  const int rc = enqueue_factor(h, d_upper_val, nullptr);
+  if (rc != FC_OK) return rc;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
 }

@@ -82,7 +82,11 @@ typedef struct fc_symbolic_arrays {
 
 /* Views of the analysis' arrays (valid while sym lives). */
 int fc_symbolic_get(const fc_symbolic *sym, fc_symbolic_arrays *out);
-/* An analysis from a caller's arrays (copied); checked for consistency, FC_INTERNAL if not. */
+/* An analysis from a caller's arrays (copied). FC_INVALID_ARGUMENT for a negative length or a
+ * missing array; FC_INTERNAL (with the reason in the message) unless first/rptr span the columns
+ * and rows, each supernode's rows are its own columns followed by increasing rows below, perm is
+ * a permutation, upper_ptr spans the nnz entries, and every (crow, ccol) lies in the lower
+ * triangle. The update lists, tasks and top are copied for fc_symbolic_get only. */
 int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_status *status);
 
 /* ---- numeric factorisation on a B200 (replaces Factor::from_symbolic, cholesky.rs:1549-1554) ----

@@ -86,3 +86,78 @@ def test_import_round_trips_an_analysis():
     lib.fc_symbolic_get(h, C.byref(back))
     assert back.ns == arrays.ns and back.entries == arrays.entries
     lib.fc_symbolic_free(h)
+
+
+def _import_with(arrays, **changes):
+    """fc_symbolic_import of a copy of `arrays` with some arrays replaced; returns the status."""
+    import ctypes as C
+    lib = _lib.load()
+    a = _lib.SymbolicArrays()
+    C.pointer(a)[0] = arrays
+    keep = []
+    for name, (values, length) in changes.items():
+        dtype = np.int32 if name in ("rows", "upper_idx", "lidx", "crow", "ccol") else np.int64
+        v = np.ascontiguousarray(values, dtype)
+        keep.append(v)
+        setattr(a, name, v.ctypes.data_as(type(getattr(a, name))))
+        if length is not None:
+            setattr(a, length, int(v.size))
+    st = _lib.Status()
+    h = C.c_void_p()
+    rc = lib.fc_symbolic_import(C.byref(a), C.byref(h), C.byref(st))
+    if rc == 0:
+        lib.fc_symbolic_free(h)
+    return rc, st.message.decode()
+
+
+def test_import_refuses_inconsistent_arrays():
+    """Every array the device plan indexes with is checked before it is used: a corrupted copy
+    of a real analysis is refused with FC_INTERNAL and the reason, a negative length with
+    FC_INVALID_ARGUMENT, and the unchanged copy is accepted."""
+    import ctypes as C
+    up = UpperColumns.from_symmetric(H.panels_matrix())
+    s = Symbolic(up, 2**62)
+    lib = _lib.load()
+    arrays = _lib.SymbolicArrays()
+    assert lib.fc_symbolic_get(s.handle, C.byref(arrays)) == 0
+    a = s.arrays()
+    n, ns = a["n"], a["ns"]
+    assert ns > 2
+    assert _import_with(arrays)[0] == 0
+
+    perm = a["perm"].copy()
+    perm[1] = perm[0]
+    assert _import_with(arrays, perm=(perm, None)) == (5, "perm is not a permutation")
+
+    rows = a["rows"].copy()
+    t = next(t for t in range(ns) if a["rptr"][t + 1] - a["rptr"][t] > a["first"][t + 1] - a["first"][t] + 1)
+    below = a["rptr"][t] + a["first"][t + 1] - a["first"][t]
+    rows[below], rows[below + 1] = rows[below + 1], rows[below]
+    rc, msg = _import_with(arrays, rows=(rows, None))
+    assert rc == 5 and "increasing rows below" in msg
+    rows = a["rows"].copy()
+    rows[a["rptr"][t]] += 1  # a supernode's own column replaced
+    assert _import_with(arrays, rows=(rows, None))[0] == 5
+    rows = a["rows"].copy()
+    rows[a["rptr"][t + 1] - 1] = n  # a row past the matrix
+    assert _import_with(arrays, rows=(rows, None))[0] == 5
+
+    first = a["first"].copy()
+    first[-1] = n + 1
+    assert _import_with(arrays, first=(first, None))[0] == 5
+
+    crow, ccol = a["crow"].copy(), a["ccol"].copy()
+    e = int(np.flatnonzero(crow != ccol)[0])
+    crow[e], ccol[e] = ccol[e], crow[e]  # an entry above the diagonal
+    assert _import_with(arrays, crow=(crow, None), ccol=(ccol, None)) == \
+        (5, "an entry's coordinates outside the lower triangle")
+
+    upper_ptr = np.zeros(n + 1, np.int64)  # spans no entries
+    assert _import_with(arrays, upper_ptr=(upper_ptr, None)) == (5, "upper_ptr does not span the entries")
+
+    bad = _lib.SymbolicArrays()
+    C.pointer(bad)[0] = arrays
+    bad.rows_len = -1
+    st = _lib.Status()
+    h = C.c_void_p()
+    assert lib.fc_symbolic_import(C.byref(bad), C.byref(h), C.byref(st)) == 8  # FC_INVALID_ARGUMENT
