@@ -791,6 +791,11 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   double flops = 0;
   for (int64_t s = 0; s < ns; ++s) {
     const int64_t m = sym.height(s), w = sym.width(s), u = m - w;
+    if (m * w > INT32_MAX) {
+      // the assembly addresses a supernode's own panel with 32-bit offsets
+      set_status(st, FC_TOO_LARGE, -1, m * w, INT32_MAX, "a supernode's panel holds more than 2^31 - 1 entries");
+      return FC_TOO_LARGE;
+    }
     h->width[s] = (int32_t)w;
     h->height[s] = (int32_t)m;
     h->loff[s] = lsum;

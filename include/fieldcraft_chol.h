@@ -91,7 +91,9 @@ int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_statu
 
 /* ---- numeric factorisation on a B200 (replaces Factor::from_symbolic, cholesky.rs:1549-1554) ----
  * fc_chol_create uploads the structure and plans the level schedule on `device`; no values yet.
- * It copies what it needs: sym may be freed afterwards. */
+ * It copies what it needs: sym may be freed afterwards. FC_TOO_LARGE (entries = the panel's size,
+ * limit = 2^31 - 1) when one supernode's panel m x w holds more entries than 32-bit offsets
+ * address; FC_OUT_OF_MEMORY when the device arenas do not fit. */
 int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **out, fc_status *status);
 void fc_chol_destroy(fc_chol *h);
 /* Runs on this CUDA stream (cudaStream_t); NULL for the handle's own stream. */
