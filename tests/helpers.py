@@ -182,3 +182,67 @@ def band_matrix():
 def sin_solution(n: int) -> np.ndarray:
     """x_i = sin(0.37 i) (cholesky.rs:1676)."""
     return np.sin(np.arange(n, dtype=np.float64) * 0.37)
+
+
+def shifted_grid(n, sigma: float):
+    """A 3D grid Laplacian, 3 uncoupled unknowns per point, shifted by sigma, and the count of its
+    eigenvalues below sigma (crates/solver/src/ldlt.rs:594-635): rows built point by point, each
+    point's diagonal then its couplings to the next point along x, y and z."""
+    nx, ny, nz = n
+    point = lambda i, j, k: i + nx * (j + ny * k)  # noqa: E731
+    rows = [[] for _ in range(3 * nx * ny * nz)]
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                p = 3 * point(i, j, k)
+                for a in range(3):
+                    rows[p + a].append((p + a, 6.0 - sigma))
+                nxt = [point(i + 1, j, k) if i + 1 < nx else None, point(i, j + 1, k) if j + 1 < ny else None,
+                       point(i, j, k + 1) if k + 1 < nz else None]
+                for q in nxt:
+                    if q is None:
+                        continue
+                    for a in range(3):
+                        rows[p + a].append((3 * q + a, -1.0))
+                        rows[3 * q + a].append((p + a, -1.0))
+    axis = lambda m: [2.0 - 2.0 * np.cos(np.pi * t / (m + 1.0)) for t in range(1, m + 1)]  # noqa: E731
+    below = 3 * sum(1 for a in axis(nx) for b in axis(ny) for c in axis(nz) if a + b + c < sigma)
+    return rows_to_csr(rows), below
+
+
+def saddle(nk: int, nb: int) -> Csr:
+    """[[K, B], [B^T, 0]] in one dense supernode, the zero-diagonal columns first
+    (crates/solver/src/ldlt.rs:656-688)."""
+    n = nk + nb
+    rows = [[] for _ in range(n)]
+    for i in range(nk):
+        for j in range(nk):
+            rows[i].append((j, 0.5 if i == j else 0.05 / (1.0 + (i + j))))
+    for c in range(nb):
+        for i in range(nk):
+            v = float((i * 7 + c * 3) % 5) - 2.0 + (3.0 if i == c else 0.0)
+            rows[i].append((nk + c, v))
+            rows[nk + c].append((i, v))
+        for d in range(nb):
+            rows[nk + c].append((nk + d, 0.0))
+    order = list(range(nk, n)) + list(range(nk))
+    inverse = [order.index(i) for i in range(n)]
+    permuted = [None] * n
+    for i, row in enumerate(rows):
+        permuted[inverse[i]] = [(inverse[c], v) for c, v in row]
+    return rows_to_csr(permuted)
+
+
+def exact_solution(n: int) -> np.ndarray:
+    """x_i = ((37 i mod 101) - 50) / 50: exact in binary on every platform
+    (crates/solver/src/ldlt.rs:791-792)."""
+    i = np.arange(n, dtype=np.int64)
+    return ((i * 37 % 101).astype(np.float64) - 50.0) / 50.0
+
+
+def fingerprint(values) -> int:
+    """FNV-1a over the bit patterns of FP64 values (crates/solver/src/ldlt.rs:755-758)."""
+    h = 0xCBF29CE484222325
+    for b in np.ascontiguousarray(values, np.float64).view(np.uint64).tolist():
+        h = ((h ^ b) * 0x100000001B3) & MASK
+    return h

@@ -212,3 +212,15 @@ def test_the_matrix_is_copied_and_reordered_whole():
     for e in range(len(slot)):
         at = slot[e]
         assert lptr[ccol[e]] <= at < lptr[ccol[e] + 1] and lidx[at] == crow[e]
+
+
+def test_cholesky_solution_keeps_the_frozen_bits():
+    """crates/solver/src/ldlt.rs:774-849 (`f64_factors_keep_their_bits`, "shifted grid, definite"):
+    the reference froze the FNV-1a fingerprint of the Cholesky solution of the 5x5x5 grid shifted
+    by -0.5 for the exact right-hand side A x. The oracle's analysis, factor, solve and product
+    reproduce it bit for bit."""
+    a, below = H.shifted_grid([5, 5, 5], -0.5)
+    assert below == 0
+    _, f = factor(a)
+    b = oracle.spmv(a.n, a.ptr, a.idx, a.val, H.exact_solution(a.n))
+    assert H.fingerprint(f.solve(b.copy())) == 15069623423640047316
