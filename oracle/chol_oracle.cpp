@@ -1,16 +1,19 @@
-// ORACLE — test infrastructure, not product code. A CPU restatement of the reference's supernodal
-// Cholesky (crates/solver/src/cholesky.rs, FieldCraft 0.8.1) and of its sparse product
-// (crates/solver/src/sparse.rs:42-50), used only by the tests, by the smoke check and by the
-// benchmark's CPU-baseline leg as the checker and the timed CPU reference. Nothing in the
-// product links or calls it.
+// ORACLE — test infrastructure, not product code. A CPU restatement of the reference's
+// supernodal Cholesky (crates/solver/src/cholesky.rs, FieldCraft 0.8.1), of its symmetric
+// indefinite LDL^T on the same structure (crates/solver/src/ldlt.rs: bounded Bunch-Kaufman pivots
+// inside supernodes) and of its sparse product (crates/solver/src/sparse.rs:42-50), used only by
+// the tests, by the smoke check and by the benchmark's CPU-baseline leg as the checker and the
+// timed CPU reference. Nothing in the product links or calls it.
 //
 // It follows the reference's operation order entry by entry: sums over a supernode's columns
 // in column order from zero, updates subtracted in supernode order, panels of PANEL columns,
 // tiles of TILE rows, no fused multiply-add (built with -ffp-contract=off, no -ffast-math), so
 // each entry of the factor is the one the reference computes. The reference is Rust with
-// crates.io dependencies that are not present here, so it cannot be built to check this bit
-// for bit; the restatement is pinned instead by every known answer the reference's own tests
-// hold (see tests/test_oracle_pins.py, which cites each).
+// crates.io dependencies that are not present here, so it cannot be built; the restatement is
+// pinned by every known answer the reference's own tests hold, among them the FNV-1a
+// fingerprints the reference froze of the bits of its Cholesky solution and of four LDL^T
+// factors and solutions, which this code reproduces bit for bit (tests/test_oracle_pins.py,
+// tests/test_oracle_ldlt.py, which cite each).
 //
 // Threads: subtree tasks run concurrently and large dense kernels split their row tiles, as in
 // cholesky.rs:1443-1529 and :625-629; neither changes any entry's operations.
@@ -40,7 +43,15 @@ constexpr uint64_t PARALLEL_WORK = 1ull << 21;  // cholesky.rs:67
 constexpr uint64_t SUBTREE_SHARE = 256;         // cholesky.rs:97
 constexpr int GROUP = 6;                        // cholesky.rs:870
 
-enum Code : int32_t { OK = 0, NOT_POSITIVE_DEFINITE = 1, TOO_LARGE = 3, OUT_OF_MEMORY = 4, INTERNAL = 5, CANCELLED = 6 };
+enum Code : int32_t {
+  OK = 0, NOT_POSITIVE_DEFINITE = 1, SINGULAR = 2, TOO_LARGE = 3, OUT_OF_MEMORY = 4, INTERNAL = 5, CANCELLED = 6
+};
+
+// The pivots of an LDL^T factor's block diagonal D per column (cholesky.rs:447-457): a 1 x 1
+// pivot, or the first or second column of a 2 x 2 one.
+enum PivotKind : int8_t { PIVOT_ONE = 0, PIVOT_FIRST = 1, PIVOT_SECOND = 2 };
+constexpr double ALPHA = 0.6403882032022076;  // ldlt.rs:77: (1 + sqrt 17) / 8
+constexpr int ROOK_STEPS = 64;                // ldlt.rs:81
 
 struct Error {
   Code code;
@@ -277,6 +288,9 @@ struct or_factor {
   std::vector<std::vector<double>> values;
 };
 
+struct LdltBlock;
+struct or_ldlt;
+
 namespace {
 
 // Symbolic::new (cholesky.rs:1212-1378).
@@ -427,16 +441,37 @@ struct PanelRef {
   }
 };
 
+// times_d (cholesky.rs:458-481): row <- row D, with D the block diagonal the trapezoid holds
+// for its columns k0.. and `pivots` their pivots from k0.
+void times_d(double *row, int64_t len, const PanelRef &l, int64_t k0, const int8_t *pivots) {
+  int64_t k = 0;
+  while (k < len) {
+    if (pivots[k] == PIVOT_FIRST) {
+      const double a = row[k], b = k + 1 < len ? row[k + 1] : 0.0;
+      const double d11 = l.at(k0 + k, k0 + k), d21 = l.at(k0 + k + 1, k0 + k), d22 = l.at(k0 + k + 1, k0 + k + 1);
+      row[k] = a * d11 + b * d21;
+      if (k + 1 < len) row[k + 1] = a * d21 + b * d22;
+      k += 2;
+    } else {
+      row[k] *= l.at(k0 + k, k0 + k);
+      k += 1;
+    }
+  }
+}
+
 // products (cholesky.rs:531-630) with the reference's packing and micro-tiles (MR x NR, two
-// columns a pass); tiles[t][c * TILE + i]. Returns false on a tile outside the panel.
+// columns a pass); tiles[t][c * TILE + i]. Y is L, or L D when `pivots` (of the columns k0..)
+// are given. Returns false on a tile outside the panel.
 bool products_tiled(const PanelRef &l, int64_t k0, int64_t kw, int64_t p, int64_t mu, int64_t wu,
-                    std::vector<std::vector<double>> &tiles) {
+                    std::vector<std::vector<double>> &tiles, const int8_t *pivots = nullptr) {
   std::vector<double> yt(wu * kw, 0.0);
   for (int64_t k = 0; k < kw; ++k) {
     const double *col = l.column(k0 + k, p, wu);
     if (!col) return false;
     for (int64_t c = 0; c < wu; ++c) yt[c * kw + k] = col[c];
   }
+  if (pivots && kw > 0)
+    for (int64_t c = 0; c < wu; ++c) times_d(&yt[c * kw], kw, l, k0, pivots);
   int64_t nb = (wu + NR - 1) / NR;
   std::vector<double> yp(nb * kw * NR, 0.0);
   for (int64_t c = 0; c < wu; ++c)
@@ -579,14 +614,16 @@ struct Lower {
   std::vector<double> val, diag, scale;
 };
 
-// Context::supernode (cholesky.rs:1047-1188): assemble, then panels.
-Error supernode(const or_sym &s, const Lower &a, int64_t j, std::vector<std::vector<double>> &values) {
+// Context::assemble (cholesky.rs:1044-1125): supernode j's columns of A, then minus the
+// product L_K Y_K^T of every descendant K that reaches it, in supernode order (Y = L, or L D when
+// `pivots_of(k)` is not null). `values_of(k)` is descendant k's trapezoid.
+template <class ValuesOf, class PivotsOf>
+Error assemble(const or_sym &s, const Lower &a, int64_t j, double *own, int64_t own_size, ValuesOf values_of,
+               PivotsOf pivots_of) {
   const int32_t *rows = s.rows_of(j);
   int64_t m = s.height(j), w = s.width(j), f = s.first[j];
-  std::vector<double> &ownv = values[j];
-  double *own = ownv.data();
-  int64_t own_size = (int64_t)ownv.size();
-  std::fill(ownv.begin(), ownv.end(), 0.0);
+  if (own_size != trapezoid_size(m, w)) return {INTERNAL, -1};
+  std::fill(own, own + own_size, 0.0);
   for (int64_t c = 0; c < w; ++c)
     for (int64_t p = s.pattern.ptr[f + c]; p < s.pattern.ptr[f + c + 1]; ++p) {
       int32_t r = s.pattern.idx[p];
@@ -609,10 +646,25 @@ Error supernode(const or_sym &s, const Lower &a, int64_t j, std::vector<std::vec
       if (at >= m || rows[at] != kr[i]) return {INTERNAL, -1};
       relative.push_back(at);
     }
-    PanelRef lk{km, values[u.k].data(), (int64_t)values[u.k].size()};
-    if (!products_tiled(lk, 0, kw, u.p1, mu, wu, tiles)) return {INTERNAL, -1};
+    const std::vector<double> &vk = values_of(u.k);
+    PanelRef lk{km, vk.data(), (int64_t)vk.size()};
+    if (!products_tiled(lk, 0, kw, u.p1, mu, wu, tiles, pivots_of(u.k))) return {INTERNAL, -1};
     if (!subtract(own, own_size, m, tiles, mu, wu, [&](int64_t i) { return relative[i]; })) return {INTERNAL, -1};
   }
+  return {OK, -1};
+}
+
+// Context::supernode (cholesky.rs:1131-1188): assemble, then panels.
+Error supernode(const or_sym &s, const Lower &a, int64_t j, std::vector<std::vector<double>> &values) {
+  int64_t m = s.height(j), w = s.width(j), f = s.first[j];
+  std::vector<double> &ownv = values[j];
+  double *own = ownv.data();
+  int64_t own_size = (int64_t)ownv.size();
+  Error assembled = assemble(
+      s, a, j, own, own_size, [&](int64_t k) -> const std::vector<double> & { return values[k]; },
+      [](int64_t) -> const int8_t * { return nullptr; });
+  if (assembled.code != OK) return assembled;
+  std::vector<std::vector<double>> tiles;
   for (int64_t c0 = 0; c0 < w; c0 += PANEL) {
     int64_t c1 = std::min(c0 + PANEL, w), pw = c1 - c0;
     if (c0 > 0) {
@@ -652,7 +704,8 @@ Error supernode(const or_sym &s, const Lower &a, int64_t j, std::vector<std::vec
 // Symbolic::factor (cholesky.rs:1443-1529): subtree tasks concurrently, each in order, then
 // the supernodes above them in order; the earliest failing column in postorder is reported,
 // named by its original column.
-Error factor(const or_sym &s, const Lower &a, std::vector<std::vector<double>> &values, const volatile int32_t *cancel) {
+template <class Supernode>
+Error factor(const or_sym &s, const volatile int32_t *cancel, Supernode supernode) {
   int64_t ntasks = (int64_t)s.task_lo.size();
   std::vector<Error> failed(ntasks, Error{OK, -1});
   std::mutex broken_lock;
@@ -665,8 +718,8 @@ Error factor(const or_sym &s, const Lower &a, std::vector<std::vector<double>> &
         if (broken.code == OK) broken = {CANCELLED, -1};
         break;
       }
-      Error e = supernode(s, a, j, values);
-      if (e.code == NOT_POSITIVE_DEFINITE) {
+      Error e = supernode(j);
+      if (e.code == NOT_POSITIVE_DEFINITE || e.code == SINGULAR) {
         failed[t] = e;
         break;
       }
@@ -682,13 +735,13 @@ Error factor(const or_sym &s, const Lower &a, std::vector<std::vector<double>> &
   for (auto &e : failed)
     if (e.code != OK && (earliest.code == OK || e.column < earliest.column)) earliest = e;
   auto named = [&](Error e) {
-    if (e.code == NOT_POSITIVE_DEFINITE) e.column = s.perm[e.column];
+    if (e.code == NOT_POSITIVE_DEFINITE || e.code == SINGULAR) e.column = s.perm[e.column];
     return e;
   };
   for (int64_t j : s.top) {
     if (cancelled()) return {CANCELLED, -1};
     if (earliest.code != OK && s.first[j] > earliest.column) break;
-    Error e = supernode(s, a, j, values);
+    Error e = supernode(j);
     if (e.code != OK) return named(e);
   }
   if (earliest.code != OK) return named(earliest);
@@ -743,6 +796,299 @@ void solve_group(const or_factor &fac, double *x, int kk) {
       double d = t[offset(m, q)];
       for (int j = 0; j < kk; ++j) own[q * kk + j] = sum[j] / d;
     }
+  }
+}
+
+// ---- symmetric indefinite LDL^T (ldlt.rs) --------------------------------------------------
+// The same supernodes, tasks and products as the Cholesky factor; inside a supernode, pivots
+// chosen by the bounded Bunch-Kaufman (rook) search among the supernode's own columns.
+
+// One supernode of an LDL^T factor (ldlt.rs:88-98): L below the pivots and D on them in the lower
+// trapezoid by columns in pivot order; order[c] is the own column (symbolic order) at pivot c.
+}  // namespace
+
+struct LdltBlock {
+  std::vector<double> values;
+  std::vector<int8_t> pivots;
+  std::vector<int64_t> order;
+  int64_t two_by_two = 0;
+};
+
+struct or_ldlt {
+  const or_sym *sym = nullptr;
+  std::vector<LdltBlock> blocks;
+};
+
+namespace {
+
+// interchange (ldlt.rs:128-143): symmetric interchange of local columns p < q of an m-row lower
+// trapezoid: the rows of the columns before p, the diagonals, the strip between them and the
+// rows below q.
+void interchange(std::vector<double> &v, int64_t m, int64_t p, int64_t q) {
+  auto at = [m](int64_t r, int64_t c) { return offset(m, c) + r - c; };
+  for (int64_t c = 0; c < p; ++c) std::swap(v[at(p, c)], v[at(q, c)]);
+  std::swap(v[at(p, p)], v[at(q, q)]);
+  for (int64_t c = p + 1; c < q; ++c) std::swap(v[at(c, p)], v[at(q, c)]);
+  for (int64_t r = q + 1; r < m; ++r) std::swap(v[at(r, p)], v[at(r, q)]);
+}
+
+// largest (ldlt.rs:145-163): the largest magnitude of v over [lo, hi) except `skip`, with the
+// lowest such index; NaN at the first entry that is not a number.
+std::pair<int64_t, double> largest(const std::vector<double> &v, int64_t lo, int64_t hi, int64_t skip) {
+  std::pair<int64_t, double> best{lo, 0.0};
+  for (int64_t i = lo; i < hi; ++i) {
+    if (i == skip) continue;
+    const double x = i < (int64_t)v.size() ? std::fabs(v[i]) : 0.0;
+    if (std::isnan(x)) return {i, x};
+    if (x > best.second) best = {i, x};
+  }
+  return best;
+}
+
+struct LdltScratch {
+  std::vector<double> a, b, w;  // the searched column, a candidate, a row of L D (ldlt.rs:165-172)
+};
+
+// Block::current (ldlt.rs:173-192): column c (local, >= k) of the part still to factor, rows
+// k..m, into out: the trapezoid's entries less the products with the panel's factored columns
+// c0..k, whose L D row is formed from L and D.
+void ldlt_current(const LdltBlock &b, int64_t m, int64_t c0, int64_t k, int64_t c, std::vector<double> &out,
+                  std::vector<double> &w) {
+  const PanelRef t{m, b.values.data(), (int64_t)b.values.size()};
+  for (int64_t r = k; r < m; ++r) out[r] = r >= c ? t.at(r, c) : t.at(c, r);
+  w.clear();
+  for (int64_t q = c0; q < k; ++q) w.push_back(t.at(c, q));
+  if (!w.empty()) times_d(w.data(), (int64_t)w.size(), t, c0, b.pivots.data() + c0);
+  for (int64_t q = c0; q < k; ++q) {
+    const double wq = w[q - c0];
+    const double *l = t.column(q, k, m - k);
+    for (int64_t r = 0; r < m - k; ++r) out[k + r] -= l[r] * wq;
+  }
+}
+
+// Block::swap (ldlt.rs:194-204): local columns p and q (pivot positions >= k) in the trapezoid,
+// the order and the current columns.
+void ldlt_swap(LdltBlock &b, int64_t m, int64_t p, int64_t q, LdltScratch &sc) {
+  if (p == q) return;
+  if (p > q) std::swap(p, q);
+  interchange(b.values, m, p, q);
+  std::swap(b.order[p], b.order[q]);
+  std::swap(sc.a[p], sc.a[q]);
+  std::swap(sc.b[p], sc.b[q]);
+}
+
+// Block::one (ldlt.rs:206-221): a 1 x 1 pivot at k from the current column.
+void ldlt_one(LdltBlock &b, int64_t m, int64_t k, const std::vector<double> &col) {
+  const double d = col[k];
+  const int64_t start = offset(m, k);
+  b.values[start] = d;
+  for (int64_t r = k + 1; r < m; ++r) b.values[start + r - k] = col[r] / d;
+  b.pivots[k] = PIVOT_ONE;
+}
+
+// Block::two (ldlt.rs:223-248): a 2 x 2 pivot at k, k + 1 from the current columns a (k) and
+// b (k + 1).
+void ldlt_two(LdltBlock &blk, int64_t m, int64_t k, const std::vector<double> &a, const std::vector<double> &b) {
+  const double d11 = a[k], d21 = a[k + 1], d22 = b[k + 1];
+  const double det = d11 * d22 - d21 * d21;
+  const int64_t s0 = offset(m, k), s1 = offset(m, k + 1);
+  blk.values[s0] = d11;
+  blk.values[s0 + 1] = d21;
+  blk.values[s1] = d22;
+  for (int64_t r = k + 2; r < m; ++r) {
+    const double x = a[r], y = b[r];
+    blk.values[s0 + r - k] = (x * d22 - y * d21) / det;
+    blk.values[s1 + r - k - 1] = (y * d11 - x * d21) / det;
+  }
+  blk.pivots[k] = PIVOT_FIRST;
+  blk.pivots[k + 1] = PIVOT_SECOND;
+  blk.two_by_two += 1;
+}
+
+// Block::panel (ldlt.rs:250-335): the panel from column c0 of a supernode with m rows and w
+// columns whose first column is f (postorder), pivots chosen among the columns c0..w by the rook
+// search, each column brought up to date with the panel's columns before it. `end` receives
+// where the panel ended (one column past c0 + PANEL after a closing 2 x 2 pivot).
+Error ldlt_panel(LdltBlock &blk, int64_t m, int64_t w, int64_t c0, int64_t f, const Lower &lower, LdltScratch &sc,
+                 int64_t &end_out) {
+  const int64_t end = std::min(c0 + PANEL, w);
+  auto scale = [&](int64_t at) { return lower.scale[f + blk.order[at]]; };
+  auto singular = [&](int64_t at) { return Error{SINGULAR, f + blk.order[at]}; };
+  int64_t k = c0;
+  while (k < end) {
+    ldlt_current(blk, m, c0, k, k, sc.a, sc.w);
+    const double akk = std::fabs(sc.a[k]);
+    const auto first = largest(sc.a, k + 1, w, NONE);
+    const int64_t r0 = first.first;
+    const double omega_k = first.second;
+    if (!std::isfinite(akk) || !std::isfinite(omega_k)) return singular(k);
+    bool two = false;
+    int64_t p = k, pi = k, pr = k;
+    if (akk >= ALPHA * omega_k) {
+      p = k;
+    } else {
+      // the rook search: `a` holds column i, `b` the candidate r
+      int64_t i = k, r = r0;
+      double omega_i = omega_k;
+      int step = 0;
+      for (;;) {
+        ldlt_current(blk, m, c0, k, r, sc.b, sc.w);
+        const auto next = largest(sc.b, k, w, r);
+        const double omega_r = next.second, arr = std::fabs(sc.b[r]);
+        if (!std::isfinite(arr) || !std::isfinite(omega_r)) return singular(k);
+        step += 1;
+        if (arr >= ALPHA * omega_r) {
+          std::swap(sc.a, sc.b);
+          p = r;
+          break;
+        }
+        if (omega_r <= omega_i || step >= ROOK_STEPS) {
+          two = true;
+          pi = i;
+          pr = r;
+          break;
+        }
+        std::swap(sc.a, sc.b);
+        i = r;
+        omega_i = omega_r;
+        r = next.first;
+      }
+    }
+    if (!two) {
+      ldlt_swap(blk, m, k, p, sc);
+      if (!(std::fabs(sc.a[k]) > PIVOT_TOLERANCE * scale(k))) return singular(k);
+      ldlt_one(blk, m, k, sc.a);
+      k += 1;
+    } else {
+      // i to k, then r to k + 1 (r was at k if i took its place)
+      ldlt_swap(blk, m, k, pi, sc);
+      ldlt_swap(blk, m, k + 1, pr == k ? pi : pr, sc);
+      const double offdiagonal = std::fabs(sc.a[k + 1]);
+      const double size = std::max(scale(k), scale(k + 1));
+      if (!(offdiagonal > PIVOT_TOLERANCE * size)) return singular(k);
+      ldlt_two(blk, m, k, sc.a, sc.b);
+      k += 2;
+    }
+  }
+  end_out = k;
+  return {OK, -1};
+}
+
+// supernode (ldlt.rs:337-363): assemble with the descendants' L D, then panels; after each
+// panel the rest of the supernode minus the panel's L D L^T by the tiled products.
+Error ldlt_supernode(const or_sym &s, const Lower &a, int64_t j, std::vector<LdltBlock> &blocks) {
+  const int64_t m = s.height(j), w = s.width(j), f = s.first[j];
+  LdltBlock &own = blocks[j];
+  Error assembled = assemble(
+      s, a, j, own.values.data(), (int64_t)own.values.size(),
+      [&](int64_t k) -> const std::vector<double> & { return blocks[k].values; },
+      [&](int64_t k) -> const int8_t * { return blocks[k].pivots.data(); });
+  if (assembled.code != OK) return assembled;
+  own.pivots.assign(w, PIVOT_ONE);
+  own.order.resize(w);
+  for (int64_t c = 0; c < w; ++c) own.order[c] = c;
+  own.two_by_two = 0;
+  LdltScratch sc;
+  sc.a.assign(m, 0.0);
+  sc.b.assign(m, 0.0);
+  std::vector<std::vector<double>> tiles;
+  int64_t c0 = 0;
+  while (c0 < w) {
+    int64_t c1 = c0;
+    Error e = ldlt_panel(own, m, w, c0, f, a, sc, c1);
+    if (e.code != OK) return e;
+    if (c1 < w) {
+      const PanelRef l{m, own.values.data(), (int64_t)own.values.size()};
+      if (!products_tiled(l, c0, c1 - c0, c1, m - c1, w - c1, tiles, own.pivots.data() + c0)) return {INTERNAL, -1};
+      if (!subtract(own.values.data(), (int64_t)own.values.size(), m, tiles, m - c1, w - c1,
+                    [&](int64_t i) { return c1 + i; }))
+        return {INTERNAL, -1};
+    }
+    c0 = c1;
+  }
+  return {OK, -1};
+}
+
+// solve_group with LDL^T's unit L, block diagonal D and pivot order (cholesky.rs:904-1037), `kk`
+// right-hand sides interleaved: L z = P b and D^-1 by supernodes, each supernode's own unknowns
+// left in pivot order for the backward pass; then L^T x = z in reverse, each supernode
+// scattering its unknowns back from pivot order.
+void ldlt_solve_group(const or_sym &s, const std::vector<LdltBlock> &blocks, double *x, int kk) {
+  std::vector<double> y;
+  for (int64_t k = 0; k < s.ns; ++k) {
+    const int32_t *rows = s.rows_of(k);
+    const int64_t m = s.height(k), f = s.first[k], w = s.width(k);
+    const LdltBlock &blk = blocks[k];
+    const PanelRef t{m, blk.values.data(), (int64_t)blk.values.size()};
+    double *own = x + f * kk;
+    y.assign(w * kk, 0.0);
+    for (int64_t c = 0; c < w; ++c)
+      for (int j = 0; j < kk; ++j) y[c * kk + j] = own[blk.order[c] * kk + j];
+    for (int64_t q = 0; q < w; ++q) {
+      const int64_t end = q + (blk.pivots[q] == PIVOT_FIRST ? 2 : 1);
+      double yq[GROUP];
+      for (int j = 0; j < kk; ++j) yq[j] = y[q * kk + j];
+      for (int64_t r = end; r < w; ++r) {
+        const double l = t.at(r, q);
+        for (int j = 0; j < kk; ++j) y[r * kk + j] -= l * yq[j];
+      }
+      for (int64_t r = w; r < m; ++r) {
+        const double l = t.at(r, q);
+        double *v = x + (int64_t)rows[r] * kk;
+        for (int j = 0; j < kk; ++j) v[j] -= l * yq[j];
+      }
+    }
+    int64_t c = 0;
+    while (c < w) {
+      if (blk.pivots[c] == PIVOT_FIRST) {
+        const double d11 = t.at(c, c), d21 = t.at(c + 1, c), d22 = t.at(c + 1, c + 1);
+        const double det = d11 * d22 - d21 * d21;
+        for (int j = 0; j < kk; ++j) {
+          const double p = y[c * kk + j], q = y[(c + 1) * kk + j];
+          y[c * kk + j] = (d22 * p - d21 * q) / det;
+          y[(c + 1) * kk + j] = (d11 * q - d21 * p) / det;
+        }
+        c += 2;
+      } else {
+        const double d = t.at(c, c);
+        for (int j = 0; j < kk; ++j) y[c * kk + j] /= d;
+        c += 1;
+      }
+    }
+    std::memcpy(own, y.data(), sizeof(double) * w * kk);
+  }
+  for (int64_t k = s.ns - 1; k >= 0; --k) {
+    const int32_t *rows = s.rows_of(k);
+    const int64_t m = s.height(k), f = s.first[k], w = s.width(k);
+    const LdltBlock &blk = blocks[k];
+    const PanelRef t{m, blk.values.data(), (int64_t)blk.values.size()};
+    double *own = x + f * kk;
+    y.assign(own, own + w * kk);
+    for (int64_t c = w - 1; c >= 0; --c) {
+      // reverse pivot groups, ascending columns within each 2 x 2 group
+      int64_t q = c, end = c + 1;
+      if (blk.pivots[c] == PIVOT_SECOND && c > 0) {
+        q = c - 1;
+        end = c + 1;
+      } else if (blk.pivots[c] == PIVOT_FIRST) {
+        q = c + 1;
+        end = c + 2;
+      }
+      double sum[GROUP];
+      for (int j = 0; j < kk; ++j) sum[j] = y[q * kk + j];
+      for (int64_t r = end; r < w; ++r) {
+        const double l = t.at(r, q);
+        for (int j = 0; j < kk; ++j) sum[j] -= l * y[r * kk + j];
+      }
+      for (int64_t r = w; r < m; ++r) {
+        const double l = t.at(r, q);
+        const double *v = x + (int64_t)rows[r] * kk;
+        for (int j = 0; j < kk; ++j) sum[j] -= l * v[j];
+      }
+      for (int j = 0; j < kk; ++j) y[q * kk + j] = sum[j];
+    }
+    for (int64_t pos = 0; pos < w; ++pos)
+      for (int j = 0; j < kk; ++j) own[blk.order[pos] * kk + j] = y[pos * kk + j];
   }
 }
 
@@ -902,29 +1248,36 @@ int or_postorder(int64_t n, const int64_t *parent, int64_t *post) {
   return (int)q.size() == n ? 0 : -1;
 }
 
+// Symbolic::numeric (cholesky.rs:1392-1416): the values in postorder, the diagonal and the
+// largest magnitude of each row (= column) of the symmetric matrix.
+static Lower lower_of(const or_sym *s, const double *upper_val) {
+  Lower a;
+  const Pattern &p = s->pattern;
+  a.val.assign(p.idx.size(), 0.0);
+  a.diag.assign(s->n, 0.0);
+  a.scale.assign(s->n, 0.0);
+  for (size_t e = 0; e < p.slot.size(); ++e) {
+    double v = upper_val[e];
+    a.val[p.slot[e]] = v;
+    int64_t r = p.crow[e], c = p.ccol[e];
+    if (r == c) a.diag[c] = v;
+    a.scale[r] = std::max(a.scale[r], std::fabs(v));
+    a.scale[c] = std::max(a.scale[c], std::fabs(v));
+  }
+  return a;
+}
+
 // Symbolic::numeric + allocate + factor. column_out receives the failing original column.
 int or_factor_new(const or_sym *s, const double *upper_val, const int32_t *cancel, or_factor **out, int64_t *column_out) {
   *out = nullptr;
   *column_out = -1;
   try {
-    Lower a;
-    const Pattern &p = s->pattern;
-    a.val.assign(p.idx.size(), 0.0);
-    a.diag.assign(s->n, 0.0);
-    a.scale.assign(s->n, 0.0);
-    for (size_t e = 0; e < p.slot.size(); ++e) {
-      double v = upper_val[e];
-      a.val[p.slot[e]] = v;
-      int64_t r = p.crow[e], c = p.ccol[e];
-      if (r == c) a.diag[c] = v;
-      a.scale[r] = std::max(a.scale[r], std::fabs(v));
-      a.scale[c] = std::max(a.scale[c], std::fabs(v));
-    }
+    Lower a = lower_of(s, upper_val);
     auto f = new or_factor();
     f->sym = s;
     f->values.resize(s->ns);
     for (int64_t j = 0; j < s->ns; ++j) f->values[j].assign(trapezoid_size(s->height(j), s->width(j)), 0.0);
-    Error e = factor(*s, a, f->values, cancel);
+    Error e = factor(*s, cancel, [&](int64_t j) { return supernode(*s, a, j, f->values); });
     if (e.code != OK) {
       *column_out = e.column;
       delete f;
@@ -1003,6 +1356,107 @@ int or_subtract(double *own, int64_t own_size, int64_t m, const double *tiles_fl
     at += cols * TILE;
   }
   return subtract(own, own_size, m, tiles, mu, wu, [&](int64_t i) { return rel[i]; }) ? 0 : -1;
+}
+
+// LdltFactor::from_symbolic (ldlt.rs:378-392): numeric + allocate + factor with pivoting.
+// column_out receives the failing original column (SINGULAR).
+int or_ldlt_new(const or_sym *s, const double *upper_val, const int32_t *cancel, or_ldlt **out, int64_t *column_out) {
+  *out = nullptr;
+  *column_out = -1;
+  try {
+    Lower a = lower_of(s, upper_val);
+    auto f = new or_ldlt();
+    f->sym = s;
+    f->blocks.resize(s->ns);
+    for (int64_t j = 0; j < s->ns; ++j) f->blocks[j].values.assign(trapezoid_size(s->height(j), s->width(j)), 0.0);
+    Error e = factor(*s, cancel, [&](int64_t j) { return ldlt_supernode(*s, a, j, f->blocks); });
+    if (e.code != OK) {
+      *column_out = e.column;
+      delete f;
+      return e.code;
+    }
+    *out = f;
+    return OK;
+  } catch (const std::bad_alloc &) {
+    return OUT_OF_MEMORY;
+  }
+}
+
+void or_ldlt_free(or_ldlt *f) { delete f; }
+
+// The factor's values (L below the pivots, D on them), supernode by supernode.
+int64_t or_ldlt_values(const or_ldlt *f, double *dst) {
+  int64_t at = 0;
+  for (auto &b : f->blocks) {
+    if (dst) std::memcpy(dst + at, b.values.data(), sizeof(double) * b.values.size());
+    at += (int64_t)b.values.size();
+  }
+  return at;
+}
+
+// Every supernode's pivots (0 one, 1 first, 2 second of a 2 x 2) and local order, end to end in
+// postorder (n entries each).
+void or_ldlt_pivots(const or_ldlt *f, int64_t *pivots, int64_t *order) {
+  int64_t at = 0;
+  for (auto &b : f->blocks) {
+    for (size_t c = 0; c < b.pivots.size(); ++c) {
+      pivots[at + (int64_t)c] = b.pivots[c];
+      order[at + (int64_t)c] = b.order[c];
+    }
+    at += (int64_t)b.pivots.size();
+  }
+}
+
+// 0: the 2 x 2 pivots; 1, 2: the positive and negative eigenvalue counts (Sylvester's law on D,
+// ldlt.rs:415-447).
+int64_t or_ldlt_info(const or_ldlt *f, int what) {
+  int64_t two = 0, positive = 0, negative = 0;
+  const or_sym &s = *f->sym;
+  for (int64_t k = 0; k < s.ns; ++k) {
+    const LdltBlock &b = f->blocks[k];
+    two += b.two_by_two;
+    const PanelRef t{s.height(k), b.values.data(), (int64_t)b.values.size()};
+    int64_t c = 0;
+    while (c < (int64_t)b.pivots.size()) {
+      if (b.pivots[c] == PIVOT_FIRST) {
+        const double d11 = t.at(c, c), d21 = t.at(c + 1, c), d22 = t.at(c + 1, c + 1);
+        const double det = d11 * d22 - d21 * d21;
+        if (det < 0.0) {
+          positive += 1;
+          negative += 1;
+        } else if (d11 + d22 > 0.0) {
+          positive += 2;
+        } else {
+          negative += 2;
+        }
+        c += 2;
+      } else {
+        if (t.at(c, c) > 0.0)
+          positive += 1;
+        else
+          negative += 1;
+        c += 1;
+      }
+    }
+  }
+  return what == 0 ? two : what == 1 ? positive : negative;
+}
+
+// LdltFactor::solve_many (ldlt.rs:404-413): b column-major n x nrhs (ld = n), in place, by
+// groups of GROUP.
+int or_ldlt_solve(const or_ldlt *f, double *b, int64_t nrhs) {
+  const or_sym &s = *f->sym;
+  const int64_t n = s.n;
+  std::vector<double> x(n * GROUP);
+  for (int64_t g0 = 0; g0 < nrhs; g0 += GROUP) {
+    int kk = (int)std::min<int64_t>(GROUP, nrhs - g0);
+    for (int64_t i = 0; i < n; ++i)
+      for (int j = 0; j < kk; ++j) x[i * kk + j] = b[(g0 + j) * n + s.perm[i]];
+    ldlt_solve_group(s, f->blocks, x.data(), kk);
+    for (int64_t i = 0; i < n; ++i)
+      for (int j = 0; j < kk; ++j) b[(g0 + j) * n + s.perm[i]] = x[i * kk + j];
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -1,6 +1,6 @@
 """ORACLE (test infrastructure): ctypes access to ``liboracle.so``, the CPU restatement of the
-reference's supernodal Cholesky (chol_oracle.cpp). Used only by the tests, by the smoke check and
-by the benchmark's CPU-baseline leg, as the checker and the timed CPU reference."""
+reference's supernodal Cholesky and LDL^T (chol_oracle.cpp). Used only by the tests, by the smoke
+check and by the benchmark's CPU-baseline leg, as the checker and the timed CPU reference."""
 from __future__ import annotations
 
 import ctypes as C
@@ -31,6 +31,12 @@ _SIG = {
     "or_spmv": (None, [i64, P, P, P, P, P]),
     "or_products": (i64, [i64, P, i64, i64, i64, i64, i64, i64, C.c_int, P]),
     "or_subtract": (C.c_int, [P, i64, i64, P, i64, i64, P]),
+    "or_ldlt_new": (C.c_int, [P, P, P, C.POINTER(P), P]),
+    "or_ldlt_free": (None, [P]),
+    "or_ldlt_values": (i64, [P, P]),
+    "or_ldlt_pivots": (None, [P, P, P]),
+    "or_ldlt_info": (i64, [P, C.c_int]),
+    "or_ldlt_solve": (C.c_int, [P, P, i64]),
 }
 _lib = None
 
@@ -135,6 +141,76 @@ class Fac:
         if getattr(self, "h", None):
             load().or_factor_free(self.h)
             self.h = None
+
+
+class Ldlt:
+    """The symmetric indefinite factor P A P^T = L D L^T on an analysis (ldlt.rs LdltFactor):
+    bounded Bunch-Kaufman pivots inside supernodes."""
+
+    def __init__(self, sym: Sym, upper_val, cancel=None):
+        self.sym = sym
+        v = np.ascontiguousarray(upper_val, np.float64)
+        col = np.zeros(1, np.int64)
+        h = P()
+        rc = load().or_ldlt_new(sym.h, _p(v), C.byref(cancel) if cancel is not None else None, C.byref(h), _p(col))
+        if rc != 0:
+            raise OracleError(rc, int(col[0]))
+        self.h = h
+
+    def values(self):
+        count = load().or_ldlt_values(self.h, None)
+        out = np.empty(count, np.float64)
+        load().or_ldlt_values(self.h, _p(out))
+        return out
+
+    def pivots(self):
+        """(pivots, order): per postorder column its pivot kind (0 one, 1 first, 2 second of a
+        2 x 2) and the supernode-local column at that pivot position."""
+        n = self.sym.info("n")
+        piv, order = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        load().or_ldlt_pivots(self.h, _p(piv), _p(order))
+        return piv, order
+
+    def two_by_two(self) -> int:
+        return int(load().or_ldlt_info(self.h, 0))
+
+    def inertia(self):
+        """(positive, negative) eigenvalue counts."""
+        return int(load().or_ldlt_info(self.h, 1)), int(load().or_ldlt_info(self.h, 2))
+
+    def solve(self, b):
+        """b: [n] or Fortran [n, k]; solved in place and returned."""
+        b = np.asfortranarray(b, dtype=np.float64)
+        k = 1 if b.ndim == 1 else b.shape[1]
+        load().or_ldlt_solve(self.h, _p(b), int(k))
+        return b
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            load().or_ldlt_free(self.h)
+            self.h = None
+
+
+def solve_refined(n, ptr, idx, val, factor, b, steps: int, cholesky: bool = False):
+    """Symmetric::solve_refined (ldlt.rs:524-560): solve, then x += A^-1 (b - A x) while the
+    residual's largest magnitude shrinks, at most `steps` times; a Cholesky solution is returned
+    as solved. `factor` has .solve; (ptr, idx, val) is the matrix by rows, both triangles."""
+    rhs = np.array(b, np.float64)
+    x = factor.solve(rhs.copy())
+    if cholesky:
+        return x
+    r = rhs - spmv(n, ptr, idx, val, x)
+    size = float(np.max(np.abs(r))) if n else 0.0
+    for _ in range(steps):
+        if not size > 0.0:
+            break
+        trial = x + factor.solve(r.copy())
+        nxt = rhs - spmv(n, ptr, idx, val, trial)
+        nsize = float(np.max(np.abs(nxt)))
+        if not nsize < size:
+            break
+        x, r, size = trial, nxt, nsize
+    return x
 
 
 def upper_from_symmetric(n, ptr, idx, val):

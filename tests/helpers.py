@@ -246,3 +246,36 @@ def fingerprint(values) -> int:
     for b in np.ascontiguousarray(values, np.float64).view(np.uint64).tolist():
         h = ((h ^ b) * 0x100000001B3) & MASK
     return h
+
+
+def hex_pattern(n: int, sigma: float, nested_dissection) -> Csr:
+    """The stiffness pattern of a hex8 mesh on an n^3 grid of nodes (27 neighbours, 3 unknowns a
+    node), ordered by `nested_dissection(xyz, adjacency)`, diagonally dominant and shifted by
+    sigma (crates/solver/src/ldlt.rs:979-1020)."""
+    node = lambda i, j, k: i + n * (j + n * k)  # noqa: E731
+    nodes = n ** 3
+    xyz = np.array([[v % n, (v // n) % n, v // (n * n)] for v in range(nodes)], np.float64)
+    adjacency = [[] for _ in range(nodes)]
+    for k in range(n):
+        for j in range(n):
+            for i in range(n):
+                for t in range(27):
+                    x, y, z = i + t % 3, j + (t // 3) % 3, k + t // 9
+                    if 1 <= x <= n and 1 <= y <= n and 1 <= z <= n:
+                        adjacency[node(i, j, k)].append(node(x - 1, y - 1, z - 1))
+    order = nested_dissection(xyz, adjacency)
+    place = np.zeros(nodes, np.int64)
+    place[np.asarray(order)] = np.arange(nodes)
+    rows = [[] for _ in range(3 * nodes)]
+    for v, adj in enumerate(adjacency):
+        for w in adj:
+            for a in range(3):
+                for b in range(3):
+                    if v == w:
+                        value = 30.0 - sigma if a == b else 0.5
+                    elif a == b:
+                        value = -1.0
+                    else:
+                        value = 0.01 * ((v + w) % 3)
+                    rows[3 * place[v] + a].append((3 * place[w] + b, value))
+    return rows_to_csr(rows)
