@@ -601,7 +601,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *_
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.0;
   const int nk = (K + GEMM_KC - 1) / GEMM_KC;
-#pragma unroll
   const bool gather = tp->flags & 16;
   const int32_t *brows = tp->b_rows;
   const int64_t bsk = tp->b_sk;
