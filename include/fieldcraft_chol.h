@@ -36,7 +36,7 @@ extern "C" {
 
 /* Precision of the numeric phase. */
 #define FC_PRECISION_FP64 0
-#define FC_PRECISION_FP32_IR 1 /* FP32 factor (FP64 fallback for weak pivots), FP64 refinement */
+#define FC_PRECISION_FP32_IR 1 /* FP32 factor of S A S, every diagonal block in FP64; FP64 refinement */
 
 typedef struct fc_status {
   int32_t code;
