@@ -1,0 +1,53 @@
+"""TEST INFRASTRUCTURE: builds and loads the CPU emulation of the device LDL^T panel
+(ldlt_emulation.cpp beside this file), which runs the kernel's own source on host threads."""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "ldlt_emulation.cpp"
+HEADER = HERE.parent.parent / "fieldcraft_b200" / "csrc" / "cuda" / "ldlt_panel.cuh"
+LIB = HERE / "libldlt_emulation.so"
+_lib = None
+
+
+def build():
+    if LIB.exists() and LIB.stat().st_mtime >= max(SRC.stat().st_mtime, HEADER.stat().st_mtime):
+        return
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-ffp-contract=off", "-fno-fast-math",
+                    "-Wall", "-Wextra", f"-I{HEADER.parent.parent}", "-o", str(LIB), str(SRC)], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB))
+        _lib.emu_ldlt_front.restype = C.c_int
+        _lib.emu_ldlt_front.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.c_int, C.c_void_p]
+    return _lib
+
+
+def factor_front(front: np.ndarray, w: int, scale: np.ndarray, threads: int, jitter: int = 0):
+    """Factors an m x w front (rows >= columns meaningful) with the panel source on `threads`
+    host threads. Returns (result, F, pivots, order, 2 x 2 count): result -1, or the own column
+    found singular; -2 / -3 when the threads disagreed."""
+    m = front.shape[0]
+    F = np.asfortranarray(front[:, :w], dtype=np.float64).copy(order="F")
+    scale = np.ascontiguousarray(scale, np.float64)
+    order = np.zeros(w, np.int32)
+    pivots = np.zeros(w, np.int8)
+    twos = C.c_int(0)
+    rc = load().emu_ldlt_front(m, w, F.ctypes.data, scale.ctypes.data, order.ctypes.data, pivots.ctypes.data,
+                               threads, jitter, C.byref(twos))
+    return rc, F, pivots, order, twos.value
+
+
+def packed(F: np.ndarray, w: int) -> np.ndarray:
+    """The front's lower trapezoid by columns (the reference's layout)."""
+    return np.concatenate([F[c:, c] for c in range(w)]) if w else np.zeros(0)

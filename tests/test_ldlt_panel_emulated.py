@@ -1,0 +1,154 @@
+"""The device LDL^T panel (fieldcraft_b200/csrc/cuda/ldlt_panel.cuh) run on host threads by
+tests/native/ldlt_emulation.cpp, against the oracle's LDL^T (crates/solver/src/ldlt.rs): the
+same source the kernel compiles, so its pivots, interchanges, 1 x 1 and 2 x 2 stores, the
+update coefficients W and its synchronisation are checked without a GPU. Fronts whose factor
+depends only on A (dense single-supernode matrices, and leaf supernodes of sparse ones) must
+come out bit for bit the oracle's on any number of threads."""
+import numpy as np
+import pytest
+
+import helpers as H
+from native import emulation as E
+from oracle import oracle
+
+SINGULAR = 2
+
+
+def dense_csr(A):
+    n = A.shape[0]
+    return H.rows_to_csr([[(j, A[i, j]) for j in range(n) if A[i, j] != 0 or i == j] for i in range(n)])
+
+
+def indefinite(n, seed, zero_every=3):
+    rng = np.random.default_rng(seed)
+    B = rng.standard_normal((n, n))
+    A = B + B.T
+    A[np.arange(1, n, zero_every), np.arange(1, n, zero_every)] = 0.0  # zero diagonals: 2 x 2 pivots
+    return A
+
+
+def oracle_ldlt(a):
+    ptr, idx, val = oracle.upper_from_symmetric(a.n, a.ptr, a.idx, a.val)
+    s = oracle.Sym(a.n, ptr, idx)
+    return s, oracle.Ldlt(s, val)
+
+
+def bits(x):
+    return np.ascontiguousarray(x, np.float64).view(np.uint64)
+
+
+@pytest.mark.parametrize("n", [1, 2, 11, 63, 64, 65, 129, 200])
+@pytest.mark.parametrize("threads", [1, 5, 32])
+def test_dense_fronts_are_the_oracles_bit_for_bit(n, threads):
+    """One supernode (a dense matrix), panels of 64 with the update of the later columns between
+    them: values, pivots, order and the count of 2 x 2 pivots as the oracle's."""
+    A = indefinite(n, seed=n)
+    s, f = oracle_ldlt(dense_csr(A))
+    assert s.info("ns") == 1 and np.array_equal(s.array("perm"), np.arange(n))
+    rc, F, piv, order, twos = E.factor_front(np.tril(A), n, np.max(np.abs(A), axis=0), threads)
+    assert rc == -1
+    opiv, oorder = f.pivots()
+    assert np.array_equal(piv, opiv) and np.array_equal(order, oorder)
+    assert twos == f.two_by_two()
+    assert np.array_equal(bits(E.packed(F, n)), bits(f.values()))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_no_thread_reads_what_another_moved(seed):
+    """Random delays after every barrier (seeded) change which thread runs ahead; a thread that
+    wrote what another had yet to read would change a bit or a branch."""
+    A = indefinite(96, seed=100 + seed, zero_every=2)
+    s, f = oracle_ldlt(dense_csr(A))
+    rc, F, piv, order, _ = E.factor_front(np.tril(A), 96, np.max(np.abs(A), axis=0), threads=6, jitter=seed + 1)
+    assert rc == -1
+    assert np.array_equal(order, f.pivots()[1])
+    assert np.array_equal(bits(E.packed(F, 96)), bits(f.values()))
+
+
+def test_saddle_point_front():
+    """ldlt.rs:656-698: zero diagonals first, so the search must pivot past them in 2 x 2 pairs."""
+    a = H.saddle(8, 3)
+    s, f = oracle_ldlt(a)
+    A = np.zeros((a.n, a.n))
+    for i in range(a.n):
+        A[i, a.idx[a.ptr[i]:a.ptr[i + 1]]] = a.val[a.ptr[i]:a.ptr[i + 1]]
+    perm = s.array("perm")
+    Ap = A[np.ix_(perm, perm)]
+    assert s.info("ns") == 1
+    rc, F, piv, order, twos = E.factor_front(np.tril(Ap), a.n, np.max(np.abs(A), axis=0)[perm], threads=4)
+    assert rc == -1 and twos == f.two_by_two() == 3
+    assert np.array_equal(bits(E.packed(F, a.n)), bits(f.values()))
+
+
+def leaf_fronts(a, s):
+    """The leaf supernodes' fronts (no descendant updates): A's entries of their columns at
+    their rows, in the analysis' order; with the largest |A| of each column."""
+    perm = s.array("perm")
+    first, rptr, rows, uptr = s.array("first"), s.array("rptr"), s.array("rows"), s.array("uptr")
+    n = a.n
+    A = np.zeros((n, n))
+    for i in range(n):
+        A[i, a.idx[a.ptr[i]:a.ptr[i + 1]]] = a.val[a.ptr[i]:a.ptr[i + 1]]
+    Ap = A[np.ix_(perm, perm)]
+    scale = np.max(np.abs(A), axis=0)[perm]
+    trap = [sum(rptr[k + 1] - rptr[k] - c for c in range(first[k + 1] - first[k])) for k in range(len(first) - 1)]
+    offs = np.concatenate([[0], np.cumsum(trap)])
+    for k in range(len(first) - 1):
+        if uptr[k + 1] != uptr[k]:
+            continue
+        f0, w = first[k], first[k + 1] - first[k]
+        rk = rows[rptr[k]:rptr[k + 1]]
+        front = np.zeros((len(rk), w))
+        for c in range(w):
+            front[c:, c] = Ap[rk[c:], f0 + c]
+        yield k, front, w, scale[f0:f0 + w], slice(offs[k], offs[k + 1]), slice(f0, f0 + w)
+
+
+@pytest.mark.parametrize("case", ["grid", "hex", "blocks"])
+def test_leaf_fronts_with_rows_below(case):
+    """Fronts taller than their columns (rows of later supernodes below the pivots): the
+    interchanges move those rows' entries too, and L is stored for them."""
+    if case == "grid":
+        a = H.shifted_grid([7, 6, 5], 3.3)[0]
+    elif case == "hex":
+        from test_oracle_ldlt import nested_dissection
+        a = H.hex_pattern(5, 22.0, nested_dissection)
+    else:
+        # two dense indefinite blocks of 100 and 40 columns sharing a 10-column separator
+        n1, n2, ns = 100, 40, 10
+        n = n1 + n2 + ns
+        A = np.zeros((n, n))
+        A[:n1, :n1] = indefinite(n1, seed=7)
+        A[n1:n1 + n2, n1:n1 + n2] = indefinite(n2, seed=8)
+        rng = np.random.default_rng(9)
+        C = rng.standard_normal((n1 + n2, ns))
+        A[:n1 + n2, n1 + n2:] = C
+        A[n1 + n2:, :n1 + n2] = C.T
+        A[n1 + n2:, n1 + n2:] = np.eye(ns) * 50.0
+        a = dense_csr(A)
+    s, f = oracle_ldlt(a)
+    values = f.values()
+    opiv, oorder = f.pivots()
+    checked = 0
+    for k, front, w, scale, vslice, cslice in leaf_fronts(a, s):
+        rc, F, piv, order, _ = E.factor_front(front, w, scale, threads=4)
+        assert rc == -1, k
+        assert np.array_equal(piv, opiv[cslice]) and np.array_equal(order, oorder[cslice]), k
+        assert np.array_equal(bits(E.packed(F, w)), bits(values[vslice])), k
+        checked += 1
+    assert checked > 0
+    if case == "blocks":
+        assert max(front.shape[0] - w for _, front, w, *_ in leaf_fronts(a, s)) > 0
+
+
+def test_singular_columns_are_the_oracles():
+    """A rank-one matrix and a NaN: the column the panel reports is the one the oracle names."""
+    v = np.arange(1.0, 8.0)
+    for A in [np.outer(v, v), indefinite(9, seed=4)]:
+        if A.shape[0] == 9:
+            A[4, 6] = A[6, 4] = np.nan
+        with pytest.raises(oracle.OracleError) as e:
+            oracle_ldlt(dense_csr(A))
+        assert e.value.code == SINGULAR
+        rc, *_ = E.factor_front(np.tril(A), A.shape[0], np.max(np.abs(A), axis=0), threads=3)
+        assert rc == e.value.column
