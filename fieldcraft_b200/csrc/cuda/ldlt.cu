@@ -4,6 +4,7 @@
 // the device's block (threads, __syncthreads) and its per-supernode state.
 #include <cstdint>
 
+#include "cuda/kernels.cuh"
 #include "cuda/ldlt_panel.cuh"
 
 namespace fc {
@@ -15,18 +16,22 @@ struct DeviceBlock {
   __device__ void sync() { __syncthreads(); }
 };
 
-// One front's panel step: the front and its state (Front), and where its columns start in the
-// analysis' postorder (`first`, for the failing column's name).
+// One front's panel step: the front and its state (Front), where its columns start in the
+// analysis' postorder (`first`, for the failing column's name), and the GEMM tasks of the update
+// of its later own columns (`slots`, `nslots` of them: update_tiles for the earliest end).
 struct PanelTask {
   Front front;
   int64_t first;
+  fc::GemmTask *slots;
+  int32_t nslots;
   int32_t s;
-  int32_t pad;
 };
 
 // Per supernode s: pos[s] is where its next panel starts (w when done), twos[s] counts its 2 x 2
 // pivots. A singular column lowers *failed to its postorder index (the first failing column in
-// postorder is the one reported) and ends the supernode.
+// postorder is the one reported) and ends the supernode. After the panel the CTA writes the
+// update of the later own columns as GEMM tasks (C -= L_panel W^T on the lower tiles, for the
+// launch that follows); the slots it does not need stay empty (M = N = K = 0: no work).
 __global__ void __launch_bounds__(MAX_THREADS) ldlt_panel_kernel(const PanelTask *__restrict__ tasks,
                                                                  int32_t *__restrict__ pos,
                                                                  int32_t *__restrict__ twos,
@@ -35,22 +40,47 @@ __global__ void __launch_bounds__(MAX_THREADS) ldlt_panel_kernel(const PanelTask
   const PanelTask &task = tasks[blockIdx.x];
   const Front &f = task.front;
   const int c0 = pos[task.s];
-  if (c0 >= f.w) return;
-  DeviceBlock blk;
-  int end = c0, made = 0;
-  const int singular = panel(blk, sh, f, c0, &end, &made);
-  if (singular >= 0) {
-    if (threadIdx.x == 0) {
-      atomicMin(failed, (unsigned long long)(task.first + singular));
-      pos[task.s] = f.w;
+  int end = f.w;
+  bool ok = false;
+  if (c0 < f.w) {
+    DeviceBlock blk;
+    int made = 0;
+    end = c0;
+    const int singular = panel(blk, sh, f, c0, &end, &made);
+    if (singular >= 0) {
+      if (threadIdx.x == 0) {
+        atomicMin(failed, (unsigned long long)(task.first + singular));
+        pos[task.s] = f.w;
+      }
+      end = f.w;
+    } else {
+      ok = true;
+      panel_w(blk, f, c0, end);
+      if (threadIdx.x == 0) twos[task.s] += made;
     }
-    return;
   }
-  panel_w(blk, f, c0, end);
-  if (threadIdx.x == 0) {
-    pos[task.s] = end;
-    twos[task.s] += made;
+  // the update tasks (every slot written, so a finished or failed front leaves only empty ones)
+  for (int q = threadIdx.x; q < task.nslots; q += blockDim.x) {
+    fc::GemmTask g{};
+    Tile t;
+    if (ok && update_tile(f.m, f.w, end, q, t)) {
+      g.C = f.F + t.i0 + (int64_t)t.j0 * f.m;
+      g.c_si = 1, g.c_sj = f.m;
+      g.A = f.F + t.i0 + (int64_t)c0 * f.m;
+      g.a_si = 1, g.a_sk = f.m;
+      g.B = f.W + (t.j0 - end);
+      g.b_sj = 1, g.b_sk = f.ld_w;
+      g.M = t.M, g.N = t.N, g.K = end - c0;
+      g.flags = t.lower ? 1 : 0;
+    } else {
+      g.C = f.F, g.A = f.F, g.B = f.F;
+      g.c_si = g.a_si = g.b_sj = 1;
+      g.c_sj = g.a_sk = g.b_sk = 1;
+    }
+    task.slots[q] = g;
   }
+  if (!ok) return;
+  if (threadIdx.x == 0) pos[task.s] = end;
 }
 
 }  // namespace ldlt

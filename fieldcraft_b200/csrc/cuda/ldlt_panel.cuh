@@ -298,5 +298,40 @@ FC_LDLT_FN void panel_w(Block &blk, const Front &f, int c0, int c1) {
   blk.sync();
 }
 
+// The update of the later own columns by a panel that ended at c1, as tiles of at most 64 x 64:
+// the front's rows [c1, m) of its columns [c1, w), lower part only; column blocks of 64 from c1,
+// in each the row blocks from the diagonal down. Tile `slot` of that list, or false past its end.
+struct Tile {
+  int64_t i0;   // first row
+  int j0;       // first column
+  int M, N;     // rows, columns
+  bool lower;   // a diagonal tile: only rows >= columns
+};
+constexpr int TILE_ROWS = 64;
+
+FC_LDLT_FN bool update_tile(int64_t m, int w, int c1, int64_t slot, Tile &t) {
+  for (int j0 = c1; j0 < w; j0 += TILE_ROWS) {
+    const int64_t rows = (m - j0 + TILE_ROWS - 1) / TILE_ROWS;
+    if (slot < rows) {
+      t.i0 = j0 + slot * TILE_ROWS;
+      t.j0 = j0;
+      t.M = (int)(m - t.i0 < TILE_ROWS ? m - t.i0 : TILE_ROWS);
+      t.N = w - j0 < TILE_ROWS ? w - j0 : TILE_ROWS;
+      t.lower = slot == 0;
+      return true;
+    }
+    slot -= rows;
+  }
+  return false;
+}
+
+// The tiles of that update: at most this many for a panel that ends at c1 or later (the count
+// falls as c1 grows), so a plan sized for the earliest end holds every case.
+FC_LDLT_FN int64_t update_tiles(int64_t m, int w, int c1) {
+  int64_t count = 0;
+  for (int j0 = c1; j0 < w; j0 += TILE_ROWS) count += (m - j0 + TILE_ROWS - 1) / TILE_ROWS;
+  return count;
+}
+
 }  // namespace ldlt
 }  // namespace fc

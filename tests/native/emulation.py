@@ -30,6 +30,9 @@ def load():
         _lib.emu_ldlt_front.restype = C.c_int
         _lib.emu_ldlt_front.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_int, C.c_void_p]
+        _lib.emu_update_tiles.restype = C.c_int64
+        _lib.emu_update_tiles.argtypes = [C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_int64]
     return _lib
 
 
@@ -51,3 +54,15 @@ def factor_front(front: np.ndarray, w: int, scale: np.ndarray, threads: int, jit
 def packed(F: np.ndarray, w: int) -> np.ndarray:
     """The front's lower trapezoid by columns (the reference's layout)."""
     return np.concatenate([F[c:, c] for c in range(w)]) if w else np.zeros(0)
+
+
+def update_tiles(m: int, w: int, c1: int):
+    """The update tiles after a panel that ended at c1: a list of (i0, j0, M, N, lower)."""
+    lib = load()
+    count = lib.emu_update_tiles(m, w, c1, None, None, None, None, None, 0)
+    assert count >= 0, "update_tiles disagrees with update_tile"
+    i0, j0 = np.zeros(count, np.int64), np.zeros(count, np.int32)
+    M, N, low = np.zeros(count, np.int32), np.zeros(count, np.int32), np.zeros(count, np.int8)
+    lib.emu_update_tiles(m, w, c1, i0.ctypes.data, j0.ctypes.data, M.ctypes.data, N.ctypes.data, low.ctypes.data,
+                         count)
+    return list(zip(i0.tolist(), j0.tolist(), M.tolist(), N.tolist(), low.astype(bool).tolist()))

@@ -76,8 +76,8 @@ extern "C" {
 
 // Factors one front (m x w column-major in F, rows >= columns meaningful) with the panel source
 // on `threads` host threads, panel after panel; between panels the later own columns take the
-// panel's update in the oracle's order (each entry's sum over the panel's columns from zero, then
-// one subtraction). scale[w]: the largest |A| of each own column. Fills order[w] and pivots[w];
+// panel's update over the kernel's update tiles (update_tile), each entry in the oracle's order
+// (its sum over the panel's columns from zero, then one subtraction). scale[w]: the largest |A| of each own column. Fills order[w] and pivots[w];
 // *twos receives the 2 x 2 pivots. jitter: 0, or a seed for random delays after barriers.
 // Returns -1, the own column found singular, -2 when the threads returned different results,
 // -3 when they reached different barriers.
@@ -117,16 +117,44 @@ int emu_ldlt_front(int64_t m, int w, double *F, const double *scale, int32_t *or
       if (result[t] != result[0] || (result[0] < 0 && (end[t] != end[0] || made[t] != made[0]))) return -2;
     if (result[0] >= 0) return result[0];
     *twos += made[0];
+    // the update tile by tile, as the GEMM tasks the kernel writes would apply it
     const int c1 = end[0], kw = c1 - c0;
-    for (int c = c1; c < w; ++c)
-      for (int64_t i = c; i < m; ++i) {
-        double s = 0.0;
-        for (int j = 0; j < kw; ++j) s += F[i + (int64_t)(c0 + j) * m] * W[(c - c1) + (int64_t)j * f.ld_w];
-        F[i + (int64_t)c * m] -= s;
-      }
+    L::Tile tile;
+    for (int64_t slot = 0; L::update_tile(m, w, c1, slot, tile); ++slot)
+      for (int jj = 0; jj < tile.N; ++jj)
+        for (int ii = 0; ii < tile.M; ++ii) {
+          const int64_t i = tile.i0 + ii;
+          const int c = tile.j0 + jj;
+          if (tile.lower && i < c) continue;
+          double s = 0.0;
+          for (int j = 0; j < kw; ++j) s += F[i + (int64_t)(c0 + j) * m] * W[(c - c1) + (int64_t)j * f.ld_w];
+          F[i + (int64_t)c * m] -= s;
+        }
     c0 = c1;
   }
   return -1;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Every update tile of a front (m rows, w own columns) after a panel that ended at c1: rows
+// i0[], columns j0[], sizes M[], N[], lower[] for at most cap tiles; returns the count, which
+// update_tiles must give.
+int64_t emu_update_tiles(int64_t m, int w, int c1, int64_t *i0, int32_t *j0, int32_t *M, int32_t *N, int8_t *lower,
+                         int64_t cap) {
+  fc::ldlt::Tile t;
+  int64_t count = 0;
+  for (int64_t slot = 0; fc::ldlt::update_tile(m, w, c1, slot, t); ++slot, ++count)
+    if (count < cap) {
+      i0[count] = t.i0;
+      j0[count] = t.j0;
+      M[count] = t.M;
+      N[count] = t.N;
+      lower[count] = t.lower;
+    }
+  return count == fc::ldlt::update_tiles(m, w, c1) ? count : -1;
 }
 
 }  // extern "C"

@@ -152,3 +152,25 @@ def test_singular_columns_are_the_oracles():
         assert e.value.code == SINGULAR
         rc, *_ = E.factor_front(np.tril(A), A.shape[0], np.max(np.abs(A), axis=0), threads=3)
         assert rc == e.value.column
+
+
+@pytest.mark.parametrize("m,w", [(64, 64), (65, 65), (130, 129), (300, 200), (1000, 257)])
+def test_update_tiles_cover_the_later_columns_once(m, w):
+    """The GEMM tiles a panel writes for the update of the later own columns: every entry of rows
+    [c1, m) x columns [c1, w) on or below the diagonal exactly once, nothing else; a later end
+    never needs more tiles than the earliest (the plan reserves that many)."""
+    for c0 in range(0, w, 64):
+        for c1 in (c0 + 64, c0 + 65):
+            if c1 > w:
+                continue
+            hits = np.zeros((m, w), np.int32)
+            for i0, j0, M, N, lower in E.update_tiles(m, w, c1):
+                assert 0 < M <= 64 and 0 < N <= 64 and i0 >= j0 and lower == (i0 == j0)
+                r = np.arange(i0, i0 + M)[:, None]
+                c = np.arange(j0, j0 + N)[None, :]
+                hits[i0:i0 + M, j0:j0 + N] += (r >= c) if lower else 1
+            want = np.zeros((m, w), np.int32)
+            for c in range(c1, w):
+                want[c:, c] = 1
+            assert np.array_equal(hits, want), (c0, c1)
+            assert len(E.update_tiles(m, w, c1)) <= len(E.update_tiles(m, w, c0 + 64))
