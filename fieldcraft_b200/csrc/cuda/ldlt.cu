@@ -83,5 +83,29 @@ __global__ void __launch_bounds__(MAX_THREADS) ldlt_panel_kernel(const PanelTask
   if (threadIdx.x == 0) pos[task.s] = end;
 }
 
+// After a level's panels, per front (one CTA each): W21 = L21 D into w21[s] (leading dimension
+// m - w, for the update-matrix GEMM), then D out of the front into d / e at the front's first
+// postorder column (split_d), leaving its own block unit lower for the solve.
+struct AfterTask {
+  Front front;
+  double *w21;
+  double *d, *e;
+};
+
+__global__ void __launch_bounds__(MAX_THREADS) ldlt_after_kernel(const AfterTask *__restrict__ tasks) {
+  const AfterTask &task = tasks[blockIdx.x];
+  DeviceBlock blk;
+  if (task.front.m > task.front.w) front_w21(blk, task.front, task.w21, task.front.m - task.front.w);
+  split_d(blk, task.front, task.d, task.e);
+}
+
+// y <- D^-1 y between the solve's forward and backward passes: n unknowns in postorder, R
+// right-hand sides row-major; one thread per unknown (the second column of a 2 x 2 pivot idles).
+__global__ void ldlt_d_inverse_kernel(int64_t n, int R, const double *__restrict__ d, const double *__restrict__ e,
+                                      const int8_t *__restrict__ pivots, double *__restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    apply_d_inverse(i, R, d, e, pivots, y);
+}
+
 }  // namespace ldlt
 }  // namespace fc

@@ -298,6 +298,65 @@ FC_LDLT_FN void panel_w(Block &blk, const Front &f, int c0, int c1) {
   blk.sync();
 }
 
+// W21 = L21 D: the rows [w, m) of the front times its block diagonal, ld_out x w, for the update
+// matrix U = -L21 W21^T the parent assembles (products' Y for a descendant, cholesky.rs:531-548,
+// with times_d's operations).
+template <class Block>
+FC_LDLT_FN void front_w21(Block &blk, const Front &f, double *out, int64_t ld_out) {
+  for (int64_t r = f.w + blk.tid(); r < f.m; r += blk.size()) {
+    double *o = out + (r - f.w);
+    int k = 0;
+    while (k < f.w) {
+      if (f.pivots[k] == PIVOT_FIRST) {
+        const double x = at(f, r, k), y = at(f, r, k + 1);
+        const double d11 = at(f, k, k), d21 = at(f, k + 1, k), d22 = at(f, k + 1, k + 1);
+        o[k * ld_out] = add(mul(x, d11), mul(y, d21));
+        o[(k + 1) * ld_out] = add(mul(x, d21), mul(y, d22));
+        k += 2;
+      } else {
+        o[k * ld_out] = mul(at(f, r, k), at(f, k, k));
+        k += 1;
+      }
+    }
+  }
+  blk.sync();
+}
+
+// D out of a factored front: d[c] receives D's diagonal and e[c] its subdiagonal (the 2 x 2
+// pivots' d21 at their first column, else 0); the front's own block becomes unit lower (ones on
+// the diagonal, zeros where a 2 x 2 pivot's d21 was), the form the triangular solve reads.
+template <class Block>
+FC_LDLT_FN void split_d(Block &blk, const Front &f, double *d, double *e) {
+  for (int c = blk.tid(); c < f.w; c += blk.size()) {
+    d[c] = at(f, c, c);
+    e[c] = f.pivots[c] == PIVOT_FIRST ? at(f, c + 1, c) : 0.0;
+  }
+  blk.sync();
+  for (int c = blk.tid(); c < f.w; c += blk.size()) {
+    at(f, c, c) = 1.0;
+    if (f.pivots[c] == PIVOT_FIRST) at(f, c + 1, c) = 0.0;
+  }
+  blk.sync();
+}
+
+// y <- D^-1 y for the unknowns [0, n) of R right-hand sides (row-major, y[i * R + j]), D given by
+// its diagonal d, subdiagonal e and the pivot kinds (the solve's block step, cholesky.rs:946-974).
+// One thread per pivot group: a 1 x 1 pivot or the first column of a 2 x 2 one.
+FC_LDLT_FN void apply_d_inverse(int64_t i, int R, const double *d, const double *e, const int8_t *pivots, double *y) {
+  if (pivots[i] == PIVOT_SECOND) return;
+  if (pivots[i] == PIVOT_FIRST) {
+    const double d11 = d[i], d21 = e[i], d22 = d[i + 1];
+    const double det = sub(mul(d11, d22), mul(d21, d21));
+    for (int j = 0; j < R; ++j) {
+      const double p = y[i * R + j], q = y[(i + 1) * R + j];
+      y[i * R + j] = sub(mul(d22, p), mul(d21, q)) / det;
+      y[(i + 1) * R + j] = sub(mul(d11, q), mul(d21, p)) / det;
+    }
+  } else {
+    for (int j = 0; j < R; ++j) y[i * R + j] = y[i * R + j] / d[i];
+  }
+}
+
 // The update of the later own columns by a panel that ended at c1, as tiles of at most 64 x 64:
 // the front's rows [c1, m) of its columns [c1, w), lower part only; column blocks of 64 from c1,
 // in each the row blocks from the diagonal down. Tile `slot` of that list, or false past its end.

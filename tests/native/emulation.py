@@ -30,6 +30,11 @@ def load():
         _lib.emu_ldlt_front.restype = C.c_int
         _lib.emu_ldlt_front.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_int, C.c_void_p]
+        _lib.emu_ldlt_after.restype = C.c_int
+        _lib.emu_ldlt_after.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_int]
+        _lib.emu_apply_d_inverse.restype = None
+        _lib.emu_apply_d_inverse.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.emu_update_tiles.restype = C.c_int64
         _lib.emu_update_tiles.argtypes = [C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_int64]
@@ -66,3 +71,25 @@ def update_tiles(m: int, w: int, c1: int):
     lib.emu_update_tiles(m, w, c1, i0.ctypes.data, j0.ctypes.data, M.ctypes.data, N.ctypes.data, low.ctypes.data,
                          count)
     return list(zip(i0.tolist(), j0.tolist(), M.tolist(), N.tolist(), low.astype(bool).tolist()))
+
+
+def after_factor(F: np.ndarray, w: int, pivots: np.ndarray, threads: int):
+    """W21 = L21 D and D split out of a factored front (F changed in place to unit lower).
+    Returns (W21 [(m - w) x w], d, e)."""
+    m = F.shape[0]
+    w21 = np.zeros((max(m - w, 1), w), order="F")
+    d, e = np.zeros(w), np.zeros(w)
+    piv = np.ascontiguousarray(pivots, np.int8)
+    rc = load().emu_ldlt_after(m, w, F.ctypes.data, piv.ctypes.data, w21.ctypes.data, d.ctypes.data, e.ctypes.data,
+                               threads)
+    assert rc == 0
+    return w21[:m - w], d, e
+
+
+def apply_d_inverse(d, e, pivots, y):
+    """y [n, R] (C order) <- D^-1 y."""
+    y = np.ascontiguousarray(y, np.float64)
+    load().emu_apply_d_inverse(y.shape[0], y.shape[1], np.ascontiguousarray(d).ctypes.data,
+                               np.ascontiguousarray(e).ctypes.data, np.ascontiguousarray(pivots, np.int8).ctypes.data,
+                               y.ctypes.data)
+    return y

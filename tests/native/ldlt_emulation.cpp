@@ -158,3 +158,32 @@ int64_t emu_update_tiles(int64_t m, int w, int c1, int64_t *i0, int32_t *j0, int
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// After a front is factored (emu_ldlt_front): W21 = L21 D into w21 (ld m - w), then D out of the
+// front into d and e (split_d), on `threads` host threads. Returns 0, or -3 on a divergence.
+int emu_ldlt_after(int64_t m, int w, double *F, const int8_t *pivots, double *w21, double *d, double *e, int threads) {
+  namespace L = fc::ldlt;
+  if (threads < 1 || threads > MAX_EMULATED) return -2;
+  Checks checks;
+  for (int t = 0; t < threads; ++t) checks.count[t] = 0;
+  L::Front f{F, m, w, nullptr, nullptr, const_cast<int8_t *>(pivots), nullptr, nullptr, nullptr, 0};
+  Barrier barrier(threads);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&, t] {
+      HostBlock blk{t, threads, &barrier, &checks, std::mt19937((uint32_t)t)};
+      L::front_w21(blk, f, w21, m - w > 0 ? m - w : 1);
+      L::split_d(blk, f, d, e);
+    });
+  for (auto &th : pool) th.join();
+  return checks.diverged ? -3 : 0;
+}
+
+// y <- D^-1 y over n unknowns of R right-hand sides (row-major), one call per pivot group.
+void emu_apply_d_inverse(int64_t n, int R, const double *d, const double *e, const int8_t *pivots, double *y) {
+  for (int64_t i = 0; i < n; ++i) fc::ldlt::apply_d_inverse(i, R, d, e, pivots, y);
+}
+
+}  // extern "C"

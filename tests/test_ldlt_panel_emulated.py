@@ -174,3 +174,62 @@ def test_update_tiles_cover_the_later_columns_once(m, w):
                 want[c:, c] = 1
             assert np.array_equal(hits, want), (c0, c1)
             assert len(E.update_tiles(m, w, c1)) <= len(E.update_tiles(m, w, c0 + 64))
+
+
+def test_w21_split_and_d_inverse():
+    """After the panels: W21 = L21 D with times_d's operations (the Y of a descendant's product,
+    cholesky.rs:531-548), D split from a unit lower L, and D^-1 applied as the solve's block step
+    (cholesky.rs:946-974): each bit for bit the restatement below."""
+    n1, n2, ns = 100, 40, 10
+    n = n1 + n2 + ns
+    A = np.zeros((n, n))
+    A[:n1, :n1] = indefinite(n1, seed=7)
+    A[n1:n1 + n2, n1:n1 + n2] = indefinite(n2, seed=8)
+    Cc = np.random.default_rng(9).standard_normal((n1 + n2, ns))
+    A[:n1 + n2, n1 + n2:] = Cc
+    A[n1 + n2:, :n1 + n2] = Cc.T
+    A[n1 + n2:, n1 + n2:] = np.eye(ns) * 50.0
+    a = dense_csr(A)
+    s, f = oracle_ldlt(a)
+    k, front, w, scale, _, _ = max(leaf_fronts(a, s), key=lambda t: t[2])
+    m = front.shape[0]
+    assert m > w
+    rc, F, piv, order, twos = E.factor_front(front, w, scale, threads=4)
+    assert rc == -1 and twos > 0
+    L = F.copy()
+    w21, d, e = E.after_factor(F, w, piv, threads=5)
+    # W21 by times_d on each row below
+    want = np.zeros((m - w, w))
+    for r in range(w, m):
+        c = 0
+        while c < w:
+            if piv[c] == 1:
+                x, y = L[r, c], L[r, c + 1]
+                d11, d21, d22 = L[c, c], L[c + 1, c], L[c + 1, c + 1]
+                want[r - w, c] = x * d11 + y * d21
+                want[r - w, c + 1] = x * d21 + y * d22
+                c += 2
+            else:
+                want[r - w, c] = L[r, c] * L[c, c]
+                c += 1
+    assert np.array_equal(bits(w21), bits(want))
+    assert np.array_equal(d, np.diag(L)[:w])
+    assert np.array_equal(e[piv == 1], L[np.flatnonzero(piv == 1) + 1, np.flatnonzero(piv == 1)])
+    assert np.all(np.diag(F)[:w] == 1.0) and np.all(F[np.flatnonzero(piv == 1) + 1, np.flatnonzero(piv == 1)] == 0.0)
+    # D^-1 on 3 right-hand sides
+    y = np.random.default_rng(1).standard_normal((w, 3))
+    got = E.apply_d_inverse(d, e, piv, y.copy())
+    ref = y.copy()
+    c = 0
+    while c < w:
+        if piv[c] == 1:
+            d11, d21, d22 = d[c], e[c], d[c + 1]
+            det = d11 * d22 - d21 * d21
+            p, q = y[c].copy(), y[c + 1].copy()
+            ref[c] = (d22 * p - d21 * q) / det
+            ref[c + 1] = (d11 * q - d21 * p) / det
+            c += 2
+        else:
+            ref[c] = y[c] / d[c]
+            c += 1
+    assert np.array_equal(bits(got), bits(ref))
