@@ -1,8 +1,10 @@
 """fieldcraft_b200: the numeric phase of FieldCraft's supernodal sparse Cholesky (the direct solve
 behind its implicit FEM analyses, K u = f) rebuilt for NVIDIA B200, behind the reference's own
 factorise/solve API. See include/fieldcraft_chol.h for the C ABI."""
-from .cholesky import (FP32_IR, FP64, Cancelled, Csr, DeviceError, Factor, FactorError, Internal, Timeout,
-                       NotPositiveDefinite, OutOfMemory, Singular, Symbolic, TooLarge, UpperColumns)
+from .cholesky import (FP32_IR, FP64, LDLT, Cancelled, Csr, DeviceError, Factor, FactorError, Inertia, Internal,
+                       LdltFactor, NotPositiveDefinite, OutOfMemory, Singular, Symbolic, Timeout, TooLarge,
+                       UpperColumns)
 
 __all__ = ["Csr", "UpperColumns", "Symbolic", "Factor", "FactorError", "NotPositiveDefinite", "Singular",
-           "TooLarge", "OutOfMemory", "Internal", "Cancelled", "Timeout", "DeviceError", "FP64", "FP32_IR"]
+           "TooLarge", "OutOfMemory", "Internal", "Cancelled", "Timeout", "DeviceError", "FP64", "FP32_IR", "LDLT",
+           "LdltFactor", "Inertia"]

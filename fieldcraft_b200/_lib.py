@@ -47,6 +47,7 @@ SIGNATURES = {
     "fc_chol_solve_device_async": (i32, [P, P, i32, i64]),
     "fc_chol_solve_device_noalloc": (i32, [P, P, i32, i64, C.POINTER(Status)]),
     "fc_chol_values": (i32, [P, P, C.POINTER(Status)]),
+    "fc_chol_inertia": (i32, [P, P, P, P, C.POINTER(Status)]),
     "fc_chol_stat": (i64, [P, i32]),
     "fc_chol_refine_solve_device": (i32, [P, P, P, P, P, P, i32, i64, f64, i32, P, P, C.POINTER(Status)]),
     "fc_chol_option": (i32, [P, i32, i64]),

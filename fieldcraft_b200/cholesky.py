@@ -18,7 +18,7 @@ from ._lib import Status
 
 FC_OK, FC_NOT_POSITIVE_DEFINITE, FC_SINGULAR, FC_TOO_LARGE, FC_OUT_OF_MEMORY = 0, 1, 2, 3, 4
 FC_INTERNAL, FC_CANCELLED, FC_TIMEOUT, FC_INVALID_ARGUMENT, FC_CUDA_ERROR = 5, 6, 7, 8, 9
-FP64, FP32_IR = 0, 1
+FP64, FP32_IR, LDLT = 0, 1, 2
 
 
 class FactorError(Exception):
@@ -309,3 +309,42 @@ class Factor:
             self.close()
         except TypeError:  # interpreter shutdown: the module's globals are gone
             pass
+
+
+@dataclass(frozen=True)
+class Inertia:
+    """The counts of positive and negative eigenvalues (ldlt.rs:83-89)."""
+    positive: int
+    negative: int
+
+
+class LdltFactor(Factor):
+    """The symmetric indefinite factor P A P^T = L D L^T on the GPU (LdltFactor, ldlt.rs:365-447):
+    bounded Bunch-Kaufman pivots inside the supernodes of the same analysis. Factors, values and
+    inertia; the device solve is not built yet, so solves raise ValueError."""
+
+    def __init__(self, symbolic: Symbolic, device: int = 0):
+        super().__init__(symbolic, LDLT, device)
+
+    @staticmethod
+    def new(a: UpperColumns, max_entries: int, device: int = 0, cancel: C.c_int32 | None = None) -> "LdltFactor":
+        """LdltFactor::new (ldlt.rs:374-376): the analysis, then the pivoted numeric phase
+        (Singular for a column with no acceptable pivot in its supernode)."""
+        f = LdltFactor(Symbolic(a, max_entries), device)
+        f.factor(a.val, cancel)
+        return f
+
+    def _counts(self):
+        pos, neg, two = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        st = Status()
+        _lib.load().fc_chol_inertia(self.handle, C.byref(pos), C.byref(neg), C.byref(two), C.byref(st))
+        raise_for(st)
+        return pos.value, neg.value, two.value
+
+    def inertia(self) -> Inertia:
+        """Sylvester's law on D (ldlt.rs:415-447)."""
+        pos, neg, _ = self._counts()
+        return Inertia(pos, neg)
+
+    def two_by_two(self) -> int:
+        return self._counts()[2]

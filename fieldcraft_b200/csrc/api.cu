@@ -23,6 +23,7 @@
 #include <cuda.h>  // CUtensorMap and its encoder's signature (looked up through the runtime)
 
 #include "cuda/kernels.cuh"
+#include "cuda/ldlt_launch.cuh"
 #include "device_buf.hpp"
 #include "host/symbolic.hpp"
 
@@ -49,7 +50,9 @@ enum Kind {
   K_GEMM_F64,    // FP64 throughout (the diagonal blocks' inverses)
   K_GEMM_TC,     // FP32 3xTF32 on tcgen05 (the update matrices of the mixed-precision factor)
   K_SOLVE_THIN_FWD, K_SOLVE_THIN_BWD,  // the thin supernodes' steps of a solve level
-  K_PACK_TC                            // the tcgen05 products' operands packed (K-major hi | lo)
+  K_PACK_TC,                           // the tcgen05 products' operands packed (K-major hi | lo)
+  K_LDLT_PANEL,                        // LDL^T: pivoted panel steps (they write the next GEMM's tasks)
+  K_LDLT_AFTER                         // LDL^T: W21 = L21 D and D out of the fronts
 };
 
 struct Launch {
@@ -105,6 +108,12 @@ struct fc_chol {
   // level), their pack and tile tasks, and one TMA tensor map per supernode
   DeviceBuf d_pack, d_pack_t, d_tc_t, d_maps;
   int64_t pack_len = 0;
+  // the symmetric indefinite factor (FC_PRECISION_LDLT): the rows' largest |A| (as bits), each
+  // column's place in its supernode, the pivot orders and kinds, the panels' progress and 2 x 2
+  // counts, the first singular column, per-level scratch, D (diagonal, subdiagonal), the tasks
+  bool ldlt = false;
+  DeviceBuf d_lscale, d_llocal, d_lorder, d_lpivots, d_lpos, d_ltwos, d_lfailed, d_lscratch, d_ldd, d_lde;
+  DeviceBuf d_lpanel, d_lafter;
   fc::Tree tree{};
   std::vector<Launch> program;
   cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch), lowest priority
@@ -767,12 +776,168 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   return FC_OK;
 }
 
+// The symmetric indefinite factor's program (FC_PRECISION_LDLT, one stream), per level: the
+// fronts' assembly; ceil(w / 64) pivoted panel steps, each followed by the GEMM of the update
+// tasks the panel step wrote (slots sized for the earliest panel end, the rest left empty);
+// W21 = L21 D and D out of the fronts; the update matrices -L21 W21^T; the children's entries in
+// them. The panels' scratch (two columns and W per front) and W21 are reused level after level.
+int plan_ldlt_upload(fc_chol *h, fc_status *st) {
+  namespace L = fc::ldlt;
+  if (h->factor_graph) {
+    cudaGraphExecDestroy(h->factor_graph);
+    h->factor_graph = nullptr;
+  }
+  h->program.clear();
+  const std::vector<std::vector<int64_t>> lv = levels_of(h);
+  auto ldw = [](int w) { return std::max(w - L::PANEL, 1); };
+  auto up32 = [](int64_t x) { return (x + 31) / 32 * 32; };
+  int64_t most = 0;
+  for (const auto &S : lv) {
+    int64_t need = 0;
+    for (int64_t s : S) {
+      const int64_t m = h->height[s], w = h->width[s];
+      need += 2 * up32(m) + up32((int64_t)ldw((int)w) * (L::PANEL + 1)) + up32((m - w) * w);
+    }
+    most = std::max(most, need);
+  }
+  const int64_t n = h->n;
+  cudaStream_t stream = h->stream;
+  cudaError_t e = cudaSuccess;
+  if (h->d_lscratch.alloc(sizeof(double) * (size_t)std::max<int64_t>(most, 1)) != cudaSuccess ||
+      h->d_lscale.alloc(sizeof(double) * (size_t)std::max<int64_t>(n, 1)) != cudaSuccess ||
+      h->d_lorder.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)) != cudaSuccess ||
+      h->d_lpivots.alloc((size_t)std::max<int64_t>(n, 1)) != cudaSuccess ||
+      h->d_lpos.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(h->ns, 1)) != cudaSuccess ||
+      h->d_ltwos.alloc(sizeof(int32_t) * (size_t)std::max<int64_t>(h->ns, 1)) != cudaSuccess ||
+      h->d_lfailed.alloc(sizeof(unsigned long long)) != cudaSuccess ||
+      h->d_ldd.alloc(sizeof(double) * (size_t)std::max<int64_t>(n, 1)) != cudaSuccess ||
+      h->d_lde.alloc(sizeof(double) * (size_t)std::max<int64_t>(n, 1)) != cudaSuccess) {
+    set_status(st, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the LDL^T factor");
+    return FC_OUT_OF_MEMORY;
+  }
+  {
+    std::vector<int32_t> local(n);
+    for (int64_t s = 0; s < h->ns; ++s)
+      for (int64_t j = h->first[s]; j < h->first[s + 1]; ++j) local[j] = (int32_t)(j - h->first[s]);
+    if ((e = upload(h->d_llocal, local, stream)) != cudaSuccess) return cuda_fail(st, e, "upload of the LDL^T plan");
+  }
+  auto Lp = [&](int64_t off) { return static_cast<double *>(arena_at(h->d_L, h, off)); };
+  auto Up = [&](int64_t off) { return static_cast<double *>(arena_at(h->d_U, h, off)); };
+  double *scratch = h->d_lscratch.as<double>();
+  std::vector<fc::AssembleTask> asm_t;
+  std::vector<int4> ranges;
+  std::vector<fc::GemmTask> gemm_t;
+  std::vector<L::PanelTask> pan_t;
+  std::vector<int64_t> pan_slot;  // each panel task's first slot in gemm_t (its pointer set at upload)
+  std::vector<L::AfterTask> aft_t;
+  for (size_t l = 0; l < lv.size(); ++l) {
+    const auto &S = lv[l];
+    int64_t off = (int64_t)asm_t.size();
+    for (int64_t s : S) assemble_tiles(h, s, fc::ASM_L, asm_t, ranges);
+    push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
+    // the level's fronts and their scratch
+    std::vector<L::Front> fronts;
+    std::vector<double *> w21;
+    int64_t at = 0;
+    int P = 0;
+    for (int64_t s : S) {
+      const int m = h->height[s], w = h->width[s];
+      const int64_t f = h->first[s];
+      L::Front fr{};
+      fr.F = Lp(h->loff[s]);
+      fr.m = m;
+      fr.w = w;
+      fr.scale = h->d_lscale.as<double>() + f;
+      fr.order = h->d_lorder.as<int32_t>() + f;
+      fr.pivots = h->d_lpivots.as<int8_t>() + f;
+      fr.a = scratch + at;
+      at += up32(m);
+      fr.b = scratch + at;
+      at += up32(m);
+      fr.W = scratch + at;
+      fr.ld_w = ldw(w);
+      at += up32((int64_t)ldw(w) * (L::PANEL + 1));
+      w21.push_back(scratch + at);
+      at += up32((int64_t)(m - w) * w);
+      fronts.push_back(fr);
+      P = std::max(P, (w + L::PANEL - 1) / L::PANEL);
+    }
+    for (int p = 0; p < P; ++p) {
+      const int64_t po = (int64_t)pan_t.size(), go = (int64_t)gemm_t.size();
+      for (size_t q = 0; q < S.size(); ++q) {
+        const int64_t s = S[q];
+        const int m = h->height[s], w = h->width[s];
+        if (p * L::PANEL >= w) continue;
+        const int earliest = (p + 1) * L::PANEL;
+        const int64_t slots = earliest < w ? L::update_tiles(m, w, earliest) : 0;
+        L::PanelTask t{};
+        t.front = fronts[q];
+        t.first = h->first[s];
+        t.nslots = (int32_t)slots;
+        t.s = (int32_t)s;
+        pan_t.push_back(t);
+        pan_slot.push_back((int64_t)gemm_t.size());
+        for (int64_t k = 0; k < slots; ++k) {
+          gemm_t.push_back(fc::GemmTask{});  // empty until the panel step writes it
+        }
+      }
+      push(h->program, K_LDLT_PANEL, po, (int64_t)pan_t.size() - po, (int)l);
+      push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+    }
+    const int64_t ao = (int64_t)aft_t.size();
+    for (size_t q = 0; q < S.size(); ++q) {
+      const int64_t f = h->first[S[q]];
+      aft_t.push_back({fronts[q], w21[q], h->d_ldd.as<double>() + f, h->d_lde.as<double>() + f});
+    }
+    push(h->program, K_LDLT_AFTER, ao, (int64_t)aft_t.size() - ao, (int)l);
+    // the update matrices: U = -L21 W21^T (lower tiles)
+    const int64_t go = (int64_t)gemm_t.size();
+    for (size_t q = 0; q < S.size(); ++q) {
+      const int64_t s = S[q];
+      const int m = h->height[s], w = h->width[s], u = m - w;
+      const int64_t lo = h->loff[s], uo = h->uoff[s];
+      for (int bj = 0; bj < u; bj += fc::GEMM_TN)
+        for (int bi = bj; bi < u; bi += fc::GEMM_TM) {
+          fc::GemmTask g{};
+          g.C = Up(uo + bi + (int64_t)bj * u);
+          g.A = Lp(lo + w + bi);
+          g.B = w21[q] + bj;
+          g.c_si = 1, g.c_sj = u, g.a_si = 1, g.a_sk = m, g.b_sj = 1, g.b_sk = u;
+          g.M = std::min(fc::GEMM_TM, u - bi);
+          g.N = std::min(fc::GEMM_TN, u - bj);
+          g.K = w;
+          g.flags = (bi == bj ? 1 : 0) | 2;
+          gemm_t.push_back(g);
+        }
+    }
+    push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+    // the children's entries on top of the update matrices
+    off = (int64_t)asm_t.size();
+    for (int64_t s : S)
+      if (h->height[s] > h->width[s] && h->kid_ptr[s + 1] > h->kid_ptr[s]) assemble_tiles(h, s, fc::ASM_U, asm_t, ranges);
+    push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
+  }
+  h->gemm_tasks = (int64_t)gemm_t.size();
+  if ((e = upload(h->d_asm, asm_t, stream)) != cudaSuccess || (e = upload(h->d_ranges, ranges, stream)) != cudaSuccess ||
+      (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
+    return cuda_fail(st, e, "upload of the LDL^T plan");
+  for (size_t q = 0; q < pan_t.size(); ++q) pan_t[q].slots = h->d_gemm.as<fc::GemmTask>() + pan_slot[q];
+  if ((e = upload(h->d_lpanel, pan_t, stream)) != cudaSuccess || (e = upload(h->d_lafter, aft_t, stream)) != cudaSuccess)
+    return cuda_fail(st, e, "upload of the LDL^T plan");
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
+  for (cudaEvent_t ev : h->lane_events)
+    if (ev) cudaEventDestroy(ev);
+  h->lane_events.assign(h->program.size(), nullptr);
+  return FC_OK;
+}
+
 int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   const int64_t ns = sym.ns, n = sym.n;
   h->n = n;
   h->ns = ns;
   h->entries = sym.entries;
   h->fp32 = h->precision == FC_PRECISION_FP32_IR;
+  h->ldlt = h->precision == FC_PRECISION_LDLT;
   h->esize = h->fp32 ? sizeof(float) : sizeof(double);
   h->nnz = (int64_t)sym.upper_idx.size();
   h->first = sym.first;
@@ -945,7 +1110,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
   UP(h->d_perm, h->perm);
   UP(h->d_toff, h->toff);
   UP(h->d_doff, h->doff);
-  if (h->fp32) {
+  if (h->fp32 || h->ldlt) {
     std::vector<int32_t> a_row(h->nnz), a_col(h->nnz);
     for (int64_t q = 0; q < h->nnz; ++q) {
       a_row[q] = sym.crow[a_src[q]];
@@ -1009,7 +1174,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       return fail_status(st, f);
     }
   }
-  return plan_factor_upload(h, st);
+  return h->ldlt ? plan_ldlt_upload(h, st) : plan_factor_upload(h, st);
 }
 
 cudaEvent_t next_event(fc_chol *h) {
@@ -1092,6 +1257,16 @@ int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *canc
 int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
   const cudaStream_t user = h->stream;
   cudaMemsetAsync(h->d_status.p, 0xff, sizeof(fc::DeviceStatus), user);
+  if (h->ldlt) {
+    // the rows' largest |A| from the values, every supernode's pivots reset, no panel done
+    cudaMemsetAsync(h->d_lscale.p, 0, sizeof(double) * (size_t)std::max<int64_t>(h->n, 1), user);
+    cudaMemsetAsync(h->d_lpos.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(h->ns, 1), user);
+    cudaMemsetAsync(h->d_ltwos.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(h->ns, 1), user);
+    cudaMemsetAsync(h->d_lfailed.p, 0xff, sizeof(unsigned long long), user);
+    fc::ldlt::launch_reset(h->n, h->d_llocal.as<int32_t>(), h->d_lorder.as<int32_t>(), h->d_lpivots.as<int8_t>(), user);
+    fc::ldlt::launch_scale(h->nnz, h->d_a_src.as<int64_t>(), h->d_a_row.as<int32_t>(), h->d_a_col.as<int32_t>(), d_val,
+                           h->d_lscale.as<unsigned long long>(), user);
+  }
   if (h->fp32) fc::launch_scale(h->n, h->d_diag_src.as<int64_t>(), d_val, h->d_scale.as<double>(), user);
   const fc::GemmKind gk = h->fp32 ? fc::GemmKind::F32_TF32X3 : fc::GemmKind::F64;
   const fc::Tree &t = h->tree;
@@ -1150,6 +1325,11 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
                         h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st);
         break;
       case K_GEMM_F64: fc::launch_gemm(h->d_gemm.as<fc::GemmTask>() + l.off, l.count, fc::GemmKind::F64, st); break;
+      case K_LDLT_PANEL:
+        fc::ldlt::launch_panel(h->d_lpanel.as<fc::ldlt::PanelTask>() + l.off, l.count, h->d_lpos.as<int32_t>(),
+                               h->d_ltwos.as<int32_t>(), h->d_lfailed.as<unsigned long long>(), st);
+        break;
+      case K_LDLT_AFTER: fc::ldlt::launch_after(h->d_lafter.as<fc::ldlt::AfterTask>() + l.off, l.count, st); break;
     }
     if (lanes && l.record) cudaEventRecord(h->lane_events[li], st);
     ++launches;
@@ -1174,8 +1354,26 @@ int read_status(fc_chol *h, fc_status *st) {
     set_status(st, FC_NOT_POSITIVE_DEFINITE, orig, 0, 0, "the pivot is not positive (relative to the diagonal)");
     return FC_NOT_POSITIVE_DEFINITE;
   }
+  if (h->ldlt) {
+    unsigned long long failed = ULLONG_MAX;
+    e = cudaMemcpy(&failed, h->d_lfailed.p, sizeof(failed), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(st, e, "factorisation");
+    if (failed != ULLONG_MAX) {
+      const int64_t col = (int64_t)failed;
+      set_status(st, FC_SINGULAR, col < h->n ? h->perm[col] : col, 0, 0,
+                 "no pivot in the column's supernode exceeds the tolerance (singular to working precision)");
+      return FC_SINGULAR;
+    }
+  }
   set_status(st, FC_OK);
   return FC_OK;
+}
+
+// The LDL^T factor's solve is not built yet: its solves are refused.
+bool ldlt_refused(const fc_chol *h, fc_status *st) {
+  if (!h->ldlt) return false;
+  set_status(st, FC_INVALID_ARGUMENT, -1, 0, 0, "the LDL^T factor has no device solve yet");
+  return true;
 }
 
 // The solve's program for R right-hand sides (built once per R). Forward, level by level: a thin
@@ -2297,7 +2495,8 @@ int fc_symbolic_import(const fc_symbolic_arrays *in, fc_symbolic **out, fc_statu
 }
 
 int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **out, fc_status *status) {
-  if (!sym || !out || (precision != FC_PRECISION_FP64 && precision != FC_PRECISION_FP32_IR)) {
+  if (!sym || !out ||
+      (precision != FC_PRECISION_FP64 && precision != FC_PRECISION_FP32_IR && precision != FC_PRECISION_LDLT)) {
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null argument or unknown precision");
     return FC_INVALID_ARGUMENT;
   }
@@ -2485,7 +2684,7 @@ int fc_chol_factor_device(fc_chol *h, const double *d_upper_val, int64_t nnz, fc
 int64_t fc_chol_entries(const fc_chol *h) { return h ? h->entries : -1; }
 
 int fc_chol_solve_device_async(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld) {
-  if (!h || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) return FC_INVALID_ARGUMENT;
+  if (!h || h->ldlt || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) return FC_OK;
   std::lock_guard<std::mutex> g(h->lock);
   cudaSetDevice(h->device);
@@ -2499,6 +2698,7 @@ int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_s
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
+  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;
@@ -2520,6 +2720,7 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
+  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;
@@ -2611,6 +2812,7 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
+  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;
@@ -2751,6 +2953,7 @@ int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *st
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
+  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;
@@ -2788,6 +2991,31 @@ int fc_chol_values(fc_chol *h, double *dst, fc_status *status) {
     set_status(status, FC_OK);
     return FC_OK;
   }
+  if (h->ldlt) {
+    // L as the fronts hold it (own blocks unit lower), D put back on their diagonals and at the
+    // 2 x 2 pivots' first subdiagonal entries: the reference's Block::values
+    std::vector<double> rect((size_t)std::max<int64_t>(h->l_len, 1)), d(h->n), sub(h->n);
+    std::vector<int8_t> piv(h->n);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(rect.data(), h->d_L.p, sizeof(double) * (size_t)h->l_len, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(d.data(), h->d_ldd.p, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(sub.data(), h->d_lde.p, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(piv.data(), h->d_lpivots.p, (size_t)h->n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(status, e, "values");
+    int64_t at = 0;
+    for (int64_t s = 0; s < h->ns; ++s) {
+      const int64_t m = h->height[s], w = h->width[s], f = h->first[s];
+      const double *F = rect.data() + h->loff[s];
+      for (int64_t c = 0; c < w; ++c) {
+        for (int64_t r = c; r < m; ++r) dst[at + r - c] = F[r + c * m];
+        dst[at] = d[f + c];
+        if (piv[f + c] == fc::ldlt::PIVOT_FIRST && c + 1 < m) dst[at + 1] = sub[f + c];
+        at += m - c;
+      }
+    }
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
   DeviceBuf tmp;
   if (tmp.alloc(sizeof(double) * (size_t)h->entries) != cudaSuccess) {
     set_status(status, FC_OUT_OF_MEMORY, -1, h->entries, 0, "device memory for the copy");
@@ -2797,6 +3025,53 @@ int fc_chol_values(fc_chol *h, double *dst, fc_status *status) {
   cudaError_t e = cudaMemcpyAsync(dst, tmp.p, sizeof(double) * h->entries, cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return cuda_fail(status, e, "values");
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_inertia(fc_chol *h, int64_t *positive, int64_t *negative, int64_t *two_by_two, fc_status *status) {
+  if (!h || !positive || !negative || !two_by_two) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null argument");
+    return FC_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  if (!h->ldlt) {  // a Cholesky factor's matrix is positive definite (ldlt.rs:500-506)
+    *positive = h->n, *negative = 0, *two_by_two = 0;
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  cudaSetDevice(h->device);
+  std::vector<double> d(h->n), sub(h->n);
+  std::vector<int8_t> piv(h->n);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess && h->n > 0) e = cudaMemcpy(d.data(), h->d_ldd.p, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && h->n > 0) e = cudaMemcpy(sub.data(), h->d_lde.p, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && h->n > 0) e = cudaMemcpy(piv.data(), h->d_lpivots.p, (size_t)h->n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(status, e, "inertia");
+  // Sylvester's law on D (ldlt.rs:415-447): a 1 x 1 pivot by its sign; a 2 x 2 one has one of
+  // each sign when its determinant is negative, else both of the sign of its trace
+  int64_t pos = 0, neg = 0, twos = 0;
+  for (int64_t c = 0; c < h->n;) {
+    if (piv[c] == fc::ldlt::PIVOT_FIRST && c + 1 < h->n) {
+      const double d11 = d[c], d21 = sub[c], d22 = d[c + 1];
+      const double det = d11 * d22 - d21 * d21;
+      if (det < 0.0)
+        pos += 1, neg += 1;
+      else if (d11 + d22 > 0.0)
+        pos += 2;
+      else
+        neg += 2;
+      twos += 1;
+      c += 2;
+    } else {
+      if (d[c] > 0.0)
+        pos += 1;
+      else
+        neg += 1;
+      c += 1;
+    }
+  }
+  *positive = pos, *negative = neg, *two_by_two = twos;
   set_status(status, FC_OK);
   return FC_OK;
 }

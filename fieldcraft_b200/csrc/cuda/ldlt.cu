@@ -4,8 +4,7 @@
 // the device's block (threads, __syncthreads) and its per-supernode state.
 #include <cstdint>
 
-#include "cuda/kernels.cuh"
-#include "cuda/ldlt_panel.cuh"
+#include "cuda/ldlt_launch.cuh"
 
 namespace fc {
 namespace ldlt {
@@ -14,17 +13,6 @@ struct DeviceBlock {
   __device__ int tid() const { return threadIdx.x; }
   __device__ int size() const { return blockDim.x; }
   __device__ void sync() { __syncthreads(); }
-};
-
-// One front's panel step: the front and its state (Front), where its columns start in the
-// analysis' postorder (`first`, for the failing column's name), and the GEMM tasks of the update
-// of its later own columns (`slots`, `nslots` of them: update_tiles for the earliest end).
-struct PanelTask {
-  Front front;
-  int64_t first;
-  fc::GemmTask *slots;
-  int32_t nslots;
-  int32_t s;
 };
 
 // Per supernode s: pos[s] is where its next panel starts (w when done), twos[s] counts its 2 x 2
@@ -83,15 +71,6 @@ __global__ void __launch_bounds__(MAX_THREADS) ldlt_panel_kernel(const PanelTask
   if (threadIdx.x == 0) pos[task.s] = end;
 }
 
-// After a level's panels, per front (one CTA each): W21 = L21 D into w21[s] (leading dimension
-// m - w, for the update-matrix GEMM), then D out of the front into d / e at the front's first
-// postorder column (split_d), leaving its own block unit lower for the solve.
-struct AfterTask {
-  Front front;
-  double *w21;
-  double *d, *e;
-};
-
 __global__ void __launch_bounds__(MAX_THREADS) ldlt_after_kernel(const AfterTask *__restrict__ tasks) {
   const AfterTask &task = tasks[blockIdx.x];
   DeviceBlock blk;
@@ -105,6 +84,60 @@ __global__ void ldlt_d_inverse_kernel(int64_t n, int R, const double *__restrict
                                       const int8_t *__restrict__ pivots, double *__restrict__ y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     apply_d_inverse(i, R, d, e, pivots, y);
+}
+
+// Lower.scale (cholesky.rs:1392-1416): each entry's magnitude to its row's and its column's
+// largest, as the bits of non-negative doubles (ordered as integers); a NaN changes nothing, as
+// in f64::max. scale_bits starts at zero.
+__global__ void ldlt_scale_kernel(int64_t nnz, const int64_t *__restrict__ a_src, const int32_t *__restrict__ a_row,
+                                  const int32_t *__restrict__ a_col, const double *__restrict__ val,
+                                  unsigned long long *__restrict__ scale_bits) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x) {
+    const double v = fabs(val[a_src[q]]);
+    if (isnan(v)) continue;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    atomicMax(scale_bits + a_row[q], b);
+    atomicMax(scale_bits + a_col[q], b);
+  }
+}
+
+// Each supernode's pivots start as its columns in order, every one a 1 x 1 pivot.
+__global__ void ldlt_reset_kernel(int64_t n, const int32_t *__restrict__ local, int32_t *__restrict__ order,
+                                  int8_t *__restrict__ pivots) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    order[i] = local[i];
+    pivots[i] = PIVOT_ONE;
+  }
+}
+
+namespace {
+int grid_for(int64_t count, int threads) {
+  const int64_t blocks = (count + threads - 1) / threads;
+  return (int)(blocks < 4096 ? (blocks > 0 ? blocks : 1) : 4096);
+}
+}  // namespace
+
+void launch_panel(const PanelTask *tasks, int count, int32_t *pos, int32_t *twos, unsigned long long *failed,
+                  cudaStream_t st) {
+  if (count > 0) ldlt_panel_kernel<<<count, MAX_THREADS, 0, st>>>(tasks, pos, twos, failed);
+}
+
+void launch_after(const AfterTask *tasks, int count, cudaStream_t st) {
+  if (count > 0) ldlt_after_kernel<<<count, MAX_THREADS, 0, st>>>(tasks);
+}
+
+void launch_scale(int64_t nnz, const int64_t *a_src, const int32_t *a_row, const int32_t *a_col, const double *val,
+                  unsigned long long *scale_bits, cudaStream_t st) {
+  if (nnz > 0) ldlt_scale_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, a_src, a_row, a_col, val, scale_bits);
+}
+
+void launch_reset(int64_t n, const int32_t *local, int32_t *order, int8_t *pivots, cudaStream_t st) {
+  if (n > 0) ldlt_reset_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, local, order, pivots);
+}
+
+void launch_d_inverse(int64_t n, int R, const double *d, const double *e, const int8_t *pivots, double *y,
+                      cudaStream_t st) {
+  if (n > 0) ldlt_d_inverse_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, R, d, e, pivots, y);
 }
 
 }  // namespace ldlt

@@ -16,9 +16,11 @@
 
 #if defined(__CUDACC__)
 #define FC_LDLT_FN __device__ __forceinline__
+#define FC_LDLT_HD __host__ __device__ __forceinline__  // arithmetic the host plan shares
 #else
 #include <cmath>
 #define FC_LDLT_FN inline
+#define FC_LDLT_HD inline
 #endif
 
 namespace fc {
@@ -368,7 +370,7 @@ struct Tile {
 };
 constexpr int TILE_ROWS = 64;
 
-FC_LDLT_FN bool update_tile(int64_t m, int w, int c1, int64_t slot, Tile &t) {
+FC_LDLT_HD bool update_tile(int64_t m, int w, int c1, int64_t slot, Tile &t) {
   for (int j0 = c1; j0 < w; j0 += TILE_ROWS) {
     const int64_t rows = (m - j0 + TILE_ROWS - 1) / TILE_ROWS;
     if (slot < rows) {
@@ -386,7 +388,7 @@ FC_LDLT_FN bool update_tile(int64_t m, int w, int c1, int64_t slot, Tile &t) {
 
 // The tiles of that update: at most this many for a panel that ends at c1 or later (the count
 // falls as c1 grows), so a plan sized for the earliest end holds every case.
-FC_LDLT_FN int64_t update_tiles(int64_t m, int w, int c1) {
+FC_LDLT_HD int64_t update_tiles(int64_t m, int w, int c1) {
   int64_t count = 0;
   for (int j0 = c1; j0 < w; j0 += TILE_ROWS) count += (m - j0 + TILE_ROWS - 1) / TILE_ROWS;
   return count;

@@ -37,6 +37,11 @@ extern "C" {
 /* Precision of the numeric phase. */
 #define FC_PRECISION_FP64 0
 #define FC_PRECISION_FP32_IR 1 /* FP32 factor of S A S, every diagonal block in FP64; FP64 refinement */
+/* FP64 symmetric indefinite P A P^T = L D L^T (LdltFactor, crates/solver/src/ldlt.rs): bounded
+ * Bunch-Kaufman pivots inside supernodes, on the same analysis. This build factors only: its
+ * values (fc_chol_values, the reference's Block::values) and inertia (fc_chol_inertia); its solves
+ * return FC_INVALID_ARGUMENT. A column with no pivot is FC_SINGULAR (FactorError::Singular). */
+#define FC_PRECISION_LDLT 2
 
 typedef struct fc_status {
   int32_t code;
@@ -138,6 +143,9 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
  * trapezoid by columns (column c holds rows c..m, cholesky.rs:418-425, 1534-1542). dst has
  * fc_chol_entries(h) doubles. */
 int fc_chol_values(fc_chol *h, double *dst, fc_status *status);
+/* LdltFactor::inertia and two_by_two (ldlt.rs:399-447): the counts of positive and negative
+ * eigenvalues of A (Sylvester's law on D) and of 2 x 2 pivots; a Cholesky factor's are (n, 0, 0). */
+int fc_chol_inertia(fc_chol *h, int64_t *positive, int64_t *negative, int64_t *two_by_two, fc_status *status);
 
 /* Solve A x = b to a relative residual in FP64 around the handle's factor (the mixed-precision
  * mode's FP32 factor of S A S, or the FP64 factor) as the preconditioner M: by default conjugate
