@@ -110,12 +110,32 @@ __global__ void ldlt_reset_kernel(int64_t n, const int32_t *__restrict__ local, 
   }
 }
 
+__global__ void __launch_bounds__(64) ldlt_inverse_kernel(const InverseTask *__restrict__ tasks) {
+  const InverseTask &t = tasks[blockIdx.x];
+  DeviceBlock blk;
+  unit_lower_inverse(blk, t.L, t.ldl, t.nb, t.X, t.ldx);
+}
+
+__global__ void __launch_bounds__(MAX_THREADS) ldlt_permute_kernel(const PermuteTask *__restrict__ tasks) {
+  const PermuteTask &t = tasks[blockIdx.x];
+  DeviceBlock blk;
+  permute_rows_below(blk, t.front, t.from, t.tmp);
+}
+
 namespace {
 int grid_for(int64_t count, int threads) {
   const int64_t blocks = (count + threads - 1) / threads;
   return (int)(blocks < 4096 ? (blocks > 0 ? blocks : 1) : 4096);
 }
 }  // namespace
+
+void launch_inverse(const InverseTask *tasks, int count, cudaStream_t st) {
+  if (count > 0) ldlt_inverse_kernel<<<count, 64, 0, st>>>(tasks);
+}
+
+void launch_permute(const PermuteTask *tasks, int count, cudaStream_t st) {
+  if (count > 0) ldlt_permute_kernel<<<count, MAX_THREADS, 0, st>>>(tasks);
+}
 
 void launch_panel(const PanelTask *tasks, int count, int32_t *pos, int32_t *twos, unsigned long long *failed,
                   cudaStream_t st) {

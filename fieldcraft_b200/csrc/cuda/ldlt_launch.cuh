@@ -31,6 +31,25 @@ struct AfterTask {
   double *d, *e;
 };
 
+// The solve's 64 x 64 inverse of one unit lower diagonal block: L (leading dimension ldl, nb
+// columns) into X (leading dimension ldx) in the inverse arena.
+struct InverseTask {
+  const double *L;
+  double *X;
+  int64_t ldl, ldx;
+  int32_t nb, pad;
+};
+
+// A front's rows below its own columns put in the solve's order (row w + i takes old row
+// w + from[i]), through `tmp` (m - w entries).
+struct PermuteTask {
+  Front front;
+  const int32_t *from;
+  double *tmp;
+};
+
+void launch_inverse(const InverseTask *tasks, int count, cudaStream_t st);
+void launch_permute(const PermuteTask *tasks, int count, cudaStream_t st);
 void launch_panel(const PanelTask *tasks, int count, int32_t *pos, int32_t *twos, unsigned long long *failed,
                   cudaStream_t st);
 void launch_after(const AfterTask *tasks, int count, cudaStream_t st);

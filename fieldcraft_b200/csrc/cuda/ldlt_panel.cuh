@@ -359,6 +359,39 @@ FC_LDLT_FN void apply_d_inverse(int64_t i, int R, const double *d, const double 
   }
 }
 
+// X = L^-1 for an nb x nb unit lower block of a front (nb <= 64; L's diagonal is not read),
+// column-major with leading dimension ldx: column j by forward substitution, x_i = -sum over
+// k in [j, i) of L(i, k) x_k, summed in k order from zero. One thread per column; the strictly
+// upper part of X is left as it is (zero in the solve's inverse arena).
+template <class Block>
+FC_LDLT_FN void unit_lower_inverse(Block &blk, const double *Lb, int64_t ldl, int nb, double *X, int64_t ldx) {
+  for (int j = blk.tid(); j < nb; j += blk.size()) {
+    double *x = X + (int64_t)j * ldx;
+    x[j] = 1.0;
+    for (int i = j + 1; i < nb; ++i) {
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s = add(s, mul(Lb[i + (int64_t)k * ldl], x[k]));
+      x[i] = -s;
+    }
+  }
+  blk.sync();
+}
+
+// Rows [w, m) of every own column of a front put in a new order: row w + i takes the old row
+// w + from[i] (from: a permutation of [0, m - w)). One column at a time through `tmp` (m - w
+// entries), threads over its rows.
+template <class Block>
+FC_LDLT_FN void permute_rows_below(Block &blk, const Front &f, const int32_t *from, double *tmp) {
+  const int64_t u = f.m - f.w;
+  for (int c = 0; c < f.w; ++c) {
+    double *col = f.F + f.w + (int64_t)c * f.m;
+    for (int64_t i = blk.tid(); i < u; i += blk.size()) tmp[i] = col[from[i]];
+    blk.sync();
+    for (int64_t i = blk.tid(); i < u; i += blk.size()) col[i] = tmp[i];
+    blk.sync();
+  }
+}
+
 // The update of the later own columns by a panel that ended at c1, as tiles of at most 64 x 64:
 // the front's rows [c1, m) of its columns [c1, w), lower part only; column blocks of 64 from c1,
 // in each the row blocks from the diagonal down. Tile `slot` of that list, or false past its end.

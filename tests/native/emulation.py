@@ -35,6 +35,10 @@ def load():
                                         C.c_int]
         _lib.emu_apply_d_inverse.restype = None
         _lib.emu_apply_d_inverse.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.emu_unit_lower_inverse.restype = C.c_int
+        _lib.emu_unit_lower_inverse.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_int]
+        _lib.emu_permute_rows_below.restype = C.c_int
+        _lib.emu_permute_rows_below.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         _lib.emu_update_tiles.restype = C.c_int64
         _lib.emu_update_tiles.argtypes = [C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_int64]
@@ -93,3 +97,19 @@ def apply_d_inverse(d, e, pivots, y):
                                np.ascontiguousarray(e).ctypes.data, np.ascontiguousarray(pivots, np.int8).ctypes.data,
                                y.ctypes.data)
     return y
+
+
+def unit_lower_inverse(Lb: np.ndarray, threads: int) -> np.ndarray:
+    """X = Lb^-1 for a unit lower block (its diagonal not read), zero above the diagonal."""
+    nb = Lb.shape[0]
+    L = np.asfortranarray(Lb, np.float64)
+    X = np.zeros((nb, nb), order="F")
+    assert load().emu_unit_lower_inverse(L.ctypes.data, nb, nb, X.ctypes.data, nb, threads) == 0
+    return X
+
+
+def permute_rows_below(F: np.ndarray, w: int, frm: np.ndarray, threads: int) -> np.ndarray:
+    G = np.asfortranarray(F, np.float64).copy(order="F")
+    frm = np.ascontiguousarray(frm, np.int32)
+    assert load().emu_permute_rows_below(G.shape[0], w, G.ctypes.data, frm.ctypes.data, threads) == 0
+    return G

@@ -187,3 +187,42 @@ void emu_apply_d_inverse(int64_t n, int R, const double *d, const double *e, con
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// X = L^-1 of a unit lower nb x nb block (column-major, leading dimensions ldl and ldx) on
+// `threads` host threads. Returns 0, or -3 on a divergence.
+int emu_unit_lower_inverse(const double *Lb, int64_t ldl, int nb, double *X, int64_t ldx, int threads) {
+  if (threads < 1 || threads > MAX_EMULATED) return -2;
+  Checks checks;
+  for (int t = 0; t < threads; ++t) checks.count[t] = 0;
+  Barrier barrier(threads);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&, t] {
+      HostBlock blk{t, threads, &barrier, &checks, std::mt19937((uint32_t)t)};
+      fc::ldlt::unit_lower_inverse(blk, Lb, ldl, nb, X, ldx);
+    });
+  for (auto &th : pool) th.join();
+  return checks.diverged ? -3 : 0;
+}
+
+// The rows below the own columns of an m x w front permuted (row w + i takes old row w + from[i]).
+int emu_permute_rows_below(int64_t m, int w, double *F, const int32_t *from, int threads) {
+  if (threads < 1 || threads > MAX_EMULATED) return -2;
+  Checks checks;
+  for (int t = 0; t < threads; ++t) checks.count[t] = 0;
+  Barrier barrier(threads);
+  std::vector<double> tmp((size_t)(m - w > 0 ? m - w : 1));
+  fc::ldlt::Front f{F, m, w, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&, t] {
+      HostBlock blk{t, threads, &barrier, &checks, std::mt19937((uint32_t)t)};
+      fc::ldlt::permute_rows_below(blk, f, from, tmp.data());
+    });
+  for (auto &th : pool) th.join();
+  return checks.diverged ? -3 : 0;
+}
+
+}  // extern "C"

@@ -233,3 +233,34 @@ def test_w21_split_and_d_inverse():
             ref[c] = y[c] / d[c]
             c += 1
     assert np.array_equal(bits(got), bits(ref))
+
+
+@pytest.mark.parametrize("nb", [1, 2, 17, 64])
+def test_unit_lower_inverse(nb):
+    """The solve's 64 x 64 diagonal-block inverses of the unit lower L: each column by forward
+    substitution in k order (bit for bit the loop below), and L X = I to rounding."""
+    rng = np.random.default_rng(nb)
+    L = np.tril(rng.standard_normal((nb, nb)) * 0.3, -1) + np.diag(rng.standard_normal(nb) * 7)  # diagonal ignored
+    X = E.unit_lower_inverse(L, threads=5)
+    want = np.zeros((nb, nb))
+    for j in range(nb):
+        want[j, j] = 1.0
+        for i in range(j + 1, nb):
+            s = 0.0
+            for k in range(j, i):
+                s = s + L[i, k] * want[k, j]
+            want[i, j] = -s
+    assert np.array_equal(bits(X), bits(want))
+    Lu = np.tril(L, -1) + np.eye(nb)
+    assert np.max(np.abs(Lu @ X - np.eye(nb))) < 1e-12
+
+
+def test_rows_below_permuted():
+    """A front's rows below its own columns reordered in place, every own column the same way."""
+    rng = np.random.default_rng(2)
+    m, w = 200, 70
+    F = rng.standard_normal((m, w))
+    frm = rng.permutation(m - w)
+    G = E.permute_rows_below(F, w, frm, threads=7)
+    assert np.array_equal(G[:w], F[:w])
+    assert np.array_equal(G[w:], F[w:][frm])
