@@ -25,6 +25,7 @@
 #include "cuda/kernels.cuh"
 #include "cuda/ldlt_launch.cuh"
 #include "device_buf.hpp"
+#include "host/ldlt_fold.hpp"
 #include "host/symbolic.hpp"
 
 struct fc_symbolic {
@@ -2333,6 +2334,21 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 extern "C" {
 
 const char *fc_version(void) { return "fieldcraft-b200 0.1.0 (sm_100a)"; }
+
+// Not part of the public ABI: the LDL^T solve's structure folding (host/ldlt_fold.cpp) on a
+// caller's arrays, for tests. Outputs: perm_out[n], rows_out[rptr[ns]], from_out (the rows-below
+// count), rel_out (the same count less the roots'). Returns 0, or -1 on inconsistent input.
+int fc_test_ldlt_fold(int64_t n, int64_t ns, const int64_t *first, const int64_t *rptr, const int32_t *rows,
+                      const int64_t *perm, const int64_t *sparent, const int32_t *order, int64_t *perm_out,
+                      int32_t *rows_out, int32_t *from_out, int32_t *rel_out) {
+  fc::LdltFold f;
+  if (!fc::ldlt_fold(n, ns, first, rptr, rows, perm, sparent, order, f)) return -1;
+  std::copy(f.perm.begin(), f.perm.end(), perm_out);
+  std::copy(f.rows.begin(), f.rows.end(), rows_out);
+  std::copy(f.from.begin(), f.from.end(), from_out);
+  std::copy(f.rel.begin(), f.rel.end(), rel_out);
+  return 0;
+}
 
 int fc_symbolic_analyse(int64_t n, const int64_t *ptr, const int32_t *idx, uint64_t max_entries, fc_symbolic **out,
                         fc_status *status) {
