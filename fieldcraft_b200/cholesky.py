@@ -320,8 +320,8 @@ class Inertia:
 
 class LdltFactor(Factor):
     """The symmetric indefinite factor P A P^T = L D L^T on the GPU (LdltFactor, ldlt.rs:365-447):
-    bounded Bunch-Kaufman pivots inside the supernodes of the same analysis. Factors, values and
-    inertia; the device solve is not built yet, so solves raise ValueError."""
+    bounded Bunch-Kaufman pivots inside the supernodes of the same analysis. Factors, values,
+    inertia, solve and solve_many (level by level; the refined solve is the Cholesky factor's)."""
 
     def __init__(self, symbolic: Symbolic, device: int = 0):
         super().__init__(symbolic, LDLT, device)

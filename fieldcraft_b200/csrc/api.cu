@@ -53,7 +53,8 @@ enum Kind {
   K_SOLVE_THIN_FWD, K_SOLVE_THIN_BWD,  // the thin supernodes' steps of a solve level
   K_PACK_TC,                           // the tcgen05 products' operands packed (K-major hi | lo)
   K_LDLT_PANEL,                        // LDL^T: pivoted panel steps (they write the next GEMM's tasks)
-  K_LDLT_AFTER                         // LDL^T: W21 = L21 D and D out of the fronts
+  K_LDLT_AFTER,                        // LDL^T: W21 = L21 D and D out of the fronts
+  K_LDLT_INVERSE                       // LDL^T: the 64 x 64 inverses of the unit lower diagonal blocks
 };
 
 struct Launch {
@@ -114,7 +115,16 @@ struct fc_chol {
   // counts, the first singular column, per-level scratch, D (diagonal, subdiagonal), the tasks
   bool ldlt = false;
   DeviceBuf d_lscale, d_llocal, d_lorder, d_lpivots, d_lpos, d_ltwos, d_lfailed, d_lscratch, d_ldd, d_lde;
-  DeviceBuf d_lpanel, d_lafter;
+  DeviceBuf d_lpanel, d_lafter, d_linv;
+  // the LDL^T solve's structure: the pivot orders folded in after each factorisation (host/
+  // ldlt_fold.cpp), its rows, relative maps and permutation on the device, the L21 rows' move;
+  // the structure's own rows and maps kept for the next fold; the tree the solve's kernels read
+  bool ldlt_folded = false;
+  std::vector<int32_t> ldlt_rows0, ldlt_rel0;
+  std::vector<int64_t> ldlt_sparent, ldlt_from_off;
+  std::vector<int32_t> ldlt_from;
+  DeviceBuf d_lsrows, d_lsrel, d_lsperm, d_lfrom, d_ltmp, d_lperm_t;
+  fc::Tree stree{};
   fc::Tree tree{};
   std::vector<Launch> program;
   cudaStream_t side = nullptr;            // lane 1 of the factorisation (see Launch), lowest priority
@@ -831,6 +841,14 @@ int plan_ldlt_upload(fc_chol *h, fc_status *st) {
   std::vector<L::PanelTask> pan_t;
   std::vector<int64_t> pan_slot;  // each panel task's first slot in gemm_t (its pointer set at upload)
   std::vector<L::AfterTask> aft_t;
+  std::vector<L::InverseTask> inv_t;
+  // the structure's rows and relative maps (the solve's are folded from them after each
+  // factorisation) and the supernodal tree's parents
+  h->ldlt_rows0 = h->rows;
+  h->ldlt_rel0 = h->rel;
+  h->ldlt_sparent.assign(h->ns, -1);
+  for (int64_t s = 0; s < h->ns; ++s)
+    for (int64_t q = h->kid_ptr[s]; q < h->kid_ptr[s + 1]; ++q) h->ldlt_sparent[h->kids[q]] = s;
   for (size_t l = 0; l < lv.size(); ++l) {
     const auto &S = lv[l];
     int64_t off = (int64_t)asm_t.size();
@@ -891,6 +909,35 @@ int plan_ldlt_upload(fc_chol *h, fc_status *st) {
       aft_t.push_back({fronts[q], w21[q], h->d_ldd.as<double>() + f, h->d_lde.as<double>() + f});
     }
     push(h->program, K_LDLT_AFTER, ao, (int64_t)aft_t.size() - ao, (int)l);
+    // the solve's diagonal-block inverses: 64 x 64 ones of the unit lower own blocks, then the
+    // doubling to blocks of up to SB columns (as the Cholesky factor's, from its panels' inverses)
+    const int64_t io = (int64_t)inv_t.size();
+    for (int64_t s : S) {
+      const int m = h->height[s], w = h->width[s];
+      for (int c0 = 0; c0 < w; c0 += L::PANEL) {
+        int bw;
+        const int64_t ib = inv_block(h, s, c0 / fc::SB, bw), in = c0 % fc::SB;
+        L::InverseTask t{};
+        t.L = Lp(h->loff[s] + c0 + (int64_t)c0 * m);
+        t.ldl = m;
+        t.X = h->d_Dinv.as<double>() + ib + in + in * bw;
+        t.ldx = bw;
+        t.nb = std::min(L::PANEL, w - c0);
+        inv_t.push_back(t);
+      }
+    }
+    push(h->program, K_LDLT_INVERSE, io, (int64_t)inv_t.size() - io, (int)l);
+    for (int hh = fc::NB; hh < fc::SB; hh *= 2) {
+      std::vector<fc::GemmTask> first_t, second_t;
+      inverse_doubling(h, S, h->d_T.as<double>(), hh, &first_t, &second_t);
+      if (first_t.empty()) break;
+      int64_t d0 = (int64_t)gemm_t.size();
+      gemm_t.insert(gemm_t.end(), first_t.begin(), first_t.end());
+      push(h->program, K_GEMM_MIXED, d0, (int64_t)first_t.size(), (int)l);
+      d0 = (int64_t)gemm_t.size();
+      gemm_t.insert(gemm_t.end(), second_t.begin(), second_t.end());
+      push(h->program, K_GEMM_F64, d0, (int64_t)second_t.size(), (int)l);
+    }
     // the update matrices: U = -L21 W21^T (lower tiles)
     const int64_t go = (int64_t)gemm_t.size();
     for (size_t q = 0; q < S.size(); ++q) {
@@ -923,7 +970,8 @@ int plan_ldlt_upload(fc_chol *h, fc_status *st) {
       (e = upload(h->d_gemm, gemm_t, stream)) != cudaSuccess)
     return cuda_fail(st, e, "upload of the LDL^T plan");
   for (size_t q = 0; q < pan_t.size(); ++q) pan_t[q].slots = h->d_gemm.as<fc::GemmTask>() + pan_slot[q];
-  if ((e = upload(h->d_lpanel, pan_t, stream)) != cudaSuccess || (e = upload(h->d_lafter, aft_t, stream)) != cudaSuccess)
+  if ((e = upload(h->d_lpanel, pan_t, stream)) != cudaSuccess || (e = upload(h->d_lafter, aft_t, stream)) != cudaSuccess ||
+      (e = upload(h->d_linv, inv_t, stream)) != cudaSuccess)
     return cuda_fail(st, e, "upload of the LDL^T plan");
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(st, e, "plan upload");
   for (cudaEvent_t ev : h->lane_events)
@@ -1241,6 +1289,7 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
 // Enqueues the factor's program (as a replayed graph when it can). Returns FC_CANCELLED when the
 // flag was set between levels.
 int enqueue_factor(fc_chol *h, const double *d_val, const volatile int32_t *cancel) {
+  h->ldlt_folded = false;
   if (cancel || h->profiling || !h->graphs) return enqueue_factor_direct(h, d_val, cancel);
   if (!h->factor_graph || h->factor_graph_val != d_val || h->factor_graph_stream != h->stream) {
     if (!capture(h, &h->factor_graph, [&] { enqueue_factor_direct(h, d_val, nullptr); })) {
@@ -1331,6 +1380,7 @@ int enqueue_factor_direct(fc_chol *h, const double *d_val, const volatile int32_
                                h->d_ltwos.as<int32_t>(), h->d_lfailed.as<unsigned long long>(), st);
         break;
       case K_LDLT_AFTER: fc::ldlt::launch_after(h->d_lafter.as<fc::ldlt::AfterTask>() + l.off, l.count, st); break;
+      case K_LDLT_INVERSE: fc::ldlt::launch_inverse(h->d_linv.as<fc::ldlt::InverseTask>() + l.off, l.count, st); break;
     }
     if (lanes && l.record) cudaEventRecord(h->lane_events[li], st);
     ++launches;
@@ -1370,11 +1420,72 @@ int read_status(fc_chol *h, fc_status *st) {
   return FC_OK;
 }
 
-// The LDL^T factor's solve is not built yet: its solves are refused.
+// The LDL^T factor solves level by level only (not refined, not without allocation, not
+// persistent): those paths are refused for it.
 bool ldlt_refused(const fc_chol *h, fc_status *st) {
   if (!h->ldlt) return false;
-  set_status(st, FC_INVALID_ARGUMENT, -1, 0, 0, "the LDL^T factor has no device solve yet");
+  set_status(st, FC_INVALID_ARGUMENT, -1, 0, 0, "the LDL^T factor solves through fc_chol_solve(_device) only");
   return true;
+}
+
+// The LDL^T solve's structure, once per factorisation: the pivot orders read back and folded
+// into the structure (host/ldlt_fold.cpp), the solve's rows, relative maps and permutation
+// uploaded, each front's rows below moved to their new order, and the solve's plan dropped (the
+// next solve plans on the folded structure). Its own blocks are unit lower (split_d), so the
+// Cholesky solve then runs on them as it is, with D^-1 between its passes.
+int ldlt_prepare_solve(fc_chol *h, fc_status *st) {
+  if (h->ldlt_folded) return FC_OK;
+  const int64_t n = h->n, ns = h->ns;
+  std::vector<int32_t> order(n);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess && n > 0)
+    e = cudaMemcpy(order.data(), h->d_lorder.p, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(st, e, "the LDL^T factor's pivot orders");
+  std::vector<int64_t> rptr(h->rows_off.begin(), h->rows_off.end());
+  rptr.push_back((int64_t)h->ldlt_rows0.size());
+  if (ns == 0) rptr.assign(1, 0);
+  fc::LdltFold fold;
+  if (!fc::ldlt_fold(n, ns, h->first.data(), rptr.data(), h->ldlt_rows0.data(), h->perm.data(), h->ldlt_sparent.data(),
+                     order.data(), fold)) {
+    set_status(st, FC_INTERNAL, -1, 0, 0, "the LDL^T factor's pivot orders are not permutations");
+    return FC_INTERNAL;
+  }
+  std::vector<fc::ldlt::PermuteTask> moves;
+  if ((e = upload(h->d_lsrows, fold.rows, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_lsrel, fold.rel, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_lsperm, fold.perm, h->stream)) != cudaSuccess ||
+      (e = upload(h->d_lfrom, fold.from, h->stream)) != cudaSuccess ||
+      (e = h->d_ltmp.alloc(sizeof(double) * (size_t)std::max<int64_t>(fold.from_off[ns], 1))) != cudaSuccess)
+    return cuda_fail(st, e, "the LDL^T solve's structure");
+  for (int64_t s = 0; s < ns; ++s) {
+    const int m = h->height[s], w = h->width[s];
+    if (m == w) continue;
+    fc::ldlt::PermuteTask t{};
+    t.front.F = static_cast<double *>(arena_at(h->d_L, h, h->loff[s]));
+    t.front.m = m;
+    t.front.w = w;
+    t.from = h->d_lfrom.as<int32_t>() + fold.from_off[s];
+    t.tmp = h->d_ltmp.as<double>() + fold.from_off[s];
+    moves.push_back(t);
+  }
+  if ((e = upload(h->d_lperm_t, moves, h->stream)) != cudaSuccess) return cuda_fail(st, e, "the LDL^T solve's structure");
+  fc::ldlt::launch_permute(h->d_lperm_t.as<fc::ldlt::PermuteTask>(), (int)moves.size(), h->stream);
+  if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess)
+    return cuda_fail(st, e, "the LDL^T solve's structure");
+  h->ldlt_from = std::move(fold.from);
+  h->ldlt_from_off = std::move(fold.from_off);
+  h->rows = std::move(fold.rows);  // what the solve's planner reads
+  h->rel = std::move(fold.rel);
+  h->stree = h->tree;
+  h->stree.rows = h->d_lsrows.as<int32_t>();
+  h->stree.rel = h->d_lsrel.as<int32_t>();
+  h->solve_R = 0;
+  if (h->solve_graph) {
+    cudaGraphExecDestroy(h->solve_graph);
+    h->solve_graph = nullptr;
+  }
+  h->ldlt_folded = true;
+  return FC_OK;
 }
 
 // The solve's program for R right-hand sides (built once per R). Forward, level by level: a thin
@@ -1622,7 +1733,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
           g.a_si = m, g.a_sk = 1;
           g.B = x + j0;
           g.b_sj = 1, g.b_sk = R;
-          g.b_rows = h->d_rows.as<int32_t>() + h->rows_off[s] + w;
+          g.b_rows = (h->ldlt ? h->d_lsrows : h->d_rows).as<int32_t>() + h->rows_off[s] + w;
           g.flags = 16;
           g.M = std::min(fc::GEMM_TM, w - i0), g.N = std::min(fc::GEMM_TN, R - j0), g.K = u;
           sp.add(g, es, sizeof(double), j0 == 0);
@@ -2192,7 +2303,7 @@ std::vector<char> beside(const std::vector<Launch> &prog) {
 void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveBuffers &b, int R, int64_t &launches,
                        const std::vector<cudaEvent_t> *events = nullptr, size_t *ev = nullptr) {
   const cudaStream_t main = h->stream;
-  const fc::Tree &t = h->tree;
+  const fc::Tree &t = h->ldlt ? h->stree : h->tree;
   const bool lanes = events && ev && h->side;
   const std::vector<char> side = lanes ? beside(prog) : std::vector<char>(prog.size(), 0);
   bool forked = false;
@@ -2244,6 +2355,10 @@ void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld);
 // Solves for the R right-hand sides in device memory at d_b (column-major, leading dimension ld),
 // as a replayed graph when it can.
 int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
+  if (h->ldlt) {
+    const int rc = ldlt_prepare_solve(h, st);
+    if (rc != FC_OK) return rc;
+  }
   const int before = h->solve_R;
   int rc = plan_solve(h, R, st);
   if (rc != FC_OK) return rc;
@@ -2270,7 +2385,7 @@ int enqueue_solve(fc_chol *h, double *d_b, int R, int64_t ld, fc_status *st) {
 
 void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   int64_t launches = 0;
-  if (h->dag) {
+  if (h->dag && !h->ldlt) {
     cudaMemsetAsync(h->d_dcount.p, 0, sizeof(int32_t) * (size_t)h->dag_counters, h->stream);
     cudaMemsetAsync(h->d_dctl.p, 0, sizeof(fc::DagControl), h->stream);
     fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
@@ -2289,13 +2404,20 @@ void enqueue_solve_direct(fc_chol *h, double *d_b, int R, int64_t ld) {
   const SolveBuffers b = own_buffers(h);
   // the thin backward chunks' counters start at zero (their last chunk also leaves them so)
   cudaMemsetAsync(h->d_tcount.p, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(h->solve_tcount, 1), h->stream);
-  fc::launch_permute_in(h->d_perm.as<int64_t>(), h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
+  // the LDL^T factor's solve permutes through its folded order and applies D^-1 between the passes
+  const int64_t *perm = h->ldlt ? h->d_lsperm.as<int64_t>() : h->d_perm.as<int64_t>();
+  fc::launch_permute_in(perm, h->n, d_b, ld, h->d_x.as<double>(), R, h->tree.scale, h->stream);
   // the thin launches beside the wide ones (not while profiling: then every launch is timed alone)
   const bool lanes = h->side && !h->profiling && h->solve_events.size() >= solve_events_needed(h);
   size_t ev = 0;
   run_solve_program(h, h->fwd, b, R, launches, lanes ? &h->solve_events : nullptr, &ev);
+  if (h->ldlt) {
+    fc::ldlt::launch_d_inverse(h->n, R, h->d_ldd.as<double>(), h->d_lde.as<double>(), h->d_lpivots.as<int8_t>(), b.x2,
+                               h->stream);
+    ++launches;
+  }
   run_solve_program(h, h->bwd, b, R, launches, lanes ? &h->solve_events : nullptr, &ev);
-  fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, h->d_x.as<double>(), R, d_b, ld, h->tree.scale, h->stream);
+  fc::launch_permute_out(perm, h->n, h->d_x.as<double>(), R, d_b, ld, h->tree.scale, h->stream);
   h->last_solve_launches = launches + 2;
 }
 
@@ -2534,7 +2656,7 @@ int fc_chol_create(const fc_symbolic *sym, int precision, int device, fc_chol **
     const char *mma_sync = std::getenv("FC_TF32_MMA_SYNC");
     h->tc = !(mma_sync && mma_sync[0] == '1');
     const char *persistent = std::getenv("FC_SOLVE_PERSISTENT");
-    h->dag = persistent && persistent[0] == '1';
+    h->dag = persistent && persistent[0] == '1' && precision != FC_PRECISION_LDLT;
   }
   fc::configure_kernels();
   if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -2643,7 +2765,7 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
   };
   switch (option) {
     case FC_OPTION_SOLVE_SCHEDULE:
-      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      if ((value != 0 && value != 1) || (value == 1 && h->ldlt)) return FC_INVALID_ARGUMENT;
       h->dag = value == 1;
       replan();
       return FC_OK;
@@ -2700,7 +2822,7 @@ int fc_chol_factor_device(fc_chol *h, const double *d_upper_val, int64_t nnz, fc
 int64_t fc_chol_entries(const fc_chol *h) { return h ? h->entries : -1; }
 
 int fc_chol_solve_device_async(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld) {
-  if (!h || h->ldlt || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) return FC_INVALID_ARGUMENT;
+  if (!h || nrhs < 0 || (nrhs > 0 && (!d_b || ld < h->n))) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) return FC_OK;
   std::lock_guard<std::mutex> g(h->lock);
   cudaSetDevice(h->device);
@@ -2714,7 +2836,6 @@ int fc_chol_solve_device(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld, fc_s
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
-  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;
@@ -2969,7 +3090,6 @@ int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *st
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
-  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;
@@ -3018,12 +3138,17 @@ int fc_chol_values(fc_chol *h, double *dst, fc_status *status) {
     if (e == cudaSuccess) e = cudaMemcpy(sub.data(), h->d_lde.p, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(piv.data(), h->d_lpivots.p, (size_t)h->n, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(status, e, "values");
+    // after a solve the rows below are in the solve's order: row w + i holds row w + from[i]
     int64_t at = 0;
     for (int64_t s = 0; s < h->ns; ++s) {
       const int64_t m = h->height[s], w = h->width[s], f = h->first[s];
       const double *F = rect.data() + h->loff[s];
+      std::vector<int64_t> to(m - w);  // the structure's row w + j is at row w + to[j]
+      for (int64_t i = 0; i < m - w; ++i) to[i] = i;
+      if (h->ldlt_folded)
+        for (int64_t i = 0; i < m - w; ++i) to[h->ldlt_from[h->ldlt_from_off[s] + i]] = i;
       for (int64_t c = 0; c < w; ++c) {
-        for (int64_t r = c; r < m; ++r) dst[at + r - c] = F[r + c * m];
+        for (int64_t r = c; r < m; ++r) dst[at + r - c] = F[(r >= w ? w + to[r - w] : r) + c * m];
         dst[at] = d[f + c];
         if (piv[f + c] == fc::ldlt::PIVOT_FIRST && c + 1 < m) dst[at + 1] = sub[f + c];
         at += m - c;

@@ -38,9 +38,11 @@ extern "C" {
 #define FC_PRECISION_FP64 0
 #define FC_PRECISION_FP32_IR 1 /* FP32 factor of S A S, every diagonal block in FP64; FP64 refinement */
 /* FP64 symmetric indefinite P A P^T = L D L^T (LdltFactor, crates/solver/src/ldlt.rs): bounded
- * Bunch-Kaufman pivots inside supernodes, on the same analysis. This build factors only: its
- * values (fc_chol_values, the reference's Block::values) and inertia (fc_chol_inertia); its solves
- * return FC_INVALID_ARGUMENT. A column with no pivot is FC_SINGULAR (FactorError::Singular). */
+ * Bunch-Kaufman pivots inside supernodes, on the same analysis; values (fc_chol_values, the
+ * reference's Block::values), inertia (fc_chol_inertia) and solves through fc_chol_solve and
+ * fc_chol_solve_device (the first solve after a factorisation folds the pivot orders into the
+ * solve's structure, which waits for the stream); refined, no-alloc and persistent solves return
+ * FC_INVALID_ARGUMENT. A column with no pivot is FC_SINGULAR (FactorError::Singular). */
 #define FC_PRECISION_LDLT 2
 
 typedef struct fc_status {

@@ -1,10 +1,12 @@
 """The device LDL^T factor (FC_PRECISION_LDLT) against the oracle's (crates/solver/src/ldlt.rs):
 inertia exactly, the factor's values within 1e-11 of the largest entry where the pivots are the
 same (the updates run on the FP64 tensor pipe with fused multiply-adds, so a near tie in the rook
-search may choose another, equally valid pivot), singular columns named, solves refused.
+search may choose another, equally valid pivot), solutions within 1e-10 of the oracle's and
+solve_many bit for bit the single solves, values unchanged by a solve, singular columns named.
 
 Skipped until these kernels have run on a GPU: the panel's source is checked bit for bit on the
-CPU (tests/test_ldlt_panel_emulated.py); the plan and the launches have not run yet."""
+CPU (tests/test_ldlt_panel_emulated.py) and the solve's structure by tests/test_ldlt_fold.py; the
+plan and the launches have not run yet."""
 import numpy as np
 import pytest
 
@@ -41,6 +43,26 @@ def test_factor_and_inertia_match_the_oracle(cuda, name):
         assert np.max(np.abs(gv - ov)) <= 1e-11 * np.max(np.abs(ov))
 
 
+@pytest.mark.parametrize("name", list(CASES))
+def test_solves_match_the_oracle(cuda, name):
+    a = CASES[name]()
+    g, o = both(a)
+    before = g.values()
+    rng = np.random.default_rng(5)
+    B = np.asfortranarray(rng.standard_normal((a.n, 7)))
+    want = o.solve(B.copy(order="F"))
+    got = B.copy(order="F")
+    g.solve_many(got)
+    assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))
+    alone = np.stack([np.ascontiguousarray(B[:, j]) for j in range(7)], axis=1)
+    for j in range(7):
+        x = np.ascontiguousarray(B[:, j])
+        g.solve(x)
+        alone[:, j] = x
+    assert np.array_equal(alone.view(np.uint64), got.view(np.uint64))
+    assert np.array_equal(g.values(), before)  # the solve's row moves are undone in the values
+
+
 def test_singular_columns_and_refused_solves(cuda):
     n = 12
     rows = []
@@ -53,4 +75,4 @@ def test_singular_columns_and_refused_solves(cuda):
     assert 0 <= e.value.column < n
     g, _ = both(H.saddle(8, 3))
     with pytest.raises(ValueError):
-        g.solve(np.ones(g.n))
+        g.option(g.SOLVE_SCHEDULE, 1)  # the persistent solve is the Cholesky factor's only
