@@ -348,3 +348,85 @@ class LdltFactor(Factor):
 
     def two_by_two(self) -> int:
         return self._counts()[2]
+
+
+class Kind:
+    """Which factorization a symmetric solve uses (ldlt.rs:452-463)."""
+    DEFINITE, INDEFINITE, AUTO = 0, 1, 2
+
+
+class Symmetric:
+    """A factored symmetric matrix, Cholesky or LDL^T (ldlt.rs:465-561): Kind.AUTO tries Cholesky
+    and takes LDL^T when the matrix is not positive definite, one analysis serving both."""
+
+    def __init__(self, factor: Factor):
+        self.factor = factor
+
+    @staticmethod
+    def new(a: UpperColumns, max_entries: int, kind: int = Kind.DEFINITE, device: int = 0) -> "Symmetric":
+        if kind == Kind.DEFINITE:
+            return Symmetric(Factor.new(a, max_entries, FP64, device))
+        if kind == Kind.INDEFINITE:
+            return Symmetric(LdltFactor.new(a, max_entries, device))
+        sym = Symbolic(a, max_entries)
+        f = Factor(sym, FP64, device)
+        try:
+            f.factor(a.val)
+            return Symmetric(f)
+        except NotPositiveDefinite:
+            f.close()
+        g = LdltFactor(sym, device)
+        g.factor(a.val)
+        return Symmetric(g)
+
+    @property
+    def n(self) -> int:
+        return self.factor.n
+
+    def is_cholesky(self) -> bool:
+        return not isinstance(self.factor, LdltFactor)
+
+    def entries(self) -> int:
+        return self.factor.entries()
+
+    def inertia(self) -> Inertia:
+        """A Cholesky factor's matrix is positive definite (ldlt.rs:500-506)."""
+        if self.is_cholesky():
+            return Inertia(self.n, 0)
+        return self.factor.inertia()
+
+    def solve(self, b: np.ndarray):
+        self.factor.solve(b)
+
+    def solve_many(self, bs):
+        self.factor.solve_many(bs)
+
+    def solve_refined(self, a: Csr, b: np.ndarray, steps: int):
+        """Solve, then refine with the residual against `a` (both triangles) while its largest
+        magnitude shrinks, at most `steps` times (ldlt.rs:524-560); Cholesky solutions are
+        returned as solved. The products are the reference's Csr::mul, on the host."""
+        rhs = b.copy()
+        self.solve(b)
+        if self.is_cholesky():
+            return
+
+        def residual(x):
+            rows = np.repeat(np.arange(a.n), np.diff(a.ptr))
+            ax = np.zeros(a.n)
+            np.add.at(ax, rows, a.val * x[a.idx])
+            return rhs - ax
+
+        r = residual(b)
+        size = float(np.max(np.abs(r))) if a.n else 0.0
+        for _ in range(steps):
+            if not size > 0.0:
+                break
+            dx = r.copy()
+            self.solve(dx)
+            trial = b + dx
+            nxt = residual(trial)
+            nsize = float(np.max(np.abs(nxt)))
+            if not nsize < size:
+                break
+            b[:] = trial
+            r, size = nxt, nsize

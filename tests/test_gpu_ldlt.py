@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import helpers as H
-from fieldcraft_b200 import LdltFactor, Singular, UpperColumns
+from fieldcraft_b200 import Kind, LdltFactor, NotPositiveDefinite, Singular, Symmetric, UpperColumns
 from oracle import oracle
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="the device LDL^T has not run on a GPU yet")]
@@ -76,3 +76,19 @@ def test_singular_columns_and_refused_solves(cuda):
     g, _ = both(H.saddle(8, 3))
     with pytest.raises(ValueError):
         g.option(g.SOLVE_SCHEDULE, 1)  # the persistent solve is the Cholesky factor's only
+
+
+def test_auto_selection_and_refinement(cuda):
+    """ldlt.rs:959-978: Kind.AUTO keeps Cholesky for a definite matrix and takes LDL^T for an
+    indefinite one; refinement brings the solution to 1e-12; Kind.DEFINITE refuses the indefinite."""
+    spd, _ = H.shifted_grid([4, 4, 4], -1.0)
+    assert Symmetric.new(UpperColumns.from_symmetric(spd), 2**62, Kind.AUTO).is_cholesky()
+    ind, below = H.shifted_grid([4, 4, 4], 4.4)
+    s = Symmetric.new(UpperColumns.from_symmetric(ind), 2**62, Kind.AUTO)
+    assert not s.is_cholesky() and s.inertia().negative == below
+    x = np.cos(np.arange(ind.n, dtype=np.float64))
+    b = oracle.spmv(ind.n, ind.ptr, ind.idx, ind.val, x)
+    s.solve_refined(ind, b, 3)
+    assert np.all(np.abs(b - x) < 1e-12)
+    with pytest.raises(NotPositiveDefinite):
+        Symmetric.new(UpperColumns.from_symmetric(ind), 2**62, Kind.DEFINITE)
