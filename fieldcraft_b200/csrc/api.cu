@@ -1420,11 +1420,11 @@ int read_status(fc_chol *h, fc_status *st) {
   return FC_OK;
 }
 
-// The LDL^T factor solves level by level only (not refined, not without allocation, not
-// persistent): those paths are refused for it.
+// The LDL^T factor solves level by level (refined by plain refinement only; not without
+// allocation, not persistent): the no-alloc solve is refused for it.
 bool ldlt_refused(const fc_chol *h, fc_status *st) {
   if (!h->ldlt) return false;
-  set_status(st, FC_INVALID_ARGUMENT, -1, 0, 0, "the LDL^T factor solves through fc_chol_solve(_device) only");
+  set_status(st, FC_INVALID_ARGUMENT, -1, 0, 0, "the LDL^T factor has no solve without allocation");
   return true;
 }
 
@@ -2949,7 +2949,11 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "right-hand side length");
     return FC_INVALID_ARGUMENT;
   }
-  if (ldlt_refused(h, status)) return FC_INVALID_ARGUMENT;
+  if (h->ldlt && h->refine_pcg) {  // conjugate gradients needs a positive definite preconditioner
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0,
+               "the LDL^T factor refines by plain refinement only (FC_OPTION_REFINEMENT = 1)");
+    return FC_INVALID_ARGUMENT;
+  }
   if (nrhs == 0 || h->n == 0) {
     set_status(status, FC_OK);
     return FC_OK;

@@ -41,8 +41,10 @@ extern "C" {
  * Bunch-Kaufman pivots inside supernodes, on the same analysis; values (fc_chol_values, the
  * reference's Block::values), inertia (fc_chol_inertia) and solves through fc_chol_solve and
  * fc_chol_solve_device (the first solve after a factorisation folds the pivot orders into the
- * solve's structure, which waits for the stream); refined, no-alloc and persistent solves return
- * FC_INVALID_ARGUMENT. A column with no pivot is FC_SINGULAR (FactorError::Singular). */
+ * solve's structure, which waits for the stream), and fc_chol_refine_solve_device by plain
+ * refinement (FC_OPTION_REFINEMENT = 1; conjugate gradients needs a definite preconditioner);
+ * no-alloc and persistent solves return FC_INVALID_ARGUMENT. A column with no pivot is
+ * FC_SINGULAR (FactorError::Singular). */
 #define FC_PRECISION_LDLT 2
 
 typedef struct fc_status {

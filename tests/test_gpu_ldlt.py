@@ -92,3 +92,22 @@ def test_auto_selection_and_refinement(cuda):
     assert np.all(np.abs(b - x) < 1e-12)
     with pytest.raises(NotPositiveDefinite):
         Symmetric.new(UpperColumns.from_symmetric(ind), 2**62, Kind.DEFINITE)
+
+
+def test_plain_refinement_on_the_device(cuda):
+    """fc_chol_refine_solve_device with the LDL^T factor: plain refinement (FC_OPTION_REFINEMENT = 1)
+    reaches 1e-12 on an indefinite grid; conjugate gradients (the default) is refused, since it
+    needs a positive definite preconditioner."""
+    torch = cuda
+    a, _ = H.shifted_grid([7, 6, 5], 3.3)
+    g, _ = both(a)
+    csr = tuple(torch.from_numpy(v).cuda() for v in (a.ptr, a.idx, a.val))
+    x_true = np.sin(np.arange(a.n) * 0.37)
+    b = torch.from_numpy(oracle.spmv(a.n, a.ptr, a.idx, a.val, x_true)).cuda().reshape(1, a.n)
+    x = torch.zeros_like(b)
+    with pytest.raises(ValueError):
+        g.refine_solve_device(csr, b, x, 1, a.n, tol=1e-12, max_iter=10)
+    g.option(g.REFINEMENT, 1)
+    rel, its = g.refine_solve_device(csr, b, x, 1, a.n, tol=1e-12, max_iter=10)
+    assert rel[0] <= 1e-12 and its >= 1
+    assert np.max(np.abs(x.cpu().numpy()[0] - x_true)) < 1e-9
