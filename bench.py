@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--profile-kernels", choices=["fp32-factor", "unet"], default=None,
                     help="a short run for a profiler: two FP32 factorisations of the --n-el block, or the "
                          "U-Net's forward and backward passes on a 64x64x8 plate, twice")
+    ap.add_argument("--ldlt", type=int, default=0, metavar="N_EL",
+                    help="instead: the symmetric indefinite LDL^T (factor, inertia and solve of 16 RHS) on the "
+                         "N_EL^3 lognormal block shifted by 2%% of its mean diagonal, against the oracle's LDL^T")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=2,
                     help="workload: 2 (default) the 48^3 block the metric is quoted on; 1 cantilever, 3 256 "
                          "uneven boxes batched, 4 64^3 random-field block to 1e-12, 5 128x128x8 plate (NN-FCG)")
@@ -281,6 +284,95 @@ def block_csr(parts):
     return Csr(col0, np.concatenate(ptr), np.concatenate(idx).astype(np.int32), np.concatenate(val))
 
 
+def shifted(problem, theta: float):
+    """The problem's K - theta * mean(diag K) * I (indefinite for theta above the lowest eigenvalue's
+    share): the full CSR and the upper triangle by columns."""
+    from fieldcraft_b200.cholesky import Csr, UpperColumns
+    csr = problem.csr
+    rows = np.repeat(np.arange(csr.n), np.diff(csr.ptr))
+    on = csr.idx == rows
+    sigma = theta * float(np.mean(csr.val[on]))
+    val = csr.val.copy()
+    val[on] -= sigma
+    a = Csr(csr.n, csr.ptr, csr.idx, val)
+    return a, UpperColumns.from_symmetric(a), sigma
+
+
+def run_ldlt(args, torch, lib, local: int):
+    """The symmetric indefinite factor (FC_PRECISION_LDLT) on a shifted lognormal block: per step
+    the factorisation from values in HBM, the solve of 16 right-hand sides (the first after a
+    factorisation folds the pivot orders into the solve's structure) and the residual, timed on
+    the device; the inertia; the oracle's LDL^T on a bounded sample, scaled by factor flops. One
+    JSON line."""
+    from fieldcraft_b200 import LDLT, Factor, Symbolic, problems
+    from fieldcraft_b200.cholesky import Status, raise_for
+    from oracle import oracle
+    R = 16
+    p = problems.lognormal_block(args.ldlt, nrhs=R, seed=SEED)
+    a, up, sigma = shifted(p, 0.02)
+    full_flops, _ = factor_flops(p)
+    n = a.n
+    f = Factor(Symbolic(up, 2**62), precision=LDLT, device=local)
+    stream = torch.cuda.Stream()
+    f.set_stream(stream.cuda_stream)
+    d_val = torch.from_numpy(up.val).cuda()
+    csr_dev = tuple(torch.from_numpy(v).cuda() for v in (a.ptr, a.idx, a.val))
+    d_f = torch.from_numpy(np.ascontiguousarray(p.rhs.T)).cuda()
+    d_x, d_r = torch.empty_like(d_f), torch.empty_like(d_f)
+    fnorm = torch.linalg.vector_norm(d_f, dim=1)
+
+    def step():
+        with torch.cuda.stream(stream):
+            assert lib.fc_chol_factor_device_async(f.handle, C.c_void_p(d_val.data_ptr()), up.val.size) == 0
+            d_x.copy_(d_f)
+            assert lib.fc_chol_solve_device_async(f.handle, C.c_void_p(d_x.data_ptr()), R, n) == 0
+            lib.fc_csr_spmv_device(n, *(C.c_void_p(v.data_ptr()) for v in csr_dev), C.c_void_p(d_x.data_ptr()),
+                                   C.c_void_p(d_r.data_ptr()), R, n, C.c_void_p(stream.cuda_stream))
+            d_r.sub_(d_f)
+            return torch.linalg.vector_norm(d_r, dim=1) / fnorm
+
+    for _ in range(args.warmup):
+        step()
+    st = Status()
+    lib.fc_chol_check(f.handle, C.byref(st))
+    raise_for(st)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rel = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    pos, neg, two = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+    lib.fc_chol_inertia(f.handle, C.byref(pos), C.byref(neg), C.byref(two), C.byref(st))
+    raise_for(st)
+    # the oracle's LDL^T on a bounded sample (the same generator and shift at SAMPLE_EL^3)
+    sample = problems.lognormal_block(SAMPLE_EL, nrhs=R, seed=SEED)
+    sa, sup, _ = shifted(sample, 0.02)
+    sflops, _ = factor_flops(sample)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    t0 = time.perf_counter()
+    sym = oracle.Sym(sup.n, sup.ptr, sup.idx)
+    of = oracle.Ldlt(sym, sup.val)
+    of.solve(sample.rhs.copy(order="F"))
+    t_cpu = time.perf_counter() - t0
+    line = {
+        "metric": "s per LDL^T factorisation + 16 solves (symmetric indefinite, FP64)", "value": ms / 1e3,
+        "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"hex8 block {args.ldlt}^3 lognormal E, K - {sigma:.4g} I (2% of the mean diagonal), "
+                               f"{R} RHS", "n": n, "inertia": [pos.value, neg.value], "two_by_two": two.value},
+        "relres_max": float(rel.max().item()),
+        "cpu_baseline": {"value": t_cpu * full_flops / sflops, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": f"oracle LDL^T factor + {R} solves of the shifted {SAMPLE_EL}^3 block took "
+                                   f"{t_cpu:.3f} s; scaled by Cholesky factor flops {full_flops:.3e}/{sflops:.3e}"},
+    }
+    print(json.dumps(line), flush=True)
+    f.close()
+
+
 def run_config(args, cfg: int, torch, lib, local: int):
     """Configs other than the headline: FP64 direct solve vs FP32+IR to the config's tolerance on
     the same K (and, for the plate, the learned preconditioner), each timed on the device from
@@ -450,6 +542,12 @@ def main():
     lib = _lib.load()
     if args.profile_kernels:
         profile_kernels(args, torch, lib)
+        return
+    if args.ldlt:
+        if rank == 0:
+            run_ldlt(args, torch, lib, local)
+        if world > 1:
+            dist.destroy_process_group()
         return
     if args.config != 2:
         if rank == 0:
