@@ -233,3 +233,26 @@ def test_auto_selection_and_refinement():
     b = oracle.spmv(ind.n, ind.ptr, ind.idx, ind.val, x)
     got = oracle.solve_refined(ind.n, ind.ptr, ind.idx, ind.val, f, b, 3)
     assert np.all(np.abs(got - x) < 1e-12)
+
+
+def test_shifted_stiffness_block():
+    """A hex8 stiffness matrix shifted past its lowest eigenvalues (the workload of
+    `bench.py --ldlt`): the pivots inside supernodes solve it to the path's 1e-10 with negative
+    eigenvalues and 2 x 2 pivots present."""
+    from fieldcraft_b200 import problems
+    from fieldcraft_b200.cholesky import UpperColumns
+    p = problems.lognormal_block(12, nrhs=3, seed=2024)
+    csr = p.csr
+    rows = np.repeat(np.arange(csr.n), np.diff(csr.ptr))
+    on = csr.idx == rows
+    val = csr.val.copy()
+    val[on] -= 0.02 * float(np.mean(csr.val[on]))
+    a = Csr(csr.n, csr.ptr, csr.idx, val)
+    up = UpperColumns.from_symmetric(a)
+    s = oracle.Sym(a.n, up.ptr, up.idx)
+    f = oracle.Ldlt(s, up.val)
+    assert f.inertia()[1] > 0 and f.two_by_two() > 0
+    x = f.solve(p.rhs.copy(order="F"))
+    for j in range(3):
+        r = oracle.spmv(a.n, a.ptr, a.idx, a.val, x[:, j]) - p.rhs[:, j]
+        assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(p.rhs[:, j])
