@@ -209,7 +209,8 @@ int64_t fc_chol_trace_read(fc_chol *h, int64_t *out, int64_t cap);
  * `kinds` entries), then clears them. Kinds: 0 front assembly, 1 panel (factor,
  * invert and solve below a diagonal block), 3 GEMM of the factor, 10 and 11 the two GEMMs of a
  * doubling step of the diagonal-block inverses, 12 the tcgen05 GEMM of the mixed-precision factor
- * and 15 the packing of its operands;
+ * and 15 the packing of its operands; 16 the LDL^T factor's pivoted panel steps, 17 its W21 and D
+ * split, 18 its unit lower block inverses;
  * 19 GEMM, 20 front assembly, 22 forward inverse, 23
  * backward inverse of the solve (level by level), 24 forward, 25 backward persistent launch of the
  * solve, 29 forward, 30 backward step of the thin supernodes (32 covers all). */
