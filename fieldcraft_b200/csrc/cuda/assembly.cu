@@ -1,0 +1,117 @@
+// K_ff of a structured hex8 box assembled on the device (include/fieldcraft_fem.h): the element
+// matrices (host/hex8.hpp, one thread per element), then every entry as the sum over the elements
+// holding both its nodes in element label order (host/assembly.hpp, one thread per row), the
+// host builder's operations in its order, so the values are its bits.
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/fieldcraft_fem.h"
+#include "device_buf.hpp"
+#include "host/assembly.hpp"
+
+struct fc_fem_device {
+  fc::assembly::Box box{};
+  int64_t n = 0, nnz = 0, elements = 0;
+  int device = 0;
+  fc::host::DeviceBuf d_ptr, d_idx, d_node, d_ke, d_bad;
+};
+
+namespace {
+
+__global__ void element_kernel(fc::assembly::Box box, int64_t elements, const double *__restrict__ young, double nu,
+                               double *__restrict__ ke, int *__restrict__ bad) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < elements; e += (int64_t)gridDim.x * blockDim.x) {
+    double x[24];
+    fc::assembly::element_corners(box, e, x);
+    if (!fc::hex8::stiffness(x, young[e], nu, ke + e * 576)) atomicExch(bad, 1);
+  }
+}
+
+__global__ void entry_kernel(fc::assembly::Box box, int64_t n, const int64_t *__restrict__ ptr,
+                             const int32_t *__restrict__ idx, const int64_t *__restrict__ node,
+                             const double *__restrict__ ke, double *__restrict__ val) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = node[r / 3];
+    const int a = (int)(r % 3);
+    for (int64_t q = ptr[r]; q < ptr[r + 1]; ++q) {
+      const int32_t col = idx[q];
+      val[q] = fc::assembly::entry(box, v, a, node[col / 3], col % 3, ke);
+    }
+  }
+}
+
+int blocks_for(int64_t count) {
+  const int64_t b = (count + 127) / 128;
+  return (int)(b < 8192 ? (b > 0 ? b : 1) : 8192);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fc_fem_device_create(int nx, int ny, int nz, double lx, double ly, double lz, int64_t n, const int64_t *ptr,
+                         const int32_t *idx, const int64_t *eq, int device, fc_fem_device **out) {
+  if (!out || nx <= 0 || ny <= 0 || nz <= 0 || n < 0 || n % 3 != 0 || (n > 0 && (!ptr || !idx || !eq)) ||
+      !(lx > 0 && ly > 0 && lz > 0))
+    return FC_FEM_INVALID;
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return FC_FEM_INVALID;
+  auto d = new fc_fem_device();
+  d->box = {nx, ny, nz, lx, ly, lz};
+  d->n = n;
+  d->nnz = n > 0 ? ptr[n] : 0;
+  d->elements = (int64_t)nx * ny * nz;
+  d->device = device;
+  const int64_t nodes = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  std::vector<int64_t> node(n / 3, -1), hptr(ptr, ptr + n + 1);
+  std::vector<int32_t> hidx(idx, idx + d->nnz);
+  bool ok = true;
+  for (int64_t v = 0; v < nodes && ok; ++v) {
+    const int64_t e = eq[3 * v];
+    if (e < 0) continue;
+    if (e % 3 != 0 || e / 3 >= n / 3 || eq[3 * v + 1] != e + 1 || eq[3 * v + 2] != e + 2) ok = false;
+    else node[e / 3] = v;
+  }
+  for (int64_t k = 0; k < n / 3 && ok; ++k) ok = node[k] >= 0;
+  for (int64_t q = 0; q < d->nnz && ok; ++q) ok = hidx[q] >= 0 && hidx[q] < n;
+  if (!ok) {
+    delete d;
+    return FC_FEM_INVALID;
+  }
+  cudaStream_t st = nullptr;
+  if (fc::host::upload(d->d_ptr, hptr, st) != cudaSuccess || fc::host::upload(d->d_idx, hidx, st) != cudaSuccess ||
+      fc::host::upload(d->d_node, node, st) != cudaSuccess ||
+      d->d_ke.alloc(sizeof(double) * 576 * (size_t)d->elements) != cudaSuccess ||
+      d->d_bad.alloc(sizeof(int)) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+    delete d;
+    return FC_FEM_NOMEM;
+  }
+  *out = d;
+  return FC_FEM_OK;
+}
+
+int fc_fem_assemble_device(fc_fem_device *d, const double *d_young, double poisson, double *d_val, void *stream) {
+  if (!d || !d_young || (d->nnz > 0 && !d_val)) return FC_FEM_INVALID;
+  cudaSetDevice(d->device);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(d->d_bad.p, 0, sizeof(int), st);
+  element_kernel<<<blocks_for(d->elements), 128, 0, st>>>(d->box, d->elements, d_young, poisson, d->d_ke.as<double>(),
+                                                         d->d_bad.as<int>());
+  entry_kernel<<<blocks_for(d->n), 128, 0, st>>>(d->box, d->n, d->d_ptr.as<int64_t>(), d->d_idx.as<int32_t>(),
+                                                 d->d_node.as<int64_t>(), d->d_ke.as<double>(), d_val);
+  int bad = 0;
+  if (cudaMemcpyAsync(&bad, d->d_bad.p, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return FC_FEM_INVALID;
+  return bad ? FC_FEM_INVALID : FC_FEM_OK;
+}
+
+void fc_fem_device_free(fc_fem_device *d) {
+  if (!d) return;
+  cudaSetDevice(d->device);
+  delete d;
+}
+
+}  // extern "C"

@@ -2,6 +2,8 @@
 // numbering, element stiffness and assembly of K_ff. Declared in include/fieldcraft_fem.h, whose
 // head names the reference files each part restates.
 #include "fieldcraft_fem.h"
+#include "assembly.hpp"
+#include "hex8.hpp"
 
 #include <algorithm>
 #include <atomic>
@@ -290,87 +292,9 @@ std::vector<int64_t> fill_reducing(const Graph &g, const double *xyz) {
 
 // ---- hex8 element ----------------------------------------------------------------------------
 
-// Natural coordinates of the corners (crates/fem/src/shape.rs:51-52).
-const double HEX_CORNERS[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
-                                  {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
-// Two-point Gauss-Legendre abscissa (crates/fem/src/quadrature.rs:31).
-const double GAUSS2 = 0.5773502691896258;
-
+// The element's stiffness (host/hex8.hpp, shared with the device assembly).
 bool hex8_stiffness(const double *xyz, double young, double nu, double *k) {
-  if (!(young > 0.0) || !(nu > -1.0 && nu < 0.5)) return false;
-  // Isotropic elasticity (crates/fem/src/material.rs:40-53).
-  const double lambda = young * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
-  const double mu = young / (2.0 * (1.0 + nu));
-  double d[6][6] = {};
-  for (int i = 0; i < 3; ++i) {
-    for (int j = 0; j < 3; ++j) d[i][j] = lambda;
-    d[i][i] = lambda + 2.0 * mu;
-    d[i + 3][i + 3] = mu;
-  }
-  std::memset(k, 0, sizeof(double) * 576);
-  const double g[2] = {-GAUSS2, GAUSS2};
-  // Points with xi fastest, then eta, then zeta; every weight is 1 (quadrature.rs:78-90).
-  for (int pz = 0; pz < 2; ++pz)
-    for (int py = 0; py < 2; ++py)
-      for (int px = 0; px < 2; ++px) {
-        const double xi[3] = {g[px], g[py], g[pz]};
-        const double weight = 1.0 * 1.0 * 1.0;
-        double dn[8][3];
-        for (int i = 0; i < 8; ++i) {
-          const double *c = HEX_CORNERS[i];
-          double f[3] = {1.0 + xi[0] * c[0], 1.0 + xi[1] * c[1], 1.0 + xi[2] * c[2]};
-          dn[i][0] = c[0] * f[1] * f[2] / 8.0;
-          dn[i][1] = c[1] * f[0] * f[2] / 8.0;
-          dn[i][2] = c[2] * f[0] * f[1] / 8.0;
-        }
-        double jm[3][3] = {};
-        for (int i = 0; i < 8; ++i)
-          for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) jm[a][b] += dn[i][a] * xyz[3 * i + b];
-        const double det = jm[0][0] * (jm[1][1] * jm[2][2] - jm[1][2] * jm[2][1]) -
-                           jm[0][1] * (jm[1][0] * jm[2][2] - jm[1][2] * jm[2][0]) +
-                           jm[0][2] * (jm[1][0] * jm[2][1] - jm[1][1] * jm[2][0]);
-        if (!(det > 0.0) || !std::isfinite(det)) return false;
-        double inv[3][3];
-        for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j) {
-            int j1 = (j + 1) % 3, j2 = (j + 2) % 3, i1 = (i + 1) % 3, i2 = (i + 2) % 3;
-            inv[i][j] = (jm[j1][i1] * jm[j2][i2] - jm[j1][i2] * jm[j2][i1]) / det;
-          }
-        double dx[8][3];
-        for (int i = 0; i < 8; ++i)
-          for (int b = 0; b < 3; ++b)
-            dx[i][b] = inv[b][0] * dn[i][0] + inv[b][1] * dn[i][1] + inv[b][2] * dn[i][2];
-        const double w = det * weight;
-        // Upper blocks j >= i, mirrored, so K is exactly symmetric (element.rs:745-774).
-        for (int j = 0; j < 8; ++j) {
-          const double *gj = dx[j];
-          const double bj[6][3] = {{gj[0], 0, 0}, {0, gj[1], 0}, {0, 0, gj[2]},
-                                   {gj[1], gj[0], 0}, {gj[2], 0, gj[0]}, {0, gj[2], gj[1]}};
-          double db[6][3];
-          for (int s = 0; s < 6; ++s)
-            for (int c = 0; c < 3; ++c) {
-              double acc = 0.0;
-              for (int t = 0; t < 6; ++t) acc += d[s][t] * bj[t][c];
-              db[s][c] = acc;
-            }
-          for (int i = 0; i <= j; ++i) {
-            const double *gi = dx[i];
-            const double bi[6][3] = {{gi[0], 0, 0}, {0, gi[1], 0}, {0, 0, gi[2]},
-                                     {gi[1], gi[0], 0}, {gi[2], 0, gi[0]}, {0, gi[2], gi[1]}};
-            for (int r = 0; r < 3; ++r)
-              for (int c = (i == j ? r : 0); c < 3; ++c) {
-                double acc = 0.0;
-                for (int s = 0; s < 6; ++s) acc += bi[s][r] * db[s][c];
-                const double v = w * acc;
-                const int row = 3 * i + r, col = 3 * j + c;
-                k[row * 24 + col] += v;
-                if (row != col) k[col * 24 + row] += v;
-              }
-          }
-        }
-      }
-  return true;
+  return fc::hex8::stiffness(xyz, young, nu, k);
 }
 
 int hardware_threads(int threads) {
@@ -389,6 +313,29 @@ struct fc_problem {
 };
 
 extern "C" {
+
+// Not part of the public ABI: K_ff of a box assembled entry by entry on the host with the device
+// assembly's code (host/assembly.hpp), for tests; val[ptr[n]] in the pattern's order. eq as
+// fc_fem_equations gives it. Returns FC_FEM_OK, or FC_FEM_INVALID for an invalid element.
+int fc_test_fem_assemble_host(int nx, int ny, int nz, double lx, double ly, double lz, int64_t n, const int64_t *ptr,
+                              const int32_t *idx, const int64_t *eq, const double *young, double poisson,
+                              double *val) {
+  const fc::assembly::Box box{nx, ny, nz, lx, ly, lz};
+  const int64_t elements = (int64_t)nx * ny * nz, nodes = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  std::vector<double> ke((size_t)elements * 576);
+  for (int64_t e = 0; e < elements; ++e) {
+    double x[24];
+    fc::assembly::element_corners(box, e, x);
+    if (!fc::hex8::stiffness(x, young[e], poisson, ke.data() + e * 576)) return FC_FEM_INVALID;
+  }
+  std::vector<int64_t> node(n / 3);
+  for (int64_t v = 0; v < nodes; ++v)
+    if (eq[3 * v] >= 0) node[eq[3 * v] / 3] = v;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t q = ptr[r]; q < ptr[r + 1]; ++q)
+      val[q] = fc::assembly::entry(box, node[r / 3], (int)(r % 3), node[idx[q] / 3], idx[q] % 3, ke.data());
+  return FC_FEM_OK;
+}
 
 int fc_hex8_stiffness(const double *xyz24, double young, double poisson, double *out576) {
   if (!xyz24 || !out576) return FC_FEM_INVALID;

@@ -26,6 +26,7 @@ class Problem:
     nodes_xyz: np.ndarray   # [nodes, 3]
     rhs: np.ndarray = field(default=None)  # [n, nrhs], Fortran order
     young: np.ndarray = field(default=None)  # element moduli (when the workload keeps them)
+    lengths: tuple = field(default=None)     # the box's lx, ly, lz
 
     @property
     def n(self) -> int:
@@ -61,7 +62,43 @@ def box(nx, ny, nz, lx, ly, lz, young, poisson, clamped_nodes, name="box", threa
         lib.fc_fem_free(h)
     i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
     xyz = np.stack([lx * i / nx, ly * j / ny, lz * k / nz], axis=-1).transpose(2, 1, 0, 3).reshape(-1, 3)
-    return Problem(name, (nx, ny, nz), Csr(int(n), ptr, idx, val), order, eq, xyz)
+    return Problem(name, (nx, ny, nz), Csr(int(n), ptr, idx, val), order, eq, xyz,
+                   lengths=(float(lx), float(ly), float(lz)))
+
+
+class DeviceAssembly:
+    """K_ff of a box problem assembled on the GPU (fc_fem_device_*): the builder's values bit for
+    bit, from element moduli in device memory."""
+
+    def __init__(self, p: Problem, device: int = 0):
+        lib = _lib.load()
+        nx, ny, nz = p.dims
+        lx, ly, lz = p.lengths
+        self._keep = [np.ascontiguousarray(a) for a in (p.csr.ptr, p.csr.idx, p.eq)]
+        h = C.c_void_p()
+        rc = lib.fc_fem_device_create(nx, ny, nz, lx, ly, lz, p.n, *(_lib.ptr(a) for a in self._keep), device,
+                                      C.byref(h))
+        if rc != 0:
+            raise ValueError(f"fc_fem_device_create failed ({rc})")
+        self.handle = h
+
+    def assemble(self, young, val, poisson: float = 0.3, stream_ptr: int | None = None):
+        """val (a CUDA tensor of nnz doubles) <- K_ff's values for the moduli `young` (a CUDA tensor)."""
+        rc = _lib.load().fc_fem_assemble_device(self.handle, C.c_void_p(young.data_ptr()), float(poisson),
+                                                C.c_void_p(val.data_ptr()), C.c_void_p(stream_ptr or 0))
+        if rc != 0:
+            raise ValueError(f"fc_fem_assemble_device failed ({rc})")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().fc_fem_device_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except TypeError:
+            pass
 
 
 def node_grid(nx, ny, nz):

@@ -62,6 +62,20 @@ int64_t fc_fill(int64_t n, const int64_t *adj_ptr, const int32_t *adj_idx, const
  * DOFs node by node (x, y, z), row-major into out[576]. */
 int fc_hex8_stiffness(const double *xyz24, double young, double poisson, double *out576);
 
+/* K_ff assembled on a GPU (no reference counterpart: the reference assembles on the host,
+ * analysis.rs:199-234): every element's matrix, then every entry as the sum over the elements
+ * holding both its nodes in element label order; the builder's operations in its order, so the
+ * values are fc_fem_box's bits. A context holds the box (nx, ny, nz elements of lx, ly, lz), its
+ * pattern (ptr[n+1], idx, as fc_fem_csr gives them), its equations (eq[3 nodes], as
+ * fc_fem_equations gives them) and 576 doubles per element of device scratch. Assembly takes the
+ * moduli d_young[nx ny nz] in device memory and writes d_val[ptr[n]] in the pattern's order on
+ * `stream` (a cudaStream_t), waiting for it; FC_FEM_INVALID for a bad modulus or element. */
+typedef struct fc_fem_device fc_fem_device;
+int fc_fem_device_create(int nx, int ny, int nz, double lx, double ly, double lz, int64_t n, const int64_t *ptr,
+                         const int32_t *idx, const int64_t *eq, int device, fc_fem_device **out);
+int fc_fem_assemble_device(fc_fem_device *d, const double *d_young, double poisson, double *d_val, void *stream);
+void fc_fem_device_free(fc_fem_device *d);
+
 #ifdef __cplusplus
 }
 #endif
