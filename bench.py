@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--ldlt", type=int, default=0, metavar="N_EL",
                     help="instead: the symmetric indefinite LDL^T (factor, inertia and solve of 16 RHS) on the "
                          "N_EL^3 lognormal block shifted by 2%% of its mean diagonal, against the oracle's LDL^T")
+    ap.add_argument("--assembly", type=int, default=0, metavar="N_EL",
+                    help="instead: K_ff of the N_EL^3 lognormal block assembled on the device (element matrices "
+                         "and the gather), checked bit for bit against the host builder")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=2,
                     help="workload: 2 (default) the 48^3 block the metric is quoted on; 1 cantilever, 3 256 "
                          "uneven boxes batched, 4 64^3 random-field block to 1e-12, 5 128x128x8 plate (NN-FCG)")
@@ -373,6 +376,55 @@ def run_ldlt(args, torch, lib, local: int):
     f.close()
 
 
+def run_assembly(args, torch, lib, local: int):
+    """K_ff of the N_EL^3 lognormal block on the device (fc_fem_assemble_device) from element moduli
+    in HBM, per step timed on the device; the values checked against the host builder's bit for
+    bit; the host builder's whole run (mesh, order, pattern, assembly) and the same entry-by-entry
+    assembly on one host thread beside it. One JSON line."""
+    from fieldcraft_b200 import problems
+    n_el = args.assembly
+    t0 = time.perf_counter()
+    p = problems.lognormal_block(n_el, nrhs=1, seed=SEED)
+    t_builder = time.perf_counter() - t0
+    d = problems.DeviceAssembly(p, device=local)
+    young = torch.from_numpy(p.young).cuda()
+    val = torch.empty(p.csr.val.size, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        d.assemble(young, val, stream_ptr=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        d.assemble(young, val, stream_ptr=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    same = bool(np.array_equal(val.cpu().numpy().view(np.uint64), p.csr.val.view(np.uint64)))
+    fn = lib.fc_test_fem_assemble_host
+    fn.restype = C.c_int
+    keep = [np.ascontiguousarray(a) for a in (p.csr.ptr, p.csr.idx, p.eq, p.young)]
+    out = np.empty(p.csr.val.size)
+    t0 = time.perf_counter()
+    fn(n_el, n_el, n_el, C.c_double(float(n_el)), C.c_double(float(n_el)), C.c_double(float(n_el)), C.c_int64(p.n),
+       *(C.c_void_p(a.ctypes.data) for a in keep), C.c_double(0.3), C.c_void_p(out.ctypes.data))
+    t_host = time.perf_counter() - t0
+    elements = n_el ** 3
+    line = {
+        "metric": "s per assembly of K_ff on the device (element matrices + gather)", "value": ms / 1e3, "unit": "s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"hex8 block {n_el}^3 lognormal E, z=0 clamped", "elements": elements, "n": p.n,
+                   "nnz": int(p.csr.val.size)},
+        "bitwise_equal_to_host_builder": same,
+        "cpu_baseline": {"value": t_host, "unit": "s", "cores": 1, "kind": "port",
+                         "sample": "the same entry-by-entry assembly on one host thread; the host builder's whole "
+                                   f"run (mesh, order, pattern, parallel assembly) took {t_builder:.2f} s"},
+    }
+    print(json.dumps(line), flush=True)
+    d.close()
+
+
 def run_config(args, cfg: int, torch, lib, local: int):
     """Configs other than the headline: FP64 direct solve vs FP32+IR to the config's tolerance on
     the same K (and, for the plate, the learned preconditioner), each timed on the device from
@@ -542,6 +594,12 @@ def main():
     lib = _lib.load()
     if args.profile_kernels:
         profile_kernels(args, torch, lib)
+        return
+    if args.assembly:
+        if rank == 0:
+            run_assembly(args, torch, lib, local)
+        if world > 1:
+            dist.destroy_process_group()
         return
     if args.ldlt:
         if rank == 0:
