@@ -161,3 +161,38 @@ def test_import_refuses_inconsistent_arrays():
     st = _lib.Status()
     h = C.c_void_p()
     assert lib.fc_symbolic_import(C.byref(bad), C.byref(h), C.byref(st)) == 8  # FC_INVALID_ARGUMENT
+
+
+def test_upper_columns_are_the_oracles():
+    """UpperColumns::from_symmetric (cholesky.rs:112-145) in the Python mirror and in the oracle:
+    the same columns, rows and values, on matrices with empty rows and unsymmetric storage order."""
+    rng = np.random.default_rng(4)
+    for n in [0, 1, 7, 40]:
+        dense = np.zeros((n, n))
+        mask = rng.random((n, n)) < 0.2
+        dense[mask] = rng.standard_normal(mask.sum())
+        dense = dense + dense.T
+        if n > 3:
+            dense[2, :] = dense[:, 2] = 0.0  # an empty row
+        csr = Csr.from_dense(dense)
+        up = UpperColumns.from_symmetric(csr)
+        ptr, idx, val = oracle.upper_from_symmetric(csr.n, csr.ptr, csr.idx, csr.val)
+        assert np.array_equal(up.ptr, ptr) and np.array_equal(up.idx, idx) and np.array_equal(up.val, val)
+
+
+def test_status_codes_raise_the_reference_errors():
+    """FactorError (cholesky.rs:346-361) from the ABI's codes: the variant, its column or sizes."""
+    import fieldcraft_b200.cholesky as M
+    cases = [(1, M.NotPositiveDefinite), (2, M.Singular), (3, M.TooLarge), (4, M.OutOfMemory), (5, M.Internal),
+             (6, M.Cancelled), (7, M.Timeout), (8, ValueError), (9, M.DeviceError)]
+    for code, kind in cases:
+        st = _lib.Status()
+        st.code, st.column, st.entries, st.limit, st.message = code, 17, 100, 10, b"why"
+        with pytest.raises(kind) as e:
+            M.raise_for(st)
+        if code in (1, 2):
+            assert e.value.column == 17
+        if code == 3:
+            assert (e.value.entries, e.value.limit) == (100, 10)
+    st = _lib.Status()
+    M.raise_for(st)  # FC_OK
