@@ -15,7 +15,8 @@ struct fc_fem_device {
   fc::assembly::Box box{};
   int64_t n = 0, nnz = 0, elements = 0;
   int device = 0;
-  fc::host::DeviceBuf d_ptr, d_idx, d_node, d_ke, d_bad;
+  int64_t dofs = 0;  // 3 nodes
+  fc::host::DeviceBuf d_ptr, d_idx, d_node, d_eq, d_ke, d_bad;
 };
 
 namespace {
@@ -42,6 +43,16 @@ __global__ void entry_kernel(fc::assembly::Box box, int64_t n, const int64_t *__
   }
 }
 
+// The reactions (zero at free DOFs) and the expanded motion over every DOF, one thread per DOF.
+__global__ void reaction_kernel(fc::assembly::Box box, int64_t dofs, const int64_t *__restrict__ eq,
+                                const double *__restrict__ q, const double *__restrict__ f,
+                                const double *__restrict__ ke, double *__restrict__ r, double *__restrict__ u) {
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < dofs; d += (int64_t)gridDim.x * blockDim.x) {
+    if (u) u[d] = fc::assembly::expanded(eq, q, d);
+    if (r) r[d] = eq[d] >= 0 ? 0.0 : fc::assembly::reaction(box, d / 3, (int)(d % 3), eq, q, f ? f[d] : 0.0, ke);
+  }
+}
+
 int blocks_for(int64_t count) {
   const int64_t b = (count + 127) / 128;
   return (int)(b < 8192 ? (b > 0 ? b : 1) : 8192);
@@ -65,6 +76,8 @@ int fc_fem_device_create(int nx, int ny, int nz, double lx, double ly, double lz
   d->elements = (int64_t)nx * ny * nz;
   d->device = device;
   const int64_t nodes = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  d->dofs = 3 * nodes;
+  std::vector<int64_t> heq(eq, eq + 3 * nodes);
   std::vector<int64_t> node(n / 3, -1), hptr(ptr, ptr + n + 1);
   std::vector<int32_t> hidx(idx, idx + d->nnz);
   bool ok = true;
@@ -82,7 +95,7 @@ int fc_fem_device_create(int nx, int ny, int nz, double lx, double ly, double lz
   }
   cudaStream_t st = nullptr;
   if (fc::host::upload(d->d_ptr, hptr, st) != cudaSuccess || fc::host::upload(d->d_idx, hidx, st) != cudaSuccess ||
-      fc::host::upload(d->d_node, node, st) != cudaSuccess ||
+      fc::host::upload(d->d_node, node, st) != cudaSuccess || fc::host::upload(d->d_eq, heq, st) != cudaSuccess ||
       d->d_ke.alloc(sizeof(double) * 576 * (size_t)d->elements) != cudaSuccess ||
       d->d_bad.alloc(sizeof(int)) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
     delete d;
@@ -106,6 +119,16 @@ int fc_fem_assemble_device(fc_fem_device *d, const double *d_young, double poiss
       cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
     return FC_FEM_INVALID;
   return bad ? FC_FEM_INVALID : FC_FEM_OK;
+}
+
+int fc_fem_reactions_device(fc_fem_device *d, const double *d_q, const double *d_f, double *d_r, double *d_u,
+                            void *stream) {
+  if (!d || (d->n > 0 && !d_q) || (!d_r && !d_u)) return FC_FEM_INVALID;
+  cudaSetDevice(d->device);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  reaction_kernel<<<blocks_for(d->dofs), 128, 0, st>>>(d->box, d->dofs, d->d_eq.as<int64_t>(), d_q, d_f,
+                                                       d->d_ke.as<double>(), d_r, d_u);
+  return cudaStreamSynchronize(st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? FC_FEM_OK : FC_FEM_INVALID;
 }
 
 void fc_fem_device_free(fc_fem_device *d) {

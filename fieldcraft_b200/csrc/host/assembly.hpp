@@ -56,5 +56,32 @@ FC_HEX8_FN double entry(const Box &b, int64_t v, int a, int64_t w, int c, const 
   return acc;
 }
 
+// u over every DOF from the free equations' values q: eq[3 v + a] its equation or -1 (a held
+// DOF, zero motion) (Reduction::expand, crates/solver/src/constraints.rs:929-939).
+FC_HEX8_FN double expanded(const int64_t *eq, const double *q, int64_t dof) {
+  const int64_t e = eq[dof];
+  return e >= 0 ? q[e] : 0.0;
+}
+
+// The reaction at DOF (v, a): row 3 v + a of the whole K times u (over every DOF, held ones at
+// zero), the row's entries in column order, less the applied load f_va (Reduction::reactions,
+// constraints.rs:1001-1015, a plain clamp's T_p row). The row's columns are the DOFs of the nodes
+// sharing an element with v, by node index then direction.
+FC_HEX8_FN double reaction(const Box &b, int64_t v, int a, const int64_t *eq, const double *q, double f_va,
+                           const double *ke) {
+  const int64_t px = b.nx + 1, py = b.ny + 1, pz = b.nz + 1;
+  const int64_t iv = v % px, jv = (v / px) % py, kv = v / (px * py);
+  double ku = 0.0;
+  for (int64_t dk = -1; dk <= 1; ++dk)
+    for (int64_t dj = -1; dj <= 1; ++dj)
+      for (int64_t di = -1; di <= 1; ++di) {
+        const int64_t i = iv + di, j = jv + dj, k = kv + dk;
+        if (i < 0 || j < 0 || k < 0 || i >= px || j >= py || k >= pz) continue;
+        const int64_t w = i + px * (j + py * k);
+        for (int c = 0; c < 3; ++c) ku = hex8::add(ku, hex8::mul(entry(b, v, a, w, c, ke), expanded(eq, q, 3 * w + c)));
+      }
+  return hex8::sub(ku, f_va);
+}
+
 }  // namespace assembly
 }  // namespace fc

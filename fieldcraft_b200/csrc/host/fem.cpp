@@ -337,6 +337,23 @@ int fc_test_fem_assemble_host(int nx, int ny, int nz, double lx, double ly, doub
   return FC_FEM_OK;
 }
 
+// Not part of the public ABI: the reactions at the held DOFs (zero elsewhere) for the free
+// equations' solution q and the loads f over every DOF, with the device assembly's code, for tests.
+int fc_test_fem_reactions_host(int nx, int ny, int nz, double lx, double ly, double lz, const int64_t *eq,
+                               const double *young, double poisson, const double *q, const double *f, double *r) {
+  const fc::assembly::Box box{nx, ny, nz, lx, ly, lz};
+  const int64_t elements = (int64_t)nx * ny * nz, nodes = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  std::vector<double> ke((size_t)elements * 576);
+  for (int64_t e = 0; e < elements; ++e) {
+    double x[24];
+    fc::assembly::element_corners(box, e, x);
+    if (!fc::hex8::stiffness(x, young[e], poisson, ke.data() + e * 576)) return FC_FEM_INVALID;
+  }
+  for (int64_t d = 0; d < 3 * nodes; ++d)
+    r[d] = eq[d] >= 0 ? 0.0 : fc::assembly::reaction(box, d / 3, (int)(d % 3), eq, q, f[d], ke.data());
+  return FC_FEM_OK;
+}
+
 int fc_hex8_stiffness(const double *xyz24, double young, double poisson, double *out576) {
   if (!xyz24 || !out576) return FC_FEM_INVALID;
   return hex8_stiffness(xyz24, young, poisson, out576) ? FC_FEM_OK : FC_FEM_INVALID;

@@ -89,6 +89,15 @@ class DeviceAssembly:
         if rc != 0:
             raise ValueError(f"fc_fem_assemble_device failed ({rc})")
 
+    def reactions(self, q, r=None, u=None, f=None, stream_ptr: int | None = None):
+        """After assemble(): from the free solution q (a CUDA tensor of n doubles), the motion of every
+        DOF into u and the reactions at the held DOFs into r (CUDA tensors of 3 nodes doubles, either
+        may be None), with the loads f over every DOF (None: none)."""
+        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+        rc = _lib.load().fc_fem_reactions_device(self.handle, p(q), p(f), p(r), p(u), C.c_void_p(stream_ptr or 0))
+        if rc != 0:
+            raise ValueError(f"fc_fem_reactions_device failed ({rc})")
+
     def close(self):
         if getattr(self, "handle", None):
             _lib.load().fc_fem_device_free(self.handle)

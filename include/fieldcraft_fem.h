@@ -74,6 +74,13 @@ typedef struct fc_fem_device fc_fem_device;
 int fc_fem_device_create(int nx, int ny, int nz, double lx, double ly, double lz, int64_t n, const int64_t *ptr,
                          const int32_t *idx, const int64_t *eq, int device, fc_fem_device **out);
 int fc_fem_assemble_device(fc_fem_device *d, const double *d_young, double poisson, double *d_val, void *stream);
+/* After fc_fem_assemble_device, from the free equations' solution d_q[n] (device): the motion of
+ * every DOF d_u[3 nodes] (zero where held; Reduction::expand, constraints.rs:929-939) and the
+ * reactions d_r[3 nodes] at the held DOFs, K u - f over each whole row in column order (zero at
+ * free DOFs; Reduction::reactions, constraints.rs:1001-1015), with the loads d_f[3 nodes] (NULL:
+ * none). Either output may be NULL. Waits for `stream`. */
+int fc_fem_reactions_device(fc_fem_device *d, const double *d_q, const double *d_f, double *d_r, double *d_u,
+                            void *stream);
 void fc_fem_device_free(fc_fem_device *d);
 
 #ifdef __cplusplus

@@ -56,3 +56,60 @@ def test_device_assembly_is_the_builders(cuda):
     with pytest.raises(ValueError):
         d.assemble(young, val)
     d.close()
+
+
+def host_reactions(nx, ny, nz, lx, ly, lz, p, young, q, f_full, poisson=0.3):
+    lib = _lib.load()
+    fn = lib.fc_test_fem_reactions_host
+    fn.restype = C.c_int
+    young = np.ascontiguousarray(np.broadcast_to(np.asarray(young, np.float64), (nx * ny * nz,)))
+    r = np.empty(p.eq.size)
+    keep = [np.ascontiguousarray(a, np.float64) if a.dtype.kind == "f" else np.ascontiguousarray(a)
+            for a in (p.eq, young, q, f_full)]
+    rc = fn(nx, ny, nz, C.c_double(lx), C.c_double(ly), C.c_double(lz), C.c_void_p(keep[0].ctypes.data),
+            C.c_void_p(keep[1].ctypes.data), C.c_double(poisson), C.c_void_p(keep[2].ctypes.data),
+            C.c_void_p(keep[3].ctypes.data), C.c_void_p(r.ctypes.data))
+    assert rc == 0
+    return r
+
+
+def test_reactions_balance_the_loads():
+    """The reactions at the clamped face (constraints.rs:1001-1015, a plain clamp) for the
+    oracle's solution of the cantilever (1 kN total, -z): they balance the applied load in every
+    direction, and the free DOFs carry none."""
+    from oracle import oracle
+    p = problems.cantilever()
+    up = p.upper()
+    s = oracle.Sym(up.n, up.ptr, up.idx)
+    q = oracle.Fac(s, up.val).solve(p.rhs[:, 0].copy())
+    r = host_reactions(40, 4, 4, 100.0, 10.0, 10.0, p, 210e3, q, np.zeros(p.eq.size))
+    held = p.eq < 0
+    assert np.all(r[~held] == 0.0) and np.any(r[held] != 0.0)
+    dofs = np.flatnonzero(held)
+    total = np.array([r[dofs[dofs % 3 == a]].sum() for a in range(3)])
+    applied = np.array([0.0, 0.0, -1000.0])
+    assert np.max(np.abs(total + applied)) <= 1e-8 * 1000.0, total
+
+
+@pytest.mark.gpu
+@pytest.mark.skip(reason="the device reactions have not run on a GPU yet")
+def test_device_reactions_are_the_hosts(cuda):
+    """fc_fem_reactions_device: the motion of every DOF and the reactions at the held ones, as the
+    host code gives them for the same solution, bit for bit."""
+    from oracle import oracle
+    torch = cuda
+    p = problems.cantilever()
+    up = p.upper()
+    q = oracle.Fac(oracle.Sym(up.n, up.ptr, up.idx), up.val).solve(p.rhs[:, 0].copy())
+    d = problems.DeviceAssembly(p)
+    young = torch.full((40 * 4 * 4,), 210e3, dtype=torch.float64, device="cuda")
+    val = torch.empty(p.csr.val.size, dtype=torch.float64, device="cuda")
+    d.assemble(young, val)
+    r = torch.empty(p.eq.size, dtype=torch.float64, device="cuda")
+    u = torch.empty_like(r)
+    d.reactions(torch.from_numpy(q).cuda(), r=r, u=u)
+    want = host_reactions(40, 4, 4, 100.0, 10.0, 10.0, p, 210e3, q, np.zeros(p.eq.size))
+    assert np.array_equal(r.cpu().numpy().view(np.uint64), want.view(np.uint64))
+    expected_u = np.where(p.eq >= 0, q[np.maximum(p.eq, 0)], 0.0)
+    assert np.array_equal(u.cpu().numpy(), expected_u)
+    d.close()
