@@ -74,6 +74,7 @@ SIGNATURES = {
     "fc_fem_device_create": (i32, [i32, i32, i32, f64, f64, f64, i64, P, P, P, i32, C.POINTER(P)]),
     "fc_fem_assemble_device": (i32, [P, P, f64, P, P]),
     "fc_fem_reactions_device": (i32, [P, P, P, P, P, P]),
+    "fc_fem_stresses_device": (i32, [P, P, f64, P, P, P, P, P]),
     "fc_fem_device_free": (None, [P]),
     # fieldcraft_unet.h
     "fc_unet_create": (i32, [i32, i32, i32, i64, P, P, f64, u64, i32, C.POINTER(P), C.POINTER(Status)]),

@@ -1,7 +1,8 @@
 // K_ff of a structured hex8 box assembled on the device (include/fieldcraft_fem.h): the element
 // matrices (host/hex8.hpp, one thread per element), then every entry as the sum over the elements
 // holding both its nodes in element label order (host/assembly.hpp, one thread per row), the
-// host builder's operations in its order, so the values are its bits.
+// host builder's operations in its order, so the values are its bits. After the solve: the motion
+// of every DOF, the reactions at the held ones, and the stresses (host/stress.hpp).
 #include <cstdint>
 #include <vector>
 
@@ -10,6 +11,7 @@
 #include "../../include/fieldcraft_fem.h"
 #include "device_buf.hpp"
 #include "host/assembly.hpp"
+#include "host/stress.hpp"
 
 struct fc_fem_device {
   fc::assembly::Box box{};
@@ -17,6 +19,7 @@ struct fc_fem_device {
   int device = 0;
   int64_t dofs = 0;  // 3 nodes
   fc::host::DeviceBuf d_ptr, d_idx, d_node, d_eq, d_ke, d_bad;
+  fc::host::DeviceBuf d_corner;  // stress recovery: each element's corner values (48 doubles)
 };
 
 namespace {
@@ -50,6 +53,38 @@ __global__ void reaction_kernel(fc::assembly::Box box, int64_t dofs, const int64
   for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < dofs; d += (int64_t)gridDim.x * blockDim.x) {
     if (u) u[d] = fc::assembly::expanded(eq, q, d);
     if (r) r[d] = eq[d] >= 0 ? 0.0 : fc::assembly::reaction(box, d / 3, (int)(d % 3), eq, q, f ? f[d] : 0.0, ke);
+  }
+}
+
+// Stress recovery: per element its Gauss-point and corner stresses (one thread per element),
+// then per node the mean over its elements and its von Mises stress (one thread per node).
+__global__ void stress_element_kernel(fc::assembly::Box box, int64_t elements, const double *__restrict__ young,
+                                      double nu, const double *__restrict__ u, double *__restrict__ points,
+                                      double *__restrict__ corner, int *__restrict__ bad) {
+  const int64_t px = box.nx + 1, py = box.ny + 1;
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < elements; e += (int64_t)gridDim.x * blockDim.x) {
+    double x[24], ue[24], pts[48];
+    fc::assembly::element_corners(box, e, x);
+    const int64_t ex = e % box.nx, ey = (e / box.nx) % box.ny, ez = e / ((int64_t)box.nx * box.ny);
+    for (int c = 0; c < 8; ++c) {
+      const int64_t v = (ex + off[c][0]) + px * ((ey + off[c][1]) + py * (ez + off[c][2]));
+      for (int a = 0; a < 3; ++a) ue[3 * c + a] = u[3 * v + a];
+    }
+    if (!fc::stress::element_stresses(x, young[e], nu, ue, pts, corner + e * 48)) atomicExch(bad, 1);
+    if (points)
+      for (int q = 0; q < 48; ++q) points[e * 48 + q] = pts[q];
+  }
+}
+
+__global__ void stress_node_kernel(fc::assembly::Box box, int64_t nodes, const double *__restrict__ corner,
+                                   double *__restrict__ nodal, double *__restrict__ von_mises) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nodes; v += (int64_t)gridDim.x * blockDim.x) {
+    double s[6];
+    fc::stress::nodal_mean(box, v, corner, s);
+    if (nodal)
+      for (int k = 0; k < 6; ++k) nodal[v * 6 + k] = s[k];
+    if (von_mises) von_mises[v] = fc::stress::von_mises(s);
   }
 }
 
@@ -129,6 +164,25 @@ int fc_fem_reactions_device(fc_fem_device *d, const double *d_q, const double *d
   reaction_kernel<<<blocks_for(d->dofs), 128, 0, st>>>(d->box, d->dofs, d->d_eq.as<int64_t>(), d_q, d_f,
                                                        d->d_ke.as<double>(), d_r, d_u);
   return cudaStreamSynchronize(st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? FC_FEM_OK : FC_FEM_INVALID;
+}
+
+int fc_fem_stresses_device(fc_fem_device *d, const double *d_young, double poisson, const double *d_u,
+                           double *d_points, double *d_nodal, double *d_von_mises, void *stream) {
+  if (!d || !d_young || !d_u) return FC_FEM_INVALID;
+  cudaSetDevice(d->device);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!d->d_corner.p && d->d_corner.alloc(sizeof(double) * 48 * (size_t)d->elements) != cudaSuccess)
+    return FC_FEM_NOMEM;
+  cudaMemsetAsync(d->d_bad.p, 0, sizeof(int), st);
+  stress_element_kernel<<<blocks_for(d->elements), 128, 0, st>>>(d->box, d->elements, d_young, poisson, d_u, d_points,
+                                                                  d->d_corner.as<double>(), d->d_bad.as<int>());
+  stress_node_kernel<<<blocks_for(d->dofs / 3), 128, 0, st>>>(d->box, d->dofs / 3, d->d_corner.as<double>(), d_nodal,
+                                                               d_von_mises);
+  int bad = 0;
+  if (cudaMemcpyAsync(&bad, d->d_bad.p, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return FC_FEM_INVALID;
+  return bad ? FC_FEM_INVALID : FC_FEM_OK;
 }
 
 void fc_fem_device_free(fc_fem_device *d) {

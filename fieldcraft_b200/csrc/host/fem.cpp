@@ -4,6 +4,7 @@
 #include "fieldcraft_fem.h"
 #include "assembly.hpp"
 #include "hex8.hpp"
+#include "stress.hpp"
 
 #include <algorithm>
 #include <atomic>
@@ -351,6 +352,35 @@ int fc_test_fem_reactions_host(int nx, int ny, int nz, double lx, double ly, dou
   }
   for (int64_t d = 0; d < 3 * nodes; ++d)
     r[d] = eq[d] >= 0 ? 0.0 : fc::assembly::reaction(box, d / 3, (int)(d % 3), eq, q, f[d], ke.data());
+  return FC_FEM_OK;
+}
+
+// Not part of the public ABI: stress recovery with the device code (host/stress.hpp) on the host,
+// for tests. u over every DOF (3 nodes); points[elements * 48], nodal_node[nodes * 6] (the mean
+// over the elements holding each node), von_mises[nodes].
+int fc_test_fem_stresses_host(int nx, int ny, int nz, double lx, double ly, double lz, const double *young,
+                              double poisson, const double *u, double *points, double *nodal_node,
+                              double *von_mises) {
+  const fc::assembly::Box box{nx, ny, nz, lx, ly, lz};
+  const int64_t elements = (int64_t)nx * ny * nz, nodes = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  const int64_t px = nx + 1, py = ny + 1;
+  std::vector<double> nodal((size_t)elements * 48);
+  for (int64_t e = 0; e < elements; ++e) {
+    double x[24], ue[24];
+    fc::assembly::element_corners(box, e, x);
+    const int64_t ex = e % nx, ey = (e / nx) % ny, ez = e / ((int64_t)nx * ny);
+    const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int c = 0; c < 8; ++c) {
+      const int64_t v = (ex + off[c][0]) + px * ((ey + off[c][1]) + py * (ez + off[c][2]));
+      for (int a = 0; a < 3; ++a) ue[3 * c + a] = u[3 * v + a];
+    }
+    if (!fc::stress::element_stresses(x, young[e], poisson, ue, points + e * 48, nodal.data() + e * 48))
+      return FC_FEM_INVALID;
+  }
+  for (int64_t v = 0; v < nodes; ++v) {
+    fc::stress::nodal_mean(box, v, nodal.data(), nodal_node + v * 6);
+    von_mises[v] = fc::stress::von_mises(nodal_node + v * 6);
+  }
   return FC_FEM_OK;
 }
 

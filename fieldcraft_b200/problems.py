@@ -98,6 +98,17 @@ class DeviceAssembly:
         if rc != 0:
             raise ValueError(f"fc_fem_reactions_device failed ({rc})")
 
+    def stresses(self, young, u, points=None, nodal=None, von_mises=None, poisson: float = 0.3,
+                 stream_ptr: int | None = None):
+        """Stress recovery from the motion of every DOF u (a CUDA tensor of 3 nodes doubles): the
+        Gauss-point stresses (elements x 48), the nodal means (nodes x 6), the von Mises stress
+        (nodes); CUDA tensors or None."""
+        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+        rc = _lib.load().fc_fem_stresses_device(self.handle, p(young), float(poisson), p(u), p(points), p(nodal),
+                                                p(von_mises), C.c_void_p(stream_ptr or 0))
+        if rc != 0:
+            raise ValueError(f"fc_fem_stresses_device failed ({rc})")
+
     def close(self):
         if getattr(self, "handle", None):
             _lib.load().fc_fem_device_free(self.handle)

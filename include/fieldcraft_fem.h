@@ -81,6 +81,13 @@ int fc_fem_assemble_device(fc_fem_device *d, const double *d_young, double poiss
  * none). Either output may be NULL. Waits for `stream`. */
 int fc_fem_reactions_device(fc_fem_device *d, const double *d_q, const double *d_f, double *d_r, double *d_u,
                             void *stream);
+/* Stress recovery (analysis.rs:478-540, element.rs:587-670, 775-860, material.rs:88-93) from the
+ * motion of every DOF d_u[3 nodes]: per element the stresses at its 2 x 2 x 2 Gauss points
+ * d_points[elements * 48] (xi fastest; xx yy zz xy xz yz), extrapolated to its corners; per node
+ * the mean over the elements holding it d_nodal[nodes * 6] and its von Mises stress
+ * d_von_mises[nodes]. Any output may be NULL. Waits for `stream`. */
+int fc_fem_stresses_device(fc_fem_device *d, const double *d_young, double poisson, const double *d_u,
+                           double *d_points, double *d_nodal, double *d_von_mises, void *stream);
 void fc_fem_device_free(fc_fem_device *d);
 
 #ifdef __cplusplus
