@@ -133,3 +133,82 @@ def test_fold_and_solve_on_the_folded_structure(name):
     got[new_perm] = y
     assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))  # the path's accuracy bar
     assert np.max(np.abs(got - x_true)) < 1e-9
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_fold_on_random_sparse_indefinite_matrices(seed):
+    """Random sparse symmetric matrices with small and negative diagonals (2 x 2 pivots, many
+    supernodes, interchanges): the folded structure's solve is the oracle's to the path's bar."""
+    rng = np.random.default_rng(seed)
+    n = 150
+    rows = [[] for _ in range(n)]
+    for i in range(n):
+        rows[i].append((i, float(rng.choice([0.05, -3.0, 4.0, 8.0]))))
+    for _ in range(3 * n):
+        i, j = rng.integers(0, n, 2)
+        if i != j:
+            v = float(rng.standard_normal())
+            rows[i].append((int(j), v))
+            rows[j].append((int(i), v))
+    merged = []
+    for r in rows:
+        acc = {}
+        for c, v in r:
+            acc[c] = acc.get(c, 0.0) + v
+        merged.append(sorted(acc.items()))
+    a = H.rows_to_csr(merged)
+    ptr, idx, val = oracle.upper_from_symmetric(a.n, a.ptr, a.idx, a.val)
+    s = oracle.Sym(a.n, ptr, idx)
+    try:
+        f = oracle.Ldlt(s, val)
+    except oracle.OracleError:
+        pytest.skip("singular within a supernode")
+    piv, order = f.pivots()
+    new_perm, new_rows, frm, rel = fold(s, order)
+    first, rptr = s.array("first"), s.array("rptr")
+    values = f.values()
+    ns = s.info("ns")
+    L, D, E = [], np.zeros(n), np.zeros(n)
+    at, at_from = 0, 0
+    for k in range(ns):
+        f0, w, m = first[k], first[k + 1] - first[k], rptr[k + 1] - rptr[k]
+        F = np.zeros((m, w))
+        for c in range(w):
+            F[c:, c] = values[at:at + m - c]
+            at += m - c
+        for c in range(w):
+            D[f0 + c] = F[c, c]
+            F[c, c] = 1.0
+            if piv[f0 + c] == 1:
+                E[f0 + c] = F[c + 1, c]
+                F[c + 1, c] = 0.0
+        F[w:] = F[w:][frm[at_from:at_from + m - w]]
+        at_from += m - w
+        L.append(F)
+    b = rng.standard_normal(n)
+    want = f.solve(b.copy())
+    y = b[new_perm].copy()
+    for k in range(ns):
+        f0, w, m = first[k], first[k + 1] - first[k], rptr[k + 1] - rptr[k]
+        r = new_rows[rptr[k]:rptr[k + 1]]
+        for q in range(w):
+            y[r[q + 1:m]] -= L[k][q + 1:m, q] * y[f0 + q]
+    c = 0
+    while c < n:
+        if piv[c] == 1:
+            d11, d21, d22 = D[c], E[c], D[c + 1]
+            det = d11 * d22 - d21 * d21
+            p_, q_ = y[c], y[c + 1]
+            y[c], y[c + 1] = (d22 * p_ - d21 * q_) / det, (d11 * q_ - d21 * p_) / det
+            c += 2
+        else:
+            y[c] /= D[c]
+            c += 1
+    for k in reversed(range(ns)):
+        f0, w, m = first[k], first[k + 1] - first[k], rptr[k + 1] - rptr[k]
+        r = new_rows[rptr[k]:rptr[k + 1]]
+        for q in reversed(range(w)):
+            y[f0 + q] -= float(L[k][q + 1:m, q] @ y[r[q + 1:m]])
+    got = np.empty(n)
+    got[new_perm] = y
+    assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))
