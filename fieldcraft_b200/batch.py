@@ -56,6 +56,7 @@ class BatchFactor:
     stacked vectors; a failing pivot is reported as (system, column)."""
 
     def __init__(self, parts: list[UpperColumns], max_entries: int, precision: int = FP64, device: int = 0):
+        self._csr_dev = None
         self.sizes = np.array([p.n for p in parts], np.int64)
         self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
         self.nnz = np.array([int(p.ptr[-1]) for p in parts], np.int64)
@@ -91,6 +92,40 @@ class BatchFactor:
             block[self.offsets[b]:self.offsets[b + 1], :] = r.reshape(self.sizes[b], k)
         self.factor_.solve_many(block)
         return [block[self.offsets[b]:self.offsets[b + 1], :].copy() for b in range(len(rhs))]
+
+    def refine_solve(self, csrs, rhs: list[np.ndarray], tol: float = 1e-10, torch=None, max_iter: int = 40):
+        """Iterative refinement in FP64 around the batch's factor (FP32 or FP64) until every system
+        reaches ||b_s - A_s x_s|| <= tol ||b_s|| for each of its right-hand sides: each system's
+        right-hand sides are scaled to unit norm and the stacked system is refined to
+        tol / sqrt(systems), which bounds every system's own residual by tol. `csrs` are the
+        systems' rows (Csr); returns the solutions in the shapes of `rhs`."""
+        import torch as _torch_default
+        torch = torch or _torch_default
+        k = rhs[0].shape[1] if rhs[0].ndim == 2 else 1
+        if getattr(self, "_csr_dev", None) is None:
+            ptr, idx, val = [np.zeros(1, np.int64)], [], []
+            z = 0
+            for b, c in enumerate(csrs):
+                ptr.append(c.ptr[1:].astype(np.int64) + z)
+                idx.append(c.idx.astype(np.int64) + self.offsets[b])
+                val.append(c.val)
+                z += int(c.ptr[-1])
+            self._csr_dev = (torch.from_numpy(np.concatenate(ptr)).cuda(),
+                             torch.from_numpy(np.concatenate(idx).astype(np.int32)).cuda(),
+                             torch.from_numpy(np.concatenate(val).astype(np.float64)).cuda())
+        block = np.zeros((k, self.n))
+        scale = np.ones((len(rhs), k))
+        for b, r in enumerate(rhs):
+            r = r.reshape(self.sizes[b], k)
+            nb = np.linalg.norm(r, axis=0)
+            scale[b] = np.where(nb > 0, nb, 1.0)
+            block[:, self.offsets[b]:self.offsets[b + 1]] = (r / scale[b]).T
+        d_b = torch.from_numpy(block).cuda()
+        d_x = torch.zeros_like(d_b)
+        self.factor_.refine_solve_device(self._csr_dev, d_b, d_x, k, self.n, tol=tol / np.sqrt(len(rhs)),
+                                         max_iter=max_iter)
+        x = d_x.cpu().numpy()
+        return [(x[:, self.offsets[b]:self.offsets[b + 1]].T * scale[b]).copy() for b in range(len(rhs))]
 
     def entries(self) -> int:
         return self.factor_.entries()

@@ -37,6 +37,11 @@ _SIG = {
     "or_ldlt_pivots": (None, [P, P, P]),
     "or_ldlt_info": (i64, [P, C.c_int]),
     "or_ldlt_solve": (C.c_int, [P, P, i64]),
+    "or_fem_box": (C.c_int, [i64, i64, i64, C.c_double, C.c_double, C.c_double, P, C.c_double, P, C.c_int,
+                             C.POINTER(P)]),
+    "or_fem_info": (i64, [P, C.c_int]),
+    "or_fem_export": (None, [P, P, P, P, P, P]),
+    "or_fem_free": (None, [P]),
 }
 _lib = None
 
@@ -52,10 +57,17 @@ def build():
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
+def _stale() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    return any(src.stat().st_mtime > t for src in HERE.glob("*.cpp") if src.exists())
+
+
 def load():
     global _lib
     if _lib is None:
-        if not LIB.exists():
+        if _stale():
             build()
         lib = C.CDLL(str(LIB))
         for k, (r, a) in _SIG.items():
@@ -71,6 +83,30 @@ def _p(a):
 
 def set_threads(t: int):
     load().or_set_threads(int(t))
+
+
+def fem_box(nx, ny, nz, lx, ly, lz, young, nu, clamped_nodes, threads=0):
+    """The oracle's own K_ff of an nx x ny x nz hex8 box (fem_oracle.cpp): `young` per element
+    (label order) or one value, `clamped_nodes` a boolean mask over the nodes. Returns (n, ptr,
+    idx, val, order, eq): K_ff by rows, the node elimination order and each mesh DOF's equation."""
+    import os
+    lib = load()
+    ne = nx * ny * nz
+    young = np.ascontiguousarray(np.broadcast_to(np.asarray(young, np.float64), (ne,)), np.float64)
+    clamped = np.ascontiguousarray(clamped_nodes, np.uint8)
+    h = P()
+    rc = lib.or_fem_box(nx, ny, nz, lx, ly, lz, young.ctypes.data, float(nu), clamped.ctypes.data,
+                        int(threads or os.cpu_count() or 1), C.byref(h))
+    if rc != 0:
+        raise OracleError(rc)
+    try:
+        n, nnz, nodes = (int(lib.or_fem_info(h, w)) for w in range(3))
+        ptr, idx, val = np.empty(n + 1, np.int64), np.empty(nnz, np.int32), np.empty(nnz)
+        order, eq = np.empty(nodes, np.int64), np.empty(3 * nodes, np.int64)
+        lib.or_fem_export(h, ptr.ctypes.data, idx.ctypes.data, val.ctypes.data, order.ctypes.data, eq.ctypes.data)
+    finally:
+        lib.or_fem_free(h)
+    return n, ptr, idx, val, order, eq
 
 
 class OracleError(Exception):

@@ -41,7 +41,6 @@ def test_entry_by_entry_assembly_is_the_builders(case):
 
 
 @pytest.mark.gpu
-@pytest.mark.skip(reason="the device assembly has not run on a GPU yet")
 def test_device_assembly_is_the_builders(cuda):
     """fc_fem_assemble_device: K_ff on the GPU from element moduli in device memory, the
     builder's values bit for bit."""
@@ -92,7 +91,6 @@ def test_reactions_balance_the_loads():
 
 
 @pytest.mark.gpu
-@pytest.mark.skip(reason="the device reactions have not run on a GPU yet")
 def test_device_reactions_are_the_hosts(cuda):
     """fc_fem_reactions_device: the motion of every DOF and the reactions at the held ones, as the
     host code gives them for the same solution, bit for bit."""
@@ -156,7 +154,6 @@ def test_a_linear_field_gives_its_constant_stress():
 
 
 @pytest.mark.gpu
-@pytest.mark.skip(reason="the device stress recovery has not run on a GPU yet")
 def test_device_stresses_are_the_hosts(cuda):
     """fc_fem_stresses_device: Gauss-point stresses, nodal means and von Mises as the host code gives
     them for the same motion, bit for bit."""

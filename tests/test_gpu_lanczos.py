@@ -1,16 +1,15 @@
 """Shift-invert block Lanczos on the GPU factor (fieldcraft_b200/lanczos.py ShiftInvert): every
 Lanczos block one solve_many of the Cholesky factor of K - sigma I; the lowest eigenvalues of a
 hex8 stiffness matrix against the dense eigenproblem's, to 1e-8 relative.
-
-Skipped until its first GPU run: the iteration is checked on the CPU against the reference's own
-test (tests/test_lanczos.py) and the factor's solves by tests/test_gpu_factor.py."""
+The iteration itself is checked on the CPU against the reference's own test
+(tests/test_lanczos.py)."""
 import numpy as np
 import pytest
 
 from fieldcraft_b200 import problems
 from fieldcraft_b200.lanczos import ShiftInvert, Wanted, lanczos
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="the GPU Lanczos operator has not run on a GPU yet")]
+pytestmark = pytest.mark.gpu
 
 
 def test_lowest_modes_of_a_stiffness_matrix(cuda):

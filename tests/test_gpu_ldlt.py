@@ -3,10 +3,8 @@ inertia exactly, the factor's values within 1e-11 of the largest entry where the
 same (the updates run on the FP64 tensor pipe with fused multiply-adds, so a near tie in the rook
 search may choose another, equally valid pivot), solutions within 1e-10 of the oracle's and
 solve_many bit for bit the single solves, values unchanged by a solve, singular columns named.
-
-Skipped until these kernels have run on a GPU: the panel's source is checked bit for bit on the
-CPU (tests/test_ldlt_panel_emulated.py) and the solve's structure by tests/test_ldlt_fold.py; the
-plan and the launches have not run yet."""
+The panel's source is also checked bit for bit on the CPU (tests/test_ldlt_panel_emulated.py) and
+the solve's structure by tests/test_ldlt_fold.py."""
 import numpy as np
 import pytest
 
@@ -14,7 +12,7 @@ import helpers as H
 from fieldcraft_b200 import Kind, LdltFactor, NotPositiveDefinite, Singular, Symmetric, UpperColumns
 from oracle import oracle
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="the device LDL^T has not run on a GPU yet")]
+pytestmark = pytest.mark.gpu
 
 
 def both(a):
