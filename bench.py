@@ -611,6 +611,167 @@ def run_config(args, cfg: int, torch, lib, local: int):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_sharded(args, torch, rank: int, world: int, local: int):
+    """The 256 uneven boxes over `world` GPUs (one rank each): ShardedBatch gives each rank a share
+    of about equal estimated factor work, each rank factors its share and refines it to 1e-10 per
+    system from inputs in its own HBM (no collective on the data path), the step time is the
+    slowest rank's (CUDA events, max over ranks), and one all-gather brings every solution to
+    every rank at the end (timed apart). FP64 and FP32+IR. One JSON line from rank 0."""
+    import torch.distributed as dist
+    from fieldcraft_b200 import FP32_IR, FP64, problems
+    from fieldcraft_b200.batch import ShardedBatch
+    boxes = list(problems.uneven_boxes(count=256, lo=4, hi=24, nrhs=8, seed=11))
+    out = {}
+    for prec in (FP64, FP32_IR):
+        sb = ShardedBatch(boxes, rank, world, precision=prec, device=local)
+        sb.upload(torch)
+        times, worst = [], 0.0
+        for it in range(args.warmup + args.steps):
+            dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = sb.step(tol=1e-10)
+            e1.record()
+            e1.synchronize()
+            if it >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+                worst = max(worst, float(np.max(r[0])) if r is not None else 0.0)
+        t = torch.tensor([float(np.mean(times)), worst], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        torch.cuda.synchronize()
+        g0 = time.perf_counter()
+        xs = sb.gather(sb.local_solutions(), torch=torch, device=f"cuda:{local}")
+        gather_s = time.perf_counter() - g0
+        # every system's own residual, on the host of rank 0 (the gathered solutions)
+        res = 0.0
+        if rank == 0:
+            from oracle import oracle
+            for b, x in zip(boxes, xs):
+                for j in range(x.shape[1]):
+                    rr = oracle.spmv(b.n, b.csr.ptr, b.csr.idx, b.csr.val, x[:, j]) - b.rhs[:, j]
+                    res = max(res, float(np.linalg.norm(rr) / np.linalg.norm(b.rhs[:, j])))
+        out[prec] = {"ms": float(t[0].item()), "relres_max": float(t[1].item()), "gather_s": gather_s,
+                     "per_system_relres_max": res, "share_systems": len(sb.share)}
+        sb.close()
+    if rank == 0:
+        ms = out[FP64]["ms"]
+        line = {
+            "metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "256 independent hex8 boxes, nx,ny,nz ~ U{4..24}, E ~ U[70,210] GPa, "
+                                   "nu ~ U[0.25,0.35], z=0 clamped, 8 RHS each, sharded over the GPUs by estimated "
+                                   "factor work", "config": 3, "systems": len(boxes), "parallelism": f"shard x{world}"},
+            "relres_max": out[FP64]["relres_max"], "per_system_relres_max": out[FP64]["per_system_relres_max"],
+            "gather_s": out[FP64]["gather_s"],
+            "fp32_ir": {"value": out[FP32_IR]["ms"] / 1e3, "unit": UNIT,
+                        "speedup_vs_fp64": ms / out[FP32_IR]["ms"], "relres_max": out[FP32_IR]["relres_max"],
+                        "per_system_relres_max": out[FP32_IR]["per_system_relres_max"]},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def hbm_peak() -> tuple:
+    """The measured HBM copy bandwidth (GB/s) and where it comes from."""
+    mp = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(mp.read_text())["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s (no measured peaks file)"
+
+
+def recorded_traffic(kernel: str, n_el: int):
+    """DRAM bytes per launch of `kernel` from the ncu capture recorded in profiles/traffic.json,
+    used only while the kernel's source is the one captured (its SHA-256 recorded beside the
+    figure); otherwise None and why."""
+    import hashlib
+    rec_file = ROOT / "profiles" / "traffic.json"
+    try:
+        rec = json.loads(rec_file.read_text())[kernel]
+    except (OSError, KeyError, ValueError):
+        return None, "no ncu capture recorded for this kernel"
+    src = ROOT / rec["source"]
+    sha = hashlib.sha256(src.read_bytes()).hexdigest() if src.exists() else None
+    if sha != rec["source_sha256"]:
+        return None, f"the recorded ncu capture was of another build of {rec['source']}"
+    if rec.get("n_el") not in (None, n_el):
+        return None, "the recorded capture is scaled to another workload size"
+    return int(rec["bytes_per_launch"]), rec["how"]
+
+
+def stream_time(torch, stream, fn, reps: int = 5, warm: int = 2) -> float:
+    """Median milliseconds of fn() on `stream` (CUDA events), after warm-up."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def solve_only(lib, f, d_x, d_f, R, n, stream):
+    import torch
+    with torch.cuda.stream(stream):
+        d_x.copy_(d_f)
+        assert lib.fc_chol_solve_device_async(f.handle, C.c_void_p(d_x.data_ptr()), R, n) == 0
+
+
+def assembly_bytes(f) -> float:
+    """The front assembly's algorithmic bytes per factorisation (FP64 entries): every value of A
+    read once, every child's update-matrix entry (lower triangle) read once, every front entry
+    (the L trapezoid and the update matrix's lower triangle) written once."""
+    from fieldcraft_b200.cholesky import Symbolic  # noqa: F401
+    a = f.symbolic.arrays()
+    w = np.diff(a["first"]).astype(np.float64)
+    m = np.diff(a["rptr"]).astype(np.float64)
+    u = m - w
+    lower_u = u * (u + 1) / 2
+    trap = w * m - w * (w - 1) / 2
+    has_parent = u > 0
+    nnz_upper = float(a["nnz"]) if "nnz" in a else float(a["slot"].size)
+    return 8.0 * (nnz_upper + lower_u[has_parent].sum() + trap.sum() + lower_u.sum())
+
+
+def roofline_table(p, f, ms_k, cnt_k, gemm_flops, dgemm, solve_graph_ms, spmv_ms, R, hbm):
+    """Achieved rate and fraction of peak for every kernel class of the step, from algorithmic
+    work over CUDA-event times: the FP64 update GEMM (flops, against cuBLAS DGEMM measured in the
+    run), the front assembly (bytes, HBM), the triangular solve of R right-hand sides (bytes and
+    flops; timed alone, graph replay), the residual SpMV (bytes, HBM)."""
+    hbm_gbs, hbm_src = hbm
+    entries = float(f.entries())
+    n, nnz = p.n, float(p.csr.idx.size)
+    asm_b = assembly_bytes(f)
+    asm_ms = float(ms_k[0])
+    solve_b = 2 * entries * 8 + 2 * n * R * 8
+    solve_fl = 4 * entries * R
+    spmv_b = (nnz * 12 + (n + 1) * 8 + 2 * n * 8) * R
+    out = {
+        "gemm": {"bound": "tensor", "achieved": gemm_flops / (ms_k[3] * 1e-3) / 1e12, "peak": dgemm,
+                 "unit": "TFLOP/s", "ms": float(ms_k[3]), "launches": int(cnt_k[3])},
+        "assemble": {"bound": "hbm", "achieved": asm_b / (asm_ms * 1e-3) / 1e9, "peak": hbm_gbs, "unit": "GB/s",
+                     "bytes": asm_b, "ms": asm_ms, "launches": int(cnt_k[0]),
+                     "algorithmic": "8 B per value of A, per child update entry read, per front entry written"},
+        "solve": {"bound": "tensor", "achieved": solve_fl / (solve_graph_ms * 1e-3) / 1e12, "peak": dgemm,
+                  "unit": "TFLOP/s", "ms": solve_graph_ms, "gbs": solve_b / (solve_graph_ms * 1e-3) / 1e9,
+                  "gbs_frac": solve_b / (solve_graph_ms * 1e-3) / 1e9 / hbm_gbs,
+                  "algorithmic": f"4 |L| R flops; 2 |L| 8 + 2 n R 8 bytes (R = {R}); timed alone"},
+        "spmv": {"bound": "hbm", "achieved": spmv_b / (spmv_ms * 1e-3) / 1e9, "peak": hbm_gbs, "unit": "GB/s",
+                 "ms": spmv_ms, "algorithmic": "(12 nnz + 8 (n+1) + 16 n) bytes per right-hand side"},
+        "panel": {"bound": "latency", "ms": float(ms_k[1]), "launches": int(cnt_k[1])},
+        "hbm_peak_source": hbm_src,
+    }
+    for k in ("gemm", "assemble", "solve", "spmv"):
+        out[k]["frac"] = out[k]["achieved"] / out[k]["peak"]
+    return out
+
+
 def profile_kernels(args, torch, lib):
     """Runs for a profiler (no timing): the FP32 factorisation of the --n-el block twice (the
     tcgen05 update GEMMs), or the U-Net's forward and backward passes twice."""
@@ -670,6 +831,10 @@ def main():
             run_ldlt(args, torch, lib, local)
         if world > 1:
             dist.destroy_process_group()
+        return
+    if args.config == 3 and world > 1:
+        run_batch_sharded(args, torch, rank, world, local)
+        dist.destroy_process_group()
         return
     if args.config != 2:
         if rank == 0:
@@ -779,12 +944,13 @@ def main():
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
     factor_ms = float(ms_k[0:4].sum() + ms_k[10:13].sum() + ms_k[15])
     solve_ms = float(ms_k[16:32].sum())
-    traffic = None
-    tf = ROOT / "profiles" / "gemm_kernel_traffic_block48.md"  # an ncu capture's summary
-    if tf.exists() and args.n_el == N_EL:
-        for line_ in tf.read_text().splitlines():
-            if line_.startswith("bytes_per_launch:"):
-                traffic = int(line_.split(":")[1])
+    traffic, traffic_note = recorded_traffic("gemm_kernel", args.n_el)
+    # the solve and the residual product alone, on the same stream (graph replay, CUDA events)
+    solve_graph_ms = stream_time(torch, stream, lambda: solve_only(lib, f, d_x, d_f, R, n, stream), reps=5)
+    spmv_ms = stream_time(torch, stream, lambda: lib.fc_csr_spmv_device(
+        n, C.c_void_p(d_ptr.data_ptr()), C.c_void_p(d_idx.data_ptr()), C.c_void_p(d_kv.data_ptr()),
+        C.c_void_p(d_x.data_ptr()), C.c_void_p(d_r.data_ptr()), R, n, C.c_void_p(stream.cuda_stream)), reps=5)
+    kernel_roofline = roofline_table(p, f, ms_k, cnt_k, gemm_flops, peak, solve_graph_ms, spmv_ms, R, hbm_peak())
 
     # end to end through the public API with pinned host buffers
     hv = torch.from_numpy(up.val).pin_memory()
@@ -905,10 +1071,12 @@ def main():
                      "launches": {name: int(cnt_k[k]) for k, name in KERNEL_KINDS}},
         "roofline": {"kernel": "gemm_kernel (FP64 DMMA, factor updates)", "bound": "tensor",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
-                                                        "has no FP64 figure)",
+                     "traffic": traffic, "traffic_source": traffic_note,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 "
+                                    "figure)",
                      "algorithmic": "useful flops of the factor's GEMM tasks (2 K per lower-triangle output)",
-                     "flops_per_step": gemm_flops, "ms_per_step": float(gemm_ms), "launches": int(cnt_k[3])},
+                     "flops_per_step": gemm_flops, "ms_per_step": float(gemm_ms), "launches": int(cnt_k[3]),
+                     "kernels": kernel_roofline},
         "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(up.val.nbytes + hb.numel() * 8),
                 "d2h_bytes_per_step": int(hx.numel() * 8 + 32), "relres_max": e2e_res},
         "gpu_launches": int(launches_per_step * args.steps),

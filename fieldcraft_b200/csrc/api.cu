@@ -144,6 +144,9 @@ struct fc_chol {
   // the solve as two dependency-driven persistent launches instead of level by level
   // (FC_OPTION_SOLVE_SCHEDULE, or FC_SOLVE_PERSISTENT=1 in the environment)
   bool dag = false;
+  // the solve's launches with few output tiles split K over thread-block clusters (default) or in
+  // chunks summed by their last CTA (FC_OPTION_SOLVE_CLUSTER = 0)
+  bool solve_cluster = true;
   DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
   int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
   int dag_grid = 0;
@@ -1542,10 +1545,13 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
 // result does not either. Partials and counters are offsets into buffers given at launch, reused
 // launch after launch.
 constexpr int SOLVE_KC = 256;
+// With clusters a chunk is SOLVE_CLUSTER times longer: each CTA of the cluster walks SOLVE_KC of it.
+constexpr int SOLVE_KC_CLUSTER = SOLVE_KC * fc::SOLVE_CLUSTER;
 
 struct SplitPush {
   SolvePlan &p;
   int waves_tiles;  // a launch with fewer output tiles (per block of right-hand sides) is split
+  bool cluster;     // split over thread-block clusters (else in chunks of separate CTAs)
   std::vector<std::pair<fc::GemmTask, std::pair<size_t, size_t>>> pending;
   int tiles = 0;
   // g's K range [0, K) may be split; a_es / b_es: bytes of an A / B element; first: g is in the
@@ -1555,27 +1561,29 @@ struct SplitPush {
     tiles += first ? 1 : 0;
   }
   // the end of a launch: its tasks go to the plan (split when the launch is short of tiles); its
-  // partials and counters are free again after it
-  void close() {
+  // partials and counters are free again after it. Returns whether the launch runs on clusters.
+  bool close() {
     const bool split = tiles < waves_tiles;
+    const bool on_clusters = split && cluster;
+    const int kc = on_clusters ? SOLVE_KC_CLUSTER : SOLVE_KC;
     int64_t at = 0;
     int32_t cnt = 0;
     for (auto &pg : pending) {
       const fc::GemmTask &g = pg.first;
-      if (!split || g.K <= SOLVE_KC + SOLVE_KC / 2) {
+      if (!split || g.K <= kc + kc / 2) {
         p.gemm.push_back(g);
         continue;
       }
-      const int chunks = (g.K + SOLVE_KC - 1) / SOLVE_KC;
+      const int chunks = (g.K + kc - 1) / kc;
       for (int q = 0; q < chunks; ++q) {
         fc::GemmTask c = g;
-        const int64_t k0 = (int64_t)q * SOLVE_KC;
+        const int64_t k0 = (int64_t)q * kc;
         c.A = static_cast<const char *>(g.A) + k0 * g.a_sk * (int64_t)pg.second.first;
         if (g.flags & 16)
           c.b_rows = g.b_rows + k0;  // B's rows through the row list
         else
           c.B = static_cast<const char *>(g.B) + k0 * g.b_sk * (int64_t)pg.second.second;
-        c.K = (int)std::min<int64_t>(SOLVE_KC, g.K - k0);
+        c.K = (int)std::min<int64_t>(kc, g.K - k0);
         c.flags = g.flags | 8;
         c.part_off = at, c.chunks = chunks, c.chunk = q, c.counter = (int32_t)p.tcount + cnt;
         p.gemm.push_back(c);
@@ -1587,6 +1595,7 @@ struct SplitPush {
     p.scount = std::max<int64_t>(p.scount, cnt);
     pending.clear();
     tiles = 0;
+    return on_clusters;
   }
 };
 
@@ -1596,7 +1605,7 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
   const std::vector<int64_t> &voff = p.voff;
   std::vector<fc::RowTask> &rows = p.rows;
   std::vector<fc::GemmTask> &gemm = p.gemm;
-  SplitPush sp{p, 2 * prop_sms(h->device)};
+  SplitPush sp{p, 2 * prop_sms(h->device), h->solve_cluster};
   const size_t es = h->esize;
   p.psum = 0, p.scount = 0;
   std::vector<Launch> &fwd = p.fwd, &bwd = p.bwd;
@@ -1666,8 +1675,8 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
             sp.add(g, sizeof(double), sizeof(double), j0 == 0);
           }
       }
-      sp.close();
-      push(fwd, K_SOLVE_FWD, go, (int64_t)gemm.size() - go, (int)l);
+      bool cl = sp.close();
+      push(fwd, K_SOLVE_FWD, go, (int64_t)gemm.size() - go, (int)l, cl ? 1 : 0);
       go = (int64_t)gemm.size();
       for (int64_t s : S) {
         const int w = h->width[s], m = h->height[s];
@@ -1692,8 +1701,8 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
           r0 = r1;
         }
       }
-      sp.close();
-      push(fwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+      cl = sp.close();
+      push(fwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l, cl ? 1 : 0);
     }
   }
   // backward
@@ -1739,8 +1748,8 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
           sp.add(g, es, sizeof(double), j0 == 0);
         }
     }
-    sp.close();
-    push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+    bool cl = sp.close();
+    push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l, cl ? 1 : 0);
     // blocks of SB columns from the last: z = Dinv^T x2 (into x), then the own rows above the
     // block -= L(block, rows)^T z
     int K = 0;
@@ -1769,8 +1778,8 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
             sp.add(g, sizeof(double), sizeof(double), j0 == 0);
           }
       }
-      sp.close();
-      push(bwd, K_SOLVE_BWD, go, (int64_t)gemm.size() - go, (int)l);
+      cl = sp.close();
+      push(bwd, K_SOLVE_BWD, go, (int64_t)gemm.size() - go, (int)l, cl ? 1 : 0);
       go = (int64_t)gemm.size();
       for (int64_t s : S) {
         const int w = h->width[s], m = h->height[s];
@@ -1792,8 +1801,8 @@ void solve_tasks(const fc_chol *h, int R, double *x, double *x2, double *v, Solv
             sp.add(g, es, sizeof(double), j0 == 0);
           }
       }
-      sp.close();
-      if ((int64_t)gemm.size() > go) push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l);
+      cl = sp.close();
+      if ((int64_t)gemm.size() > go) push(bwd, K_GEMM, go, (int64_t)gemm.size() - go, (int)l, cl ? 1 : 0);
     }
   }
 }
@@ -2330,10 +2339,18 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
         fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st);
         break;
       case K_SOLVE_FWD:  // the diagonal blocks' inverses applied (FP64 throughout)
-      case K_SOLVE_BWD: fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st, b.part, b.tcount); break;
+      case K_SOLVE_BWD:
+        if (l.width == 1)
+          fc::launch_gemm_cluster(b.gemm + l.off, l.count, false, st, b.part, b.tcount);
+        else
+          fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st, b.part, b.tcount);
+        break;
       case K_GEMM:
-        fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st, b.part,
-                        b.tcount);
+        if (l.width == 1)
+          fc::launch_gemm_cluster(b.gemm + l.off, l.count, h->fp32, st, b.part, b.tcount);
+        else
+          fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st, b.part,
+                          b.tcount);
         break;
       case K_SOLVE_THIN_FWD:
         fc::launch_thin_fwd(t, h->fp32, b.x, b.x2, b.v, b.voff, R, b.lg, b.thin + l.off, b.tranges, l.count, st);
@@ -2786,6 +2803,11 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       h->refine_pcg = value == 0;
       return FC_OK;
+    case FC_OPTION_SOLVE_CLUSTER:
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      h->solve_cluster = value == 1;
+      replan();
+      return FC_OK;
     case FC_OPTION_FP32_UPDATES: {
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       if (h->tc == (value == 0)) return FC_OK;
@@ -2934,6 +2956,7 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
   run_solve_program(h, p.fwd, b, R, launches);
   run_solve_program(h, p.bwd, b, R, launches);
   fc::launch_permute_out(h->d_perm.as<int64_t>(), h->n, b.x, R, d_b, ld, h->tree.scale, h->stream);
+  h->last_solve_launches = launches + 2;
   e = cudaStreamSynchronize(h->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(status, e, "solve");

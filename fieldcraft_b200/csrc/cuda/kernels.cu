@@ -10,6 +10,8 @@
 #include <climits>
 #include <cstdio>
 
+#include <cooperative_groups.h>
+
 #include "kernels.cuh"
 #include "tiles.cuh"
 
@@ -577,38 +579,37 @@ __device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)
   gemm_store<T>(tp, tp->flags, acc, wm, wn, g, tg);
 }
 
+// The main loop of a 64 x 64 tile of C -= A B^T over K range [kbeg, kend) of the task: 3-stage
+// cp.async ring in `gsm`, DMMA into acc (this thread's fragments).
 template <class TA>
-__global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *__restrict__ tasks, double *part,
-                                                               int32_t *counters) {
+__device__ __forceinline__ void gemm_mainloop(const GemmTask *tp, int kbeg, int kend, double (&acc)[2][4][4],
+                                              double *gsm) {
   constexpr int SA = tile_stride<TA>();
-  extern __shared__ __align__(16) double gsm[];
   double(*Bs)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm);
   TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + GEMM_STAGES * GEMM_KC * SROW);
-  const GemmTask *tp = tasks + blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tg = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int K = tp->K;
-  const TA *abase = static_cast<const TA *>(tp->A);
-  const double *bbase = static_cast<const double *>(tp->B);
+  const int K = kend - kbeg;
+  const bool gather = tp->flags & 16;
+  const TA *abase = static_cast<const TA *>(tp->A) + (int64_t)kbeg * tp->a_sk;
+  const double *bbase = static_cast<const double *>(tp->B) + (gather ? 0 : (int64_t)kbeg * tp->b_sk);
   TileLoader<TA, GEMM_KC> la;
   TileLoader<double, GEMM_KC> lb;
   la.init(abase, tp->a_si, tp->a_sk, tp->M, tid);
   lb.init(bbase, tp->b_sj, tp->b_sk, tp->N, tid);
-  double acc[2][4][4];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.0;
   const int nk = (K + GEMM_KC - 1) / GEMM_KC;
-  const bool gather = tp->flags & 16;
-  const int32_t *brows = tp->b_rows;
+  const int32_t *brows = gather ? tp->b_rows + kbeg : nullptr;
   const int64_t bsk = tp->b_sk;
-  auto load_b = [&](int stage, int kbase) {
+  auto load_b = [&](int stage, int kb) {
     if (gather)
-      lb.load_rows(Bs[stage], kbase, K, bbase, brows, bsk, bbase);
+      lb.load_rows(Bs[stage], kb, K, bbase, brows, bsk, bbase);
     else
-      lb.load(Bs[stage], kbase, K, bbase);
+      lb.load(Bs[stage], kb, K, bbase);
   };
   for (int st = 0; st < GEMM_STAGES - 1; ++st) {
     if (st < nk) {
@@ -650,7 +651,108 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *_
     }
   }
   cp_async_wait<0>();
+}
+
+template <class TA>
+__global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *__restrict__ tasks, double *part,
+                                                               int32_t *counters) {
+  extern __shared__ __align__(16) double gsm[];
+  const GemmTask *tp = tasks + blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  double acc[2][4][4];
+  gemm_mainloop<TA>(tp, 0, tp->K, acc, gsm);
   gemm_epilogue<double>(tp, acc, wm, wn, g, tg, part, counters);
+}
+
+// ---- the solve's short products, K split over a thread-block cluster -------------------------
+// A launch of the solve with few output tiles leaves most SMs idle and each CTA walks a long K
+// alone. Here the 8 CTAs of a cluster share one 64 x 64 tile: CTA rank q takes the q-th of 8 equal
+// slices of K (multiples of GEMM_KC), keeps its partial tile in its shared memory, and after a
+// cluster barrier each CTA adds the 8 partials of 8 of the tile's rows in rank order, reading the
+// others' shared memory directly (distributed shared memory), and applies the task's epilogue to
+// those rows. A chunk of a longer sum (flag 8) stores its rows' totals as the chunk's partial; the
+// last cluster to finish (an atomic count) adds the chunks in order, each CTA its 8 rows. Every
+// sum's order depends on K alone, not on the number of right-hand sides.
+template <class TA>
+__global__ void __cluster_dims__(SOLVE_CLUSTER, 1, 1) __launch_bounds__(GEMM_THREADS, 3)
+    gemm_cluster_kernel(const GemmTask *__restrict__ tasks, double *part, int32_t *counters) {
+  extern __shared__ __align__(16) double gsm[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int q = (int)cluster.block_rank();
+  const GemmTask *tp = tasks + blockIdx.x / SOLVE_CLUSTER;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int K = tp->K;
+  const int slice = ((K + SOLVE_CLUSTER - 1) / SOLVE_CLUSTER + GEMM_KC - 1) / GEMM_KC * GEMM_KC;
+  const int kb = min(K, q * slice), ke = min(K, kb + slice);
+  double acc[2][4][4];
+  gemm_mainloop<TA>(tp, kb, ke, acc, gsm);
+  __syncthreads();  // the ring is drained: its space takes the partial tile
+  double *mine = gsm;  // [i * 64 + j]
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        mine[(wm + r * 16 + g + 8 * (e >> 1)) * 64 + wn + c * 8 + 2 * tg + (e & 1)] = acc[r][c][e];
+  cluster.sync();
+  // this CTA's 8 rows: 512 values, 4 a thread, the 8 partials added in rank order
+  constexpr int ROWS = 64 / SOLVE_CLUSTER, PER = ROWS * 64 / GEMM_THREADS;
+  double tot[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * GEMM_THREADS, i = q * ROWS + e / 64, j = e % 64;
+    double sum = 0.0;
+#pragma unroll
+    for (int p = 0; p < SOLVE_CLUSTER; ++p) sum += cluster.map_shared_rank(mine, p)[i * 64 + j];
+    tot[u] = sum;
+  }
+  const int M = tp->M, N = tp->N, flags = tp->flags;
+  if (flags & 8) {
+    // a chunk of a split sum: its rows' totals are the chunk's partial; the last cluster adds them
+    __shared__ int last;
+    double *P = part + tp->part_off;
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * GEMM_THREADS;
+      P[(int64_t)tp->chunk * 4096 + q * ROWS * 64 + e] = tot[u];
+    }
+    __threadfence();
+    cluster.sync();  // every CTA's rows are stored (and the peers are done with `mine`)
+    if (q == 0 && tid == 0) {
+      const int done = atomicAdd(counters + tp->counter, 1) == tp->chunks - 1;
+      for (int p = 0; p < SOLVE_CLUSTER; ++p) *cluster.map_shared_rank(&last, p) = done;
+    }
+    cluster.sync();
+    if (!last) return;
+    __threadfence();
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * GEMM_THREADS;
+      double sum = 0.0;
+      for (int c = 0; c < tp->chunks; ++c) sum += __ldcg(P + (int64_t)c * 4096 + q * ROWS * 64 + e);
+      tot[u] = sum;
+    }
+    cluster.sync();  // every CTA has read the counter's round
+    if (q == 0 && tid == 0) counters[tp->counter] = 0;
+  } else {
+    cluster.sync();  // the peers are done reading this CTA's partial
+  }
+  const bool lower = flags & 1;
+  double *C = static_cast<double *>(tp->C);
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int e = tid + u * GEMM_THREADS, i = q * ROWS + e / 64, j = e % 64;
+    if (i < M && j < N && (!lower || i >= j)) {
+      double *dst = C + (int64_t)i * tp->c_si + (int64_t)j * tp->c_sj;
+      *dst = (flags & 4) ? tot[u] : (flags & 2) ? -tot[u] : *dst - tot[u];
+    }
+  }
 }
 
 // ---- tiled C -= A B^T in FP32 by 3xTF32 on the tensor pipe ---------------------------------------
@@ -1221,6 +1323,8 @@ void configure_kernels() {
   set_smem(panel_kernel<float>, panel_smem<float>(64));
   set_smem(gemm_kernel<double>, gemm_smem<double>());
   set_smem(gemm_kernel<float>, gemm_smem<float>());
+  set_smem(gemm_cluster_kernel<double>, gemm_smem<double>());
+  set_smem(gemm_cluster_kernel<float>, gemm_smem<float>());
   set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
   configure_solve_dag();
   done = true;
@@ -1261,6 +1365,17 @@ void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t s
       break;
     case GemmKind::F32_TF32X3: gemm_tf32x3_kernel<<<count, GEMM_THREADS, GEMM_F32_SMEM, st>>>(tasks); break;
   }
+}
+
+void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part,
+                         int32_t *counters) {
+  if (count <= 0) return;
+  configure_kernels();
+  const unsigned grid = (unsigned)count * SOLVE_CLUSTER;
+  if (fp32_a)
+    gemm_cluster_kernel<float><<<grid, GEMM_THREADS, gemm_smem<float>(), st>>>(tasks, part, counters);
+  else
+    gemm_cluster_kernel<double><<<grid, GEMM_THREADS, gemm_smem<double>(), st>>>(tasks, part, counters);
 }
 
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,

@@ -24,6 +24,8 @@ constexpr int SPLIT_K = 512;  // K chunk of the persistent solve's split product
 // inverses of the panels, by doubling), so a solve step is a GEMM over SB columns, not a chain of
 // SB / 64 dependent panel steps.
 constexpr int SB = 1024;
+// The solve's short products split K over a cluster of this many CTAs (gemm_cluster_kernel).
+constexpr int SOLVE_CLUSTER = 8;
 
 // A child as its parent's assembly reads it: its update matrix (offset, height) and relative map.
 struct KidMeta {
@@ -241,6 +243,9 @@ void launch_panel(const Tree &t, bool fp32, const double *upper_val, const Panel
 // part and counters: the partial sums and counters of split tasks (flag 8), null when there are none.
 void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st, double *part = nullptr,
                  int32_t *counters = nullptr);
+// The same tasks (FP64 B and C; A FP64 or FP32) with K split over clusters of SOLVE_CLUSTER CTAs.
+void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part,
+                         int32_t *counters);
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R,
                            const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st);

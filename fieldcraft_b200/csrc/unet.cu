@@ -21,11 +21,9 @@ using bf16 = __nv_bfloat16;
 
 namespace {
 
-constexpr int C = 32, CIO = 16, LAYERS = 11;
-// (cin, cout, level) of each convolution, in forward order
-constexpr int LAYER_CIN[LAYERS] = {CIO, C, C, C, C, C, C, C, C, C, C};
-constexpr int LAYER_COUT[LAYERS] = {C, C, C, C, C, C, C, C, C, C, CIO};
-constexpr int LAYER_LEVEL[LAYERS] = {0, 0, 1, 1, 2, 2, 1, 1, 0, 0, 0};
+constexpr int C = 32, CIO = 16;
+constexpr int MAX_LEVELS = 8;
+constexpr int MAX_LAYERS = 4 * MAX_LEVELS - 1;
 
 __global__ void f32_to_bf16_kernel(int64_t n, const float *__restrict__ a, bf16 *__restrict__ b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -60,6 +58,61 @@ __global__ void residual_inplace_kernel(int64_t n, const double *__restrict__ b,
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     r[i] = b[i] - r[i];
 }
+// Nodal block-Jacobi: per node k (equations 3k..3k+2) the inverse of K's 3 x 3 diagonal block,
+// from the rows of K (columns sorted); ok[0] is cleared for a block that is not positive definite.
+__global__ void block_jacobi_kernel(int64_t nodes, const int64_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+                                    const double *__restrict__ val, double *__restrict__ inv, int *ok) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nodes; k += (int64_t)gridDim.x * blockDim.x) {
+    double a[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int i = 0; i < 3; ++i) {
+      const int64_t row = 3 * k + i;
+      for (int64_t q = ptr[row]; q < ptr[row + 1]; ++q) {
+        const int64_t c = idx[q] - 3 * k;
+        if (c >= 0 && c < 3) a[i][c] = val[q];
+      }
+    }
+    // the inverse by cofactors (a symmetric 3 x 3)
+    const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1], c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2],
+                 c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+    const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+    double *o = inv + 9 * k;
+    if (!(det > 0.0) || !(a[0][0] > 0.0)) {
+      *ok = 0;
+      for (int q = 0; q < 9; ++q) o[q] = 0.0;
+      continue;
+    }
+    const double d = 1.0 / det;
+    o[0] = c00 * d;
+    o[1] = c01 * d;
+    o[2] = c02 * d;
+    o[3] = c01 * d;
+    o[4] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * d;
+    o[5] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * d;
+    o[6] = c02 * d;
+    o[7] = o[5];
+    o[8] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * d;
+  }
+}
+// z += B r, B the nodal block-Jacobi inverse
+__global__ void block_jacobi_add_kernel(int64_t nodes, const double *__restrict__ inv, const double *__restrict__ r,
+                                        double *__restrict__ z) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nodes; k += (int64_t)gridDim.x * blockDim.x) {
+    const double *o = inv + 9 * k;
+    const double r0 = r[3 * k], r1 = r[3 * k + 1], r2 = r[3 * k + 2];
+    z[3 * k] += o[0] * r0 + o[1] * r1 + o[2] * r2;
+    z[3 * k + 1] += o[3] * r0 + o[4] * r1 + o[5] * r2;
+    z[3 * k + 2] += o[6] * r0 + o[7] * r1 + o[8] * r2;
+  }
+}
+// acc = first ? g s : acc + g s (FP32 gradients of a minibatch)
+__global__ void accumulate_kernel(int64_t n, const float *__restrict__ g, float s, bool first, float *__restrict__ acc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    acc[i] = first ? g[i] * s : acc[i] + g[i] * s;
+}
+__global__ void add_scalar_kernel(const double *__restrict__ a, double *__restrict__ acc, bool first) {
+  acc[0] = first ? a[0] : acc[0] + a[0];
+}
+
 int blocks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
 Grid coarser(const Grid &g) { return Grid{(g.X + 1) / 2, (g.Y + 1) / 2, (g.Z + 1) / 2}; }
@@ -71,19 +124,27 @@ struct fc_unet {
   cudaStream_t stream = nullptr;
   int64_t n = 0;
   double kref = 1.0;
-  Grid g[3];
-  int64_t w_off[LAYERS], b_off[LAYERS], wb_off[LAYERS];
+  int levels = 3, layers = 11;
+  Grid g[MAX_LEVELS];
+  int lcin[MAX_LAYERS], lcout[MAX_LAYERS], llevel[MAX_LAYERS];
+  int64_t w_off[MAX_LAYERS], b_off[MAX_LAYERS], wb_off[MAX_LAYERS];
   int64_t params = 0, wcount = 0;
   DeviceBuf p, grad, m, v;   // FP32 parameters, gradients and Adam moments
+  DeviceBuf gacc;            // a minibatch's summed gradients
   DeviceBuf wb, wt;          // BF16 weights and their flipped transposes
   DeviceBuf eq, feat;
-  // activations (BF16, channels last)
-  DeviceBuf x, a0, s0, p1, a1, s1, p2, a2, m2, u1, a3, d1, u0, a4, d0, y;
-  // gradients
-  DeviceBuf dy, g0a, g0b, gs0, g1a, g1b, gs1, g2a, g2b;
+  // activations (BF16, channels last), per level: the (pooled) input, the two convolutions of the
+  // way down (s = the skip), the way up: u = upsampled + skip, its two convolutions b, d
+  DeviceBuf x, y, pin[MAX_LEVELS], a[MAX_LEVELS], s[MAX_LEVELS], u[MAX_LEVELS], b[MAX_LEVELS], d[MAX_LEVELS];
+  // gradients per level
+  DeviceBuf dy, ga[MAX_LEVELS], gb[MAX_LEVELS], gs[MAX_LEVELS];
   DeviceBuf part;            // weight-gradient partials
   DeviceBuf scal, dotpart;   // device scalars: [0,1] input scales, [2..] dots; dot partials
   DeviceBuf tz, td, tf;      // training: network output and its difference; FP32 grid copies
+  DeviceBuf bj;              // nodal block-Jacobi inverses (9 doubles a node), added to the output
+  bool has_bj = false;
+  bool net_on = true;         // false: the preconditioner is the block-Jacobi part alone
+  int64_t last_net_iterations = 0, last_dropped = 0;
   bool weights_stale = true;
   std::mutex lock;
 };
@@ -98,10 +159,10 @@ cudaError_t alloc_bf16(DeviceBuf &b, const Grid &g, int c) { return b.alloc(size
 void refresh_weights(fc_unet *u) {
   if (!u->weights_stale) return;
   cudaStream_t st = u->stream;
-  for (int l = 0; l < LAYERS; ++l) {
-    const int64_t nw = (int64_t)27 * LAYER_CIN[l] * LAYER_COUT[l];
+  for (int l = 0; l < u->layers; ++l) {
+    const int64_t nw = (int64_t)27 * u->lcin[l] * u->lcout[l];
     fc::unet::to_bf16(nw, u->p.as<float>() + u->w_off[l], B(u->wb) + u->wb_off[l], st);
-    fc::unet::flip_weights(LAYER_CIN[l], LAYER_COUT[l], B(u->wb) + u->wb_off[l], B(u->wt) + u->wb_off[l], st);
+    fc::unet::flip_weights(u->lcin[l], u->lcout[l], B(u->wb) + u->wb_off[l], B(u->wt) + u->wb_off[l], st);
   }
   u->weights_stale = false;
 }
@@ -109,69 +170,72 @@ void refresh_weights(fc_unet *u) {
 const Grid &G(const fc_unet *u, int level) { return u->g[level]; }
 
 void conv(fc_unet *u, int l, const DeviceBuf &in, DeviceBuf &out, bool relu) {
-  fc::unet::conv3(G(u, LAYER_LEVEL[l]), LAYER_CIN[l], LAYER_COUT[l], B(in), B(u->wb) + u->wb_off[l],
+  fc::unet::conv3(G(u, u->llevel[l]), u->lcin[l], u->lcout[l], B(in), B(u->wb) + u->wb_off[l],
                   u->p.as<float>() + u->b_off[l], relu, nullptr, B(out), u->stream);
 }
 // the input gradient of layer l from its output gradient: conv with the flipped weights, then
 // the ReLU mask of the layer's input (mask null: no ReLU there)
 void conv_t(fc_unet *u, int l, const DeviceBuf &dout, const DeviceBuf *mask, DeviceBuf &din) {
-  fc::unet::conv3(G(u, LAYER_LEVEL[l]), LAYER_COUT[l], LAYER_CIN[l], B(dout), B(u->wt) + u->wb_off[l], nullptr, false,
+  fc::unet::conv3(G(u, u->llevel[l]), u->lcout[l], u->lcin[l], B(dout), B(u->wt) + u->wb_off[l], nullptr, false,
                   mask ? B(*mask) : nullptr, B(din), u->stream);
 }
 void conv_dw(fc_unet *u, int l, const DeviceBuf &in, const DeviceBuf &dout) {
-  fc::unet::conv3_dw(G(u, LAYER_LEVEL[l]), LAYER_CIN[l], LAYER_COUT[l], B(in), B(dout), u->part.as<float>(),
+  fc::unet::conv3_dw(G(u, u->llevel[l]), u->lcin[l], u->lcout[l], B(in), B(dout), u->part.as<float>(),
                      u->grad.as<float>() + u->w_off[l], u->grad.as<float>() + u->b_off[l], u->stream);
 }
 
-// y = net(x)
+// the level's input on the way down: x at the top, the pooled skip of the level above below it
+const DeviceBuf &input_of(const fc_unet *u, int lv) { return lv == 0 ? u->x : u->pin[lv]; }
+// what the level returns upwards: the bottom's second convolution, or the way up's last one
+const DeviceBuf &low_of(const fc_unet *u, int lv) { return lv == u->levels - 1 ? u->s[lv] : u->d[lv]; }
+DeviceBuf &low_of(fc_unet *u, int lv) { return lv == u->levels - 1 ? u->s[lv] : u->d[lv]; }
+
+// y = net(x): per level on the way down two convolutions (the second's output is the skip) and a
+// 2x2x2 average pooling, two at the bottom, per level on the way up nearest upsampling plus the
+// skip and two convolutions, then the output convolution (layers in this order).
 void forward(fc_unet *u) {
   refresh_weights(u);
   cudaStream_t st = u->stream;
-  conv(u, 0, u->x, u->a0, true);
-  conv(u, 1, u->a0, u->s0, true);
-  fc::unet::pool(u->g[0], u->g[1], B(u->s0), B(u->p1), st);
-  conv(u, 2, u->p1, u->a1, true);
-  conv(u, 3, u->a1, u->s1, true);
-  fc::unet::pool(u->g[1], u->g[2], B(u->s1), B(u->p2), st);
-  conv(u, 4, u->p2, u->a2, true);
-  conv(u, 5, u->a2, u->m2, true);
-  fc::unet::up_add(u->g[1], u->g[2], B(u->m2), B(u->s1), B(u->u1), st);
-  conv(u, 6, u->u1, u->a3, true);
-  conv(u, 7, u->a3, u->d1, true);
-  fc::unet::up_add(u->g[0], u->g[1], B(u->d1), B(u->s0), B(u->u0), st);
-  conv(u, 8, u->u0, u->a4, true);
-  conv(u, 9, u->a4, u->d0, true);
-  conv(u, 10, u->d0, u->y, false);
+  const int D = u->levels;
+  int l = 0;
+  for (int lv = 0; lv < D; ++lv) {
+    conv(u, l++, input_of(u, lv), u->a[lv], true);
+    conv(u, l++, u->a[lv], u->s[lv], true);
+    if (lv < D - 1) fc::unet::pool(u->g[lv], u->g[lv + 1], B(u->s[lv]), B(u->pin[lv + 1]), st);
+  }
+  for (int lv = D - 2; lv >= 0; --lv) {
+    fc::unet::up_add(u->g[lv], u->g[lv + 1], B(low_of(u, lv + 1)), B(u->s[lv]), B(u->u[lv]), st);
+    conv(u, l++, u->u[lv], u->b[lv], true);
+    conv(u, l++, u->b[lv], u->d[lv], true);
+  }
+  conv(u, l, low_of(u, 0), u->y, false);
 }
 
 // parameters' gradients from dL/dy (in u->dy), after forward() on the same input
 void backward(fc_unet *u) {
   cudaStream_t st = u->stream;
-  conv_dw(u, 10, u->d0, u->dy);
-  conv_t(u, 10, u->dy, &u->d0, u->g0a);
-  conv_dw(u, 9, u->a4, u->g0a);
-  conv_t(u, 9, u->g0a, &u->a4, u->g0b);
-  conv_dw(u, 8, u->u0, u->g0b);
-  conv_t(u, 8, u->g0b, nullptr, u->gs0);  // dL/du0: to d1 (upsampled) and to s0 (skip)
-  fc::unet::up_adjoint(u->g[0], u->g[1], B(u->gs0), B(u->d1), B(u->g1a), st);
-  conv_dw(u, 7, u->a3, u->g1a);
-  conv_t(u, 7, u->g1a, &u->a3, u->g1b);
-  conv_dw(u, 6, u->u1, u->g1b);
-  conv_t(u, 6, u->g1b, nullptr, u->gs1);  // dL/du1: to m2 and to s1
-  fc::unet::up_adjoint(u->g[1], u->g[2], B(u->gs1), B(u->m2), B(u->g2a), st);
-  conv_dw(u, 5, u->a2, u->g2a);
-  conv_t(u, 5, u->g2a, &u->a2, u->g2b);
-  conv_dw(u, 4, u->p2, u->g2b);
-  conv_t(u, 4, u->g2b, nullptr, u->g2a);  // dL/dp2
-  fc::unet::pool_adjoint(u->g[1], u->g[2], B(u->g2a), B(u->gs1), B(u->s1), B(u->g1a), st);  // dL/ds1
-  conv_dw(u, 3, u->a1, u->g1a);
-  conv_t(u, 3, u->g1a, &u->a1, u->g1b);
-  conv_dw(u, 2, u->p1, u->g1b);
-  conv_t(u, 2, u->g1b, nullptr, u->g1a);  // dL/dp1
-  fc::unet::pool_adjoint(u->g[0], u->g[1], B(u->g1a), B(u->gs0), B(u->s0), B(u->g0a), st);  // dL/ds0
-  conv_dw(u, 1, u->a0, u->g0a);
-  conv_t(u, 1, u->g0a, &u->a0, u->g0b);
-  conv_dw(u, 0, u->x, u->g0b);
+  const int D = u->levels;
+  int l = u->layers - 1;
+  conv_dw(u, l, low_of(u, 0), u->dy);
+  conv_t(u, l, u->dy, &low_of(u, 0), u->ga[0]);  // dL/d(top output), through its activation
+  for (int lv = 0; lv < D - 1; ++lv) {  // the way up, from the top level to the coarsest
+    l -= 2;
+    conv_dw(u, l + 1, u->b[lv], u->ga[lv]);
+    conv_t(u, l + 1, u->ga[lv], &u->b[lv], u->gb[lv]);
+    conv_dw(u, l, u->u[lv], u->gb[lv]);
+    conv_t(u, l, u->gb[lv], nullptr, u->gs[lv]);  // dL/du: to the skip and, upsampled, below
+    fc::unet::up_adjoint(u->g[lv], u->g[lv + 1], B(u->gs[lv]), B(low_of(u, lv + 1)), B(u->ga[lv + 1]), st);
+  }
+  for (int lv = D - 1; lv >= 0; --lv) {  // the way down, from the bottom up
+    l -= 2;
+    conv_dw(u, l + 1, u->a[lv], u->ga[lv]);
+    conv_t(u, l + 1, u->ga[lv], &u->a[lv], u->gb[lv]);
+    conv_dw(u, l, input_of(u, lv), u->gb[lv]);
+    if (lv == 0) break;
+    conv_t(u, l, u->gb[lv], nullptr, u->ga[lv]);  // dL/d(pooled input)
+    fc::unet::pool_adjoint(u->g[lv - 1], u->g[lv], B(u->ga[lv]), B(u->gs[lv - 1]), B(u->s[lv - 1]),
+                           B(u->ga[lv - 1]), st);  // dL/d(skip of the level above), masked
+  }
 }
 
 double *scal(fc_unet *u, int k) { return u->scal.as<double>() + k; }
@@ -186,6 +250,36 @@ void apply(fc_unet *u, const double *r, double *z) {
   forward(u);
   cudaMemsetAsync(z, 0, sizeof(double) * (size_t)u->n, st);
   fc::unet::gather_output(u->g[0], u->eq.as<int64_t>(), B(u->y), scal(u, 0), z, st);
+  if (u->has_bj) block_jacobi_add_kernel<<<blocks(u->n / 3), 256, 0, st>>>(u->n / 3, u->bj.as<double>(), r, z);
+}
+
+// z = B r alone (the network left out)
+void apply_jacobi(fc_unet *u, const double *r, double *z) {
+  cudaMemsetAsync(z, 0, sizeof(double) * (size_t)u->n, u->stream);
+  block_jacobi_add_kernel<<<blocks(u->n / 3), 256, 0, u->stream>>>(u->n / 3, u->bj.as<double>(), r, z);
+}
+
+// The loss of the pair (r, e) and its gradient into u->grad (forward and backward of the network).
+void pair_gradient(fc_unet *u, const double *d_r, const double *d_e, const int64_t *d_ptr, const int32_t *d_idx,
+                   const double *d_val, double *d_loss) {
+  cudaStream_t st = u->stream;
+  double *z = u->tz.as<double>(), *d = u->td.as<double>();
+  apply(u, d_r, z);
+  sub_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, z, d_e, d);
+  if (d_ptr) {
+    // energy norm: loss = d.Kd / e.r (e.r = e.K e), dL/dz = 2 Kd / e.r
+    fc::launch_spmv(u->n, d_ptr, d_idx, d_val, d, u->n, z, u->n, 1, st);
+    const double *a[2] = {d, d_e}, *b[2] = {z, d_r};
+    fc::unet::dots(u->n, 2, a, b, u->dotpart.as<double>(), scal(u, 4), st);
+    loss_grad_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, scal(u, 4), z, d_loss);
+    d = z;
+  } else {
+    const double *a[2] = {d, d_e}, *b[2] = {d, d_e};
+    fc::unet::dots(u->n, 2, a, b, u->dotpart.as<double>(), scal(u, 4), st);
+    loss_grad_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, scal(u, 4), d, d_loss);
+  }
+  fc::unet::scatter_grad(u->g[0], u->eq.as<int64_t>(), d, scal(u, 0), B(u->dy), st);
+  backward(u);
 }
 
 int cuda_fail(fc_status *st, cudaError_t e, const char *where) {
@@ -197,9 +291,11 @@ int cuda_fail(fc_status *st, cudaError_t e, const char *where) {
 
 extern "C" {
 
-int fc_unet_create(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t *eq, const float *feat, double kref,
-                   uint64_t seed, int32_t device, fc_unet **out, fc_status *status) {
-  if (!out || nx < 1 || ny < 1 || nz < 1 || n < 1 || !eq || !feat || !(kref > 0)) {
+int fc_unet_create_levels(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t *eq, const float *feat,
+                          double kref, int32_t levels, uint64_t seed, int32_t device, fc_unet **out,
+                          fc_status *status) {
+  if (!out || nx < 1 || ny < 1 || nz < 1 || n < 1 || !eq || !feat || !(kref > 0) || levels < 1 ||
+      levels > MAX_LEVELS) {
     set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "bad network arguments");
     return FC_INVALID_ARGUMENT;
   }
@@ -210,20 +306,28 @@ int fc_unet_create(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t 
   u->device = device;
   u->n = n;
   u->kref = kref;
+  u->levels = levels;
   u->g[0] = Grid{nx + 1, ny + 1, nz + 1};
-  u->g[1] = coarser(u->g[0]);
-  u->g[2] = coarser(u->g[1]);
+  for (int lv = 1; lv < levels; ++lv) u->g[lv] = coarser(u->g[lv - 1]);
+  // the layers in forward order: (cin, cout, level)
+  int L = 0;
+  for (int lv = 0; lv < levels; ++lv)
+    for (int q = 0; q < 2; ++q) u->lcin[L] = (lv == 0 && q == 0) ? CIO : C, u->lcout[L] = C, u->llevel[L++] = lv;
+  for (int lv = levels - 2; lv >= 0; --lv)
+    for (int q = 0; q < 2; ++q) u->lcin[L] = C, u->lcout[L] = C, u->llevel[L++] = lv;
+  u->lcin[L] = C, u->lcout[L] = CIO, u->llevel[L++] = 0;
+  u->layers = L;
   int64_t off = 0, woff = 0;
   size_t part = 8192;
-  for (int l = 0; l < LAYERS; ++l) {
-    const int64_t nw = (int64_t)27 * LAYER_CIN[l] * LAYER_COUT[l];
+  for (int l = 0; l < L; ++l) {
+    const int64_t nw = (int64_t)27 * u->lcin[l] * u->lcout[l];
     u->w_off[l] = off;
     off += nw;
     u->b_off[l] = off;
-    off += LAYER_COUT[l];
+    off += u->lcout[l];
     u->wb_off[l] = woff;
     woff += nw;
-    part = std::max(part, (size_t)fc::unet::dw_chunks(u->g[LAYER_LEVEL[l]]) * (size_t)nw);
+    part = std::max(part, (size_t)fc::unet::dw_chunks(u->g[u->llevel[l]]) * (size_t)nw);
   }
   u->params = off;
   u->wcount = woff;
@@ -231,28 +335,30 @@ int fc_unet_create(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t 
   std::vector<float> host(off, 0.f);
   std::mt19937_64 rng(seed);
   std::normal_distribution<float> normal(0.f, 1.f);
-  for (int l = 0; l < LAYERS - 1; ++l) {  // the last layer starts at zero: M(r) = 0, a loss of one
-    const float sd = std::sqrt(2.f / (27.f * (l == 0 ? 4 : LAYER_CIN[l])));
-    const int64_t nw = (int64_t)27 * LAYER_CIN[l] * LAYER_COUT[l];
+  for (int l = 0; l < L - 1; ++l) {  // the last layer starts at zero: M(r) = 0, a loss of one
+    const float sd = std::sqrt(2.f / (27.f * (l == 0 ? 4 : u->lcin[l])));
+    const int64_t nw = (int64_t)27 * u->lcin[l] * u->lcout[l];
     for (int64_t q = 0; q < nw; ++q) host[u->w_off[l] + q] = sd * normal(rng);
   }
   bool ok = u->p.alloc(sizeof(float) * off) == cudaSuccess && u->grad.alloc(sizeof(float) * off) == cudaSuccess &&
             u->m.alloc(sizeof(float) * off) == cudaSuccess && u->v.alloc(sizeof(float) * off) == cudaSuccess &&
+            u->gacc.alloc(sizeof(float) * off) == cudaSuccess &&
             u->wb.alloc(sizeof(bf16) * woff) == cudaSuccess && u->wt.alloc(sizeof(bf16) * woff) == cudaSuccess &&
             u->eq.alloc(sizeof(int64_t) * 3 * nodes) == cudaSuccess &&
             u->feat.alloc(sizeof(float) * nodes) == cudaSuccess && u->part.alloc(sizeof(float) * part) == cudaSuccess &&
             u->scal.alloc(sizeof(double) * 64) == cudaSuccess &&
             u->dotpart.alloc(sizeof(double) * 8 * 512) == cudaSuccess &&
             u->tz.alloc(sizeof(double) * n) == cudaSuccess && u->td.alloc(sizeof(double) * n) == cudaSuccess;
-  const Grid &g0 = u->g[0], &g1 = u->g[1], &g2 = u->g[2];
-  ok = ok && alloc_bf16(u->x, g0, CIO) == cudaSuccess && alloc_bf16(u->y, g0, CIO) == cudaSuccess &&
-       alloc_bf16(u->dy, g0, CIO) == cudaSuccess;
-  for (DeviceBuf *b : {&u->a0, &u->s0, &u->u0, &u->a4, &u->d0, &u->g0a, &u->g0b, &u->gs0})
-    ok = ok && alloc_bf16(*b, g0, C) == cudaSuccess;
-  for (DeviceBuf *b : {&u->p1, &u->a1, &u->s1, &u->u1, &u->a3, &u->d1, &u->g1a, &u->g1b, &u->gs1})
-    ok = ok && alloc_bf16(*b, g1, C) == cudaSuccess;
-  for (DeviceBuf *b : {&u->p2, &u->a2, &u->m2, &u->g2a, &u->g2b}) ok = ok && alloc_bf16(*b, g2, C) == cudaSuccess;
-  ok = ok && u->tf.alloc(sizeof(float) * (size_t)g0.voxels() * CIO) == cudaSuccess;
+  ok = ok && alloc_bf16(u->x, u->g[0], CIO) == cudaSuccess && alloc_bf16(u->y, u->g[0], CIO) == cudaSuccess &&
+       alloc_bf16(u->dy, u->g[0], CIO) == cudaSuccess;
+  for (int lv = 0; lv < levels && ok; ++lv) {
+    const Grid &g = u->g[lv];
+    for (DeviceBuf *b : {&u->a[lv], &u->s[lv], &u->ga[lv], &u->gb[lv]}) ok = ok && alloc_bf16(*b, g, C) == cudaSuccess;
+    if (lv > 0) ok = ok && alloc_bf16(u->pin[lv], g, C) == cudaSuccess;
+    if (lv < levels - 1)
+      for (DeviceBuf *b : {&u->u[lv], &u->b[lv], &u->d[lv], &u->gs[lv]}) ok = ok && alloc_bf16(*b, g, C) == cudaSuccess;
+  }
+  ok = ok && u->tf.alloc(sizeof(float) * (size_t)u->g[0].voxels() * CIO) == cudaSuccess;
   if (!ok) {
     delete u;
     set_status(status, FC_OUT_OF_MEMORY, -1, 0, 0, "device memory for the network");
@@ -272,6 +378,50 @@ int fc_unet_create(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t 
   *out = u;
   set_status(status, FC_OK);
   return FC_OK;
+}
+
+int fc_unet_create(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t *eq, const float *feat, double kref,
+                   uint64_t seed, int32_t device, fc_unet **out, fc_status *status) {
+  return fc_unet_create_levels(nx, ny, nz, n, eq, feat, kref, 3, seed, device, out, status);
+}
+
+int fc_unet_set_operator(fc_unet *u, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val) {
+  if (!u || u->n % 3 != 0) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(u->lock);
+  cudaSetDevice(u->device);
+  if (!d_ptr) {
+    u->has_bj = false;
+    return FC_OK;
+  }
+  if (!d_idx || !d_val) return FC_INVALID_ARGUMENT;
+  const int64_t nodes = u->n / 3;
+  if (!u->bj.p && u->bj.alloc(sizeof(double) * 9 * (size_t)nodes) != cudaSuccess) return FC_OUT_OF_MEMORY;
+  int *ok = u->scal.as<int>() + 2 * 60;  // a flag in the last scalar slots
+  int one = 1;
+  cudaMemcpyAsync(ok, &one, sizeof(int), cudaMemcpyHostToDevice, u->stream);
+  block_jacobi_kernel<<<blocks(nodes), 256, 0, u->stream>>>(nodes, d_ptr, d_idx, d_val, u->bj.as<double>(), ok);
+  cudaMemcpyAsync(&one, ok, sizeof(int), cudaMemcpyDeviceToHost, u->stream);
+  if (cudaStreamSynchronize(u->stream) != cudaSuccess) return FC_CUDA_ERROR;
+  u->has_bj = one != 0;
+  return one ? FC_OK : FC_NOT_POSITIVE_DEFINITE;
+}
+
+int fc_unet_enable(fc_unet *u, int32_t on) {
+  if (!u || (!on && !u->has_bj)) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(u->lock);
+  u->net_on = on != 0;
+  return FC_OK;
+}
+
+int64_t fc_unet_stat(const fc_unet *u, int32_t what) {
+  if (!u) return -1;
+  switch (what) {
+    case 0: return u->levels;
+    case 1: return u->last_net_iterations;
+    case 2: return u->last_dropped;
+    case 3: return u->has_bj ? 1 : 0;
+    default: return -1;
+  }
 }
 
 void fc_unet_destroy(fc_unet *u) {
@@ -355,25 +505,29 @@ int fc_unet_train_step(fc_unet *u, const double *d_r, const double *d_e, const i
   if (!u || !d_r || !d_e || step < 1 || (d_ptr && (!d_idx || !d_val))) return FC_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(u->lock);
   cudaSetDevice(u->device);
-  cudaStream_t st = u->stream;
-  double *z = u->tz.as<double>(), *d = u->td.as<double>();
-  apply(u, d_r, z);
-  sub_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, z, d_e, d);
-  if (d_ptr) {
-    // energy norm: loss = d.Kd / e.r (e.r = e.K e), dL/dz = 2 Kd / e.r
-    fc::launch_spmv(u->n, d_ptr, d_idx, d_val, d, u->n, z, u->n, 1, st);
-    const double *a[2] = {d, d_e}, *b[2] = {z, d_r};
-    fc::unet::dots(u->n, 2, a, b, u->dotpart.as<double>(), scal(u, 4), st);
-    loss_grad_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, scal(u, 4), z, d_loss);
-    d = z;
-  } else {
-    const double *a[2] = {d, d_e}, *b[2] = {d, d_e};
-    fc::unet::dots(u->n, 2, a, b, u->dotpart.as<double>(), scal(u, 4), st);
-    loss_grad_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, scal(u, 4), d, d_loss);
-  }
-  fc::unet::scatter_grad(u->g[0], u->eq.as<int64_t>(), d, scal(u, 0), B(u->dy), st);
-  backward(u);
+  pair_gradient(u, d_r, d_e, d_ptr, d_idx, d_val, d_loss);
   fc::unet::adam(u->params, u->p.as<float>(), u->grad.as<float>(), u->m.as<float>(), u->v.as<float>(), lr, 0.9f,
+                 0.999f, 1e-8f, step, u->stream);
+  u->weights_stale = true;
+  return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
+}
+
+int fc_unet_train_batch(fc_unet *u, const double *d_r, const double *d_e, int32_t count, int64_t ld,
+                        const int64_t *d_ptr, const int32_t *d_idx, const double *d_val, float lr, int32_t step,
+                        double *d_loss) {
+  if (!u || !d_r || !d_e || count < 1 || ld < u->n || step < 1 || (d_ptr && (!d_idx || !d_val)))
+    return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(u->lock);
+  cudaSetDevice(u->device);
+  cudaStream_t st = u->stream;
+  double *one = scal(u, 8);
+  for (int32_t q = 0; q < count; ++q) {
+    pair_gradient(u, d_r + (int64_t)q * ld, d_e + (int64_t)q * ld, d_ptr, d_idx, d_val, one);
+    accumulate_kernel<<<blocks(u->params), 256, 0, st>>>(u->params, u->grad.as<float>(), 1.f / (float)count, q == 0,
+                                                         u->gacc.as<float>());
+    if (d_loss) add_scalar_kernel<<<1, 1, 0, st>>>(one, d_loss, q == 0);
+  }
+  fc::unet::adam(u->params, u->p.as<float>(), u->gacc.as<float>(), u->m.as<float>(), u->v.as<float>(), lr, 0.9f,
                  0.999f, 1e-8f, step, st);
   u->weights_stale = true;
   return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
@@ -420,10 +574,20 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
   const double target = tol * tol * bb;
   int it = 0, stored = 0;
   bool converged = bb == 0.0;
+  // The safeguard: while the network is in use, a window of SAFE_WINDOW iterations that does not
+  // lower ||r||^2 by SAFE_DROP drops it for the rest of the solve (the block-Jacobi part, when
+  // set, stays) and restarts the directions.
+  constexpr int SAFE_WINDOW = 25;
+  constexpr double SAFE_DROP = 0.25;
+  bool use_net = net != nullptr && net->net_on;
+  std::vector<double> history;
+  if (net) net->last_dropped = 0, net->last_net_iterations = 0;
   while (!converged && it < max_iter) {
     // z = M(r)
-    if (net)
+    if (use_net)
       apply(net, r, z);
+    else if (net && net->has_bj)
+      apply_jacobi(net, r, z);
     else
       copy_kernel<<<blocks(n), 256, 0, st>>>(n, r, z);
     // p = z - sum_j (z.q_j / p_j.q_j) p_j over the stored directions
@@ -468,6 +632,16 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
     stored = std::min(stored + 1, ring);
     converged = rr <= target;
     if (!(rr == rr)) break;  // NaN: give up on FCG
+    history.push_back(rr);
+    if (use_net) {
+      net->last_net_iterations = it;
+      const size_t h = history.size();
+      if (h > SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
+        use_net = false;
+        net->last_dropped = 1;
+        stored = 0;
+      }
+    }
   }
   if (iterations) *iterations = it;
   // the true residual of the returned x

@@ -21,9 +21,12 @@ def _p(t) -> C.c_void_p:
 
 
 class UNet:
-    """The 3-level, 32-channel 3D-convolution U-Net on the node grid of a box problem."""
+    """The 32-channel 3D-convolution U-Net on the node grid of a box problem (`levels` levels, 3 by
+    default). With `operator` = (ptr, idx, val) CUDA tensors of K, the preconditioner is the nodal
+    block-Jacobi inverse of K plus the network, which then learns the rest of K^-1 r."""
 
-    def __init__(self, problem: Problem, seed: int = 0, device: int = 0, kref: float | None = None):
+    def __init__(self, problem: Problem, seed: int = 0, device: int = 0, kref: float | None = None, levels: int = 3,
+                 operator=None):
         lib = _lib.load()
         nx, ny, nz = problem.dims
         if kref is None:
@@ -35,12 +38,33 @@ class UNet:
         feat = node_feature(problem)
         st = Status()
         h = C.c_void_p()
-        lib.fc_unet_create(nx, ny, nz, problem.n, _lib.ptr(eq), _lib.ptr(feat), self.kref, seed, device, C.byref(h),
-                           C.byref(st))
+        lib.fc_unet_create_levels(nx, ny, nz, problem.n, _lib.ptr(eq), _lib.ptr(feat), self.kref, int(levels), seed,
+                                  device, C.byref(h), C.byref(st))
         raise_for(st)
         self.handle = h
         self.n = problem.n
+        self.levels = int(levels)
         self.voxels = (nx + 1) * (ny + 1) * (nz + 1)
+        if operator is not None:
+            self.set_operator(operator)
+
+    def set_operator(self, csr_device):
+        """Adds the nodal block-Jacobi part of K (CUDA tensors ptr, idx, val) to the preconditioner;
+        None removes it."""
+        args = [_p(a) for a in csr_device] if csr_device is not None else [None, None, None]
+        rc = _lib.load().fc_unet_set_operator(self.handle, *args)
+        if rc != 0:
+            raise ValueError(f"fc_unet_set_operator ({rc})")
+
+    def enable(self, on: bool):
+        """False: the preconditioner is the block-Jacobi part alone (the network is not run)."""
+        if _lib.load().fc_unet_enable(self.handle, int(bool(on))) != 0:
+            raise ValueError("fc_unet_enable needs the operator set")
+
+    def stat(self, what: int) -> int:
+        """0 levels, 1 iterations of the last FCG with the network, 2 whether its safeguard dropped
+        the network, 3 whether the block-Jacobi part is set."""
+        return int(_lib.load().fc_unet_stat(self.handle, int(what)))
 
     def set_stream(self, stream_ptr: int | None):
         _lib.load().fc_unet_set_stream(self.handle, C.c_void_p(stream_ptr) if stream_ptr else None)
@@ -86,6 +110,15 @@ class UNet:
         if _lib.load().fc_unet_train_step(self.handle, _p(r), _p(e), *k, C.c_float(lr), int(step),
                                           _p(loss) if loss is not None else None) != 0:
             raise RuntimeError("fc_unet_train_step")
+
+    def train_batch(self, R, E, lr: float, step: int, loss=None, csr_device=None):
+        """One Adam step on the mean gradient of the pairs (rows of R, rows of E: CUDA tensors
+        [count, n]); `loss` (a device double) gets the sum of their losses."""
+        k = [_p(a) for a in csr_device] if csr_device is not None else [None, None, None]
+        rc = _lib.load().fc_unet_train_batch(self.handle, _p(R), _p(E), int(R.shape[0]), int(R.stride(0)), *k,
+                                             C.c_float(lr), int(step), _p(loss) if loss is not None else None)
+        if rc != 0:
+            raise RuntimeError("fc_unet_train_batch")
 
     def close(self):
         h = getattr(self, "handle", None)
@@ -143,10 +176,10 @@ def output_scale(R, E) -> float:
 
 
 def train(net: UNet, R, E, epochs: int, lr: float, torch, seed: int = 0, lr_decay: float = 0.3, csr_device=None,
-          warmup: int = 200):
-    """Adam over the pairs for `epochs` passes in a seeded order (one pair per step); the learning
-    rate ramps up over the first `warmup` steps and steps down by lr_decay for the last epoch.
-    Returns the mean loss of each epoch."""
+          warmup: int = 200, batch: int = 1):
+    """Adam over the pairs for `epochs` passes in a seeded order, `batch` pairs per step (their
+    mean gradient); the learning rate ramps up over the first `warmup` steps and steps down by
+    lr_decay for the last epoch. Returns the mean loss of each epoch."""
     loss = torch.zeros(1, dtype=torch.float64, device="cuda")
     losses = []
     rng = np.random.default_rng(seed)
@@ -155,9 +188,16 @@ def train(net: UNet, R, E, epochs: int, lr: float, torch, seed: int = 0, lr_deca
     for ep in range(epochs):
         acc = torch.zeros(1, dtype=torch.float64, device="cuda")
         rate = lr * (lr_decay if epochs > 1 and ep == epochs - 1 else 1.0)
-        for i in rng.permutation(count):
+        order = rng.permutation(count)
+        for b0 in range(0, count, batch):
             step += 1
-            net.train_step(R[i], E[i], rate * min(1.0, step / warmup), step, loss, csr_device)
+            pick = order[b0:b0 + batch]
+            lr_now = rate * min(1.0, step / warmup)
+            if batch == 1:
+                net.train_step(R[pick[0]], E[pick[0]], lr_now, step, loss, csr_device)
+            else:
+                idx = torch.from_numpy(np.ascontiguousarray(pick)).cuda()
+                net.train_batch(R.index_select(0, idx), E.index_select(0, idx), lr_now, step, loss, csr_device)
             acc += loss
         losses.append(float(acc.item()) / count)
     return losses

@@ -138,6 +138,9 @@ int fc_chol_solve_device_async(fc_chol *h, double *d_b, int32_t nrhs, int64_t ld
  * loaded on, until the process exits. Calls that need more than that are refused with
  * FC_INVALID_ARGUMENT and a message giving the size needed. The first call on each device looks
  * the array's address up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The address is kept for the life of the process: a caller that resets the device
+ * (cudaDeviceReset) or tears down and recreates its context must not call this entry point
+ * again in that process.
  * All calls share the one array and each leaves its contents behind: calls whose work overlaps on
  * the GPU (several handles or threads on one device at once) race on it. Synchronises before
  * returning. */
@@ -189,13 +192,18 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *                              x += M (b - A x).
  *   FC_OPTION_FP32_UPDATES     the mixed-precision factor's update-matrix products: 0 on tcgen05
  *                              in 128 x 128 tiles (default), 1 on mma.sync in 64 x 64 tiles
- *                              (re-plans the factorisation; takes effect from the next one). */
+ *                              (re-plans the factorisation; takes effect from the next one).
+ *   FC_OPTION_SOLVE_CLUSTER    the level-by-level solve's products in launches with few output
+ *                              tiles: 1 each tile's K split over a cluster of 8 CTAs that add
+ *                              their partials through distributed shared memory (default); 0 K
+ *                              split in chunks of separate CTAs, the last adding the partials. */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3
 #define FC_OPTION_TRACE 4
 #define FC_OPTION_REFINEMENT 5
 #define FC_OPTION_FP32_UPDATES 6
+#define FC_OPTION_SOLVE_CLUSTER 7
 int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
 /* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
  * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |

@@ -11,9 +11,12 @@
  * The network works on the hex8 mesh's node grid (nx + 1) x (ny + 1) x (nz + 1): input channels
  * are the residual's three components at each node (zero where held) and a fixed per-node feature
  * (the log of the Young's modulus around the node, normalised); the output's first three channels
- * are the correction at each node. Architecture: three levels (2x2x2 average pooling, nearest
- * upsampling, additive skips), two 3x3x3 convolutions of 32 channels with ReLU per level and side,
- * a first convolution from 16 (4 used) channels and a last one to 16 (3 used), 11 in all. */
+ * are the correction at each node. Architecture: a U-Net of `levels` levels (three by default;
+ * 2x2x2 average pooling, nearest upsampling, additive skips), two 3x3x3 convolutions of 32
+ * channels with leaky ReLU per level and side, a first convolution from 16 (4 used) channels and
+ * a last one to 16 (3 used): 4 levels - 1 convolutions in all. With the operator set
+ * (fc_unet_set_operator) the preconditioner is M(r) = B r + net(r), B the nodal 3 x 3 block-Jacobi
+ * inverse of K, and the network learns the rest of K^-1 r. */
 #ifndef FIELDCRAFT_UNET_H
 #define FIELDCRAFT_UNET_H
 
@@ -33,7 +36,22 @@ typedef struct fc_unet fc_unet;
  * layer's to zero. Host arrays. */
 int fc_unet_create(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t *eq, const float *feat, double kref,
                    uint64_t seed, int32_t device, fc_unet **out, fc_status *status);
+/* The same with `levels` levels (1..8); fc_unet_create is levels = 3. A deeper network reaches
+ * farther across the grid (its coarsest convolutions see 2^(levels-1) times as far). */
+int fc_unet_create_levels(int32_t nx, int32_t ny, int32_t nz, int64_t n, const int64_t *eq, const float *feat,
+                          double kref, int32_t levels, uint64_t seed, int32_t device, fc_unet **out,
+                          fc_status *status);
 void fc_unet_destroy(fc_unet *net);
+/* K by rows on the device (as fc_csr_spmv_device; the pointers are read here only): adds the
+ * nodal block-Jacobi part B r to the preconditioner (equations node by node, three a node: n must
+ * be a multiple of 3). d_ptr null removes it. FC_NOT_POSITIVE_DEFINITE when a 3 x 3 block is not. */
+int fc_unet_set_operator(fc_unet *net, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val);
+/* on = 0: the preconditioner is the block-Jacobi part alone (the network is not run; needs the
+ * operator set); on = 1 (the default): B r + net(r). */
+int fc_unet_enable(fc_unet *net, int32_t on);
+/* The network's numbers: 0 levels, 1 iterations of the last fc_fcg_solve that used the network,
+ * 2 whether its safeguard dropped the network, 3 whether the block-Jacobi part is set. */
+int64_t fc_unet_stat(const fc_unet *net, int32_t what);
 int fc_unet_set_stream(fc_unet *net, void *stream);
 /* Parameters (FP32, per layer: weights [27][cout][cin] then biases [cout]) and their gradients
  * after the last backward pass, as host arrays of fc_unet_param_count values. */
@@ -54,9 +72,16 @@ int fc_unet_apply(fc_unet *net, const double *d_r, double *d_z);
 int fc_unet_train_step(fc_unet *net, const double *d_r, const double *d_e, const int64_t *d_ptr, const int32_t *d_idx,
                        const double *d_val, float lr, int32_t step, double *d_loss);
 
+/* One Adam step on the mean gradient of `count` pairs (column q of d_r and d_e at q * ld, ld >= n):
+ * the losses as fc_unet_train_step; *d_loss gets their sum. */
+int fc_unet_train_batch(fc_unet *net, const double *d_r, const double *d_e, int32_t count, int64_t ld,
+                        const int64_t *d_ptr, const int32_t *d_idx, const double *d_val, float lr, int32_t step,
+                        double *d_loss);
 /* Flexible CG on A x = b (A by rows on the device, as fc_csr_spmv_device), x from zero, with the
  * network as preconditioner (net null: plain CG), keeping `keep` (1..8) earlier directions
- * A-orthogonal. Stops when ||b - A x|| <= tol ||b|| or after max_iter iterations; then, when not
+ * A-orthogonal. A safeguard drops the network for the rest of the solve when 25 iterations with it
+ * lower ||r||^2 by less than a factor 4 (the block-Jacobi part, if set, stays; fc_unet_stat says
+ * whether and when). Stops when ||b - A x|| <= tol ||b|| or after max_iter iterations; then, when not
  * converged and `fallback` (a factor of A) is given, x is the Cholesky solution and *used_fallback
  * is 1. *relres is the relative residual of the x returned (recomputed for the fallback). Returns
  * FC_TIMEOUT when neither reached the tolerance. */

@@ -19,8 +19,21 @@ import numpy as np
 
 C, CIO = 32, 16
 SLOPE = 0.05  # leaky ReLU: x for x > 0, SLOPE x otherwise
-LAYERS = [(CIO, C, 0), (C, C, 0), (C, C, 1), (C, C, 1), (C, C, 2), (C, C, 2), (C, C, 1), (C, C, 1), (C, C, 0),
-          (C, C, 0), (C, CIO, 0)]  # (cin, cout, level)
+
+
+def layers(levels: int = 3):
+    """(cin, cout, level) of each convolution in forward order for a network of `levels` levels:
+    two per level on the way down (the first from the CIO input channels), two at the bottom, two
+    per level on the way up, and the output convolution to CIO channels (4 levels - 1 in all)."""
+    out = []
+    for lv in range(levels):
+        out += [(CIO if lv == 0 else C, C, lv), (C, C, lv)]
+    for lv in range(levels - 2, -1, -1):
+        out += [(C, C, lv), (C, C, lv)]
+    return out + [(C, CIO, 0)]
+
+
+LAYERS = layers(3)
 
 
 def bf16(a) -> np.ndarray:
@@ -31,10 +44,10 @@ def bf16(a) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def split_params(flat: np.ndarray):
+def split_params(flat: np.ndarray, levels: int = 3):
     """The flat FP32 parameter vector (per layer: weights [27][cout][cin], then biases) as lists."""
     ws, bs, off = [], [], 0
-    for cin, cout, _ in LAYERS:
+    for cin, cout, _ in layers(levels):
         nw = 27 * cin * cout
         ws.append(np.asarray(flat[off:off + nw], np.float64).reshape(27, cout, cin))
         off += nw
@@ -120,76 +133,76 @@ def pool_adjoint(dc, shape_f):
 
 
 class Net:
-    """forward(x) -> y, keeping what backward(dy) needs; backward returns (grads_w, grads_b)."""
+    """forward(x) -> y, keeping what backward(dy) needs; backward returns (grads_w, grads_b).
+    `levels` levels: per level on the way down two convolutions (the second's output is the skip)
+    and a 2x2x2 average pooling, two convolutions at the bottom, per level on the way up nearest
+    upsampling plus the skip and two convolutions, then the output convolution."""
 
-    def __init__(self, flat_params: np.ndarray, use_bf16: bool = True):
-        self.ws, self.bs = split_params(flat_params)
+    def __init__(self, flat_params: np.ndarray, use_bf16: bool = True, levels: int = 3):
+        self.levels = levels
+        self.ws, self.bs = split_params(flat_params, levels)
         self.q = bf16 if use_bf16 else (lambda a: np.asarray(a, np.float64))
         self.ws = [self.q(w) for w in self.ws]
 
     def forward(self, x):
-        q, W, Bv = self.q, self.ws, self.bs
+        q, W, Bv, D = self.q, self.ws, self.bs, self.levels
         relu = lambda a: np.where(a > 0, a, SLOPE * a)
-        s = self.s = {}
-        g0 = x.shape[:3]
-        g1 = coarser(g0)
-        s["x"] = q(x)
-        s["a0"] = q(relu(conv(s["x"], W[0], Bv[0])))
-        s["s0"] = q(relu(conv(s["a0"], W[1], Bv[1])))
-        s["p1"] = q(pool(s["s0"]))
-        s["a1"] = q(relu(conv(s["p1"], W[2], Bv[2])))
-        s["s1"] = q(relu(conv(s["a1"], W[3], Bv[3])))
-        s["p2"] = q(pool(s["s1"]))
-        s["a2"] = q(relu(conv(s["p2"], W[4], Bv[4])))
-        s["m2"] = q(relu(conv(s["a2"], W[5], Bv[5])))
-        s["u1"] = q(up(s["m2"], g1) + s["s1"])
-        s["a3"] = q(relu(conv(s["u1"], W[6], Bv[6])))
-        s["d1"] = q(relu(conv(s["a3"], W[7], Bv[7])))
-        s["u0"] = q(up(s["d1"], g0) + s["s0"])
-        s["a4"] = q(relu(conv(s["u0"], W[8], Bv[8])))
-        s["d0"] = q(relu(conv(s["a4"], W[9], Bv[9])))
-        s["y"] = q(conv(s["d0"], W[10], Bv[10]))
+        s = self.s = {"x": q(x)}
+        inp, k = s["x"], 0
+        for lv in range(D):  # down, then the bottom
+            s[f"in{lv}"] = inp
+            s[f"a{lv}"] = q(relu(conv(inp, W[k], Bv[k])))
+            s[f"s{lv}"] = q(relu(conv(s[f"a{lv}"], W[k + 1], Bv[k + 1])))
+            k += 2
+            if lv < D - 1:
+                inp = q(pool(s[f"s{lv}"]))
+        low = s[f"s{D - 1}"]
+        for lv in range(D - 2, -1, -1):  # up
+            s[f"u{lv}"] = q(up(low, s[f"s{lv}"].shape[:3]) + s[f"s{lv}"])
+            s[f"b{lv}"] = q(relu(conv(s[f"u{lv}"], W[k], Bv[k])))
+            s[f"d{lv}"] = q(relu(conv(s[f"b{lv}"], W[k + 1], Bv[k + 1])))
+            k += 2
+            low = s[f"d{lv}"]
+        s["top"] = low
+        s["y"] = q(conv(low, W[k], Bv[k]))
         return s["y"]
 
     def backward(self, dy):
-        q, W, s = self.q, self.ws, self.s
+        q, W, s, D = self.q, self.ws, self.s, self.levels
         mask = lambda a: np.where(a > 0, 1.0, SLOPE)
-        g0, g1, g2 = s["x"].shape[:3], s["p1"].shape[:3], s["p2"].shape[:3]
-        gw, gb = [None] * 11, [None] * 11
+        nl = len(W)
+        gw, gb = [None] * nl, [None] * nl
         dy = q(dy)
-        gw[10], gb[10] = conv_dw(s["d0"], dy)
-        g = q(conv_t(dy, W[10]) * mask(s["d0"]))
-        gw[9], gb[9] = conv_dw(s["a4"], g)
-        g = q(conv_t(g, W[9]) * mask(s["a4"]))
-        gw[8], gb[8] = conv_dw(s["u0"], g)
-        gs0 = q(conv_t(g, W[8]))
-        g = q(up_adjoint(gs0, g1) * mask(s["d1"]))
-        gw[7], gb[7] = conv_dw(s["a3"], g)
-        g = q(conv_t(g, W[7]) * mask(s["a3"]))
-        gw[6], gb[6] = conv_dw(s["u1"], g)
-        gs1 = q(conv_t(g, W[6]))
-        g = q(up_adjoint(gs1, g2) * mask(s["m2"]))
-        gw[5], gb[5] = conv_dw(s["a2"], g)
-        g = q(conv_t(g, W[5]) * mask(s["a2"]))
-        gw[4], gb[4] = conv_dw(s["p2"], g)
-        g = q(conv_t(g, W[4]))
-        g = q((pool_adjoint(g, g1) + gs1) * mask(s["s1"]))
-        gw[3], gb[3] = conv_dw(s["a1"], g)
-        g = q(conv_t(g, W[3]) * mask(s["a1"]))
-        gw[2], gb[2] = conv_dw(s["p1"], g)
-        g = q(conv_t(g, W[2]))
-        g = q((pool_adjoint(g, g0) + gs0) * mask(s["s0"]))
-        gw[1], gb[1] = conv_dw(s["a0"], g)
-        g = q(conv_t(g, W[1]) * mask(s["a0"]))
-        gw[0], gb[0] = conv_dw(s["x"], g)
+        k = nl - 1
+        gw[k], gb[k] = conv_dw(s["top"], dy)
+        g = q(conv_t(dy, W[k]) * mask(s["top"]))  # dL/d(top), through its activation
+        gskip = {}
+        for lv in range(0, D - 1):  # up path, from the top level down to the coarsest
+            k -= 2
+            gw[k + 1], gb[k + 1] = conv_dw(s[f"b{lv}"], g)
+            g = q(conv_t(g, W[k + 1]) * mask(s[f"b{lv}"]))
+            gw[k], gb[k] = conv_dw(s[f"u{lv}"], g)
+            gu = q(conv_t(g, W[k]))  # dL/du: to the skip and, upsampled, to the level below
+            gskip[lv] = gu
+            below = s[f"d{lv + 1}"] if lv + 1 < D - 1 else s[f"s{D - 1}"]
+            g = q(up_adjoint(gu, below.shape[:3]) * mask(below))
+        for lv in range(D - 1, -1, -1):  # down path, from the bottom up
+            k -= 2
+            gw[k + 1], gb[k + 1] = conv_dw(s[f"a{lv}"], g)
+            g = q(conv_t(g, W[k + 1]) * mask(s[f"a{lv}"]))
+            gw[k], gb[k] = conv_dw(s[f"in{lv}"], g)
+            if lv == 0:
+                break
+            g = q(conv_t(g, W[k]))  # dL/d(pooled input of level lv)
+            g = q((pool_adjoint(g, s[f"s{lv - 1}"].shape[:3]) + gskip[lv - 1]) * mask(s[f"s{lv - 1}"]))
         return gw, gb
 
 
-def init_params(seed: int) -> np.ndarray:
+def init_params(seed: int, levels: int = 3) -> np.ndarray:
     """Random parameters of the network's layout (for checks; not the GPU's initialisation)."""
     rng = np.random.default_rng(seed)
     ws, bs = [], []
-    for cin, cout, _ in LAYERS:
+    for cin, cout, _ in layers(levels):
         ws.append(rng.standard_normal((27, cout, cin)) * np.sqrt(2.0 / (27 * cin)))
         bs.append(rng.standard_normal(cout) * 0.05)
     return join_params(ws, bs).astype(np.float32)

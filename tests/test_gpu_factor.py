@@ -131,6 +131,31 @@ def test_split_solve_does_not_depend_on_how_many_are_solved(cuda):
     assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rhs[69])
 
 
+def test_cluster_split_solve(cuda):
+    """The 16^3 block's short solve products run with K split over 8-CTA clusters (the default) or
+    in chunks of separate CTAs: both match the oracle; the cluster form is bit for bit the same on
+    every run and for a right-hand side alone or among 70."""
+    p = problems.lognormal_block(16, nrhs=1)
+    csr = p.csr
+    f = Factor.new(UpperColumns.from_symmetric(csr), 2**62)
+    _, ref = oracle_factor(csr)
+    rng = np.random.default_rng(8)
+    rhs = np.asfortranarray(rng.standard_normal((csr.n, 70)))
+    exp = ref.solve(rhs.copy())
+    runs = {}
+    for cluster in (1, 0, 1):
+        f.option(Factor.SOLVE_CLUSTER, cluster)
+        x = rhs.copy(order="F")
+        f.solve_many(x)
+        for j in range(x.shape[1]):
+            assert np.linalg.norm(x[:, j] - exp[:, j]) <= SOLVE_TOL * np.linalg.norm(exp[:, j]), (cluster, j)
+        runs.setdefault(cluster, []).append(x)
+    assert np.array_equal(runs[1][0].view(np.uint64), runs[1][1].view(np.uint64))
+    alone = np.ascontiguousarray(rhs[:, 5])
+    f.solve(alone)
+    assert np.array_equal(alone.view(np.uint64), runs[1][0][:, 5].copy().view(np.uint64))
+
+
 def test_factorisation_is_deterministic(cuda):
     csr = problems.lognormal_block(10, nrhs=1).csr
     up = UpperColumns.from_symmetric(csr)

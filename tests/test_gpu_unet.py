@@ -20,12 +20,13 @@ def small_plate(nx=10, ny=9, nz=3, seed=5):
     return problems.plate(nx, ny, nz, corr=3.0, contrast=100.0, seed=seed, nrhs=4)
 
 
-def test_forward_and_backward_match_the_oracle(cuda):
+@pytest.mark.parametrize("levels", [3, 5])
+def test_forward_and_backward_match_the_oracle(cuda, levels):
     torch = cuda
     from fieldcraft_b200.unet import UNet
-    p = small_plate()
-    net = UNet(p, seed=1)
-    flat = U.init_params(2)
+    p = small_plate() if levels <= 3 else small_plate(20, 17, 3)
+    net = UNet(p, seed=1, levels=levels)
+    flat = U.init_params(2, levels)
     net.set_params(flat)
     nx, ny, nz = p.dims
     shape = (nz + 1, ny + 1, nx + 1)
@@ -36,7 +37,7 @@ def test_forward_and_backward_match_the_oracle(cuda):
     y = torch.empty_like(dx)
     net.forward_grid(dx, y)
     net.backward_grid(dyd)
-    ref = U.Net(flat.astype(np.float64), use_bf16=True)
+    ref = U.Net(flat.astype(np.float64), use_bf16=True, levels=levels)
     yr = ref.forward(x.astype(np.float64))
     gw, gb = ref.backward(dy.astype(np.float64))
     got_y = y.cpu().numpy().reshape(yr.shape)
@@ -44,7 +45,7 @@ def test_forward_and_backward_match_the_oracle(cuda):
     got = net.grads()
     exp = U.join_params(gw, gb)
     off, errs = 0, []
-    for l, (cin, cout, _) in enumerate(U.LAYERS):
+    for l, (cin, cout, _) in enumerate(U.layers(levels)):
         nw = 27 * cin * cout
         for name, a, b in (("w", got[off:off + nw], exp[off:off + nw]),
                            ("b", got[off + nw:off + nw + cout], exp[off + nw:off + nw + cout])):
@@ -84,6 +85,43 @@ def test_training_and_fcg_gain_over_plain_cg(cuda):
             err = torch.linalg.vector_norm(x - exact) / torch.linalg.vector_norm(exact)
             assert err.item() < 1e-6
     assert max(its_nn) < 0.5 * min(its_cg), (its_nn, its_cg)
+
+
+def test_block_jacobi_batches_and_the_safeguard(cuda):
+    """With K's nodal block-Jacobi part the preconditioner is B r + net(r): an untrained network
+    (last layer zero) is then block-Jacobi PCG itself, as the network switched off; minibatch
+    training lowers the loss; a network of random weights is dropped by FCG's safeguard
+    (which says so) and the solve still converges on block Jacobi."""
+    torch = cuda
+    from fieldcraft_b200.unet import UNet, fcg, output_scale, train, training_pairs
+    p = problems.plate(24, 24, 4, corr=4.0, contrast=100.0, seed=9, nrhs=2)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62))
+    f.factor(up.val)
+    csr = tuple(torch.from_numpy(a).cuda() for a in (p.csr.ptr, p.csr.idx, p.csr.val))
+    R, E = training_pairs(f, p, 256, seed=3, torch=torch)
+    b = torch.from_numpy(np.ascontiguousarray(p.rhs[:, 0])).cuda()
+    net = UNet(p, seed=0, kref=output_scale(R, E), levels=4, operator=csr)
+    assert net.stat(3) == 1 and net.stat(0) == 4
+    runs = []
+    for on in (False, True):
+        net.enable(on)
+        x = torch.zeros_like(b)
+        runs.append(fcg(csr, b, x, net=net, tol=1e-10, max_iter=3000, keep=4))
+    assert runs[0][0] == runs[1][0] and runs[0][1] <= 1e-10  # an untrained network adds nothing
+    losses = train(net, R, E, epochs=3, lr=1e-3, torch=torch, csr_device=csr, batch=8, warmup=20)
+    assert losses[-1] < losses[0], losses
+    x = torch.zeros_like(b)
+    it, rel, fb = fcg(csr, b, x, net=net, tol=1e-10, max_iter=3000, keep=4)
+    assert rel <= 1e-10 and not fb
+    # random weights ten times their initial scale make a network whose output swamps B r with
+    # noise: FCG stalls on it, the safeguard drops it, and the solve converges on block Jacobi
+    bad = UNet(p, seed=0, kref=output_scale(R, E), levels=3, operator=csr)
+    bad.set_params(10.0 * U.init_params(7, 3))
+    x = torch.zeros_like(b)
+    it, rel, fb = fcg(csr, b, x, net=bad, tol=1e-10, max_iter=3000, keep=4)
+    assert rel <= 1e-10 and not fb
+    assert bad.stat(2) == 1 and bad.stat(1) < it
 
 
 def test_fcg_falls_back_to_cholesky(cuda):

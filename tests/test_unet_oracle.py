@@ -1,6 +1,7 @@
 """The learned preconditioner's CPU oracle checked against itself: its analytic gradients against
 finite differences (float64, no BF16 rounding), and the adjoint pairs it is built from."""
 import numpy as np
+import pytest
 
 from oracle import unet_oracle as U
 
@@ -17,24 +18,25 @@ def test_adjoint_pairs():
     assert np.isclose(np.sum(U.pool(f) * c), np.sum(f * U.pool_adjoint(c, (3, 5, 4))))
 
 
-def test_gradients_match_finite_differences():
+@pytest.mark.parametrize("levels", [2, 3, 5])
+def test_gradients_match_finite_differences(levels):
     rng = np.random.default_rng(5)
-    flat = U.init_params(1).astype(np.float64)
-    shape = (3, 5, 4)
+    flat = U.init_params(1, levels).astype(np.float64)
+    shape = (3, 5, 4) if levels <= 3 else (3, 9, 11)
     x = rng.standard_normal(shape + (U.CIO,))
     dy = rng.standard_normal(shape + (U.CIO,))
-    net = U.Net(flat, use_bf16=False)
+    net = U.Net(flat, use_bf16=False, levels=levels)
     net.forward(x)
     gw, gb = net.backward(dy)
     grad = U.join_params(gw, gb)
 
     def loss(p):
-        return float(np.sum(U.Net(p, use_bf16=False).forward(x) * dy))
+        return float(np.sum(U.Net(p, use_bf16=False, levels=levels).forward(x) * dy))
 
     # probe entries of every layer (weights and biases)
     probes = []
     off = 0
-    for cin, cout, _ in U.LAYERS:
+    for cin, cout, _ in U.layers(levels):
         nw = 27 * cin * cout
         probes += [off + int(rng.integers(nw)), off + nw + int(rng.integers(cout))]
         off += nw + cout

@@ -13,7 +13,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from fieldcraft_b200 import Factor, _lib, problems
+from fieldcraft_b200 import FP32_IR, FP64, Factor, Symbolic, _lib, problems
 from fieldcraft_b200._lib import Status
 
 pytestmark = pytest.mark.gpu
@@ -64,6 +64,27 @@ def test_no_alloc_solve_matches_the_ordinary_solve(cuda):
     assert ((x - ref1).norm() / ref1.norm()).item() <= SOLVE_TOL
     fb.close()
     fc.close()
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_IR], ids=["fp64", "fp32_ir"])
+def test_no_alloc_solve_with_split_products(cuda, precision):
+    """The 16^3 block: its top separator (867 columns) makes the solve split long products in
+    chunks that the last CTA adds (partials and counters in the scratch), and its thin
+    supernodes with more than 128 rows below sum their backward steps in chunks the same way.
+    With the FP64 factor and with the mixed-precision one (a 4-byte L); two calls in a row."""
+    torch = cuda
+    lib = _lib.load()
+    p = problems.lognormal_block(16, nrhs=5)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62), precision=precision)
+    f.factor(up.val)
+    b = column_major(torch, p.rhs)
+    ref = ordinary(lib, f, b, 5, p.n)
+    for _ in range(2):
+        x = no_alloc(lib, f, b, 5, p.n)
+        assert ((x - ref).norm() / ref.norm()).item() <= SOLVE_TOL
+    assert f.stat(8) > 0  # the launches of the last solve are counted
+    f.close()
 
 
 def test_no_alloc_solve_refuses_more_than_its_scratch(cuda):
