@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--profile-only", action="store_true", help="a short run for ncu (no baselines, no e2e)")
     ap.add_argument("--no-nn", action="store_true", help="skip the learned-preconditioner measurement")
+    ap.add_argument("--nn-pairs", type=int, default=256, help="training pairs of the headline's learned preconditioner")
+    ap.add_argument("--nn-epochs", type=int, default=3, help="training epochs of the learned preconditioner")
     ap.add_argument("--profile-kernels", choices=["fp32-factor", "unet"], default=None,
                     help="a short run for a profiler: two FP32 factorisations of the --n-el block, or the "
                          "U-Net's forward and backward passes on a 64x64x8 plate, twice")
@@ -271,19 +273,33 @@ def oracle_spmv(w, x):
     return oracle.spmv(w.n, w.ptr, w.idx, w.val, x)
 
 
-def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap: int, chol_ms: float) -> dict:
-    """The learned preconditioner on the same K: pairs (r, K^-1 r) from the Cholesky solve, Adam
-    training on the GPU, then flexible CG to rel-res 1e-10 from zero on held-out right-hand sides,
-    with and without the network (both capped at `cap` iterations, the Cholesky solve as fallback).
-    chol_ms: the FP64 Cholesky's time for one right-hand side (factor + solve) on the same K."""
+def nn_levels(p) -> int:
+    """U-Net levels for a box problem's node grid: pooling until the longest side is about 8 nodes."""
+    longest = max(p.dims) + 1
+    levels = 1
+    while longest > 8 and levels < 6:
+        longest = (longest + 1) // 2
+        levels += 1
+    return levels
+
+
+def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap: int, chol_ms: float,
+                 batch: int = 8, levels: int | None = None) -> dict:
+    """The learned preconditioner on the same K: pairs (r, K^-1 r) from the Cholesky solve, minibatch
+    Adam training on the GPU of a U-Net whose output is added to K's nodal block-Jacobi part, then
+    flexible CG to rel-res 1e-10 from zero on held-out right-hand sides with the network ('nn_fcg'),
+    with the block-Jacobi part alone ('bj') and with no preconditioner ('cg'), all capped at `cap`
+    iterations with the Cholesky solve as fallback. chol_ms: the FP64 Cholesky's time for one
+    right-hand side (factor + solve) on the same K."""
     from fieldcraft_b200.unet import UNet, fcg, output_scale, train, training_pairs
+    levels = levels or nn_levels(p)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     R, E = training_pairs(factor64, p, pairs, seed=SEED + 5, torch=torch)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    net = UNet(p, seed=0, kref=output_scale(R, E))
-    losses = train(net, R, E, epochs=epochs, lr=3e-4, torch=torch, csr_device=csr_dev)
+    net = UNet(p, seed=0, kref=output_scale(R, E), levels=levels, operator=csr_dev)
+    losses = train(net, R, E, epochs=epochs, lr=1e-3, torch=torch, csr_device=csr_dev, batch=batch, warmup=50)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     del R, E
@@ -293,7 +309,9 @@ def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap
         exact = b.clone()
         factor64.solve_device(exact, 1, p.n)
         row = {}
-        for name, use in (("nn_fcg", net), ("cg", None)):
+        for name, use, on in (("nn_fcg", net, True), ("bj", net, False), ("cg", None, True)):
+            if use is not None:
+                use.enable(on)
             x = torch.zeros_like(b)
             torch.cuda.synchronize()
             ta = time.perf_counter()
@@ -302,16 +320,23 @@ def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap
             dt = time.perf_counter() - ta
             err = float((torch.linalg.vector_norm(x - exact) / torch.linalg.vector_norm(exact)).item())
             row[name] = {"iterations": it, "s": dt, "relres": rel, "fallback": fb, "err_vs_cholesky": err}
+            if name == "nn_fcg":
+                row[name]["network_iterations"] = net.stat(1)
+                row[name]["network_dropped"] = bool(net.stat(2))
+        net.enable(True)
         runs.append(row)
     nn_s = [r["nn_fcg"]["s"] for r in runs]
     net.close()
     return {"value": float(np.mean(nn_s)), "unit": UNIT,
             "speedup_vs_fp64": (chol_ms / 1e3) / float(np.mean(nn_s)),
-            "fp64_cholesky_1rhs_s": chol_ms / 1e3, "pairs": pairs, "epochs": epochs, "pairs_s": t1 - t0,
-            "train_s": t2 - t1, "loss_by_epoch": losses, "cap": cap, "rhs": runs,
-            "what": "3-level 32-channel BF16 3D-conv U-Net trained (energy-norm loss, Adam) on pairs from the "
-                    "Cholesky solve; flexible CG (4 kept directions) from zero to rel-res 1e-10 on held-out "
-                    "right-hand sides; 'cg' is the same solver without the network; a run that did not converge "
+            "speedup_vs_cg": float(np.mean([r["cg"]["s"] for r in runs])) / float(np.mean(nn_s)),
+            "fp64_cholesky_1rhs_s": chol_ms / 1e3, "pairs": pairs, "epochs": epochs, "batch": batch,
+            "levels": levels, "pairs_s": t1 - t0, "train_s": t2 - t1, "loss_by_epoch": losses, "cap": cap,
+            "rhs": runs,
+            "what": f"{levels}-level 32-channel BF16 3D-conv U-Net added to K's nodal block-Jacobi inverse, trained "
+                    "(energy-norm loss, minibatch Adam) on pairs from the Cholesky solve; flexible CG (4 kept "
+                    "directions) from zero to rel-res 1e-10 on held-out right-hand sides; 'bj' the same solver "
+                    "with the block-Jacobi part alone, 'cg' with no preconditioner; a run that did not converge "
                     "within the cap falls back to the Cholesky solve (fallback true, time included)"}
 
 
@@ -560,7 +585,7 @@ def run_config(args, cfg: int, torch, lib, local: int):
                     "relres_max": res[FP32_IR]["relres_max"], "speedup_vs_fp64": res[FP64]["ms"] / res[FP32_IR]["ms"]},
     }
     if tuned:
-        names = {"1": "solve_schedule", "5": "refinement", "6": "fp32_updates"}
+        names = {"1": "solve_schedule", "5": "refinement", "6": "fp32_updates", "7": "solve_cluster"}
         line["autotuned"] = {("fp64" if prec == FP64 else "fp32_ir"):
                              {"options": {names[k]: v for k, v in t["options"].items()},
                               "candidates_ms": t["ms"]} for prec, t in tuned.items()}
@@ -591,8 +616,8 @@ def run_config(args, cfg: int, torch, lib, local: int):
             e1.record(stream)
             e1.synchronize()
             tt.append(e0.elapsed_time(e1))
-        line["nn_fcg"] = nn_fcg_block(p, keep64, csr_dev, torch, pairs=2000, epochs=2, cols=range(min(R, 2)),
-                                      cap=3000, chol_ms=float(np.min(tt[1:])))
+        line["nn_fcg"] = nn_fcg_block(p, keep64, csr_dev, torch, pairs=2000, epochs=args.nn_epochs,
+                                      cols=range(min(R, 2)), cap=3000, chol_ms=float(np.min(tt[1:])))
     if not args.no_cpu_baseline and owl is not None:
         threads = os.cpu_count() or 1
         r = oracle_full_run(owl, threads, 0.0, max_runs=1)
@@ -995,8 +1020,8 @@ def main():
             e1.synchronize()
             tt.append(e0.elapsed_time(e1))
         f.set_stream(None)
-        nn = nn_fcg_block(p, f, (d_ptr, d_idx, d_kv), torch, pairs=256, epochs=2, cols=[0], cap=1500,
-                          chol_ms=float(np.min(tt[1:])))
+        nn = nn_fcg_block(p, f, (d_ptr, d_idx, d_kv), torch, pairs=args.nn_pairs, epochs=args.nn_epochs, cols=[0],
+                          cap=1500, chol_ms=float(np.min(tt[1:])))
         f.set_stream(stream.cuda_stream)
     # FP32 (3xTF32) factorisation of S A S + FP64 refinement to the same rel-res, same system
     fp32 = None

@@ -1,7 +1,8 @@
 """Chooses a handle's execution variants by timing them on the system itself: the kernels' tile
 shapes for the mixed-precision factor's update products (tcgen05 128 x 128 or mma.sync 64 x 64),
-the solve's schedule (level by level, or one persistent dependency-driven launch per direction)
-and, for a factor used as a preconditioner, conjugate gradients or plain refinement. Each
+the solve's schedule (level by level, or one persistent dependency-driven launch per direction),
+how the level-by-level solve splits the K of its short products (8-CTA clusters or chunks) and,
+for a factor used as a preconditioner, conjugate gradients or plain refinement. Each
 candidate is run (factorisation + solve to the tolerance, device-timed with CUDA events) and the
 fastest is kept in the handle; results can be cached in a JSON file keyed by the system's shape.
 No reference counterpart (the reference has one CPU code path)."""
@@ -17,11 +18,14 @@ from .cholesky import FP32_IR, Factor
 
 
 def candidates(precision: int) -> list[dict]:
-    schedules = [0, 1]
+    # the solve: level by level with its short products' K split over 8-CTA clusters or in chunks
+    # of separate CTAs, or the persistent dependency-driven launch (where the split does not apply)
+    solves = [{Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 0}, {Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 1},
+              {Factor.SOLVE_SCHEDULE: 1, Factor.SOLVE_CLUSTER: 0}]
     if precision == FP32_IR:
-        return [{Factor.FP32_UPDATES: u, Factor.SOLVE_SCHEDULE: s, Factor.REFINEMENT: r}
-                for u, s, r in itertools.product([0, 1], schedules, [0, 1])]
-    return [{Factor.SOLVE_SCHEDULE: s} for s in schedules]
+        return [{Factor.FP32_UPDATES: u, **sv, Factor.REFINEMENT: r}
+                for u, sv, r in itertools.product([0, 1], solves, [0, 1])]
+    return [dict(sv) for sv in solves]
 
 
 def signature(factor: Factor, precision: int, nrhs: int) -> str:

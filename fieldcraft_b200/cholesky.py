@@ -346,6 +346,16 @@ class LdltFactor(Factor):
         pos, neg, _ = self._counts()
         return Inertia(pos, neg)
 
+    def pivots(self):
+        """(pivots, order): per column in postorder its pivot kind (0 one, 1 first, 2 second of a
+        2 x 2) and the supernode-local column at that pivot position, as the oracle reports them."""
+        piv = np.zeros(self.n, np.int8)
+        order = np.zeros(self.n, np.int32)
+        st = Status()
+        _lib.load().fc_chol_ldlt_pivots(self.handle, _lib.ptr(piv), _lib.ptr(order), C.byref(st))
+        raise_for(st)
+        return piv.astype(np.int64), order.astype(np.int64)
+
     def two_by_two(self) -> int:
         return self._counts()[2]
 

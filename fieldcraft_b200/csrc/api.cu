@@ -144,9 +144,9 @@ struct fc_chol {
   // the solve as two dependency-driven persistent launches instead of level by level
   // (FC_OPTION_SOLVE_SCHEDULE, or FC_SOLVE_PERSISTENT=1 in the environment)
   bool dag = false;
-  // the solve's launches with few output tiles split K over thread-block clusters (default) or in
-  // chunks summed by their last CTA (FC_OPTION_SOLVE_CLUSTER = 0)
-  bool solve_cluster = true;
+  // the solve's launches with few output tiles split K in chunks summed by their last CTA (default)
+  // or over thread-block clusters (FC_OPTION_SOLVE_CLUSTER = 1)
+  bool solve_cluster = false;
   DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
   int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
   int dag_grid = 0;
@@ -3139,6 +3139,25 @@ int fc_chol_solve(fc_chol *h, double *b, int32_t nrhs, int64_t ld, fc_status *st
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(status, e, "solve");
   if ((rc = solve_wait_status(h, status)) != FC_OK) return rc;
+  set_status(status, FC_OK);
+  return FC_OK;
+}
+
+int fc_chol_ldlt_pivots(fc_chol *h, int8_t *pivots, int32_t *order, fc_status *status) {
+  if (!h || !h->ldlt || (h->n > 0 && (!pivots || !order))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "not an LDL^T factor, or a null argument");
+    return FC_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> g(h->lock);
+  cudaSetDevice(h->device);
+  if (h->n == 0) {
+    set_status(status, FC_OK);
+    return FC_OK;
+  }
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(pivots, h->d_lpivots.p, (size_t)h->n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(order, h->d_lorder.p, sizeof(int32_t) * (size_t)h->n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(status, e, "pivots");
   set_status(status, FC_OK);
   return FC_OK;
 }

@@ -1309,9 +1309,17 @@ __global__ void pack_kernel(Tree t, const int64_t *__restrict__ toff, double *__
   }
 }
 
+// Every kernel of the factorisation and the solve asks for the same split of the SM's L1 and
+// shared memory (all of it shared): consecutive launches with different preferred splits make an
+// SM reconfigure between them, which it can only do once it has drained.
+template <class K>
+void max_shared(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+}
 template <class K>
 void set_smem(K kernel, size_t bytes) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  max_shared(kernel);
 }
 
 }  // namespace
@@ -1326,6 +1334,13 @@ void configure_kernels() {
   set_smem(gemm_cluster_kernel<double>, gemm_smem<double>());
   set_smem(gemm_cluster_kernel<float>, gemm_smem<float>());
   set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
+  max_shared(assemble_kernel<double>);
+  max_shared(assemble_kernel<float>);
+  max_shared(thin_fwd_kernel<double>);
+  max_shared(thin_fwd_kernel<float>);
+  max_shared(thin_bwd_kernel<double>);
+  max_shared(thin_bwd_kernel<float>);
+  max_shared(solve_assemble_kernel);
   configure_solve_dag();
   done = true;
 }
@@ -1337,6 +1352,7 @@ void launch_scale(int64_t n, const int64_t *diag_src, const double *val, double 
 void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const AssembleTask *tasks, const int4 *ranges,
                      int count, cudaStream_t st) {
   if (count <= 0) return;
+  configure_kernels();
   if (fp32)
     assemble_kernel<float><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
   else
@@ -1380,12 +1396,15 @@ void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStre
 
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,
                            const int2 *ranges, int count, cudaStream_t st) {
-  if (count > 0) solve_assemble_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks, ranges);
+  if (count <= 0) return;
+  configure_kernels();
+  solve_assemble_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks, ranges);
 }
 
 void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, double *v, const int64_t *voff, int R,
                      int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st) {
   if (count <= 0) return;
+  configure_kernels();
   if (fp32)
     thin_fwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, v, voff, R, lg, tasks, ranges);
   else
@@ -1395,6 +1414,7 @@ void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, doub
 void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int R, int lg, const ThinBwdTask *tasks,
                      double *part, int32_t *counters, int count, cudaStream_t st) {
   if (count <= 0) return;
+  configure_kernels();
   if (fp32)
     thin_bwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
   else

@@ -496,7 +496,10 @@ int fc_unet_apply(fc_unet *u, const double *d_r, double *d_z) {
   if (!u || !d_r || !d_z) return FC_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(u->lock);
   cudaSetDevice(u->device);
-  apply(u, d_r, d_z);
+  if (u->net_on)
+    apply(u, d_r, d_z);
+  else
+    apply_jacobi(u, d_r, d_z);
   return cudaGetLastError() == cudaSuccess ? FC_OK : FC_CUDA_ERROR;
 }
 
@@ -574,9 +577,10 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
   const double target = tol * tol * bb;
   int it = 0, stored = 0;
   bool converged = bb == 0.0;
-  // The safeguard: while the network is in use, a window of SAFE_WINDOW iterations that does not
-  // lower ||r||^2 by SAFE_DROP drops it for the rest of the solve (the block-Jacobi part, when
-  // set, stays) and restarts the directions.
+  // The safeguard: while the network is in use, from iteration 2 SAFE_WINDOW on, a window of
+  // SAFE_WINDOW iterations that does not lower ||r||^2 by SAFE_DROP drops it for the rest of the
+  // solve (the block-Jacobi part, when set, stays; the kept directions stay A-orthogonal, so FCG
+  // goes on with them).
   constexpr int SAFE_WINDOW = 25;
   constexpr double SAFE_DROP = 0.25;
   bool use_net = net != nullptr && net->net_on;
@@ -636,10 +640,9 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
     if (use_net) {
       net->last_net_iterations = it;
       const size_t h = history.size();
-      if (h > SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
+      if (h >= 2 * SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
         use_net = false;
         net->last_dropped = 1;
-        stored = 0;
       }
     }
   }

@@ -168,6 +168,74 @@ def training_pairs(factor: Factor, problem: Problem, count: int, seed: int, torc
     return R, E
 
 
+def block_jacobi(problem: Problem, torch):
+    """The inverses of K's nodal 3 x 3 diagonal blocks (equations node by node, three a node), as a
+    CUDA tensor [n / 3, 3, 3]."""
+    csr = problem.csr
+    n = csr.n
+    rows = np.repeat(np.arange(n), np.diff(csr.ptr))
+    keep = (csr.idx // 3) == (rows // 3)
+    blocks = np.zeros((n // 3, 3, 3))
+    blocks[rows[keep] // 3, rows[keep] % 3, csr.idx[keep] % 3] = csr.val[keep]
+    return torch.from_numpy(np.linalg.inv(blocks)).cuda()
+
+
+def krylov_pairs(factor: Factor, problem: Problem, csr_device, count: int, seed: int, torch,
+                 snapshots=(0, 2, 5, 10, 20, 40, 80, 160), block: int = 32):
+    """`count` pairs (r, K^-1 r) whose r are the residuals that block-Jacobi preconditioned CG
+    leaves on random right-hand sides (random top-face pressures and white noise, half each) at the
+    iterations `snapshots`: the inputs a preconditioner meets inside the Krylov solve, in which
+    the smooth, slowly converging parts dominate more and more. Each r is scaled to unit norm; e =
+    K^-1 r from the Cholesky solve. Returns two CUDA tensors [count, n] (FP64)."""
+    from .problems import top_pressures
+    lib = _lib.load()
+    n = problem.n
+    per = len(snapshots)
+    rhs_count = (count + per - 1) // per
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    Binv = block_jacobi(problem, torch)
+    ptr, idx, val = csr_device
+    out = torch.empty((rhs_count * per, n), dtype=torch.float64, device="cuda")
+    at = 0
+    for b0 in range(0, rhs_count, block):
+        k = min(block, rhs_count - b0)
+        half = k // 2
+        B = torch.empty((k, n), dtype=torch.float64, device="cuda")
+        B[:half] = torch.randn((half, n), dtype=torch.float64, device="cuda", generator=g)
+        B[half:] = torch.from_numpy(np.ascontiguousarray(top_pressures(problem, k - half, seed + 31 + b0).T)).cuda()
+        X = torch.zeros_like(B)
+        Rr = B.clone()
+        prec = lambda r: torch.einsum("kab,jkb->jka", Binv, r.view(r.shape[0], n // 3, 3)).reshape(r.shape)  # noqa
+        Z = prec(Rr)
+        P = Z.clone()
+        rz = (Rr * Z).sum(dim=1)
+        Q = torch.empty_like(B)
+        for it in range(max(snapshots) + 1):
+            if it in snapshots:
+                out[at:at + k] = Rr / torch.linalg.vector_norm(Rr, dim=1, keepdim=True)
+                at += k
+            if it == max(snapshots):
+                break
+            lib.fc_csr_spmv_device(n, C.c_void_p(ptr.data_ptr()), C.c_void_p(idx.data_ptr()),
+                                   C.c_void_p(val.data_ptr()), C.c_void_p(P.data_ptr()), C.c_void_p(Q.data_ptr()), k,
+                                   n, None)
+            alpha = rz / (P * Q).sum(dim=1)
+            X += alpha[:, None] * P
+            Rr -= alpha[:, None] * Q
+            Z = prec(Rr)
+            rz_new = (Rr * Z).sum(dim=1)
+            P = Z + (rz_new / rz)[:, None] * P
+            rz = rz_new
+    R = out[:count].contiguous()
+    E = R.clone()
+    for s in range(0, count, 64):
+        e = min(count, s + 64)
+        factor.solve_device(E[s:e], e - s, n)
+    torch.cuda.synchronize()
+    return R, E
+
+
 def output_scale(R, E) -> float:
     """The network's output scale for pairs (r, K^-1 r): the median of ||r|| / ||e||, so that the
     network's outputs are of order one."""

@@ -150,6 +150,10 @@ int fc_chol_solve_device_noalloc(fc_chol *h, double *d_b, int32_t nrhs, int64_t 
  * trapezoid by columns (column c holds rows c..m, cholesky.rs:418-425, 1534-1542). dst has
  * fc_chol_entries(h) doubles. */
 int fc_chol_values(fc_chol *h, double *dst, fc_status *status);
+/* The LDL^T factor's pivots (ldlt.rs:399-447, Pivot): per column in postorder its kind (0 a 1 x 1
+ * pivot, 1 / 2 the first / second column of a 2 x 2) and the supernode-local column at that pivot
+ * position. n entries each; FC_INVALID_ARGUMENT for a Cholesky factor. */
+int fc_chol_ldlt_pivots(fc_chol *h, int8_t *pivots, int32_t *order, fc_status *status);
 /* LdltFactor::inertia and two_by_two (ldlt.rs:399-447): the counts of positive and negative
  * eigenvalues of A (Sylvester's law on D) and of 2 x 2 pivots; a Cholesky factor's are (n, 0, 0). */
 int fc_chol_inertia(fc_chol *h, int64_t *positive, int64_t *negative, int64_t *two_by_two, fc_status *status);
@@ -194,9 +198,9 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *                              in 128 x 128 tiles (default), 1 on mma.sync in 64 x 64 tiles
  *                              (re-plans the factorisation; takes effect from the next one).
  *   FC_OPTION_SOLVE_CLUSTER    the level-by-level solve's products in launches with few output
- *                              tiles: 1 each tile's K split over a cluster of 8 CTAs that add
- *                              their partials through distributed shared memory (default); 0 K
- *                              split in chunks of separate CTAs, the last adding the partials. */
+ *                              tiles: 0 K split in chunks of separate CTAs, the last adding the
+ *                              partials (default); 1 each tile's K split over a cluster of 8 CTAs
+ *                              that add their partials through distributed shared memory. */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3

@@ -64,7 +64,8 @@ int fc_unet_get_grads(fc_unet *net, float *host);
  * parameters' gradients. */
 int fc_unet_forward_grid(fc_unet *net, const float *d_x, float *d_y);
 int fc_unet_backward_grid(fc_unet *net, const float *d_dy);
-/* z = M(r): the network applied to an equation vector (scaled by ||r|| so that M(a r) = a M(r)). */
+/* z = M(r): the network applied to an equation vector (scaled by ||r|| so that M(a r) = a M(r)),
+ * plus B r when the operator is set; B r alone while the network is switched off. */
 int fc_unet_apply(fc_unet *net, const double *d_r, double *d_z);
 /* One Adam step on one pair (r, e = K^-1 r): loss = ||M(r) - e||^2 / ||e||^2, or with K given by
  * rows (d_ptr non-null) the energy norm (M(r) - e)^T K (M(r) - e) / e^T r; written to *d_loss (a
@@ -79,9 +80,9 @@ int fc_unet_train_batch(fc_unet *net, const double *d_r, const double *d_e, int3
                         double *d_loss);
 /* Flexible CG on A x = b (A by rows on the device, as fc_csr_spmv_device), x from zero, with the
  * network as preconditioner (net null: plain CG), keeping `keep` (1..8) earlier directions
- * A-orthogonal. A safeguard drops the network for the rest of the solve when 25 iterations with it
- * lower ||r||^2 by less than a factor 4 (the block-Jacobi part, if set, stays; fc_unet_stat says
- * whether and when). Stops when ||b - A x|| <= tol ||b|| or after max_iter iterations; then, when not
+ * A-orthogonal. A safeguard drops the network for the rest of the solve when, from iteration 50 on,
+ * 25 iterations with it lower ||r||^2 by less than a factor 4 (the block-Jacobi part, if set,
+ * stays; fc_unet_stat says whether and when). Stops when ||b - A x|| <= tol ||b|| or after max_iter iterations; then, when not
  * converged and `fallback` (a factor of A) is given, x is the Cholesky solution and *used_fallback
  * is 1. *relres is the relative residual of the x returned (recomputed for the fallback). Returns
  * FC_TIMEOUT when neither reached the tolerance. */

@@ -1,7 +1,9 @@
 """The device LDL^T factor (FC_PRECISION_LDLT) against the oracle's (crates/solver/src/ldlt.rs):
 inertia exactly, the factor's values within 1e-11 of the largest entry where the pivots are the
-same (the updates run on the FP64 tensor pipe with fused multiply-adds, so a near tie in the rook
-search may choose another, equally valid pivot), solutions within 1e-10 of the oracle's and
+same (1e-9 where element growth amplifies rounding; see VALUES_TOL), the pivots themselves the
+same in most supernodes (the updates run on the FP64 tensor pipe with fused multiply-adds, so an
+exact tie in the rook search, common on a uniform grid, may break the other way: another, equally
+valid factor), solutions within 1e-10 of the oracle's and
 solve_many bit for bit the single solves, values unchanged by a solve, singular columns named.
 The panel's source is also checked bit for bit on the CPU (tests/test_ldlt_panel_emulated.py) and
 the solve's structure by tests/test_ldlt_fold.py."""
@@ -30,15 +32,49 @@ CASES = {
 }
 
 
+# Values where the pivots agree: to rounding on the definite grid, the saddle point and the
+# indefinite grid. The wide indefinite grid has supernodes of one column, which cannot pivot (rows
+# below are never candidates): their small 1 x 1 pivots give multipliers up to 6 761, which carry
+# the rounding of the cancellation that made each pivot (the tensor pipe's fused multiply-adds
+# against the oracle's separate ones) to their ancestors, amplified; there the values agree to
+# 1e-9 of the largest entry (measured 4.5e-10) and the solutions still to 1e-10 (below).
+VALUES_TOL = {"grid indefinite": 1e-11, "saddle": 1e-11, "grid definite": 1e-11, "grid wide": 1e-9}
+
+
+def supernode_of_entries(o, n):
+    """Per value of the reference layout (supernode by supernode, each its trapezoid by columns),
+    the supernode it belongs to; and per column, its supernode."""
+    first, rptr = o.sym.array("first"), o.sym.array("rptr")
+    ent, col = [], []
+    for s in range(first.size - 1):
+        w, m = int(first[s + 1] - first[s]), int(rptr[s + 1] - rptr[s])
+        ent.append(np.full(w * m - w * (w - 1) // 2, s))
+        col.append(np.full(w, s))
+    return np.concatenate(ent), np.concatenate(col)
+
+
 @pytest.mark.parametrize("name", list(CASES))
 def test_factor_and_inertia_match_the_oracle(cuda, name):
+    """Inertia exactly. Where a supernode took the oracle's pivots (kinds and orders), its values
+    within VALUES_TOL of the largest entry. A uniform grid's matrix has many exactly equal magnitudes,
+    and the tensor-pipe updates round differently from the oracle's, so the rook search may break
+    a tie the other way in some supernodes: such a factor is another valid one (its solves are
+    checked against the oracle's below); most supernodes must still agree."""
     a = CASES[name]()
     g, o = both(a)
     assert (g.inertia().positive, g.inertia().negative) == o.inertia()
     gv, ov = g.values(), o.values()
     assert gv.shape == ov.shape
-    if g.two_by_two() == o.two_by_two():
-        assert np.max(np.abs(gv - ov)) <= 1e-11 * np.max(np.abs(ov))
+    gp, go = g.pivots()
+    op, oo = o.pivots()
+    ent_sn, col_sn = supernode_of_entries(o, a.n)
+    ns = int(col_sn.max()) + 1 if col_sn.size else 0
+    differs = np.zeros(ns, bool)
+    np.logical_or.at(differs, col_sn, (gp != op) | (go != oo))
+    same = ~differs[ent_sn]
+    assert differs.mean() <= 0.25, differs.mean()
+    if same.any():
+        assert np.max(np.abs(gv[same] - ov[same])) <= VALUES_TOL[name] * np.max(np.abs(ov))
 
 
 @pytest.mark.parametrize("name", list(CASES))
