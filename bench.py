@@ -905,7 +905,7 @@ def main():
         ms_k = np.zeros(kinds)
         cnt_k = np.zeros(kinds, np.int64)
         lib.fc_chol_profile(f.handle, 1)
-        step()
+        relres = step()
         lib.fc_chol_profile_read(f.handle, ms_k.ctypes.data, cnt_k.ctypes.data, kinds)
         lib.fc_chol_profile(f.handle, 0)
         for _ in range(args.warmup):

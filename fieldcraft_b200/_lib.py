@@ -42,6 +42,8 @@ SIGNATURES = {
     "fc_chol_factor_device_async": (i32, [P, P, i64]),
     "fc_chol_check": (i32, [P, C.POINTER(Status)]),
     "fc_chol_ldlt_pivots": (i32, [P, P, P, C.POINTER(Status)]),
+    "fc_chol_batch_analyse": (i32, [i32, P, P, P, u64, C.POINTER(P), P, C.POINTER(Status)]),
+    "fc_chol_batch_locate": (i32, [i32, P, i64, C.POINTER(i32), C.POINTER(i64)]),
     "fc_chol_entries": (i64, [P]),
     "fc_chol_solve": (i32, [P, P, i32, i64, C.POINTER(Status)]),
     "fc_chol_solve_device": (i32, [P, P, i32, i64, C.POINTER(Status)]),

@@ -58,18 +58,21 @@ class BatchFactor:
     def __init__(self, parts: list[UpperColumns], max_entries: int, precision: int = FP64, device: int = 0):
         self._csr_dev = None
         self.sizes = np.array([p.n for p in parts], np.int64)
-        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
         self.nnz = np.array([int(p.ptr[-1]) for p in parts], np.int64)
-        whole = block_diagonal(parts)
-        self.n = whole.n
-        self.symbolic = Symbolic(whole, max_entries)
+        self.symbolic, self.offsets = Symbolic.batch(parts, max_entries)  # fc_chol_batch_analyse
+        self.n = self.symbolic.n
         self.factor_ = Factor(self.symbolic, precision, device)
-        self._whole_pattern = whole
 
     def locate(self, column: int) -> tuple[int, int]:
-        """The system and its own column of a column of the stacked matrix."""
-        b = int(np.searchsorted(self.offsets, column, side="right") - 1)
-        return b, int(column - self.offsets[b])
+        """The system and its own column of a column of the stacked matrix (fc_chol_batch_locate)."""
+        import ctypes as C
+        from . import _lib
+        b, local = C.c_int32(0), C.c_int64(0)
+        rc = _lib.load().fc_chol_batch_locate(len(self.sizes), _lib.ptr(self.offsets), int(column), C.byref(b),
+                                              C.byref(local))
+        if rc != 0:
+            raise ValueError(f"column {column} is outside the batch")
+        return int(b.value), int(local.value)
 
     def factor(self, values: list[np.ndarray]):
         """New values for every system (each in its UpperColumns order). A failing pivot raises

@@ -152,6 +152,29 @@ class Symbolic:
         self.handle = h
         self.n = a.n
 
+    @staticmethod
+    def batch(parts: list[UpperColumns], max_entries: int) -> tuple["Symbolic", np.ndarray]:
+        """The analysis of independent systems as one block-diagonal matrix (fc_chol_batch_analyse):
+        (the Symbolic, each system's first unknown with the total last)."""
+        lib = _lib.load()
+        count = len(parts)
+        ns = np.array([p.n for p in parts], np.int64)
+        ptrs = [np.ascontiguousarray(p.ptr, np.int64) for p in parts]
+        idxs = [np.ascontiguousarray(p.idx, np.int32) for p in parts]
+        P = (C.c_void_p * max(count, 1))(*[C.c_void_p(a.ctypes.data) for a in ptrs])
+        I = (C.c_void_p * max(count, 1))(*[C.c_void_p(a.ctypes.data) for a in idxs])  # noqa: E741
+        offsets = np.zeros(count + 1, np.int64)
+        st = Status()
+        h = C.c_void_p()
+        lib.fc_chol_batch_analyse(count, _lib.ptr(ns), P, I, min(int(max_entries), 2**64 - 1), C.byref(h),
+                                  _lib.ptr(offsets), C.byref(st))
+        raise_for(st)
+        sym = Symbolic.__new__(Symbolic)
+        sym.handle = h
+        sym.n = int(offsets[-1]) if count else 0
+        sym._keep = (ptrs, idxs)
+        return sym, offsets
+
     def arrays(self) -> dict:
         """Copies of the analysis' arrays (fc_symbolic_arrays)."""
         lib = _lib.load()

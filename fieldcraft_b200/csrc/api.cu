@@ -2514,6 +2514,50 @@ int fc_symbolic_analyse(int64_t n, const int64_t *ptr, const int32_t *idx, uint6
   return FC_OK;
 }
 
+int fc_chol_batch_analyse(int32_t count, const int64_t *n, const int64_t *const *ptr, const int32_t *const *idx,
+                          uint64_t max_entries, fc_symbolic **out, int64_t *offsets, fc_status *status) {
+  if (!out || count < 0 || (count > 0 && (!n || !ptr || !idx || !offsets))) {
+    set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "null or negative argument");
+    return FC_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  try {
+    // diag(A_0, A_1, ...) by columns: each system's columns shifted by its first unknown
+    std::vector<int64_t> bptr(1, 0);
+    std::vector<int32_t> bidx;
+    int64_t at = 0;
+    for (int32_t b = 0; b < count; ++b) {
+      if (n[b] < 0 || (n[b] > 0 && (!ptr[b] || !idx[b]))) {
+        set_status(status, FC_INVALID_ARGUMENT, -1, 0, 0, "system " + std::to_string(b) + ": bad pattern");
+        return FC_INVALID_ARGUMENT;
+      }
+      offsets[b] = at;
+      if (at + n[b] > INT32_MAX) {
+        set_status(status, FC_TOO_LARGE, -1, 0, 0, "the batch has more than 2^31 unknowns");
+        return FC_TOO_LARGE;
+      }
+      for (int64_t k = 0; k < n[b]; ++k) {
+        for (int64_t q = ptr[b][k]; q < ptr[b][k + 1]; ++q) bidx.push_back((int32_t)(idx[b][q] + at));
+        bptr.push_back((int64_t)bidx.size());
+      }
+      at += n[b];
+    }
+    if (count > 0) offsets[count] = at;
+    return fc_symbolic_analyse(at, bptr.data(), bidx.data(), max_entries, out, status);
+  } catch (const std::bad_alloc &) {
+    set_status(status, FC_OUT_OF_MEMORY, -1, 0, 0, "host memory for the batch's analysis");
+    return FC_OUT_OF_MEMORY;
+  }
+}
+
+int fc_chol_batch_locate(int32_t count, const int64_t *offsets, int64_t column, int32_t *system, int64_t *local) {
+  if (count < 1 || !offsets || !system || !local || column < 0 || column >= offsets[count]) return FC_INVALID_ARGUMENT;
+  const int64_t *hit = std::upper_bound(offsets, offsets + count + 1, column) - 1;
+  *system = (int32_t)(hit - offsets);
+  *local = column - *hit;
+  return FC_OK;
+}
+
 void fc_symbolic_free(fc_symbolic *sym) { delete sym; }
 
 int fc_symbolic_get(const fc_symbolic *sym, fc_symbolic_arrays *o) {

@@ -67,6 +67,19 @@ int fc_symbolic_analyse(int64_t n, const int64_t *ptr, const int32_t *idx, uint6
                         fc_symbolic **out, fc_status *status);
 void fc_symbolic_free(fc_symbolic *sym);
 
+/* Batches (no reference counterpart; the reference factors one system at a time): `count`
+ * independent systems, system b's upper triangle by columns in n[b], ptr[b], idx[b], analysed as
+ * the one block-diagonal matrix diag(A_0, A_1, ...). Its elimination forest is the union of the
+ * systems' trees, so no supernode spans two systems, and one handle made from the result
+ * (fc_chol_create) factors and solves every system in the same launches: values and right-hand
+ * sides end to end, system b's unknowns from offsets[b] (offsets[count + 1] is filled; the last is
+ * the total). FC_TOO_LARGE when the whole batch's factor would pass max_entries. */
+int fc_chol_batch_analyse(int32_t count, const int64_t *n, const int64_t *const *ptr, const int32_t *const *idx,
+                          uint64_t max_entries, fc_symbolic **out, int64_t *offsets, fc_status *status);
+/* A column of the batch (a failing pivot's, FC_NOT_POSITIVE_DEFINITE) as its system and that
+ * system's own column. */
+int fc_chol_batch_locate(int32_t count, const int64_t *offsets, int64_t column, int32_t *system, int64_t *local);
+
 /* The arrays of the reference's Symbolic, for a caller that ran its own analysis (the Rust
  * side) or wants to check this one. Field meanings follow cholesky.rs:385-415, 728-737,
  * 1195-1207; the update lists are by target supernode in CSR form. */

@@ -42,3 +42,32 @@ def test_factor_cost_is_the_sum_of_squared_column_counts():
         m, w = rptr[k + 1] - rptr[k], first[k + 1] - first[k]
         want += sum(float(m - c) ** 2 for c in range(w))
     assert factor_cost(p) == want
+
+
+def test_batch_abi_is_the_block_diagonal_analysis():
+    """fc_chol_batch_analyse gives the analysis of diag(A_0, A_1, ...) array for array, with each
+    system's first unknown; fc_chol_batch_locate maps a batch column back to (system, column)."""
+    import ctypes as C
+
+    from fieldcraft_b200 import Symbolic, _lib, problems
+    from fieldcraft_b200.batch import block_diagonal
+    boxes = list(problems.uneven_boxes(count=7, lo=2, hi=6, nrhs=1, seed=13))
+    parts = [b.upper() for b in boxes]
+    sym, offsets = Symbolic.batch(parts, 2**62)
+    ref = Symbolic(block_diagonal(parts), 2**62)
+    a, b = sym.arrays(), ref.arrays()
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+    assert offsets.tolist() == [0] + np.cumsum([p.n for p in parts]).tolist()
+    lib = _lib.load()
+    for col in (0, offsets[3] - 1, offsets[3], offsets[-1] - 1):
+        s, loc = C.c_int32(0), C.c_int64(0)
+        assert lib.fc_chol_batch_locate(len(parts), _lib.ptr(offsets), int(col), C.byref(s), C.byref(loc)) == 0
+        assert offsets[s.value] + loc.value == col and 0 <= loc.value < parts[s.value].n
+    assert lib.fc_chol_batch_locate(len(parts), _lib.ptr(offsets), int(offsets[-1]), C.byref(s), C.byref(loc)) != 0
+    # the whole batch refused before any numeric memory, as one system would be
+    from fieldcraft_b200 import TooLarge
+    import pytest
+    with pytest.raises(TooLarge):
+        Symbolic.batch(parts, 10)
