@@ -156,6 +156,7 @@ struct fc_chol {
   bool dag_plant = false;                 // test hook: the next plan holds a dependency nothing meets
   int64_t last_factor_launches = 0, last_solve_launches = 0;
   double gemm_flops_factor = 0, gemm_flops_solve = 0;
+  double gemm_flops_updates = 0;  // the factor's K_GEMM launches alone (the inverse doubling apart)
   int64_t gemm_big_ordinal = -1, gemm_trail_ordinal = -1;  // the factor's heaviest GEMM launches
   // per-launch event timing (fc_chol_profile)
   bool profiling = false;
@@ -702,6 +703,10 @@ int plan_factor_upload(fc_chol *h, fc_status *st) {
   h->gemm_tasks = (int64_t)(gemm_t.size() + tc_t.size());
   h->gemm_flops_factor = 0;
   for (const auto &g : gemm_t) h->gemm_flops_factor += task_flops(g);
+  h->gemm_flops_updates = 0;
+  for (const Launch &l : h->program)
+    if (l.kind == K_GEMM)
+      for (int64_t q = l.off; q < l.off + l.count; ++q) h->gemm_flops_updates += task_flops(gemm_t[q]);
   for (const auto &g : tc_t) {
     double outputs = (double)g.M * g.N;
     if (g.flags & 1) {
@@ -3325,6 +3330,7 @@ int64_t fc_chol_stat(const fc_chol *h, int what) {
     case 12: return h->gemm_trail_ordinal;
     case 13: return h->dag ? h->dag_fwd : 0;
     case 14: return h->dag ? h->dag_bwd : 0;
+    case 15: return (int64_t)h->gemm_flops_updates;
   }
   return -1;
 }

@@ -1309,17 +1309,9 @@ __global__ void pack_kernel(Tree t, const int64_t *__restrict__ toff, double *__
   }
 }
 
-// Every kernel of the factorisation and the solve asks for the same split of the SM's L1 and
-// shared memory (all of it shared): consecutive launches with different preferred splits make an
-// SM reconfigure between them, which it can only do once it has drained.
-template <class K>
-void max_shared(K kernel) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
-}
 template <class K>
 void set_smem(K kernel, size_t bytes) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  max_shared(kernel);
 }
 
 }  // namespace
@@ -1334,13 +1326,6 @@ void configure_kernels() {
   set_smem(gemm_cluster_kernel<double>, gemm_smem<double>());
   set_smem(gemm_cluster_kernel<float>, gemm_smem<float>());
   set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
-  max_shared(assemble_kernel<double>);
-  max_shared(assemble_kernel<float>);
-  max_shared(thin_fwd_kernel<double>);
-  max_shared(thin_fwd_kernel<float>);
-  max_shared(thin_bwd_kernel<double>);
-  max_shared(thin_bwd_kernel<float>);
-  max_shared(solve_assemble_kernel);
   configure_solve_dag();
   done = true;
 }

@@ -54,6 +54,11 @@ __global__ void copy_kernel(int64_t n, const double *__restrict__ a, double *__r
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = a[i];
 }
+// t = b - t (t holds A x)
+__global__ void residual_from_kernel(int64_t n, const double *__restrict__ b, double *__restrict__ t) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    t[i] = b[i] - t[i];
+}
 __global__ void residual_inplace_kernel(int64_t n, const double *__restrict__ b, double *__restrict__ r) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     r[i] = b[i] - r[i];
@@ -582,6 +587,8 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
   // solve (the block-Jacobi part, when set, stays; the kept directions stay A-orthogonal, so FCG
   // goes on with them).
   constexpr int SAFE_WINDOW = 25;
+  constexpr int MAX_REPLACEMENTS = 8;  // residual replacements at most (see below)
+  int replacements = 0;
   constexpr double SAFE_DROP = 0.25;
   bool use_net = net != nullptr && net->net_on;
   std::vector<double> history;
@@ -636,6 +643,24 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
     stored = std::min(stored + 1, ring);
     converged = rr <= target;
     if (!(rr == rr)) break;  // NaN: give up on FCG
+    if (converged && replacements < MAX_REPLACEMENTS) {
+      // the recurrence says converged: check b - A x itself; when rounding has let the two drift
+      // apart, go on from the true residual (the kept directions restart)
+      fc::launch_spmv(n, d_ptr, d_idx, d_val, d_x, n, tmp, n, 1, st);
+      residual_from_kernel<<<blocks(n), 256, 0, st>>>(n, d_b, tmp);
+      const double *a[1] = {tmp}, *b2[1] = {tmp};
+      fc::unet::dots(n, 1, a, b2, part.as<double>(), s + 5, st);
+      double tr = 0.0;
+      cudaMemcpyAsync(&tr, s + 5, sizeof(double), cudaMemcpyDeviceToHost, st);
+      e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return cuda_fail(status, e, "FCG");
+      if (!(tr <= target)) {
+        copy_kernel<<<blocks(n), 256, 0, st>>>(n, tmp, r);
+        stored = 0;
+        converged = false;
+        ++replacements;
+      }
+    }
     history.push_back(rr);
     if (use_net) {
       net->last_net_iterations = it;

@@ -192,7 +192,8 @@ int fc_chol_refine_solve_device(fc_chol *h, const int64_t *d_ptr, const int32_t 
  * the factor's GEMM tasks, 10 flops of the last solve plan's GEMM tasks, 11 the ordinal among the
  * factor's GEMM launches of the one with the most flops, 12 the same among the launches whose
  * tasks all have K <= 64 (the panels' updates of later columns), 13 and 14 the tasks of the
- * persistent solve's forward and backward lists. */
+ * persistent solve's forward and backward lists, 15 flops of the factor's update GEMM launches
+ * alone (9 without the diagonal blocks' inverse doubling). */
 int64_t fc_chol_stat(const fc_chol *h, int what);
 
 /* Execution options of a handle (no reference counterpart). Each takes effect from the next solve.

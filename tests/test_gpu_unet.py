@@ -7,7 +7,7 @@ some BF16 roundings by one unit: outputs agree to 2e-2 of their largest entry, e
 gradients to 2e-2 in norm (and every entry to 0.1 of the layer's largest); the first two layers'
 gradients, which carry the rounding of every layer above them, to 5e-2 in norm. A deeper network
 puts four more BF16-rounded layers on the gradients' path per level: its norm tolerances are
-1 + 2 (levels - 3) times these, its largest-entry tolerance 1 + 0.5 (levels - 3) times."""
+1 + 2.5 (levels - 3) times these, its largest-entry tolerance 1 + 0.5 (levels - 3) times."""
 import numpy as np
 import pytest
 
@@ -56,10 +56,11 @@ def test_forward_and_backward_match_the_oracle(cuda, levels):
         off += nw + cout
     # the first layers' gradients pass through every layer, and each level beyond three adds four
     # BF16-rounded layers on the way: the tolerances grow with the depth
-    deep, top_deep = 1.0 + 2.0 * (levels - 3), 1.0 + 0.5 * (levels - 3)
+    deep, top_deep = 1.0 + 2.5 * (levels - 3), 1.0 + 0.5 * (levels - 3)
+    worst = sorted(errs, key=lambda e: -e[2])[:8]
     for l, name, rel, top in errs:
         tol = (TOL if l >= 2 else 2.5 * TOL) * deep
-        assert rel <= tol and top <= 0.1 * top_deep, errs
+        assert rel <= tol and top <= 0.1 * top_deep, [(a, b, round(float(c), 4), round(float(d), 4)) for a, b, c, d in worst]
 
 
 def test_training_and_fcg_gain_over_plain_cg(cuda):
