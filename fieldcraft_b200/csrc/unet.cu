@@ -149,6 +149,7 @@ struct fc_unet {
   DeviceBuf bj;              // nodal block-Jacobi inverses (9 doubles a node), added to the output
   bool has_bj = false;
   bool net_on = true;         // false: the preconditioner is the block-Jacobi part alone
+  bool safeguard = true;      // FCG drops a stalling network (fc_unet_enable 2: it never does)
   int64_t last_net_iterations = 0, last_dropped = 0;
   bool weights_stale = true;
   std::mutex lock;
@@ -412,9 +413,10 @@ int fc_unet_set_operator(fc_unet *u, const int64_t *d_ptr, const int32_t *d_idx,
 }
 
 int fc_unet_enable(fc_unet *u, int32_t on) {
-  if (!u || (!on && !u->has_bj)) return FC_INVALID_ARGUMENT;
+  if (!u || on < 0 || on > 2 || (!on && !u->has_bj)) return FC_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> g(u->lock);
   u->net_on = on != 0;
+  u->safeguard = on != 2;
   return FC_OK;
 }
 
@@ -665,7 +667,7 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
     if (use_net) {
       net->last_net_iterations = it;
       const size_t h = history.size();
-      if (h >= 2 * SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
+      if (net->safeguard && h >= 2 * SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
         use_net = false;
         net->last_dropped = 1;
       }

@@ -56,9 +56,11 @@ class UNet:
         if rc != 0:
             raise ValueError(f"fc_unet_set_operator ({rc})")
 
-    def enable(self, on: bool):
-        """False: the preconditioner is the block-Jacobi part alone (the network is not run)."""
-        if _lib.load().fc_unet_enable(self.handle, int(bool(on))) != 0:
+    def enable(self, on, safeguard: bool = True):
+        """False: the preconditioner is the block-Jacobi part alone (the network is not run);
+        True: B r + net(r), FCG's safeguard on unless `safeguard` is False."""
+        code = 0 if not on else (1 if safeguard else 2)
+        if _lib.load().fc_unet_enable(self.handle, code) != 0:
             raise ValueError("fc_unet_enable needs the operator set")
 
     def stat(self, what: int) -> int:

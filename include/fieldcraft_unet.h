@@ -47,7 +47,7 @@ void fc_unet_destroy(fc_unet *net);
  * be a multiple of 3). d_ptr null removes it. FC_NOT_POSITIVE_DEFINITE when a 3 x 3 block is not. */
 int fc_unet_set_operator(fc_unet *net, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val);
 /* on = 0: the preconditioner is the block-Jacobi part alone (the network is not run; needs the
- * operator set); on = 1 (the default): B r + net(r). */
+ * operator set); on = 1 (the default): B r + net(r); on = 2: the same without FCG's safeguard. */
 int fc_unet_enable(fc_unet *net, int32_t on);
 /* The network's numbers: 0 levels, 1 iterations of the last fc_fcg_solve that used the network,
  * 2 whether its safeguard dropped the network, 3 whether the block-Jacobi part is set. */
