@@ -439,12 +439,16 @@ __global__ void axpy_dev_kernel(int64_t n, const double *__restrict__ alpha, dou
 
 struct DirPtrs {
   const double *p[MAX_PAIRS];
+  int slot[MAX_PAIRS];  // where each direction's denominator p_j.q_j is kept
 };
 __global__ void fcg_direction_kernel(int64_t n, int m, const double *__restrict__ z, DirPtrs pj,
                                      const double *__restrict__ num, const double *__restrict__ den,
                                      double *__restrict__ p) {
   double beta[MAX_PAIRS];
-  for (int j = 0; j < m; ++j) beta[j] = den[j] != 0.0 ? num[j] / den[j] : 0.0;
+  for (int j = 0; j < m; ++j) {
+    const double d = den[pj.slot[j]];
+    beta[j] = d != 0.0 ? num[j] / d : 0.0;
+  }
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double v = z[i];
     for (int j = 0; j < m; ++j) v -= beta[j] * pj.p[j][i];
@@ -587,11 +591,27 @@ void axpy_dev(int64_t n, const double *alpha, double sign, const double *x, doub
   axpy_dev_kernel<<<grid_for(n), 256, 0, st>>>(n, alpha, sign, x, y);
 }
 
-void fcg_direction(int64_t n, int m, const double *z, const double *const *pj, const double *num, const double *den,
-                   double *p, cudaStream_t st) {
+void fcg_direction(int64_t n, int m, const double *z, const double *const *pj, const int *slot, const double *num,
+                   const double *den, double *p, cudaStream_t st) {
   DirPtrs dp{};
-  for (int j = 0; j < m && j < MAX_PAIRS; ++j) dp.p[j] = pj[j];
+  for (int j = 0; j < m && j < MAX_PAIRS; ++j) dp.p[j] = pj[j], dp.slot[j] = slot[j];
   fcg_direction_kernel<<<grid_for(n), 256, 0, st>>>(n, m, z, dp, num, den, p);
+}
+
+// alpha = s[0] / s[1] (p.r / p.q; 0 when p.q is 0), kept: *den = s[1]; x += alpha p; r -= alpha q
+__global__ void fcg_update_kernel(int64_t n, const double *__restrict__ s, double *__restrict__ den,
+                                  const double *__restrict__ p, const double *__restrict__ q, double *__restrict__ x,
+                                  double *__restrict__ r) {
+  const double alpha = s[1] != 0.0 ? s[0] / s[1] : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *den = s[1];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    r[i] -= alpha * q[i];
+  }
+}
+void fcg_update(int64_t n, const double *s, double *den, const double *p, const double *q, double *x, double *r,
+                cudaStream_t st) {
+  fcg_update_kernel<<<grid_for(n), 256, 0, st>>>(n, s, den, p, q, x, r);
 }
 
 void input_scales(int64_t n, const double *nrm2, double kref, double *s, cudaStream_t st) {

@@ -71,9 +71,13 @@ void dots(int64_t n, int pairs, const double *const *a, const double *const *b, 
           cudaStream_t st);
 // y += alpha[0] * x (alpha on the device, sign s: y += s alpha x)
 void axpy_dev(int64_t n, const double *alpha, double sign, const double *x, double *y, cudaStream_t st);
-// p = z - sum_j beta_j p_j with beta_j = num[j] / den[j] (device scalars), q = A p done by the caller
-void fcg_direction(int64_t n, int m, const double *z, const double *const *pj, const double *num, const double *den,
-                   double *p, cudaStream_t st);
+// p = z - sum_j beta_j p_j with beta_j = num[j] / den[slot[j]] (device scalars), q = A p done by
+// the caller
+void fcg_direction(int64_t n, int m, const double *z, const double *const *pj, const int *slot, const double *num,
+                   const double *den, double *p, cudaStream_t st);
+// alpha = s[0] / s[1] (0 when s[1] is 0), *den = s[1], x += alpha p, r -= alpha q
+void fcg_update(int64_t n, const double *s, double *den, const double *p, const double *q, double *x, double *r,
+                cudaStream_t st);
 // The norms' scalars for the input scaling of the network: s[0] = sqrt(n) / ||r||,
 // s[1] = ||r|| / (sqrt(n) kref); nrm2 = ||r||^2 from dots.
 void input_scales(int64_t n, const double *nrm2, double kref, double *s, cudaStream_t st);

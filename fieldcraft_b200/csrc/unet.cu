@@ -46,10 +46,6 @@ __global__ void loss_grad_kernel(int64_t n, const double *__restrict__ s, double
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     d[i] *= c;
 }
-// alpha = s[0] / s[1] (p.r / p.q)
-__global__ void ratio_kernel(const double *__restrict__ s, double *__restrict__ alpha) {
-  alpha[0] = s[1] != 0.0 ? s[0] / s[1] : 0.0;
-}
 __global__ void copy_kernel(int64_t n, const double *__restrict__ a, double *__restrict__ b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = a[i];
@@ -570,7 +566,9 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
   double *r = vec.as<double>(), *z = r + n, *tmp = z + n;
   std::vector<double *> P(ring), Q(ring);
   for (int j = 0; j < ring; ++j) P[j] = tmp + n * (1 + 2 * j), Q[j] = P[j] + n;
-  double *s = sc.as<double>();  // [0] b.b [1] r.r [2] p.r [3] p.q [4] alpha [8..8+ring) z.q_j [16..16+ring) p_j.q_j
+  // [0] b.b [1] r.r [2] p.r [3] p.q [5] b - A x squared [8..8+ring) z.q_j [16..16+ring) p_j.q_j
+  // [32..32+CHECK) the last iterations' r.r
+  double *s = sc.as<double>();
   cudaMemsetAsync(d_x, 0, sizeof(double) * n, st);
   copy_kernel<<<blocks(n), 256, 0, st>>>(n, d_b, r);
   {
@@ -595,6 +593,12 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
   bool use_net = net != nullptr && net->net_on;
   std::vector<double> history;
   if (net) net->last_dropped = 0, net->last_net_iterations = 0;
+  // ||r||^2 of each iteration lands in a ring of device scalars (s + 32 + it % CHECK); the host
+  // reads them every CHECK iterations (one synchronisation per CHECK iterations), then decides on
+  // convergence, the safeguard and a residual replacement in iteration order.
+  constexpr int CHECK = 8;
+  int since = 0;
+  double ring_rr[CHECK];
   while (!converged && it < max_iter) {
     // z = M(r)
     if (use_net)
@@ -603,7 +607,8 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
       apply_jacobi(net, r, z);
     else
       copy_kernel<<<blocks(n), 256, 0, st>>>(n, r, z);
-    // p = z - sum_j (z.q_j / p_j.q_j) p_j over the stored directions
+    // p = z - sum_j (z.q_j / p_j.q_j) p_j over the stored directions (the denominators were kept
+    // in s + 16 + slot when each direction was made)
     double *p = P[it % ring], *q = Q[it % ring];
     const int m = std::min(stored, ring);
     std::vector<const double *> pj, qj, zz;
@@ -618,10 +623,7 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
     }
     if (!slot.empty()) {
       fc::unet::dots(n, (int)slot.size(), zz.data(), qj.data(), part.as<double>(), s + 8, st);
-      // the denominators p_j.q_j were kept when each direction was made
-      for (size_t j = 0; j < slot.size(); ++j)
-        cudaMemcpyAsync(s + 24 + j, s + 16 + slot[j], sizeof(double), cudaMemcpyDeviceToDevice, st);
-      fc::unet::fcg_direction(n, (int)slot.size(), z, pj.data(), s + 8, s + 24, p, st);
+      fc::unet::fcg_direction(n, (int)slot.size(), z, pj.data(), slot.data(), s + 8, s + 16, p, st);
     } else {
       copy_kernel<<<blocks(n), 256, 0, st>>>(n, z, p);
     }
@@ -630,21 +632,38 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
       const double *a[2] = {p, p}, *b[2] = {r, q};
       fc::unet::dots(n, 2, a, b, part.as<double>(), s + 2, st);
     }
-    cudaMemcpyAsync(s + 16 + (it % ring), s + 3, sizeof(double), cudaMemcpyDeviceToDevice, st);
-    ratio_kernel<<<1, 1, 0, st>>>(s + 2, s + 4);
-    fc::unet::axpy_dev(n, s + 4, 1.0, p, d_x, st);
-    fc::unet::axpy_dev(n, s + 4, -1.0, q, r, st);
+    // alpha = p.r / p.q (kept as this direction's denominator), x += alpha p, r -= alpha q
+    fc::unet::fcg_update(n, s + 2, s + 16 + (it % ring), p, q, d_x, r, st);
     {
       const double *a[1] = {r}, *b[1] = {r};
-      fc::unet::dots(n, 1, a, b, part.as<double>(), s + 1, st);
+      fc::unet::dots(n, 1, a, b, part.as<double>(), s + 32 + (it % CHECK), st);
     }
-    cudaMemcpyAsync(&rr, s + 1, sizeof(double), cudaMemcpyDeviceToHost, st);
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_fail(status, e, "FCG");
     ++it;
     stored = std::min(stored + 1, ring);
-    converged = rr <= target;
-    if (!(rr == rr)) break;  // NaN: give up on FCG
+    if (++since < CHECK && it < max_iter) continue;
+    cudaMemcpyAsync(ring_rr, s + 32, sizeof(double) * CHECK, cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(status, e, "FCG");
+    bool nan = false;
+    for (int k = it - since; k < it && !converged; ++k) {
+      rr = ring_rr[k % CHECK];
+      if (!(rr == rr)) {
+        nan = true;
+        break;
+      }
+      converged = rr <= target;
+      history.push_back(rr);
+      if (use_net) {
+        net->last_net_iterations = k + 1;
+        const size_t h = history.size();
+        if (net->safeguard && h >= 2 * SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
+          use_net = false;
+          net->last_dropped = 1;
+        }
+      }
+    }
+    since = 0;
+    if (nan) break;  // NaN: give up on FCG
     if (converged && replacements < MAX_REPLACEMENTS) {
       // the recurrence says converged: check b - A x itself; when rounding has let the two drift
       // apart, go on from the true residual (the kept directions restart)
@@ -661,15 +680,6 @@ int fc_fcg_solve(fc_unet *net, fc_chol *fallback, int64_t n, const int64_t *d_pt
         stored = 0;
         converged = false;
         ++replacements;
-      }
-    }
-    history.push_back(rr);
-    if (use_net) {
-      net->last_net_iterations = it;
-      const size_t h = history.size();
-      if (net->safeguard && h >= 2 * SAFE_WINDOW && rr > SAFE_DROP * history[h - 1 - SAFE_WINDOW]) {
-        use_net = false;
-        net->last_dropped = 1;
       }
     }
   }
