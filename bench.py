@@ -706,10 +706,11 @@ def hbm_peak() -> tuple:
         return 6650.0, "fallback 6.65 TB/s (no measured peaks file)"
 
 
-def recorded_traffic(kernel: str, n_el: int):
-    """DRAM bytes per launch of `kernel` from the ncu capture recorded in profiles/traffic.json,
-    used only while the kernel's source is the one captured (its SHA-256 recorded beside the
-    figure); otherwise None and why."""
+def recorded_traffic(kernel: str, flops_per_launch: float):
+    """DRAM bytes per launch of `kernel`: the DRAM bytes per useful flop of an ncu capture of a
+    small case recorded in profiles/traffic.json, times this run's useful flops per launch. Used
+    only while the kernel's source is the one captured (its SHA-256 recorded beside the figure);
+    otherwise None and why."""
     import hashlib
     rec_file = ROOT / "profiles" / "traffic.json"
     try:
@@ -720,9 +721,7 @@ def recorded_traffic(kernel: str, n_el: int):
     sha = hashlib.sha256(src.read_bytes()).hexdigest() if src.exists() else None
     if sha != rec["source_sha256"]:
         return None, f"the recorded ncu capture was of another build of {rec['source']}"
-    if rec.get("n_el") not in (None, n_el):
-        return None, "the recorded capture is scaled to another workload size"
-    return int(rec["bytes_per_launch"]), rec["how"]
+    return int(rec["bytes_per_useful_flop"] * flops_per_launch), f"{rec['case']}; {rec['how']}"
 
 
 def stream_time(torch, stream, fn, reps: int = 5, warm: int = 2) -> float:
@@ -969,7 +968,7 @@ def main():
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12
     factor_ms = float(ms_k[0:4].sum() + ms_k[10:13].sum() + ms_k[15])
     solve_ms = float(ms_k[16:32].sum())
-    traffic, traffic_note = recorded_traffic("gemm_kernel", args.n_el)
+    traffic, traffic_note = recorded_traffic("gemm_kernel", gemm_flops / max(1, int(cnt_k[3])))
     # the solve and the residual product alone, on the same stream (graph replay, CUDA events)
     solve_graph_ms = stream_time(torch, stream, lambda: solve_only(lib, f, d_x, d_f, R, n, stream), reps=5)
     spmv_ms = stream_time(torch, stream, lambda: lib.fc_csr_spmv_device(

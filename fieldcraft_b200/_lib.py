@@ -95,6 +95,7 @@ SIGNATURES = {
     "fc_unet_set_operator": (i32, [P, P, P, P]),
     "fc_unet_stat": (i64, [P, i32]),
     "fc_unet_enable": (i32, [P, i32]),
+    "fc_unet_set_odd": (i32, [P, i32]),
     "fc_unet_train_batch": (i32, [P, P, P, i32, i64, P, P, P, C.c_float, i32, P]),
     "fc_fcg_solve": (i32, [P, P, i64, P, P, P, P, P, f64, i32, i32, C.POINTER(i32), C.POINTER(f64), C.POINTER(i32),
                            C.POINTER(Status)]),

@@ -114,6 +114,20 @@ __global__ void add_scalar_kernel(const double *__restrict__ a, double *__restri
   acc[0] = first ? a[0] : acc[0] + a[0];
 }
 
+// the odd network's two passes: P = (s0, s1 / 2), M = (-s0, -s1 / 2) from s = (s0, s1)
+__global__ void odd_scales_kernel(const double *__restrict__ s, double *__restrict__ P, double *__restrict__ M) {
+  P[0] = s[0], P[1] = 0.5 * s[1];
+  M[0] = -s[0], M[1] = -0.5 * s[1];
+}
+__global__ void add_kernel(int64_t n, const double *__restrict__ a, double *__restrict__ z) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] += a[i];
+}
+__global__ void add_f32_kernel(int64_t n, const float *__restrict__ a, float *__restrict__ z) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] += a[i];
+}
+
 int blocks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
 Grid coarser(const Grid &g) { return Grid{(g.X + 1) / 2, (g.Y + 1) / 2, (g.Z + 1) / 2}; }
@@ -146,6 +160,10 @@ struct fc_unet {
   bool has_bj = false;
   bool net_on = true;         // false: the preconditioner is the block-Jacobi part alone
   bool safeguard = true;      // FCG drops a stalling network (fc_unet_enable 2: it never does)
+  // odd: M(r) = B r + (net(r) - net(-r)) / 2, so that M(-r) = -M(r) and M(0) = 0 (a part of the
+  // output that does not depend on r, from the biases and the modulus channel, cancels)
+  bool odd = true;
+  DeviceBuf tz2, gtmp;        // the second pass's output and gradients
   int64_t last_net_iterations = 0, last_dropped = 0;
   bool weights_stale = true;
   std::mutex lock;
@@ -242,16 +260,31 @@ void backward(fc_unet *u) {
 
 double *scal(fc_unet *u, int k) { return u->scal.as<double>() + k; }
 
-// z = M(r) on u's stream
+// z = M(r) on u's stream. The odd network runs twice, on +r then on -r (the second pass's
+// activations stay for a backward pass: scales at scal 12..13, the first's at 10..11).
 void apply(fc_unet *u, const double *r, double *z) {
   cudaStream_t st = u->stream;
   const double *a[1] = {r}, *b[1] = {r};
+  const int64_t *eq = u->eq.as<int64_t>();
   fc::unet::dots(u->n, 1, a, b, u->dotpart.as<double>(), scal(u, 2), st);
   fc::unet::input_scales(u->n, scal(u, 2), u->kref, scal(u, 0), st);
-  fc::unet::scatter_input(u->g[0], u->eq.as<int64_t>(), r, u->feat.as<float>(), scal(u, 0), B(u->x), st);
-  forward(u);
   cudaMemsetAsync(z, 0, sizeof(double) * (size_t)u->n, st);
-  fc::unet::gather_output(u->g[0], u->eq.as<int64_t>(), B(u->y), scal(u, 0), z, st);
+  if (u->odd) {
+    odd_scales_kernel<<<1, 1, 0, st>>>(scal(u, 0), scal(u, 10), scal(u, 12));
+    fc::unet::scatter_input(u->g[0], eq, r, u->feat.as<float>(), scal(u, 10), B(u->x), st);
+    forward(u);
+    fc::unet::gather_output(u->g[0], eq, B(u->y), scal(u, 10), z, st);
+    double *z2 = u->tz2.as<double>();
+    cudaMemsetAsync(z2, 0, sizeof(double) * (size_t)u->n, st);
+    fc::unet::scatter_input(u->g[0], eq, r, u->feat.as<float>(), scal(u, 12), B(u->x), st);
+    forward(u);
+    fc::unet::gather_output(u->g[0], eq, B(u->y), scal(u, 12), z2, st);
+    add_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, z2, z);
+  } else {
+    fc::unet::scatter_input(u->g[0], eq, r, u->feat.as<float>(), scal(u, 0), B(u->x), st);
+    forward(u);
+    fc::unet::gather_output(u->g[0], eq, B(u->y), scal(u, 0), z, st);
+  }
   if (u->has_bj) block_jacobi_add_kernel<<<blocks(u->n / 3), 256, 0, st>>>(u->n / 3, u->bj.as<double>(), r, z);
 }
 
@@ -280,8 +313,22 @@ void pair_gradient(fc_unet *u, const double *d_r, const double *d_e, const int64
     fc::unet::dots(u->n, 2, a, b, u->dotpart.as<double>(), scal(u, 4), st);
     loss_grad_kernel<<<blocks(u->n), 256, 0, st>>>(u->n, scal(u, 4), d, d_loss);
   }
-  fc::unet::scatter_grad(u->g[0], u->eq.as<int64_t>(), d, scal(u, 0), B(u->dy), st);
+  const int64_t *eq = u->eq.as<int64_t>();
+  if (!u->odd) {
+    fc::unet::scatter_grad(u->g[0], eq, d, scal(u, 0), B(u->dy), st);
+    backward(u);
+    return;
+  }
+  // the second pass (-r) is the one whose activations are live: its gradients first, kept aside;
+  // then the first pass (+r) again, forward and backward, and the two added
+  fc::unet::scatter_grad(u->g[0], eq, d, scal(u, 12), B(u->dy), st);
   backward(u);
+  cudaMemcpyAsync(u->gtmp.p, u->grad.p, sizeof(float) * (size_t)u->params, cudaMemcpyDeviceToDevice, st);
+  fc::unet::scatter_input(u->g[0], eq, d_r, u->feat.as<float>(), scal(u, 10), B(u->x), st);
+  forward(u);
+  fc::unet::scatter_grad(u->g[0], eq, d, scal(u, 10), B(u->dy), st);
+  backward(u);
+  add_f32_kernel<<<blocks(u->params), 256, 0, st>>>(u->params, u->gtmp.as<float>(), u->grad.as<float>());
 }
 
 int cuda_fail(fc_status *st, cudaError_t e, const char *where) {
@@ -350,7 +397,8 @@ int fc_unet_create_levels(int32_t nx, int32_t ny, int32_t nz, int64_t n, const i
             u->feat.alloc(sizeof(float) * nodes) == cudaSuccess && u->part.alloc(sizeof(float) * part) == cudaSuccess &&
             u->scal.alloc(sizeof(double) * 64) == cudaSuccess &&
             u->dotpart.alloc(sizeof(double) * 8 * 512) == cudaSuccess &&
-            u->tz.alloc(sizeof(double) * n) == cudaSuccess && u->td.alloc(sizeof(double) * n) == cudaSuccess;
+            u->tz.alloc(sizeof(double) * n) == cudaSuccess && u->td.alloc(sizeof(double) * n) == cudaSuccess &&
+            u->tz2.alloc(sizeof(double) * n) == cudaSuccess && u->gtmp.alloc(sizeof(float) * off) == cudaSuccess;
   ok = ok && alloc_bf16(u->x, u->g[0], CIO) == cudaSuccess && alloc_bf16(u->y, u->g[0], CIO) == cudaSuccess &&
        alloc_bf16(u->dy, u->g[0], CIO) == cudaSuccess;
   for (int lv = 0; lv < levels && ok; ++lv) {
@@ -406,6 +454,13 @@ int fc_unet_set_operator(fc_unet *u, const int64_t *d_ptr, const int32_t *d_idx,
   if (cudaStreamSynchronize(u->stream) != cudaSuccess) return FC_CUDA_ERROR;
   u->has_bj = one != 0;
   return one ? FC_OK : FC_NOT_POSITIVE_DEFINITE;
+}
+
+int fc_unet_set_odd(fc_unet *u, int32_t odd) {
+  if (!u) return FC_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> g(u->lock);
+  u->odd = odd != 0;
+  return FC_OK;
 }
 
 int fc_unet_enable(fc_unet *u, int32_t on) {

@@ -63,6 +63,11 @@ class UNet:
         if _lib.load().fc_unet_enable(self.handle, code) != 0:
             raise ValueError("fc_unet_enable needs the operator set")
 
+    def set_odd(self, odd: bool):
+        """True (the default): the network part of M is (net(r) - net(-r)) / 2 (M odd in r)."""
+        if _lib.load().fc_unet_set_odd(self.handle, int(bool(odd))) != 0:
+            raise ValueError("fc_unet_set_odd")
+
     def stat(self, what: int) -> int:
         """0 levels, 1 iterations of the last FCG with the network, 2 whether its safeguard dropped
         the network, 3 whether the block-Jacobi part is set."""

@@ -46,6 +46,11 @@ void fc_unet_destroy(fc_unet *net);
  * nodal block-Jacobi part B r to the preconditioner (equations node by node, three a node: n must
  * be a multiple of 3). d_ptr null removes it. FC_NOT_POSITIVE_DEFINITE when a 3 x 3 block is not. */
 int fc_unet_set_operator(fc_unet *net, const int64_t *d_ptr, const int32_t *d_idx, const double *d_val);
+/* odd != 0 (the default): the network part of M is (net(r) - net(-r)) / 2, two passes, so that
+ * M(-r) = -M(r) and M(0) = 0 as for a linear preconditioner (a part of the output that does not
+ * depend on r, from the biases and the modulus channel, cancels; training sees the same form);
+ * odd = 0: net(r), one pass. */
+int fc_unet_set_odd(fc_unet *net, int32_t odd);
 /* on = 0: the preconditioner is the block-Jacobi part alone (the network is not run; needs the
  * operator set); on = 1 (the default): B r + net(r); on = 2: the same without FCG's safeguard. */
 int fc_unet_enable(fc_unet *net, int32_t on);
