@@ -147,6 +147,7 @@ struct fc_chol {
   // the solve's launches with few output tiles split K in chunks summed by their last CTA (default)
   // or over thread-block clusters (FC_OPTION_SOLVE_CLUSTER = 1)
   bool solve_cluster = false;
+  bool solve_narrow = true;  // the solve's products in 64 x 8 / 64 x 16 tiles for up to 16 right-hand sides
   DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
   int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
   int dag_grid = 0;
@@ -2318,6 +2319,7 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
                        const std::vector<cudaEvent_t> *events = nullptr, size_t *ev = nullptr) {
   const cudaStream_t main = h->stream;
   const fc::Tree &t = h->ldlt ? h->stree : h->tree;
+  const bool narrow = h->solve_narrow && R <= 16;  // every task's N is R then
   const bool lanes = events && ev && h->side;
   const std::vector<char> side = lanes ? beside(prog) : std::vector<char>(prog.size(), 0);
   bool forked = false;
@@ -2347,12 +2349,16 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
       case K_SOLVE_BWD:
         if (l.width == 1)
           fc::launch_gemm_cluster(b.gemm + l.off, l.count, false, st, b.part, b.tcount);
+        else if (narrow)
+          fc::launch_gemm_narrow(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount);
         else
           fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st, b.part, b.tcount);
         break;
       case K_GEMM:
         if (l.width == 1)
           fc::launch_gemm_cluster(b.gemm + l.off, l.count, h->fp32, st, b.part, b.tcount);
+        else if (narrow)
+          fc::launch_gemm_narrow(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount);
         else
           fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st, b.part,
                           b.tcount);
@@ -2855,6 +2861,11 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
     case FC_OPTION_SOLVE_CLUSTER:
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       h->solve_cluster = value == 1;
+      replan();
+      return FC_OK;
+    case FC_OPTION_SOLVE_NARROW:
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      h->solve_narrow = value == 1;
       replan();
       return FC_OK;
     case FC_OPTION_FP32_UPDATES: {

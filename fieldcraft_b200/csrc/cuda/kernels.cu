@@ -666,6 +666,148 @@ __global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *_
   gemm_epilogue<double>(tp, acc, wm, wn, g, tg, part, counters);
 }
 
+// ---- the solve's products for a few right-hand sides -------------------------------------------
+// With at most 16 right-hand sides a 64 x 64 tile spends most of its DMMA work on zero columns.
+// This kernel's tile is 64 x NW (NW = 8 or 16 columns): warp w takes rows [16 w, 16 w + 16) with
+// NW / 8 fragments of 8 columns. Its K loop is gemm_kernel's (the same stages, the same m16n8k8
+// instruction over the same K order) and a split sum's chunks are added in the same order, so every
+// element's bits are the ones gemm_kernel gives: a column's solution does not depend on how many
+// right-hand sides were solved together. B rows are NW + 4 doubles apart, so a half-warp's fragment
+// reads of 4 k-rows x 4 columns fall in distinct banks.
+template <int NW>
+__host__ __device__ constexpr int narrow_row() {
+  return NW + 4;
+}
+template <class TA, int NW>
+__host__ __device__ constexpr size_t gemm_narrow_smem() {
+  return GEMM_STAGES * GEMM_KC * (sizeof(TA) * tile_stride<TA>() + sizeof(double) * narrow_row<NW>());
+}
+
+template <class TA, int NW>
+__global__ void __launch_bounds__(GEMM_THREADS, 6) gemm_narrow_kernel(const GemmTask *__restrict__ tasks, double *part,
+                                                                      int32_t *counters) {
+  constexpr int NF = NW / 8, SA = tile_stride<TA>(), SN = narrow_row<NW>();
+  constexpr int BPER = NW * GEMM_KC / GEMM_THREADS;  // B elements per thread per stage
+  static_assert(BPER >= 1 && NW * GEMM_KC % GEMM_THREADS == 0, "narrow tile");
+  extern __shared__ __align__(16) double gsm[];
+  double(*Bs)[GEMM_KC][SN] = reinterpret_cast<double(*)[GEMM_KC][SN]>(gsm);
+  TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + GEMM_STAGES * GEMM_KC * SN);
+  const GemmTask *tp = tasks + blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tg = lane & 3;
+  const int wm = warp * 16;
+  const int K = tp->K, N = tp->N;
+  const bool gather = tp->flags & 16;
+  const TA *abase = static_cast<const TA *>(tp->A);
+  const double *bbase = static_cast<const double *>(tp->B);
+  const int64_t bsj = tp->b_sj, bsk = tp->b_sk;
+  const int32_t *brows = tp->b_rows;
+  TileLoader<TA, GEMM_KC> la;
+  la.init(abase, tp->a_si, tp->a_sk, tp->M, tid);
+  // B element (k, j) at B + k b_sk + j b_sj (through the row list: B + rows[k] b_sk + j, b_sj = 1);
+  // this thread's: j fixed, k = k0 + q * dk (the unit-stride index runs along the warp)
+  const bool jfast = bsj == 1;
+  const int bj = jfast ? tid % NW : tid / GEMM_KC;
+  const int bk0 = jfast ? tid / NW : tid % GEMM_KC;
+  const int bdk = jfast ? GEMM_THREADS / NW : 0;
+  const int bdj = jfast ? 0 : GEMM_THREADS / GEMM_KC;
+  auto load_b = [&](int stage, int kb) {
+#pragma unroll
+    for (int q = 0; q < BPER; ++q) {
+      const int k = bk0 + q * bdk, j = bj + q * bdj;
+      const bool ok = j < N && kb + k < K;
+      const double *src = bbase;
+      if (ok) src = gather ? bbase + (int64_t)brows[kb + k] * bsk + j : bbase + (int64_t)(kb + k) * bsk + j * bsj;
+      cp_async<sizeof(double)>(&Bs[stage][k][j], src, ok ? (int)sizeof(double) : 0);
+    }
+  };
+  double acc[NF][4];
+#pragma unroll
+  for (int c = 0; c < NF; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
+  const int nk = (K + GEMM_KC - 1) / GEMM_KC;
+  for (int st = 0; st < GEMM_STAGES - 1; ++st) {
+    if (st < nk) {
+      la.load(As[st], st * GEMM_KC, K, abase);
+      load_b(st, st * GEMM_KC);
+    }
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<GEMM_STAGES - 2>();
+    __syncthreads();
+    const int pf = kt + GEMM_STAGES - 1;
+    if (pf < nk) {
+      la.load(As[pf % GEMM_STAGES], pf * GEMM_KC, K, abase);
+      load_b(pf % GEMM_STAGES, pf * GEMM_KC);
+    }
+    cp_async_commit();
+    const int st = kt % GEMM_STAGES;
+#pragma unroll
+    for (int kk = 0; kk < GEMM_KC; kk += 8) {
+      double av[4], bv[NF][2];
+      const int i = wm + g;
+      av[0] = (double)As[st][kk + tg][i];
+      av[1] = (double)As[st][kk + tg][i + 8];
+      av[2] = (double)As[st][kk + tg + 4][i];
+      av[3] = (double)As[st][kk + tg + 4][i + 8];
+#pragma unroll
+      for (int c = 0; c < NF; ++c) {
+        bv[c][0] = Bs[st][kk + tg][c * 8 + g];
+        bv[c][1] = Bs[st][kk + tg + 4][c * 8 + g];
+      }
+#pragma unroll
+      for (int c = 0; c < NF; ++c) dmma16(acc[c], av, bv[c]);
+    }
+  }
+  cp_async_wait<0>();
+  // fragment element e of column block c: row wm + g + 8 (e >> 1), column 8 c + 2 tg + (e & 1)
+  int flags = tp->flags;
+  if (flags & 8) {
+    __shared__ int last;
+    double *P = part + tp->part_off;
+    double *mine = P + (int64_t)tp->chunk * 4096;
+#pragma unroll
+    for (int c = 0; c < NF; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) mine[(wm + g + 8 * (e >> 1)) * 64 + c * 8 + 2 * tg + (e & 1)] = acc[c][e];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counters + tp->counter, 1) == tp->chunks - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double tot[NF][4];
+#pragma unroll
+    for (int c = 0; c < NF; ++c) tot[c][0] = tot[c][1] = tot[c][2] = tot[c][3] = 0.0;
+    for (int q = 0; q < tp->chunks; ++q) {
+      const double *Pq = P + (int64_t)q * 4096;
+#pragma unroll
+      for (int c = 0; c < NF; ++c)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) tot[c][e] += __ldcg(Pq + (wm + g + 8 * (e >> 1)) * 64 + c * 8 + 2 * tg + (e & 1));
+    }
+    if (threadIdx.x == 0) counters[tp->counter] = 0;
+#pragma unroll
+    for (int c = 0; c < NF; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[c][e] = tot[c][e];
+    flags &= ~8;
+  }
+  const int M = tp->M;
+  const bool lower = flags & 1;
+  double *C = static_cast<double *>(tp->C);
+#pragma unroll
+  for (int c = 0; c < NF; ++c)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = wm + g + 8 * (e >> 1), j = c * 8 + 2 * tg + (e & 1);
+      if (i < M && j < N && (!lower || i >= j)) {
+        double *dst = C + (int64_t)i * tp->c_si + (int64_t)j * tp->c_sj;
+        *dst = (flags & 4) ? acc[c][e] : (flags & 2) ? -acc[c][e] : *dst - acc[c][e];
+      }
+    }
+}
+
 // ---- the solve's short products, K split over a thread-block cluster -------------------------
 // A launch of the solve with few output tiles leaves most SMs idle and each CTA walks a long K
 // alone. Here the 8 CTAs of a cluster share one 64 x 64 tile: CTA rank q takes the q-th of 8 equal
@@ -1325,6 +1467,10 @@ void configure_kernels() {
   set_smem(gemm_kernel<float>, gemm_smem<float>());
   set_smem(gemm_cluster_kernel<double>, gemm_smem<double>());
   set_smem(gemm_cluster_kernel<float>, gemm_smem<float>());
+  set_smem(gemm_narrow_kernel<double, 8>, gemm_narrow_smem<double, 8>());
+  set_smem(gemm_narrow_kernel<float, 8>, gemm_narrow_smem<float, 8>());
+  set_smem(gemm_narrow_kernel<double, 16>, gemm_narrow_smem<double, 16>());
+  set_smem(gemm_narrow_kernel<float, 16>, gemm_narrow_smem<float, 16>());
   set_smem(gemm_tf32x3_kernel, GEMM_F32_SMEM);
   configure_solve_dag();
   done = true;
@@ -1365,6 +1511,24 @@ void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t s
       gemm_kernel<float><<<count, GEMM_THREADS, gemm_smem<float>(), st>>>(tasks, part, counters);
       break;
     case GemmKind::F32_TF32X3: gemm_tf32x3_kernel<<<count, GEMM_THREADS, GEMM_F32_SMEM, st>>>(tasks); break;
+  }
+}
+
+void launch_gemm_narrow(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
+                        int32_t *counters) {
+  if (count <= 0) return;
+  configure_kernels();
+  if (cols <= 8) {
+    if (fp32_a)
+      gemm_narrow_kernel<float, 8><<<count, GEMM_THREADS, gemm_narrow_smem<float, 8>(), st>>>(tasks, part, counters);
+    else
+      gemm_narrow_kernel<double, 8><<<count, GEMM_THREADS, gemm_narrow_smem<double, 8>(), st>>>(tasks, part, counters);
+  } else {
+    if (fp32_a)
+      gemm_narrow_kernel<float, 16><<<count, GEMM_THREADS, gemm_narrow_smem<float, 16>(), st>>>(tasks, part, counters);
+    else
+      gemm_narrow_kernel<double, 16><<<count, GEMM_THREADS, gemm_narrow_smem<double, 16>(), st>>>(tasks, part,
+                                                                                                  counters);
   }
 }
 

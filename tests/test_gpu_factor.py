@@ -11,7 +11,9 @@ import numpy as np
 import pytest
 
 import helpers as H
-from fieldcraft_b200 import Cancelled, Factor, NotPositiveDefinite, Symbolic, TooLarge, UpperColumns, problems
+from fieldcraft_b200 import (FP32_IR, FP64, Cancelled, Factor, NotPositiveDefinite, Symbolic, TooLarge, UpperColumns,
+                              _lib, problems)
+from fieldcraft_b200._lib import Status
 from fieldcraft_b200.cholesky import Csr
 from oracle import oracle
 
@@ -129,6 +131,38 @@ def test_split_solve_does_not_depend_on_how_many_are_solved(cuda):
     assert same(alone[0], many[0]) and same(alone[3], many[3]) and same(alone[69], many[69])
     r = oracle.spmv(csr.n, csr.ptr, csr.idx, csr.val, alone[69]) - rhs[69]
     assert np.linalg.norm(r) <= 1e-10 * np.linalg.norm(rhs[69])
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_IR], ids=["fp64", "fp32_ir"])
+def test_narrow_solve_tiles_give_the_same_bits(cuda, precision):
+    """With up to 16 right-hand sides the solve's products run in 64 x 8 / 64 x 16 tiles; with the
+    option off in the 64 x 64 tiles. On the 16^3 block (split products, thin chunks), for the FP64
+    factor and the FP32 one (a 4-byte L widened in the products), 1, 7 and 16 right-hand sides
+    give the same bits both ways, and the same bits as among 70."""
+    torch = cuda
+    lib = _lib.load()
+    p = problems.lognormal_block(16, nrhs=1)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62), precision=precision)
+    f.factor(up.val)
+    rng = np.random.default_rng(9)
+    rhs = torch.from_numpy(rng.standard_normal((70, p.n))).cuda()  # row j: right-hand side j
+
+    def solve(k):
+        x = rhs[:k].clone()
+        st = Status()
+        assert lib.fc_chol_solve_device(f.handle, C.c_void_p(x.data_ptr()), k, p.n, C.byref(st)) == 0, st.message
+        return x
+
+    many = solve(70)
+    for k in (1, 7, 16):
+        f.option(Factor.SOLVE_NARROW, 1)
+        narrow = solve(k)
+        f.option(Factor.SOLVE_NARROW, 0)
+        wide = solve(k)
+        assert torch.equal(narrow, wide) and torch.equal(narrow, many[:k]), k
+    f.option(Factor.SOLVE_NARROW, 1)
+    f.close()
 
 
 def test_cluster_split_solve(cuda):

@@ -136,10 +136,12 @@ def test_block_jacobi_batches_and_the_safeguard(cuda):
 
 
 def test_odd_network_is_odd_in_the_residual(cuda):
-    """The default preconditioner B r + (net(r) - net(-r)) / 2 is odd in r exactly (IEEE negation
-    and subtraction are exact): M(-r) = -M(r) bit for bit and M(0) = 0. With the odd form switched
-    off, a network with nonzero biases gives M(0) != 0 (its output has a part that does not depend
-    on r)."""
+    """The network sees r scaled to unit RMS beside each node's modulus and its output is scaled
+    back by |r|, so M(t r) = t M(r) for t > 0 but not for t < 0: a part of the output comes from the
+    modulus channel and the biases, whatever the sign of r. The default preconditioner
+    B r + (net(r) - net(-r)) / 2 cancels that part and is odd in r exactly (IEEE negation and
+    subtraction are exact): M(-r) = -M(r) bit for bit, and M(0) = 0. With the odd form switched off
+    M(-r) != -M(r)."""
     torch = cuda
     from fieldcraft_b200.unet import UNet
     p = small_plate()
@@ -154,8 +156,9 @@ def test_odd_network_is_odd_in_the_residual(cuda):
     assert torch.equal(zm, -z) and z.abs().max().item() > 0
     assert z0.abs().max().item() == 0.0
     net.set_odd(False)
-    net.apply(torch.zeros_like(r), z0)
-    assert z0.abs().max().item() > 0
+    net.apply(r, z)
+    net.apply(-r, zm)
+    assert ((zm + z).norm() / z.norm()).item() > 1e-3
     net.close()
 
 
