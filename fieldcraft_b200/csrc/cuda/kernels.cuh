@@ -23,7 +23,7 @@ constexpr int SPLIT_K = 512;  // K chunk of the persistent solve's split product
 // of its diagonal blocks of up to SB columns are formed during the factorisation (from the 64 x 64
 // inverses of the panels, by doubling), so a solve step is a GEMM over SB columns, not a chain of
 // SB / 64 dependent panel steps.
-constexpr int SB = 1024;
+constexpr int SB = 2048;
 // The solve's short products split K over a cluster of this many CTAs (gemm_cluster_kernel).
 constexpr int SOLVE_CLUSTER = 8;
 
