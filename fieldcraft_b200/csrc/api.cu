@@ -534,10 +534,12 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         int bw;
         const int64_t ib = inv_block(h, s, c0 / fc::SB, bw), in = c0 % fc::SB;
         const int64_t ioff = ib + in + in * bw;
+        // every CTA of the panel stores its share of the factored block and its inverse (keep:
+        // the panel's CTA count, pad: this CTA's place among them)
         if (c1 >= m) panel_t.push_back({(int32_t)s, c0, c1, m, m, 1, doff, ioff, bw, 0});
-        for (int r0 = c1; r0 < m; r0 += fc::PANEL_ROWS)
-          panel_t.push_back(
-              {(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), r0 == c1 ? 1 : 0, doff, ioff, bw, 0});
+        const int nrt = (m - c1 + fc::PANEL_ROWS - 1) / fc::PANEL_ROWS;
+        for (int r0 = c1, q = 0; r0 < m; r0 += fc::PANEL_ROWS, ++q)
+          panel_t.push_back({(int32_t)s, c0, c1, r0, std::min(m, r0 + fc::PANEL_ROWS), nrt, doff, ioff, bw, q});
         const int bs = p / OP * OP * NB, be = std::min(w, bs + OP * NB);  // this panel's block
         if (c1 < be) tiles(s, c1, be, c0, c1, gemm_t);                     // within the block
         if (c1 == be && be < w) {                                         // past the block

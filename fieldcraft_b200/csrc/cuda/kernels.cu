@@ -203,9 +203,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
                                                               const PanelTask *__restrict__ tasks,
                                                               DeviceStatus *status, int p8max) {
   extern __shared__ double sm[];
-  double *a = sm;                   // factor, column-major, ld 65 (p8max columns)
-  double *inv = a + p8max * 65;     // inv[k * TS + i] = Linv(i, k) (p8max rows)
-  double *tt = inv + p8max * TS;    // scratch of the inversion's products (<= 1024 doubles)
+  double *inv = sm;                 // inv[k * TS + i] = Linv(i, k) (p8max rows)
+  double *a = inv + p8max * TS;     // factor, column-major, ld 65 (p8max columns)
+  double *tt = a + p8max * 65;      // scratch of the inversion's products (<= 1024 doubles)
+  T *bt2 = reinterpret_cast<T *>(a);  // after the factor is stored: the second row tile (a and tt)
   double *dg = tt + 1024;           // the matrix's own diagonal entries of the panel's columns
   double *dv = dg + 64;             // the pivots' reciprocals
   T *bt = reinterpret_cast<T *>(dv + 64);  // rows below: bt[k * S + r] = L(r0 + r, c0 + k)
@@ -218,13 +219,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
   const int nb8 = (pw + 7) >> 3, P8 = 8 * nb8, K4 = (pw + 3) & ~3;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) fail = pw;
-  // the matrix's own diagonal entries first (two dependent loads each), then the block's lower
-  // triangle, identity past pw (so the padded block inverts to the same leading pw x pw inverse)
-  for (int c = tid; c < pw; c += PANEL_THREADS) {
-    const int64_t j = f + c0 + c, ds = t.diag_src[j];
-    const double d = ds >= 0 ? val[ds] : 0.0;
-    dg[c] = t.scale ? d * t.scale[j] * t.scale[j] : d;
-  }
+  // the block's lower triangle (identity past pw, so the padded block inverts to the same leading
+  // pw x pw inverse) and the first row tile in flight first, then the matrix's own diagonal
+  // entries (two dependent loads each) while those land
+  if (rows > 0) load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, min(rows, 64), pw, K4);
   if (sizeof(T) == 8) {
     for (int c = warp; c < P8; c += PANEL_THREADS / 32)
       for (int r = lane; r < P8; r += 32) {
@@ -251,9 +249,13 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
         if (c < P8 && r < P8) a[c * 65 + r] = (double)v[ci][ri];
       }
   }
-  for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
-  if (rows > 0) load_tile<T>(bt, Ls + task.r0 + (int64_t)c0 * m, 1, m, min(rows, 64), pw, K4);
   cp_async_commit();
+  for (int c = tid; c < pw; c += PANEL_THREADS) {
+    const int64_t j = f + c0 + c, ds = t.diag_src[j];
+    const double d = ds >= 0 ? val[ds] : 0.0;
+    dg[c] = t.scale ? d * t.scale[j] * t.scale[j] : d;
+  }
+  for (int e = tid; e < P8 * TS; e += PANEL_THREADS) inv[e] = 0.0;
   cp_async_wait<0>();
   __syncthreads();
   // right-looking by strips of 8 columns with look-ahead: warp 0 factors a strip (two rows a
@@ -378,20 +380,34 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
     }
     __syncthreads();
   }
-  if (task.keep) {
+  {
+    // this CTA's columns of the factored block and its inverse (the panel's CTAs share the stores)
     double *Dp = t.D + task.doff, *Ip = t.Dinv + task.ioff;
-    for (int c = warp; c < pw; c += PANEL_THREADS / 32)
+    const int nw = PANEL_THREADS / 32;
+    for (int c = task.part * nw + warp; c < pw; c += task.keep * nw)
       for (int r = lane; r < pw; r += 32) {
         Dp[c * pw + r] = r >= c ? a[c * 65 + r] : 0.0;
         Dp[pw * pw + c * pw + r] = inv[c * TS + r];
         Ip[(int64_t)c * task.ild + r] = r >= c ? inv[c * TS + r] : 0.0;
       }
-    if (tid == 0 && fail < pw) atomicMin(&status->failed_column, (unsigned long long)(f + c0 + fail));
+    if (tid == 0 && task.part == 0 && fail < pw)
+      atomicMin(&status->failed_column, (unsigned long long)(f + c0 + fail));
   }
-  // the rows below, 64 at a time (the first 64 loaded with the block)
+  // the rows below, 64 at a time: the first 64 loaded with the block, the next 64 into the factor's
+  // and the scratch's space (free once the factor is stored) while the first are solved, any
+  // further ones one after another
+  if (rows > 64) {
+    __syncthreads();  // every thread is done with a and tt
+    load_tile<T>(bt2, Ls + task.r0 + 64 + (int64_t)c0 * m, 1, m, min(64, rows - 64), pw, K4);
+    cp_async_commit();
+  }
   for (int rr = 0; rr < rows; rr += 64) {
     const int nrr = min(64, rows - rr);
-    if (rr > 0) {
+    const T *tile = rr == 64 ? bt2 : bt;
+    if (rr == 64) {
+      cp_async_wait<0>();
+      __syncthreads();
+    } else if (rr > 64) {
       __syncthreads();  // the previous rows' tile is read
       load_tile<T>(bt, Ls + task.r0 + rr + (int64_t)c0 * m, 1, m, nrr, pw, K4);
       cp_async_commit();
@@ -400,7 +416,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
     }
     double acc[4][4][2];
     zero_acc(acc);
-    mma_tiles<T>(bt, inv, K4, acc);
+    mma_tiles<T>(tile, inv, K4, acc);
     T *dst = Ls + task.r0 + rr + (int64_t)c0 * m;
     each_acc(acc, [&](int i, int c, double v) {
       if (i < nrr && c < pw) dst[i + (int64_t)c * m] = T(v);

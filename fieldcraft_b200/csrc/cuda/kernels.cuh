@@ -75,14 +75,16 @@ struct AssembleTask {
   int32_t m, w, k0, pad;  // its height and width; its first child's place in the kid lists
 };
 // Panel [c0, c1) of supernode s: factor its diagonal block, invert it, and solve the rows
-// [r0, r1) below it (r0 >= c1; an empty range for a task that only keeps the block). The task
-// with `keep` set writes the factored block and its inverse to the diagonal arena at `doff` and
-// reports the pivots; every task of the panel factors the block itself (no CTA waits on another).
+// [r0, r1) below it (r0 >= c1; an empty range for a task that only keeps the block). Every task of
+// the panel factors the block itself (no CTA waits on another) and writes its share of the factored
+// block and its inverse (to the diagonal arena at `doff` and to Dinv at `ioff`); part 0 reports the
+// pivots.
 struct PanelTask {
-  int32_t s, c0, c1, r0, r1, keep;
-  int64_t doff;
-  int64_t ioff;  // keep task: where the block's inverse goes in Dinv (leading dimension ild)
-  int32_t ild, pad;
+  int32_t s, c0, c1, r0, r1;
+  int32_t keep;  // the panel's CTA count: each stores columns part, part + keep, ... (times 4 warps)
+  int64_t doff;  // of the factored block and its inverse
+  int64_t ioff;  // where the block's inverse goes in Dinv (leading dimension ild)
+  int32_t ild, part;
 };
 // C(i, j) -= sum_k A(i, k) B(j, k) for i < M, j < N, k < K, strided operands. Flags: 1 touches
 // i >= j only (a diagonal tile of a symmetric matrix); 2 stores C = -sum instead of subtracting;
