@@ -550,7 +550,8 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             const int32_t map = (int32_t)maps.size();
             maps.push_back({blk_at, ub, wpad});
             for (int r0 = 0; r0 < ub; r0 += fc::TC_PACK_ROWS)
-              blk_pack.push_back({(int32_t)s, r0, wpad, kw, blk_at, bs, be});
+              for (int k0 = 0; k0 < wpad; k0 += fc::TC_PACK_K)
+                blk_pack.push_back({(int32_t)s, r0, wpad, kw, blk_at, bs, be, k0, std::min(wpad, k0 + fc::TC_PACK_K)});
             blk_at += ((int64_t)ub * 2 * wpad + 63) / 64 * 64;
             tc_tiles(s, be, nx, map, kw, wpad, be, tc_next);
             if (nx < w) tc_tiles(s, nx, w, map, kw, wpad, be, tc_rest);
@@ -629,7 +630,9 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         const int wpad = (w + fc::TC_KPAD - 1) / fc::TC_KPAD * fc::TC_KPAD;
         const int32_t map = (int32_t)maps.size();
         maps.push_back({at, u, wpad});
-        for (int r0 = 0; r0 < u; r0 += fc::TC_PACK_ROWS) pack_t.push_back({(int32_t)s, r0, wpad, w, at, 0, w});
+        for (int r0 = 0; r0 < u; r0 += fc::TC_PACK_ROWS)
+          for (int k0 = 0; k0 < wpad; k0 += fc::TC_PACK_K)
+            pack_t.push_back({(int32_t)s, r0, wpad, w, at, 0, w, k0, std::min(wpad, k0 + fc::TC_PACK_K)});
         at += ((int64_t)u * 2 * wpad + 63) / 64 * 64;  // 256-byte aligned regions
         const int64_t uo = h->uoff[s];
         for (int bj = 0; bj < u; bj += fc::GEMM_TC_N)

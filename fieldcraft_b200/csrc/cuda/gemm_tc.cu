@@ -240,9 +240,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2) syrk_tc_kernel(const TcTask *__
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_COLS));
 }
 
-// P rows [r0, r0 + TC_PACK_ROWS) of a block of supernode s's L (FP32 in the L arena, column-major):
-// hi and lo as K-major rows, through a shared tile so that both the reads (down a column) and the
-// writes (along a row) are coalesced.
+// P rows [r0, r0 + TC_PACK_ROWS), columns [k0, k1), of a block of supernode s's L (FP32 in the L
+// arena, column-major): hi and lo as K-major rows, through a shared tile so that both the reads
+// (down a column) and the writes (along a row) are coalesced.
 __global__ void __launch_bounds__(256) pack_tc_kernel(Tree t, const PackTask *__restrict__ tasks,
                                                        float *__restrict__ P) {
   __shared__ float tile[TC_KPAD][TC_PACK_ROWS + 1];
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(256) pack_tc_kernel(Tree t, const PackTask *__
   const float *Lb = static_cast<const float *>(t.L) + t.loff[s] + (int64_t)task.c0 * m + task.row0;
   const int r0 = task.r0, nr = min(TC_PACK_ROWS, u - r0), wpad = task.wpad;
   float *Pp = P + task.poff;
-  for (int kc = 0; kc < wpad; kc += TC_KPAD) {
+  for (int kc = task.k0; kc < task.k1; kc += TC_KPAD) {
     for (int e = threadIdx.x; e < TC_KPAD * TC_PACK_ROWS; e += blockDim.x) {
       const int k = e / TC_PACK_ROWS, r = e - k * TC_PACK_ROWS;
       tile[k][r] = kc + k < w && r < nr ? Lb[(int64_t)(kc + k) * m + r0 + r] : 0.f;

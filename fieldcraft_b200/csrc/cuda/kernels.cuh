@@ -226,7 +226,11 @@ struct PackTask {
   int32_t s, r0, wpad, kw;  // rows [r0, r0 + TC_PACK_ROWS) of the packed block, kw columns
   int64_t poff;
   int32_t c0, row0;  // the block: columns [c0, c0 + kw) of L from front row row0 down
+  int32_t k0, k1;    // this task's packed columns [k0, k1) (multiples of TC_KPAD; k1 <= wpad)
 };
+// A pack task's columns: a wide block is packed by several tasks side by side, not column chunk
+// after column chunk in one CTA.
+constexpr int TC_PACK_K = 256;
 struct TcTask {
   int32_t map, bi, bj, M, N, K, wpad, flags;
   float *C;
