@@ -250,9 +250,12 @@ int32_t child_ranges(const fc_chol *h, int64_t s, int lo, int hi, std::vector<in
   return at;
 }
 
+// The assembly tile's columns: an FP32 front's tiles are twice as wide (the same bytes).
+int assemble_cols(const fc_chol *h) { return h->fp32 ? fc::ASSEMBLE_COLS_F32 : fc::ASSEMBLE_COLS; }
+
 // Assembly tiles of supernode s (see assemble_kernel): ASM_L over the L panel's columns, or the
 // update matrix's columns as ASM_U (only tiles some child lands in: the rest keep what the GEMM
-// stored) or ASM_U_PRODUCT (all tiles). A block of ASSEMBLE_COLS columns is cut into row tiles
+// stored) or ASM_U_PRODUCT (all tiles). A block of assemble_cols(h) columns is cut into row tiles
 // of ASSEMBLE_ROWS from its first column down; each tile's child ranges come from `at`, per child
 // the first row of its update matrix whose place in the front is >= r, for every r in [0, m].
 void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::AssembleTask> &out,
@@ -273,8 +276,9 @@ void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::Assem
     }
   }
   const int64_t f = h->first[s];
-  for (int j0 = jlo; j0 < jhi; j0 += fc::ASSEMBLE_COLS) {
-    const int j1 = std::min(jhi, j0 + fc::ASSEMBLE_COLS);
+  const int cols = assemble_cols(h);
+  for (int j0 = jlo; j0 < jhi; j0 += cols) {
+    const int j1 = std::min(jhi, j0 + cols);
     for (int i0 = j0; i0 < m; i0 += fc::ASSEMBLE_ROWS) {
       const int i1 = std::min(m, i0 + fc::ASSEMBLE_ROWS);
       const int32_t base = (int32_t)ranges.size();
@@ -1105,7 +1109,7 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
       if (r == c) diag_src[c] = e;
     }
   }
-  // within each block of ASSEMBLE_COLS columns of a supernode, the entries by their row in the
+  // within each block of assemble_cols(h) columns of a supernode, the entries by their row in the
   // front (an assembly tile takes the contiguous run of its rows)
   std::vector<int32_t> a_lrow(h->nnz);
   {
@@ -1113,8 +1117,9 @@ int build(fc_chol *h, const fc::Symbolic &sym, fc_status *st) {
     std::vector<int64_t> src2, dst2;
     for (int64_t s = 0; s < ns; ++s) {
       const int64_t f = sym.first[s], w = sym.first[s + 1] - f, m = sym.height(s);
-      for (int64_t j0 = 0; j0 < w; j0 += fc::ASSEMBLE_COLS) {
-        const int64_t b0 = a_ptr[f + j0], b1 = a_ptr[f + std::min(w, j0 + fc::ASSEMBLE_COLS)];
+      const int64_t cols = assemble_cols(h);
+      for (int64_t j0 = 0; j0 < w; j0 += cols) {
+        const int64_t b0 = a_ptr[f + j0], b1 = a_ptr[f + std::min(w, j0 + cols)];
         run.clear();
         for (int64_t q = b0; q < b1; ++q) run.emplace_back((int32_t)((a_dst[q] - h->loff[s]) % m), q);
         std::sort(run.begin(), run.end());

@@ -48,7 +48,7 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
 }
 
 // ---- front assembly ----------------------------------------------------------------------------
-// One tile of supernode s's front: columns [j0, j1) (at most ASSEMBLE_COLS) by rows [i0, i1) (at
+// One tile of supernode s's front: columns [j0, j1) (at most COLS) by rows [i0, i1) (at
 // most ASSEMBLE_ROWS), built in shared memory and written once. The tile starts as
 //   ASM_L          zero, then A's entries (columns of the L panel, assembled before the panel is
 //                  factored; with a scale, the entries of S A S, S = diag(A)^-1/2);
@@ -61,13 +61,14 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
 // fall in the tile; only its lower triangle (row >= column) is read. No destination is read and
 // written through global memory: the child's rows and values stream in coalesced, the scatter is
 // to shared memory, and every entry of the tile's lower part is stored once.
-template <class T>
-__global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, const double *__restrict__ val,
-                                                                    const AssembleTask *__restrict__ tasks,
-                                                                    const int4 *__restrict__ ranges) {
-  static_assert(ASSEMBLE_ROWS == ASSEMBLE_THREADS && ASSEMBLE_COLS * 32 == ASSEMBLE_THREADS, "tile shape");
-  __shared__ T tile[ASSEMBLE_COLS][ASSEMBLE_ROWS];
-  __shared__ T lj[ASSEMBLE_THIN][ASSEMBLE_COLS];
+template <class T, int COLS>
+__global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
+    assemble_kernel(Tree t, const double *__restrict__ val, const AssembleTask *__restrict__ tasks,
+                    const int4 *__restrict__ ranges) {
+  constexpr int WARPS = ASSEMBLE_THREADS / 32, CPW = COLS / WARPS;  // child columns a warp takes
+  static_assert(ASSEMBLE_ROWS == ASSEMBLE_THREADS && CPW * WARPS == COLS && CPW >= 1, "tile shape");
+  __shared__ T tile[COLS][ASSEMBLE_ROWS];
+  __shared__ T lj[ASSEMBLE_THIN][COLS];
   __shared__ int4 s_rg[ASSEMBLE_KIDS];
   __shared__ KidMeta s_km[ASSEMBLE_KIDS];
   const AssembleTask task = tasks[blockIdx.x];
@@ -97,9 +98,9 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
     __syncthreads();
     if (ii < nr) {
       // the row's values of L21 four at a time in flight, then their dot products
-      T acc[ASSEMBLE_COLS];
+      T acc[COLS];
 #pragma unroll
-      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = T(0);
+      for (int jj = 0; jj < COLS; ++jj) acc[jj] = T(0);
       for (int k0 = 0; k0 < w; k0 += 4) {
         T a[4];
 #pragma unroll
@@ -108,25 +109,25 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
         for (int k = 0; k < 4; ++k)
           if (k0 + k < w) {
 #pragma unroll
-            for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) acc[jj] = fma(a[k], lj[k0 + k][jj], acc[jj]);
+            for (int jj = 0; jj < COLS; ++jj) acc[jj] = fma(a[k], lj[k0 + k][jj], acc[jj]);
           }
       }
 #pragma unroll
-      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) tile[jj][ii] = -acc[jj];
+      for (int jj = 0; jj < COLS; ++jj) tile[jj][ii] = -acc[jj];
     }
   } else if (task.mode == ASM_U) {
     if (ii < nr) {
-      T v[ASSEMBLE_COLS];
+      T v[COLS];
 #pragma unroll
-      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj)
+      for (int jj = 0; jj < COLS; ++jj)
         if (jj < nc && r >= j0 + jj) v[jj] = column(jj)[r];
 #pragma unroll
-      for (int jj = 0; jj < ASSEMBLE_COLS; ++jj)
+      for (int jj = 0; jj < COLS; ++jj)
         if (jj < nc && r >= j0 + jj) tile[jj][ii] = v[jj];
     }
   } else {
 #pragma unroll
-    for (int jj = 0; jj < ASSEMBLE_COLS; ++jj) tile[jj][ii] = T(0);
+    for (int jj = 0; jj < COLS; ++jj) tile[jj][ii] = T(0);
     __syncthreads();
     // A's entries of the tile: the block's entries are sorted by row, [e0, e1) are this tile's
     for (int64_t e = task.e0 + tid; e < task.e1; e += ASSEMBLE_THREADS) {
@@ -136,39 +137,50 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, 6) assemble_kernel(Tree t, c
     }
   }
   __syncthreads();
-  // the children: warp q takes the child's q-th column in the tile (a child has at most one column
-  // per tile column), its lanes the rows, eight loads a lane in flight before the adds
+  // the children: warp q takes the child's columns q, q + WARPS, ... in the tile (a child has at
+  // most one column per tile column), its lanes the rows, eight loads a lane a column in flight
+  // before the adds
   for (int q = 0; q < nk; ++q) {
     const int4 g = q < ASSEMBLE_KIDS ? s_rg[q] : ranges[task.ranges + q];
-    const int jc = g.x + warp;
     if (g.x < g.y && g.z < g.w) {
-      if (jc < g.y) {
+      if (g.x + warp < g.y) {
         const KidMeta km = q < ASSEMBLE_KIDS ? s_km[q] : t.kid_meta[task.k0 + q];
         const int32_t *rel = t.rel + km.rel_off;
-        const T *src = static_cast<const T *>(t.U) + km.uoff + (int64_t)jc * km.uc;
-        const int a = g.z > jc ? g.z : jc;
-        int at[ASSEMBLE_ROWS / 32];
-        T v[ASSEMBLE_ROWS / 32];
-        const int relj = rel[jc];
+        int at[CPW][ASSEMBLE_ROWS / 32], jjs[CPW];
+        T v[CPW][ASSEMBLE_ROWS / 32];
 #pragma unroll
-        for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k) {
-          const int ic = a + lane + 32 * k;
-          if (ic < g.w) {
-            at[k] = rel[ic];
-            v[k] = src[ic];
+        for (int c = 0; c < CPW; ++c) {
+          const int jc = g.x + warp + WARPS * c;
+          jjs[c] = -1;
+          if (jc < g.y) {
+            const T *src = static_cast<const T *>(t.U) + km.uoff + (int64_t)jc * km.uc;
+            const int a = g.z > jc ? g.z : jc;
+            jjs[c] = rel[jc] - j0;
+#pragma unroll
+            for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k) {
+              const int ic = a + lane + 32 * k;
+              at[c][k] = -1;
+              if (ic < g.w) {
+                at[c][k] = rel[ic];
+                v[c][k] = src[ic];
+              }
+            }
           }
         }
-        const int jj = relj - j0;
 #pragma unroll
-        for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k)
-          if (a + lane + 32 * k < g.w) tile[jj][at[k] - i0] += v[k];
+        for (int c = 0; c < CPW; ++c)
+          if (jjs[c] >= 0) {
+#pragma unroll
+            for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k)
+              if (at[c][k] >= 0) tile[jjs[c]][at[c][k] - i0] += v[c][k];
+          }
       }
       __syncthreads();
     }
   }
   if (ii < nr) {
 #pragma unroll
-    for (int jj = 0; jj < ASSEMBLE_COLS; ++jj)
+    for (int jj = 0; jj < COLS; ++jj)
       if (jj < nc && r >= j0 + jj) column(jj)[r] = tile[jj][ii];
   }
 }
@@ -1501,9 +1513,9 @@ void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const As
   if (count <= 0) return;
   configure_kernels();
   if (fp32)
-    assemble_kernel<float><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
+    assemble_kernel<float, ASSEMBLE_COLS_F32><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
   else
-    assemble_kernel<double><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
+    assemble_kernel<double, ASSEMBLE_COLS><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
 }
 
 void launch_panel(const Tree &t, bool fp32, const double *upper_val, const PanelTask *tasks, int count,
