@@ -233,7 +233,7 @@ struct PackTask {
 };
 // A pack task's columns: a wide block is packed by several tasks side by side, not column chunk
 // after column chunk in one CTA.
-constexpr int TC_PACK_K = 256;
+constexpr int TC_PACK_K = 64;
 struct TcTask {
   int32_t map, bi, bj, M, N, K, wpad, flags;
   float *C;
