@@ -585,7 +585,8 @@ def run_config(args, cfg: int, torch, lib, local: int):
                     "relres_max": res[FP32_IR]["relres_max"], "speedup_vs_fp64": res[FP64]["ms"] / res[FP32_IR]["ms"]},
     }
     if tuned:
-        names = {"1": "solve_schedule", "5": "refinement", "6": "fp32_updates", "7": "solve_cluster"}
+        names = {"1": "solve_schedule", "5": "refinement", "6": "fp32_updates", "7": "solve_cluster", "8": "solve_narrow",
+                 "9": "solve_deep"}
         line["autotuned"] = {("fp64" if prec == FP64 else "fp32_ir"):
                              {"options": {names[k]: v for k, v in t["options"].items()},
                               "candidates_ms": t["ms"]} for prec, t in tuned.items()}

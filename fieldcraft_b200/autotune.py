@@ -1,7 +1,9 @@
 """Chooses a handle's execution variants by timing them on the system itself: the kernels' tile
-shapes for the mixed-precision factor's update products (tcgen05 128 x 128 or mma.sync 64 x 64),
-the solve's schedule (level by level, or one persistent dependency-driven launch per direction),
-how the level-by-level solve splits the K of its short products (8-CTA clusters or chunks) and,
+shapes for the mixed-precision factor's update products (tcgen05 128 x 128 or mma.sync 64 x 64)
+and for the solve's products with few right-hand sides (64 x 8 / 64 x 16 or 64 x 64, and the
+short launches' copy ring of 8 or 3 stages), the solve's schedule (level by level, or one
+persistent dependency-driven launch per direction), how the level-by-level solve splits the K of
+its short products (8-CTA clusters or chunks) and,
 for a factor used as a preconditioner, conjugate gradients or plain refinement. Each
 candidate is run (factorisation + solve to the tolerance, device-timed with CUDA events) and the
 fastest is kept in the handle; results can be cached in a JSON file keyed by the system's shape.
@@ -17,11 +19,18 @@ from . import _lib
 from .cholesky import FP32_IR, Factor
 
 
-def candidates(precision: int) -> list[dict]:
+def candidates(precision: int, nrhs: int = 64) -> list[dict]:
     # the solve: level by level with its short products' K split over 8-CTA clusters or in chunks
-    # of separate CTAs, or the persistent dependency-driven launch (where the split does not apply)
-    solves = [{Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 0}, {Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 1},
-              {Factor.SOLVE_SCHEDULE: 1, Factor.SOLVE_CLUSTER: 0}]
+    # of separate CTAs, or the persistent dependency-driven launch (where the split does not apply);
+    # with at most 16 right-hand sides also the products' tile shape (64 x 8 / 64 x 16 or 64 x 64)
+    # and, for the narrow tiles, the copy ring of the short launches (8 stages or 3)
+    base = {Factor.SOLVE_NARROW: 1, Factor.SOLVE_DEEP: 1}
+    solves = [{Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 0, **base},
+              {Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 1, **base},
+              {Factor.SOLVE_SCHEDULE: 1, Factor.SOLVE_CLUSTER: 0, **base}]
+    if nrhs <= 16:
+        solves += [{Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 0, Factor.SOLVE_NARROW: 1, Factor.SOLVE_DEEP: 0},
+                   {Factor.SOLVE_SCHEDULE: 0, Factor.SOLVE_CLUSTER: 0, Factor.SOLVE_NARROW: 0, Factor.SOLVE_DEEP: 0}]
     if precision == FP32_IR:
         return [{Factor.FP32_UPDATES: u, **sv, Factor.REFINEMENT: r}
                 for u, sv, r in itertools.product([0, 1], solves, [0, 1])]
@@ -49,7 +58,7 @@ def autotune(factor: Factor, precision: int, d_val, nnz: int, csr_device, d_b, n
     x = torch.zeros_like(d_b)
     timings = {}
     best, best_ms = None, float("inf")
-    for cand in candidates(precision):
+    for cand in candidates(precision, nrhs):
         for k, v in cand.items():
             factor.option(k, v)
         runs = []

@@ -148,6 +148,7 @@ struct fc_chol {
   // or over thread-block clusters (FC_OPTION_SOLVE_CLUSTER = 1)
   bool solve_cluster = false;
   bool solve_narrow = true;  // the solve's products in 64 x 8 / 64 x 16 tiles for up to 16 right-hand sides
+  bool solve_deep = true;    // the solve's short product launches with the deeper cp.async ring
   DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
   int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
   int dag_grid = 0;
@@ -2330,6 +2331,10 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
   const cudaStream_t main = h->stream;
   const fc::Tree &t = h->ldlt ? h->stree : h->tree;
   const bool narrow = h->solve_narrow && R <= 16;  // every task's N is R then
+  // with few right-hand sides, a launch of fewer CTAs than two per SM: each CTA walks its K with
+  // the deeper ring (with 64-column tiles the ring's shared memory would leave one CTA an SM,
+  // and the measured solve was slower)
+  const int short_launch = h->solve_deep && narrow ? 2 * prop_sms(h->device) : 0;
   const bool lanes = events && ev && h->side;
   const std::vector<char> side = lanes ? beside(prog) : std::vector<char>(prog.size(), 0);
   bool forked = false;
@@ -2359,6 +2364,8 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
       case K_SOLVE_BWD:
         if (l.width == 1)
           fc::launch_gemm_cluster(b.gemm + l.off, l.count, false, st, b.part, b.tcount);
+        else if (l.count < short_launch)
+          fc::launch_gemm_solve(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount);
         else if (narrow)
           fc::launch_gemm_narrow(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount);
         else
@@ -2367,6 +2374,8 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
       case K_GEMM:
         if (l.width == 1)
           fc::launch_gemm_cluster(b.gemm + l.off, l.count, h->fp32, st, b.part, b.tcount);
+        else if (l.count < short_launch)
+          fc::launch_gemm_solve(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount);
         else if (narrow)
           fc::launch_gemm_narrow(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount);
         else
@@ -2876,6 +2885,11 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
     case FC_OPTION_SOLVE_NARROW:
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       h->solve_narrow = value == 1;
+      replan();
+      return FC_OK;
+    case FC_OPTION_SOLVE_DEEP:
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      h->solve_deep = value == 1;
       replan();
       return FC_OK;
     case FC_OPTION_FP32_UPDATES: {

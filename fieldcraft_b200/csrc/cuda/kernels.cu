@@ -443,9 +443,13 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(Tree t, const doub
 // A operand (the solve's L21^T v on an FP32 factor) is staged as FP32 and widened when read.
 constexpr int SROW = 68;
 constexpr int GEMM_STAGES = 3;
-template <class TA>
+// The solve's short launches with few right-hand sides run with a deeper ring: they have few
+// output tiles (often fewer than SMs), and a CTA's K loop is then bound by how many bytes it keeps
+// in flight.
+constexpr int SOLVE_STAGES = 8;
+template <class TA, int STAGES = GEMM_STAGES>
 __host__ __device__ constexpr size_t gemm_smem() {
-  return GEMM_STAGES * GEMM_KC * (sizeof(TA) * tile_stride<TA>() + sizeof(double) * SROW);
+  return STAGES * GEMM_KC * (sizeof(TA) * tile_stride<TA>() + sizeof(double) * SROW);
 }
 
 // This thread's elements of a 64 x KC operand tile: a fixed row and k = k0 + 2q when the rows
@@ -609,12 +613,12 @@ __device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)
 
 // The main loop of a 64 x 64 tile of C -= A B^T over K range [kbeg, kend) of the task: 3-stage
 // cp.async ring in `gsm`, DMMA into acc (this thread's fragments).
-template <class TA>
+template <class TA, int STAGES = GEMM_STAGES>
 __device__ __forceinline__ void gemm_mainloop(const GemmTask *tp, int kbeg, int kend, double (&acc)[2][4][4],
                                               double *gsm) {
   constexpr int SA = tile_stride<TA>();
   double(*Bs)[GEMM_KC][SROW] = reinterpret_cast<double(*)[GEMM_KC][SROW]>(gsm);
-  TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + GEMM_STAGES * GEMM_KC * SROW);
+  TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + STAGES * GEMM_KC * SROW);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tg = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
@@ -639,7 +643,7 @@ __device__ __forceinline__ void gemm_mainloop(const GemmTask *tp, int kbeg, int 
     else
       lb.load(Bs[stage], kb, K, bbase);
   };
-  for (int st = 0; st < GEMM_STAGES - 1; ++st) {
+  for (int st = 0; st < STAGES - 1; ++st) {
     if (st < nk) {
       la.load(As[st], st * GEMM_KC, K, abase);
       load_b(st, st * GEMM_KC);
@@ -647,15 +651,15 @@ __device__ __forceinline__ void gemm_mainloop(const GemmTask *tp, int kbeg, int 
     cp_async_commit();
   }
   for (int kt = 0; kt < nk; ++kt) {
-    cp_async_wait<GEMM_STAGES - 2>();
+    cp_async_wait<STAGES - 2>();
     __syncthreads();
-    const int pf = kt + GEMM_STAGES - 1;
+    const int pf = kt + STAGES - 1;
     if (pf < nk) {
-      la.load(As[pf % GEMM_STAGES], pf * GEMM_KC, K, abase);
-      load_b(pf % GEMM_STAGES, pf * GEMM_KC);
+      la.load(As[pf % STAGES], pf * GEMM_KC, K, abase);
+      load_b(pf % STAGES, pf * GEMM_KC);
     }
     cp_async_commit();
-    const int st = kt % GEMM_STAGES;
+    const int st = kt % STAGES;
 #pragma unroll
     for (int kk = 0; kk < GEMM_KC; kk += 8) {
       double av[2][4], bv[4][2];
@@ -681,16 +685,16 @@ __device__ __forceinline__ void gemm_mainloop(const GemmTask *tp, int kbeg, int 
   cp_async_wait<0>();
 }
 
-template <class TA>
-__global__ void __launch_bounds__(GEMM_THREADS, 3) gemm_kernel(const GemmTask *__restrict__ tasks, double *part,
-                                                               int32_t *counters) {
+template <class TA, int STAGES = GEMM_STAGES>
+__global__ void __launch_bounds__(GEMM_THREADS, STAGES == GEMM_STAGES ? 3 : 1)
+    gemm_kernel(const GemmTask *__restrict__ tasks, double *part, int32_t *counters) {
   extern __shared__ __align__(16) double gsm[];
   const GemmTask *tp = tasks + blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, tg = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   double acc[2][4][4];
-  gemm_mainloop<TA>(tp, 0, tp->K, acc, gsm);
+  gemm_mainloop<TA, STAGES>(tp, 0, tp->K, acc, gsm);
   gemm_epilogue<double>(tp, acc, wm, wn, g, tg, part, counters);
 }
 
@@ -706,20 +710,20 @@ template <int NW>
 __host__ __device__ constexpr int narrow_row() {
   return NW + 4;
 }
-template <class TA, int NW>
+template <class TA, int NW, int STAGES = GEMM_STAGES>
 __host__ __device__ constexpr size_t gemm_narrow_smem() {
-  return GEMM_STAGES * GEMM_KC * (sizeof(TA) * tile_stride<TA>() + sizeof(double) * narrow_row<NW>());
+  return STAGES * GEMM_KC * (sizeof(TA) * tile_stride<TA>() + sizeof(double) * narrow_row<NW>());
 }
 
-template <class TA, int NW>
-__global__ void __launch_bounds__(GEMM_THREADS, 6) gemm_narrow_kernel(const GemmTask *__restrict__ tasks, double *part,
-                                                                      int32_t *counters) {
+template <class TA, int NW, int STAGES = GEMM_STAGES>
+__global__ void __launch_bounds__(GEMM_THREADS, STAGES == GEMM_STAGES ? 6 : 2)
+    gemm_narrow_kernel(const GemmTask *__restrict__ tasks, double *part, int32_t *counters) {
   constexpr int NF = NW / 8, SA = tile_stride<TA>(), SN = narrow_row<NW>();
   constexpr int BPER = NW * GEMM_KC / GEMM_THREADS;  // B elements per thread per stage
   static_assert(BPER >= 1 && NW * GEMM_KC % GEMM_THREADS == 0, "narrow tile");
   extern __shared__ __align__(16) double gsm[];
   double(*Bs)[GEMM_KC][SN] = reinterpret_cast<double(*)[GEMM_KC][SN]>(gsm);
-  TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + GEMM_STAGES * GEMM_KC * SN);
+  TA(*As)[GEMM_KC][SA] = reinterpret_cast<TA(*)[GEMM_KC][SA]>(gsm + STAGES * GEMM_KC * SN);
   const GemmTask *tp = tasks + blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tg = lane & 3;
@@ -753,7 +757,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 6) gemm_narrow_kernel(const Gemm
 #pragma unroll
   for (int c = 0; c < NF; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
   const int nk = (K + GEMM_KC - 1) / GEMM_KC;
-  for (int st = 0; st < GEMM_STAGES - 1; ++st) {
+  for (int st = 0; st < STAGES - 1; ++st) {
     if (st < nk) {
       la.load(As[st], st * GEMM_KC, K, abase);
       load_b(st, st * GEMM_KC);
@@ -761,15 +765,15 @@ __global__ void __launch_bounds__(GEMM_THREADS, 6) gemm_narrow_kernel(const Gemm
     cp_async_commit();
   }
   for (int kt = 0; kt < nk; ++kt) {
-    cp_async_wait<GEMM_STAGES - 2>();
+    cp_async_wait<STAGES - 2>();
     __syncthreads();
-    const int pf = kt + GEMM_STAGES - 1;
+    const int pf = kt + STAGES - 1;
     if (pf < nk) {
-      la.load(As[pf % GEMM_STAGES], pf * GEMM_KC, K, abase);
-      load_b(pf % GEMM_STAGES, pf * GEMM_KC);
+      la.load(As[pf % STAGES], pf * GEMM_KC, K, abase);
+      load_b(pf % STAGES, pf * GEMM_KC);
     }
     cp_async_commit();
-    const int st = kt % GEMM_STAGES;
+    const int st = kt % STAGES;
 #pragma unroll
     for (int kk = 0; kk < GEMM_KC; kk += 8) {
       double av[4], bv[NF][2];
@@ -1495,6 +1499,10 @@ void configure_kernels() {
   set_smem(gemm_kernel<float>, gemm_smem<float>());
   set_smem(gemm_cluster_kernel<double>, gemm_smem<double>());
   set_smem(gemm_cluster_kernel<float>, gemm_smem<float>());
+  set_smem(gemm_narrow_kernel<double, 8, SOLVE_STAGES>, gemm_narrow_smem<double, 8, SOLVE_STAGES>());
+  set_smem(gemm_narrow_kernel<float, 8, SOLVE_STAGES>, gemm_narrow_smem<float, 8, SOLVE_STAGES>());
+  set_smem(gemm_narrow_kernel<double, 16, SOLVE_STAGES>, gemm_narrow_smem<double, 16, SOLVE_STAGES>());
+  set_smem(gemm_narrow_kernel<float, 16, SOLVE_STAGES>, gemm_narrow_smem<float, 16, SOLVE_STAGES>());
   set_smem(gemm_narrow_kernel<double, 8>, gemm_narrow_smem<double, 8>());
   set_smem(gemm_narrow_kernel<float, 8>, gemm_narrow_smem<float, 8>());
   set_smem(gemm_narrow_kernel<double, 16>, gemm_narrow_smem<double, 16>());
@@ -1539,6 +1547,27 @@ void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t s
       gemm_kernel<float><<<count, GEMM_THREADS, gemm_smem<float>(), st>>>(tasks, part, counters);
       break;
     case GemmKind::F32_TF32X3: gemm_tf32x3_kernel<<<count, GEMM_THREADS, GEMM_F32_SMEM, st>>>(tasks); break;
+  }
+}
+
+void launch_gemm_solve(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
+                       int32_t *counters) {
+  if (count <= 0) return;
+  configure_kernels();
+  constexpr int S = SOLVE_STAGES;
+  if (cols <= 8) {
+    if (fp32_a)
+      gemm_narrow_kernel<float, 8, S><<<count, GEMM_THREADS, gemm_narrow_smem<float, 8, S>(), st>>>(tasks, part, counters);
+    else
+      gemm_narrow_kernel<double, 8, S><<<count, GEMM_THREADS, gemm_narrow_smem<double, 8, S>(), st>>>(tasks, part,
+                                                                                                      counters);
+  } else {
+    if (fp32_a)
+      gemm_narrow_kernel<float, 16, S><<<count, GEMM_THREADS, gemm_narrow_smem<float, 16, S>(), st>>>(tasks, part,
+                                                                                                      counters);
+    else
+      gemm_narrow_kernel<double, 16, S><<<count, GEMM_THREADS, gemm_narrow_smem<double, 16, S>(), st>>>(tasks, part,
+                                                                                                        counters);
   }
 }
 

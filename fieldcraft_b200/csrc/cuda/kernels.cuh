@@ -256,6 +256,10 @@ void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t s
 // tiles, each element's bits those of launch_gemm's F64 / F32A_F64 kernels.
 void launch_gemm_narrow(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
                         int32_t *counters);
+// The solve's products with at most 16 right-hand sides (every task's N <= cols <= 16) in 64 x 8 /
+// 64 x 16 tiles with a deeper cp.async ring: the same bits as launch_gemm_narrow.
+void launch_gemm_solve(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
+                       int32_t *counters);
 // The same tasks (FP64 B and C; A FP64 or FP32) with K split over clusters of SOLVE_CLUSTER CTAs.
 void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part,
                          int32_t *counters);

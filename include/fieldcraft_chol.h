@@ -218,7 +218,11 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *   FC_OPTION_SOLVE_NARROW     with at most 16 right-hand sides, the level-by-level solve's
  *                              products in 64 x 8 or 64 x 16 tiles: 1 (default) on, 0 in the
  *                              64 x 64 tiles of more right-hand sides. The results are the same
- *                              bit for bit (the same products in the same order). */
+ *                              bit for bit (the same products in the same order).
+ *   FC_OPTION_SOLVE_DEEP       1 (default): with at most 16 right-hand sides, the level-by-level
+ *                              solve's product launches of fewer CTAs than two per SM run with an
+ *                              8-stage copy ring (more bytes in flight a CTA); 0: the factor's
+ *                              3-stage ring. The same bits. */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3
@@ -227,6 +231,7 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
 #define FC_OPTION_FP32_UPDATES 6
 #define FC_OPTION_SOLVE_CLUSTER 7
 #define FC_OPTION_SOLVE_NARROW 8
+#define FC_OPTION_SOLVE_DEEP 9
 int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
 /* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
  * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |

@@ -138,7 +138,8 @@ def test_narrow_solve_tiles_give_the_same_bits(cuda, precision):
     """With up to 16 right-hand sides the solve's products run in 64 x 8 / 64 x 16 tiles; with the
     option off in the 64 x 64 tiles. On the 16^3 block (split products, thin chunks), for the FP64
     factor and the FP32 one (a 4-byte L widened in the products), 1, 7 and 16 right-hand sides
-    give the same bits both ways, and the same bits as among 70."""
+    give the same bits both ways, and the same bits as among 70; 70 give the same bits with the
+    short launches' deeper copy ring on and off."""
     torch = cuda
     lib = _lib.load()
     p = problems.lognormal_block(16, nrhs=1)
@@ -155,6 +156,10 @@ def test_narrow_solve_tiles_give_the_same_bits(cuda, precision):
         return x
 
     many = solve(70)
+    f.option(Factor.SOLVE_DEEP, 0)
+    shallow = solve(70)
+    f.option(Factor.SOLVE_DEEP, 1)
+    assert torch.equal(many, shallow)  # the deeper copy ring of short launches changes no bit
     for k in (1, 7, 16):
         f.option(Factor.SOLVE_NARROW, 1)
         narrow = solve(k)
@@ -386,7 +391,7 @@ def test_autotuner_picks_a_working_variant(cuda, tmp_path):
     d_b = torch.from_numpy(np.ascontiguousarray(rhs.T)).cuda()
     cache = tmp_path / "tune.json"
     res = autotune(f, FP32_IR, d_val, up.val.size, device_csr(torch, csr), d_b, 2, 1e-10, torch, repeats=1, cache=cache)
-    assert len(res["ms"]) == len(candidates(FP32_IR)) and cache.exists()
+    assert len(res["ms"]) == len(candidates(FP32_IR, 2)) and cache.exists()
     again = autotune(f, FP32_IR, d_val, up.val.size, device_csr(torch, csr), d_b, 2, 1e-10, torch, cache=cache)
     assert again["options"] == res["options"]
     x = torch.zeros_like(d_b)
