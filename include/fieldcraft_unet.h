@@ -87,7 +87,8 @@ int fc_unet_train_batch(fc_unet *net, const double *d_r, const double *d_e, int3
  * network as preconditioner (net null: plain CG), keeping `keep` (1..8) earlier directions
  * A-orthogonal. A safeguard drops the network for the rest of the solve when, from iteration 50 on,
  * 25 iterations with it lower ||r||^2 by less than a factor 4 (the block-Jacobi part, if set,
- * stays; fc_unet_stat says whether and when). Stops when ||b - A x|| <= tol ||b|| or after max_iter
+ * stays; fc_unet_stat says whether and when) and restarts from the true residual b - A x with no
+ * kept directions. Stops when ||b - A x|| <= tol ||b|| or after max_iter
  * iterations (the host reads the residuals every 8 iterations, so up to 7 more may run past the
  * one that reached it); when the recurrence's residual reaches the tolerance but b - A x itself
  * does not (rounding has let them drift apart), FCG goes on from the true residual, at most 8

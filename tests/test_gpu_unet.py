@@ -100,9 +100,10 @@ def test_training_and_fcg_gain_over_plain_cg(cuda):
 
 def test_block_jacobi_batches_and_the_safeguard(cuda):
     """With K's nodal block-Jacobi part the preconditioner is B r + net(r): an untrained network
-    (last layer zero) is then block-Jacobi PCG itself, as the network switched off; minibatch
-    training lowers the loss; a network of random weights is dropped by FCG's safeguard
-    (which says so) and the solve still converges on block Jacobi."""
+    (last layer zero) is then block-Jacobi PCG itself, as the network switched off (safeguard off,
+    the same iterations); minibatch training lowers the loss; a network of random weights is
+    dropped by FCG's safeguard (which says so), and the solve restarts and converges on block
+    Jacobi."""
     torch = cuda
     from fieldcraft_b200.unet import UNet, fcg, output_scale, train, training_pairs
     p = problems.plate(24, 24, 4, corr=4.0, contrast=100.0, seed=9, nrhs=2)
@@ -116,23 +117,26 @@ def test_block_jacobi_batches_and_the_safeguard(cuda):
     assert net.stat(3) == 1 and net.stat(0) == 4
     runs = []
     for on in (False, True):
-        net.enable(on)
+        net.enable(on, safeguard=False)
         x = torch.zeros_like(b)
         runs.append(fcg(csr, b, x, net=net, tol=1e-10, max_iter=3000, keep=4))
     assert runs[0][0] == runs[1][0] and runs[0][1] <= 1e-10  # an untrained network adds nothing
+    net.enable(True)
     losses = train(net, R, E, epochs=3, lr=1e-3, torch=torch, csr_device=csr, batch=8, warmup=20)
     assert losses[-1] < losses[0], losses
     x = torch.zeros_like(b)
     it, rel, fb = fcg(csr, b, x, net=net, tol=1e-10, max_iter=3000, keep=4)
     assert rel <= 1e-10 and not fb
     # random weights three times their initial scale make a network whose output swamps B r with
-    # noise: FCG stalls on it, the safeguard drops it, and the solve converges on block Jacobi
+    # noise: FCG stalls on it, the safeguard drops it and restarts from the true residual, and the
+    # solve converges on block Jacobi within the network's iterations plus block Jacobi's own
     bad = UNet(p, seed=0, kref=output_scale(R, E), levels=3, operator=csr)
     bad.set_params(3.0 * U.init_params(7, 3))
     x = torch.zeros_like(b)
     it, rel, fb = fcg(csr, b, x, net=bad, tol=1e-10, max_iter=3000, keep=4)
     assert rel <= 1e-10 and not fb
     assert bad.stat(2) == 1 and bad.stat(1) < it
+    assert it <= bad.stat(1) + runs[0][0] + 50, (it, bad.stat(1), runs[0][0])
 
 
 def test_odd_network_is_odd_in_the_residual(cuda):
