@@ -253,11 +253,12 @@ int32_t child_ranges(const fc_chol *h, int64_t s, int lo, int hi, std::vector<in
 
 // The assembly tile's columns: an FP32 front's tiles are twice as wide (the same bytes).
 int assemble_cols(const fc_chol *h) { return h->fp32 ? fc::ASSEMBLE_COLS_F32 : fc::ASSEMBLE_COLS; }
+int assemble_rows(const fc_chol *h) { return h->fp32 ? fc::ASSEMBLE_ROWS_F32 : fc::ASSEMBLE_ROWS; }
 
 // Assembly tiles of supernode s (see assemble_kernel): ASM_L over the L panel's columns, or the
 // update matrix's columns as ASM_U (only tiles some child lands in: the rest keep what the GEMM
 // stored) or ASM_U_PRODUCT (all tiles). A block of assemble_cols(h) columns is cut into row tiles
-// of ASSEMBLE_ROWS from its first column down; each tile's child ranges come from `at`, per child
+// of assemble_rows(h) from its first column down; each tile's child ranges come from `at`, per child
 // the first row of its update matrix whose place in the front is >= r, for every r in [0, m].
 void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::AssembleTask> &out,
                     std::vector<int4> &ranges) {
@@ -280,8 +281,8 @@ void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::Assem
   const int cols = assemble_cols(h);
   for (int j0 = jlo; j0 < jhi; j0 += cols) {
     const int j1 = std::min(jhi, j0 + cols);
-    for (int i0 = j0; i0 < m; i0 += fc::ASSEMBLE_ROWS) {
-      const int i1 = std::min(m, i0 + fc::ASSEMBLE_ROWS);
+    for (int i0 = j0; i0 < m; i0 += assemble_rows(h)) {
+      const int i1 = std::min(m, i0 + assemble_rows(h));
       const int32_t base = (int32_t)ranges.size();
       bool touched = false;
       for (int64_t q = 0; q < nk; ++q) {

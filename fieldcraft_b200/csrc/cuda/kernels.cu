@@ -49,7 +49,7 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
 
 // ---- front assembly ----------------------------------------------------------------------------
 // One tile of supernode s's front: columns [j0, j1) (at most COLS) by rows [i0, i1) (at
-// most ASSEMBLE_ROWS), built in shared memory and written once. The tile starts as
+// most ROWS, a thread each), built in shared memory and written once. The tile starts as
 //   ASM_L          zero, then A's entries (columns of the L panel, assembled before the panel is
 //                  factored; with a scale, the entries of S A S, S = diag(A)^-1/2);
 //   ASM_U          the update matrix's tile as its GEMM stored it (-L21 L21^T);
@@ -61,13 +61,13 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
 // fall in the tile; only its lower triangle (row >= column) is read. No destination is read and
 // written through global memory: the child's rows and values stream in coalesced, the scatter is
 // to shared memory, and every entry of the tile's lower part is stored once.
-template <class T, int COLS>
-__global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
+template <class T, int COLS, int ROWS>
+__global__ void __launch_bounds__(ROWS, ROWS == 256 ? 6 : 8)
     assemble_kernel(Tree t, const double *__restrict__ val, const AssembleTask *__restrict__ tasks,
                     const int4 *__restrict__ ranges) {
-  constexpr int WARPS = ASSEMBLE_THREADS / 32, CPW = COLS / WARPS;  // child columns a warp takes
-  static_assert(ASSEMBLE_ROWS == ASSEMBLE_THREADS && CPW * WARPS == COLS && CPW >= 1, "tile shape");
-  __shared__ T tile[COLS][ASSEMBLE_ROWS];
+  constexpr int THREADS = ROWS, WARPS = THREADS / 32, CPW = COLS / WARPS;  // child columns a warp takes
+  static_assert(CPW * WARPS == COLS && CPW >= 1, "tile shape");
+  __shared__ T tile[COLS][ROWS];
   __shared__ T lj[ASSEMBLE_THIN][COLS];
   __shared__ int4 s_rg[ASSEMBLE_KIDS];
   __shared__ KidMeta s_km[ASSEMBLE_KIDS];
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
   // thread tid owns tile row tid for the initial values and the store
   const int ii = tid, r = i0 + tid;
   if (task.mode == ASM_U_PRODUCT) {
-    for (int q = tid; q < w * nc; q += ASSEMBLE_THREADS) {
+    for (int q = tid; q < w * nc; q += THREADS) {
       const int k = q / nc, jj = q - k * nc;
       lj[k][jj] = Ls[(int64_t)k * m + j0 + jj];
     }
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
     for (int jj = 0; jj < COLS; ++jj) tile[jj][ii] = T(0);
     __syncthreads();
     // A's entries of the tile: the block's entries are sorted by row, [e0, e1) are this tile's
-    for (int64_t e = task.e0 + tid; e < task.e1; e += ASSEMBLE_THREADS) {
+    for (int64_t e = task.e0 + tid; e < task.e1; e += THREADS) {
       const int p = (int)(t.a_dst[e] - task.loff), J = p / m, row = p - J * m;
       const double a = t.scale ? val[t.a_src[e]] * t.scale[t.a_row[e]] * t.scale[t.a_col[e]] : val[t.a_src[e]];
       tile[J - j0][row - i0] = T(a);
@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
       if (g.x + warp < g.y) {
         const KidMeta km = q < ASSEMBLE_KIDS ? s_km[q] : t.kid_meta[task.k0 + q];
         const int32_t *rel = t.rel + km.rel_off;
-        int at[CPW][ASSEMBLE_ROWS / 32], jjs[CPW];
-        T v[CPW][ASSEMBLE_ROWS / 32];
+        int at[CPW][ROWS / 32], jjs[CPW];
+        T v[CPW][ROWS / 32];
 #pragma unroll
         for (int c = 0; c < CPW; ++c) {
           const int jc = g.x + warp + WARPS * c;
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
             const int a = g.z > jc ? g.z : jc;
             jjs[c] = rel[jc] - j0;
 #pragma unroll
-            for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k) {
+            for (int k = 0; k < ROWS / 32; ++k) {
               const int ic = a + lane + 32 * k;
               at[c][k] = -1;
               if (ic < g.w) {
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(ASSEMBLE_THREADS, COLS == 8 ? 6 : 4)
         for (int c = 0; c < CPW; ++c)
           if (jjs[c] >= 0) {
 #pragma unroll
-            for (int k = 0; k < ASSEMBLE_ROWS / 32; ++k)
+            for (int k = 0; k < ROWS / 32; ++k)
               if (at[c][k] >= 0) tile[jjs[c]][at[c][k] - i0] += v[c][k];
           }
       }
@@ -1521,9 +1521,10 @@ void launch_assemble(const Tree &t, bool fp32, const double *upper_val, const As
   if (count <= 0) return;
   configure_kernels();
   if (fp32)
-    assemble_kernel<float, ASSEMBLE_COLS_F32><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
+    assemble_kernel<float, ASSEMBLE_COLS_F32, ASSEMBLE_ROWS_F32>
+        <<<count, ASSEMBLE_ROWS_F32, 0, st>>>(t, upper_val, tasks, ranges);
   else
-    assemble_kernel<double, ASSEMBLE_COLS><<<count, ASSEMBLE_THREADS, 0, st>>>(t, upper_val, tasks, ranges);
+    assemble_kernel<double, ASSEMBLE_COLS, ASSEMBLE_ROWS><<<count, ASSEMBLE_ROWS, 0, st>>>(t, upper_val, tasks, ranges);
 }
 
 void launch_panel(const Tree &t, bool fp32, const double *upper_val, const PanelTask *tasks, int count,

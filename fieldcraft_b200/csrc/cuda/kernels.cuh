@@ -16,10 +16,11 @@ constexpr int PANEL_ROWS = 128;  // rows of a panel solved by one CTA (64 at a t
 // A front is assembled by tiles of ASSEMBLE_COLS columns by ASSEMBLE_ROWS rows, one CTA each
 // (a thread per row, a warp per child column); a supernode at most ASSEMBLE_THIN columns wide has
 // its update matrix formed by the assembly itself instead of by a GEMM.
-constexpr int ASSEMBLE_COLS = 8, ASSEMBLE_ROWS = 256, ASSEMBLE_THREADS = 256, ASSEMBLE_THIN = 16;
-// An FP32 front (mixed precision) is assembled by tiles of twice the columns: the same bytes a tile,
-// half the tiles.
-constexpr int ASSEMBLE_COLS_F32 = 16;
+constexpr int ASSEMBLE_COLS = 8, ASSEMBLE_ROWS = 256, ASSEMBLE_THIN = 16;
+// An FP32 front (mixed precision) is assembled by tiles of 16 columns by 128 rows (a thread a row,
+// each warp four child columns): the bytes of a 256-row FP64 tile over half its rows, and eight
+// CTAs an SM.
+constexpr int ASSEMBLE_COLS_F32 = 16, ASSEMBLE_ROWS_F32 = 128;
 constexpr int ASSEMBLE_KIDS = 8;  // children whose ranges a tile keeps in shared memory (the rest: global)
 constexpr int SPLIT_K = 512;  // K chunk of the persistent solve's split products
 // The solve applies the inverse of a supernode's diagonal block SB columns at a time: the inverses
