@@ -149,6 +149,7 @@ struct fc_chol {
   bool solve_cluster = false;
   bool solve_narrow = true;  // the solve's products in 64 x 8 / 64 x 16 tiles for up to 16 right-hand sides
   bool solve_deep = true;    // the solve's short product launches with the deeper cp.async ring
+  bool asm_first = true;     // wide update matrices: children added before the panels (lane 1)
   DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
   int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
   int dag_grid = 0;
@@ -257,7 +258,7 @@ int assemble_rows(const fc_chol *h) { return h->fp32 ? fc::ASSEMBLE_ROWS_F32 : f
 
 // Assembly tiles of supernode s (see assemble_kernel): ASM_L over the L panel's columns, or the
 // update matrix's columns as ASM_U (only tiles some child lands in: the rest keep what the GEMM
-// stored) or ASM_U_PRODUCT (all tiles). A block of assemble_cols(h) columns is cut into row tiles
+// stored), ASM_U_PRODUCT or ASM_U_FIRST (all tiles). A block of assemble_cols(h) columns is cut into row tiles
 // of assemble_rows(h) from its first column down; each tile's child ranges come from `at`, per child
 // the first row of its update matrix whose place in the front is >= r, for every r in [0, m].
 void assemble_tiles(const fc_chol *h, int64_t s, int mode, std::vector<fc::AssembleTask> &out,
@@ -475,12 +476,40 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
         }
     }
   };
+  // a wide supernode (more than ASSEMBLE_THIN columns) with children gets its update matrix's
+  // children contributions first (ASM_U_FIRST, on lane 1 beside its panels) and its update GEMM
+  // subtracts -L21 L21^T from them; without children the GEMM stores -L21 L21^T
+  auto u_first = [&](int64_t s) {
+    return h->asm_first && h->height[s] > h->width[s] && h->width[s] > fc::ASSEMBLE_THIN &&
+           h->kid_ptr[s + 1] > h->kid_ptr[s];
+  };
   for (size_t l = 0; l < lv.size(); ++l) {
     join();
     const auto &S = lv[l];
     int64_t off = (int64_t)asm_t.size();
     for (int64_t s : S) assemble_tiles(h, s, fc::ASM_L, asm_t, ranges);
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
+    // the wide update matrices' children contributions, on lane 1 once the level's children are
+    // complete (after the last lane-0 launch so far), beside the level's panels
+    int pre_asm = -1;
+    {
+      const int64_t uo = (int64_t)asm_t.size();
+      for (int64_t s : S)
+        if (u_first(s)) assemble_tiles(h, s, fc::ASM_U_FIRST, asm_t, ranges);
+      if ((int64_t)asm_t.size() > uo) {
+        int prev0 = -1;
+        for (int q = (int)h->program.size() - 1; q >= 0 && prev0 < 0; --q)
+          if (h->program[q].lane == 0) prev0 = q;
+        push(h->program, K_ASSEMBLE, uo, (int64_t)asm_t.size() - uo, (int)l);
+        Launch &a = h->program.back();
+        a.lane = 1;
+        if (prev0 >= 0) {
+          a.dep = prev0;
+          h->program[prev0].record = true;
+        }
+        pre_asm = (int)h->program.size() - 1;
+      }
+    }
     int P = 0;
     for (int64_t s : S) P = std::max(P, (h->width[s] + NB - 1) / NB);
     // Two-level blocking: panels are grouped in outer blocks of OUTER_PANELS. A panel's update of
@@ -646,7 +675,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             fc::TcTask g{};
             g.map = map, g.bi = bi, g.bj = bj;
             g.M = std::min(fc::GEMM_TC_M, u - bi), g.N = std::min(fc::GEMM_TC_N, u - bj), g.K = w, g.wpad = wpad;
-            g.flags = (bi == bj ? 1 : 0) | 2;
+            g.flags = (bi == bj ? 1 : 0) | (u_first(s) ? 0 : 2);
             g.C = static_cast<float *>(Up(uo + bi + (int64_t)bj * u));
             g.c_sj = u;
             tc_t.push_back(g);
@@ -655,6 +684,10 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       h->pack_len = std::max(h->pack_len, std::max(at, blk_at));
       push(h->program, K_PACK_TC, po, (int64_t)pack_t.size() - po, (int)l);
       push(h->program, K_GEMM_TC, to, (int64_t)tc_t.size() - to, (int)l);
+      if (pre_asm >= 0 && (int64_t)tc_t.size() > to) {  // the products subtract from the children's sum
+        h->program.back().dep = pre_asm;
+        h->program[pre_asm].record = true;
+      }
     } else {
       int64_t go = (int64_t)gemm_t.size();
       for (int64_t s : S) {
@@ -671,11 +704,19 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
             g.M = std::min(fc::GEMM_TM, u - bi);
             g.N = std::min(fc::GEMM_TN, u - bj);
             g.K = w;
-            g.flags = (bi == bj ? 1 : 0) | 2;
+            g.flags = (bi == bj ? 1 : 0) | (u_first(s) ? 0 : 2);
             gemm_t.push_back(g);
           }
       }
       push(h->program, K_GEMM, go, (int64_t)gemm_t.size() - go, (int)l);
+      if (pre_asm >= 0 && (int64_t)gemm_t.size() > go) {
+        // the products subtract from the children's sum (lane 1); they also read the columns the
+        // level's lane-1 updates wrote, which come after the children's sum on that lane
+        Launch &g = h->program.back();
+        g.dep = pending_join >= 0 ? pending_join : pre_asm;
+        h->program[g.dep].record = true;
+        pending_join = -1;
+      }
     }
     // the children's contributions to the update matrices, on top of -L21 L21^T
     // (a thin supernode's update matrix is formed here whole, -L21 L21^T included)
@@ -685,7 +726,7 @@ void plan_factor(fc_chol *h, const std::vector<std::vector<int64_t>> &lv, std::v
       if (m == w) continue;
       if (w <= fc::ASSEMBLE_THIN)
         assemble_tiles(h, s, fc::ASM_U_PRODUCT, asm_t, ranges);
-      else if (h->kid_ptr[s + 1] > h->kid_ptr[s])
+      else if (h->kid_ptr[s + 1] > h->kid_ptr[s] && !u_first(s))
         assemble_tiles(h, s, fc::ASM_U, asm_t, ranges);
     }
     push(h->program, K_ASSEMBLE, off, (int64_t)asm_t.size() - off, (int)l);
@@ -2893,6 +2934,13 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
       h->solve_deep = value == 1;
       replan();
       return FC_OK;
+    case FC_OPTION_CHILDREN_FIRST: {
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      if (h->asm_first == (value == 1)) return FC_OK;
+      h->asm_first = value == 1;
+      fc_status ignore{};
+      return h->ldlt ? FC_OK : plan_factor_upload(h, &ignore);
+    }
     case FC_OPTION_FP32_UPDATES: {
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       if (h->tc == (value == 0)) return FC_OK;

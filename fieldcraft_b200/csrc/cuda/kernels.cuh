@@ -71,7 +71,9 @@ struct Tree {
 // Front tile columns [j0, j1) x rows [i0, i1) of supernode s; ranges[q] (from `ranges`) is child
 // q's {columns lo, hi, rows lo, hi} of its update matrix that land in the tile; [e0, e1) are the
 // input entries of an ASM_L tile.
-enum AssembleMode : int32_t { ASM_L = 0, ASM_U = 1, ASM_U_PRODUCT = 2 };
+// ASM_U_FIRST: an update matrix's tile from zero with the children's contributions, written
+// before its supernode's panels; the update GEMM then subtracts -L21 L21^T from it.
+enum AssembleMode : int32_t { ASM_L = 0, ASM_U = 1, ASM_U_PRODUCT = 2, ASM_U_FIRST = 3 };
 struct AssembleTask {
   int32_t s, j0, j1, i0, i1, mode, ranges, nk;  // nk: the supernode's children
   int64_t e0, e1;

@@ -222,7 +222,12 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *   FC_OPTION_SOLVE_DEEP       1 (default): with at most 16 right-hand sides, the level-by-level
  *                              solve's product launches of fewer CTAs than two per SM run with an
  *                              8-stage copy ring (more bytes in flight a CTA); 0: the factor's
- *                              3-stage ring. The same bits. */
+ *                              3-stage ring. The same bits.
+ *   FC_OPTION_CHILDREN_FIRST   1 (default): a supernode wider than 16 columns with children gets
+ *                              its update matrix's children contributions summed first, beside
+ *                              its panels, and its update product subtracts -L21 L21^T from them;
+ *                              0: the product stores -L21 L21^T and the children are added after
+ *                              it (re-plans the factorisation; the factor agrees to rounding). */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3
@@ -232,6 +237,7 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
 #define FC_OPTION_SOLVE_CLUSTER 7
 #define FC_OPTION_SOLVE_NARROW 8
 #define FC_OPTION_SOLVE_DEEP 9
+#define FC_OPTION_CHILDREN_FIRST 10
 int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
 /* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
  * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |

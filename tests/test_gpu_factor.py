@@ -170,6 +170,31 @@ def test_narrow_solve_tiles_give_the_same_bits(cuda, precision):
     f.close()
 
 
+@pytest.mark.parametrize("precision", [FP64, FP32_IR], ids=["fp64", "fp32_ir"])
+def test_children_first_update_matrices(cuda, precision):
+    """The wide supernodes' update matrices take their children's contributions first (beside the
+    panels) and the update product subtracts from them (the default), or the product stores and
+    the children are added after it: on the 16^3 block both factors agree to rounding (1e-12 of
+    the largest entry in FP64, 1e-5 in FP32), the FP64 one matches the oracle, and the factorisation
+    stays bit for bit repeatable."""
+    p = problems.lognormal_block(16, nrhs=1)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62), precision=precision)
+    vals = {}
+    for on in (1, 0, 1):
+        f.option(Factor.CHILDREN_FIRST, on)
+        f.factor(up.val)
+        vals.setdefault(on, []).append(f.values())
+    assert np.array_equal(vals[1][0], vals[1][1])
+    big = np.max(np.abs(vals[0][0]))
+    assert np.max(np.abs(vals[1][0] - vals[0][0])) <= (1e-12 if precision == FP64 else 1e-5) * big
+    if precision == FP64:
+        _, ref = oracle_factor(p.csr)
+        rv = ref.values()
+        assert np.max(np.abs(vals[1][0] - rv)) <= FACTOR_TOL * np.max(np.abs(rv))
+    f.close()
+
+
 def test_cluster_split_solve(cuda):
     """The 16^3 block's short solve products run with K split over 8-CTA clusters (the default) or
     in chunks of separate CTAs: both match the oracle; the cluster form is bit for bit the same on
