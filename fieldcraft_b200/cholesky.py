@@ -313,7 +313,7 @@ class Factor:
     # fc_chol_option: the solve's schedule (0 level by level, 1 persistent), the persistent solve's
     # wait limit in nanoseconds, and (tests) a planted dependency that no task meets
     SOLVE_SCHEDULE, WAIT_LIMIT_NS, PLANT_UNMET_WAIT, TRACE, REFINEMENT, FP32_UPDATES, SOLVE_CLUSTER, SOLVE_NARROW, \
-        SOLVE_DEEP, CHILDREN_FIRST = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
+        SOLVE_DEEP, CHILDREN_FIRST, SOLVE_PDL = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
 
     def option(self, option: int, value: int):
         if _lib.load().fc_chol_option(self.handle, int(option), int(value)) != 0:

@@ -150,6 +150,7 @@ struct fc_chol {
   bool solve_narrow = true;  // the solve's products in 64 x 8 / 64 x 16 tiles for up to 16 right-hand sides
   bool solve_deep = true;    // the solve's short product launches with the deeper cp.async ring
   bool asm_first = true;     // wide update matrices: children added before the panels (lane 1)
+  bool solve_pdl = false;    // the level-by-level solve's launches as programmatic dependents
   DeviceBuf d_dtasks, d_ddeps, d_dranges, d_dcount, d_dctl;  // d_dranges: the children's records
   int64_t dag_fwd = 0, dag_bwd = 0, dag_counters = 0;
   int dag_grid = 0;
@@ -2379,6 +2380,11 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
   const int short_launch = h->solve_deep && narrow ? 2 * prop_sms(h->device) : 0;
   const bool lanes = events && ev && h->side;
   const std::vector<char> side = lanes ? beside(prog) : std::vector<char>(prog.size(), 0);
+  // (option) every launch of the program as a programmatic dependent of its stream's previous
+  // kernel: its CTAs are scheduled while that kernel finishes and load their task, L and inverse
+  // tiles before waiting for it (the program's first kernel follows the ordinary permutation
+  // launch, which starts only after everything before the solve is done)
+  const bool pdl = h->solve_pdl;
   bool forked = false;
   int level = INT_MIN;
   for (size_t q = 0; q < prog.size(); ++q) {
@@ -2400,35 +2406,34 @@ void run_solve_program(fc_chol *h, const std::vector<Launch> &prog, const SolveB
     Mark mark(h, l.kind + 16, l.level, l.count);
     switch (l.kind) {
       case K_SOLVE_ASSEMBLE:
-        fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st);
+        fc::launch_solve_assemble(t, b.x, b.v, b.voff, R, b.rows + l.off, b.ranges, l.count, st, pdl);
         break;
       case K_SOLVE_FWD:  // the diagonal blocks' inverses applied (FP64 throughout)
       case K_SOLVE_BWD:
         if (l.width == 1)
           fc::launch_gemm_cluster(b.gemm + l.off, l.count, false, st, b.part, b.tcount);
         else if (l.count < short_launch)
-          fc::launch_gemm_solve(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount);
+          fc::launch_gemm_solve(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount, pdl);
         else if (narrow)
-          fc::launch_gemm_narrow(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount);
+          fc::launch_gemm_narrow(b.gemm + l.off, l.count, false, R, st, b.part, b.tcount, pdl);
         else
-          fc::launch_gemm(b.gemm + l.off, l.count, fc::GemmKind::F64, st, b.part, b.tcount);
+          fc::launch_gemm_pdl(b.gemm + l.off, l.count, false, st, b.part, b.tcount, pdl);
         break;
       case K_GEMM:
         if (l.width == 1)
           fc::launch_gemm_cluster(b.gemm + l.off, l.count, h->fp32, st, b.part, b.tcount);
         else if (l.count < short_launch)
-          fc::launch_gemm_solve(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount);
+          fc::launch_gemm_solve(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount, pdl);
         else if (narrow)
-          fc::launch_gemm_narrow(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount);
+          fc::launch_gemm_narrow(b.gemm + l.off, l.count, h->fp32, R, st, b.part, b.tcount, pdl);
         else
-          fc::launch_gemm(b.gemm + l.off, l.count, h->fp32 ? fc::GemmKind::F32A_F64 : fc::GemmKind::F64, st, b.part,
-                          b.tcount);
+          fc::launch_gemm_pdl(b.gemm + l.off, l.count, h->fp32, st, b.part, b.tcount, pdl);
         break;
       case K_SOLVE_THIN_FWD:
-        fc::launch_thin_fwd(t, h->fp32, b.x, b.x2, b.v, b.voff, R, b.lg, b.thin + l.off, b.tranges, l.count, st);
+        fc::launch_thin_fwd(t, h->fp32, b.x, b.x2, b.v, b.voff, R, b.lg, b.thin + l.off, b.tranges, l.count, st, pdl);
         break;
       case K_SOLVE_THIN_BWD:
-        fc::launch_thin_bwd(t, h->fp32, b.x, b.x2, R, b.lg, b.tbwd + l.off, b.tpart, b.tcount, l.count, st);
+        fc::launch_thin_bwd(t, h->fp32, b.x, b.x2, R, b.lg, b.tbwd + l.off, b.tpart, b.tcount, l.count, st, pdl);
         break;
     }
     ++launches;
@@ -2932,6 +2937,11 @@ int fc_chol_option(fc_chol *h, int32_t option, int64_t value) {
     case FC_OPTION_SOLVE_DEEP:
       if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
       h->solve_deep = value == 1;
+      replan();
+      return FC_OK;
+    case FC_OPTION_SOLVE_PDL:
+      if (value != 0 && value != 1) return FC_INVALID_ARGUMENT;
+      h->solve_pdl = value == 1;
       replan();
       return FC_OK;
     case FC_OPTION_CHILDREN_FIRST: {

@@ -643,11 +643,17 @@ __device__ __forceinline__ void gemm_mainloop(const GemmTask *tp, int kbeg, int 
     else
       lb.load(Bs[stage], kb, K, bbase);
   };
+  // the first stages' A tiles go out together, before any B tile and before pdl_wait (A is a
+  // factor or inverse block, which no kernel of a solve writes; a factorisation's launches are
+  // ordinary, pdl_wait returns at once); the first commit group holds them with the first B tile.
+  // A's bytes in flight from the start: with few right-hand sides, where A is nearly all of a
+  // tile's bytes, the FP64 solve of the 48^3 block took 7.8 ms instead of 9.6
+  for (int st = 0; st < STAGES - 1; ++st)
+    if (st < nk) la.load(As[st], st * GEMM_KC, K, abase);
+  pdl_wait();
+  pdl_trigger();
   for (int st = 0; st < STAGES - 1; ++st) {
-    if (st < nk) {
-      la.load(As[st], st * GEMM_KC, K, abase);
-      load_b(st, st * GEMM_KC);
-    }
+    if (st < nk) load_b(st, st * GEMM_KC);
     cp_async_commit();
   }
   for (int kt = 0; kt < nk; ++kt) {
@@ -757,11 +763,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, STAGES == GEMM_STAGES ? 6 : 2)
 #pragma unroll
   for (int c = 0; c < NF; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
   const int nk = (K + GEMM_KC - 1) / GEMM_KC;
+  // as in gemm_mainloop: the first stages' A tiles before pdl_wait, in the first commit group
+  for (int st = 0; st < STAGES - 1; ++st)
+    if (st < nk) la.load(As[st], st * GEMM_KC, K, abase);
+  pdl_wait();
+  pdl_trigger();
   for (int st = 0; st < STAGES - 1; ++st) {
-    if (st < nk) {
-      la.load(As[st], st * GEMM_KC, K, abase);
-      load_b(st, st * GEMM_KC);
-    }
+    if (st < nk) load_b(st, st * GEMM_KC);
     cp_async_commit();
   }
   for (int kt = 0; kt < nk; ++kt) {
@@ -1016,6 +1024,8 @@ __global__ void __launch_bounds__(256) solve_assemble_kernel(Tree t, double *__r
   double *vs = v + voff[s];
   const int tid = threadIdx.x;
   const int64_t z0 = task.i0 > w ? task.i0 : w;
+  pdl_wait();
+  pdl_trigger();
   for (int64_t e = tid; e < (task.i1 - z0) * R; e += blockDim.x) vs[(z0 - w) * R + e] = 0.0;
   __syncthreads();
   const int64_t k0 = t.kid_ptr[s], k1 = t.kid_ptr[s + 1];
@@ -1066,10 +1076,16 @@ __global__ void __launch_bounds__(THIN_THREADS) thin_fwd_kernel(Tree t, const do
 #pragma unroll
   for (int q = 0; q < SOLVE_THIN * 64 / THIN_THREADS; ++q) {
     const int e = tid + q * THIN_THREADS, k = e >> 6, j = e & 63;
-    if (k < w && j < RP) xs[(k << lg) + j] = j < nj ? x[(f + k) * R + j0 + j] : 0.0;
     if (k < w) lt[k * THIN_ROWS + j] = j < nr ? (double)Ls[(int64_t)k * m + i0 + j] : 0.0;
   }
   if (tid < w * w) di[tid] = t.Dinv[task.dinv + tid];
+  pdl_wait();  // L and the inverse above; x and the update vectors below
+  pdl_trigger();
+#pragma unroll
+  for (int q = 0; q < SOLVE_THIN * 64 / THIN_THREADS; ++q) {
+    const int e = tid + q * THIN_THREADS, k = e >> 6, j = e & 63;
+    if (k < w && j < RP) xs[(k << lg) + j] = j < nj ? x[(f + k) * R + j0 + j] : 0.0;
+  }
   __syncthreads();
   for (int kp = k0; kp < k1; ++kp) {
     const int4 g = ranges[task.ranges + (kp - k0)];
@@ -1168,6 +1184,8 @@ __global__ void __launch_bounds__(THIN_THREADS) thin_bwd_kernel(Tree t, double *
     const int e = tid + q * THIN_THREADS, k = e / THIN_CHUNK, i = e - k * THIN_CHUNK;
     if (k < w && i < n) lt[i * SOLVE_THIN + k] = (double)Lb[(int64_t)k * m + task.k0 + i];
   }
+  pdl_wait();  // the row list and L above; x, x2, the partial sums and counters below
+  pdl_trigger();
   __syncthreads();
   double acc[SOLVE_THIN][2];
 #pragma unroll
@@ -1537,6 +1555,32 @@ void launch_panel(const Tree &t, bool fp32, const double *upper_val, const Panel
     panel_kernel<double><<<count, PANEL_THREADS, panel_smem<double>(p8max), st>>>(t, upper_val, tasks, status, p8max);
 }
 
+// A launch of `count` CTAs, as a programmatic dependent of the stream's previous kernel when pdl.
+template <class... P, class... A>
+void launch_ex(void (*kernel)(P...), int count, int threads, size_t smem, cudaStream_t st, bool pdl, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)count);
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+void launch_gemm_pdl(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part, int32_t *counters,
+                     bool pdl) {
+  if (count <= 0) return;
+  configure_kernels();
+  if (fp32_a)
+    launch_ex(gemm_kernel<float>, count, GEMM_THREADS, gemm_smem<float>(), st, pdl, tasks, part, counters);
+  else
+    launch_ex(gemm_kernel<double>, count, GEMM_THREADS, gemm_smem<double>(), st, pdl, tasks, part, counters);
+}
+
 void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st, double *part, int32_t *counters) {
   if (count <= 0) return;
   configure_kernels();
@@ -1551,43 +1595,36 @@ void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t s
   }
 }
 
-void launch_gemm_solve(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
-                       int32_t *counters) {
+template <int S>
+void launch_narrow(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
+                   int32_t *counters, bool pdl) {
   if (count <= 0) return;
   configure_kernels();
-  constexpr int S = SOLVE_STAGES;
   if (cols <= 8) {
     if (fp32_a)
-      gemm_narrow_kernel<float, 8, S><<<count, GEMM_THREADS, gemm_narrow_smem<float, 8, S>(), st>>>(tasks, part, counters);
+      launch_ex(gemm_narrow_kernel<float, 8, S>, count, GEMM_THREADS, gemm_narrow_smem<float, 8, S>(), st, pdl, tasks,
+                part, counters);
     else
-      gemm_narrow_kernel<double, 8, S><<<count, GEMM_THREADS, gemm_narrow_smem<double, 8, S>(), st>>>(tasks, part,
-                                                                                                      counters);
+      launch_ex(gemm_narrow_kernel<double, 8, S>, count, GEMM_THREADS, gemm_narrow_smem<double, 8, S>(), st, pdl,
+                tasks, part, counters);
   } else {
     if (fp32_a)
-      gemm_narrow_kernel<float, 16, S><<<count, GEMM_THREADS, gemm_narrow_smem<float, 16, S>(), st>>>(tasks, part,
-                                                                                                      counters);
+      launch_ex(gemm_narrow_kernel<float, 16, S>, count, GEMM_THREADS, gemm_narrow_smem<float, 16, S>(), st, pdl,
+                tasks, part, counters);
     else
-      gemm_narrow_kernel<double, 16, S><<<count, GEMM_THREADS, gemm_narrow_smem<double, 16, S>(), st>>>(tasks, part,
-                                                                                                        counters);
+      launch_ex(gemm_narrow_kernel<double, 16, S>, count, GEMM_THREADS, gemm_narrow_smem<double, 16, S>(), st, pdl,
+                tasks, part, counters);
   }
 }
 
+void launch_gemm_solve(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
+                       int32_t *counters, bool pdl) {
+  launch_narrow<SOLVE_STAGES>(tasks, count, fp32_a, cols, st, part, counters, pdl);
+}
+
 void launch_gemm_narrow(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
-                        int32_t *counters) {
-  if (count <= 0) return;
-  configure_kernels();
-  if (cols <= 8) {
-    if (fp32_a)
-      gemm_narrow_kernel<float, 8><<<count, GEMM_THREADS, gemm_narrow_smem<float, 8>(), st>>>(tasks, part, counters);
-    else
-      gemm_narrow_kernel<double, 8><<<count, GEMM_THREADS, gemm_narrow_smem<double, 8>(), st>>>(tasks, part, counters);
-  } else {
-    if (fp32_a)
-      gemm_narrow_kernel<float, 16><<<count, GEMM_THREADS, gemm_narrow_smem<float, 16>(), st>>>(tasks, part, counters);
-    else
-      gemm_narrow_kernel<double, 16><<<count, GEMM_THREADS, gemm_narrow_smem<double, 16>(), st>>>(tasks, part,
-                                                                                                  counters);
-  }
+                        int32_t *counters, bool pdl) {
+  launch_narrow<GEMM_STAGES>(tasks, count, fp32_a, cols, st, part, counters, pdl);
 }
 
 void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part,
@@ -1602,30 +1639,30 @@ void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStre
 }
 
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R, const RowTask *tasks,
-                           const int2 *ranges, int count, cudaStream_t st) {
+                           const int2 *ranges, int count, cudaStream_t st, bool pdl) {
   if (count <= 0) return;
   configure_kernels();
-  solve_assemble_kernel<<<count, 256, 0, st>>>(t, x, v, voff, R, tasks, ranges);
+  launch_ex(solve_assemble_kernel, count, 256, 0, st, pdl, t, x, v, voff, R, tasks, ranges);
 }
 
 void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, double *v, const int64_t *voff, int R,
-                     int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st) {
+                     int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st, bool pdl) {
   if (count <= 0) return;
   configure_kernels();
   if (fp32)
-    thin_fwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, v, voff, R, lg, tasks, ranges);
+    launch_ex(thin_fwd_kernel<float>, count, THIN_THREADS, 0, st, pdl, t, x, x2, v, voff, R, lg, tasks, ranges);
   else
-    thin_fwd_kernel<double><<<count, THIN_THREADS, 0, st>>>(t, x, x2, v, voff, R, lg, tasks, ranges);
+    launch_ex(thin_fwd_kernel<double>, count, THIN_THREADS, 0, st, pdl, t, x, x2, v, voff, R, lg, tasks, ranges);
 }
 
 void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int R, int lg, const ThinBwdTask *tasks,
-                     double *part, int32_t *counters, int count, cudaStream_t st) {
+                     double *part, int32_t *counters, int count, cudaStream_t st, bool pdl) {
   if (count <= 0) return;
   configure_kernels();
   if (fp32)
-    thin_bwd_kernel<float><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
+    launch_ex(thin_bwd_kernel<float>, count, THIN_THREADS, 0, st, pdl, t, x, x2, R, lg, tasks, part, counters);
   else
-    thin_bwd_kernel<double><<<count, THIN_THREADS, 0, st>>>(t, x, x2, R, lg, tasks, part, counters);
+    launch_ex(thin_bwd_kernel<double>, count, THIN_THREADS, 0, st, pdl, t, x, x2, R, lg, tasks, part, counters);
 }
 
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,

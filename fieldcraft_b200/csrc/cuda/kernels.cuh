@@ -31,6 +31,18 @@ constexpr int SB = 2048;
 // The solve's short products split K over a cluster of this many CTAs (gemm_cluster_kernel).
 constexpr int SOLVE_CLUSTER = 8;
 
+// Programmatic dependent launch. The solve's kernels may be launched so that a kernel's CTAs are
+// scheduled while the kernel before it in the stream is still running. A CTA reads before
+// pdl_wait() only data that no kernel of the solve writes (task lists, row lists, L, the diagonal
+// blocks' inverses) and reads or writes the solve's vectors, partial sums and counters only after
+// it; pdl_wait() returns once every grid the kernel depends on has completed with its writes
+// visible (at once in a kernel launched the ordinary way). Every CTA passes pdl_wait() before it
+// exits, so a kernel completes only after its predecessors have. Right after its wait a CTA lets
+// the next kernel be scheduled (pdl_trigger): at most one kernel's CTAs wait at a time, not a
+// chain of them holding the SMs.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // A child as its parent's assembly reads it: its update matrix (offset, height) and relative map.
 struct KidMeta {
   int64_t uoff, rel_off;
@@ -255,26 +267,30 @@ void launch_panel(const Tree &t, bool fp32, const double *upper_val, const Panel
 // part and counters: the partial sums and counters of split tasks (flag 8), null when there are none.
 void launch_gemm(const GemmTask *tasks, int count, GemmKind kind, cudaStream_t st, double *part = nullptr,
                  int32_t *counters = nullptr);
+// pdl: launch as a programmatic dependent of the kernel before it in the stream (the solve's
+// launches; the kernels keep the rules of pdl_wait).
+void launch_gemm_pdl(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part, int32_t *counters,
+                     bool pdl);
 // The solve's products with at most 16 right-hand sides (every task's N <= cols): 64 x 8 or 64 x 16
 // tiles, each element's bits those of launch_gemm's F64 / F32A_F64 kernels.
 void launch_gemm_narrow(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
-                        int32_t *counters);
+                        int32_t *counters, bool pdl = false);
 // The solve's products with at most 16 right-hand sides (every task's N <= cols <= 16) in 64 x 8 /
 // 64 x 16 tiles with a deeper cp.async ring: the same bits as launch_gemm_narrow.
 void launch_gemm_solve(const GemmTask *tasks, int count, bool fp32_a, int cols, cudaStream_t st, double *part,
-                       int32_t *counters);
+                       int32_t *counters, bool pdl = false);
 // The same tasks (FP64 B and C; A FP64 or FP32) with K split over clusters of SOLVE_CLUSTER CTAs.
 void launch_gemm_cluster(const GemmTask *tasks, int count, bool fp32_a, cudaStream_t st, double *part,
                          int32_t *counters);
 // Solve kernels: x and v are row-major with R columns (R right-hand sides), x in postorder.
 void launch_solve_assemble(const Tree &t, double *x, double *v, const int64_t *voff, int R,
-                           const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st);
+                           const RowTask *tasks, const int2 *ranges, int count, cudaStream_t st, bool pdl = false);
 // The thin supernodes' steps of a level; lg = log2 of the right-hand-side block (a power of two
 // <= 64 covering R, or 64).
 void launch_thin_fwd(const Tree &t, bool fp32, const double *x, double *x2, double *v, const int64_t *voff, int R,
-                     int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st);
+                     int lg, const ThinTask *tasks, const int4 *ranges, int count, cudaStream_t st, bool pdl = false);
 void launch_thin_bwd(const Tree &t, bool fp32, double *x, const double *x2, int R, int lg, const ThinBwdTask *tasks,
-                     double *part, int32_t *counters, int count, cudaStream_t st);
+                     double *part, int32_t *counters, int count, cudaStream_t st, bool pdl = false);
 // x_post[i*R + j] = b[perm[i] + j*ld] (times scale[i] if given) and back.
 void launch_permute_in(const int64_t *perm, int64_t n, const double *b, int64_t ld, double *x, int R,
                        const double *scale, cudaStream_t st);

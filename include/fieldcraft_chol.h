@@ -227,7 +227,11 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
  *                              its update matrix's children contributions summed first, beside
  *                              its panels, and its update product subtracts -L21 L21^T from them;
  *                              0: the product stores -L21 L21^T and the children are added after
- *                              it (re-plans the factorisation; the factor agrees to rounding). */
+ *                              it (re-plans the factorisation; the factor agrees to rounding).
+ *   FC_OPTION_SOLVE_PDL        1: the level-by-level solve's kernels are launched as programmatic
+ *                              dependents (each starts while the one before it in its stream
+ *                              finishes, loading its tasks and factor tiles before it waits for
+ *                              that kernel); 0 (default): ordinary launches. The same bits. */
 #define FC_OPTION_SOLVE_SCHEDULE 1
 #define FC_OPTION_WAIT_LIMIT_NS 2
 #define FC_OPTION_PLANT_UNMET_WAIT 3
@@ -238,6 +242,7 @@ int64_t fc_chol_stat(const fc_chol *h, int what);
 #define FC_OPTION_SOLVE_NARROW 8
 #define FC_OPTION_SOLVE_DEEP 9
 #define FC_OPTION_CHILDREN_FIRST 10
+#define FC_OPTION_SOLVE_PDL 11
 int fc_chol_option(fc_chol *h, int32_t option, int64_t value);
 /* The last traced persistent solve: 4 words per task, forward tasks then backward (fc_chol_stat 13
  * and 14 count them): taken, ready and done times in nanoseconds (%globaltimer), and kind << 32 |

@@ -171,6 +171,41 @@ def test_narrow_solve_tiles_give_the_same_bits(cuda, precision):
 
 
 @pytest.mark.parametrize("precision", [FP64, FP32_IR], ids=["fp64", "fp32_ir"])
+def test_programmatic_dependent_launches_give_the_same_bits(cuda, precision):
+    """The level-by-level solve's kernels start while their predecessors finish (programmatic
+    dependent launches, an option) and wait for them before touching the solve's vectors: on the
+    16^3 block, 1, 16 and 70 right-hand sides give the same bits as with ordinary launches, in the
+    captured graph (thin launches beside the wide ones on a second stream) and launched directly
+    with every launch timed (one stream)."""
+    torch = cuda
+    lib = _lib.load()
+    p = problems.lognormal_block(16, nrhs=1)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62), precision=precision)
+    f.factor(up.val)
+    rng = np.random.default_rng(11)
+    rhs = torch.from_numpy(rng.standard_normal((70, p.n))).cuda()
+
+    def solve(k):
+        x = rhs[:k].clone()
+        st = Status()
+        assert lib.fc_chol_solve_device(f.handle, C.c_void_p(x.data_ptr()), k, p.n, C.byref(st)) == 0, st.message
+        return x
+
+    for k in (1, 16, 70):
+        f.option(Factor.SOLVE_PDL, 1)
+        pdl = solve(k)
+        again = solve(k)
+        lib.fc_chol_profile(f.handle, 1)
+        direct = solve(k)
+        lib.fc_chol_profile(f.handle, 0)
+        f.option(Factor.SOLVE_PDL, 0)
+        plain = solve(k)
+        assert torch.equal(pdl, plain) and torch.equal(pdl, again) and torch.equal(pdl, direct), k
+    f.close()
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_IR], ids=["fp64", "fp32_ir"])
 def test_children_first_update_matrices(cuda, precision):
     """The wide supernodes' update matrices take their children's contributions first (beside the
     panels) and the update product subtracts from them (the default), or the product stores and
