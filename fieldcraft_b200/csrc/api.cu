@@ -1600,7 +1600,9 @@ void solve_offsets(const fc_chol *h, int R, SolvePlan &p) {
 
 // In a solve launch with too few output tiles to fill the GPU twice, a GEMM whose K is long is
 // split in chunks of SOLVE_KC: the chunks run as separate CTAs and the last one adds their
-// partials in order (GemmTask flag 8). The choice depends on the tiles of one block of 64
+// partials in order, in groups of SPLIT_GROUP chunks when there are more (GemmTask flag 8: with
+// the last chunk alone adding 30 partial tiles, a top supernode's backward product took twice its
+// main loop's time). The choice depends on the tiles of one block of 64
 // right-hand sides and on K, not on how many right-hand sides are solved together, so a column's
 // result does not either. Partials and counters are offsets into buffers given at launch, reused
 // launch after launch.
@@ -1648,8 +1650,9 @@ struct SplitPush {
         c.part_off = at, c.chunks = chunks, c.chunk = q, c.counter = (int32_t)p.tcount + cnt;
         p.gemm.push_back(c);
       }
-      at += (int64_t)chunks * 4096;
-      ++cnt;
+      // the chunks' partials, then the groups' sums; a counter for the sum and one a group
+      at += (int64_t)(chunks + fc::split_groups(chunks)) * 4096;
+      cnt += 1 + fc::split_groups(chunks);
     }
     p.psum = std::max(p.psum, at);
     p.scount = std::max<int64_t>(p.scount, cnt);

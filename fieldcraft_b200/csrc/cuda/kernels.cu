@@ -552,17 +552,68 @@ __device__ __forceinline__ void gemm_store(const GemmTask *tp, int flags, const 
   }
 }
 
-// The tile by the task's flags; for one chunk of a split sum (flag 8, FP64 C): its partial is
-// stored, and the last chunk to finish adds all the partials in chunk order (each thread over its
-// own fragment positions, a chunk's loads in flight together) and writes the total.
+// One chunk of a split sum (GemmTask flag 8): v[e] is this thread's value at position at[e] of
+// the 64 x 64 tile. Stores the chunk's partial and, in the CTA that finishes the sum, leaves the
+// total in v and returns true (false in every other CTA). Additions run in the order the split
+// fixes (chunks in order within a group, groups in order), each thread over its own positions
+// with a chunk's loads in flight together.
+template <int E>
+__device__ __forceinline__ bool split_sum(const GemmTask *tp, double *part, int32_t *counters, double (&v)[E],
+                                          const int (&at)[E]) {
+  __shared__ int last;
+  double *P = part + tp->part_off;
+  const int chunks = tp->chunks, groups = split_groups(chunks);
+  const int grp = groups ? tp->chunk / SPLIT_GROUP : 0;
+  const int q0 = groups ? grp * SPLIT_GROUP : 0, qn = groups ? min(SPLIT_GROUP, chunks - q0) : chunks;
+  // adds tiles [t0, t0 + tn) of `src` in order into v
+  auto add_tiles = [&](const double *src, int t0, int tn) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = 0.0;
+    for (int q = t0; q < t0 + tn; ++q) {
+      const double *Pq = src + (int64_t)q * 4096;
+      double u[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) u[e] = __ldcg(Pq + at[e]);
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] += u[e];
+    }
+  };
+  double *mine = P + (int64_t)tp->chunk * 4096;
+#pragma unroll
+  for (int e = 0; e < E; ++e) mine[at[e]] = v[e];
+  __threadfence();
+  __syncthreads();
+  int32_t *cnt = counters + tp->counter + (groups ? 1 + grp : 0);
+  if (threadIdx.x == 0) last = atomicAdd(cnt, 1) == qn - 1;
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  add_tiles(P, q0, qn);
+  if (threadIdx.x == 0) *cnt = 0;
+  if (!groups) return true;
+  double *sums = P + (int64_t)chunks * 4096;  // the groups' sums, after the chunks' partials
+#pragma unroll
+  for (int e = 0; e < E; ++e) sums[(int64_t)grp * 4096 + at[e]] = v[e];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counters + tp->counter, 1) == groups - 1;
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  add_tiles(sums, 0, groups);
+  if (threadIdx.x == 0) counters[tp->counter] = 0;
+  return true;
+}
+
+// The tile by the task's flags; for one chunk of a split sum (flag 8, FP64 C): split_sum, then the
+// CTA that finishes the sum writes the total.
 template <class T, class V>
 __device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)[2][4][4], int wm, int wn, int g,
                                               int tg, double *part = nullptr, int32_t *counters = nullptr) {
   if constexpr (sizeof(T) == sizeof(double)) {
     if (tp->flags & 8) {
-      __shared__ int last;
-      double *P = part + tp->part_off;
-      double *mine = P + (int64_t)tp->chunk * 4096;
+      double v[32];
+      int at[32];
 #pragma unroll
       for (int r = 0; r < 2; ++r)
 #pragma unroll
@@ -570,40 +621,17 @@ __device__ __forceinline__ void gemm_epilogue(const GemmTask *tp, const V (&acc)
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
-            mine[i * 64 + j] = acc[r][c][e];
+            v[(r * 4 + c) * 4 + e] = acc[r][c][e];
+            at[(r * 4 + c) * 4 + e] = i * 64 + j;
           }
-      __threadfence();
-      __syncthreads();
-      if (threadIdx.x == 0) last = atomicAdd(counters + tp->counter, 1) == tp->chunks - 1;
-      __syncthreads();
-      if (!last) return;
-      __threadfence();
+      if (!split_sum(tp, part, counters, v, at)) return;
       double tot[2][4][4];
 #pragma unroll
       for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c)
 #pragma unroll
-          for (int e = 0; e < 4; ++e) tot[r][c][e] = 0.0;
-      for (int q = 0; q < tp->chunks; ++q) {
-        const double *Pq = P + (int64_t)q * 4096;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          double v[4][4];
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int i = wm + r * 16 + g + 8 * (e >> 1), j = wn + c * 8 + 2 * tg + (e & 1);
-              v[c][e] = __ldcg(Pq + i * 64 + j);
-            }
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) tot[r][c][e] += v[c][e];
-        }
-      }
-      if (threadIdx.x == 0) counters[tp->counter] = 0;
+          for (int e = 0; e < 4; ++e) tot[r][c][e] = v[(r * 4 + c) * 4 + e];
       gemm_store<T>(tp, tp->flags & ~8, tot, wm, wn, g, tg);
       return;
     }
@@ -803,34 +831,20 @@ __global__ void __launch_bounds__(GEMM_THREADS, STAGES == GEMM_STAGES ? 6 : 2)
   // fragment element e of column block c: row wm + g + 8 (e >> 1), column 8 c + 2 tg + (e & 1)
   int flags = tp->flags;
   if (flags & 8) {
-    __shared__ int last;
-    double *P = part + tp->part_off;
-    double *mine = P + (int64_t)tp->chunk * 4096;
+    double v[NF * 4];
+    int at[NF * 4];
 #pragma unroll
     for (int c = 0; c < NF; ++c)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) mine[(wm + g + 8 * (e >> 1)) * 64 + c * 8 + 2 * tg + (e & 1)] = acc[c][e];
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(counters + tp->counter, 1) == tp->chunks - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    double tot[NF][4];
-#pragma unroll
-    for (int c = 0; c < NF; ++c) tot[c][0] = tot[c][1] = tot[c][2] = tot[c][3] = 0.0;
-    for (int q = 0; q < tp->chunks; ++q) {
-      const double *Pq = P + (int64_t)q * 4096;
-#pragma unroll
-      for (int c = 0; c < NF; ++c)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) tot[c][e] += __ldcg(Pq + (wm + g + 8 * (e >> 1)) * 64 + c * 8 + 2 * tg + (e & 1));
-    }
-    if (threadIdx.x == 0) counters[tp->counter] = 0;
+      for (int e = 0; e < 4; ++e) {
+        v[c * 4 + e] = acc[c][e];
+        at[c * 4 + e] = (wm + g + 8 * (e >> 1)) * 64 + c * 8 + 2 * tg + (e & 1);
+      }
+    if (!split_sum(tp, part, counters, v, at)) return;
 #pragma unroll
     for (int c = 0; c < NF; ++c)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc[c][e] = tot[c][e];
+      for (int e = 0; e < 4; ++e) acc[c][e] = v[c * 4 + e];
     flags &= ~8;
   }
   const int M = tp->M;

@@ -23,6 +23,13 @@ constexpr int ASSEMBLE_COLS = 8, ASSEMBLE_ROWS = 256, ASSEMBLE_THIN = 16;
 constexpr int ASSEMBLE_COLS_F32 = 16, ASSEMBLE_ROWS_F32 = 128;
 constexpr int ASSEMBLE_KIDS = 8;  // children whose ranges a tile keeps in shared memory (the rest: global)
 constexpr int SPLIT_K = 512;  // K chunk of the persistent solve's split products
+// Chunks of a split sum added by one CTA (GemmTask flag 8): a sum of more chunks is added in
+// groups of this many, then the groups' sums, each by the last CTA to finish its part.
+constexpr int SPLIT_GROUP = 8;
+// Counters and partial tiles (of 4096 doubles) that a split sum of `chunks` chunks takes.
+__host__ __device__ constexpr int split_groups(int chunks) {
+  return chunks > SPLIT_GROUP ? (chunks + SPLIT_GROUP - 1) / SPLIT_GROUP : 0;
+}
 // The solve applies the inverse of a supernode's diagonal block SB columns at a time: the inverses
 // of its diagonal blocks of up to SB columns are formed during the factorisation (from the 64 x 64
 // inverses of the panels, by doubling), so a solve step is a GEMM over SB columns, not a chain of
@@ -109,8 +116,13 @@ struct PanelTask {
 // 4 stores C = +sum. Flag 16 (FP64 B, unit j stride): B's row k is at B + b_rows[k] * b_sk (a
 // gather through a row list). Flag 8 (FP64 C only): this task is chunk `chunk` of `chunks` of one split
 // sum over K; each chunk stores its 64 x 64 partial at part + part_off + chunk * 4096 (`part`
-// given at launch), and the last chunk to finish (counters[counter], reset by it) adds the
-// partials in chunk order and applies the total to C by the other flags. No chunk waits.
+// given at launch). With at most SPLIT_GROUP chunks the last chunk to finish (counters[counter],
+// reset by it) adds the partials in chunk order and applies the total to C by the other flags.
+// With more, the chunks form groups of SPLIT_GROUP (the last group shorter): the last chunk of a
+// group to finish (counters[counter + 1 + group]) adds the group's partials in chunk order and
+// stores the group's sum after the partials (part_off + (chunks + group) * 4096); the last group
+// to finish (counters[counter]) adds the group sums in group order and applies the total. The
+// order of every addition is fixed by the split, whichever CTA finishes last. No chunk waits.
 struct GemmTask {
   void *C;
   const void *A;

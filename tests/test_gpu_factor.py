@@ -109,11 +109,14 @@ def test_solve_many_is_each_solve_bit_for_bit(cuda):
         assert np.array_equal(a.view(np.uint64), t.view(np.uint64))
 
 
-def test_split_solve_does_not_depend_on_how_many_are_solved(cuda):
+@pytest.mark.parametrize("n_el", [16, 24])
+def test_split_solve_does_not_depend_on_how_many_are_solved(cuda, n_el):
     """The 16^3 block's top separator (867 columns) makes the solve split its long GEMMs in chunks
-    whose last CTA adds the partials: a right-hand side's solution is still bit for bit the same
-    solved alone, among 5, and among 70 (two blocks of 64 right-hand sides)."""
-    csr = problems.lognormal_block(16, nrhs=1).csr
+    whose last CTA adds the partials; the 24^3 block's backward products over the rows below its
+    second-level separators take more chunks than one CTA adds (groups of chunks, then the groups'
+    sums): a right-hand side's solution is still bit for bit the same solved alone, among 5, and
+    among 70 (two blocks of 64 right-hand sides)."""
+    csr = problems.lognormal_block(n_el, nrhs=1).csr
     f = Factor.new(UpperColumns.from_symmetric(csr), 2**62)
     rng = np.random.default_rng(5)
     rhs = rng.standard_normal((70, csr.n))
