@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-nn", action="store_true", help="skip the learned-preconditioner measurement")
     ap.add_argument("--nn-pairs", type=int, default=256, help="training pairs of the headline's learned preconditioner")
     ap.add_argument("--nn-epochs", type=int, default=3, help="training epochs of the learned preconditioner")
+    ap.add_argument("--nn-plate", type=int, default=64, metavar="N",
+                    help="the headline line's learned preconditioner on an N x N x 8 plate (the config-5 "
+                         "workload at N = 128) with on-policy training; 0: on the headline's own K")
     ap.add_argument("--profile-kernels", choices=["fp32-factor", "unet"], default=None,
                     help="a short run for a profiler: two FP32 factorisations of the --n-el block, or the "
                          "U-Net's forward and backward passes on a 64x64x8 plate, twice")
@@ -273,6 +276,42 @@ def oracle_spmv(w, x):
     return oracle.spmv(w.n, w.ptr, w.idx, w.val, x)
 
 
+def nn_plate_block(size: int, torch, lib) -> dict:
+    """nn_fcg_block on the size x size x 8 plate (problems.plate: the config-5 workload at 128):
+    1 000 Cholesky pairs for 8 epochs, then three on-policy rounds of 24 right-hand sides x 9
+    snapshots for 4 epochs each, a 3-level network, two held-out right-hand sides. On the 128 x 128
+    x 8 plate itself the same schedule left the loss near 0.6 and the network was dropped."""
+    from fieldcraft_b200 import Factor, Symbolic, problems
+    p = problems.plate(size, size, 8, nrhs=2)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62))
+    n = p.n
+    d_val = torch.from_numpy(up.val).cuda()
+    csr = tuple(torch.from_numpy(a).cuda() for a in (p.csr.ptr, p.csr.idx, p.csr.val))
+    b = torch.from_numpy(np.ascontiguousarray(p.rhs[:, 0])).cuda()
+    stream = torch.cuda.Stream()
+    f.set_stream(stream.cuda_stream)
+    tt = []
+    for _ in range(3):
+        x = b.clone()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            assert lib.fc_chol_factor_device_async(f.handle, C.c_void_p(d_val.data_ptr()), up.val.size) == 0
+            assert lib.fc_chol_solve_device_async(f.handle, C.c_void_p(x.data_ptr()), 1, n) == 0
+        e1.record(stream)
+        e1.synchronize()
+        tt.append(e0.elapsed_time(e1))
+    f.set_stream(None)
+    out = nn_fcg_block(p, f, csr, torch, pairs=1000, epochs=8, cols=[0, 1], cap=3000, chol_ms=float(np.min(tt[1:])),
+                       batch=16, levels=3, lr=3e-4, rounds=3, round_rhs=24, round_epochs=4, round_lr=2e-4)
+    out["problem"] = (f"plate {size}x{size}x8 (n = {n}), E a lognormal random field (contrast 100), side faces "
+                      f"clamped, held-out random top-face pressures")
+    f.close()
+    return out
+
+
 def nn_levels(p) -> int:
     """U-Net levels for a box problem's node grid: pooling until the longest side is about 8 nodes."""
     longest = max(p.dims) + 1
@@ -284,14 +323,17 @@ def nn_levels(p) -> int:
 
 
 def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap: int, chol_ms: float,
-                 batch: int = 8, levels: int | None = None) -> dict:
+                 batch: int = 8, levels: int | None = None, lr: float = 1e-3, rounds: int = 0, round_rhs: int = 24,
+                 round_epochs: int = 4, round_lr: float = 2e-4) -> dict:
     """The learned preconditioner on the same K: pairs (r, K^-1 r) from the Cholesky solve, minibatch
-    Adam training on the GPU of a U-Net whose output is added to K's nodal block-Jacobi part, then
-    flexible CG to rel-res 1e-10 from zero on held-out right-hand sides with the network ('nn_fcg'),
-    with the block-Jacobi part alone ('bj') and with no preconditioner ('cg'), all capped at `cap`
-    iterations with the Cholesky solve as fallback; each timed on its second run. chol_ms: the FP64 Cholesky's time for one
-    right-hand side (factor + solve) on the same K."""
-    from fieldcraft_b200.unet import UNet, fcg, output_scale, train, training_pairs
+    Adam training on the GPU of a U-Net whose output is added to K's nodal block-Jacobi part (then
+    `rounds` on-policy rounds: pairs from the residuals of the network's own Krylov solve, see
+    train_on_policy), then flexible CG to rel-res 1e-10 from zero on held-out right-hand sides with
+    the network ('nn_fcg'), with the block-Jacobi part alone ('bj') and with no preconditioner
+    ('cg'), all capped at `cap` iterations with the Cholesky solve as fallback; each timed on its
+    second run. chol_ms: the FP64 Cholesky's time for one right-hand side (factor + solve) on the
+    same K."""
+    from fieldcraft_b200.unet import UNet, fcg, output_scale, train, train_on_policy, training_pairs
     levels = levels or nn_levels(p)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -299,7 +341,11 @@ def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     net = UNet(p, seed=0, kref=output_scale(R, E), levels=levels, operator=csr_dev)
-    losses = train(net, R, E, epochs=epochs, lr=1e-3, torch=torch, csr_device=csr_dev, batch=batch, warmup=50)
+    losses = train(net, R, E, epochs=epochs, lr=lr, torch=torch, csr_device=csr_dev, batch=batch, warmup=50)
+    round_losses = []
+    if rounds:
+        R, E, round_losses = train_on_policy(net, factor64, p, csr_dev, R, E, rounds, round_rhs, round_epochs,
+                                             round_lr, torch, batch=batch, seed=SEED)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     del R, E
@@ -333,8 +379,10 @@ def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap
     return {"value": float(np.mean(nn_s)), "unit": UNIT,
             "speedup_vs_fp64": (chol_ms / 1e3) / float(np.mean(nn_s)),
             "speedup_vs_cg": float(np.mean([r["cg"]["s"] for r in runs])) / float(np.mean(nn_s)),
-            "fp64_cholesky_1rhs_s": chol_ms / 1e3, "pairs": pairs, "epochs": epochs, "batch": batch,
+            "fp64_cholesky_1rhs_s": chol_ms / 1e3, "pairs": pairs, "epochs": epochs, "batch": batch, "lr": lr,
             "levels": levels, "pairs_s": t1 - t0, "train_s": t2 - t1, "loss_by_epoch": losses, "cap": cap,
+            "on_policy_rounds": rounds, "on_policy_pairs_per_round": round_rhs * 9 if rounds else 0,
+            "on_policy_epochs": round_epochs if rounds else 0, "on_policy_loss_by_round": round_losses,
             "rhs": runs,
             "what": f"{levels}-level 32-channel BF16 3D-conv U-Net added to K's nodal block-Jacobi inverse, trained "
                     "(energy-norm loss, minibatch Adam) on pairs from the Cholesky solve; flexible CG (4 kept "
@@ -1013,9 +1061,14 @@ def main():
     e2e_res = float(((d_r - d_f).norm(dim=1) / fnorm).max().item())
 
     stats = {"supernodes": f.stat(4), "levels": f.stat(0), "l_bytes": f.stat(2)}
-    # the learned preconditioner on the same K (a short training; see nn_fcg_block)
+    # the learned preconditioner: on a plate with on-policy training (nn_plate_block), or on the
+    # same K (a short training; see nn_fcg_block)
     nn = None
-    if not args.no_nn:
+    if not args.no_nn and args.nn_plate:
+        f.set_stream(None)
+        nn = nn_plate_block(args.nn_plate, torch, lib)
+        f.set_stream(stream.cuda_stream)
+    elif not args.no_nn:
         b1 = d_f[0:1].clone()
         tt = []
         for it in range(3):

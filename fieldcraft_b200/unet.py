@@ -243,6 +243,60 @@ def krylov_pairs(factor: Factor, problem: Problem, csr_device, count: int, seed:
     return R, E
 
 
+def policy_pairs(net: UNet, factor: Factor, problem: Problem, csr_device, nrhs: int, seed: int, torch,
+                 snapshots=(1, 2, 3, 5, 8, 12, 20, 30, 45)):
+    """Pairs (r, K^-1 r) whose r are the residuals that conjugate gradients preconditioned by the
+    network's current M (block Jacobi plus the network) leaves at the iterations `snapshots` on
+    `nrhs` random top-face pressures: the inputs the network meets inside its own Krylov solve,
+    which change as it learns. Each r of unit norm; e from the Cholesky solve. Returns two CUDA
+    tensors [nrhs * len(snapshots), n] (FP64)."""
+    from .problems import top_pressures
+    lib = _lib.load()
+    n = problem.n
+    ptr, idx, val = csr_device
+    B = torch.from_numpy(np.ascontiguousarray(top_pressures(problem, nrhs, seed).T)).cuda()
+    rec = []
+    z = torch.empty(n, dtype=torch.float64, device="cuda")
+    q = torch.empty_like(z)
+    for j in range(nrhs):
+        r = B[j].clone()
+        net.apply(r, z)
+        d = z.clone()
+        rz = float(r @ z)
+        for it in range(1, max(snapshots) + 1):
+            lib.fc_csr_spmv_device(n, _p(ptr), _p(idx), _p(val), _p(d), _p(q), 1, n, None)
+            r -= (rz / float(d @ q)) * q
+            if it in snapshots:
+                rec.append(r / torch.linalg.vector_norm(r))
+            net.apply(r, z)
+            rz_new = float(r @ z)
+            d = z + (rz_new / rz) * d
+            rz = rz_new
+    R = torch.stack(rec)
+    E = R.clone()
+    for s in range(0, R.shape[0], 64):
+        e = min(R.shape[0], s + 64)
+        factor.solve_device(E[s:e], e - s, n)
+    torch.cuda.synchronize()
+    return R, E
+
+
+def train_on_policy(net: UNet, factor: Factor, problem: Problem, csr_device, R, E, rounds: int, nrhs: int,
+                    epochs: int, lr: float, torch, batch: int = 16, seed: int = 0):
+    """`rounds` rounds of: pairs from the network's own Krylov residuals (policy_pairs) added to the
+    training set (R, E), then `epochs` passes over the whole set. A network trained on the
+    Cholesky pairs alone can make flexible CG diverge on the residuals it meets after a few
+    iterations; these rounds teach it those. Returns (R, E, each round's last-epoch loss)."""
+    losses = []
+    for rd in range(rounds):
+        Rn, En = policy_pairs(net, factor, problem, csr_device, nrhs, seed + 100 + rd, torch)
+        R = torch.cat([R, Rn])
+        E = torch.cat([E, En])
+        losses.append(train(net, R, E, epochs=epochs, lr=lr, torch=torch, csr_device=csr_device, batch=batch,
+                            warmup=20, seed=seed + 1 + rd)[-1])
+    return R, E, losses
+
+
 def output_scale(R, E) -> float:
     """The network's output scale for pairs (r, K^-1 r): the median of ||r|| / ||e||, so that the
     network's outputs are of order one."""

@@ -181,3 +181,38 @@ def test_fcg_falls_back_to_cholesky(cuda):
     from fieldcraft_b200 import Timeout
     with pytest.raises(Timeout):
         fcg(csr, b, torch.zeros_like(b), net=None, fallback=None, tol=1e-10, max_iter=3)
+
+
+def test_on_policy_pairs_and_rounds(cuda):
+    """policy_pairs takes the residuals of the network's own preconditioned CG at the snapshot
+    iterations: unit norm, and each e solves K e = r (the Cholesky solve); an untrained network is
+    block-Jacobi PCG, so its residuals are that solver's. A train_on_policy round adds those pairs
+    to the set and trains on all of it."""
+    torch = cuda
+    from fieldcraft_b200 import _lib
+    from fieldcraft_b200.unet import UNet, output_scale, policy_pairs, train_on_policy, training_pairs
+    import ctypes as C
+    p = problems.plate(24, 24, 4, corr=4.0, contrast=100.0, seed=9, nrhs=2)
+    up = p.upper()
+    f = Factor(Symbolic(up, 2**62))
+    f.factor(up.val)
+    csr = tuple(torch.from_numpy(a).cuda() for a in (p.csr.ptr, p.csr.idx, p.csr.val))
+    R, E = training_pairs(f, p, 64, seed=3, torch=torch)
+    net = UNet(p, seed=0, kref=output_scale(R, E), levels=3, operator=csr)
+    snaps = (1, 3, 8)
+    Rp, Ep = policy_pairs(net, f, p, csr, 4, seed=21, torch=torch, snapshots=snaps)
+    assert Rp.shape == (4 * len(snaps), p.n) and Ep.shape == Rp.shape
+    assert torch.allclose(torch.linalg.vector_norm(Rp, dim=1), torch.ones(Rp.shape[0], dtype=Rp.dtype, device="cuda"))
+    KE = torch.empty_like(Ep[0])
+    lib = _lib.load()
+    for k in range(Rp.shape[0]):
+        lib.fc_csr_spmv_device(p.n, *(C.c_void_p(a.data_ptr()) for a in csr), C.c_void_p(Ep[k].data_ptr()),
+                               C.c_void_p(KE.data_ptr()), 1, p.n, None)
+        assert float(torch.linalg.vector_norm(KE - Rp[k])) <= 1e-9
+    # later snapshots of one solve are residuals of a converging solver: different directions
+    assert abs(float(Rp[0] @ Rp[2])) < 0.99
+    R2, E2, losses = train_on_policy(net, f, p, csr, R, E, rounds=1, nrhs=2, epochs=1, lr=2e-4, torch=torch,
+                                     batch=8)
+    assert R2.shape[0] == 64 + 2 * 9 and E2.shape == R2.shape and len(losses) == 1 and np.isfinite(losses[0])
+    net.close()
+    f.close()
