@@ -974,6 +974,7 @@ def main():
             print(json.dumps({"profile_only": True, "n": n, "gemm_factor_launches": int(cnt_k[3]),
                               "gemm_big_ordinal": f.stat(11), "gemm_trail_ordinal": f.stat(12),
                               "gemm_solve_launches": int(cnt_k[19]), "panel_launches": int(cnt_k[1]),
+                              "gemm_useful_flops_factor": f.stat(9) + f.stat(10),
                               "relres_max": float(relres.max().item())}), flush=True)
         f.close()
         if world > 1:
