@@ -330,8 +330,8 @@ def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap
     `rounds` on-policy rounds: pairs from the residuals of the network's own Krylov solve, see
     train_on_policy), then flexible CG to rel-res 1e-10 from zero on held-out right-hand sides with
     the network ('nn_fcg'), with the block-Jacobi part alone ('bj') and with no preconditioner
-    ('cg'), all capped at `cap` iterations with the Cholesky solve as fallback; each timed on its
-    second run. chol_ms: the FP64 Cholesky's time for one right-hand side (factor + solve) on the
+    ('cg'), all capped at `cap` iterations with the Cholesky solve as fallback; each the median of
+    three timed runs after an untimed one. chol_ms: the FP64 Cholesky's time for one right-hand side (factor + solve) on the
     same K."""
     from fieldcraft_b200.unet import UNet, fcg, output_scale, train, train_on_policy, training_pairs
     levels = levels or nn_levels(p)
@@ -359,16 +359,21 @@ def nn_fcg_block(p, factor64, csr_dev, torch, pairs: int, epochs: int, cols, cap
             if use is not None:
                 use.enable(on)
             # one untimed run first (first-call set-up, clocks up after the host-side phases), then
-            # the timed one
-            for timed in (False, True):
+            # three timed ones, their median reported (the solve synchronises with the host every
+            # few iterations, so one stall of the host shows in a single run)
+            times = []
+            for timed in (False, True, True, True):
                 x = torch.zeros_like(b)
                 torch.cuda.synchronize()
                 ta = time.perf_counter()
                 it, rel, fb = fcg(csr_dev, b, x, net=use, fallback=factor64, tol=1e-10, max_iter=cap, keep=4)
                 torch.cuda.synchronize()
-                dt = time.perf_counter() - ta
+                if timed:
+                    times.append(time.perf_counter() - ta)
+            dt = float(np.median(times))
             err = float((torch.linalg.vector_norm(x - exact) / torch.linalg.vector_norm(exact)).item())
-            row[name] = {"iterations": it, "s": dt, "relres": rel, "fallback": fb, "err_vs_cholesky": err}
+            row[name] = {"iterations": it, "s": dt, "s_runs": times, "relres": rel, "fallback": fb,
+                         "err_vs_cholesky": err}
             if name == "nn_fcg":
                 row[name]["network_iterations"] = net.stat(1)
                 row[name]["network_dropped"] = bool(net.stat(2))
